@@ -1,0 +1,327 @@
+"""Benchmark: IMC track segments per second on the 2-D RZ crooked-pipe time step.
+
+One "step" is one full implicit Monte Carlo time step of the 60x210 crooked pipe
+(2e6 source particles per step, census combed to 6.67e6): Fleck factor, boundary and
+emission sources, tracking of the whole bank to census, material update, comb.
+
+  value   track segments/s with the whole step on the device (device material callables),
+          inputs resident in HBM; timed with CUDA events on the launching stream.
+  e2e     the same metric through the drop-in API (radtranbook_b200.imc2d.step) with the
+          reference driver's NumPy material callables: host evaluation of sigma / cv /
+          inv_eos and the host copies of T, Tr, e every step are inside the timed region.
+  roofline  tracking kernel: algorithmic bytes = 72 B per 2-D segment (one 36-byte particle
+          record loaded and stored per segment) x segments / kernel time (CUDA events in the
+          library around the tracking launch), against the measured HBM copy bandwidth.
+  cpu_baseline  the FP64 CPU oracle (a C++ port of the reference step, OpenMP over all host
+          threads) on a reduced-particle sample of the same problem.
+
+--impl reference runs that CPU port as the reference arm.  With --gpus N > 1 (torchrun),
+each rank runs an independent replica (own Philox key, full per-GPU particle count) and the
+per-cell tallies are averaged with one NCCL all-reduce per step ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "IMC track-segments/s and FOM=1/(rel.var*time) on 1 B200: plain vs batched/adjoint"
+UNIT = "track-segments/s"
+B_SEG_2D = 72  # bytes per 2-D gray segment: 36-byte record loaded + stored
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self):
+        if not getattr(self, "out", ""):
+            return None
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_oracle_run(scale: float, steps: int, warmup: int, nthreads: int):
+    """Crooked pipe on the FP64 CPU oracle at `scale` x the particle counts."""
+    from oracle import oracle as O
+    from radtranbook_b200 import problems
+
+    p = problems.crooked_pipe(scale=scale)
+    e1, e2 = p["edges1"], p["edges2"]
+    vol = O.flat2d(np.pi * (e1[1:] ** 2 - e1[:-1] ** 2)[:, None] * np.diff(e2)[None, :])
+    rc = 0.5 * (e1[:-1] + e1[1:])
+    face = [None, None, np.where(rc < 0.5, 0.5, 0.0), None]
+    run = O.OracleGray("rz", e1, e2, vol, 0x5EED0001, p["Ntarget"], p["Tinit"], p["Tr_init"], p["eos_host"],
+                       p["inv_eos_host"], nthreads=nthreads)
+    kw = dict(Ntarget=p["Ntarget"], Nboundary=p["Nboundary"], Nsource=0, Nmax=p["Nmax"], face_T=face, dt=p["dt"],
+              sigma_a_func=p["sigma_host"], inv_eos=p["inv_eos_host"], cv=p["cv_host"], reflect=p["reflect"],
+              max_events=1_000_000)
+    for _ in range(warmup):
+        run.step(**kw)
+    seg = 0
+    hist = 0
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        r = run.step(**kw)
+        seg += int(r["stats"][0])
+        hist += int(r["n_transported"])
+    dt = time.perf_counter() - t0
+    return seg / dt, hist / dt, dt, seg
+
+
+def run_reference(args, rank: int, world: int):
+    if rank != 0:
+        return
+    nthreads = os.cpu_count() or 1
+    scale = args.cpu_scale
+    per_step = []
+    segs = 0
+    # each step: one bounded sample of the workload (the crooked pipe at scale x particles)
+    v, h, dt, seg = cpu_oracle_run(scale, args.steps, args.warmup, nthreads)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt / max(args.steps, 1) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "crooked_pipe_rz_60x210", "source_particles_per_step": int(round(2e6 * scale)),
+                   "nmax": int(round(6.67e6 * scale)), "sample_scale": scale},
+        "histories_per_s": h,
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port",
+                         "sample": f"crooked pipe, {scale:g} x particles ({int(round(2e6 * scale))} src/step), "
+                                   f"{args.warmup} warm-up + {args.steps} timed steps, FP64 C++ oracle, OpenMP"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def _gpu_steps(p, state, steps, use_device, dist=None):
+    """Run `steps` drop-in steps; return (segments, histories)."""
+    from radtranbook_b200 import imc2d
+
+    sig = p["sigma_dev"] if use_device else p["sigma_host"]
+    cv = p["cv_dev"] if use_device else p["cv_host"]
+    inv = p["inv_eos_dev"] if use_device else p["inv_eos_host"]
+    seg = hist = 0
+    for _ in range(steps):
+        state, info = imc2d.step(state, p["Ntarget"], p["Nboundary"], 0, p["Nmax"], p["T_boundary"], p["dt"],
+                                 p["edges1"], p["edges2"], sig, inv, cv, p["source"], reflect=p["reflect"],
+                                 geometry="rz", boundary_source_func=p["boundary_source_func"],
+                                 _allreduce=dist)
+        te = info["profiling"]["transport_events"]
+        seg += te["total"]
+        hist += te["n_particles_transported"]
+    return state, seg, hist, info
+
+
+def run_ours(args, rank: int, world: int):
+    import torch
+
+    from radtranbook_b200 import _lib, imc2d, problems
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    lib = _lib.load()
+    dist = None
+    if world > 1:
+        import torch.distributed as td
+
+        dist = td
+    p = problems.crooked_pipe(scale=args.scale)
+    seed = 0x5EED0001 + 0x1000003 * rank
+
+    def fresh():
+        return imc2d.init_simulation(p["Ntarget"], p["Tinit"], p["Tr_init"], p["edges1"], p["edges2"], p["eos_dev"],
+                                     p["inv_eos_dev"], geometry="rz", seed=seed)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---------------- device-resident value ----------------
+    state = fresh()
+    state, _, _, _ = _gpu_steps(p, state, args.warmup, True, dist)
+    eng = state._engine
+    barrier()
+    s0 = torch.cuda.Event(enable_timing=True)
+    s1 = torch.cuda.Event(enable_timing=True)
+    launches0 = lib.imc_kernel_launches()
+    track_ms = []
+    segs_per_step = []
+    clocks = ClockSampler(dev.index)
+    with clocks:
+        s0.record()
+        seg = hist = 0
+        for _ in range(args.steps):
+            state, sg, hs, info = _gpu_steps(p, state, 1, True, dist)
+            seg += sg
+            hist += hs
+            track_ms.append(info["profiling"]["phase_times_s"]["transport"] * 1e3)
+            segs_per_step.append(sg)
+        s1.record()
+        barrier()
+    launches = lib.imc_kernel_launches() - launches0
+    ms = s0.elapsed_time(s1)
+    tmax = ms
+    if dist is not None:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tmax = float(t.item())
+        tot = torch.tensor([float(seg), float(hist)], device=dev, dtype=torch.float64)
+        dist.all_reduce(tot)
+        seg_all, hist_all = float(tot[0]), float(tot[1])
+    else:
+        seg_all, hist_all = float(seg), float(hist)
+    value = seg_all / (tmax * 1e-3)
+
+    # ---------------- end to end through the drop-in API with host callables ----------------
+    state2 = fresh()
+    state2, _, _, _ = _gpu_steps(p, state2, args.warmup, False, dist)
+    barrier()
+    tr0 = dict(_lib.TRANSFER)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    state2, seg2, hist2, _ = _gpu_steps(p, state2, args.steps, False, dist)
+    e1.record()
+    barrier()
+    ms2 = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms2], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms2 = float(t.item())
+        t2 = torch.tensor([float(seg2)], device=dev, dtype=torch.float64)
+        dist.all_reduce(t2)
+        seg2 = float(t2.item())
+    h2d = (_lib.TRANSFER["h2d"] - tr0["h2d"]) / args.steps
+    d2h = (_lib.TRANSFER["d2h"] - tr0["d2h"]) / args.steps
+    e2e = seg2 / (ms2 * 1e-3)
+
+    if rank != 0:
+        return
+    peak, peak_kind = measured_peaks()
+    # dominant kernel: tracking.  per-launch average over the timed steps
+    seg_per_launch = float(np.mean(segs_per_step))
+    t_launch = float(np.mean(track_ms)) * 1e-3
+    achieved = B_SEG_2D * seg_per_launch / t_launch / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": None, "kernel": "k_track<RZ>", "peak_source": peak_kind,
+            "segments_per_launch": seg_per_launch, "bytes_per_segment_algorithmic": B_SEG_2D,
+            "track_ms_per_launch": t_launch * 1e3}
+    cpu = None
+    if not args.no_cpu_baseline:
+        v, h, dtc, _ = cpu_oracle_run(args.cpu_scale, args.cpu_steps, 1, os.cpu_count() or 1)
+        cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+               "sample": f"crooked pipe, {args.cpu_scale:g} x particles, 1 warm-up + {args.cpu_steps} timed steps, "
+                         f"FP64 C++ oracle, OpenMP ({dtc:.1f} s)", "histories_per_s": h}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": tmax / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "crooked_pipe_rz_60x210", "source_particles_per_step": p["Ntarget"] + p["Nboundary"],
+                   "nmax": p["Nmax"], "scale": args.scale, "precision": "f32 tracking, f64 tallies/ledger",
+                   "l2": "bank of ~8.7e6 particles x 32 B > 126 MB L2 (inputs larger than L2)",
+                   "parallelism": f"replicas{world}" if world > 1 else "single"},
+        "histories_per_s": hist_all / (tmax * 1e-3),
+        "segments_per_step": seg_all / args.steps,
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches),
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=float, default=1.0, help="particle-count scale of the workload")
+    ap.add_argument("--cpu-scale", type=float, default=0.02)
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as td
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        try:
+            run_ours(args, rank, world)
+        finally:
+            td.destroy_process_group()
+    else:
+        run_ours(args, rank, world)
+
+
+if __name__ == "__main__":
+    main()

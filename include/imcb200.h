@@ -1,0 +1,191 @@
+/*
+ * imcb200.h — C ABI of the B200 implicit Monte Carlo (Fleck-Cummings) time-step engine.
+ *
+ * The reference (DrRyanMc/RadTranBook) exposes its time step as Python functions; the
+ * calls below are what a binding of those functions needs, split where the reference
+ * hands control back to user material callables:
+ *
+ *   IMC/IMC1D.py:908    step(state, Ntarget, Nboundary, Nsource, NMax, T_boundary, dt, mesh,
+ *                            sigma_a_func, inv_eos, cv, source, reflect, theta, ...)
+ *   IMC/IMC2D.py:1591   step(state, ..., edges1, edges2, ..., geometry='xy'|'rz', ...)
+ *   MG_IMC/MG_IMC2D.py:1635  step(state, ..., energy_edges, sigma_a_funcs, ...)
+ *
+ *   imc_step_transport  = reference lines from the Fleck factor through the transport
+ *                         kernel (IMC/IMC1D.py:932-1017, IMC/IMC2D.py:1646-1797,
+ *                         MG_IMC/MG_IMC2D.py:1703-1976)
+ *   imc_material_update = internal_energy += dep - emitted / V; Tr from the path-length
+ *                         intensity (IMC/IMC1D.py:1021-1035, IMC/IMC2D.py:1801-1810)
+ *   imc_comb            = the stochastic comb (IMC/IMC1D.py:770-828, IMC/IMC2D.py:1448-1511,
+ *                         MG_IMC/MG_IMC2D.py:1314-1378)
+ *   imc_init_census     = the equilibrium initial census of init_simulation
+ *                         (IMC/IMC1D.py:220-248,535-575; IMC/IMC2D.py:1110-1188)
+ *
+ * Conventions
+ *   - Every pointer in a struct is DEVICE memory, caller-owned.  The library never
+ *     allocates or frees; scratch lives in a caller-provided workspace of
+ *     imc_workspace_bytes() bytes (256-byte aligned).
+ *   - All work is stream-ordered on the cudaStream_t passed in (a CUstream is accepted).
+ *     Calls that return sizes synchronise that stream before returning.
+ *   - Errors are returned as imc_status; nothing throws across the ABI.
+ *   - Cells are flattened c = i + nx*j (1-D: ny = 1).  Multigroup arrays are [g][c].
+ *   - Particle state is FP32 (tracking precision); tallies, energies and the ledger are
+ *     FP64.
+ */
+#ifndef IMCB200_H
+#define IMCB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define IMC_API __attribute__((visibility("default")))
+#else
+#define IMC_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum imc_status {
+  IMC_OK = 0,
+  IMC_ERR_BANK_OVERFLOW = 1,   /* report.required_capacity says how much is needed */
+  IMC_ERR_EVENT_CAP = 2,       /* safety cap on events per history reached */
+  IMC_ERR_NONFINITE = 3,       /* NaN/Inf or non-positive temperature in inputs */
+  IMC_ERR_BAD_GEOMETRY = 4,    /* unknown geometry / inconsistent mesh */
+  IMC_ERR_TIMEOUT = 5,         /* a bounded device wait gave up */
+  IMC_ERR_CUDA = 6,            /* CUDA runtime error (see imc_last_cuda_error) */
+  IMC_ERR_INVALID_ARG = 7,
+  IMC_ERR_WORKSPACE = 8        /* workspace too small */
+} imc_status;
+
+enum { IMC_GEOM_SLAB = 0, IMC_GEOM_SPHERE = 1, IMC_GEOM_XY = 2, IMC_GEOM_RZ = 3 };
+
+/* statistics slots (uint64) */
+enum {
+  IMC_STAT_EVENTS = 0, IMC_STAT_BOUNDARY = 1, IMC_STAT_SCATTER = 2, IMC_STAT_CENSUS = 3,
+  IMC_STAT_CAPTURE = 4, IMC_STAT_FLOOR = 5, IMC_STAT_REFLECT = 6, IMC_STAT_CAP = 7,
+  IMC_STAT_ESCAPE = 8, IMC_STAT_N = 9
+};
+
+typedef struct imc_mesh {
+  int32_t geometry;        /* IMC_GEOM_* */
+  int32_t nx, ny;          /* cells per direction; ny = 1 in 1-D */
+  int32_t n_groups;        /* 1 = gray */
+  const double* edges1;    /* nx+1 (x | r) */
+  const double* edges2;    /* ny+1 (y | z); 1-D: {0, 1} */
+  const double* volume;    /* nx*ny cell volumes (1-D slab: dx; sphere: 4/3 pi dr^3) */
+  const double* group_edges; /* n_groups+1 photon energies (keV), MG only */
+} imc_mesh;
+
+typedef struct imc_bank {  /* structure-of-arrays particle bank */
+  float* pos1;             /* x | r */
+  float* pos2;             /* y | z (unused in 1-D) */
+  float* dir1;             /* mu | u_x | mu_perp */
+  float* dir2;             /* u_y | eta (unused in 1-D) */
+  float* weight;           /* energy weight (GJ); 0 = dead */
+  float* time;             /* birth time within the step (ns); census = 0 */
+  int32_t* cell;           /* flat cell */
+  int32_t* group;          /* photon group (MG) or NULL */
+  int64_t size;            /* live entries (host-side count) */
+  int64_t capacity;
+} imc_bank;
+
+typedef struct imc_material {   /* per-cell state at the start of the step (FP64) */
+  const double* temperature;    /* T (keV), [c] */
+  const double* sigma;          /* true absorption opacity (1/cm), [g][c] */
+  const double* cv;             /* rho c_v (GJ/cm^3/keV), [c] */
+  const double* source;         /* fixed source power density, [c], or NULL */
+} imc_material;
+
+typedef struct imc_step_params {
+  uint64_t seed;                /* Philox key */
+  uint32_t step;                /* time-step index (Philox counter word 2) */
+  int32_t reflect[4];           /* -dir1, +dir1, -dir2, +dir2 faces */
+  double dt, theta;
+  int64_t n_target, n_boundary, n_source;
+  const double* face_T[4];      /* per-face-cell boundary temperatures or NULL
+                                   (sides 0/1: ny entries, 2/3: nx entries; 1-D: 1) */
+  int64_t max_events;           /* events per history cap (2-D reference); <= 0: none */
+  int32_t rz_linear_source;     /* RZ emission with the linear r/z tilt */
+  int32_t mg_reference_rules;   /* MG: MG_IMC2D event rules (no scatter cap) */
+  double t_emit_floor;
+  int32_t block_size;           /* tracking launch shape; 0 = tuned default */
+  int32_t blocks_per_sm;
+  int32_t chunk;                /* histories claimed per warp ticket */
+  int32_t reserved;
+} imc_step_params;
+
+typedef struct imc_tallies {    /* device outputs, overwritten by each step */
+  double* dep;                  /* [g][c] energy deposited per unit volume */
+  double* si;                   /* [g][c] path-length scalar intensity */
+  double* emitted;              /* [c] emission energy issued from matter (GJ) */
+  double* sigma_a;              /* [g][c] Fleck absorption (out) */
+  double* sigma_s;              /* [g][c] effective scatter (out) */
+  double* escaped;              /* [4 + n_groups] escaped energy by side, then by group */
+  unsigned long long* stats;    /* [IMC_STAT_N] */
+} imc_tallies;
+
+typedef struct imc_step_report {  /* host-side summary of imc_step_transport */
+  int64_t n_boundary, n_source, n_emission;
+  int64_t n_transported;
+  int64_t required_capacity;
+  double boundary_emission, source_emission, emission_total;
+  double weight_floor;
+  float ms_sources, ms_transport;  /* device time of source fill and of tracking */
+} imc_step_report;
+
+typedef struct imc_comb_report {
+  int64_t n_in, n_out;
+  int64_t required_capacity;
+  double energy_before, energy_after;
+} imc_comb_report;
+
+/* Workspace bytes for a mesh and a bank capacity. */
+IMC_API size_t imc_workspace_bytes(const imc_mesh* mesh, int64_t bank_capacity);
+
+/* Equilibrium initial census at radiation temperature tr[c] into an empty bank.
+ * (IMC/IMC1D.py:220-248, IMC/IMC2D.py:1110-1188, MG_IMC/MG_IMC2D.py:992-1235) */
+IMC_API imc_status imc_init_census(const imc_mesh* mesh, const double* tr, int64_t n_target,
+                           double t_emit_floor, uint64_t seed, imc_bank* bank, void* workspace,
+                           size_t workspace_bytes, int64_t* n_out, void* stream);
+
+/* Fleck factor, boundary / fixed / emission sources appended to the bank in the
+ * reference's order, then tracking of the whole bank to census.  Tallies are zeroed
+ * and written.  Returns IMC_ERR_BANK_OVERFLOW (bank untouched) when the sources do not
+ * fit; report->required_capacity says how much does. */
+IMC_API imc_status imc_step_transport(const imc_mesh* mesh, const imc_material* mat,
+                              const imc_step_params* par, imc_bank* bank, imc_tallies* tal,
+                              void* workspace, size_t workspace_bytes, imc_step_report* report,
+                              void* stream);
+
+/* e[c] += sum_g dep[g][c] - emitted[c]/V[c]; tr[c] = (sum_g si[g][c] / (a c))^(1/4). */
+IMC_API imc_status imc_material_update(const imc_mesh* mesh, const imc_tallies* tal, double* e,
+                               double* tr, void* stream);
+
+/* Stochastic comb of bank `in` into bank `out` (census times reset to 0).
+ * per_group != 0 combs per (cell, group) bin (MG).  disc[bin] = energy before - after. */
+IMC_API imc_status imc_comb(const imc_mesh* mesh, const imc_bank* in, imc_bank* out, int64_t n_max,
+                    uint64_t seed, uint32_t step, int32_t per_group, double* disc,
+                    void* workspace, size_t workspace_bytes, imc_comb_report* report,
+                    void* stream);
+
+/* Sum of live weights (FP64) and of e[c]*V[c]; host results. */
+IMC_API imc_status imc_energy_totals(const imc_mesh* mesh, const imc_bank* bank, const double* e,
+                             double* radiation, double* internal, void* workspace,
+                             size_t workspace_bytes, void* stream);
+
+/* Philox-4x32-10 on the device, for known-answer tests: n counters (4 words each) with
+ * one key -> n outputs. */
+IMC_API imc_status imc_philox(const uint32_t* ctr, uint32_t key0, uint32_t key1, uint32_t* out,
+                      int64_t n, void* stream);
+
+IMC_API const char* imc_status_str(imc_status s);
+IMC_API int imc_last_cuda_error(void);
+/* number of kernels this library launched since load (diagnostic) */
+IMC_API unsigned long long imc_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IMCB200_H */

@@ -1,0 +1,962 @@
+/*
+ * ORACLE — test infrastructure only.  Never linked into, or called by, the product
+ * (radtranbook_b200).  Only tests/, __graft_entry__.smoke() and bench.py's CPU
+ * baseline leg load it, as the checker / CPU baseline.
+ *
+ * An FP64, history-based CPU restatement of the reference implicit Monte Carlo
+ * (Fleck-Cummings) time step of DrRyanMc/RadTranBook:
+ *   gray 1-D slab    IMC/IMC1D.py:75-130 (move_particle), 133-200 (move_particles),
+ *                    203-291 (emission + linear-T tilt), 220-248 (IC), 294-316 (fixed
+ *                    source), 319-329 (boundary), 770-828 (comb), 908-1124 (step)
+ *   gray 1-D sphere  IMC/IMC1D.py:336-436, 439-532, 535-763
+ *   gray 2-D xy/rz   IMC/IMC2D.py:157-489 (boundary), 711-935 (events), 938-1107
+ *                    (history loop), 1110-1445 (IC / sources), 1448-1511 (comb),
+ *                    1591-1897 (step)
+ *   multigroup xy/rz MG_IMC/MG_IMC2D.py:202-254 (Planck sampler), 580-771 (events),
+ *                    774-989 (history loop), 1237-1267 (emission groups),
+ *                    1270-1378 (comb), 1635-2122 (step)
+ * It differs from the reference in exactly one way on purpose: random numbers come
+ * from Philox-4x32-10 streams keyed by (seed) with counter (index, block, step, tag),
+ * the same streams the CUDA path draws, so the two can be compared history by history.
+ * The uniforms are 24-bit values exactly representable in FP32 and FP64.
+ * Everything else (geometry, estimators, caps, ordering of the census bank, comb) is
+ * the reference's algorithm; the few deliberate reference-quirk decisions are noted
+ * where they occur.
+ */
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+#include "philox_ref.h"
+
+using oracle::draw;
+using oracle::Draw4;
+
+namespace {
+
+constexpr double C_LIGHT = 29.98;   /* cm/ns        IMC/IMC1D.py:68 */
+constexpr double A_RAD = 0.01372;   /* GJ/cm^3/keV^4 IMC/IMC1D.py:69 */
+constexpr double PI = 3.14159265358979323846;
+constexpr double BIG = 1e30;
+
+enum { G_SLAB = 0, G_SPHERE = 1, G_XY = 2, G_RZ = 3 };
+enum { EV_CENSUS = 0, EV_BOUNDARY = 1, EV_SCATTER = 2 };
+/* face crossed: 0 none, 1 +dir1, 2 -dir1, 3 +dir2, 4 -dir2 */
+enum { X_NONE = 0, X_IP = 1, X_IM = 2, X_JP = 3, X_JM = 4 };
+/* unified statistics layout */
+enum { S_EVENTS = 0, S_BOUNDARY, S_SCATTER, S_CENSUS, S_CAPTURE, S_FLOOR, S_REFLECT, S_CAP, S_ESCAPE, S_N };
+
+struct EventOut {
+  double w, d1, d2, p1, p2, dep, dep_i, dcen;
+  int cross, evt;
+};
+
+/* ---- effective-scatter distance with the reference's optically-thick cap ----
+ * IMC/IMC1D.py:83-88, IMC/IMC2D.py:758-765: a sigma_s*L > 1e4 cell uses sigma = 1e4/L.
+ * The capped distance reuses the same uniform (the reference draws a fresh one; the
+ * distribution is identical). */
+inline double scatter_distance(double ss, double L, double u, double thresh) {
+  if (ss * L > 10000.0) return -std::log(u) / (10000.0 / L);
+  if (ss > thresh) return -std::log(u) / ss;
+  return BIG;
+}
+
+/* ---- 1-D slab event: IMC/IMC1D.py:75-130 ---- */
+EventOut event_slab(double w, double mu, double x, double xl, double xr, double sa, double ss,
+                    double dcen, double u0, double u1) {
+  EventOut o{};
+  const double dx = xr - xl;
+  double db = (mu > 0) ? (xr - x) / mu : (xl - x) / mu;
+  if (db < 0) db = 0;
+  const double ds = scatter_distance(ss, dx, u0, 1e-10);
+  double d = db;
+  int evt = EV_BOUNDARY;
+  if (ds < d) { d = ds; evt = EV_SCATTER; }
+  if (dcen < d) { d = dcen; evt = EV_CENSUS; }
+  double xn = x + mu * d, mun = mu;
+  int cross = X_NONE;
+  if (evt == EV_BOUNDARY) {
+    if (mu > 0) { xn = xr; cross = X_IP; } else { xn = xl; cross = X_IM; }
+  } else if (evt == EV_SCATTER) {
+    mun = 2.0 * u1 - 1.0;
+  }
+  xn = std::min(std::max(xn, xl), xr);
+  const double wf = std::exp(-sa * d);
+  const double wn = w * wf;
+  const double lost = w - wn;
+  o.dep = lost / dx;
+  o.dep_i = (sa > 1e-10) ? lost / sa / dx : w * d / dx;
+  o.w = wn; o.d1 = mun; o.p1 = xn; o.dcen = dcen - d; o.cross = cross; o.evt = evt;
+  return o;
+}
+
+/* ---- 1-D spherical event: IMC/IMC1D.py:336-436 (stable root forms) ---- */
+EventOut event_sphere(double w, double mu, double r, double r0, double r1, double sa, double ss,
+                      double dcen, double u0, double u1) {
+  EventOut o{};
+  const double b2 = r * r * (1.0 - mu * mu);
+  double q = std::sqrt(std::max(r1 * r1 - b2, 0.0));
+  double d_out = (mu >= 0) ? (r1 - r) * (r1 + r) / std::max(q + r * mu, 1e-300) : q - r * mu;
+  if (d_out < 0) d_out = 0;
+  double d_in = BIG;
+  if (mu < 0 && r0 > 0) {
+    const double disc = r0 * r0 - b2;
+    if (disc > 0) {
+      d_in = (r - r0) * (r + r0) / (std::sqrt(disc) - r * mu);
+      if (d_in < 0) d_in = 0;
+    }
+  }
+  const bool hit_outer = d_out <= d_in;
+  const double db = hit_outer ? d_out : d_in;
+  const double ds = scatter_distance(ss, r1 - r0, u0, 1e-10);
+  double d = db;
+  int evt = EV_BOUNDARY;
+  if (ds < d) { d = ds; evt = EV_SCATTER; }
+  if (dcen < d) { d = dcen; evt = EV_CENSUS; }
+  const double rn2 = r * r + 2.0 * r * d * mu + d * d;
+  double rn = rn2 > 0 ? std::sqrt(rn2) : 0.0;
+  double mun = rn > 1e-15 ? (r * mu + d) / rn : 1.0;
+  int cross = X_NONE;
+  if (evt == EV_BOUNDARY) {
+    if (hit_outer) { rn = r1; mun = r1 > 1e-15 ? (r * mu + d) / r1 : 1.0; cross = X_IP; }
+    else { rn = r0; mun = r0 > 1e-15 ? (r * mu + d) / r0 : -1.0; cross = X_IM; }
+  } else if (evt == EV_SCATTER) {
+    mun = 2.0 * u1 - 1.0;
+  }
+  mun = std::min(1.0, std::max(-1.0, mun));
+  rn = std::min(std::max(rn, r0), r1);
+  const double vol = (4.0 / 3.0) * PI * (r1 * r1 * r1 - r0 * r0 * r0);
+  const double wn = w * std::exp(-sa * d);
+  const double lost = w - wn;
+  o.dep = lost / vol;
+  o.dep_i = (sa > 1e-10) ? lost / sa / vol : w * d / vol;
+  o.w = wn; o.d1 = mun; o.p1 = rn; o.dcen = dcen - d; o.cross = cross; o.evt = evt;
+  return o;
+}
+
+/* ---- 2-D Cartesian event: IMC/IMC2D.py:739-823 ---- */
+EventOut event_xy(double w, double ux, double uy, double x, double y, double xl, double xr,
+                  double yl, double yr, double sa, double ss, double dcen, double u0, double u1,
+                  double u2) {
+  EventOut o{};
+  double sx = BIG, sy = BIG;
+  if (ux > 0) sx = (xr - x) / ux; else if (ux < 0) sx = (xl - x) / ux;
+  if (uy > 0) sy = (yr - y) / uy; else if (uy < 0) sy = (yl - y) / uy;
+  if (sx < 0) sx = 0;
+  if (sy < 0) sy = 0;
+  const double ds = scatter_distance(ss, std::min(xr - xl, yr - yl), u0, 1e-12);
+  const double sb = sx < sy ? sx : sy;
+  double s = sb;
+  int evt = EV_BOUNDARY;
+  if (ds < s) { s = ds; evt = EV_SCATTER; }
+  if (dcen < s) { s = dcen; evt = EV_CENSUS; }
+  double xn = x + ux * s, yn = y + uy * s, uxn = ux, uyn = uy;
+  int cross = X_NONE;
+  if (evt == EV_BOUNDARY) {
+    if (sx <= sy) { if (ux > 0) { xn = xr; cross = X_IP; } else { xn = xl; cross = X_IM; } }
+    else { if (uy > 0) { yn = yr; cross = X_JP; } else { yn = yl; cross = X_JM; } }
+  } else if (evt == EV_SCATTER) {
+    /* IMC/IMC2D.py:695-701: 3-D isotropic, u_z dropped */
+    const double uz = 2.0 * u1 - 1.0, phi = 2.0 * PI * u2;
+    const double rxy = std::sqrt(std::max(0.0, 1.0 - uz * uz));
+    uxn = rxy * std::cos(phi); uyn = rxy * std::sin(phi);
+  }
+  const double wn = w * std::exp(-sa * s);
+  const double lost = w - wn;
+  o.dep = lost;
+  o.dep_i = (sa > 1e-12) ? lost / sa : w * s;
+  o.w = wn; o.d1 = uxn; o.d2 = uyn; o.p1 = xn; o.p2 = yn; o.dcen = dcen - s;
+  o.cross = cross; o.evt = evt;
+  return o;
+}
+
+/* ---- cylinder distances, IMC/IMC2D.py:711-736, written with the cancellation-free
+ * root forms.  l^2 + 2 r mu l + (r^2 - R^2) = 0, path length s = l / sqrt(1-eta^2). ---- */
+inline double rz_outer_l(double r, double mu, double R, double b2) {
+  const double q = std::sqrt(std::max(R * R - b2, 0.0));
+  double l = (mu >= 0) ? (R - r) * (R + r) / std::max(q + r * mu, 1e-300) : q - r * mu;
+  return l < 0 ? 0 : l;
+}
+inline double rz_inner_l(double r, double mu, double R, double b2) {
+  if (!(R > 0) || !(mu < 0)) return BIG;
+  const double disc = R * R - b2;
+  if (!(disc > 0)) return BIG;
+  double l = (r - R) * (r + R) / (std::sqrt(disc) - r * mu);
+  return l < 0 ? 0 : l;
+}
+
+/* ---- 2-D cylindrical r-z event: IMC/IMC2D.py:826-935 ---- */
+EventOut event_rz(double w, double mu, double eta, double r, double z, double rin, double rout,
+                  double zlo, double zhi, double sa, double ss, double dcen, double u0, double u1,
+                  double u2) {
+  EventOut o{};
+  const double sin2 = 1.0 - eta * eta;
+  double s_rin = BIG, s_rout = BIG;
+  if (sin2 >= 1e-15) {
+    const double st = std::sqrt(sin2);
+    const double b2 = r * r * (1.0 - mu * mu);
+    s_rout = rz_outer_l(r, mu, rout, b2) / st;
+    const double li = rz_inner_l(r, mu, rin, b2);
+    if (li < BIG) s_rin = li / st;
+  }
+  double s_zlo = BIG, s_zhi = BIG;
+  if (eta > 1e-15) s_zhi = std::max((zhi - z) / eta, 0.0);
+  else if (eta < -1e-15) s_zlo = std::max((zlo - z) / eta, 0.0);
+  const double ds = scatter_distance(ss, std::min(rout - rin, zhi - zlo), u0, 1e-12);
+  double sb = s_rin;
+  if (s_rout < sb) sb = s_rout;
+  if (s_zlo < sb) sb = s_zlo;
+  if (s_zhi < sb) sb = s_zhi;
+  double s = sb;
+  int evt = EV_BOUNDARY;
+  if (ds < s) { s = ds; evt = EV_SCATTER; }
+  if (dcen < s) { s = dcen; evt = EV_CENSUS; }
+  const double l = s * std::sqrt(std::max(sin2, 0.0));
+  double rn = std::sqrt(std::max(r * r + 2.0 * r * mu * l + l * l, 0.0));
+  double zn = z + s * eta;
+  double mun = mu, etan = eta;
+  if (rn > 1e-15 && l > 0) mun = std::min(1.0, std::max(-1.0, (r * mu + l) / rn));
+  int cross = X_NONE;
+  if (evt == EV_BOUNDARY) {
+    /* no 1e-12 nudges: the cell index, not the position, decides the cell */
+    if (sb == s_rin) { rn = rin; cross = X_IM; }
+    else if (sb == s_rout) { rn = rout; cross = X_IP; }
+    else if (sb == s_zlo) { zn = zlo; cross = X_JM; }
+    else { zn = zhi; cross = X_JP; }
+  } else if (evt == EV_SCATTER) {
+    /* IMC/IMC2D.py:704-708 */
+    etan = 2.0 * u1 - 1.0;
+    mun = std::cos(2.0 * PI * u2);
+  }
+  if (cross != X_IM && cross != X_IP) rn = std::min(std::max(rn, rin), rout);
+  if (cross != X_JM && cross != X_JP) zn = std::min(std::max(zn, zlo), zhi);
+  const double wn = w * std::exp(-sa * s);
+  const double lost = w - wn;
+  o.dep = lost;
+  o.dep_i = (sa > 1e-12) ? lost / sa : w * s;
+  o.w = wn; o.d1 = mun; o.d2 = etan; o.p1 = rn; o.p2 = zn; o.dcen = dcen - s;
+  o.cross = cross; o.evt = evt;
+  return o;
+}
+
+/* ---- problem / bank ---- */
+struct Problem {
+  int geom = 0, nx = 1, ny = 1, ng = 1;
+  std::vector<double> e1, e2, vol;
+  uint64_t seed = 0;
+};
+
+struct Bank {
+  std::vector<double> w, d1, d2, t, p1, p2;
+  std::vector<int> cell, grp;
+  size_t size() const { return w.size(); }
+  void resize(size_t n) {
+    w.resize(n); d1.resize(n); d2.resize(n); t.resize(n);
+    p1.resize(n); p2.resize(n); cell.resize(n); grp.resize(n);
+  }
+  void push(double w_, double d1_, double d2_, double t_, double p1_, double p2_, int c, int g) {
+    w.push_back(w_); d1.push_back(d1_); d2.push_back(d2_); t.push_back(t_);
+    p1.push_back(p1_); p2.push_back(p2_); cell.push_back(c); grp.push_back(g);
+  }
+};
+
+struct Oracle {
+  Problem P;
+  Bank B;
+};
+
+inline int ncells(const Problem& P) { return P.nx * P.ny; }
+
+/* Canonical FP64 total: 1024 strided partial sums, then a halving tree.  The CUDA path
+ * reduces in exactly this order (one 1024-thread block), so totals, and the integer
+ * source counts derived from them, agree bit for bit. */
+double canon_sum(const double* x, long long n) {
+  double part[1024];
+  for (int t = 0; t < 1024; ++t) {
+    double s = 0;
+    for (long long i = t; i < n; i += 1024) s += x[i];
+    part[t] = s;
+  }
+  for (int h = 512; h >= 1; h >>= 1)
+    for (int i = 0; i < h; ++i) part[i] += part[i + h];
+  return part[0];
+}
+inline double pow4(double T) { const double t2 = T * T; return t2 * t2; }
+inline double pow3(double T) { return T * T * T; }
+inline bool is1d(const Problem& P) { return P.geom == G_SLAB || P.geom == G_SPHERE; }
+
+int locate(const std::vector<double>& e, double v) {
+  /* np.searchsorted(edges, v, side='right') - 1, clamped into the mesh */
+  int i = (int)(std::upper_bound(e.begin(), e.end(), v) - e.begin()) - 1;
+  const int n = (int)e.size() - 1;
+  return std::min(std::max(i, 0), n - 1);
+}
+
+/* isotropic direction for the geometry from two uniforms */
+inline void iso_dir(int geom, double ua, double ub, double& d1, double& d2) {
+  if (is1d(Problem{geom})) { d1 = 2.0 * ua - 1.0; d2 = 0; return; }
+  if (geom == G_XY) {
+    const double uz = 2.0 * ua - 1.0, phi = 2.0 * PI * ub;
+    const double rxy = std::sqrt(std::max(0.0, 1.0 - uz * uz));
+    d1 = rxy * std::cos(phi); d2 = rxy * std::sin(phi);
+  } else {
+    d2 = 2.0 * ua - 1.0;            /* eta */
+    d1 = std::cos(2.0 * PI * ub);    /* mu_perp */
+  }
+}
+
+}  // namespace
+
+/* ======================================================================================
+ * C API
+ * ==================================================================================== */
+extern "C" {
+
+/* per-event pins (used against golden vectors recorded from the reference) */
+void orc_event(int geom, const double* in, double* out) {
+  /* in: w d1 d2 p1 p2 lo1 hi1 lo2 hi2 sa ss dcen u0 u1 u2 */
+  EventOut o;
+  switch (geom) {
+    case G_SLAB: o = event_slab(in[0], in[1], in[3], in[5], in[6], in[9], in[10], in[11], in[12], in[13]); break;
+    case G_SPHERE: o = event_sphere(in[0], in[1], in[3], in[5], in[6], in[9], in[10], in[11], in[12], in[13]); break;
+    case G_XY: o = event_xy(in[0], in[1], in[2], in[3], in[4], in[5], in[6], in[7], in[8], in[9], in[10], in[11], in[12], in[13], in[14]); break;
+    default: o = event_rz(in[0], in[1], in[2], in[3], in[4], in[5], in[6], in[7], in[8], in[9], in[10], in[11], in[12], in[13], in[14]); break;
+  }
+  out[0] = o.w; out[1] = o.d1; out[2] = o.d2; out[3] = o.p1; out[4] = o.p2;
+  out[5] = o.dep; out[6] = o.dep_i; out[7] = o.dcen; out[8] = o.cross; out[9] = o.evt;
+}
+
+void orc_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
+  oracle::philox4x32_10(ctr, key, out);
+}
+
+void* orc_create(int geom, int nx, int ny, int ng, const double* e1, const double* e2,
+                 const double* vol, uint64_t seed) {
+  Oracle* o = new Oracle();
+  o->P.geom = geom; o->P.nx = nx; o->P.ny = ny; o->P.ng = ng; o->P.seed = seed;
+  o->P.e1.assign(e1, e1 + nx + 1);
+  o->P.e2.assign(e2, e2 + ny + 1);
+  /* cell volumes come from the caller (the host computes them once, as the reference
+   * does, and hands the same array to every implementation) */
+  o->P.vol.assign(vol, vol + (size_t)nx * ny);
+  return o;
+}
+
+void orc_destroy(void* h) { delete (Oracle*)h; }
+
+long long orc_size(void* h) { return (long long)((Oracle*)h)->B.size(); }
+
+void orc_volumes(void* h, double* out) {
+  Oracle* o = (Oracle*)h;
+  std::copy(o->P.vol.begin(), o->P.vol.end(), out);
+}
+
+void orc_get_bank(void* h, double* w, double* d1, double* d2, double* t, double* p1, double* p2,
+                  int* cell, int* grp) {
+  Bank& B = ((Oracle*)h)->B;
+  const size_t n = B.size();
+  std::copy(B.w.begin(), B.w.begin() + n, w);
+  std::copy(B.d1.begin(), B.d1.begin() + n, d1);
+  std::copy(B.d2.begin(), B.d2.begin() + n, d2);
+  std::copy(B.t.begin(), B.t.begin() + n, t);
+  std::copy(B.p1.begin(), B.p1.begin() + n, p1);
+  std::copy(B.p2.begin(), B.p2.begin() + n, p2);
+  std::copy(B.cell.begin(), B.cell.begin() + n, cell);
+  std::copy(B.grp.begin(), B.grp.begin() + n, grp);
+}
+
+void orc_set_bank(void* h, long long n, const double* w, const double* d1, const double* d2,
+                  const double* t, const double* p1, const double* p2, const int* cell,
+                  const int* grp) {
+  Bank& B = ((Oracle*)h)->B;
+  B.w.assign(w, w + n); B.d1.assign(d1, d1 + n); B.d2.assign(d2, d2 + n);
+  B.t.assign(t, t + n); B.p1.assign(p1, p1 + n); B.p2.assign(p2, p2 + n);
+  B.cell.assign(cell, cell + n);
+  if (grp) B.grp.assign(grp, grp + n); else B.grp.assign(n, 0);
+}
+
+/* ---------------- initial census (gray) ----------------
+ * slab: IMC/IMC1D.py:220-248 (counts ceil(N E_c/E), no minimum)
+ * sphere: IMC/IMC1D.py:535-575
+ * xy/rz: IMC/IMC2D.py:1110-1188 (counts max(1, ceil(N E_c/E)))
+ * Draws: index k of the IC particle, block 0, step 0, TAG_IC. */
+long long orc_init_ic(void* h, long long N, const double* Tr, double T_emit_floor) {
+  Oracle* o = (Oracle*)h;
+  Problem& P = o->P;
+  Bank& B = o->B;
+  B.resize(0);
+  const int nc = ncells(P);
+  std::vector<double> E(nc);
+  for (int c = 0; c < nc; ++c) {
+    E[c] = A_RAD * pow4(Tr[c]) * P.vol[c];
+    if (T_emit_floor > 0 && Tr[c] < T_emit_floor) E[c] = 0;
+  }
+  const double Et = canon_sum(E.data(), nc);
+  if (N <= 0 || (is1d(P) && Et <= 0)) return 0;
+  uint32_t k = 0;
+  /* 1-D orders by cell i; 2-D by (i outer, j inner) as the reference loops */
+  std::vector<int> order;
+  if (is1d(P)) { for (int i = 0; i < P.nx; ++i) order.push_back(i); }
+  else { for (int i = 0; i < P.nx; ++i) for (int j = 0; j < P.ny; ++j) order.push_back(i + P.nx * j); }
+  for (int c : order) {
+    long long n;
+    if (is1d(P)) n = (long long)std::ceil(E[c] / Et * (double)N);
+    else n = std::max(1LL, (long long)std::ceil((double)N * E[c] / std::max(Et, 1e-300)));
+    if (n <= 0) continue;
+    const double wgt = E[c] / (double)n;
+    const int i = c % P.nx, j = c / P.nx;
+    const double a = P.e1[i], b = P.e1[i + 1], lo = P.e2[j], hi = P.e2[j + 1];
+    for (long long q = 0; q < n; ++q, ++k) {
+      Draw4 r = draw(P.seed, k, 0, 0, oracle::TAG_IC);
+      double p1, p2 = 0, d1, d2;
+      switch (P.geom) {
+        case G_SLAB: p1 = a + r.u[0] * (b - a); break;
+        case G_SPHERE: p1 = std::cbrt(a * a * a + (b * b * b - a * a * a) * r.u[0]); break;
+        case G_XY: p1 = a + r.u[0] * (b - a); p2 = lo + r.u[1] * (hi - lo); break;
+        default: p1 = std::sqrt(a * a + (b * b - a * a) * r.u[0]); p2 = lo + r.u[1] * (hi - lo); break;
+      }
+      iso_dir(P.geom, r.u[2], r.u[3], d1, d2);
+      B.push(wgt, d1, d2, 0.0, p1, p2, c, 0);
+    }
+  }
+  return (long long)B.size();
+}
+
+/* ---------------- step phase 1: Fleck, sources, transport ---------------- */
+typedef struct {
+  uint32_t step;
+  double dt, theta;
+  const double* T;        /* material temperature per cell */
+  const double* sigma;    /* true absorption opacity per cell */
+  const double* cv;       /* heat capacity per cell */
+  long long Ntarget, Nboundary, Nsource;
+  const double* source;   /* fixed source power density per cell or NULL */
+  const double* face_T[4];/* per-face-cell boundary temperature, NULL = no source */
+  int reflect[4];
+  long long max_events;   /* <= 0: no cap (1-D reference has none) */
+  int rz_linear_source;
+  double T_emit_floor;
+  int nthreads;
+} orc_step_in;
+
+typedef struct {
+  double* dep;            /* energy deposited per unit volume, per cell */
+  double* si;             /* path-length scalar intensity per cell */
+  double* emitted;        /* emission energy removed from matter per cell (GJ) */
+  double* sigma_a;        /* Fleck-modified absorption per cell (out) */
+  double* sigma_s;        /* effective scatter per cell (out) */
+  double boundary_emission, source_emission;
+  double escaped[4];
+  long long stats[S_N];
+  long long n_transported;
+  double weight_floor;
+} orc_step_out;
+
+}  // extern "C"
+
+namespace {
+
+/* Fleck factor, IMC/IMC1D.py:933-938 (1-D asserts f in [0,1]); IMC/IMC2D.py:1646-1651 (clip). */
+void fleck(const Problem& P, const orc_step_in* in, std::vector<double>& sa, std::vector<double>& ss) {
+  const int nc = ncells(P);
+  sa.resize(nc); ss.resize(nc);
+  for (int c = 0; c < nc; ++c) {
+    const double T = in->T[c];
+    const double beta = 4.0 * A_RAD * pow3(T) / in->cv[c];
+    double f = 1.0 / (1.0 + in->theta * beta * in->sigma[c] * C_LIGHT * in->dt);
+    f = std::min(1.0, std::max(0.0, f));
+    ss[c] = in->sigma[c] * (1.0 - f);
+    sa[c] = in->sigma[c] * f;
+  }
+}
+
+/* Boundary source, shared by every geometry.  For each side with a face-temperature
+ * array: face cell chosen with probability proportional to a c T^4/4 * area * dt (the
+ * reference's multinomial, IMC/IMC2D.py:183-206, 350-412; uniform T reduces to the
+ * uniform face sampling of :284-319), equal weights total/n, position uniform in the
+ * face cell's area, half-Lambertian direction.
+ * Draws: k, blocks 0 and 1, step, TAG_BOUNDARY|side. */
+double boundary_source(const Problem& P, const orc_step_in* in, Bank& B) {
+  double total = 0;
+  for (int side = 0; side < 4; ++side) {
+    const double* Tf = in->face_T[side];
+    if (!Tf || in->Nboundary <= 0) continue;
+    if (is1d(P) && side >= 2) continue;
+    const bool along2 = (side < 2);           /* rmin/rmax/left/right: cells indexed by j */
+    const int nf = is1d(P) ? 1 : (along2 ? P.ny : P.nx);
+    std::vector<double> Ef(nf), cdf(nf);
+    double Et = 0;
+    for (int q = 0; q < nf; ++q) {
+      double area;
+      if (is1d(P)) {
+        if (P.geom == G_SLAB) area = 1.0;
+        else { const double R = side == 0 ? P.e1[0] : P.e1[P.nx]; area = 4.0 * PI * R * R; }
+      } else if (P.geom == G_XY) {
+        area = along2 ? (P.e2[q + 1] - P.e2[q]) : (P.e1[q + 1] - P.e1[q]);
+      } else {
+        if (along2) { const double R = side == 0 ? P.e1[0] : P.e1[P.nx]; area = 2.0 * PI * R * (P.e2[q + 1] - P.e2[q]); }
+        else area = PI * (P.e1[q + 1] * P.e1[q + 1] - P.e1[q] * P.e1[q]);
+      }
+      const double T = Tf[q];
+      Ef[q] = (T > 0) ? A_RAD * C_LIGHT * T * T * T * T / 4.0 * area * in->dt : 0.0;
+      Et += Ef[q];
+      cdf[q] = Et;
+    }
+    if (!(Et > 0)) continue;
+    const long long n = in->Nboundary;
+    const double wgt = Et / (double)n;
+    for (long long k = 0; k < n; ++k) {
+      Draw4 a = draw(P.seed, (uint32_t)k, 0, in->step, oracle::TAG_BOUNDARY | side);
+      Draw4 b = draw(P.seed, (uint32_t)k, 1, in->step, oracle::TAG_BOUNDARY | side);
+      int q = (int)(std::lower_bound(cdf.begin(), cdf.end(), a.u[0] * Et) - cdf.begin());
+      q = std::min(q, nf - 1);
+      while (Ef[q] <= 0 && q > 0) --q;  /* never land in a non-emitting face cell */
+      const double mu_n = std::sqrt(a.u[2]);
+      const double t = b.u[0] * in->dt;
+      double p1, p2 = 0, d1, d2 = 0;
+      int i, j = 0;
+      if (is1d(P)) {
+        i = side == 0 ? 0 : P.nx - 1;
+        p1 = side == 0 ? P.e1[0] : P.e1[P.nx];
+        d1 = side == 0 ? mu_n : -mu_n;
+      } else if (P.geom == G_XY) {
+        const double mu_t = std::sqrt(std::max(0.0, 1.0 - mu_n * mu_n));
+        const double ct = mu_t * std::cos(2.0 * PI * a.u[3]);
+        if (along2) {
+          j = q; i = side == 0 ? 0 : P.nx - 1;
+          p1 = side == 0 ? P.e1[0] : P.e1[P.nx];
+          p2 = P.e2[q] + a.u[1] * (P.e2[q + 1] - P.e2[q]);
+          d1 = side == 0 ? mu_n : -mu_n; d2 = ct;
+        } else {
+          i = q; j = side == 2 ? 0 : P.ny - 1;
+          p2 = side == 2 ? P.e2[0] : P.e2[P.ny];
+          p1 = P.e1[q] + a.u[1] * (P.e1[q + 1] - P.e1[q]);
+          d2 = side == 2 ? mu_n : -mu_n; d1 = ct;
+        }
+      } else { /* rz */
+        if (along2) {
+          j = q; i = side == 0 ? 0 : P.nx - 1;
+          p1 = side == 0 ? P.e1[0] : P.e1[P.nx];
+          p2 = P.e2[q] + a.u[1] * (P.e2[q + 1] - P.e2[q]);
+          d1 = side == 0 ? mu_n : -mu_n;      /* mu_perp */
+          d2 = 2.0 * a.u[3] - 1.0;            /* eta */
+        } else {
+          i = q; j = side == 2 ? 0 : P.ny - 1;
+          const double r0 = P.e1[q], r1 = P.e1[q + 1];
+          p1 = std::sqrt(r0 * r0 + a.u[1] * (r1 * r1 - r0 * r0));
+          p2 = side == 2 ? P.e2[0] : P.e2[P.ny];
+          d2 = side == 2 ? mu_n : -mu_n;      /* eta */
+          d1 = std::cos(2.0 * PI * a.u[3]);   /* mu_perp */
+        }
+      }
+      B.push(wgt, d1, d2, t, p1, p2, i + P.nx * j, 0);
+      total += wgt;
+    }
+  }
+  return total;
+}
+
+/* slab linear-T position sampler, IMC/IMC1D.py:203-217 (closed-form inversion) */
+double slab_linear(double dx, double s, double T, double xi) {
+  if (std::fabs(s) < 1e-6) return xi * dx;
+  const double smax = 2.0 * T / (dx * dx);
+  s = std::max(-smax, std::min(s, smax));
+  const double disc = (s / (2.0 * T) - 1.0 / dx) * (s / (2.0 * T) - 1.0 / dx) + 2.0 * s * xi / (T * dx);
+  return (-2.0 * T + s * dx + 2.0 * T * dx * std::sqrt(std::max(disc, 0.0))) / (2.0 * s);
+}
+
+/* sphere linear-T^4 CDF inversion, IMC/IMC1D.py:578-626 */
+double sphere_cdf(double r0, double r1, double a, double M, double xi) {
+  const double C = a / 3.0 * (r1 * r1 * r1 - r0 * r0 * r0) + M / 4.0 * (pow4(r1) - pow4(r0));
+  if (C <= 0) return r0 + xi * (r1 - r0);
+  const double rhs = xi * C + (a / 3.0 * r0 * r0 * r0 + M / 4.0 * pow4(r0));
+  double lo = r0, hi = r1, r = r0 + xi * (r1 - r0);
+  for (int it = 0; it < 60; ++it) {
+    const double r3 = r * r * r, r4 = r3 * r;
+    const double g = a / 3.0 * r3 + M / 4.0 * r4 - rhs;
+    if (std::fabs(g) < 1e-14 * (std::fabs(rhs) + 1e-30)) break;
+    if (g < 0) lo = r; else hi = r;
+    const double dg = r * r * (a + M * r);
+    double rn = std::fabs(dg) > 1e-30 ? r - g / dg : 0.5 * (lo + hi);
+    if (rn <= lo || rn >= hi) rn = 0.5 * (lo + hi);
+    if (std::fabs(rn - r) < 1e-14 * (r1 - r0 + 1e-30)) { r = rn; break; }
+    r = rn;
+  }
+  return r;
+}
+
+/* cylinder linear-in-r CDF inversion, IMC/IMC2D.py:1293-1323 */
+double rz_r_cdf(double r0, double r1, double a, double M, double xi) {
+  const double C = a * 0.5 * (r1 * r1 - r0 * r0) + M / 3.0 * (r1 * r1 * r1 - r0 * r0 * r0);
+  if (C <= 0) return std::sqrt(r0 * r0 + (r1 * r1 - r0 * r0) * xi);
+  const double rhs = xi * C + a * 0.5 * r0 * r0 + M / 3.0 * r0 * r0 * r0;
+  double lo = r0, hi = r1, r = std::sqrt(r0 * r0 + (r1 * r1 - r0 * r0) * xi);
+  for (int it = 0; it < 50; ++it) {
+    const double g = a * 0.5 * r * r + M / 3.0 * r * r * r - rhs;
+    if (std::fabs(g) < 1e-14 * (std::fabs(rhs) + 1e-30)) break;
+    if (g < 0) lo = r; else hi = r;
+    const double dg = a * r + M * r * r;
+    double rn = std::fabs(dg) > 1e-30 ? r - g / dg : 0.5 * (lo + hi);
+    if (rn <= lo || rn >= hi) rn = 0.5 * (lo + hi);
+    if (std::fabs(rn - r) < 1e-14 * (r1 - r0 + 1e-30)) { r = rn; break; }
+    r = rn;
+  }
+  return r;
+}
+
+/* Volume source with per-cell energies QV (counts ceil(N QV/Qtot), weights QV/n).
+ * kind: 0 = material emission (times U(0,dt), 1-D linear tilts),
+ *       1 = fixed source.  Draws: k, blocks 0 and 1, step, tag.
+ * slab: IMC/IMC1D.py:251-316; sphere :629-741; xy IMC/IMC2D.py:1191-1238;
+ * rz uniform :1241-1290, rz linear :1326-1445. */
+double volume_source(const Problem& P, const std::vector<double>& QV, const double* T, long long N,
+                     double dt, uint32_t step, uint32_t tag, bool tilt, bool rz_linear, Bank& B) {
+  const int nc = ncells(P);
+  const double Qt = canon_sum(QV.data(), nc);
+  if (!(Qt > 0) || N <= 0) return 0;
+  /* tilt data */
+  std::vector<double> slope(nc, 0.0), Mr(nc, 0.0), Mz(nc, 0.0);
+  if (tilt && P.geom == G_SLAB && P.nx > 1) {
+    const int I = P.nx;
+    auto dx = [&](int i) { return P.e1[i + 1] - P.e1[i]; };
+    for (int i = 1; i < I - 1; ++i) slope[i] = (T[i + 1] - T[i - 1]) / (dx(i + 1) + dx(i - 1)) * 2;
+    slope[0] = (T[1] - T[0]) / (dx(1) + dx(0)) * 2;
+    slope[I - 1] = (T[I - 1] - T[I - 2]) / (dx(I - 1) + dx(I - 2)) * 2;
+    for (int i = 0; i < I; ++i) {
+      if (T[i] - slope[i] * dx(i) / 2 < 0) slope[i] = 0;
+      else if (T[i] + slope[i] * dx(i) / 2 < 0) slope[i] = 0;
+    }
+  }
+  if (tilt && P.geom == G_SPHERE && P.nx > 1) {
+    const int I = P.nx;
+    std::vector<double> rm(I), T4(I);
+    for (int i = 0; i < I; ++i) { rm[i] = 0.5 * (P.e1[i] + P.e1[i + 1]); T4[i] = pow4(T[i]); }
+    for (int i = 1; i < I - 1; ++i) slope[i] = (T4[i + 1] - T4[i - 1]) / (rm[i + 1] - rm[i - 1]);
+    slope[0] = (T4[1] - T4[0]) / (rm[1] - rm[0]);
+    slope[I - 1] = (T4[I - 1] - T4[I - 2]) / (rm[I - 1] - rm[I - 2]);
+    for (int i = 0; i < I; ++i) {
+      const double a = T4[i] - slope[i] * (rm[i] - P.e1[i]);
+      const double b = T4[i] + slope[i] * (P.e1[i + 1] - rm[i]);
+      if (a < 0 || b < 0) slope[i] = 0;
+    }
+  }
+  if (P.geom == G_RZ && rz_linear) {
+    std::vector<double> rc(P.nx), zc(P.ny);
+    for (int i = 0; i < P.nx; ++i) rc[i] = 0.5 * (P.e1[i] + P.e1[i + 1]);
+    for (int j = 0; j < P.ny; ++j) zc[j] = 0.5 * (P.e2[j] + P.e2[j + 1]);
+    auto T4 = [&](int i, int j) { return pow4(std::max(T[i + P.nx * j], 0.0)); };
+    for (int i = 0; i < P.nx; ++i)
+      for (int j = 0; j < P.ny; ++j) {
+        const int c = i + P.nx * j;
+        if (P.nx == 1) Mr[c] = 0;
+        else if (i == 0) Mr[c] = (T4(i + 1, j) - T4(i, j)) / (rc[i + 1] - rc[i]);
+        else if (i == P.nx - 1) Mr[c] = (T4(i, j) - T4(i - 1, j)) / (rc[i] - rc[i - 1]);
+        else Mr[c] = (T4(i + 1, j) - T4(i - 1, j)) / (rc[i + 1] - rc[i - 1]);
+        if (P.ny == 1) Mz[c] = 0;
+        else if (j == 0) Mz[c] = (T4(i, j + 1) - T4(i, j)) / (zc[j + 1] - zc[j]);
+        else if (j == P.ny - 1) Mz[c] = (T4(i, j) - T4(i, j - 1)) / (zc[j] - zc[j - 1]);
+        else Mz[c] = (T4(i, j + 1) - T4(i, j - 1)) / (zc[j + 1] - zc[j - 1]);
+      }
+  }
+  std::vector<int> order;
+  if (is1d(P)) { for (int i = 0; i < P.nx; ++i) order.push_back(i); }
+  else { for (int i = 0; i < P.nx; ++i) for (int j = 0; j < P.ny; ++j) order.push_back(i + P.nx * j); }
+  double total = 0;
+  uint32_t k = 0;
+  for (int c : order) {
+    const long long n = (long long)std::ceil((double)N * QV[c] / Qt);
+    if (n <= 0) continue;
+    const double wgt = QV[c] / (double)n;
+    const int i = c % P.nx, j = c / P.nx;
+    const double a = P.e1[i], b = P.e1[i + 1], lo = P.e2[j], hi = P.e2[j + 1];
+    /* per-cell tilt constants */
+    double ar = 0, Mloc = 0, Pn = 0.5, sa_c = 0, M4 = 0;
+    if (P.geom == G_RZ && rz_linear) {
+      const double rcen = 0.5 * (a + b), zcen = 0.5 * (lo + hi), T4c = pow4(std::max(T[c], 0.0));
+      ar = T4c - Mr[c] * (rcen - a);
+      const double t0 = ar, t1 = ar + Mr[c] * (b - a);
+      if (t0 < 0 || t1 < 0) { ar = std::max(T4c, 0.0); Mloc = 0; } else Mloc = Mr[c];
+      const double az = T4c - Mz[c] * (zcen - lo);
+      const double z0 = std::max(az, 0.0), z1 = std::max(az + Mz[c] * (hi - lo), 0.0);
+      Pn = (z0 + z1 > 0) ? z0 / (z0 + z1) : 0.5;
+    }
+    if (P.geom == G_SPHERE && tilt) {
+      M4 = slope[i];
+      sa_c = pow4(T[i]) - M4 * (0.5 * (a + b) - a);
+    }
+    for (long long q = 0; q < n; ++q, ++k) {
+      Draw4 r = draw(P.seed, k, 0, step, tag);
+      Draw4 s = draw(P.seed, k, 1, step, tag);
+      double p1, p2 = 0, d1, d2;
+      switch (P.geom) {
+        case G_SLAB:
+          p1 = a + (tilt ? slab_linear(b - a, slope[i], T[i], r.u[0]) : r.u[0] * (b - a));
+          break;
+        case G_SPHERE:
+          if (tilt && !(std::fabs(M4) < 1e-30 || std::fabs(sa_c) < 1e-30)) p1 = sphere_cdf(a, b, sa_c, M4, r.u[0]);
+          else p1 = std::cbrt(a * a * a + (b * b * b - a * a * a) * r.u[0]);
+          break;
+        case G_XY:
+          p1 = a + r.u[0] * (b - a); p2 = lo + r.u[1] * (hi - lo);
+          break;
+        default:
+          if (rz_linear) {
+            p1 = rz_r_cdf(a, b, ar, Mloc, r.u[0]);
+            const double sq = std::sqrt(r.u[1]);
+            p2 = (s.u[1] <= Pn) ? hi - (hi - lo) * sq : lo + (hi - lo) * sq;
+          } else {
+            p1 = std::sqrt(a * a + (b * b - a * a) * r.u[0]);
+            p2 = lo + r.u[1] * (hi - lo);
+          }
+          break;
+      }
+      p1 = std::min(std::max(p1, a), b);
+      p2 = is1d(P) ? 0.0 : std::min(std::max(p2, lo), hi);
+      iso_dir(P.geom, r.u[2], r.u[3], d1, d2);
+      const double t = s.u[0] * dt;  /* reference 1-D fixed source uses U(0,1): fixed to U(0,dt) */
+      B.push(wgt, d1, d2, t, p1, p2, c, 0);
+      total += wgt;
+    }
+  }
+  return total;
+}
+
+}  // namespace
+
+extern "C" {
+
+int orc_step_transport(void* h, const orc_step_in* in, orc_step_out* out) {
+  Oracle* o = (Oracle*)h;
+  Problem& P = o->P;
+  Bank& B = o->B;
+  const int nc = ncells(P);
+  std::vector<double> sa, ss;
+  fleck(P, in, sa, ss);
+  for (int c = 0; c < nc; ++c)
+    if (!(in->T[c] > 0) && is1d(P)) return 1; /* IMC/IMC1D.py:264 asserts T > 0 */
+  if (out->sigma_a) std::copy(sa.begin(), sa.end(), out->sigma_a);
+  if (out->sigma_s) std::copy(ss.begin(), ss.end(), out->sigma_s);
+
+  /* sources appended in the reference's order: census | boundary | fixed | emission */
+  out->boundary_emission = boundary_source(P, in, B);
+  out->source_emission = 0;
+  if (in->Nsource > 0 && in->source) {
+    double smax = 0;
+    for (int c = 0; c < nc; ++c) smax = std::max(smax, in->source[c]);
+    if (smax > 0) {
+      std::vector<double> QV(nc);
+      for (int c = 0; c < nc; ++c) QV[c] = in->source[c] * in->dt * P.vol[c];
+      const bool tilt_rz = (P.geom == G_RZ) && in->rz_linear_source;
+      out->source_emission = volume_source(P, QV, in->T, in->Nsource, in->dt, in->step,
+                                           oracle::TAG_SOURCE, false, tilt_rz, B);
+    }
+  }
+  std::vector<double> E(nc);
+  for (int c = 0; c < nc; ++c) {
+    E[c] = A_RAD * C_LIGHT * pow4(std::max(in->T[c], 0.0)) * sa[c] * in->dt * P.vol[c];
+    if (in->T_emit_floor > 0 && in->T[c] < in->T_emit_floor) E[c] = 0;
+    out->emitted[c] = 0;
+  }
+  {
+    const size_t n0 = B.size();
+    if (in->Ntarget > 0)
+      volume_source(P, E, in->T, in->Ntarget, in->dt, in->step, oracle::TAG_EMISSION, true,
+                    (P.geom == G_RZ) && in->rz_linear_source, B);
+    /* matter loses exactly the energy carried by the issued emission particles */
+    for (size_t k = n0; k < B.size(); ++k) out->emitted[B.cell[k]] += B.w[k];
+  }
+
+  /* weight floor, IMC/IMC1D.py:1007, IMC/IMC2D.py:1771 */
+  const long long N = (long long)B.size();
+  double wsum = 0;
+  for (long long k = 0; k < N; ++k) wsum += B.w[k];
+  const double floor_w = 1e-10 * wsum / (double)std::max(N, 1LL);
+  out->weight_floor = floor_w;
+  out->n_transported = N;
+
+  int nth = in->nthreads > 0 ? in->nthreads : 1;
+#ifndef _OPENMP
+  nth = 1;
+#endif
+  std::vector<std::vector<double>> dep_t(nth, std::vector<double>(nc, 0.0)), si_t(nth, std::vector<double>(nc, 0.0));
+  std::vector<std::vector<long long>> st_t(nth, std::vector<long long>(S_N, 0));
+  std::vector<std::vector<double>> esc_t(nth, std::vector<double>(4, 0.0));
+  const double dt = in->dt;
+  const bool oned = is1d(P);
+
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nth)
+  for (long long k = 0; k < N; ++k) {
+    int tid = 0;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+#endif
+    double* dep = dep_t[tid].data();
+    double* si = si_t[tid].data();
+    long long* st = st_t[tid].data();
+    double* esc = esc_t[tid].data();
+    double w = B.w[k], d1 = B.d1[k], d2 = B.d2[k], p1 = B.p1[k], p2 = B.p2[k];
+    int c = B.cell[k];
+    if (!(w > 0)) continue;
+    double dcen = (dt - B.t[k]) * C_LIGHT;
+    uint32_t ev = 0;
+    bool frozen = false;
+    while (dcen > 0) {
+      int i = c % P.nx, j = c / P.nx;
+      st[S_EVENTS]++;
+      if (!oned && in->max_events > 0 && (long long)ev >= in->max_events) {
+        /* IMC/IMC2D.py:974-977: cap hit, particle stays in census with its weight */
+        st[S_CAP]++;
+        break;
+      }
+      Draw4 r = draw(P.seed, (uint32_t)k, ev, in->step, oracle::TAG_TRANSPORT);
+      ++ev;
+      EventOut e;
+      switch (P.geom) {
+        case G_SLAB: e = event_slab(w, d1, p1, P.e1[i], P.e1[i + 1], sa[c], ss[c], dcen, r.u[0], r.u[1]); break;
+        case G_SPHERE: e = event_sphere(w, d1, p1, P.e1[i], P.e1[i + 1], sa[c], ss[c], dcen, r.u[0], r.u[1]); break;
+        case G_XY: e = event_xy(w, d1, d2, p1, p2, P.e1[i], P.e1[i + 1], P.e2[j], P.e2[j + 1], sa[c], ss[c], dcen, r.u[0], r.u[1], r.u[2]); break;
+        default: e = event_rz(w, d1, d2, p1, p2, P.e1[i], P.e1[i + 1], P.e2[j], P.e2[j + 1], sa[c], ss[c], dcen, r.u[0], r.u[1], r.u[2]); break;
+      }
+      if (e.evt == EV_BOUNDARY) st[S_BOUNDARY]++;
+      else if (e.evt == EV_SCATTER) st[S_SCATTER]++;
+      else st[S_CENSUS]++;
+      if (oned) { dep[c] += e.dep; si[c] += e.dep_i / dt; }
+      else { dep[c] += e.dep / P.vol[c]; si[c] += e.dep_i / (dt * P.vol[c]); }
+      dcen = e.dcen;
+      if (!oned) {
+        /* IMC/IMC2D.py:1042-1047: at/below the floor the history stops in place,
+         * keeping its weight (position and cell from before the event) */
+        w = e.w;
+        if (w <= floor_w) { st[S_FLOOR]++; frozen = true; break; }
+      } else {
+        w = e.w;
+      }
+      d1 = e.d1; d2 = e.d2; p1 = e.p1; p2 = e.p2;
+      bool escaped = false;
+      if (e.cross != X_NONE) {
+        if (e.cross == X_IP) ++i; else if (e.cross == X_IM) --i;
+        else if (e.cross == X_JP) ++j; else --j;
+        int side = -1;
+        if (i < 0) side = 0; else if (i >= P.nx) side = 1; else if (j < 0) side = 2; else if (j >= P.ny) side = 3;
+        if (side >= 0) {
+          if (in->reflect[side]) {
+            if (side < 2) { d1 = -d1; i = side == 0 ? 0 : P.nx - 1; }
+            else { d2 = -d2; j = side == 2 ? 0 : P.ny - 1; }
+            st[S_REFLECT]++;
+          } else {
+            esc[side] += w; st[S_ESCAPE]++; w = 0; dcen = 0; escaped = true;
+          }
+        }
+        if (!escaped) c = i + P.nx * j;
+      }
+      if (oned && !escaped && w < floor_w) {
+        /* IMC/IMC1D.py:188-195; the reference deposits only for interior cells and loses
+         * the energy in the two edge cells: here every cell gets it (ledger closes). */
+        st[S_FLOOR]++;
+        dep[c] += w / P.vol[c];
+        if (sa[c] > 0) si[c] += w / dt / sa[c] / P.vol[c];
+        w = 0; dcen = 0;
+      }
+      if (!oned && w <= 1e-300) { w = 0; dcen = 0; }
+    }
+    /* a frozen history keeps the state from before its last event (IMC/IMC2D.py:1042-1051) */
+    (void)frozen;
+    B.w[k] = w; B.d1[k] = d1; B.d2[k] = d2; B.p1[k] = p1; B.p2[k] = p2; B.cell[k] = c;
+  }
+  for (int c = 0; c < nc; ++c) { out->dep[c] = 0; out->si[c] = 0; }
+  for (int s = 0; s < S_N; ++s) out->stats[s] = 0;
+  for (int s = 0; s < 4; ++s) out->escaped[s] = 0;
+  for (int t = 0; t < nth; ++t) {
+    for (int c = 0; c < nc; ++c) { out->dep[c] += dep_t[t][c]; out->si[c] += si_t[t][c]; }
+    for (int s = 0; s < S_N; ++s) out->stats[s] += st_t[t][s];
+    for (int s = 0; s < 4; ++s) out->escaped[s] += esc_t[t][s];
+  }
+  return 0;
+}
+
+/* Stochastic comb, IMC/IMC1D.py:770-828 and IMC/IMC2D.py:1448-1511 (per cell), or
+ * MG_IMC/MG_IMC2D.py:1314-1378 (per cell and group, bin = cell + ncell*group).
+ *   ecen[b] = sum of live weights; desired = max(1, round_half_even(Nmax ecen/E));
+ *   ew = ecen/desired; copies = floor(w/ew + xi), each of weight ew, in bank order.
+ * xi: Philox (pre-comb index k, block 0, step, TAG_COMB).  Sets census times to 0.
+ * disc (per bin) = ecen - ecen_after.  Returns the new bank size. */
+long long orc_comb(void* h, long long Nmax, uint32_t step, int per_group, double* disc) {
+  Oracle* o = (Oracle*)h;
+  Problem& P = o->P;
+  Bank& B = o->B;
+  const int nc = ncells(P);
+  const int nb = per_group ? nc * P.ng : nc;
+  std::vector<double> ecen(nb, 0.0), after(nb, 0.0), ew(nb, 0.0);
+  const long long N = (long long)B.size();
+  auto bin = [&](long long k) { return per_group ? B.cell[k] + nc * B.grp[k] : B.cell[k]; };
+  for (long long k = 0; k < N; ++k) if (B.w[k] > 0) ecen[bin(k)] += B.w[k];
+  double E = 0;
+  for (int b = 0; b < nb; ++b) E += ecen[b];
+  if (!(E > 0)) {
+    Bank nbk;
+    for (long long k = 0; k < N; ++k)
+      if (B.w[k] > 0) nbk.push(B.w[k], B.d1[k], B.d2[k], 0.0, B.p1[k], B.p2[k], B.cell[k], B.grp[k]);
+    B = nbk;
+    for (int b = 0; b < nb; ++b) disc[b] = 0;
+    return (long long)B.size();
+  }
+  for (int b = 0; b < nb; ++b) {
+    if (ecen[b] > 0) {
+      const double d = std::max(1.0, std::nearbyint((double)Nmax * ecen[b] / E));
+      ew[b] = ecen[b] / d;
+    }
+  }
+  Bank nbk;
+  for (long long k = 0; k < N; ++k) {
+    if (!(B.w[k] > 0)) continue;
+    const int b = bin(k);
+    if (!(ew[b] > 0)) continue;
+    Draw4 r = draw(P.seed, (uint32_t)k, 0, step, oracle::TAG_COMB);
+    const long long n = (long long)std::floor(B.w[k] / ew[b] + r.u[0]);
+    for (long long q = 0; q < n; ++q) {
+      nbk.push(ew[b], B.d1[k], B.d2[k], 0.0, B.p1[k], B.p2[k], B.cell[k], B.grp[k]);
+      after[b] += ew[b];
+    }
+  }
+  B = nbk;
+  for (int b = 0; b < nb; ++b) disc[b] = ecen[b] - after[b];
+  return (long long)B.size();
+}
+
+/* comb with caller-supplied uniforms (one per bank entry, pre-comb order, used only by
+ * the pin against the reference's own seeded comb) */
+long long orc_comb_with_xi(void* h, long long Nmax, const double* xi, double* disc) {
+  Oracle* o = (Oracle*)h;
+  Problem& P = o->P;
+  Bank& B = o->B;
+  const int nc = ncells(P);
+  std::vector<double> ecen(nc, 0.0), after(nc, 0.0), ew(nc, 0.0);
+  const long long N = (long long)B.size();
+  for (long long k = 0; k < N; ++k) if (B.w[k] > 0) ecen[B.cell[k]] += B.w[k];
+  double E = 0;
+  for (int c = 0; c < nc; ++c) E += ecen[c];
+  for (int c = 0; c < nc; ++c)
+    if (ecen[c] > 0) ew[c] = ecen[c] / std::max(1.0, std::nearbyint((double)Nmax * ecen[c] / E));
+  Bank nbk;
+  long long live = 0;
+  for (long long k = 0; k < N; ++k) {
+    if (!(B.w[k] > 0)) continue;
+    const double x = xi[live++];
+    const int c = B.cell[k];
+    if (!(ew[c] > 0)) continue;
+    const long long n = (long long)std::floor(B.w[k] / ew[c] + x);
+    for (long long q = 0; q < n; ++q) {
+      nbk.push(ew[c], B.d1[k], B.d2[k], B.t[k], B.p1[k], B.p2[k], c, B.grp[k]);
+      after[c] += ew[c];
+    }
+  }
+  B = nbk;
+  for (int c = 0; c < nc; ++c) disc[c] = ecen[c] - after[c];
+  return (long long)B.size();
+}
+
+}  // extern "C"

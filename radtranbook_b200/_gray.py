@@ -1,0 +1,294 @@
+"""Shared core of the gray drop-in step (IMC1D / IMC2D signatures).
+
+One call of :func:`gray_step` is one reference time step (IMC/IMC1D.py:908-1124,
+IMC/IMC2D.py:1591-1897): material callables are evaluated on the temperature field, the
+device engine plans and samples the sources, tracks the bank to census, updates the
+material energy, combs the census, and the energy ledger is closed in FP64.
+"""
+from __future__ import annotations
+
+import time as _time
+
+import numpy as np
+import torch
+
+from . import _lib
+from .engine import A_RAD, C_LIGHT, Engine
+from .materials import evaluate
+
+
+class GrayState:
+    """Device-resident state with the reference's field names available as NumPy arrays.
+
+    Material fields (internal_energy, temperature, radiation_temperature) are mirrored to the
+    host after every step (O(cells)); particle fields are copied from the device bank when
+    read (O(particles), only for drivers that inspect or checkpoint the census).
+    """
+
+    _PARTICLE_1D = {"weights": "weight", "mus": "dir1", "times": "time", "positions": "pos1"}
+    _PARTICLE_2D = {"weights": "weight", "dir1": "dir1", "dir2": "dir2", "times": "time", "pos1": "pos1", "pos2": "pos2"}
+
+    def __init__(self, engine: Engine, dim: int, shape: tuple, e: torch.Tensor, T: torch.Tensor, Tr: torch.Tensor,
+                 time: float, previous_total_energy: float, count: int = 0):
+        object.__setattr__(self, "_engine", engine)
+        object.__setattr__(self, "_dim", dim)
+        object.__setattr__(self, "_shape", shape)
+        object.__setattr__(self, "_e", e)
+        object.__setattr__(self, "_T", T)
+        object.__setattr__(self, "_Tr", Tr)
+        object.__setattr__(self, "_host", {})
+        self.time = time
+        self.previous_total_energy = previous_total_energy
+        self.count = count
+
+    # ---- layout helpers: flat c = i + nx*j <-> reference (nx, ny) ----
+    def grid(self, flat: torch.Tensor) -> torch.Tensor:
+        if self._dim == 1:
+            return flat
+        nx, ny = self._shape
+        return flat.view(ny, nx).t()
+
+    def flat(self, grid: torch.Tensor) -> torch.Tensor:
+        if self._dim == 1:
+            return grid.reshape(-1).contiguous()
+        return grid.t().contiguous().view(-1)
+
+    def refresh_host(self) -> None:
+        h = self._host
+        h["internal_energy"] = self.grid(self._e).cpu().numpy().copy()
+        h["temperature"] = self.grid(self._T).cpu().numpy().copy()
+        h["radiation_temperature"] = self.grid(self._Tr).cpu().numpy().copy()
+        _lib.TRANSFER["d2h"] += 3 * 8 * self._engine.nc
+
+    def __getattr__(self, name):
+        host = object.__getattribute__(self, "_host")
+        if name in ("internal_energy", "temperature", "radiation_temperature"):
+            if name not in host:
+                self.refresh_host()
+            return host[name]
+        pmap = self._PARTICLE_1D if self._dim == 1 else self._PARTICLE_2D
+        bank = object.__getattribute__(self, "_engine").bank
+        if name in pmap:
+            return bank.view(pmap[name]).double().cpu().numpy()
+        if name in ("cell_indices", "cell_i", "cell_j"):
+            c = bank.view("cell").long().cpu().numpy()
+            nx = self._shape[0]
+            if name == "cell_indices" or name == "cell_i":
+                return c % nx if self._dim == 2 else c
+            return c // nx
+        raise AttributeError(name)
+
+    def __setattr__(self, name, value):
+        if name in ("internal_energy", "temperature"):
+            t = torch.as_tensor(np.asarray(value, dtype=np.float64), device=self._engine.device)
+            (self._e if name == "internal_energy" else self._T).copy_(self.flat(t))
+            self._host.pop(name, None)
+            return
+        object.__setattr__(self, name, value)
+
+
+def _host_copy(t: torch.Tensor) -> np.ndarray:
+    a = t.cpu().numpy()
+    _lib.TRANSFER["d2h"] += a.nbytes
+    return a
+
+
+def average_tallies(dist, eng: Engine) -> None:
+    """Mean over ranks of [dep | si | escaped] with one all-reduce (the only exchange)."""
+    world = dist.get_world_size()
+    if world == 1:
+        return
+    n1, n2 = eng.dep.numel(), eng.si.numel()
+    buf = torch.cat([eng.dep, eng.si, eng.escaped])
+    dist.all_reduce(buf)
+    buf /= world
+    eng.dep.copy_(buf[:n1])
+    eng.si.copy_(buf[n1:n1 + n2])
+    eng.escaped.copy_(buf[n1 + n2:])
+
+
+def face_temperatures(dim: int, geometry: str, T_boundary, time_now: float, e1: np.ndarray, e2: np.ndarray,
+                      boundary_source_func, device, cache: dict) -> list:
+    """Per-face-cell boundary temperatures for the four sides (None = no source).
+
+    1-D: sides 0/1 = left/right (one face cell).  2-D: T_boundary order (min-1, max-1,
+    min-2, max-2) as IMC/IMC2D.py:1617-1620; with boundary_source_func the temperature of
+    each face cell is the callable at its centre (IMC/IMC2D.py:183-191, 353-396).
+    """
+    out = [None, None, None, None]
+    nsides = 2 if dim == 1 else 4
+    names = {"xy": ("left", "right", "bottom", "top"), "rz": ("rmin", "rmax", "zmin", "zmax")}
+    for q in range(nsides):
+        Tb = T_boundary[q] if q < len(T_boundary) else 0.0
+        Tb = Tb(time_now) if callable(Tb) else Tb
+        if dim == 2 and boundary_source_func is not None:
+            key = ("func", id(boundary_source_func), q)
+            if key not in cache:
+                side = names[geometry][q]
+                if q < 2:
+                    X = e1[0] if q == 0 else e1[-1]
+                    centers = 0.5 * (e2[:-1] + e2[1:])
+                    vals = np.array([boundary_source_func(X, c, side) for c in centers], dtype=np.float64)
+                else:
+                    Y = e2[0] if q == 2 else e2[-1]
+                    centers = 0.5 * (e1[:-1] + e1[1:])
+                    vals = np.array([boundary_source_func(c, Y, side) for c in centers], dtype=np.float64)
+                cache[key] = torch.as_tensor(vals, device=device) if np.any(vals > 0) else None
+            out[q] = cache[key]
+            continue
+        if Tb is None or not (float(Tb) > 0.0):
+            continue
+        n = 1 if dim == 1 else (len(e2) - 1 if q < 2 else len(e1) - 1)
+        key = ("T", q, float(Tb), n)
+        if key not in cache:
+            cache[key] = torch.full((n,), float(Tb), dtype=torch.float64, device=device)
+        out[q] = cache[key]
+    return out
+
+
+def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, sigma_a_func, inv_eos, cv,
+              source, reflect, theta, use_scalar_intensity_Tr, conserve_comb_energy, T_emit_floor=0.0,
+              rz_linear_source=True, max_events=0, boundary_source_func=None, geometry="slab",
+              fleck_assert=False, allreduce=None):
+    """allreduce: a torch.distributed module when each rank runs an independent replica of the
+    problem (its own Philox key and full particle counts); the per-cell tallies and escaped
+    energy are averaged over ranks with one all-reduce before the material update, so every
+    rank holds the same material state (replica-averaged estimate, N x the histories)."""
+    t_step_start = _time.perf_counter()
+    eng: Engine = state._engine
+    dim = state._dim
+    like = state.grid(state._T)
+    host_T = lambda: state.temperature  # noqa: E731
+    sigma = state.flat(evaluate(sigma_a_func, like, host_T, like))
+    cvv = state.flat(evaluate(cv, like, host_T, like))
+    src = None
+    if Nsource > 0 and source is not None and np.max(np.asarray(source if not isinstance(source, torch.Tensor) else source.cpu())) > 0:
+        src = state.flat(torch.as_tensor(np.asarray(source, dtype=np.float64) if not isinstance(source, torch.Tensor)
+                                         else source.double(), device=eng.device))
+    cache = state.__dict__.setdefault("_face_cache", {})
+    faces = face_temperatures(dim, geometry, T_boundary, state.time, eng.e1.cpu().numpy(), eng.e2.cpu().numpy(),
+                              boundary_source_func, eng.device, cache)
+    refl = tuple(reflect) + (False,) * (4 - len(reflect))
+    t_eval = _time.perf_counter()
+    try:
+        res = eng.transport(state._T, sigma, cvv, src, state.count, dt, theta, Ntarget, Nboundary, Nsource, faces,
+                            refl, max_events=max_events, rz_linear_source=rz_linear_source,
+                            t_emit_floor=T_emit_floor)
+    except _lib.ImcError as ex:
+        if ex.status == 3:
+            raise AssertionError("Fleck factor out of bounds / non-positive temperature in material state") from ex
+        raise
+    rep = res.report
+    t_post = _time.perf_counter()
+    world = 1
+    if allreduce is not None:
+        world = allreduce.get_world_size()
+        average_tallies(allreduce, eng)
+
+    # material update: e += dep - emitted/V ; Tr from the path-length intensity
+    eng.material_update(state._e, state._Tr)
+    Tn = evaluate(inv_eos, state.grid(state._e), lambda: _host_copy(state.grid(state._e)), like)
+    state._T.copy_(state.flat(Tn))
+    if not use_scalar_intensity_Tr:
+        live = eng.bank.view("weight") > 0
+        rad = torch.zeros(eng.nc, dtype=torch.float64, device=eng.device)
+        rad.index_add_(0, eng.bank.view("cell")[live].long(), eng.bank.view("weight")[live].double())
+        state._Tr.copy_(torch.pow(rad / eng.vol / A_RAD, 0.25))
+    stats, esc = eng.host_stats()
+    _lib.TRANSFER["d2h"] += stats.nbytes + esc.nbytes
+    boundary_loss = float(esc[:4].sum())
+
+    crep = eng.comb(Nmax, state.count)
+    comb_disc = crep.energy_before - crep.energy_after
+    if conserve_comb_energy:
+        state._e.add_(eng.disc[: eng.nc] / eng.vol)
+        Tn = evaluate(inv_eos, state.grid(state._e), lambda: _host_copy(state.grid(state._e)), like)
+        state._T.copy_(state.flat(Tn))
+    rad, internal = eng.energy_totals(state._e)
+    if allreduce is not None and world > 1:
+        t = torch.tensor([rad, comb_disc], dtype=torch.float64, device=eng.device)
+        allreduce.all_reduce(t)
+        rad, comb_disc = float(t[0]) / world, float(t[1]) / world
+    total = internal + rad
+    energy_loss = total - state.previous_total_energy - rep.boundary_emission + boundary_loss - rep.source_emission
+    closure = energy_loss + (0.0 if conserve_comb_energy else comb_disc)
+    state.time = state.time + dt
+    state.previous_total_energy = total
+    state.count += 1
+    state._host.clear()
+    state.refresh_host()
+    t_end = _time.perf_counter()
+
+    n_tr = int(rep.n_transported)
+    ev = int(stats[_lib.STAT_EVENTS])
+    info = {
+        "time": state.time,
+        "radiation_temperature": state.radiation_temperature,
+        "temperature": state.temperature,
+        "N_particles": int(eng.bank.size),
+        "total_energy": total,
+        "total_internal_energy": internal,
+        "total_radiation_energy": rad,
+        "boundary_emission": float(rep.boundary_emission),
+        "boundary_loss": boundary_loss,
+        "source_emission": float(rep.source_emission),
+        "energy_loss": energy_loss,
+        "ledger": {
+            "comb_discrepancy": comb_disc,
+            "closure": closure,
+            "relative_closure": closure / max(abs(total), 1e-300),
+            "emission": float(rep.emission_total),
+            "weight_floor": float(rep.weight_floor),
+        },
+        "profiling": {
+            "phase_times_s": {
+                "sampling": (t_eval - t_step_start) + rep.ms_sources * 1e-3,
+                "transport": rep.ms_transport * 1e-3,
+                "postprocess": t_end - t_post,
+                "total": t_end - t_step_start,
+            },
+            "transport_events": {
+                "total": ev,
+                "boundary_crossings": int(stats[_lib.STAT_BOUNDARY]),
+                "census_events": int(stats[_lib.STAT_CENSUS]),
+                "weight_floor_kills": int(stats[_lib.STAT_FLOOR]),
+                "reflections": int(stats[_lib.STAT_REFLECT]),
+                "escapes": int(stats[_lib.STAT_ESCAPE]),
+                "avg_events_per_particle": ev / max(n_tr, 1),
+                "n_particles_transported": n_tr,
+            },
+        },
+    }
+    te = info["profiling"]["transport_events"]
+    if dim == 1:
+        te["scatter_events"] = int(stats[_lib.STAT_SCATTER])
+    else:
+        te["absorption_continue_events"] = int(stats[_lib.STAT_SCATTER])
+        te["absorption_capture_events"] = int(stats[_lib.STAT_CAPTURE])
+        te["event_cap_hits"] = int(stats[_lib.STAT_CAP])
+    return state, info
+
+
+def init_state(engine: Engine, dim: int, shape: tuple, Ntarget, Tinit, Tr_init, eos, inv_eos, Ntarget_ic,
+               T_emit_floor=0.0) -> GrayState:
+    dev = engine.device
+    Tg = torch.as_tensor(np.asarray(Tinit, dtype=np.float64), device=dev)
+    Trg = torch.as_tensor(np.asarray(Tr_init, dtype=np.float64), device=dev)
+    state = GrayState(engine, dim, shape, torch.zeros(engine.nc, dtype=torch.float64, device=dev),
+                      torch.zeros(engine.nc, dtype=torch.float64, device=dev),
+                      torch.zeros(engine.nc, dtype=torch.float64, device=dev), 0.0, 0.0, 0)
+    e = evaluate(eos, Tg, lambda: np.asarray(Tinit, dtype=np.float64), Tg)
+    state._e.copy_(state.flat(e))
+    state._T.copy_(state.flat(Tg))
+    back = evaluate(inv_eos, state.grid(state._e), lambda: state.grid(state._e).cpu().numpy(), Tg)
+    assert torch.allclose(back, Tg), "Inverse EOS failed"
+    N_ic = Ntarget if Ntarget_ic is None else Ntarget_ic
+    engine.init_census(state.flat(Trg), int(N_ic), T_emit_floor)
+    rad_cell = torch.zeros(engine.nc, dtype=torch.float64, device=dev)
+    if engine.bank.size:
+        rad_cell.index_add_(0, engine.bank.view("cell").long(), engine.bank.view("weight").double())
+    state._Tr.copy_(torch.pow(rad_cell / engine.vol / A_RAD, 0.25))
+    rad, internal = engine.energy_totals(state._e)
+    state.previous_total_energy = internal + rad
+    state.refresh_host()
+    return state

@@ -1,0 +1,143 @@
+"""ctypes binding of libimcb200.so (the C ABI declared in include/imcb200.h).
+
+The library is loaded from this package directory.  Nothing here falls back to another
+implementation: if the shared object is missing, or no CUDA device is present when a
+device call is made, the call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import pathlib
+from ctypes import POINTER, c_double, c_int, c_int32, c_int64, c_uint32, c_uint64, c_ulonglong, c_void_p, c_size_t, c_char_p
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = HERE / "libimcb200.so"
+
+GEOM = {"slab": 0, "spherical": 1, "xy": 2, "rz": 3}
+
+STATUS = {
+    0: "IMC_OK",
+    1: "IMC_ERR_BANK_OVERFLOW",
+    2: "IMC_ERR_EVENT_CAP",
+    3: "IMC_ERR_NONFINITE",
+    4: "IMC_ERR_BAD_GEOMETRY",
+    5: "IMC_ERR_TIMEOUT",
+    6: "IMC_ERR_CUDA",
+    7: "IMC_ERR_INVALID_ARG",
+    8: "IMC_ERR_WORKSPACE",
+}
+OK, BANK_OVERFLOW = 0, 1
+
+STAT_EVENTS, STAT_BOUNDARY, STAT_SCATTER, STAT_CENSUS, STAT_CAPTURE, STAT_FLOOR, STAT_REFLECT, STAT_CAP, STAT_ESCAPE, STAT_N = range(10)
+
+
+class ImcMesh(ctypes.Structure):
+    _fields_ = [
+        ("geometry", c_int32), ("nx", c_int32), ("ny", c_int32), ("n_groups", c_int32),
+        ("edges1", c_void_p), ("edges2", c_void_p), ("volume", c_void_p), ("group_edges", c_void_p),
+    ]
+
+
+class ImcBank(ctypes.Structure):
+    _fields_ = [
+        ("pos1", c_void_p), ("pos2", c_void_p), ("dir1", c_void_p), ("dir2", c_void_p),
+        ("weight", c_void_p), ("time", c_void_p), ("cell", c_void_p), ("group", c_void_p),
+        ("size", c_int64), ("capacity", c_int64),
+    ]
+
+
+class ImcMaterial(ctypes.Structure):
+    _fields_ = [("temperature", c_void_p), ("sigma", c_void_p), ("cv", c_void_p), ("source", c_void_p)]
+
+
+class ImcStepParams(ctypes.Structure):
+    _fields_ = [
+        ("seed", c_uint64), ("step", c_uint32), ("reflect", c_int32 * 4),
+        ("dt", c_double), ("theta", c_double),
+        ("n_target", c_int64), ("n_boundary", c_int64), ("n_source", c_int64),
+        ("face_T", c_void_p * 4),
+        ("max_events", c_int64),
+        ("rz_linear_source", c_int32), ("mg_reference_rules", c_int32),
+        ("t_emit_floor", c_double),
+        ("block_size", c_int32), ("blocks_per_sm", c_int32), ("chunk", c_int32), ("reserved", c_int32),
+    ]
+
+
+class ImcTallies(ctypes.Structure):
+    _fields_ = [
+        ("dep", c_void_p), ("si", c_void_p), ("emitted", c_void_p), ("sigma_a", c_void_p),
+        ("sigma_s", c_void_p), ("escaped", c_void_p), ("stats", c_void_p),
+    ]
+
+
+class ImcStepReport(ctypes.Structure):
+    _fields_ = [
+        ("n_boundary", c_int64), ("n_source", c_int64), ("n_emission", c_int64),
+        ("n_transported", c_int64), ("required_capacity", c_int64),
+        ("boundary_emission", c_double), ("source_emission", c_double), ("emission_total", c_double),
+        ("weight_floor", c_double),
+        ("ms_sources", ctypes.c_float), ("ms_transport", ctypes.c_float),
+    ]
+
+
+class ImcCombReport(ctypes.Structure):
+    _fields_ = [
+        ("n_in", c_int64), ("n_out", c_int64), ("required_capacity", c_int64),
+        ("energy_before", c_double), ("energy_after", c_double),
+    ]
+
+
+# name -> (restype, argtypes); every symbol declared in include/imcb200.h
+SIGNATURES = {
+    "imc_workspace_bytes": (c_size_t, [POINTER(ImcMesh), c_int64]),
+    "imc_init_census": (c_int, [POINTER(ImcMesh), c_void_p, c_int64, c_double, c_uint64, POINTER(ImcBank),
+                                c_void_p, c_size_t, POINTER(c_int64), c_void_p]),
+    "imc_step_transport": (c_int, [POINTER(ImcMesh), POINTER(ImcMaterial), POINTER(ImcStepParams),
+                                   POINTER(ImcBank), POINTER(ImcTallies), c_void_p, c_size_t,
+                                   POINTER(ImcStepReport), c_void_p]),
+    "imc_material_update": (c_int, [POINTER(ImcMesh), POINTER(ImcTallies), c_void_p, c_void_p, c_void_p]),
+    "imc_comb": (c_int, [POINTER(ImcMesh), POINTER(ImcBank), POINTER(ImcBank), c_int64, c_uint64, c_uint32,
+                         c_int32, c_void_p, c_void_p, c_size_t, POINTER(ImcCombReport), c_void_p]),
+    "imc_energy_totals": (c_int, [POINTER(ImcMesh), POINTER(ImcBank), c_void_p, POINTER(c_double),
+                                  POINTER(c_double), c_void_p, c_size_t, c_void_p]),
+    "imc_philox": (c_int, [c_void_p, c_uint32, c_uint32, c_void_p, c_int64, c_void_p]),
+    "imc_status_str": (c_char_p, [c_int]),
+    "imc_last_cuda_error": (c_int, []),
+    "imc_kernel_launches": (c_ulonglong, []),
+}
+
+# host<->device bytes moved by the drop-in API (material callables, host mirrors)
+TRANSFER = {"h2d": 0, "d2h": 0}
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Load libimcb200.so; raise if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'` "
+                "or `python radtranbook_b200/build.py` (requires nvcc)")
+        lib = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+class ImcError(RuntimeError):
+    def __init__(self, call: str, status: int):
+        lib = load()
+        msg = lib.imc_status_str(status).decode()
+        extra = f" (cudaError {lib.imc_last_cuda_error()})" if status == 6 else ""
+        super().__init__(f"{call}: {STATUS.get(status, status)}: {msg}{extra}")
+        self.status = status
+
+
+def check(call: str, status: int) -> None:
+    if status != OK:
+        raise ImcError(call, status)

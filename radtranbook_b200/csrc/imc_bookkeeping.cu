@@ -1,0 +1,330 @@
+// imc_bookkeeping.cu — per-cell FP64 work of the time step.
+//
+// Compiled with -fmad=false: every number here is computed with the same operation order
+// as the FP64 CPU oracle, so the integer particle counts per cell (ceil(N E_c / E)) and the
+// comb targets agree exactly.
+//
+//   Fleck factor   IMC/IMC1D.py:933-938, IMC/IMC2D.py:1646-1651
+//   emission plan  IMC/IMC1D.py:251-291 (slab), 629-707 (sphere), IMC/IMC2D.py:1731-1764
+//                  with _sample_source_{xy,rz_uniform,rz_linear} :1191-1445
+//   fixed source   IMC/IMC1D.py:294-316, 710-741; IMC/IMC2D.py:1709-1728
+//   boundary       IMC/IMC1D.py:319-329, 744-763; IMC/IMC2D.py:157-489
+//   IC             IMC/IMC1D.py:220-248, 535-575; IMC/IMC2D.py:1110-1188
+//   material       IMC/IMC1D.py:1021-1035; IMC/IMC2D.py:1801-1810
+//   comb targets   IMC/IMC1D.py:786-799; IMC/IMC2D.py:1461-1468
+#include <cmath>
+#include "imc_device.cuh"
+#include "imc_internal.h"
+
+using namespace imcdev;
+
+namespace {
+
+constexpr double PI = 3.14159265358979323846;
+constexpr int NT = 1024;
+
+__device__ __forceinline__ double pow4(double T) { const double t2 = T * T; return t2 * t2; }
+__device__ __forceinline__ double pow3(double T) { return T * T * T; }
+
+// 1024 strided partial sums, then a halving tree (the oracle's canon_sum).
+__device__ double block_canon_sum(const double* x, long long n, double* red) {
+  const int t = threadIdx.x;
+  double s = 0.0;
+  for (long long i = t; i < n; i += NT) s += x[i];
+  red[t] = s;
+  __syncthreads();
+  for (int h = NT / 2; h >= 1; h >>= 1) {
+    if (t < h) red[t] += red[t + h];
+    __syncthreads();
+  }
+  const double r = red[0];
+  __syncthreads();
+  return r;
+}
+
+// Exclusive scan of per-order-position counts n[0..m) into off[0..m]; returns the total.
+__device__ long long block_scan_counts(const long long* n, long long* off, int m, long long* sh) {
+  const int t = threadIdx.x;
+  const int per = (m + NT - 1) / NT;
+  const int lo = min(t * per, m), hi = min(lo + per, m);
+  long long s = 0;
+  for (int o = lo; o < hi; ++o) s += n[o];
+  sh[t] = s;
+  __syncthreads();
+  // Hillis-Steele inclusive scan of the 1024 thread totals
+  for (int d = 1; d < NT; d <<= 1) {
+    const long long v = (t >= d) ? sh[t - d] : 0;
+    __syncthreads();
+    sh[t] += v;
+    __syncthreads();
+  }
+  long long run = sh[t] - s;  // exclusive
+  for (int o = lo; o < hi; ++o) { off[o] = run; run += n[o]; }
+  const long long total = sh[NT - 1];
+  if (t == 0) off[m] = total;
+  __syncthreads();
+  return total;
+}
+
+// order position o = i*ny + j (the reference's i-outer, j-inner source loops)
+__device__ __forceinline__ int order_to_cell(int o, int nx, int ny) {
+  const int i = o / ny, j = o - (o / ny) * ny;
+  return i + nx * j;
+}
+
+// Volume-source counts (ceil(N QV_c / Q), in source order), per-cell weights and the
+// energy actually issued per cell (n_c times the FP32 weight, exact in FP64).
+__device__ long long plan_volume(const double* QV, long long N, int nx, int ny, int nc, long long* cnt,
+                                 long long* off, float* w, double* issued, double* red, long long* sh) {
+  const double Qt = block_canon_sum(QV, nc, red);
+  for (int o = threadIdx.x; o < nc; o += NT) {
+    const int c = order_to_cell(o, nx, ny);
+    long long n = 0;
+    if (Qt > 0.0 && N > 0) n = (long long)ceil((double)N * QV[c] / Qt);
+    cnt[o] = n;
+    const float wc = n > 0 ? (float)(QV[c] / (double)n) : 0.f;
+    w[c] = wc;
+    issued[c] = (double)n * (double)wc;
+  }
+  __syncthreads();
+  return block_scan_counts(cnt, off, nc, sh);
+}
+
+__global__ void __launch_bounds__(NT) k_plan(PlanArgs a) {
+  __shared__ double red[NT];
+  __shared__ long long sh[NT];
+  const int t = threadIdx.x;
+  const int nc = a.nc;
+  for (int q = t; q <= a.nx; q += NT) a.e1f[q] = (float)a.e1[q];
+  for (int q = t; q <= a.ny; q += NT) a.e2f[q] = (float)a.e2[q];
+  const bool oned = (a.geom == G_SLAB || a.geom == G_SPHERE);
+
+  // ---- Fleck factor and emission energy per cell (gray) ----
+  for (int c = t; c < nc; c += NT) {
+    const double T = a.T[c];
+    if (!isfinite(T) || (oned && !(T > 0.0)) || !isfinite(a.sigma[c]) || !(a.cv[c] > 0.0)) atomicOr(a.err, 2);
+    const double beta = 4.0 * A_RAD * pow3(T) / a.cv[c];
+    double f = 1.0 / (1.0 + a.theta * beta * a.sigma[c] * C_LIGHT * a.dt);
+    f = fmin(1.0, fmax(0.0, f));
+    const double ss = a.sigma[c] * (1.0 - f);
+    const double sa = a.sigma[c] * f;
+    a.sa[c] = sa; a.ss[c] = ss;
+    a.saf[c] = (float)sa; a.ssf[c] = (float)ss;
+    double E = A_RAD * C_LIGHT * pow4(fmax(T, 0.0)) * sa * a.dt * a.vol[c];
+    if (a.t_emit_floor > 0.0 && T < a.t_emit_floor) E = 0.0;
+    a.emit_E[c] = E;
+  }
+  __syncthreads();
+
+  // ---- emission counts / weights / offsets ----
+  const long long n_emit = plan_volume(a.emit_E, a.n_target, a.nx, a.ny, nc, a.emit_n, a.emit_off,
+                                       a.emit_w, a.emitted, red, sh);
+  const double e_emit = block_canon_sum(a.emitted, nc, red);
+
+  // ---- tilt constants (emission; fixed-source RZ tilt uses the same T) ----
+  for (int c = t; c < nc; c += NT) {
+    const int i = c % a.nx, j = c / a.nx;
+    double* tl = a.tilt + 4 * c;
+    tl[0] = tl[1] = tl[2] = tl[3] = 0.0;
+    if (a.geom == G_SLAB && a.nx > 1) {
+      // IMC/IMC1D.py:254-262: centred slopes of T, zeroed when an edge value goes negative
+      auto dx = [&](int k) { return a.e1[k + 1] - a.e1[k]; };
+      double s;
+      if (i == 0) s = (a.T[1] - a.T[0]) / (dx(1) + dx(0)) * 2.0;
+      else if (i == a.nx - 1) s = (a.T[i] - a.T[i - 1]) / (dx(i) + dx(i - 1)) * 2.0;
+      else s = (a.T[i + 1] - a.T[i - 1]) / (dx(i + 1) + dx(i - 1)) * 2.0;
+      if (a.T[i] - s * dx(i) / 2.0 < 0.0) s = 0.0;
+      else if (a.T[i] + s * dx(i) / 2.0 < 0.0) s = 0.0;
+      tl[0] = s;
+    } else if (a.geom == G_SPHERE && a.nx > 1) {
+      // IMC/IMC1D.py:643-659: slope of T^4 between cell-centre radii
+      auto rm = [&](int k) { return 0.5 * (a.e1[k] + a.e1[k + 1]); };
+      double M;
+      if (i == 0) M = (pow4(a.T[1]) - pow4(a.T[0])) / (rm(1) - rm(0));
+      else if (i == a.nx - 1) M = (pow4(a.T[i]) - pow4(a.T[i - 1])) / (rm(i) - rm(i - 1));
+      else M = (pow4(a.T[i + 1]) - pow4(a.T[i - 1])) / (rm(i + 1) - rm(i - 1));
+      const double lo = pow4(a.T[i]) - M * (rm(i) - a.e1[i]);
+      const double hi = pow4(a.T[i]) + M * (a.e1[i + 1] - rm(i));
+      if (lo < 0.0 || hi < 0.0) M = 0.0;
+      tl[0] = M;
+      tl[1] = pow4(a.T[i]) - M * (0.5 * (a.e1[i] + a.e1[i + 1]) - a.e1[i]);
+    } else if (a.geom == G_RZ && a.rz_linear) {
+      // IMC/IMC2D.py:1350-1417
+      auto T4 = [&](int ii, int jj) { return pow4(fmax(a.T[ii + a.nx * jj], 0.0)); };
+      auto rc = [&](int k) { return 0.5 * (a.e1[k] + a.e1[k + 1]); };
+      auto zc = [&](int k) { return 0.5 * (a.e2[k] + a.e2[k + 1]); };
+      double Mr, Mz;
+      if (a.nx == 1) Mr = 0.0;
+      else if (i == 0) Mr = (T4(i + 1, j) - T4(i, j)) / (rc(i + 1) - rc(i));
+      else if (i == a.nx - 1) Mr = (T4(i, j) - T4(i - 1, j)) / (rc(i) - rc(i - 1));
+      else Mr = (T4(i + 1, j) - T4(i - 1, j)) / (rc(i + 1) - rc(i - 1));
+      if (a.ny == 1) Mz = 0.0;
+      else if (j == 0) Mz = (T4(i, j + 1) - T4(i, j)) / (zc(j + 1) - zc(j));
+      else if (j == a.ny - 1) Mz = (T4(i, j) - T4(i, j - 1)) / (zc(j) - zc(j - 1));
+      else Mz = (T4(i, j + 1) - T4(i, j - 1)) / (zc(j + 1) - zc(j - 1));
+      const double r0 = a.e1[i], r1 = a.e1[i + 1], z0 = a.e2[j], z1 = a.e2[j + 1];
+      const double T4c = pow4(fmax(a.T[c], 0.0));
+      double ar = T4c - Mr * (0.5 * (r0 + r1) - r0);
+      double Mloc;
+      const double t0 = ar, t1 = ar + Mr * (r1 - r0);
+      if (t0 < 0.0 || t1 < 0.0) { ar = fmax(T4c, 0.0); Mloc = 0.0; } else Mloc = Mr;
+      const double az = T4c - Mz * (0.5 * (z0 + z1) - z0);
+      const double q0 = fmax(az, 0.0), q1 = fmax(az + Mz * (z1 - z0), 0.0);
+      const double Pn = (q0 + q1 > 0.0) ? q0 / (q0 + q1) : 0.5;
+      tl[0] = ar; tl[1] = Mloc; tl[2] = Pn;
+    }
+  }
+  __syncthreads();
+
+  // ---- fixed source (reference: only when max(source) > 0) ----
+  long long n_src = 0;
+  double e_src = 0.0;
+  if (a.source && a.n_source > 0) {
+    double smax = 0.0;
+    for (int c = t; c < nc; c += NT) {
+      smax = fmax(smax, a.source[c]);
+      a.src_QV[c] = a.source[c] * a.dt * a.vol[c];
+    }
+    red[t] = smax;
+    __syncthreads();
+    for (int h = NT / 2; h >= 1; h >>= 1) { if (t < h) red[t] = fmax(red[t], red[t + h]); __syncthreads(); }
+    const bool any = red[0] > 0.0;
+    __syncthreads();
+    if (any) {
+      n_src = plan_volume(a.src_QV, a.n_source, a.nx, a.ny, nc, a.src_n, a.src_off, a.src_w,
+                          a.src_issued, red, sh);
+      e_src = block_canon_sum(a.src_issued, nc, red);
+    }
+  }
+
+  // ---- boundary faces (one thread per side, sequential cumulative sums) ----
+  if (t < 4) {
+    const int side = t;
+    a.plan->n_bnd[side] = 0;
+    a.plan->e_bnd[side] = 0.0;
+    const double* Tf = a.face_T[side];
+    if (Tf && a.n_boundary > 0 && !(oned && side >= 2)) {
+      const bool along2 = side < 2;
+      const int nf = oned ? 1 : (along2 ? a.ny : a.nx);
+      double* Ef = a.face + (size_t)(side * 2 + 0) * a.nf;
+      double* cdf = a.face + (size_t)(side * 2 + 1) * a.nf;
+      double Et = 0.0;
+      for (int q = 0; q < nf; ++q) {
+        double area;
+        if (oned) {
+          if (a.geom == G_SLAB) area = 1.0;
+          else { const double R = side == 0 ? a.e1[0] : a.e1[a.nx]; area = 4.0 * PI * R * R; }
+        } else if (a.geom == G_XY) {
+          area = along2 ? (a.e2[q + 1] - a.e2[q]) : (a.e1[q + 1] - a.e1[q]);
+        } else {
+          if (along2) { const double R = side == 0 ? a.e1[0] : a.e1[a.nx]; area = 2.0 * PI * R * (a.e2[q + 1] - a.e2[q]); }
+          else area = PI * (a.e1[q + 1] * a.e1[q + 1] - a.e1[q] * a.e1[q]);
+        }
+        const double T = Tf[q];
+        Ef[q] = (T > 0.0) ? A_RAD * C_LIGHT * T * T * T * T / 4.0 * area * a.dt : 0.0;
+        Et += Ef[q];
+        cdf[q] = Et;
+      }
+      if (Et > 0.0) {
+        a.plan->n_bnd[side] = a.n_boundary;
+        const float wq = (float)(Et / (double)a.n_boundary);
+        a.plan->e_bnd[side] = (double)a.n_boundary * (double)wq;
+      }
+    }
+  }
+  if (t == 0) {
+    a.plan->n_emit = n_emit; a.plan->e_emit = e_emit;
+    a.plan->n_src = n_src; a.plan->e_src = e_src;
+  }
+}
+
+__global__ void __launch_bounds__(NT) k_ic_plan(IcArgs a) {
+  __shared__ double red[NT];
+  __shared__ long long sh[NT];
+  const int t = threadIdx.x;
+  const int nc = a.nc;
+  const bool oned = (a.geom == G_SLAB || a.geom == G_SPHERE);
+  double* E = a.E;
+  for (int c = t; c < nc; c += NT) {
+    double e = A_RAD * pow4(a.tr[c]) * a.vol[c];
+    if (a.t_emit_floor > 0.0 && a.tr[c] < a.t_emit_floor) e = 0.0;
+    E[c] = e;
+  }
+  __syncthreads();
+  const double Et = block_canon_sum(E, nc, red);
+  const long long N = a.n_target;
+  for (int o = t; o < nc; o += NT) {
+    const int c = order_to_cell(o, a.nx, a.ny);
+    long long n = 0;
+    if (N > 0) {
+      if (oned) n = Et > 0.0 ? (long long)ceil(E[c] / Et * (double)N) : 0;
+      else n = max(1LL, (long long)ceil((double)N * E[c] / fmax(Et, 1e-300)));
+    }
+    a.n[o] = n;
+    a.w[c] = n > 0 ? (float)(E[c] / (double)n) : 0.f;
+  }
+  __syncthreads();
+  const long long tot = block_scan_counts(a.n, a.off, nc, sh);
+  if (t == 0) { a.plan->n_emit = tot; }
+}
+
+__global__ void k_material(MatArgs a) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.nc) return;
+  double dep = 0.0, si = 0.0;
+  for (int g = 0; g < a.ng; ++g) { dep += a.dep[(size_t)g * a.nc + c]; si += a.si[(size_t)g * a.nc + c]; }
+  a.e[c] = a.e[c] + dep - a.emitted[c] / a.vol[c];
+  const double x = si / A_RAD / C_LIGHT;
+  a.tr[c] = x > 0.0 ? sqrt(sqrt(x)) : 0.0;
+}
+
+__global__ void __launch_bounds__(NT) k_comb_plan(CombPlanArgs a) {
+  __shared__ double red[NT];
+  const double E = block_canon_sum(a.ecen, a.nb, red);
+  for (int b = threadIdx.x; b < a.nb; b += NT) {
+    const double ec = a.ecen[b];
+    double ew = 0.0;
+    if (E > 0.0 && ec > 0.0) ew = ec / fmax(1.0, rint((double)a.n_max * ec / E));
+    a.ew[b] = ew;
+  }
+  if (threadIdx.x == 0) a.plan->comb_e_before = E;
+}
+
+__global__ void __launch_bounds__(NT) k_canon_eV(const double* e, const double* vol, int nc, double* out) {
+  __shared__ double red[NT];
+  const int t = threadIdx.x;
+  double s = 0.0;
+  for (int c = t; c < nc; c += NT) s += e[c] * vol[c];
+  red[t] = s;
+  __syncthreads();
+  for (int h = NT / 2; h >= 1; h >>= 1) { if (t < h) red[t] += red[t + h]; __syncthreads(); }
+  if (t == 0) *out = red[0];
+}
+
+}  // namespace
+
+cudaError_t imc_launch_plan(const PlanArgs& a, cudaStream_t s) {
+  ++g_imc_launches;
+  k_plan<<<1, NT, 0, s>>>(a);
+  return cudaGetLastError();
+}
+cudaError_t imc_launch_ic_plan(const IcArgs& a, cudaStream_t s) {
+  ++g_imc_launches;
+  k_ic_plan<<<1, NT, 0, s>>>(a);
+  return cudaGetLastError();
+}
+cudaError_t imc_launch_material(const MatArgs& a, cudaStream_t s) {
+  ++g_imc_launches;
+  k_material<<<(a.nc + 255) / 256, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+cudaError_t imc_launch_comb_plan(const CombPlanArgs& a, cudaStream_t s) {
+  ++g_imc_launches;
+  k_comb_plan<<<1, NT, 0, s>>>(a);
+  return cudaGetLastError();
+}
+cudaError_t imc_launch_canon_sum_eV(const double* e, const double* vol, int nc, double* out, cudaStream_t s) {
+  ++g_imc_launches;
+  k_canon_eV<<<1, NT, 0, s>>>(e, vol, nc, out);
+  return cudaGetLastError();
+}

@@ -1,0 +1,177 @@
+// imc_comb.cu — stochastic comb of the census bank (IMC/IMC1D.py:770-828,
+// IMC/IMC2D.py:1448-1511, MG_IMC/MG_IMC2D.py:1270-1378).
+//
+//   1. ecen[b]  = sum of live weights per bin (cell, or cell + nc*group)      k_comb_ecen
+//   2. ew[b]    = ecen / max(1, rint(Nmax ecen / E))                          k_comb_plan
+//   3. n_k      = floor(w_k / ew[b] + xi_k), xi from Philox (k, 0, step, TAG_COMB);
+//      per-block totals                                                       k_comb_count
+//   4. exclusive scan of block totals                                         k_comb_scan
+//   5. copies written in bank order (block-local scan + block offset)         k_comb_scatter
+//   6. disc[b] = ecen - (copies in b) * FP32(ew)                              k_comb_disc
+// Order of the output bank = order of the input bank, so the result is deterministic.
+#include "imc_device.cuh"
+#include "imc_internal.h"
+
+using namespace imcdev;
+
+namespace {
+
+constexpr int CB = 1024;  // comb block
+
+__device__ __forceinline__ int bin_of(const CombArgs& a, long long k) {
+  return a.per_group ? a.cell[k] + a.nc * a.group[k] : a.cell[k];
+}
+
+__global__ void __launch_bounds__(256) k_comb_ecen(CombArgs a) {
+  __shared__ WarpStage stages[8];
+  WarpStage* st = stages + (threadIdx.x >> 5);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  // block-uniform trip count keeps every warp converged for the aggregated reduction
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < a.n_in; base += stride) {
+    const long long k = base + threadIdx.x;
+    bool live = false;
+    int b = 0;
+    double w = 0.0;
+    if (k < a.n_in) {
+      const float wf = a.w[k];
+      if (wf > 0.f) { live = true; b = bin_of(a, k); w = (double)wf; }
+    }
+    warp_tally1(live, b, w, a.ecen, st);
+  }
+}
+
+__global__ void __launch_bounds__(CB) k_comb_count(CombArgs a) {
+  __shared__ long long sh[CB / 32];
+  const long long k = (long long)blockIdx.x * CB + threadIdx.x;
+  int n = 0;
+  if (k < a.n_in) {
+    const float wf = a.w[k];
+    if (wf > 0.f) {
+      const int b = bin_of(a, k);
+      const double ew = a.ew[b];
+      if (ew > 0.0) {
+        const U4 r = draw(a.seed, (uint32_t)k, 0, a.step, TAG_COMB);
+        n = (int)floor((double)wf / ew + u01d(r.x));
+        if (n > 0) atomicAdd(reinterpret_cast<unsigned long long*>(a.ncopy + b), (unsigned long long)n);
+      }
+    }
+    a.cnt[k] = n;
+  }
+  const unsigned ws = __reduce_add_sync(FULL, (unsigned)n);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = ws;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    unsigned long long v = sh[threadIdx.x];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    if (threadIdx.x == 0) a.blk[blockIdx.x] = (long long)v;
+  }
+}
+
+// exclusive scan of nblk block totals in place (blk[nblk] = total), single block
+__global__ void __launch_bounds__(1024) k_comb_scan(long long* blk, long long nblk, PlanDev* plan) {
+  __shared__ long long sh[1024];
+  const int t = threadIdx.x;
+  const long long per = (nblk + 1023) / 1024;
+  const long long lo = min((long long)t * per, nblk), hi = min(lo + per, nblk);
+  long long s = 0;
+  for (long long q = lo; q < hi; ++q) s += blk[q];
+  sh[t] = s;
+  __syncthreads();
+  for (int d = 1; d < 1024; d <<= 1) {
+    const long long v = t >= d ? sh[t - d] : 0;
+    __syncthreads();
+    sh[t] += v;
+    __syncthreads();
+  }
+  long long run = sh[t] - s;
+  for (long long q = lo; q < hi; ++q) { const long long x = blk[q]; blk[q] = run; run += x; }
+  if (t == 1023) { blk[nblk] = sh[1023]; plan->comb_total = sh[1023]; }
+}
+
+__global__ void __launch_bounds__(CB) k_comb_scatter(CombArgs a) {
+  __shared__ int sh[CB / 32];
+  const long long k = (long long)blockIdx.x * CB + threadIdx.x;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int n = (k < a.n_in) ? a.cnt[k] : 0;
+  // block-exclusive scan of n
+  int x = n;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) { const int y = __shfl_up_sync(FULL, x, o); if (lane >= o) x += y; }
+  if (lane == 31) sh[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int v = sh[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) { const int y = __shfl_up_sync(FULL, v, o); if (lane >= o) v += y; }
+    sh[lane] = v;
+  }
+  __syncthreads();
+  const long long start = a.blk[blockIdx.x] + (wid ? sh[wid - 1] : 0) + (x - n);
+  if (n > 0) {
+    const int b = bin_of(a, k);
+    const float wq = (float)a.ew[b];
+    const float p1 = a.p1[k], p2 = a.p2 ? a.p2[k] : 0.f, d1 = a.d1[k], d2 = a.d2 ? a.d2[k] : 0.f;
+    const int c = a.cell[k];
+    const int g = a.group ? a.group[k] : 0;
+    for (int q = 0; q < n; ++q) {
+      const long long o = start + q;
+      a.op1[o] = p1; a.od1[o] = d1;
+      if (a.op2) a.op2[o] = p2;
+      if (a.od2) a.od2[o] = d2;
+      a.ow[o] = wq; a.ot[o] = 0.f; a.ocell[o] = c;
+      if (a.ogroup) a.ogroup[o] = g;
+    }
+  }
+}
+
+__global__ void k_comb_disc(CombArgs a) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  double after = 0.0;
+  if (b < a.nb) {
+    after = (double)a.ncopy[b] * (double)(float)a.ew[b];
+    a.disc[b] = a.ecen[b] - after;
+  }
+  after = warp_sum_d(after);
+  if ((threadIdx.x & 31) == 0 && after != 0.0) atomicAdd(&a.plan->comb_e_after, after);
+}
+
+int grid_for(long long n, int block) {
+  long long g = (n + block - 1) / block;
+  if (g > 148LL * 16) g = 148LL * 16;
+  return (int)(g < 1 ? 1 : g);
+}
+
+}  // namespace
+
+cudaError_t imc_launch_comb_ecen(const CombArgs& a, cudaStream_t s) {
+  if (a.n_in <= 0) return cudaSuccess;
+  ++g_imc_launches;
+  k_comb_ecen<<<grid_for(a.n_in, 256), 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t imc_launch_comb_count(const CombArgs& a, cudaStream_t s) {
+  const long long nblk = (a.n_in + CB - 1) / CB;
+  if (nblk > 0) {
+    ++g_imc_launches;
+    k_comb_count<<<(unsigned)nblk, CB, 0, s>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  ++g_imc_launches;
+  k_comb_scan<<<1, 1024, 0, s>>>(a.blk, nblk, a.plan);
+  return cudaGetLastError();
+}
+
+cudaError_t imc_launch_comb_scatter(const CombArgs& a, cudaStream_t s) {
+  const long long nblk = (a.n_in + CB - 1) / CB;
+  if (nblk > 0) {
+    ++g_imc_launches;
+    k_comb_scatter<<<(unsigned)nblk, CB, 0, s>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  ++g_imc_launches;
+  k_comb_disc<<<(a.nb + 255) / 256, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}

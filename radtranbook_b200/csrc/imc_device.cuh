@@ -1,0 +1,159 @@
+// imc_device.cuh — device building blocks of the B200 IMC engine.
+//
+//  * Philox-4x32-10 (Salmon et al., SC'11), keyed by the run seed, counter
+//    (particle index, draw block / event number, step, stream tag).
+//  * 23-bit open-interval uniforms, identical in FP32 and FP64.
+//  * FP32 event geometry for slab / sphere / xy / rz (the reference's event
+//    functions IMC/IMC1D.py:75-130, 336-436 and IMC/IMC2D.py:711-935, rewritten in
+//    cancellation-free form; the cell index, not the position, decides the cell).
+//  * Warp-aggregated FP64 tally reduction (match_any + per-warp shared staging).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace imcdev {
+
+constexpr double C_LIGHT = 29.98;
+constexpr double A_RAD = 0.01372;
+constexpr float BIGF = 1e30f;
+constexpr unsigned FULL = 0xffffffffu;
+
+enum : int { G_SLAB = 0, G_SPHERE = 1, G_XY = 2, G_RZ = 3 };
+enum : int { EV_CENSUS = 0, EV_BOUNDARY = 1, EV_SCATTER = 2 };
+enum : int { X_NONE = 0, X_IP = 1, X_IM = 2, X_JP = 3, X_JM = 4 };
+enum : int { S_EVENTS = 0, S_BOUNDARY, S_SCATTER, S_CENSUS, S_CAPTURE, S_FLOOR, S_REFLECT, S_CAP, S_ESCAPE, S_N };
+
+enum : uint32_t {
+  TAG_TRANSPORT = 0x10000000u,
+  TAG_BOUNDARY = 0x20000000u,
+  TAG_SOURCE = 0x30000000u,
+  TAG_EMISSION = 0x40000000u,
+  TAG_IC = 0x50000000u,
+  TAG_COMB = 0x60000000u,
+};
+
+struct U4 { uint32_t x, y, z, w; };
+
+__device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    if (r) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+    const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+    const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+    c = U4{hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0};
+  }
+  return c;
+}
+
+// ((x>>9) + 0.5) * 2^-23 = (2k+1) * 2^-24, k < 2^23: 24 significant bits, so exact in
+// float and double alike, and never 0 or 1.
+__device__ __forceinline__ float u01f(uint32_t x) { return __uint2float_rn(((x >> 9) << 1) | 1u) * 5.9604644775390625e-8f; }
+__device__ __forceinline__ double u01d(uint32_t x) { return (double)(((x >> 9) << 1) | 1u) * 5.9604644775390625e-8; }
+
+__device__ __forceinline__ U4 draw(uint64_t seed, uint32_t idx, uint32_t block, uint32_t step, uint32_t tag) {
+  return philox4x32_10(U4{idx, block, step, tag}, (uint32_t)seed, (uint32_t)(seed >> 32));
+}
+
+// -log(u) for u = u01: distance in mean free paths.
+__device__ __forceinline__ float neglog_u(uint32_t x) { return -logf(u01f(x)); }
+
+// Effective-scatter distance with the optically-thick cap of the reference
+// (IMC/IMC1D.py:83-88; IMC/IMC2D.py:758-765): sigma_s*L > 1e4 uses sigma = 1e4/L.
+__device__ __forceinline__ float scatter_distance(float ss, float L, uint32_t x, float thresh, bool cap) {
+  if (cap && ss * L > 10000.0f) return neglog_u(x) * (L * 1e-4f);
+  if (ss > thresh) return neglog_u(x) / ss;
+  return BIGF;
+}
+
+struct Ev {
+  float d;       // path length of this event
+  int evt;       // EV_*
+  int cross;     // X_*
+};
+
+// ---- 1-D slab: distance to the exit face in the direction of mu ----
+__device__ __forceinline__ float slab_face(float x, float mu, float xl, float xr) {
+  const float db = (mu > 0.f ? (xr - x) : (xl - x)) / mu;
+  return fmaxf(db, 0.f);
+}
+
+// ---- sphere / cylinder: cancellation-free roots of l^2 + 2 r mu l + (r^2 - R^2) = 0 ----
+__device__ __forceinline__ float outer_root(float r, float mu, float R, float b2) {
+  const float q = sqrtf(fmaxf(fmaf(R, R, -b2), 0.f));
+  float l = (mu >= 0.f) ? (R - r) * (R + r) / fmaxf(fmaf(r, mu, q), 1e-30f) : q - r * mu;
+  return fmaxf(l, 0.f);
+}
+__device__ __forceinline__ float inner_root(float r, float mu, float R, float b2) {
+  if (!(R > 0.f) || !(mu < 0.f)) return BIGF;
+  const float disc = fmaf(R, R, -b2);
+  if (!(disc > 0.f)) return BIGF;
+  const float l = (r - R) * (r + R) / (sqrtf(disc) - r * mu);
+  return fmaxf(l, 0.f);
+}
+
+// ---- warp-aggregated FP64 reduction into global tallies ----
+// Every lane of the warp must call this (converged).  Lanes with flush=false pass any
+// key.  Lanes flushing the same cell are grouped with __match_any_sync; the lowest lane
+// of each group sums the group's values (staged in per-warp shared memory) and issues
+// one FP64 red per tally.
+struct WarpStage { double a[32]; double b[32]; };
+
+__device__ __forceinline__ void warp_tally2(bool flush, int key, double va, double vb,
+                                            double* __restrict__ ta, double* __restrict__ tb,
+                                            WarpStage* st) {
+  const unsigned fm = __ballot_sync(FULL, flush);
+  if (fm == 0u) return;
+  const int lane = threadIdx.x & 31;
+  const int k = flush ? key : -1 - lane;  // keys >= 0 for flushing lanes are cells
+  const unsigned peers = __match_any_sync(FULL, k);
+  if (__all_sync(FULL, !flush || __popc(peers) == 1)) {
+    if (flush) { atomicAdd(ta + key, va); atomicAdd(tb + key, vb); }
+    return;
+  }
+  st->a[lane] = va; st->b[lane] = vb;
+  __syncwarp();
+  if (flush && (__ffs(peers) - 1) == lane) {
+    double sa = 0.0, sb = 0.0;
+    unsigned m = peers;
+    while (m) {
+      const int l = __ffs(m) - 1;
+      m &= m - 1;
+      sa += st->a[l]; sb += st->b[l];
+    }
+    atomicAdd(ta + key, sa);
+    atomicAdd(tb + key, sb);
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ void warp_tally1(bool flush, int key, double va, double* __restrict__ ta,
+                                            WarpStage* st) {
+  const unsigned fm = __ballot_sync(FULL, flush);
+  if (fm == 0u) return;
+  const int lane = threadIdx.x & 31;
+  const unsigned peers = __match_any_sync(FULL, flush ? key : -1 - lane);
+  if (__all_sync(FULL, !flush || __popc(peers) == 1)) {
+    if (flush) atomicAdd(ta + key, va);
+    return;
+  }
+  st->a[lane] = va;
+  __syncwarp();
+  if (flush && (__ffs(peers) - 1) == lane) {
+    double sa = 0.0;
+    unsigned m = peers;
+    while (m) { const int l = __ffs(m) - 1; m &= m - 1; sa += st->a[l]; }
+    atomicAdd(ta + key, sa);
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+  return v;
+}
+__device__ __forceinline__ unsigned long long warp_sum_u(unsigned v) {
+  return (unsigned long long)__reduce_add_sync(FULL, v);
+}
+
+}  // namespace imcdev

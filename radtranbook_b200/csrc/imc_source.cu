@@ -1,0 +1,257 @@
+// imc_source.cu — fill the structure-of-arrays bank with new particles.
+//
+// One thread per new particle.  The particle's cell comes from a binary search of the
+// per-cell prefix sums computed by the planning kernel (source order: the reference's
+// i-outer / j-inner loops), so writes of consecutive threads are consecutive bank slots.
+// Sampling math is FP64 (Newton-bisection CDF inversions included) and stored as FP32.
+//
+//   volume sources  IMC/IMC1D.py:203-316 (slab emission, linear-T tilt, fixed source),
+//                   IMC/IMC1D.py:578-741 (sphere), IMC/IMC2D.py:1191-1445 (xy, rz)
+//   initial census  IMC/IMC1D.py:220-248, 535-575; IMC/IMC2D.py:1110-1188
+//   boundary        IMC/IMC1D.py:319-329, 744-763; IMC/IMC2D.py:157-489
+// Random numbers: Philox (particle index within this source, block 0/1, step, tag).
+#include <cmath>
+#include "imc_device.cuh"
+#include "imc_internal.h"
+
+using namespace imcdev;
+
+namespace {
+
+constexpr double PI = 3.14159265358979323846;
+
+__device__ __forceinline__ double pow4(double T) { const double t2 = T * T; return t2 * t2; }
+
+// slab linear-T position in [0, dx], IMC/IMC1D.py:203-217
+__device__ double slab_linear(double dx, double s, double T, double xi) {
+  if (fabs(s) < 1e-6) return xi * dx;
+  const double smax = 2.0 * T / (dx * dx);
+  s = fmax(-smax, fmin(s, smax));
+  const double q = s / (2.0 * T) - 1.0 / dx;
+  const double disc = q * q + 2.0 * s * xi / (T * dx);
+  return (-2.0 * T + s * dx + 2.0 * T * dx * sqrt(fmax(disc, 0.0))) / (2.0 * s);
+}
+
+// sphere linear-T^4 CDF inversion (bracketed Newton), IMC/IMC1D.py:578-626
+__device__ double sphere_cdf(double r0, double r1, double a, double M, double xi) {
+  const double C = a / 3.0 * (r1 * r1 * r1 - r0 * r0 * r0) + M / 4.0 * (pow4(r1) - pow4(r0));
+  if (C <= 0.0) return r0 + xi * (r1 - r0);
+  const double rhs = xi * C + (a / 3.0 * r0 * r0 * r0 + M / 4.0 * pow4(r0));
+  double lo = r0, hi = r1, r = r0 + xi * (r1 - r0);
+  for (int it = 0; it < 60; ++it) {
+    const double r3 = r * r * r, r4 = r3 * r;
+    const double g = a / 3.0 * r3 + M / 4.0 * r4 - rhs;
+    if (fabs(g) < 1e-14 * (fabs(rhs) + 1e-30)) break;
+    if (g < 0.0) lo = r; else hi = r;
+    const double dg = r * r * (a + M * r);
+    double rn = fabs(dg) > 1e-30 ? r - g / dg : 0.5 * (lo + hi);
+    if (rn <= lo || rn >= hi) rn = 0.5 * (lo + hi);
+    if (fabs(rn - r) < 1e-14 * (r1 - r0 + 1e-30)) { r = rn; break; }
+    r = rn;
+  }
+  return r;
+}
+
+// cylinder linear-in-r CDF inversion (bracketed Newton), IMC/IMC2D.py:1293-1323
+__device__ double rz_r_cdf(double r0, double r1, double a, double M, double xi) {
+  const double C = a * 0.5 * (r1 * r1 - r0 * r0) + M / 3.0 * (r1 * r1 * r1 - r0 * r0 * r0);
+  if (C <= 0.0) return sqrt(r0 * r0 + (r1 * r1 - r0 * r0) * xi);
+  const double rhs = xi * C + a * 0.5 * r0 * r0 + M / 3.0 * r0 * r0 * r0;
+  double lo = r0, hi = r1, r = sqrt(r0 * r0 + (r1 * r1 - r0 * r0) * xi);
+  for (int it = 0; it < 50; ++it) {
+    const double g = a * 0.5 * r * r + M / 3.0 * r * r * r - rhs;
+    if (fabs(g) < 1e-14 * (fabs(rhs) + 1e-30)) break;
+    if (g < 0.0) lo = r; else hi = r;
+    const double dg = a * r + M * r * r;
+    double rn = fabs(dg) > 1e-30 ? r - g / dg : 0.5 * (lo + hi);
+    if (rn <= lo || rn >= hi) rn = 0.5 * (lo + hi);
+    if (fabs(rn - r) < 1e-14 * (r1 - r0 + 1e-30)) { r = rn; break; }
+    r = rn;
+  }
+  return r;
+}
+
+__device__ __forceinline__ void iso_dir(int geom, double ua, double ub, double& d1, double& d2) {
+  if (geom == G_SLAB || geom == G_SPHERE) { d1 = 2.0 * ua - 1.0; d2 = 0.0; return; }
+  if (geom == G_XY) {
+    const double uz = 2.0 * ua - 1.0;
+    const double rxy = sqrt(fmax(0.0, 1.0 - uz * uz));
+    double sp, cp;
+    sincospi(2.0 * ub, &sp, &cp);
+    d1 = rxy * cp; d2 = rxy * sp;
+  } else {
+    d2 = 2.0 * ua - 1.0;      // eta
+    d1 = cospi(2.0 * ub);     // mu_perp
+  }
+}
+
+__global__ void k_fill_volume(FillArgs a) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < a.n; k += stride) {
+    // order position o with off[o] <= k < off[o+1]
+    int lo = 0, hi = a.nc;  // search in off[0..nc]
+    while (lo < hi) { const int mid = (lo + hi) >> 1; if (a.off[mid + 1] <= k) lo = mid + 1; else hi = mid; }
+    const int o = lo;
+    const int i = o / a.ny, j = o - i * a.ny;
+    const int c = i + a.nx * j;
+    const U4 r = draw(a.seed, (uint32_t)k, 0, a.step, a.tag);
+    const U4 s = draw(a.seed, (uint32_t)k, 1, a.step, a.tag);
+    const double u0 = u01d(r.x), u1 = u01d(r.y), u2 = u01d(r.z), u3 = u01d(r.w);
+    const double s0 = u01d(s.x), s1 = u01d(s.y);
+    const double ea = a.e1[i], eb = a.e1[i + 1];
+    double p1, p2 = 0.0;
+    switch (a.geom) {
+      case G_SLAB:
+        p1 = ea + (a.tilt_kind == 1 ? slab_linear(eb - ea, a.tilt[4 * c], a.T[c], u0) : u0 * (eb - ea));
+        break;
+      case G_SPHERE: {
+        const double M = a.tilt_kind == 2 ? a.tilt[4 * c] : 0.0;
+        const double ac = a.tilt_kind == 2 ? a.tilt[4 * c + 1] : 0.0;
+        if (a.tilt_kind == 2 && !(fabs(M) < 1e-30 || fabs(ac) < 1e-30)) p1 = sphere_cdf(ea, eb, ac, M, u0);
+        else p1 = cbrt(ea * ea * ea + (eb * eb * eb - ea * ea * ea) * u0);
+        break;
+      }
+      case G_XY:
+        p1 = ea + u0 * (eb - ea);
+        p2 = a.e2[j] + u1 * (a.e2[j + 1] - a.e2[j]);
+        break;
+      default: {
+        const double zl = a.e2[j], zh = a.e2[j + 1];
+        if (a.tilt_kind == 3) {
+          const double* tl = a.tilt + 4 * c;
+          p1 = rz_r_cdf(ea, eb, tl[0], tl[1], u0);
+          const double sq = sqrt(u1);
+          p2 = (s1 <= tl[2]) ? zh - (zh - zl) * sq : zl + (zh - zl) * sq;
+        } else {
+          p1 = sqrt(ea * ea + (eb * eb - ea * ea) * u0);
+          p2 = zl + u1 * (zh - zl);
+        }
+        break;
+      }
+    }
+    p1 = fmin(fmax(p1, ea), eb);
+    if (a.geom == G_XY || a.geom == G_RZ) p2 = fmin(fmax(p2, a.e2[j]), a.e2[j + 1]);
+    double d1, d2;
+    iso_dir(a.geom, u2, u3, d1, d2);
+    const long long b = a.base + k;
+    a.p1[b] = (float)p1; a.d1[b] = (float)d1;
+    if (a.p2) a.p2[b] = (float)p2;
+    if (a.d2) a.d2[b] = (float)d2;
+    a.wb[b] = a.w[c];
+    a.t[b] = (float)(s0 * a.time_scale);
+    a.cell[b] = c;
+    if (a.group) a.group[b] = 0;
+  }
+}
+
+__global__ void k_fill_boundary(BndArgs a) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const bool oned = (a.geom == G_SLAB || a.geom == G_SPHERE);
+  const bool along2 = a.side < 2;
+  const int nf = oned ? 1 : (along2 ? a.ny : a.nx);
+  const double* Ef = a.face;
+  const double* cdf = a.face + a.nf;
+  const double total = cdf[nf - 1];
+  const float wq = (float)(total / (double)a.n);
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < a.n; k += stride) {
+    const U4 ra = draw(a.seed, (uint32_t)k, 0, a.step, TAG_BOUNDARY | (uint32_t)a.side);
+    const U4 rb = draw(a.seed, (uint32_t)k, 1, a.step, TAG_BOUNDARY | (uint32_t)a.side);
+    const double ua0 = u01d(ra.x), ua1 = u01d(ra.y), ua2 = u01d(ra.z), ua3 = u01d(ra.w);
+    const double x = ua0 * total;
+    int lo = 0, hi = nf;  // lower_bound(cdf, x)
+    while (lo < hi) { const int mid = (lo + hi) >> 1; if (cdf[mid] < x) lo = mid + 1; else hi = mid; }
+    int q = min(lo, nf - 1);
+    while (q > 0 && Ef[q] <= 0.0) --q;
+    const double mu_n = sqrt(ua2);
+    const double t = u01d(rb.x) * a.dt;
+    double p1, p2 = 0.0, d1, d2 = 0.0;
+    int i, j = 0;
+    const int side = a.side;
+    if (oned) {
+      i = side == 0 ? 0 : a.nx - 1;
+      p1 = side == 0 ? a.e1[0] : a.e1[a.nx];
+      d1 = side == 0 ? mu_n : -mu_n;
+    } else if (a.geom == G_XY) {
+      const double mu_t = sqrt(fmax(0.0, 1.0 - mu_n * mu_n));
+      const double ct = mu_t * cospi(2.0 * ua3);
+      if (along2) {
+        j = q; i = side == 0 ? 0 : a.nx - 1;
+        p1 = side == 0 ? a.e1[0] : a.e1[a.nx];
+        p2 = a.e2[q] + ua1 * (a.e2[q + 1] - a.e2[q]);
+        d1 = side == 0 ? mu_n : -mu_n; d2 = ct;
+      } else {
+        i = q; j = side == 2 ? 0 : a.ny - 1;
+        p2 = side == 2 ? a.e2[0] : a.e2[a.ny];
+        p1 = a.e1[q] + ua1 * (a.e1[q + 1] - a.e1[q]);
+        d2 = side == 2 ? mu_n : -mu_n; d1 = ct;
+      }
+    } else {
+      if (along2) {
+        j = q; i = side == 0 ? 0 : a.nx - 1;
+        p1 = side == 0 ? a.e1[0] : a.e1[a.nx];
+        p2 = a.e2[q] + ua1 * (a.e2[q + 1] - a.e2[q]);
+        d1 = side == 0 ? mu_n : -mu_n;
+        d2 = 2.0 * ua3 - 1.0;
+      } else {
+        i = q; j = side == 2 ? 0 : a.ny - 1;
+        const double r0 = a.e1[q], r1 = a.e1[q + 1];
+        p1 = sqrt(r0 * r0 + ua1 * (r1 * r1 - r0 * r0));
+        p2 = side == 2 ? a.e2[0] : a.e2[a.ny];
+        d2 = side == 2 ? mu_n : -mu_n;
+        d1 = cospi(2.0 * ua3);
+      }
+    }
+    const long long b = a.base + k;
+    a.p1[b] = (float)p1; a.d1[b] = (float)d1;
+    if (a.p2) a.p2[b] = (float)p2;
+    if (a.d2) a.d2[b] = (float)d2;
+    a.wb[b] = wq;
+    a.t[b] = (float)t;
+    a.cell[b] = i + a.nx * j;
+    if (a.group) a.group[b] = 0;
+  }
+}
+
+__global__ void k_wsum(const float* w, long long n, double* out) {
+  __shared__ double sh[32];
+  double s = 0.0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) s += (double)w[k];
+  s = warp_sum_d(s);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+    v = warp_sum_d(v);
+    if (threadIdx.x == 0 && v != 0.0) atomicAdd(out, v);
+  }
+}
+
+int grid_for(long long n, int block) {
+  long long g = (n + block - 1) / block;
+  if (g > 148LL * 16) g = 148LL * 16;
+  return (int)(g < 1 ? 1 : g);
+}
+
+}  // namespace
+
+cudaError_t imc_launch_fill_volume(const FillArgs& a, cudaStream_t s) {
+  if (a.n <= 0) return cudaSuccess;
+  ++g_imc_launches;
+  k_fill_volume<<<grid_for(a.n, 256), 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t imc_launch_fill_boundary(const BndArgs& a, cudaStream_t s) {
+  if (a.n <= 0) return cudaSuccess;
+  ++g_imc_launches;
+  k_fill_boundary<<<grid_for(a.n, 256), 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t imc_launch_wsum(const float* w, long long n, double* out, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  ++g_imc_launches;
+  k_wsum<<<grid_for(n, 256), 256, 0, s>>>(w, n, out);
+  return cudaGetLastError();
+}

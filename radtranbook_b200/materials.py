@@ -1,0 +1,92 @@
+"""Material callables.
+
+The reference step functions receive Python callables (sigma_a_func(T), cv(T), inv_eos(e),
+eos(T)) and call them on NumPy arrays shaped like the temperature field.  The drop-in API
+accepts exactly those callables and calls them the same way (a host evaluation of the
+user's material model, O(cells) per step; particle work never leaves the GPU).
+
+Callables marked with :func:`device_callable` are called instead with CUDA torch tensors
+(float64, same shape) and must return CUDA tensors; then the whole step stays on the
+device.  The parametric materials below are device callables.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from ._lib import TRANSFER
+
+
+def device_callable(fn):
+    """Mark fn as accepting and returning CUDA torch tensors."""
+    fn._imc_device = True
+    return fn
+
+
+def is_device(fn) -> bool:
+    return bool(getattr(fn, "_imc_device", False))
+
+
+def evaluate(fn, T_dev: torch.Tensor, T_host_fn, like: torch.Tensor) -> torch.Tensor:
+    """Evaluate a material callable on the temperature field.
+
+    T_dev: device tensor in the reference's array shape.  T_host_fn: zero-argument
+    function returning the same field as a NumPy array (called only for host callables).
+    Returns a float64 device tensor broadcast to `like`'s shape.
+    """
+    if is_device(fn):
+        out = fn(T_dev)
+        if not isinstance(out, torch.Tensor):
+            out = torch.as_tensor(np.asarray(out, dtype=np.float64), device=like.device)
+        return torch.broadcast_to(out.to(like.device, torch.float64), like.shape)
+    out = fn(T_host_fn())
+    arr = np.ascontiguousarray(np.broadcast_to(np.asarray(out, dtype=np.float64), tuple(like.shape)))
+    TRANSFER["h2d"] += arr.nbytes
+    return torch.as_tensor(arr, device=like.device)
+
+
+class PowerLawOpacity:
+    """sigma(T) = A * T**(-n), optionally clamped to [lo, hi] (device callable)."""
+
+    _imc_device = True
+
+    def __init__(self, A: float, n: float, lo: float | None = None, hi: float | None = None):
+        self.A, self.n, self.lo, self.hi = float(A), float(n), lo, hi
+
+    def __call__(self, T):
+        if isinstance(T, torch.Tensor):
+            s = self.A * torch.pow(T, -self.n)
+            if self.lo is not None or self.hi is not None:
+                s = torch.clamp(s, min=self.lo, max=self.hi)
+            return s
+        s = self.A * np.power(T, -self.n)
+        if self.lo is not None or self.hi is not None:
+            s = np.clip(s, self.lo, self.hi)
+        return s
+
+
+class Constant:
+    """A constant (scalar or per-cell array) material property (device callable)."""
+
+    _imc_device = True
+
+    def __init__(self, value):
+        self.value = value
+        self._dev = None
+
+    def __call__(self, T):
+        if isinstance(T, torch.Tensor):
+            if self._dev is None or self._dev.device != T.device:
+                self._dev = torch.as_tensor(np.asarray(self.value, dtype=np.float64), device=T.device)
+            return torch.broadcast_to(self._dev, T.shape)
+        return np.broadcast_to(np.asarray(self.value, dtype=np.float64), np.shape(T))
+
+
+class LinearEOS:
+    """e = cv * T and its inverse, for a constant or per-cell cv (device callables)."""
+
+    def __init__(self, cv):
+        self.cv = Constant(cv)
+        self.eos = device_callable(lambda T: self.cv(T) * T)
+        self.inv_eos = device_callable(lambda e: e / self.cv(e))
+        self.cv_func = self.cv

@@ -1,0 +1,109 @@
+"""Benchmark workloads of the IMC engine, as reference-style problem definitions.
+
+Each function returns a dict with the mesh, material callables (host NumPy versions, as a
+reference driver writes them, and device versions) and the step parameters, so the same
+problem can be run through the drop-in API, the device engine or the CPU oracle.
+
+  marshak_slab   1-D gray slab Marshak wave: 0.20 cm, 100 cells, sigma = 300 T^-3,
+                 cv = 0.3, 1 keV left face, T0 = 1e-3 keV, dt 0.01 ns x 100
+                 (IMC/MarshakWave.py setup; 20k emission + 20k boundary / step, NMax 80k)
+  crooked_pipe   2-D RZ crooked pipe: r in [0,2], z in [0,7] on 60x210; pipe sigma 0.2,
+                 cv 0.001; wall sigma 2000, cv 0.5; 0.5 keV on z=0 for r<0.5; reflect r=0;
+                 T0 = 0.05 keV; dt 0.01 ns x 100; 2e6 source particles per step split 2:1
+                 emission:boundary, Nmax 6.67e6 (IMC/CrookedPipe2D.py geometry)
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .materials import device_callable
+
+
+def marshak_slab(scale: float = 1.0) -> dict:
+    I = 100
+    L = 0.20
+    mesh = np.array([[i * L / I, (i + 1) * L / I] for i in range(I)])
+    cv_val = 0.3
+
+    def sigma_host(T):
+        return 300.0 * np.power(T, -3.0)
+
+    @device_callable
+    def sigma_dev(T):
+        return 300.0 * torch.pow(T, -3.0)
+
+    return dict(
+        name="1-D gray slab Marshak wave (100 cells, sigma=300 T^-3)",
+        geometry="slab", mesh=mesh, dim=1,
+        Tinit=np.full(I, 0.001), Tr_init=np.full(I, 0.001),
+        sigma_host=sigma_host, sigma_dev=sigma_dev,
+        cv_host=lambda T: np.full_like(T, cv_val), cv_dev=device_callable(lambda T: torch.full_like(T, cv_val)),
+        eos_host=lambda T: cv_val * T, inv_eos_host=lambda e: e / cv_val,
+        eos_dev=device_callable(lambda T: cv_val * T), inv_eos_dev=device_callable(lambda e: e / cv_val),
+        Ntarget=int(20000 * scale), Nboundary=int(20000 * scale), Nsource=0, Nmax=int(80000 * scale),
+        T_boundary=(1.0, 0.0), reflect=(False, False), dt=0.01, n_steps=100, source=np.zeros(I),
+    )
+
+
+def crooked_pipe_thin(r: np.ndarray, z: np.ndarray) -> np.ndarray:
+    """Pipe (optically thin) region map, evaluated at cell centres."""
+    return (((r < 0.5) & (z >= 0.0) & (z <= 3.0))
+            | ((r >= 0.5) & (r < 1.5) & (z >= 2.5) & (z <= 3.0))
+            | ((r >= 1.0) & (r <= 1.5) & (z >= 3.0) & (z <= 4.0))
+            | ((r >= 0.5) & (r < 1.5) & (z >= 4.0) & (z <= 4.5))
+            | ((r < 0.5) & (z >= 4.0) & (z <= 7.0)))
+
+
+def crooked_pipe(scale: float = 1.0, nr: int = 60, nz: int = 210) -> dict:
+    r_edges = np.linspace(0.0, 2.0, nr + 1)
+    z_edges = np.linspace(0.0, 7.0, nz + 1)
+    rc = 0.5 * (r_edges[:-1] + r_edges[1:])
+    zc = 0.5 * (z_edges[:-1] + z_edges[1:])
+    R, Z = np.meshgrid(rc, zc, indexing="ij")
+    thin = crooked_pipe_thin(R, Z)
+    sig = np.where(thin, 0.2, 2000.0)
+    cvg = np.where(thin, 0.001, 0.5)
+    cache = {}
+
+    def dev(a, T):
+        key = (id(a), T.device)
+        if key not in cache:
+            cache[key] = torch.as_tensor(a, dtype=torch.float64, device=T.device)
+        return cache[key]
+
+    @device_callable
+    def sigma_dev(T):
+        return dev(sig, T)
+
+    @device_callable
+    def cv_dev(T):
+        return dev(cvg, T)
+
+    @device_callable
+    def eos_dev(T):
+        return dev(cvg, T) * T
+
+    @device_callable
+    def inv_eos_dev(e):
+        return e / dev(cvg, e)
+
+    def bsf(r, z, side):
+        return 0.5 if (side == "zmin" and r < 0.5) else 0.0
+
+    n_src = int(round(2e6 * scale))
+    n_bnd = n_src // 3
+    return dict(
+        name="2-D RZ gray crooked pipe (60x210)",
+        geometry="rz", dim=2, edges1=r_edges, edges2=z_edges,
+        Tinit=np.full((nr, nz), 0.05), Tr_init=np.full((nr, nz), 0.05),
+        sigma_host=lambda T: sig.copy(), sigma_dev=sigma_dev,
+        cv_host=lambda T: cvg.copy(), cv_dev=cv_dev,
+        eos_host=lambda T: cvg * T, inv_eos_host=lambda e: e / cvg,
+        eos_dev=eos_dev, inv_eos_dev=inv_eos_dev,
+        Ntarget=n_src - n_bnd, Nboundary=n_bnd, Nsource=0, Nmax=int(round(6.67e6 * scale)),
+        T_boundary=(0.0, 0.0, 0.0, 0.0), reflect=(True, False, False, False), boundary_source_func=bsf,
+        dt=0.01, n_steps=100, source=np.zeros((nr, nz)), thin=thin,
+        fiducials={"r=0,z=0.25": (0.0, 0.25), "r=0,z=2.75": (0.0, 2.75), "r=1.25,z=3.5": (1.25, 3.5),
+                   "r=0,z=4.25": (0.0, 4.25), "r=0,z=6.75": (0.0, 6.75)},
+    )
