@@ -51,19 +51,27 @@ def measured_peaks():
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
+        self.t0 = self.t1 = None
+
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
                                           "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
+            time.sleep(0.5)  # let the sampler start before the timed region
         except OSError:
             self.proc = None
         return self
@@ -79,24 +87,30 @@ class ClockSampler:
                 self.out, _ = self.proc.communicate()
 
     def summary(self):
+        import datetime
+
         if not getattr(self, "out", ""):
             return None
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.out.strip().splitlines():
             f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
+            if len(f) < 10:
                 continue
             try:
-                sm.append(float(f[1]))
-                smax.append(float(f[2]))
+                ts = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                if self.t0 is not None and not (self.t0 - 0.25 <= ts <= self.t1 + 0.25):
+                    continue
+                sm.append(float(f[2]))
+                smax.append(float(f[3]))
             except ValueError:
                 continue
-            for name, v in zip(names, f[5:9]):
+            for name, v in zip(names, f[6:10]):
                 if v.lower().startswith("active"):
                     reasons.add(name)
         if not sm:
-            return None
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0,
+                    "note": "no nvidia-smi sample fell inside the timed region"}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons), "samples": len(sm)}
 
 
@@ -208,6 +222,7 @@ def run_ours(args, rank: int, world: int):
     segs_per_step = []
     clocks = ClockSampler(dev.index)
     with clocks:
+        clocks.mark_start()
         s0.record()
         seg = hist = 0
         for _ in range(args.steps):
@@ -218,6 +233,7 @@ def run_ours(args, rank: int, world: int):
             segs_per_step.append(sg)
         s1.record()
         barrier()
+        clocks.mark_end()
     launches = lib.imc_kernel_launches() - launches0
     ms = s0.elapsed_time(s1)
     tmax = ms
@@ -294,12 +310,12 @@ def run_ours(args, rank: int, world: int):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0, help="particle-count scale of the workload")
-    ap.add_argument("--cpu-scale", type=float, default=0.02)
-    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--cpu-scale", type=float, default=0.5)
+    ap.add_argument("--cpu-steps", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

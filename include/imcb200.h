@@ -141,6 +141,29 @@ typedef struct imc_comb_report {
   double energy_before, energy_after;
 } imc_comb_report;
 
+/* Device-resident summary of one step, written by the asynchronous calls (the caller
+ * allocates it in device memory and copies it to the host once per step).  Bank sizes
+ * live here between the phases, so no phase needs the host to know them. */
+enum { IMC_FLAG_EVENT_CAP = 1, IMC_FLAG_NONFINITE = 2, IMC_FLAG_COMB_OVERFLOW = 4 };
+typedef struct imc_step_summary {
+  int64_t n_census;             /* bank entries before the sources (set by the caller) */
+  int64_t n_side[4];            /* boundary particles per side */
+  int64_t n_source, n_emission;
+  int64_t base_side[4];         /* first bank index of each source block */
+  int64_t base_source, base_emission;
+  int64_t n_bank;               /* entries tracked = census + sources */
+  int64_t n_out;                /* entries the comb produced (or wanted: see flags) */
+  int32_t flags;                /* IMC_FLAG_* */
+  int32_t pad;
+  double e_side[4];             /* issued boundary energy per side (GJ) */
+  double source_emission, emission_total;
+  double weight_sum;            /* sum of tracked weights; floor = 1e-10 * sum / n_bank */
+  double comb_before, comb_after;
+  double internal_energy;       /* sum_c e[c] V[c] after imc_comb_async */
+  unsigned long long stats[IMC_STAT_N];
+  double escaped[4];
+} imc_step_summary;
+
 /* Workspace bytes for a mesh and a bank capacity. */
 IMC_API size_t imc_workspace_bytes(const imc_mesh* mesh, int64_t bank_capacity);
 
@@ -169,6 +192,30 @@ IMC_API imc_status imc_comb(const imc_mesh* mesh, const imc_bank* in, imc_bank* 
                     uint64_t seed, uint32_t step, int32_t per_group, double* disc,
                     void* workspace, size_t workspace_bytes, imc_comb_report* report,
                     void* stream);
+
+/* Asynchronous forms.  Nothing is synchronised and no size is returned to the host:
+ * imc_step_transport_async reads summary->n_census (set it to the bank's live size),
+ * requires bank->capacity >= n_census + imc_source_bound(...), and writes the source
+ * counts, n_bank, weight_sum, stats and escaped energy into the device summary (the
+ * tallies' stats/escaped pointers may point into the summary).  imc_comb_async combs
+ * summary->n_bank entries of `in` into `out`, writing at most out->capacity entries; if
+ * more were needed it sets IMC_FLAG_COMB_OVERFLOW and n_out = the count needed (`in` is
+ * untouched, so the caller can grow `out` and call again).  It also writes comb_before,
+ * comb_after (= the radiation energy of `out`) and internal_energy = sum e*V. */
+IMC_API int64_t imc_source_bound(const imc_mesh* mesh, const imc_step_params* par);
+IMC_API imc_status imc_step_transport_async(const imc_mesh* mesh, const imc_material* mat,
+                                            const imc_step_params* par, imc_bank* bank,
+                                            imc_tallies* tal, void* workspace,
+                                            size_t workspace_bytes,
+                                            imc_step_summary* summary, void* stream);
+IMC_API imc_status imc_comb_async(const imc_mesh* mesh, const imc_bank* in, imc_bank* out,
+                                  int64_t n_max, uint64_t seed, uint32_t step, int32_t per_group,
+                                  double* disc, const double* e, void* workspace,
+                                  size_t workspace_bytes, imc_step_summary* summary,
+                                  void* stream);
+/* Device time (ms) of the source fill and of tracking in this host thread's last
+ * imc_step_transport[_async]; valid once that work has completed. */
+IMC_API imc_status imc_phase_times(float* ms_sources, float* ms_transport);
 
 /* Sum of live weights (FP64) and of e[c]*V[c]; host results. */
 IMC_API imc_status imc_energy_totals(const imc_mesh* mesh, const imc_bank* bank, const double* e,

@@ -53,6 +53,24 @@ class GrayState:
             return grid.reshape(-1).contiguous()
         return grid.t().contiguous().view(-1)
 
+    def host_copies(self):
+        """(device, pinned host) pairs for the end-of-step copy of e, T and Tr."""
+        hb = self.__dict__.get("_hbuf")
+        if hb is None:
+            hb = {k: torch.empty(self._engine.nc, dtype=torch.float64, pin_memory=True) for k in ("e", "T", "Tr")}
+            object.__setattr__(self, "_hbuf", hb)
+        return [(self._e, hb["e"]), (self._T, hb["T"]), (self._Tr, hb["Tr"])]
+
+    def take_host_copies(self) -> None:
+        """Host mirrors from the pinned buffers filled by the last fetch (no device access)."""
+        hb = self._hbuf
+        h = self._host
+        g = (lambda a: a) if self._dim == 1 else (lambda a: a.reshape(self._shape[1], self._shape[0]).T)
+        h["internal_energy"] = np.array(g(hb["e"].numpy()))
+        h["temperature"] = np.array(g(hb["T"].numpy()))
+        h["radiation_temperature"] = np.array(g(hb["Tr"].numpy()))
+        _lib.TRANSFER["d2h"] += 3 * 8 * self._engine.nc
+
     def refresh_host(self) -> None:
         h = self._host
         h["internal_energy"] = self.grid(self._e).cpu().numpy().copy()
@@ -99,12 +117,11 @@ def average_tallies(dist, eng: Engine) -> None:
     if world == 1:
         return
     n1, n2 = eng.dep.numel(), eng.si.numel()
-    buf = torch.cat([eng.dep, eng.si, eng.escaped])
+    buf = torch.cat([eng.dep, eng.si])
     dist.all_reduce(buf)
     buf /= world
     eng.dep.copy_(buf[:n1])
     eng.si.copy_(buf[n1:n1 + n2])
-    eng.escaped.copy_(buf[n1 + n2:])
 
 
 def face_temperatures(dim: int, geometry: str, T_boundary, time_now: float, e1: np.ndarray, e2: np.ndarray,
@@ -149,11 +166,14 @@ def face_temperatures(dim: int, geometry: str, T_boundary, time_now: float, e1: 
 def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, sigma_a_func, inv_eos, cv,
               source, reflect, theta, use_scalar_intensity_Tr, conserve_comb_energy, T_emit_floor=0.0,
               rz_linear_source=True, max_events=0, boundary_source_func=None, geometry="slab",
-              fleck_assert=False, allreduce=None):
-    """allreduce: a torch.distributed module when each rank runs an independent replica of the
+              allreduce=None):
+    """One time step.  With device material callables the host synchronises once, at the
+    end (sizes, energies and statistics come back in one device summary).
+
+    allreduce: a torch.distributed module when each rank runs an independent replica of the
     problem (its own Philox key and full particle counts); the per-cell tallies and escaped
     energy are averaged over ranks with one all-reduce before the material update, so every
-    rank holds the same material state (replica-averaged estimate, N x the histories)."""
+    rank holds the same material state (a replica-averaged estimate, N x the histories)."""
     t_step_start = _time.perf_counter()
     eng: Engine = state._engine
     dim = state._dim
@@ -162,24 +182,20 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
     sigma = state.flat(evaluate(sigma_a_func, like, host_T, like))
     cvv = state.flat(evaluate(cv, like, host_T, like))
     src = None
-    if Nsource > 0 and source is not None and np.max(np.asarray(source if not isinstance(source, torch.Tensor) else source.cpu())) > 0:
-        src = state.flat(torch.as_tensor(np.asarray(source, dtype=np.float64) if not isinstance(source, torch.Tensor)
-                                         else source.double(), device=eng.device))
+    if Nsource > 0 and source is not None:
+        src_t = source.double() if isinstance(source, torch.Tensor) else torch.as_tensor(
+            np.asarray(source, dtype=np.float64))
+        if float(src_t.max()) > 0:
+            src = state.flat(src_t.to(eng.device))
     cache = state.__dict__.setdefault("_face_cache", {})
-    faces = face_temperatures(dim, geometry, T_boundary, state.time, eng.e1.cpu().numpy(), eng.e2.cpu().numpy(),
+    if "edges" not in cache:
+        cache["edges"] = (eng.e1.cpu().numpy(), eng.e2.cpu().numpy())
+    faces = face_temperatures(dim, geometry, T_boundary, state.time, cache["edges"][0], cache["edges"][1],
                               boundary_source_func, eng.device, cache)
     refl = tuple(reflect) + (False,) * (4 - len(reflect))
     t_eval = _time.perf_counter()
-    try:
-        res = eng.transport(state._T, sigma, cvv, src, state.count, dt, theta, Ntarget, Nboundary, Nsource, faces,
-                            refl, max_events=max_events, rz_linear_source=rz_linear_source,
-                            t_emit_floor=T_emit_floor)
-    except _lib.ImcError as ex:
-        if ex.status == 3:
-            raise AssertionError("Fleck factor out of bounds / non-positive temperature in material state") from ex
-        raise
-    rep = res.report
-    t_post = _time.perf_counter()
+    eng.transport_async(state._T, sigma, cvv, src, state.count, dt, theta, Ntarget, Nboundary, Nsource, faces,
+                        refl, max_events=max_events, rz_linear_source=rz_linear_source, t_emit_floor=T_emit_floor)
     world = 1
     if allreduce is not None:
         world = allreduce.get_world_size()
@@ -189,37 +205,49 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
     eng.material_update(state._e, state._Tr)
     Tn = evaluate(inv_eos, state.grid(state._e), lambda: _host_copy(state.grid(state._e)), like)
     state._T.copy_(state.flat(Tn))
+    eng.comb_async(Nmax, state.count, state._e)
+    try:
+        sm = eng.fetch(state.host_copies())
+    except _lib.ImcError as ex:
+        if ex.status == 3:
+            raise AssertionError("Fleck factor out of bounds / non-positive temperature in material state") from ex
+        raise
+    t_post = _time.perf_counter()
+    pre_comb = eng.spare  # the tracked (pre-comb) bank after the swap
     if not use_scalar_intensity_Tr:
-        live = eng.bank.view("weight") > 0
-        rad = torch.zeros(eng.nc, dtype=torch.float64, device=eng.device)
-        rad.index_add_(0, eng.bank.view("cell")[live].long(), eng.bank.view("weight")[live].double())
-        state._Tr.copy_(torch.pow(rad / eng.vol / A_RAD, 0.25))
-    stats, esc = eng.host_stats()
-    _lib.TRANSFER["d2h"] += stats.nbytes + esc.nbytes
-    boundary_loss = float(esc[:4].sum())
-
-    crep = eng.comb(Nmax, state.count)
-    comb_disc = crep.energy_before - crep.energy_after
+        live = pre_comb.view("weight") > 0
+        rad_c = torch.zeros(eng.nc, dtype=torch.float64, device=eng.device)
+        rad_c.index_add_(0, pre_comb.view("cell")[live].long(), pre_comb.view("weight")[live].double())
+        state._Tr.copy_(torch.pow(rad_c / eng.vol / A_RAD, 0.25))
+    internal = float(sm.internal_energy)
+    rad = float(sm.comb_after)
+    comb_disc = float(sm.comb_before) - rad
+    boundary_emission = float(sum(sm.e_side))
+    boundary_loss = float(sum(sm.escaped))
+    stats = np.array(sm.stats[:], dtype=np.int64)
     if conserve_comb_energy:
         state._e.add_(eng.disc[: eng.nc] / eng.vol)
         Tn = evaluate(inv_eos, state.grid(state._e), lambda: _host_copy(state.grid(state._e)), like)
         state._T.copy_(state.flat(Tn))
-    rad, internal = eng.energy_totals(state._e)
+        internal += comb_disc
     if allreduce is not None and world > 1:
-        t = torch.tensor([rad, comb_disc], dtype=torch.float64, device=eng.device)
+        t = torch.tensor([rad, comb_disc, boundary_loss], dtype=torch.float64, device=eng.device)
         allreduce.all_reduce(t)
-        rad, comb_disc = float(t[0]) / world, float(t[1]) / world
+        rad, comb_disc, boundary_loss = (float(x) / world for x in t.cpu())
+    if conserve_comb_energy or not use_scalar_intensity_Tr:
+        state.refresh_host()
+    else:
+        state.take_host_copies()
     total = internal + rad
-    energy_loss = total - state.previous_total_energy - rep.boundary_emission + boundary_loss - rep.source_emission
+    energy_loss = total - state.previous_total_energy - boundary_emission + boundary_loss - float(sm.source_emission)
     closure = energy_loss + (0.0 if conserve_comb_energy else comb_disc)
     state.time = state.time + dt
     state.previous_total_energy = total
     state.count += 1
-    state._host.clear()
-    state.refresh_host()
     t_end = _time.perf_counter()
+    ms_src, ms_tr = eng.phase_times()
 
-    n_tr = int(rep.n_transported)
+    n_tr = int(sm.n_bank)
     ev = int(stats[_lib.STAT_EVENTS])
     info = {
         "time": state.time,
@@ -229,22 +257,22 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
         "total_energy": total,
         "total_internal_energy": internal,
         "total_radiation_energy": rad,
-        "boundary_emission": float(rep.boundary_emission),
+        "boundary_emission": boundary_emission,
         "boundary_loss": boundary_loss,
-        "source_emission": float(rep.source_emission),
+        "source_emission": float(sm.source_emission),
         "energy_loss": energy_loss,
         "ledger": {
             "comb_discrepancy": comb_disc,
             "closure": closure,
             "relative_closure": closure / max(abs(total), 1e-300),
-            "emission": float(rep.emission_total),
-            "weight_floor": float(rep.weight_floor),
+            "emission": float(sm.emission_total),
+            "weight_floor": 1e-10 * float(sm.weight_sum) / max(n_tr, 1),
         },
         "profiling": {
             "phase_times_s": {
-                "sampling": (t_eval - t_step_start) + rep.ms_sources * 1e-3,
-                "transport": rep.ms_transport * 1e-3,
-                "postprocess": t_end - t_post,
+                "sampling": (t_eval - t_step_start) + ms_src * 1e-3,
+                "transport": ms_tr * 1e-3,
+                "postprocess": max(t_end - t_step_start - (t_eval - t_step_start) - (ms_src + ms_tr) * 1e-3, 0.0),
                 "total": t_end - t_step_start,
             },
             "transport_events": {

@@ -87,6 +87,20 @@ class ImcCombReport(ctypes.Structure):
     ]
 
 
+FLAG_EVENT_CAP, FLAG_NONFINITE, FLAG_COMB_OVERFLOW = 1, 2, 4
+
+
+class ImcStepSummary(ctypes.Structure):
+    _fields_ = [
+        ("n_census", c_int64), ("n_side", c_int64 * 4), ("n_source", c_int64), ("n_emission", c_int64),
+        ("base_side", c_int64 * 4), ("base_source", c_int64), ("base_emission", c_int64),
+        ("n_bank", c_int64), ("n_out", c_int64), ("flags", c_int32), ("pad", c_int32),
+        ("e_side", c_double * 4), ("source_emission", c_double), ("emission_total", c_double),
+        ("weight_sum", c_double), ("comb_before", c_double), ("comb_after", c_double),
+        ("internal_energy", c_double), ("stats", c_ulonglong * 9), ("escaped", c_double * 4),
+    ]
+
+
 # name -> (restype, argtypes); every symbol declared in include/imcb200.h
 SIGNATURES = {
     "imc_workspace_bytes": (c_size_t, [POINTER(ImcMesh), c_int64]),
@@ -98,6 +112,13 @@ SIGNATURES = {
     "imc_material_update": (c_int, [POINTER(ImcMesh), POINTER(ImcTallies), c_void_p, c_void_p, c_void_p]),
     "imc_comb": (c_int, [POINTER(ImcMesh), POINTER(ImcBank), POINTER(ImcBank), c_int64, c_uint64, c_uint32,
                          c_int32, c_void_p, c_void_p, c_size_t, POINTER(ImcCombReport), c_void_p]),
+    "imc_source_bound": (c_int64, [POINTER(ImcMesh), POINTER(ImcStepParams)]),
+    "imc_step_transport_async": (c_int, [POINTER(ImcMesh), POINTER(ImcMaterial), POINTER(ImcStepParams),
+                                         POINTER(ImcBank), POINTER(ImcTallies), c_void_p, c_size_t, c_void_p,
+                                         c_void_p]),
+    "imc_comb_async": (c_int, [POINTER(ImcMesh), POINTER(ImcBank), POINTER(ImcBank), c_int64, c_uint64, c_uint32,
+                               c_int32, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p, c_void_p]),
+    "imc_phase_times": (c_int, [POINTER(ctypes.c_float), POINTER(ctypes.c_float)]),
     "imc_energy_totals": (c_int, [POINTER(ImcMesh), POINTER(ImcBank), c_void_p, POINTER(c_double),
                                   POINTER(c_double), c_void_p, c_size_t, c_void_p]),
     "imc_philox": (c_int, [c_void_p, c_uint32, c_uint32, c_void_p, c_int64, c_void_p]),

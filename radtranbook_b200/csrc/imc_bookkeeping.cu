@@ -100,16 +100,20 @@ __global__ void __launch_bounds__(NT) k_plan(PlanArgs a) {
   const bool oned = (a.geom == G_SLAB || a.geom == G_SPHERE);
 
   // ---- Fleck factor and emission energy per cell (gray) ----
+  const double sa_thr = oned ? 1e-10 : 1e-12;  // IMC/IMC1D.py:117, IMC/IMC2D.py:917
   for (int c = t; c < nc; c += NT) {
     const double T = a.T[c];
-    if (!isfinite(T) || (oned && !(T > 0.0)) || !isfinite(a.sigma[c]) || !(a.cv[c] > 0.0)) atomicOr(a.err, 2);
+    if (!isfinite(T) || (oned && !(T > 0.0)) || !isfinite(a.sigma[c]) || !(a.cv[c] > 0.0))
+      atomicOr(&a.sum->flags, (int)IMC_FLAG_NONFINITE);
     const double beta = 4.0 * A_RAD * pow3(T) / a.cv[c];
     double f = 1.0 / (1.0 + a.theta * beta * a.sigma[c] * C_LIGHT * a.dt);
     f = fmin(1.0, fmax(0.0, f));
     const double ss = a.sigma[c] * (1.0 - f);
     const double sa = a.sigma[c] * f;
     a.sa[c] = sa; a.ss[c] = ss;
-    a.saf[c] = (float)sa; a.ssf[c] = (float)ss;
+    a.sass[c] = make_float2((float)sa, (float)ss);
+    const double iv = 1.0 / a.vol[c];
+    a.cellf[c] = make_double2(iv, sa > sa_thr ? 1.0 / (sa * a.vol[c] * a.dt) : -1.0 / (a.vol[c] * a.dt));
     double E = A_RAD * C_LIGHT * pow4(fmax(T, 0.0)) * sa * a.dt * a.vol[c];
     if (a.t_emit_floor > 0.0 && T < a.t_emit_floor) E = 0.0;
     a.emit_E[c] = E;
@@ -200,8 +204,8 @@ __global__ void __launch_bounds__(NT) k_plan(PlanArgs a) {
   // ---- boundary faces (one thread per side, sequential cumulative sums) ----
   if (t < 4) {
     const int side = t;
-    a.plan->n_bnd[side] = 0;
-    a.plan->e_bnd[side] = 0.0;
+    a.sum->n_side[side] = 0;
+    a.sum->e_side[side] = 0.0;
     const double* Tf = a.face_T[side];
     if (Tf && a.n_boundary > 0 && !(oned && side >= 2)) {
       const bool along2 = side < 2;
@@ -226,15 +230,22 @@ __global__ void __launch_bounds__(NT) k_plan(PlanArgs a) {
         cdf[q] = Et;
       }
       if (Et > 0.0) {
-        a.plan->n_bnd[side] = a.n_boundary;
+        a.sum->n_side[side] = a.n_boundary;
         const float wq = (float)(Et / (double)a.n_boundary);
-        a.plan->e_bnd[side] = (double)a.n_boundary * (double)wq;
+        a.sum->e_side[side] = (double)a.n_boundary * (double)wq;
       }
     }
   }
+  __syncthreads();
   if (t == 0) {
-    a.plan->n_emit = n_emit; a.plan->e_emit = e_emit;
-    a.plan->n_src = n_src; a.plan->e_src = e_src;
+    // bank layout of this step: census | boundary sides 0..3 | fixed source | emission
+    long long base = a.sum->n_census;
+    for (int q = 0; q < 4; ++q) { a.sum->base_side[q] = base; base += a.sum->n_side[q]; }
+    a.sum->n_source = n_src; a.sum->base_source = base; base += n_src;
+    a.sum->n_emission = n_emit; a.sum->base_emission = base; base += n_emit;
+    a.sum->n_bank = base;
+    a.sum->source_emission = e_src;
+    a.sum->emission_total = e_emit;
   }
 }
 
@@ -265,7 +276,7 @@ __global__ void __launch_bounds__(NT) k_ic_plan(IcArgs a) {
   }
   __syncthreads();
   const long long tot = block_scan_counts(a.n, a.off, nc, sh);
-  if (t == 0) { a.plan->n_emit = tot; }
+  if (t == 0) { a.sum->n_emission = tot; a.sum->base_emission = 0; a.sum->n_bank = tot; }
 }
 
 __global__ void k_material(MatArgs a) {
@@ -287,7 +298,7 @@ __global__ void __launch_bounds__(NT) k_comb_plan(CombPlanArgs a) {
     if (E > 0.0 && ec > 0.0) ew = ec / fmax(1.0, rint((double)a.n_max * ec / E));
     a.ew[b] = ew;
   }
-  if (threadIdx.x == 0) a.plan->comb_e_before = E;
+  if (threadIdx.x == 0) a.sum->comb_before = E;
 }
 
 __global__ void __launch_bounds__(NT) k_canon_eV(const double* e, const double* vol, int nc, double* out) {

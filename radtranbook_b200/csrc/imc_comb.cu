@@ -26,13 +26,14 @@ __global__ void __launch_bounds__(256) k_comb_ecen(CombArgs a) {
   __shared__ WarpStage stages[8];
   WarpStage* st = stages + (threadIdx.x >> 5);
   const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long n_in = *a.d_n_in;
   // block-uniform trip count keeps every warp converged for the aggregated reduction
-  for (long long base = (long long)blockIdx.x * blockDim.x; base < a.n_in; base += stride) {
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < n_in; base += stride) {
     const long long k = base + threadIdx.x;
     bool live = false;
     int b = 0;
     double w = 0.0;
-    if (k < a.n_in) {
+    if (k < n_in) {
       const float wf = a.w[k];
       if (wf > 0.f) { live = true; b = bin_of(a, k); w = (double)wf; }
     }
@@ -42,21 +43,24 @@ __global__ void __launch_bounds__(256) k_comb_ecen(CombArgs a) {
 
 __global__ void __launch_bounds__(CB) k_comb_count(CombArgs a) {
   __shared__ long long sh[CB / 32];
+  __shared__ WarpStage stages[CB / 32];
   const long long k = (long long)blockIdx.x * CB + threadIdx.x;
-  int n = 0;
-  if (k < a.n_in) {
+  const long long n_in = *a.d_n_in;
+  int n = 0, b = 0;
+  if (k < n_in) {
     const float wf = a.w[k];
     if (wf > 0.f) {
-      const int b = bin_of(a, k);
+      b = bin_of(a, k);
       const double ew = a.ew[b];
       if (ew > 0.0) {
         const U4 r = draw(a.seed, (uint32_t)k, 0, a.step, TAG_COMB);
         n = (int)floor((double)wf / ew + u01d(r.x));
-        if (n > 0) atomicAdd(reinterpret_cast<unsigned long long*>(a.ncopy + b), (unsigned long long)n);
       }
     }
     a.cnt[k] = n;
   }
+  // copies per bin: warp-aggregated (the bank is largely grouped by cell)
+  warp_tally1(n > 0, b, (double)n, a.ncopy, stages + (threadIdx.x >> 5));
   const unsigned ws = __reduce_add_sync(FULL, (unsigned)n);
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = ws;
   __syncthreads();
@@ -68,7 +72,8 @@ __global__ void __launch_bounds__(CB) k_comb_count(CombArgs a) {
 }
 
 // exclusive scan of nblk block totals in place (blk[nblk] = total), single block
-__global__ void __launch_bounds__(1024) k_comb_scan(long long* blk, long long nblk, PlanDev* plan) {
+__global__ void __launch_bounds__(1024) k_comb_scan(long long* blk, long long nblk, long long out_capacity,
+                                                    imc_step_summary* sum) {
   __shared__ long long sh[1024];
   const int t = threadIdx.x;
   const long long per = (nblk + 1023) / 1024;
@@ -85,14 +90,21 @@ __global__ void __launch_bounds__(1024) k_comb_scan(long long* blk, long long nb
   }
   long long run = sh[t] - s;
   for (long long q = lo; q < hi; ++q) { const long long x = blk[q]; blk[q] = run; run += x; }
-  if (t == 1023) { blk[nblk] = sh[1023]; plan->comb_total = sh[1023]; }
+  if (t == 1023) {
+    const long long total = sh[1023];
+    blk[nblk] = total;
+    sum->n_out = total;
+    if (total > out_capacity) { atomicOr(&sum->flags, (int)IMC_FLAG_COMB_OVERFLOW); sum->n_census = 0; }
+    else sum->n_census = total;  // the combed bank is the next step's census
+  }
 }
 
 __global__ void __launch_bounds__(CB) k_comb_scatter(CombArgs a) {
   __shared__ int sh[CB / 32];
   const long long k = (long long)blockIdx.x * CB + threadIdx.x;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int n = (k < a.n_in) ? a.cnt[k] : 0;
+  const long long n_in = *a.d_n_in;
+  const int n = (k < n_in) ? a.cnt[k] : 0;
   // block-exclusive scan of n
   int x = n;
 #pragma unroll
@@ -115,6 +127,7 @@ __global__ void __launch_bounds__(CB) k_comb_scatter(CombArgs a) {
     const int g = a.group ? a.group[k] : 0;
     for (int q = 0; q < n; ++q) {
       const long long o = start + q;
+      if (o >= a.out_capacity) break;  // overflow: flagged by the scan, caller regrows
       a.op1[o] = p1; a.od1[o] = d1;
       if (a.op2) a.op2[o] = p2;
       if (a.od2) a.od2[o] = d2;
@@ -128,11 +141,11 @@ __global__ void k_comb_disc(CombArgs a) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   double after = 0.0;
   if (b < a.nb) {
-    after = (double)a.ncopy[b] * (double)(float)a.ew[b];
+    after = a.ncopy[b] * (double)(float)a.ew[b];
     a.disc[b] = a.ecen[b] - after;
   }
   after = warp_sum_d(after);
-  if ((threadIdx.x & 31) == 0 && after != 0.0) atomicAdd(&a.plan->comb_e_after, after);
+  if ((threadIdx.x & 31) == 0 && after != 0.0) atomicAdd(&a.sum->comb_after, after);
 }
 
 int grid_for(long long n, int block) {
@@ -144,14 +157,14 @@ int grid_for(long long n, int block) {
 }  // namespace
 
 cudaError_t imc_launch_comb_ecen(const CombArgs& a, cudaStream_t s) {
-  if (a.n_in <= 0) return cudaSuccess;
+  if (a.n_bound <= 0) return cudaSuccess;
   ++g_imc_launches;
-  k_comb_ecen<<<grid_for(a.n_in, 256), 256, 0, s>>>(a);
+  k_comb_ecen<<<grid_for(a.n_bound, 256), 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 
 cudaError_t imc_launch_comb_count(const CombArgs& a, cudaStream_t s) {
-  const long long nblk = (a.n_in + CB - 1) / CB;
+  const long long nblk = (a.n_bound + CB - 1) / CB;
   if (nblk > 0) {
     ++g_imc_launches;
     k_comb_count<<<(unsigned)nblk, CB, 0, s>>>(a);
@@ -159,12 +172,12 @@ cudaError_t imc_launch_comb_count(const CombArgs& a, cudaStream_t s) {
     if (e != cudaSuccess) return e;
   }
   ++g_imc_launches;
-  k_comb_scan<<<1, 1024, 0, s>>>(a.blk, nblk, a.plan);
+  k_comb_scan<<<1, 1024, 0, s>>>(a.blk, nblk, a.out_capacity, a.sum);
   return cudaGetLastError();
 }
 
 cudaError_t imc_launch_comb_scatter(const CombArgs& a, cudaStream_t s) {
-  const long long nblk = (a.n_in + CB - 1) / CB;
+  const long long nblk = (a.n_bound + CB - 1) / CB;
   if (nblk > 0) {
     ++g_imc_launches;
     k_comb_scatter<<<(unsigned)nblk, CB, 0, s>>>(a);

@@ -1,5 +1,9 @@
 // imc_internal.h — launch-argument structs and workspace layout shared by the kernels
 // of the IMC engine.  Not part of the public ABI.
+//
+// Sizes flow between phases in device memory (imc_step_summary): the host passes only
+// upper bounds used to size grids, and every kernel reads its true element count from the
+// summary, so a whole step runs without a host round trip.
 #pragma once
 #include <cstddef>
 #include <cstdint>
@@ -13,9 +17,8 @@ struct TrackArgs {
   int nx, ny, nc, ng;
   const float* e1;           // nx+1 edges (FP32 copy)
   const float* e2;           // ny+1
-  const float* sa;           // [g][c] Fleck absorption (FP32)
-  const float* ss;           // [g][c] effective scatter (FP32)
-  const double* vol;         // [c]
+  const float2* sass;        // [g][c] (Fleck absorption, effective scatter), FP32
+  const double2* cellf;      // [c] (1/V, 1/(sigma_a V dt) or -1/(V dt))
   double* dep;               // [g][c]
   double* si;                // [g][c]
   double* escaped;           // [4 + ng]
@@ -23,12 +26,11 @@ struct TrackArgs {
   float* p1; float* p2; float* d1; float* d2; float* w; float* t;
   int* cell;
   int* group;
-  long long n;               // bank entries to track
+  const int64_t* n_dev;      // bank entries to track (device)
+  const double* wsum;        // sum of their weights (device): floor = 1e-10 * wsum / n
   unsigned long long* queue; // ticket counter (zeroed before launch)
-  int* err;
+  int* flags;                // IMC_FLAG_* (device)
   float dt;
-  double dt_d;
-  const double* wsum;         // sum of bank weights: floor = 1e-10 * wsum / n
   int reflect_mask;
   long long max_events;
   int cap_is_reference;      // 1: the cap is the reference's (no error flag)
@@ -38,38 +40,28 @@ struct TrackArgs {
   const double* group_edges; // MG
 };
 
-cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, cudaStream_t s);
+cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool smem_cells, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------
 // Workspace layout (byte offsets into the caller's workspace, 256-aligned pieces)
 // ---------------------------------------------------------------------------------
 struct WsLayout {
   size_t e1f, e2f;            // float edges
-  size_t saf, ssf;            // float [ncg]
+  size_t sass;                // float2 [ncg]
+  size_t cellf;               // double2 [nc]
   size_t emit_E;              // double [ncg]  emission energy per (group,) cell
   size_t emit_n;              // int64 [nc]    emission count per cell (order position)
   size_t emit_off;            // int64 [nc+1]  exclusive offsets in source order
   size_t emit_w;              // float [nc]
   size_t tilt;                // double [4*nc] per-cell tilt constants
-  size_t src_n, src_off, src_w, src_QV, src_issued;  // fixed source (same shapes; QV/issued double [nc])
+  size_t src_n, src_off, src_w, src_QV, src_issued;  // fixed source
   size_t face;                // double [4][2][nf] per-side face energies and CDF
-  size_t plan;                // PlanDev
+  size_t summary;             // imc_step_summary used by the synchronous wrappers
   size_t queue;               // uint64 ticket counter
-  size_t err;                 // int
-  size_t wsum;                // double [4] scratch sums
   size_t ecen, ew, ncopy;     // comb: double [nb], double [nb], long long [nb]
   size_t cnt;                 // int32 [cap]    comb copies per entry
   size_t blk;                 // int64 [nblk+1] comb block totals / offsets
   size_t total;
-};
-
-struct PlanDev {              // device-side plan, copied to the host after planning
-  long long n_emit, n_src, n_bnd[4];
-  double e_emit, e_src, e_bnd[4];
-  long long comb_total;
-  double comb_e_before, comb_e_after;
-  double wsum;
-  long long pad[4];
 };
 
 WsLayout imc_ws_layout(const imc_mesh* m, int64_t capacity);
@@ -92,15 +84,15 @@ struct PlanArgs {
   double t_emit_floor;
   // outputs
   double* sa; double* ss;          // FP64 [ncg]
-  float* saf; float* ssf;          // FP32 [ncg]
+  float2* sass;                    // FP32 [ncg]
+  double2* cellf;                  // [c]
   float* e1f; float* e2f;
   double* emit_E; long long* emit_n; long long* emit_off; float* emit_w; double* tilt;
   long long* src_n; long long* src_off; float* src_w; double* src_QV; double* src_issued;
   double* emitted;                 // [c] issued emission energy per cell
   double* face;                    // [4][2][nf]
   int nf;
-  PlanDev* plan;
-  int* err;
+  imc_step_summary* sum;
 };
 cudaError_t imc_launch_plan(const PlanArgs& a, cudaStream_t s);
 
@@ -111,7 +103,7 @@ struct IcArgs {
   long long n_target;
   double t_emit_floor;
   long long* n; long long* off; float* w; double* E;
-  PlanDev* plan;
+  imc_step_summary* sum;           // n_emission = total, base_emission = 0
 };
 cudaError_t imc_launch_ic_plan(const IcArgs& a, cudaStream_t s);
 
@@ -127,26 +119,26 @@ struct CombPlanArgs {
   long long n_max;
   const double* ecen;
   double* ew;
-  PlanDev* plan;
+  imc_step_summary* sum;
 };
 cudaError_t imc_launch_comb_plan(const CombPlanArgs& a, cudaStream_t s);
 
 cudaError_t imc_launch_canon_sum_eV(const double* e, const double* vol, int nc, double* out, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------
-// Source fill kernels
+// Source fill kernels (element count and first bank index read from device memory)
 // ---------------------------------------------------------------------------------
 struct FillArgs {
   int geom, nx, ny, nc;
   const double* e1; const double* e2;
   const double* T;
-  long long n;                 // particles to write
-  long long base;              // first bank index
+  const int64_t* d_n;          // particles to write (device)
+  const int64_t* d_base;       // first bank index (device)
+  long long n_bound;           // host upper bound of *d_n (grid sizing)
   const long long* off;        // [nc+1] offsets in source order
   const float* w;              // [nc] per-cell weight
   const double* tilt;          // [4*nc] or NULL
   int tilt_kind;               // 0 none, 1 slab linear-T, 2 sphere linear-T^4, 3 rz linear
-  double dt;
   double time_scale;           // birth time = u * time_scale (dt; 0 for the IC)
   uint64_t seed; uint32_t step; uint32_t tag;
   float* p1; float* p2; float* d1; float* d2; float* wb; float* t; int* cell; int* group;
@@ -157,28 +149,32 @@ struct BndArgs {
   int geom, nx, ny, side, nf;
   const double* e1; const double* e2;
   const double* face;          // [2][nf]: energies, cumulative (total = last)
-  long long n, base;
+  const int64_t* d_n;
+  const int64_t* d_base;
+  long long n_bound;
   double dt;
   uint64_t seed; uint32_t step;
   float* p1; float* p2; float* d1; float* d2; float* wb; float* t; int* cell; int* group;
 };
 cudaError_t imc_launch_fill_boundary(const BndArgs& a, cudaStream_t s);
 
-cudaError_t imc_launch_wsum(const float* w, long long n, double* out, cudaStream_t s);
+cudaError_t imc_launch_wsum(const float* w, const int64_t* d_n, long long n_bound, double* out, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------
 // Comb kernels
 // ---------------------------------------------------------------------------------
 struct CombArgs {
   int nc, nb, per_group;
-  long long n_in;
+  const int64_t* d_n_in;       // entries to comb (device)
+  long long n_bound;           // host upper bound of *d_n_in (grid sizing)
+  long long out_capacity;
   const float* w; const int* cell; const int* group;
   const float* p1; const float* p2; const float* d1; const float* d2;
-  double* ecen; double* ew; long long* ncopy; int* cnt; long long* blk;
+  double* ecen; double* ew; double* ncopy; int* cnt; long long* blk;  // ncopy: copies per bin (exact in FP64)
   uint64_t seed; uint32_t step;
   float* op1; float* op2; float* od1; float* od2; float* ow; float* ot; int* ocell; int* ogroup;
   double* disc;
-  PlanDev* plan;
+  imc_step_summary* sum;
 };
 cudaError_t imc_launch_comb_ecen(const CombArgs& a, cudaStream_t s);
 cudaError_t imc_launch_comb_count(const CombArgs& a, cudaStream_t s);

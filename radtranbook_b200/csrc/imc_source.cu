@@ -18,8 +18,6 @@ using namespace imcdev;
 
 namespace {
 
-constexpr double PI = 3.14159265358979323846;
-
 __device__ __forceinline__ double pow4(double T) { const double t2 = T * T; return t2 * t2; }
 
 // slab linear-T position in [0, dx], IMC/IMC1D.py:203-217
@@ -87,7 +85,8 @@ __device__ __forceinline__ void iso_dir(int geom, double ua, double ub, double& 
 
 __global__ void k_fill_volume(FillArgs a) {
   const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < a.n; k += stride) {
+  const long long n = *a.d_n, base = *a.d_base;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
     // order position o with off[o] <= k < off[o+1]
     int lo = 0, hi = a.nc;  // search in off[0..nc]
     while (lo < hi) { const int mid = (lo + hi) >> 1; if (a.off[mid + 1] <= k) lo = mid + 1; else hi = mid; }
@@ -133,7 +132,7 @@ __global__ void k_fill_volume(FillArgs a) {
     if (a.geom == G_XY || a.geom == G_RZ) p2 = fmin(fmax(p2, a.e2[j]), a.e2[j + 1]);
     double d1, d2;
     iso_dir(a.geom, u2, u3, d1, d2);
-    const long long b = a.base + k;
+    const long long b = base + k;
     a.p1[b] = (float)p1; a.d1[b] = (float)d1;
     if (a.p2) a.p2[b] = (float)p2;
     if (a.d2) a.d2[b] = (float)d2;
@@ -151,9 +150,11 @@ __global__ void k_fill_boundary(BndArgs a) {
   const int nf = oned ? 1 : (along2 ? a.ny : a.nx);
   const double* Ef = a.face;
   const double* cdf = a.face + a.nf;
+  const long long n = *a.d_n, base = *a.d_base;
+  if (n <= 0) return;
   const double total = cdf[nf - 1];
-  const float wq = (float)(total / (double)a.n);
-  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < a.n; k += stride) {
+  const float wq = (float)(total / (double)n);
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
     const U4 ra = draw(a.seed, (uint32_t)k, 0, a.step, TAG_BOUNDARY | (uint32_t)a.side);
     const U4 rb = draw(a.seed, (uint32_t)k, 1, a.step, TAG_BOUNDARY | (uint32_t)a.side);
     const double ua0 = u01d(ra.x), ua1 = u01d(ra.y), ua2 = u01d(ra.z), ua3 = u01d(ra.w);
@@ -201,7 +202,7 @@ __global__ void k_fill_boundary(BndArgs a) {
         d1 = cospi(2.0 * ua3);
       }
     }
-    const long long b = a.base + k;
+    const long long b = base + k;
     a.p1[b] = (float)p1; a.d1[b] = (float)d1;
     if (a.p2) a.p2[b] = (float)p2;
     if (a.d2) a.d2[b] = (float)d2;
@@ -212,8 +213,9 @@ __global__ void k_fill_boundary(BndArgs a) {
   }
 }
 
-__global__ void k_wsum(const float* w, long long n, double* out) {
+__global__ void k_wsum(const float* w, const int64_t* d_n, double* out) {
   __shared__ double sh[32];
+  const long long n = *d_n;
   double s = 0.0;
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) s += (double)w[k];
@@ -236,22 +238,22 @@ int grid_for(long long n, int block) {
 }  // namespace
 
 cudaError_t imc_launch_fill_volume(const FillArgs& a, cudaStream_t s) {
-  if (a.n <= 0) return cudaSuccess;
+  if (a.n_bound <= 0) return cudaSuccess;
   ++g_imc_launches;
-  k_fill_volume<<<grid_for(a.n, 256), 256, 0, s>>>(a);
+  k_fill_volume<<<grid_for(a.n_bound, 256), 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 
 cudaError_t imc_launch_fill_boundary(const BndArgs& a, cudaStream_t s) {
-  if (a.n <= 0) return cudaSuccess;
+  if (a.n_bound <= 0) return cudaSuccess;
   ++g_imc_launches;
-  k_fill_boundary<<<grid_for(a.n, 256), 256, 0, s>>>(a);
+  k_fill_boundary<<<grid_for(a.n_bound, 256), 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 
-cudaError_t imc_launch_wsum(const float* w, long long n, double* out, cudaStream_t s) {
-  if (n <= 0) return cudaSuccess;
+cudaError_t imc_launch_wsum(const float* w, const int64_t* d_n, long long n_bound, double* out, cudaStream_t s) {
+  if (n_bound <= 0) return cudaSuccess;
   ++g_imc_launches;
-  k_wsum<<<grid_for(n, 256), 256, 0, s>>>(w, n, out);
+  k_wsum<<<grid_for(n_bound, 256), 256, 0, s>>>(w, d_n, out);
   return cudaGetLastError();
 }

@@ -22,9 +22,14 @@ using namespace imcdev;
 
 namespace {
 
+// Block-level counters for rare events (shared-memory atomics keep them out of registers).
+enum : int { B_CENSUS = 0, B_FLOOR, B_REFLECT, B_CAP, B_ESCAPE, B_N };
+
 template <int GEOM, bool SMEM_CELLS>
 __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ unsigned blk_cnt[B_N];
+  __shared__ double blk_esc[4];
   WarpStage* stages = reinterpret_cast<WarpStage*>(smem);
   const int nwarps = blockDim.x >> 5;
   float* E1 = reinterpret_cast<float*>(stages + nwarps);
@@ -33,33 +38,32 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   for (int q = threadIdx.x; q <= a.nx; q += blockDim.x) E1[q] = a.e1[q];
   for (int q = threadIdx.x; q <= a.ny; q += blockDim.x) E2[q] = a.e2[q];
   if (SMEM_CELLS)
-    for (int q = threadIdx.x; q < a.nc; q += blockDim.x) CS[q] = make_float2(a.sa[q], a.ss[q]);
+    for (int q = threadIdx.x; q < a.nc; q += blockDim.x) CS[q] = a.sass[q];
+  if (threadIdx.x < B_N) blk_cnt[threadIdx.x] = 0u;
+  if (threadIdx.x < 4) blk_esc[threadIdx.x] = 0.0;
   __syncthreads();
 
   const int lane = threadIdx.x & 31;
   const unsigned lt_mask = (1u << lane) - 1u;
   WarpStage* st = stages + (threadIdx.x >> 5);
+  const uint32_t n = (uint32_t)*a.n_dev;
 
   // warp-uniform chunk cursor
-  long long chunk_next = 0, chunk_end = 0;
+  uint32_t chunk_next = 0, chunk_end = 0;
   bool drained = false;
 
   // lane state
   bool has = false;
-  long long pid = 0;
+  uint32_t pid = 0, ev = 0;
   float x = 0, y = 0, u = 0, v = 0, w = 0, dcen = 0;
   int ci = 0, cj = 0;
-  uint32_t ev = 0;
-  // per-cell accumulators
-  double acc_lost = 0.0, acc_wd = 0.0;
-  // statistics / escaped energy
-  unsigned s_ev = 0, s_bd = 0, s_sc = 0, s_cen = 0, s_fl = 0, s_rf = 0, s_cap = 0, s_esc = 0;
-  double esc0 = 0, esc1 = 0, esc2 = 0, esc3 = 0;
+  double acc_lost = 0.0, acc_wd = 0.0;  // energy removed / w*s in the current cell
+  unsigned s_bd = 0, s_sc = 0;          // per-event counters (census/cap counted at finish)
 
   const float c_light = (float)C_LIGHT;
   // weight floor, IMC/IMC1D.py:1007 / IMC/IMC2D.py:1771
-  const float weight_floor = (float)(1e-10 * (*a.wsum) / (double)(a.n > 0 ? a.n : 1));
-  const float sa_thr = (GEOM == G_SLAB || GEOM == G_SPHERE) ? 1e-10f : 1e-12f;
+  const float weight_floor = (float)(1e-10 * (*a.wsum) / (double)(n > 0 ? n : 1));
+  const float ss_thr = (GEOM == G_SLAB || GEOM == G_SPHERE) ? 1e-10f : 1e-12f;
 
   for (;;) {
     // ---------------- refill idle lanes from the warp's chunk ----------------
@@ -69,28 +73,26 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
         unsigned long long base = 0;
         if (lane == 0) base = atomicAdd(a.queue, (unsigned long long)a.chunk);
         base = __shfl_sync(FULL, base, 0);
-        if ((long long)base >= a.n) { drained = true; break; }
-        chunk_next = (long long)base;
-        chunk_end = min((long long)base + a.chunk, a.n);
+        if (base >= (unsigned long long)n) { drained = true; break; }
+        chunk_next = (uint32_t)base;
+        chunk_end = (uint32_t)min(base + (unsigned long long)a.chunk, (unsigned long long)n);
       }
-      const int avail = (int)(chunk_end - chunk_next);
-      const int rank = __popc(need & lt_mask);
+      const uint32_t avail = chunk_end - chunk_next;
+      const uint32_t rank = __popc(need & lt_mask);
       if (!has && rank < avail) {
         pid = chunk_next + rank;
         w = a.w[pid];
-        const float t0 = a.t[pid];
-        dcen = (a.dt - t0) * c_light;
+        dcen = (a.dt - a.t[pid]) * c_light;
         if (w > 0.f && dcen > 0.f) {
           x = a.p1[pid]; u = a.d1[pid];
           if (GEOM == G_XY || GEOM == G_RZ) { y = a.p2[pid]; v = a.d2[pid]; }
           const int c = a.cell[pid];
-          ci = c % a.nx; cj = c / a.nx;
+          cj = c / a.nx; ci = c - cj * a.nx;
           ev = 0;
-          acc_lost = 0.0; acc_wd = 0.0;
           has = true;
         }
       }
-      chunk_next += min(__popc(need), avail);
+      chunk_next += min((uint32_t)__popc(need), avail);
       need = __ballot_sync(FULL, !has);
     }
     if (!__any_sync(FULL, has)) break;
@@ -98,50 +100,92 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
     bool flush = false;
     int flush_cell = 0;
     double f_lost = 0.0, f_wd = 0.0;
-    float f_sa = 0.f;
     if (has) {
       const int c = ci + a.nx * cj;
       float sa, ss;
       if (SMEM_CELLS) { const float2 q = CS[c]; sa = q.x; ss = q.y; }
-      else { sa = __ldg(a.sa + c); ss = __ldg(a.ss + c); }
-      ++s_ev;
+      else { const float2 q = __ldg(a.sass + c); sa = q.x; ss = q.y; }
       bool finished = false, frozen = false;
-      if (a.max_events > 0 && ev >= (uint32_t)a.max_events) {
-        // reference: cap hit -> history stops, weight stays in census
-        ++s_cap;
-        if (!a.cap_is_reference) atomicOr(a.err, 1);
+      if (ev >= (uint32_t)a.max_events) {
+        // events-per-history cap (IMC/IMC2D.py:974-977): stops, weight stays in census
+        atomicAdd(&blk_cnt[B_CAP], 1u);
+        if (!a.cap_is_reference) atomicOr(a.flags, (int)IMC_FLAG_EVENT_CAP);
         finished = true;
       } else {
-        const U4 r = draw(a.seed, (uint32_t)pid, ev, a.step, TAG_TRANSPORT);
+        const U4 r = draw(a.seed, pid, ev, a.step, TAG_TRANSPORT);
         ++ev;
-        float d, xn = x, yn = y, un = u, vn = v;
+        float d, sb, L, xn = x, yn = y, un = u, vn = v;
         int evt, cross = X_NONE;
+        // ---- distance to the cell boundary ----
+        float s_rin = BIGF, s_rout = BIGF, s_zlo = BIGF, s_zhi = BIGF, st_ = 0.f, sx = BIGF, sy = BIGF;
+        float din = BIGF, dout = BIGF;
         if (GEOM == G_SLAB) {
           const float xl = E1[ci], xr = E1[ci + 1];
-          const float db = slab_face(x, u, xl, xr);
-          const float ds = scatter_distance(ss, xr - xl, r.x, 1e-10f, true);
-          d = db; evt = EV_BOUNDARY;
-          if (ds < d) { d = ds; evt = EV_SCATTER; }
-          if (dcen < d) { d = dcen; evt = EV_CENSUS; }
+          L = xr - xl;
+          sb = slab_face(x, u, xl, xr);
+        } else if (GEOM == G_SPHERE) {
+          const float r0 = E1[ci], r1 = E1[ci + 1];
+          L = r1 - r0;
+          const float b2 = x * x * ((1.f - u) * (1.f + u));
+          dout = outer_root(x, u, r1, b2);
+          din = inner_root(x, u, r0, b2);
+          sb = fminf(dout, din);
+        } else if (GEOM == G_XY) {
+          const float xl = E1[ci], xr = E1[ci + 1], yl = E2[cj], yr = E2[cj + 1];
+          L = fminf(xr - xl, yr - yl);
+          if (u > 0.f) sx = (xr - x) / u; else if (u < 0.f) sx = (xl - x) / u;
+          if (v > 0.f) sy = (yr - y) / v; else if (v < 0.f) sy = (yl - y) / v;
+          sx = fmaxf(sx, 0.f); sy = fmaxf(sy, 0.f);
+          sb = fminf(sx, sy);
+        } else {
+          const float rin = E1[ci], rout = E1[ci + 1], zlo = E2[cj], zhi = E2[cj + 1];
+          L = fminf(rout - rin, zhi - zlo);
+          const float sin2 = (1.f - v) * (1.f + v);
+          if (sin2 >= 1e-15f) {
+            st_ = sqrtf(sin2);
+            const float b2 = x * x * ((1.f - u) * (1.f + u));
+            s_rout = outer_root(x, u, rout, b2) / st_;
+            const float li = inner_root(x, u, rin, b2);
+            if (li < BIGF) s_rin = li / st_;
+          }
+          if (v > 1e-15f) s_zhi = fmaxf((zhi - y) / v, 0.f);
+          else if (v < -1e-15f) s_zlo = fmaxf((zlo - y) / v, 0.f);
+          sb = fminf(fminf(s_rin, s_rout), fminf(s_zlo, s_zhi));
+        }
+        // ---- effective-scatter distance (reference cap: sigma_s*L > 1e4 -> 1e4/L) ----
+        // -log(u)/sigma competes with s_other = min(boundary, census); when sigma*s_other
+        // is small the scatter loses unless u > exp(-sigma*s_other), tested in FP64 with a
+        // short series, so the logarithm is evaluated only when it can win.
+        float ds = BIGF;
+        {
+          const float sig = (ss * L > 10000.0f) ? 10000.0f / L : (ss > ss_thr ? ss : 0.f);
+          if (sig > 0.f) {
+            const float s_other = fminf(sb, dcen);
+            const double t = (double)sig * (double)s_other;
+            bool may = true;
+            if (t < 0.01) {
+              const double thr = 1.0 - t * (1.0 - t * (0.5 - t * (1.0 / 6.0)));
+              may = u01d(r.x) > thr;
+            }
+            if (may) ds = (ss * L > 10000.0f) ? neglog_u(r.x) * (L * 1e-4f) : neglog_u(r.x) / ss;
+          }
+        }
+        d = sb; evt = EV_BOUNDARY;
+        if (ds < d) { d = ds; evt = EV_SCATTER; }
+        if (dcen < d) { d = dcen; evt = EV_CENSUS; }
+        // ---- move ----
+        if (GEOM == G_SLAB) {
+          const float xl = E1[ci], xr = E1[ci + 1];
           xn = fmaf(u, d, x);
           if (evt == EV_BOUNDARY) { if (u > 0.f) { xn = xr; cross = X_IP; } else { xn = xl; cross = X_IM; } }
           else { if (evt == EV_SCATTER) un = fmaf(2.f, u01f(r.y), -1.f); xn = fminf(fmaxf(xn, xl), xr); }
         } else if (GEOM == G_SPHERE) {
           const float r0 = E1[ci], r1 = E1[ci + 1];
-          const float b2 = x * x * ((1.f - u) * (1.f + u));
-          const float dout = outer_root(x, u, r1, b2);
-          const float din = inner_root(x, u, r0, b2);
-          const bool hit_outer = dout <= din;
-          const float db = hit_outer ? dout : din;
-          const float ds = scatter_distance(ss, r1 - r0, r.x, 1e-10f, true);
-          d = db; evt = EV_BOUNDARY;
-          if (ds < d) { d = ds; evt = EV_SCATTER; }
-          if (dcen < d) { d = dcen; evt = EV_CENSUS; }
           const float ax = fmaf(u, d, x);
           float rn = sqrtf(fmaf(ax, ax, d * d * ((1.f - u) * (1.f + u))));
           float mun = rn > 1e-15f ? (x * u + d) / rn : 1.f;
           if (evt == EV_BOUNDARY) {
-            if (hit_outer) { rn = r1; mun = (x * u + d) / r1; cross = X_IP; }
+            if (dout <= din) { rn = r1; mun = (x * u + d) / r1; cross = X_IP; }
             else { rn = r0; mun = (x * u + d) / r0; cross = X_IM; }
           } else {
             if (evt == EV_SCATTER) mun = fmaf(2.f, u01f(r.y), -1.f);
@@ -150,15 +194,6 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
           xn = rn; un = fminf(1.f, fmaxf(-1.f, mun));
         } else if (GEOM == G_XY) {
           const float xl = E1[ci], xr = E1[ci + 1], yl = E2[cj], yr = E2[cj + 1];
-          float sx = BIGF, sy = BIGF;
-          if (u > 0.f) sx = (xr - x) / u; else if (u < 0.f) sx = (xl - x) / u;
-          if (v > 0.f) sy = (yr - y) / v; else if (v < 0.f) sy = (yl - y) / v;
-          sx = fmaxf(sx, 0.f); sy = fmaxf(sy, 0.f);
-          const float ds = scatter_distance(ss, fminf(xr - xl, yr - yl), r.x, 1e-12f, true);
-          const float sb = fminf(sx, sy);
-          d = sb; evt = EV_BOUNDARY;
-          if (ds < d) { d = ds; evt = EV_SCATTER; }
-          if (dcen < d) { d = dcen; evt = EV_CENSUS; }
           xn = fmaf(u, d, x); yn = fmaf(v, d, y);
           if (evt == EV_BOUNDARY) {
             if (sx <= sy) { if (u > 0.f) { xn = xr; cross = X_IP; } else { xn = xl; cross = X_IM; } yn = fminf(fmaxf(yn, yl), yr); }
@@ -173,25 +208,8 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
             }
             xn = fminf(fmaxf(xn, xl), xr); yn = fminf(fmaxf(yn, yl), yr);
           }
-        } else {  // G_RZ
+        } else {
           const float rin = E1[ci], rout = E1[ci + 1], zlo = E2[cj], zhi = E2[cj + 1];
-          const float sin2 = (1.f - v) * (1.f + v);
-          float s_rin = BIGF, s_rout = BIGF, st_ = 0.f;
-          if (sin2 >= 1e-15f) {
-            st_ = sqrtf(sin2);
-            const float b2 = x * x * ((1.f - u) * (1.f + u));
-            s_rout = outer_root(x, u, rout, b2) / st_;
-            const float li = inner_root(x, u, rin, b2);
-            if (li < BIGF) s_rin = li / st_;
-          }
-          float s_zlo = BIGF, s_zhi = BIGF;
-          if (v > 1e-15f) s_zhi = fmaxf((zhi - y) / v, 0.f);
-          else if (v < -1e-15f) s_zlo = fmaxf((zlo - y) / v, 0.f);
-          const float ds = scatter_distance(ss, fminf(rout - rin, zhi - zlo), r.x, 1e-12f, true);
-          const float sb = fminf(fminf(s_rin, s_rout), fminf(s_zlo, s_zhi));
-          d = sb; evt = EV_BOUNDARY;
-          if (ds < d) { d = ds; evt = EV_SCATTER; }
-          if (dcen < d) { d = dcen; evt = EV_CENSUS; }
           const float l = d * st_;
           const float ax = fmaf(u, l, x);
           float rn = sqrtf(fmaf(ax, ax, l * l * ((1.f - u) * (1.f + u))));
@@ -215,12 +233,13 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
         acc_lost += (double)w - (double)wn;
         acc_wd += (double)(w * d);
         dcen -= d;
-        if (evt == EV_BOUNDARY) ++s_bd; else if (evt == EV_SCATTER) ++s_sc; else ++s_cen;
+        if (evt == EV_BOUNDARY) ++s_bd; else if (evt == EV_SCATTER) ++s_sc;
+        else atomicAdd(&blk_cnt[B_CENSUS], 1u);
 
         if (GEOM == G_XY || GEOM == G_RZ) {
           if (wn <= weight_floor) {
             // IMC/IMC2D.py:1043-1047: history stops in place keeping its weight
-            ++s_fl;
+            atomicAdd(&blk_cnt[B_FLOOR], 1u);
             w = wn;
             frozen = true;
             finished = true;
@@ -230,7 +249,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
           w = wn; x = xn; y = yn; u = un; v = vn;
           if (cross != X_NONE) {
             // leaving the cell: flush the accumulators for the old cell
-            flush = true; flush_cell = c; f_lost = acc_lost; f_wd = acc_wd; f_sa = sa;
+            flush = true; flush_cell = c; f_lost = acc_lost; f_wd = acc_wd;
             acc_lost = 0.0; acc_wd = 0.0;
             int ni = ci, nj = cj;
             if (cross == X_IP) ++ni; else if (cross == X_IM) --ni; else if (cross == X_JP) ++nj; else --nj;
@@ -240,11 +259,10 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
               if ((a.reflect_mask >> side) & 1) {
                 if (side < 2) { u = -u; ni = side == 0 ? 0 : a.nx - 1; }
                 else { v = -v; nj = side == 2 ? 0 : a.ny - 1; }
-                ++s_rf;
+                atomicAdd(&blk_cnt[B_REFLECT], 1u);
               } else {
-                const double we = (double)w;
-                if (side == 0) esc0 += we; else if (side == 1) esc1 += we; else if (side == 2) esc2 += we; else esc3 += we;
-                ++s_esc;
+                atomicAdd(&blk_esc[side], (double)w);
+                atomicAdd(&blk_cnt[B_ESCAPE], 1u);
                 w = 0.f;
                 finished = true;
                 ni = ci; nj = cj;
@@ -256,12 +274,12 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
             if (!finished && w < weight_floor) {
               // IMC/IMC1D.py:188-195: kill and deposit the remainder in the current cell
               // (every cell, including the two edge cells the reference skips)
-              ++s_fl;
+              atomicAdd(&blk_cnt[B_FLOOR], 1u);
               const int c2 = ci + a.nx * cj;
-              const float sa2 = SMEM_CELLS ? CS[c2].x : __ldg(a.sa + c2);
+              const double2 cf = __ldg(a.cellf + c2);
               const double rem = (double)w;
-              atomicAdd(a.dep + c2, rem / a.vol[c2]);
-              if (sa2 > 0.f) atomicAdd(a.si + c2, rem / ((double)sa2 * a.vol[c2] * a.dt_d));
+              atomicAdd(a.dep + c2, rem * cf.x);
+              if (cf.y > 0.0) atomicAdd(a.si + c2, rem * cf.y);
               w = 0.f;
               finished = true;
             }
@@ -277,7 +295,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
         // ended by crossing has already queued the old cell and holds nothing new: a 1-D
         // weight-floor kill after a crossing deposits directly.)
         if (!flush && (acc_lost != 0.0 || acc_wd != 0.0)) {
-          flush = true; flush_cell = c; f_lost = acc_lost; f_wd = acc_wd; f_sa = sa;
+          flush = true; flush_cell = c; f_lost = acc_lost; f_wd = acc_wd;
         }
         acc_lost = 0.0; acc_wd = 0.0;
         a.w[pid] = w;
@@ -291,34 +309,35 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
       }
     }
     // ---------------- converged tally flush ----------------
+    // cellf[c] = (1/V, si factor): si factor > 0 is 1/(sigma_a V dt); < 0 is -1/(V dt),
+    // meaning the cell's sigma_a is below the threshold and w*s is the estimator.
     double vd = 0.0, vs = 0.0;
     if (flush) {
-      const double vol = a.vol[flush_cell];
-      vd = f_lost / vol;
-      vs = (f_sa > sa_thr ? f_lost / (double)f_sa : f_wd) / (vol * a.dt_d);
+      const double2 cf = __ldg(a.cellf + flush_cell);
+      vd = f_lost * cf.x;
+      vs = cf.y > 0.0 ? f_lost * cf.y : -f_wd * cf.y;
     }
     warp_tally2(flush, flush_cell, vd, vs, a.dep, a.si, st);
   }
 
   // ---------------- statistics ----------------
-  const unsigned long long t_ev = warp_sum_u(s_ev), t_bd = warp_sum_u(s_bd), t_sc = warp_sum_u(s_sc),
-                           t_cen = warp_sum_u(s_cen), t_fl = warp_sum_u(s_fl), t_rf = warp_sum_u(s_rf),
-                           t_cap = warp_sum_u(s_cap), t_esc = warp_sum_u(s_esc);
-  const double e0 = warp_sum_d(esc0), e1 = warp_sum_d(esc1), e2 = warp_sum_d(esc2), e3 = warp_sum_d(esc3);
+  const unsigned long long t_bd = warp_sum_u(s_bd), t_sc = warp_sum_u(s_sc);
   if (lane == 0) {
-    if (t_ev) atomicAdd(a.stats + S_EVENTS, t_ev);
     if (t_bd) atomicAdd(a.stats + S_BOUNDARY, t_bd);
     if (t_sc) atomicAdd(a.stats + S_SCATTER, t_sc);
-    if (t_cen) atomicAdd(a.stats + S_CENSUS, t_cen);
-    if (t_fl) atomicAdd(a.stats + S_FLOOR, t_fl);
-    if (t_rf) atomicAdd(a.stats + S_REFLECT, t_rf);
-    if (t_cap) atomicAdd(a.stats + S_CAP, t_cap);
-    if (t_esc) atomicAdd(a.stats + S_ESCAPE, t_esc);
-    if (e0 != 0.0) atomicAdd(a.escaped + 0, e0);
-    if (e1 != 0.0) atomicAdd(a.escaped + 1, e1);
-    if (e2 != 0.0) atomicAdd(a.escaped + 2, e2);
-    if (e3 != 0.0) atomicAdd(a.escaped + 3, e3);
+    if (t_bd + t_sc) atomicAdd(a.stats + S_EVENTS, t_bd + t_sc);
   }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned long long cen = blk_cnt[B_CENSUS], cap = blk_cnt[B_CAP];
+    if (cen) atomicAdd(a.stats + S_CENSUS, cen);
+    if (cen + cap) atomicAdd(a.stats + S_EVENTS, cen + cap);
+    if (blk_cnt[B_FLOOR]) atomicAdd(a.stats + S_FLOOR, (unsigned long long)blk_cnt[B_FLOOR]);
+    if (blk_cnt[B_REFLECT]) atomicAdd(a.stats + S_REFLECT, (unsigned long long)blk_cnt[B_REFLECT]);
+    if (cap) atomicAdd(a.stats + S_CAP, cap);
+    if (blk_cnt[B_ESCAPE]) atomicAdd(a.stats + S_ESCAPE, (unsigned long long)blk_cnt[B_ESCAPE]);
+  }
+  if (threadIdx.x < 4 && blk_esc[threadIdx.x] != 0.0) atomicAdd(a.escaped + threadIdx.x, blk_esc[threadIdx.x]);
 }
 
 template <int GEOM, bool SM>
@@ -336,8 +355,8 @@ cudaError_t launch_one(const TrackArgs& a, int block, int grid, cudaStream_t s) 
 
 }  // namespace
 
-cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, cudaStream_t s) {
-  const bool sm = a.nc <= 4096;
+cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool sm, cudaStream_t s) {
+  ++g_imc_launches;
   switch (geom) {
     case G_SLAB: return sm ? launch_one<G_SLAB, true>(a, block, grid, s) : launch_one<G_SLAB, false>(a, block, grid, s);
     case G_SPHERE: return sm ? launch_one<G_SPHERE, true>(a, block, grid, s) : launch_one<G_SPHERE, false>(a, block, grid, s);

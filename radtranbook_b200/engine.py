@@ -15,7 +15,8 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import ImcBank, ImcCombReport, ImcMaterial, ImcMesh, ImcStepParams, ImcStepReport, ImcTallies
+from ._lib import (ImcBank, ImcCombReport, ImcMaterial, ImcMesh, ImcStepParams, ImcStepReport, ImcStepSummary,
+                   ImcTallies)
 
 A_RAD = 0.01372
 C_LIGHT = 29.98
@@ -123,6 +124,18 @@ class Engine:
         self.disc = torch.zeros(ncg, **f64)
         self.ctal = ImcTallies(_ptr(self.dep), _ptr(self.si), _ptr(self.emitted), _ptr(self.sigma_a),
                                _ptr(self.sigma_s), _ptr(self.escaped), _ptr(self.stats))
+        # device step summary (sizes, energies, statistics) and its pinned host copy; the
+        # asynchronous step writes its statistics and escaped energy straight into it
+        nsum = ctypes.sizeof(ImcStepSummary)
+        self.summary_dev = torch.zeros(nsum, dtype=torch.uint8, device=dev)
+        self.summary_host = torch.zeros(nsum, dtype=torch.uint8, pin_memory=True)
+        self.summary = ImcStepSummary.from_address(self.summary_host.data_ptr())
+        base = self.summary_dev.data_ptr()
+        self.ctal_async = ImcTallies(_ptr(self.dep), _ptr(self.si), _ptr(self.emitted), _ptr(self.sigma_a),
+                                     _ptr(self.sigma_s), base + ImcStepSummary.escaped.offset,
+                                     base + ImcStepSummary.stats.offset)
+        self._census_dev_valid = False
+        self._upper = 0
         mg = n_groups > 1
         self.bank = Bank(capacity, dev, mg)
         self.spare = Bank(capacity, dev, mg)
@@ -164,6 +177,7 @@ class Engine:
                                       self.seed, ctypes.byref(cb), wsp, wsn, ctypes.byref(n_out), self._stream())
         _lib.check("imc_init_census", st)
         self.bank.size = int(cb.size)
+        self._census_dev_valid = False
         return self.bank.size
 
     def transport(self, T: torch.Tensor, sigma: torch.Tensor, cv: torch.Tensor, source: torch.Tensor | None,
@@ -198,6 +212,7 @@ class Engine:
 
         cb = self._call_bank("imc_step_transport", run, self.bank, lambda: rep.required_capacity)
         self.bank.size = int(cb.size)
+        self._census_dev_valid = False
         res = StepResult(report=rep)
         return res
 
@@ -222,6 +237,7 @@ class Engine:
         cb = self._call_bank("imc_comb", run, dst, lambda: rep.required_capacity)
         dst.size = int(cb.size)
         self.bank, self.spare = dst, src
+        self._census_dev_valid = False
         return rep
 
     def energy_totals(self, e: torch.Tensor) -> tuple[float, float]:
@@ -236,3 +252,103 @@ class Engine:
 
     def host_stats(self) -> tuple[np.ndarray, np.ndarray]:
         return self.stats.cpu().numpy(), self.escaped.cpu().numpy()
+
+    # ------------------------------------------------------------------ asynchronous step
+    # One step = transport_async -> material_update -> (caller's inv_eos) -> comb_async ->
+    # fetch(): a single device->host copy of the summary and one stream synchronisation.
+    def _params(self, step, dt, theta, n_target, n_boundary, n_source, face_T, reflect, max_events,
+                rz_linear_source, t_emit_floor) -> ImcStepParams:
+        par = ImcStepParams()
+        par.seed = self.seed
+        par.step = int(step) & 0xFFFFFFFF
+        for q in range(4):
+            par.reflect[q] = int(bool(reflect[q])) if q < len(reflect) else 0
+            par.face_T[q] = _ptr(face_T[q]) if q < len(face_T) and face_T[q] is not None else None
+        par.dt, par.theta = float(dt), float(theta)
+        par.n_target, par.n_boundary, par.n_source = int(n_target), int(n_boundary), int(n_source)
+        par.max_events = int(max_events)
+        par.rz_linear_source = int(bool(rz_linear_source))
+        par.t_emit_floor = float(t_emit_floor)
+        par.block_size = int(self.launch["block_size"])
+        par.blocks_per_sm = int(self.launch["blocks_per_sm"])
+        par.chunk = int(self.launch["chunk"])
+        par.reserved = int(self.launch.get("smem_cells", 0))
+        return par
+
+    def _set_census_count(self, n: int) -> None:
+        self.summary_dev[:8].copy_(torch.tensor([int(n)], dtype=torch.int64).view(torch.uint8))
+        self._census_dev_valid = True
+
+    def transport_async(self, T, sigma, cv, source, step, dt, theta, n_target, n_boundary, n_source, face_T,
+                        reflect, max_events=0, rz_linear_source=True, t_emit_floor=0.0) -> int:
+        """Sources + tracking without a host synchronisation.  Returns the host upper bound
+        of the tracked bank size (the true size is in the device summary)."""
+        if not self._census_dev_valid:
+            self._set_census_count(self.bank.size)
+        self._mat = ImcMaterial(_ptr(T), _ptr(sigma), _ptr(cv), _ptr(source))
+        self._par = self._params(step, dt, theta, n_target, n_boundary, n_source, face_T, reflect, max_events,
+                                 rz_linear_source, t_emit_floor)
+        bound = int(self.lib.imc_source_bound(ctypes.byref(self.cmesh), ctypes.byref(self._par)))
+        self.bank.ensure(self.bank.size + bound)
+        wsp, wsn = self._ws(self.bank.capacity)
+        cb = self.bank.c()
+        st = self.lib.imc_step_transport_async(ctypes.byref(self.cmesh), ctypes.byref(self._mat),
+                                               ctypes.byref(self._par), ctypes.byref(cb),
+                                               ctypes.byref(self.ctal_async), wsp, wsn, self.summary_dev.data_ptr(),
+                                               self._stream())
+        _lib.check("imc_step_transport_async", st)
+        self._upper = self.bank.size + bound
+        return self._upper
+
+    def comb_async(self, n_max: int, step: int, e: torch.Tensor | None, per_group: bool = False) -> None:
+        self.spare.size = 0
+        self.spare.ensure(int(1.15 * n_max) + 2 * self.nc * self.ng + 4096)
+        self._comb_args = (int(n_max), int(step), e, per_group)
+        self._launch_comb()
+
+    def _launch_comb(self) -> None:
+        n_max, step, e, per_group = self._comb_args
+        cin = self.bank.c()
+        cin.size = self._upper
+        cout = self.spare.c()
+        wsp, wsn = self._ws(max(self._upper, self.bank.capacity))
+        st = self.lib.imc_comb_async(ctypes.byref(self.cmesh), ctypes.byref(cin), ctypes.byref(cout), n_max,
+                                     self.seed, step & 0xFFFFFFFF, int(per_group), _ptr(self.disc), _ptr(e),
+                                     wsp, wsn, self.summary_dev.data_ptr(), self._stream())
+        _lib.check("imc_comb_async", st)
+
+    def fetch(self, host_copies=()) -> ImcStepSummary:
+        """Copy the summary (and any (device, pinned host) pairs) to the host and synchronise.
+        A comb overflow is handled by growing the output bank and combing again (the input
+        bank is untouched by the comb)."""
+        stream = torch.cuda.current_stream(self.device)
+        for d, h in host_copies:
+            h.copy_(d, non_blocking=True)
+        self.summary_host.copy_(self.summary_dev, non_blocking=True)
+        stream.synchronize()
+        _lib.TRANSFER["d2h"] += self.summary_host.numel()
+        sm = self.summary
+        if sm.flags & _lib.FLAG_NONFINITE:
+            raise _lib.ImcError("imc_step_transport_async", 3)
+        if sm.flags & _lib.FLAG_EVENT_CAP:
+            raise _lib.ImcError("imc_step_transport_async", 2)
+        if sm.flags & _lib.FLAG_COMB_OVERFLOW:
+            self.spare.ensure(int(sm.n_out * 1.1) + 1024)
+            off = ImcStepSummary.flags.offset
+            self.summary_dev[off:off + 4].zero_()
+            self._launch_comb()
+            self.summary_host.copy_(self.summary_dev, non_blocking=True)
+            stream.synchronize()
+            if sm.flags & _lib.FLAG_COMB_OVERFLOW:
+                raise _lib.ImcError("imc_comb_async", 1)
+        self.spare.size = int(sm.n_out)
+        self.bank.size = int(sm.n_bank)
+        self.bank, self.spare = self.spare, self.bank
+        self._census_dev_valid = True  # the comb wrote n_census = n_out
+        return sm
+
+    def phase_times(self) -> tuple[float, float]:
+        a, b = ctypes.c_float(0), ctypes.c_float(0)
+        if self.lib.imc_phase_times(ctypes.byref(a), ctypes.byref(b)) != 0:
+            return 0.0, 0.0
+        return a.value, b.value

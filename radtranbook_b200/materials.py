@@ -40,7 +40,7 @@ def evaluate(fn, T_dev: torch.Tensor, T_host_fn, like: torch.Tensor) -> torch.Te
             out = torch.as_tensor(np.asarray(out, dtype=np.float64), device=like.device)
         return torch.broadcast_to(out.to(like.device, torch.float64), like.shape)
     out = fn(T_host_fn())
-    arr = np.ascontiguousarray(np.broadcast_to(np.asarray(out, dtype=np.float64), tuple(like.shape)))
+    arr = np.array(np.broadcast_to(np.asarray(out, dtype=np.float64), tuple(like.shape)), order="C", copy=True)
     TRANSFER["h2d"] += arr.nbytes
     return torch.as_tensor(arr, device=like.device)
 
