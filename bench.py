@@ -214,6 +214,13 @@ def run_ours(args, rank: int, world: int):
     state = fresh()
     state, _, _, _ = _gpu_steps(p, state, args.warmup, True, dist)
     eng = state._engine
+    tuned = None
+    if not args.no_tune:
+        tuned = imc2d.tune(state)
+        launch_shape = dict(eng.launch)
+        if args.tune_log:
+            with open(args.tune_log, "w") as f:
+                json.dump(tuned, f, indent=1)
     barrier()
     s0 = torch.cuda.Event(enable_timing=True)
     s1 = torch.cuda.Event(enable_timing=True)
@@ -250,6 +257,8 @@ def run_ours(args, rank: int, world: int):
 
     # ---------------- end to end through the drop-in API with host callables ----------------
     state2 = fresh()
+    if tuned is not None:
+        state2._engine.launch.update(launch_shape)
     state2, _, _, _ = _gpu_steps(p, state2, args.warmup, False, dist)
     barrier()
     tr0 = dict(_lib.TRANSFER)
@@ -295,7 +304,10 @@ def run_ours(args, rank: int, world: int):
         "config": {"workload": "crooked_pipe_rz_60x210", "source_particles_per_step": p["Ntarget"] + p["Nboundary"],
                    "nmax": p["Nmax"], "scale": args.scale, "precision": "f32 tracking, f64 tallies/ledger",
                    "l2": "bank of ~8.7e6 particles x 32 B > 126 MB L2 (inputs larger than L2)",
-                   "parallelism": f"replicas{world}" if world > 1 else "single"},
+                   "parallelism": f"replicas{world}" if world > 1 else "single",
+                   "launch": dict(eng.launch),
+                   "autotune": None if tuned is None else {"best_ms": tuned["best_ms"], "worst_ms": tuned["worst_ms"],
+                                                           "candidates": len(tuned["trials"])}},
         "histories_per_s": hist_all / (tmax * 1e-3),
         "segments_per_step": seg_all / args.steps,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
@@ -317,6 +329,8 @@ def main():
     ap.add_argument("--cpu-scale", type=float, default=0.5)
     ap.add_argument("--cpu-steps", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--tune-log", default=None, help="write the autotuner's trials to this JSON file")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

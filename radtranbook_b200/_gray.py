@@ -297,6 +297,18 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
     return state, info
 
 
+def tune(state: GrayState, grid: dict | None = None, repeats: int = 2) -> dict:
+    """Autotune the tracking launch shape on the state's census, replaying its last step's
+    transport (call after at least one step).  Installs the best shape on the engine."""
+    from .autotune import tune_tracking
+
+    eng = state._engine
+    if eng._last_transport is None:
+        raise RuntimeError("tune() needs one completed step to replay")
+    args, kwargs = eng._last_transport
+    return tune_tracking(eng, args, kwargs, grid=grid, repeats=repeats)
+
+
 def init_state(engine: Engine, dim: int, shape: tuple, Ntarget, Tinit, Tr_init, eos, inv_eos, Ntarget_ic,
                T_emit_floor=0.0) -> GrayState:
     dev = engine.device

@@ -199,8 +199,10 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   ta.group_edges = mesh->group_edges;
   const int block = par->block_size > 0 ? par->block_size : 256;
   const int bps = par->blocks_per_sm > 0 ? par->blocks_per_sm : 3;
+  // reserved: bit 0 = stage the cell table in shared memory, bit 1 = prefetch the next draw
   const bool smem_cells = (par->reserved & 1) ? true : (nc <= 4096);
-  IMC_CUDA(imc_launch_track(ta, mesh->geometry, block, sm_count() * bps, smem_cells, s));
+  const bool prefetch = (par->reserved & 2) != 0;
+  IMC_CUDA(imc_launch_track(ta, mesh->geometry, block, sm_count() * bps, smem_cells, prefetch, s));
   if (pe.ok) { IMC_CUDA(cudaEventRecord(pe.e[2], s)); pe.recorded = true; }
   return IMC_OK;
 }

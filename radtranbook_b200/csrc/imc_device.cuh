@@ -73,21 +73,21 @@ struct Ev {
 
 // ---- 1-D slab: distance to the exit face in the direction of mu ----
 __device__ __forceinline__ float slab_face(float x, float mu, float xl, float xr) {
-  const float db = (mu > 0.f ? (xr - x) : (xl - x)) / mu;
+  const float db = __fdividef(mu > 0.f ? (xr - x) : (xl - x), mu);
   return fmaxf(db, 0.f);
 }
 
 // ---- sphere / cylinder: cancellation-free roots of l^2 + 2 r mu l + (r^2 - R^2) = 0 ----
 __device__ __forceinline__ float outer_root(float r, float mu, float R, float b2) {
   const float q = sqrtf(fmaxf(fmaf(R, R, -b2), 0.f));
-  float l = (mu >= 0.f) ? (R - r) * (R + r) / fmaxf(fmaf(r, mu, q), 1e-30f) : q - r * mu;
+  float l = (mu >= 0.f) ? __fdividef((R - r) * (R + r), fmaxf(fmaf(r, mu, q), 1e-30f)) : q - r * mu;
   return fmaxf(l, 0.f);
 }
 __device__ __forceinline__ float inner_root(float r, float mu, float R, float b2) {
   if (!(R > 0.f) || !(mu < 0.f)) return BIGF;
   const float disc = fmaf(R, R, -b2);
   if (!(disc > 0.f)) return BIGF;
-  const float l = (r - R) * (r + R) / (sqrtf(disc) - r * mu);
+  const float l = __fdividef((r - R) * (r + R), sqrtf(disc) - r * mu);
   return fmaxf(l, 0.f);
 }
 

@@ -40,7 +40,8 @@ struct TrackArgs {
   const double* group_edges; // MG
 };
 
-cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool smem_cells, cudaStream_t s);
+cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool smem_cells, bool prefetch,
+                             cudaStream_t s);
 
 // ---------------------------------------------------------------------------------
 // Workspace layout (byte offsets into the caller's workspace, 256-aligned pieces)

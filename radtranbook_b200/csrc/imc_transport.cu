@@ -25,7 +25,7 @@ namespace {
 // Block-level counters for rare events (shared-memory atomics keep them out of registers).
 enum : int { B_CENSUS = 0, B_FLOOR, B_REFLECT, B_CAP, B_ESCAPE, B_N };
 
-template <int GEOM, bool SMEM_CELLS>
+template <int GEOM, bool SMEM_CELLS, bool PREFETCH>
 __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ unsigned blk_cnt[B_N];
@@ -55,6 +55,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   // lane state
   bool has = false;
   uint32_t pid = 0, ev = 0;
+  U4 rnext{0u, 0u, 0u, 0u};  // PREFETCH: the next event's draw, computed one event ahead
   float x = 0, y = 0, u = 0, v = 0, w = 0, dcen = 0;
   int ci = 0, cj = 0;
   double acc_lost = 0.0, acc_wd = 0.0;  // energy removed / w*s in the current cell
@@ -89,6 +90,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
           const int c = a.cell[pid];
           cj = c / a.nx; ci = c - cj * a.nx;
           ev = 0;
+          if (PREFETCH) rnext = draw(a.seed, pid, 0u, a.step, TAG_TRANSPORT);
           has = true;
         }
       }
@@ -112,7 +114,15 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
         if (!a.cap_is_reference) atomicOr(a.flags, (int)IMC_FLAG_EVENT_CAP);
         finished = true;
       } else {
-        const U4 r = draw(a.seed, pid, ev, a.step, TAG_TRANSPORT);
+        U4 r;
+        if (PREFETCH) {
+          // this event's numbers were drawn during the previous event; draw the next now so
+          // its dependent multiply chain overlaps this event's geometry
+          r = rnext;
+          rnext = draw(a.seed, pid, ev + 1u, a.step, TAG_TRANSPORT);
+        } else {
+          r = draw(a.seed, pid, ev, a.step, TAG_TRANSPORT);
+        }
         ++ev;
         float d, sb, L, xn = x, yn = y, un = u, vn = v;
         int evt, cross = X_NONE;
@@ -133,8 +143,8 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
         } else if (GEOM == G_XY) {
           const float xl = E1[ci], xr = E1[ci + 1], yl = E2[cj], yr = E2[cj + 1];
           L = fminf(xr - xl, yr - yl);
-          if (u > 0.f) sx = (xr - x) / u; else if (u < 0.f) sx = (xl - x) / u;
-          if (v > 0.f) sy = (yr - y) / v; else if (v < 0.f) sy = (yl - y) / v;
+          if (u > 0.f) sx = __fdividef(xr - x, u); else if (u < 0.f) sx = __fdividef(xl - x, u);
+          if (v > 0.f) sy = __fdividef(yr - y, v); else if (v < 0.f) sy = __fdividef(yl - y, v);
           sx = fmaxf(sx, 0.f); sy = fmaxf(sy, 0.f);
           sb = fminf(sx, sy);
         } else {
@@ -144,12 +154,13 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
           if (sin2 >= 1e-15f) {
             st_ = sqrtf(sin2);
             const float b2 = x * x * ((1.f - u) * (1.f + u));
-            s_rout = outer_root(x, u, rout, b2) / st_;
+            const float ist = __frcp_rn(st_);
+            s_rout = outer_root(x, u, rout, b2) * ist;
             const float li = inner_root(x, u, rin, b2);
-            if (li < BIGF) s_rin = li / st_;
+            if (li < BIGF) s_rin = li * ist;
           }
-          if (v > 1e-15f) s_zhi = fmaxf((zhi - y) / v, 0.f);
-          else if (v < -1e-15f) s_zlo = fmaxf((zlo - y) / v, 0.f);
+          if (v > 1e-15f) s_zhi = fmaxf(__fdividef(zhi - y, v), 0.f);
+          else if (v < -1e-15f) s_zlo = fmaxf(__fdividef(zlo - y, v), 0.f);
           sb = fminf(fminf(s_rin, s_rout), fminf(s_zlo, s_zhi));
         }
         // ---- effective-scatter distance (reference cap: sigma_s*L > 1e4 -> 1e4/L) ----
@@ -167,7 +178,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
               const double thr = 1.0 - t * (1.0 - t * (0.5 - t * (1.0 / 6.0)));
               may = u01d(r.x) > thr;
             }
-            if (may) ds = (ss * L > 10000.0f) ? neglog_u(r.x) * (L * 1e-4f) : neglog_u(r.x) / ss;
+            if (may) ds = (ss * L > 10000.0f) ? neglog_u(r.x) * (L * 1e-4f) : __fdividef(neglog_u(r.x), ss);
           }
         }
         d = sb; evt = EV_BOUNDARY;
@@ -214,7 +225,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
           const float ax = fmaf(u, l, x);
           float rn = sqrtf(fmaf(ax, ax, l * l * ((1.f - u) * (1.f + u))));
           yn = fmaf(d, v, y);
-          if (rn > 1e-15f && l > 0.f) un = fminf(1.f, fmaxf(-1.f, fmaf(x, u, l) / rn));
+          if (rn > 1e-15f && l > 0.f) un = fminf(1.f, fmaxf(-1.f, __fdividef(fmaf(x, u, l), rn)));
           if (evt == EV_BOUNDARY) {
             if (sb == s_rin) { rn = rin; cross = X_IM; }
             else if (sb == s_rout) { rn = rout; cross = X_IP; }
@@ -229,7 +240,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
           xn = rn;
         }
         // implicit capture; the energy removed is the exact difference of the FP32 weights
-        const float wn = w * expf(-sa * d);
+        const float wn = w * __expf(-sa * d);
         acc_lost += (double)w - (double)wn;
         acc_wd += (double)(w * d);
         dcen -= d;
@@ -340,28 +351,34 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   if (threadIdx.x < 4 && blk_esc[threadIdx.x] != 0.0) atomicAdd(a.escaped + threadIdx.x, blk_esc[threadIdx.x]);
 }
 
-template <int GEOM, bool SM>
+template <int GEOM, bool SM, bool PF>
 cudaError_t launch_one(const TrackArgs& a, int block, int grid, cudaStream_t s) {
   const int nwarps = block / 32;
   size_t sh = nwarps * sizeof(WarpStage) + sizeof(float) * (a.nx + a.ny + 4);
   if (SM) sh += sizeof(float2) * a.nc;
   if (sh > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_track<GEOM, SM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+    cudaError_t e = cudaFuncSetAttribute(k_track<GEOM, SM, PF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
     if (e != cudaSuccess) return e;
   }
-  k_track<GEOM, SM><<<grid, block, sh, s>>>(a);
+  k_track<GEOM, SM, PF><<<grid, block, sh, s>>>(a);
   return cudaGetLastError();
+}
+
+template <int GEOM>
+cudaError_t launch_geom(const TrackArgs& a, int block, int grid, bool sm, bool pf, cudaStream_t s) {
+  if (sm) return pf ? launch_one<GEOM, true, true>(a, block, grid, s) : launch_one<GEOM, true, false>(a, block, grid, s);
+  return pf ? launch_one<GEOM, false, true>(a, block, grid, s) : launch_one<GEOM, false, false>(a, block, grid, s);
 }
 
 }  // namespace
 
-cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool sm, cudaStream_t s) {
+cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool sm, bool pf, cudaStream_t s) {
   ++g_imc_launches;
   switch (geom) {
-    case G_SLAB: return sm ? launch_one<G_SLAB, true>(a, block, grid, s) : launch_one<G_SLAB, false>(a, block, grid, s);
-    case G_SPHERE: return sm ? launch_one<G_SPHERE, true>(a, block, grid, s) : launch_one<G_SPHERE, false>(a, block, grid, s);
-    case G_XY: return sm ? launch_one<G_XY, true>(a, block, grid, s) : launch_one<G_XY, false>(a, block, grid, s);
-    case G_RZ: return sm ? launch_one<G_RZ, true>(a, block, grid, s) : launch_one<G_RZ, false>(a, block, grid, s);
+    case G_SLAB: return launch_geom<G_SLAB>(a, block, grid, sm, pf, s);
+    case G_SPHERE: return launch_geom<G_SPHERE>(a, block, grid, sm, pf, s);
+    case G_XY: return launch_geom<G_XY>(a, block, grid, sm, pf, s);
+    case G_RZ: return launch_geom<G_RZ>(a, block, grid, sm, pf, s);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -140,7 +140,8 @@ class Engine:
         self.bank = Bank(capacity, dev, mg)
         self.spare = Bank(capacity, dev, mg)
         self.ws = torch.empty(0, dtype=torch.uint8, device=dev)
-        self.launch = dict(block_size=0, blocks_per_sm=0, chunk=0)
+        self.launch = dict(block_size=256, blocks_per_sm=8, chunk=128, smem_cells=0, prefetch=0)
+        self._last_transport = None
 
     # ------------------------------------------------------------------ helpers
     def _stream(self) -> int:
@@ -185,21 +186,8 @@ class Engine:
                   face_T: list, reflect, max_events: int = 0, rz_linear_source: bool = True,
                   t_emit_floor: float = 0.0) -> StepResult:
         mat = ImcMaterial(_ptr(T), _ptr(sigma), _ptr(cv), _ptr(source))
-        faces = [None if f is None else _ptr(f) for f in face_T]
-        par = ImcStepParams()
-        par.seed = self.seed
-        par.step = int(step) & 0xFFFFFFFF
-        for q in range(4):
-            par.reflect[q] = int(bool(reflect[q])) if q < len(reflect) else 0
-            par.face_T[q] = faces[q] if q < len(faces) else None
-        par.dt, par.theta = float(dt), float(theta)
-        par.n_target, par.n_boundary, par.n_source = int(n_target), int(n_boundary), int(n_source)
-        par.max_events = int(max_events)
-        par.rz_linear_source = int(bool(rz_linear_source))
-        par.t_emit_floor = float(t_emit_floor)
-        par.block_size = int(self.launch["block_size"])
-        par.blocks_per_sm = int(self.launch["blocks_per_sm"])
-        par.chunk = int(self.launch["chunk"])
+        par = self._params(step, dt, theta, n_target, n_boundary, n_source, face_T, reflect, max_events,
+                           rz_linear_source, t_emit_floor)
         rep = ImcStepReport()
         # sources add at most n_target + n_source + ncell (ceil) + 4 * n_boundary entries
         self.bank.ensure(self.bank.size + int(n_target) + int(n_source) + 2 * self.nc + 4 * int(n_boundary) + 16)
@@ -272,7 +260,7 @@ class Engine:
         par.block_size = int(self.launch["block_size"])
         par.blocks_per_sm = int(self.launch["blocks_per_sm"])
         par.chunk = int(self.launch["chunk"])
-        par.reserved = int(self.launch.get("smem_cells", 0))
+        par.reserved = int(bool(self.launch.get("smem_cells", 0))) | (int(bool(self.launch.get("prefetch", 0))) << 1)
         return par
 
     def _set_census_count(self, n: int) -> None:
@@ -285,6 +273,9 @@ class Engine:
         of the tracked bank size (the true size is in the device summary)."""
         if not self._census_dev_valid:
             self._set_census_count(self.bank.size)
+        self._last_transport = ((T, sigma, cv, source, step, dt, theta, n_target, n_boundary, n_source, face_T,
+                                 reflect), dict(max_events=max_events, rz_linear_source=rz_linear_source,
+                                                t_emit_floor=t_emit_floor))
         self._mat = ImcMaterial(_ptr(T), _ptr(sigma), _ptr(cv), _ptr(source))
         self._par = self._params(step, dt, theta, n_target, n_boundary, n_source, face_T, reflect, max_events,
                                  rz_linear_source, t_emit_floor)

@@ -16,7 +16,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from ._gray import GrayState, gray_step, init_state
+from ._gray import GrayState, gray_step, init_state, tune  # noqa: F401
 from .engine import Engine
 
 __c = 29.98
