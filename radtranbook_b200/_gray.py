@@ -201,11 +201,14 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
         world = allreduce.get_world_size()
         average_tallies(allreduce, eng)
 
-    # material update: e += dep - emitted/V ; Tr from the path-length intensity
+    # material update: e += dep - emitted/V ; Tr from the path-length intensity.  The comb
+    # does not need T, so it is queued first and a host inv_eos overlaps it on the GPU.
     eng.material_update(state._e, state._Tr)
+    eng.comb_async(Nmax, state.count, state._e)
+    if conserve_comb_energy:
+        state._e.add_(eng.disc[: eng.nc] / eng.vol)
     Tn = evaluate(inv_eos, state.grid(state._e), lambda: _host_copy(state.grid(state._e)), like)
     state._T.copy_(state.flat(Tn))
-    eng.comb_async(Nmax, state.count, state._e)
     try:
         sm = eng.fetch(state.host_copies())
     except _lib.ImcError as ex:
@@ -226,15 +229,12 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
     boundary_loss = float(sum(sm.escaped))
     stats = np.array(sm.stats[:], dtype=np.int64)
     if conserve_comb_energy:
-        state._e.add_(eng.disc[: eng.nc] / eng.vol)
-        Tn = evaluate(inv_eos, state.grid(state._e), lambda: _host_copy(state.grid(state._e)), like)
-        state._T.copy_(state.flat(Tn))
         internal += comb_disc
     if allreduce is not None and world > 1:
         t = torch.tensor([rad, comb_disc, boundary_loss], dtype=torch.float64, device=eng.device)
         allreduce.all_reduce(t)
         rad, comb_disc, boundary_loss = (float(x) / world for x in t.cpu())
-    if conserve_comb_energy or not use_scalar_intensity_Tr:
+    if not use_scalar_intensity_Tr:
         state.refresh_host()
     else:
         state.take_host_copies()

@@ -140,7 +140,7 @@ class Engine:
         self.bank = Bank(capacity, dev, mg)
         self.spare = Bank(capacity, dev, mg)
         self.ws = torch.empty(0, dtype=torch.uint8, device=dev)
-        self.launch = dict(block_size=256, blocks_per_sm=8, chunk=128, smem_cells=0, prefetch=0)
+        self.launch = dict(block_size=256, blocks_per_sm=4, chunk=512, smem_cells=0, prefetch=0)
         self._last_transport = None
 
     # ------------------------------------------------------------------ helpers
