@@ -23,7 +23,7 @@ from .engine import Bank, Engine
 DEFAULT_GRID = {
     "block_size": (128, 256),
     "blocks_per_sm": (4, 8),
-    "chunk": (256, 512, 1024, 2048, 4096),
+    "chunk": (512, 1024, 2048, 4096, 8192),
     "smem_cells": (0, 1),
     "prefetch": (0, 1),
 }

@@ -71,12 +71,21 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
     unsigned need = __ballot_sync(FULL, !has);
     while (need && !drained) {
       if (chunk_next >= chunk_end) {
-        unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(a.queue, (unsigned long long)a.chunk);
+        // guided claim: a share of what is left, at most `chunk`, at least 32, so early
+        // claims are long contiguous (coherent) runs and the drain is finely balanced
+        unsigned long long base = 0, claim = 0;
+        if (lane == 0) {
+          const unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(a.queue);
+          const unsigned long long left = cur < (unsigned long long)n ? (unsigned long long)n - cur : 0ull;
+          const unsigned long long nw = (unsigned long long)gridDim.x * (blockDim.x >> 5);
+          claim = min((unsigned long long)a.chunk, max(32ull, left / (2ull * nw)));
+          base = atomicAdd(a.queue, claim);
+        }
         base = __shfl_sync(FULL, base, 0);
+        claim = __shfl_sync(FULL, claim, 0);
         if (base >= (unsigned long long)n) { drained = true; break; }
         chunk_next = (uint32_t)base;
-        chunk_end = (uint32_t)min(base + (unsigned long long)a.chunk, (unsigned long long)n);
+        chunk_end = (uint32_t)min(base + claim, (unsigned long long)n);
       }
       const uint32_t avail = chunk_end - chunk_next;
       const uint32_t rank = __popc(need & lt_mask);
