@@ -286,6 +286,18 @@ double canon_sum(const double* x, long long n) {
   return part[0];
 }
 inline double pow4(double T) { const double t2 = T * T; return t2 * t2; }
+
+/* Neumaier-compensated accumulator: millions of event tallies per cell sum to FP64 round-off
+ * of the total, so the ledger check measures the algorithm, not the summation order. */
+struct KSum {
+  double s = 0.0, c = 0.0;
+  inline void add(double x) {
+    const double t = s + x;
+    c += (std::fabs(s) >= std::fabs(x)) ? (s - t) + x : (x - t) + s;
+    s = t;
+  }
+  inline double value() const { return s + c; }
+};
 inline double pow3(double T) { return T * T * T; }
 inline bool is1d(const Problem& P) { return P.geom == G_SLAB || P.geom == G_SPHERE; }
 
@@ -441,6 +453,7 @@ typedef struct {
   int rz_linear_source;
   double T_emit_floor;
   int nthreads;
+  int sources_only;       /* 1: Fleck + sources appended, no transport (pins) */
 } orc_step_in;
 
 typedef struct {
@@ -767,8 +780,12 @@ int orc_step_transport(void* h, const orc_step_in* in, orc_step_out* out) {
       volume_source(P, E, in->T, in->Ntarget, in->dt, in->step, oracle::TAG_EMISSION, true,
                     (P.geom == G_RZ) && in->rz_linear_source, B);
     /* matter loses exactly the energy carried by the issued emission particles */
-    for (size_t k = n0; k < B.size(); ++k) out->emitted[B.cell[k]] += B.w[k];
+    std::vector<KSum> em(nc);
+    for (size_t k = n0; k < B.size(); ++k) em[B.cell[k]].add(B.w[k]);
+    for (int c = 0; c < nc; ++c) out->emitted[c] = em[c].value();
   }
+
+  if (in->sources_only) return 0;
 
   /* weight floor, IMC/IMC1D.py:1007, IMC/IMC2D.py:1771 */
   const long long N = (long long)B.size();
@@ -782,9 +799,9 @@ int orc_step_transport(void* h, const orc_step_in* in, orc_step_out* out) {
 #ifndef _OPENMP
   nth = 1;
 #endif
-  std::vector<std::vector<double>> dep_t(nth, std::vector<double>(nc, 0.0)), si_t(nth, std::vector<double>(nc, 0.0));
+  std::vector<std::vector<KSum>> dep_t(nth, std::vector<KSum>(nc)), si_t(nth, std::vector<KSum>(nc));
   std::vector<std::vector<long long>> st_t(nth, std::vector<long long>(S_N, 0));
-  std::vector<std::vector<double>> esc_t(nth, std::vector<double>(4, 0.0));
+  std::vector<std::vector<KSum>> esc_t(nth, std::vector<KSum>(4));
   const double dt = in->dt;
   const bool oned = is1d(P);
 
@@ -794,10 +811,10 @@ int orc_step_transport(void* h, const orc_step_in* in, orc_step_out* out) {
 #ifdef _OPENMP
     tid = omp_get_thread_num();
 #endif
-    double* dep = dep_t[tid].data();
-    double* si = si_t[tid].data();
+    KSum* dep = dep_t[tid].data();
+    KSum* si = si_t[tid].data();
     long long* st = st_t[tid].data();
-    double* esc = esc_t[tid].data();
+    KSum* esc = esc_t[tid].data();
     double w = B.w[k], d1 = B.d1[k], d2 = B.d2[k], p1 = B.p1[k], p2 = B.p2[k];
     int c = B.cell[k];
     if (!(w > 0)) continue;
@@ -824,8 +841,8 @@ int orc_step_transport(void* h, const orc_step_in* in, orc_step_out* out) {
       if (e.evt == EV_BOUNDARY) st[S_BOUNDARY]++;
       else if (e.evt == EV_SCATTER) st[S_SCATTER]++;
       else st[S_CENSUS]++;
-      if (oned) { dep[c] += e.dep; si[c] += e.dep_i / dt; }
-      else { dep[c] += e.dep / P.vol[c]; si[c] += e.dep_i / (dt * P.vol[c]); }
+      if (oned) { dep[c].add(e.dep); si[c].add(e.dep_i / dt); }
+      else { dep[c].add(e.dep / P.vol[c]); si[c].add(e.dep_i / (dt * P.vol[c])); }
       dcen = e.dcen;
       if (!oned) {
         /* IMC/IMC2D.py:1042-1047: at/below the floor the history stops in place,
@@ -848,7 +865,7 @@ int orc_step_transport(void* h, const orc_step_in* in, orc_step_out* out) {
             else { d2 = -d2; j = side == 2 ? 0 : P.ny - 1; }
             st[S_REFLECT]++;
           } else {
-            esc[side] += w; st[S_ESCAPE]++; w = 0; dcen = 0; escaped = true;
+            esc[side].add(w); st[S_ESCAPE]++; w = 0; dcen = 0; escaped = true;
           }
         }
         if (!escaped) c = i + P.nx * j;
@@ -857,8 +874,8 @@ int orc_step_transport(void* h, const orc_step_in* in, orc_step_out* out) {
         /* IMC/IMC1D.py:188-195; the reference deposits only for interior cells and loses
          * the energy in the two edge cells: here every cell gets it (ledger closes). */
         st[S_FLOOR]++;
-        dep[c] += w / P.vol[c];
-        if (sa[c] > 0) si[c] += w / dt / sa[c] / P.vol[c];
+        dep[c].add(w / P.vol[c]);
+        if (sa[c] > 0) si[c].add(w / dt / sa[c] / P.vol[c]);
         w = 0; dcen = 0;
       }
       if (!oned && w <= 1e-300) { w = 0; dcen = 0; }
@@ -870,11 +887,18 @@ int orc_step_transport(void* h, const orc_step_in* in, orc_step_out* out) {
   for (int c = 0; c < nc; ++c) { out->dep[c] = 0; out->si[c] = 0; }
   for (int s = 0; s < S_N; ++s) out->stats[s] = 0;
   for (int s = 0; s < 4; ++s) out->escaped[s] = 0;
-  for (int t = 0; t < nth; ++t) {
-    for (int c = 0; c < nc; ++c) { out->dep[c] += dep_t[t][c]; out->si[c] += si_t[t][c]; }
-    for (int s = 0; s < S_N; ++s) out->stats[s] += st_t[t][s];
-    for (int s = 0; s < 4; ++s) out->escaped[s] += esc_t[t][s];
+  for (int c = 0; c < nc; ++c) {
+    KSum d, q;
+    for (int t = 0; t < nth; ++t) { d.add(dep_t[t][c].value()); q.add(si_t[t][c].value()); }
+    out->dep[c] = d.value(); out->si[c] = q.value();
   }
+  for (int s = 0; s < 4; ++s) {
+    KSum x;
+    for (int t = 0; t < nth; ++t) x.add(esc_t[t][s].value());
+    out->escaped[s] = x.value();
+  }
+  for (int t = 0; t < nth; ++t)
+    for (int s = 0; s < S_N; ++s) out->stats[s] += st_t[t][s];
   return 0;
 }
 
@@ -890,10 +914,15 @@ long long orc_comb(void* h, long long Nmax, uint32_t step, int per_group, double
   Bank& B = o->B;
   const int nc = ncells(P);
   const int nb = per_group ? nc * P.ng : nc;
-  std::vector<double> ecen(nb, 0.0), after(nb, 0.0), ew(nb, 0.0);
+  std::vector<double> ecen(nb, 0.0), ew(nb, 0.0);
+  std::vector<long long> ncopy(nb, 0);
   const long long N = (long long)B.size();
   auto bin = [&](long long k) { return per_group ? B.cell[k] + nc * B.grp[k] : B.cell[k]; };
-  for (long long k = 0; k < N; ++k) if (B.w[k] > 0) ecen[bin(k)] += B.w[k];
+  {
+    std::vector<KSum> acc(nb);
+    for (long long k = 0; k < N; ++k) if (B.w[k] > 0) acc[bin(k)].add(B.w[k]);
+    for (int b = 0; b < nb; ++b) ecen[b] = acc[b].value();
+  }
   double E = 0;
   for (int b = 0; b < nb; ++b) E += ecen[b];
   if (!(E > 0)) {
@@ -917,15 +946,20 @@ long long orc_comb(void* h, long long Nmax, uint32_t step, int per_group, double
     if (!(ew[b] > 0)) continue;
     Draw4 r = draw(P.seed, (uint32_t)k, 0, step, oracle::TAG_COMB);
     const long long n = (long long)std::floor(B.w[k] / ew[b] + r.u[0]);
-    for (long long q = 0; q < n; ++q) {
+    for (long long q = 0; q < n; ++q)
       nbk.push(ew[b], B.d1[k], B.d2[k], 0.0, B.p1[k], B.p2[k], B.cell[k], B.grp[k]);
-      after[b] += ew[b];
-    }
+    if (n > 0) ncopy[b] += n;
   }
   B = nbk;
-  for (int b = 0; b < nb; ++b) disc[b] = ecen[b] - after[b];
+  /* energy after the comb in bin b is exactly ncopy * ew (identical copies) */
+  for (int b = 0; b < nb; ++b) disc[b] = ecen[b] - (double)ncopy[b] * ew[b];
   return (long long)B.size();
 }
+
+/* position samplers, exposed for the pins against the reference's own samplers */
+double orc_slab_linear(double dx, double s, double T, double xi) { return slab_linear(dx, s, T, xi); }
+double orc_sphere_cdf(double r0, double r1, double a, double M, double xi) { return sphere_cdf(r0, r1, a, M, xi); }
+double orc_rz_r_cdf(double r0, double r1, double a, double M, double xi) { return rz_r_cdf(r0, r1, a, M, xi); }
 
 /* comb with caller-supplied uniforms (one per bank entry, pre-comb order, used only by
  * the pin against the reference's own seeded comb) */

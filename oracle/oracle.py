@@ -9,6 +9,7 @@ with the reference's step() semantics for statistical comparisons and CPU baseli
 from __future__ import annotations
 
 import ctypes
+import math
 import os
 from ctypes import POINTER, c_double, c_int, c_int64, c_longlong, c_uint32, c_uint64, c_void_p
 
@@ -29,7 +30,7 @@ class StepIn(ctypes.Structure):
         ("Ntarget", c_longlong), ("Nboundary", c_longlong), ("Nsource", c_longlong),
         ("source", c_void_p), ("face_T", c_void_p * 4), ("reflect", c_int * 4),
         ("max_events", c_longlong), ("rz_linear_source", c_int), ("T_emit_floor", c_double),
-        ("nthreads", c_int),
+        ("nthreads", c_int), ("sources_only", c_int),
     ]
 
 
@@ -65,6 +66,11 @@ def load():
         lib.orc_comb_with_xi.argtypes = [c_void_p, c_longlong, c_void_p, c_void_p]
         lib.orc_event.argtypes = [c_int, c_void_p, c_void_p]
         lib.orc_philox.argtypes = [c_void_p, c_void_p, c_void_p]
+        for f in ("orc_slab_linear", "orc_sphere_cdf", "orc_rz_r_cdf"):
+            getattr(lib, f).restype = c_double
+        lib.orc_slab_linear.argtypes = [c_double] * 4
+        lib.orc_sphere_cdf.argtypes = [c_double] * 5
+        lib.orc_rz_r_cdf.argtypes = [c_double] * 5
         _lib = lib
     return _lib
 
@@ -134,7 +140,7 @@ class Oracle:
         self.lib.orc_set_bank(self.h, len(arrs[0]), *[_p(a) for a in arrs], _p(c), _p(g))
 
     def transport(self, T, sigma, cv, source, step, dt, theta, Ntarget, Nboundary, Nsource, face_T, reflect,
-                  max_events=0, rz_linear_source=True, t_emit_floor=0.0, nthreads=None) -> dict:
+                  max_events=0, rz_linear_source=True, t_emit_floor=0.0, nthreads=None, sources_only=False) -> dict:
         keep = []
 
         def arr(x):
@@ -157,6 +163,7 @@ class Oracle:
         si.rz_linear_source = int(bool(rz_linear_source))
         si.T_emit_floor = float(t_emit_floor)
         si.nthreads = int(nthreads or os.cpu_count() or 1)
+        si.sources_only = int(bool(sources_only))
         out = {k: np.zeros(self.nc) for k in ("dep", "si", "emitted", "sigma_a", "sigma_s")}
         so = StepOut()
         so.dep, so.si, so.emitted, so.sigma_a, so.sigma_s = (_p(out[k]) for k in ("dep", "si", "emitted", "sigma_a", "sigma_s"))
@@ -233,7 +240,7 @@ class OracleGray:
             self.e = self.e + disc / self.o.vol
             self.T = flat2d(inv_eos(self.grid(self.e)))
         b = self.o.get_bank()
-        total = float(np.sum(self.e * self.o.vol) + np.sum(b["weight"]))
+        total = float(np.sum(self.e * self.o.vol) + math.fsum(b["weight"]))
         bl = float(np.sum(r["escaped"]))
         loss = total - self.prev - r["boundary_emission"] + bl - r["source_emission"]
         r["energy_loss"] = loss

@@ -1,0 +1,298 @@
+"""Generate the golden fixtures under tests/golden/ from the reference itself.
+
+Run in a container that has the reference checkout (default /root/reference, override with
+RADTRANBOOK_REF); the fixtures it writes are small .npz files committed with this script.
+
+  events.npz     the reference's own jitted event functions (IMC/IMC1D.py:75 move_particle,
+                 :336 move_particle_spherical, IMC/IMC2D.py:739 _move_particle_xy_jit,
+                 :826 _move_particle_rz_jit) on random inputs, with the uniforms they drew
+                 (Numba's `random` stream is seeded per case and replayed)
+  comb.npz       IMC/IMC1D.py:770 comb and IMC/IMC2D.py:1448 _comb on random banks, with the
+                 Python `random` draws they consumed
+  samplers.npz   IMC/IMC1D.py:203 sample_linear_density, :578 _solve_spherical_cdf,
+                 IMC/IMC2D.py:1293 _solve_r_linear_cdf
+  sources.npz    per-cell counts and weights of IMC/IMC1D.py:251 emitted_particles and
+                 IMC/IMC2D.py:1326 _sample_source_rz_linear (the deterministic part of sampling)
+  stats_*.npz    multi-seed statistics of whole reference steps (IMC1D.step, IMC2D.step):
+                 per-cell mean and standard error of material and radiation temperature
+
+The reference's random numbers cannot be reproduced by a different generator, so whole-step
+parity is statistical; the event, comb and sampler fixtures pin the arithmetic exactly.
+"""
+from __future__ import annotations
+
+import os
+import random
+import sys
+import time
+import types
+
+import numpy as np
+
+REF = os.environ.get("RADTRANBOOK_REF", "/root/reference")
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def load_reference():
+    os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/radtranbook_golden_nbcache")
+    mpl = types.ModuleType("matplotlib")
+    mpl.pyplot = types.ModuleType("matplotlib.pyplot")
+    sys.modules.setdefault("matplotlib", mpl)
+    sys.modules.setdefault("matplotlib.pyplot", mpl.pyplot)
+    sys.path.insert(0, os.path.join(REF, "IMC"))
+    import IMC1D  # noqa: E402
+    import IMC2D  # noqa: E402
+    return IMC1D, IMC2D
+
+
+def nb_helpers():
+    from numba import njit
+
+    @njit
+    def seed_py(s):
+        random.seed(s)
+
+    @njit
+    def seed_np(s):
+        np.random.seed(s)
+
+    @njit
+    def draw_py(k):
+        out = np.empty(k)
+        for i in range(k):
+            out[i] = random.random()
+        return out
+
+    @njit
+    def draw_np(k):
+        return np.random.uniform(0.0, 1.0, k)
+
+    return seed_py, seed_np, draw_py, draw_np
+
+
+def gen_events(IMC1D, IMC2D, n=400, seed=20261203):
+    """Inputs use the oracle's event layout: w d1 d2 p1 p2 lo1 hi1 lo2 hi2 sa ss dcen."""
+    seed_py, _, draw_py, _ = nb_helpers()
+    rng = np.random.default_rng(seed)
+    out = {}
+
+    def sig():
+        k = rng.integers(0, 5)
+        if k == 0:
+            return 0.0
+        return float(10 ** rng.uniform(-3, 7))
+
+    # ---- slab ----
+    rows, draws, res = [], [], []
+    for q in range(n):
+        xl = rng.uniform(0, 1); dx = 10 ** rng.uniform(-3, -1); xr = xl + dx
+        x = xl + dx * rng.choice([0.0, 1.0, rng.uniform()], p=[0.1, 0.1, 0.8])
+        mu = rng.uniform(-1, 1)
+        if x == xl and mu < 0: mu = -mu
+        if x == xr and mu > 0: mu = -mu
+        w = 10 ** rng.uniform(-3, 1); sa = sig(); ss = sig(); dcen = 10 ** rng.uniform(-4, 0)
+        seed_py(1000 + q); r = draw_py(4)
+        seed_py(1000 + q)
+        o = IMC1D.move_particle(w, mu, x, xl, xr, sa, ss, dcen)
+        rows.append([w, mu, 0, x, 0, xl, xr, 0, 1, sa, ss, dcen]); draws.append(r)
+        # (w, mu, x, new_loc, dep_w, dep_i, dcen, evt)
+        res.append([o[0], o[1], 0, o[2], 0, o[4], o[5], o[6], {1: 1, -1: 2, 0: 0}[o[3]], {1: 1, 2: 2, 3: 0}[o[7]]])
+    out["slab_in"], out["slab_r"], out["slab_out"] = np.array(rows), np.array(draws), np.array(res)
+
+    # ---- sphere ----
+    rows, draws, res = [], [], []
+    for q in range(n):
+        r0 = rng.choice([0.0, 10 ** rng.uniform(-2, 0)], p=[0.2, 0.8]); dr = 10 ** rng.uniform(-3, -1); r1 = r0 + dr
+        x = r0 + dr * rng.uniform(0.01, 0.99)
+        mu = rng.uniform(-1, 1)
+        w = 10 ** rng.uniform(-3, 1); sa = sig(); ss = sig(); dcen = 10 ** rng.uniform(-4, 0)
+        seed_py(5000 + q); r = draw_py(4)
+        seed_py(5000 + q)
+        o = IMC1D.move_particle_spherical(w, mu, x, r0, r1, sa, ss, dcen)
+        rows.append([w, mu, 0, x, 0, r0, r1, 0, 1, sa, ss, dcen]); draws.append(r)
+        res.append([o[0], o[1], 0, o[2], 0, o[4], o[5], o[6], {1: 1, -1: 2, 0: 0}[o[3]], {1: 1, 2: 2, 3: 0}[o[7]]])
+    out["sphere_in"], out["sphere_r"], out["sphere_out"] = np.array(rows), np.array(draws), np.array(res)
+
+    # ---- xy and rz ----
+    for geo in ("xy", "rz"):
+        rows, draws, res = [], [], []
+        e1 = np.concatenate([[0.0], np.cumsum(10 ** rng.uniform(-2, -0.5, 12))])
+        e2 = np.concatenate([[0.0], np.cumsum(10 ** rng.uniform(-2, -0.5, 12))])
+        for q in range(n):
+            i = int(rng.integers(0, 12)); j = int(rng.integers(0, 12))
+            a1, b1, a2, b2 = e1[i], e1[i + 1], e2[j], e2[j + 1]
+            p1 = a1 + (b1 - a1) * rng.uniform(0.02, 0.98)
+            p2 = a2 + (b2 - a2) * rng.uniform(0.02, 0.98)
+            if geo == "xy":
+                uz = rng.uniform(-1, 1); ph = rng.uniform(0, 2 * np.pi); rxy = np.sqrt(1 - uz * uz)
+                d1, d2 = rxy * np.cos(ph), rxy * np.sin(ph)
+            else:
+                d1, d2 = rng.uniform(-1, 1), rng.uniform(-1, 1)
+            w = 10 ** rng.uniform(-3, 1); sa = sig(); ss = sig(); dcen = 10 ** rng.uniform(-4, 0)
+            seed_py(9000 + q); r = draw_py(4)
+            seed_py(9000 + q)
+            fn = IMC2D._move_particle_xy_jit if geo == "xy" else IMC2D._move_particle_rz_jit
+            o = fn(w, d1, d2, p1, p2, i, j, e1, e2, sa, ss, dcen)
+            rows.append([w, d1, d2, p1, p2, a1, b1, a2, b2, sa, ss, dcen]); draws.append(r)
+            # (w, d1, d2, p1, p2, crossed, dep_w, dep_i, dcen, evt)
+            res.append([o[0], o[1], o[2], o[3], o[4], o[6], o[7], o[8], o[5], o[9]])
+        out[f"{geo}_in"], out[f"{geo}_r"], out[f"{geo}_out"] = np.array(rows), np.array(draws), np.array(res)
+    return out
+
+
+def gen_comb(IMC1D, IMC2D, seed=7):
+    rng = np.random.default_rng(seed)
+    out = {}
+    n, I = 3000, 40
+    w = rng.gamma(2.0, 1.0, n) * (rng.uniform(size=n) > 0.05)
+    cell = rng.integers(0, I, n)
+    mu = rng.uniform(-1, 1, n); t = rng.uniform(0, 0.01, n); x = rng.uniform(0, 1, n)
+    random.seed(99)
+    xi = np.array([random.random() for _ in range(int(np.sum(w > 0)))])
+    random.seed(99)
+    nw, nc, nmu, nt, nx, disc = IMC1D.comb(w.copy(), cell.copy(), mu.copy(), t.copy(), x.copy(), 2500, I)
+    out.update(c1_w=w, c1_cell=cell, c1_mu=mu, c1_t=t, c1_x=x, c1_xi=xi, c1_nmax=2500,
+               c1_out_w=nw, c1_out_cell=nc, c1_out_mu=nmu, c1_out_x=nx, c1_disc=disc)
+    nx2, ny2 = 6, 5
+    w = rng.gamma(2.0, 1.0, n) * (rng.uniform(size=n) > 0.05)
+    ci = rng.integers(0, nx2, n); cj = rng.integers(0, ny2, n)
+    d1 = rng.uniform(-1, 1, n); d2 = rng.uniform(-1, 1, n); t = np.zeros(n)
+    p1 = rng.uniform(size=n); p2 = rng.uniform(size=n)
+    random.seed(123)
+    xi = np.array([random.random() for _ in range(int(np.sum(w > 0)))])
+    random.seed(123)
+    r = IMC2D._comb(w.copy(), ci.copy(), cj.copy(), d1.copy(), d2.copy(), t.copy(), p1.copy(), p2.copy(), 2000, nx2, ny2)
+    out.update(c2_w=w, c2_ci=ci, c2_cj=cj, c2_d1=d1, c2_d2=d2, c2_p1=p1, c2_p2=p2, c2_xi=xi, c2_nmax=2000,
+               c2_nx=nx2, c2_ny=ny2, c2_out_w=r[0], c2_out_ci=r[1], c2_out_cj=r[2], c2_out_p1=r[6], c2_disc=r[8])
+    return out
+
+
+def gen_samplers(IMC1D, IMC2D, seed=11):
+    _, seed_np, _, draw_np = nb_helpers()
+    rng = np.random.default_rng(seed)
+    out = {}
+    rows, res = [], []
+    for q in range(200):
+        dx = 10 ** rng.uniform(-3, -1); T = 10 ** rng.uniform(-2, 0)
+        s = rng.uniform(-3, 3) * 2 * T / dx ** 2
+        seed_np(700 + q); xi = draw_np(5)
+        seed_np(700 + q); xs = IMC1D.sample_linear_density(dx, s, T, 5)
+        for k in range(5):
+            rows.append([dx, s, T, xi[k]]); res.append(xs[k])
+    out["slab_linear_in"], out["slab_linear_out"] = np.array(rows), np.array(res)
+    rows, res = [], []
+    for q in range(300):
+        r0 = rng.choice([0.0, 10 ** rng.uniform(-2, 0)]); r1 = r0 + 10 ** rng.uniform(-3, 0)
+        a = 10 ** rng.uniform(-4, 0); M = rng.uniform(-1, 1) * a / (r1 - r0); xi = rng.uniform()
+        rows.append([r0, r1, a, M, xi])
+        res.append([IMC1D._solve_spherical_cdf(r0, r1, a, M, xi), IMC2D._solve_r_linear_cdf(r0, r1, a, M, xi)])
+    out["cdf_in"], out["cdf_out"] = np.array(rows), np.array(res)
+    return out
+
+
+def gen_sources(IMC1D, IMC2D, seed=13):
+    rng = np.random.default_rng(seed)
+    out = {}
+    I = 50
+    mesh = np.array([[i * 0.01, (i + 1) * 0.01] for i in range(I)])
+    T = 10 ** rng.uniform(-1.5, 0, I)
+    sa = 10 ** rng.uniform(0, 3, I)
+    p = IMC1D.emitted_particles(20000, T, 0.01, mesh, sa)
+    out.update(e1d_T=T, e1d_sa=sa, e1d_N=20000, e1d_dt=0.01,
+               e1d_counts=np.bincount(p[4], minlength=I), e1d_w=np.array([p[0][p[4] == i][0] for i in range(I)]),
+               e1d_E=p[5])
+    nx, ny = 8, 10
+    r_e = np.linspace(0, 2, nx + 1); z_e = np.linspace(0, 3, ny + 1)
+    T2 = 10 ** rng.uniform(-1.5, 0, (nx, ny))
+    src = 10 ** rng.uniform(-2, 2, (nx, ny))
+    np.random.seed(5); random.seed(5)
+    r = IMC2D._sample_source_rz_linear(30000, src, T2, 0.01, r_e, z_e)
+    flat = r[6] + nx * r[7]
+    counts = np.bincount(flat, minlength=nx * ny)
+    wc = np.zeros(nx * ny)
+    for c in range(nx * ny):
+        if counts[c]:
+            wc[c] = r[0][flat == c][0]
+    out.update(rz_T=T2, rz_src=src, rz_N=30000, rz_dt=0.01, rz_r_edges=r_e, rz_z_edges=z_e,
+               rz_counts=counts, rz_w=wc)
+    return out
+
+
+def run_stats_slab(IMC1D, seeds=32, steps=5):
+    I = 100
+    mesh = np.array([[i * 0.002, (i + 1) * 0.002] for i in range(I)])
+    cv = 0.3
+    kw = dict(Ntarget=2000, Nboundary=2000, Nsource=0, NMax=8000, T_boundary=(1.0, 0.0), dt=0.01, mesh=mesh,
+              sigma_a_func=lambda T: 300.0 * T ** -3, inv_eos=lambda e: e / cv, cv=lambda T: cv + 0 * T,
+              source=np.zeros(I))
+    seed_py, seed_np, _, _ = nb_helpers()
+    Ts, Trs = [], []
+    for s in range(seeds):
+        np.random.seed(s); random.seed(s); seed_py(s); seed_np(s)
+        st = IMC1D.init_simulation(2000, np.full(I, 0.001), np.full(I, 0.001), mesh, lambda T: cv * T,
+                                   lambda e: e / cv)
+        for _ in range(steps):
+            st, info = IMC1D.step(st, kw["Ntarget"], kw["Nboundary"], 0, kw["NMax"], kw["T_boundary"], kw["dt"], mesh,
+                                  kw["sigma_a_func"], kw["inv_eos"], kw["cv"], kw["source"])
+        Ts.append(st.temperature.copy()); Trs.append(st.radiation_temperature.copy())
+    Ts, Trs = np.array(Ts), np.array(Trs)
+    return dict(T_mean=Ts.mean(0), T_se=Ts.std(0, ddof=1) / np.sqrt(seeds), Tr_mean=Trs.mean(0),
+                Tr_se=Trs.std(0, ddof=1) / np.sqrt(seeds), seeds=seeds, steps=steps, Ntarget=2000, Nboundary=2000,
+                NMax=8000, dt=0.01)
+
+
+def run_stats_rz(IMC2D, seeds=16, steps=3):
+    nr, nz = 30, 105
+    r_e = np.linspace(0, 2, nr + 1); z_e = np.linspace(0, 7, nz + 1)
+    rc = 0.5 * (r_e[:-1] + r_e[1:]); zc = 0.5 * (z_e[:-1] + z_e[1:])
+    R, Z = np.meshgrid(rc, zc, indexing="ij")
+    thin = (((R < 0.5) & (Z <= 3.0)) | ((R >= 0.5) & (R < 1.5) & (Z >= 2.5) & (Z <= 3.0))
+            | ((R >= 1.0) & (R <= 1.5) & (Z >= 3.0) & (Z <= 4.0)) | ((R >= 0.5) & (R < 1.5) & (Z >= 4.0) & (Z <= 4.5))
+            | ((R < 0.5) & (Z >= 4.0)))
+    sig = np.where(thin, 0.2, 2000.0); cvg = np.where(thin, 0.001, 0.5)
+    bsf = lambda r, z, side: 0.5 if (side == "zmin" and r < 0.5) else 0.0  # noqa: E731
+    seed_py, seed_np, _, _ = nb_helpers()
+    Ts, Trs = [], []
+    for s in range(seeds):
+        np.random.seed(s); random.seed(s); seed_py(s); seed_np(s)
+        st = IMC2D.init_simulation(6000, np.full((nr, nz), 0.05), np.full((nr, nz), 0.05), r_e, z_e,
+                                   lambda T: cvg * T, lambda e: e / cvg, geometry="rz")
+        for _ in range(steps):
+            st, info = IMC2D.step(st, 6000, 3000, 0, 30000, (0.0, 0.0, 0.0, 0.0), 0.01, r_e, z_e,
+                                  lambda T: sig.copy(), lambda e: e / cvg, lambda T: cvg.copy(), np.zeros((nr, nz)),
+                                  reflect=(True, False, False, False), geometry="rz", boundary_source_func=bsf)
+        Ts.append(st.temperature.copy()); Trs.append(st.radiation_temperature.copy())
+    Ts, Trs = np.array(Ts), np.array(Trs)
+    return dict(T_mean=Ts.mean(0), T_se=Ts.std(0, ddof=1) / np.sqrt(seeds), Tr_mean=Trs.mean(0),
+                Tr_se=Trs.std(0, ddof=1) / np.sqrt(seeds), seeds=seeds, steps=steps, nr=nr, nz=nz)
+
+
+def main():
+    t0 = time.time()
+    IMC1D, IMC2D = load_reference()
+    import contextlib
+    import io
+
+    with contextlib.redirect_stdout(io.StringIO()):
+        ev = gen_events(IMC1D, IMC2D)
+        cb = gen_comb(IMC1D, IMC2D)
+        sp = gen_samplers(IMC1D, IMC2D)
+        so = gen_sources(IMC1D, IMC2D)
+    np.savez_compressed(os.path.join(HERE, "events.npz"), **ev)
+    np.savez_compressed(os.path.join(HERE, "comb.npz"), **cb)
+    np.savez_compressed(os.path.join(HERE, "samplers.npz"), **sp)
+    np.savez_compressed(os.path.join(HERE, "sources.npz"), **so)
+    print(f"pins written ({time.time() - t0:.1f} s)")
+    if "--no-stats" not in sys.argv:
+        with contextlib.redirect_stdout(io.StringIO()):
+            s1 = run_stats_slab(IMC1D)
+        np.savez_compressed(os.path.join(HERE, "stats_slab.npz"), **s1)
+        print(f"slab statistics written ({time.time() - t0:.1f} s)")
+        with contextlib.redirect_stdout(io.StringIO()):
+            s2 = run_stats_rz(IMC2D)
+        np.savez_compressed(os.path.join(HERE, "stats_rz.npz"), **s2)
+        print(f"rz statistics written ({time.time() - t0:.1f} s)")
+
+
+if __name__ == "__main__":
+    main()
