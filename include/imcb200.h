@@ -108,12 +108,14 @@ typedef struct imc_step_params {
                                    (sides 0/1: ny entries, 2/3: nx entries; 1-D: 1) */
   int64_t max_events;           /* events per history cap (2-D reference); <= 0: none */
   int32_t rz_linear_source;     /* RZ emission with the linear r/z tilt */
-  int32_t mg_reference_rules;   /* MG: MG_IMC2D event rules (no scatter cap) */
+  int32_t mg_reference_rules;   /* unused, must be 0: with n_groups > 1 the MG_IMC2D event
+                                   rules (no scatter cap) always apply */
   double t_emit_floor;
   int32_t block_size;           /* tracking launch shape; 0 = tuned default */
   int32_t blocks_per_sm;
-  int32_t chunk;                /* histories claimed per warp ticket */
-  int32_t reserved;
+  int32_t chunk;                /* histories claimed per warp ticket (guided: at most this) */
+  int32_t reserved;             /* bit 0: shared-memory cell table; bit 1: draw prefetch */
+  const double* emission_fractions; /* MG: [g] fixed emission spectrum, or NULL = Planck */
 } imc_step_params;
 
 typedef struct imc_tallies {    /* device outputs, overwritten by each step */
@@ -122,8 +124,10 @@ typedef struct imc_tallies {    /* device outputs, overwritten by each step */
   double* emitted;              /* [c] emission energy issued from matter (GJ) */
   double* sigma_a;              /* [g][c] Fleck absorption (out) */
   double* sigma_s;              /* [g][c] effective scatter (out) */
-  double* escaped;              /* [4 + n_groups] escaped energy by side, then by group */
+  double* escaped;              /* [4] escaped energy by side */
   unsigned long long* stats;    /* [IMC_STAT_N] */
+  double* escaped_group;        /* MG: [n_groups] escaped energy by group (NULL for gray) */
+  double* boundary_group;       /* MG: [n_groups] issued boundary energy by group */
 } imc_tallies;
 
 typedef struct imc_step_report {  /* host-side summary of imc_step_transport */

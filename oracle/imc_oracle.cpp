@@ -59,8 +59,8 @@ struct EventOut {
  * IMC/IMC1D.py:83-88, IMC/IMC2D.py:758-765: a sigma_s*L > 1e4 cell uses sigma = 1e4/L.
  * The capped distance reuses the same uniform (the reference draws a fresh one; the
  * distribution is identical). */
-inline double scatter_distance(double ss, double L, double u, double thresh) {
-  if (ss * L > 10000.0) return -std::log(u) / (10000.0 / L);
+inline double scatter_distance(double ss, double L, double u, double thresh, bool cap = true) {
+  if (cap && ss * L > 10000.0) return -std::log(u) / (10000.0 / L);
   if (ss > thresh) return -std::log(u) / ss;
   return BIG;
 }
@@ -141,14 +141,14 @@ EventOut event_sphere(double w, double mu, double r, double r0, double r1, doubl
 /* ---- 2-D Cartesian event: IMC/IMC2D.py:739-823 ---- */
 EventOut event_xy(double w, double ux, double uy, double x, double y, double xl, double xr,
                   double yl, double yr, double sa, double ss, double dcen, double u0, double u1,
-                  double u2) {
+                  double u2, bool cap = true) {
   EventOut o{};
   double sx = BIG, sy = BIG;
   if (ux > 0) sx = (xr - x) / ux; else if (ux < 0) sx = (xl - x) / ux;
   if (uy > 0) sy = (yr - y) / uy; else if (uy < 0) sy = (yl - y) / uy;
   if (sx < 0) sx = 0;
   if (sy < 0) sy = 0;
-  const double ds = scatter_distance(ss, std::min(xr - xl, yr - yl), u0, 1e-12);
+  const double ds = scatter_distance(ss, std::min(xr - xl, yr - yl), u0, 1e-12, cap);
   const double sb = sx < sy ? sx : sy;
   double s = sb;
   int evt = EV_BOUNDARY;
@@ -192,7 +192,7 @@ inline double rz_inner_l(double r, double mu, double R, double b2) {
 /* ---- 2-D cylindrical r-z event: IMC/IMC2D.py:826-935 ---- */
 EventOut event_rz(double w, double mu, double eta, double r, double z, double rin, double rout,
                   double zlo, double zhi, double sa, double ss, double dcen, double u0, double u1,
-                  double u2) {
+                  double u2, bool cap = true) {
   EventOut o{};
   const double sin2 = 1.0 - eta * eta;
   double s_rin = BIG, s_rout = BIG;
@@ -206,7 +206,7 @@ EventOut event_rz(double w, double mu, double eta, double r, double z, double ri
   double s_zlo = BIG, s_zhi = BIG;
   if (eta > 1e-15) s_zhi = std::max((zhi - z) / eta, 0.0);
   else if (eta < -1e-15) s_zlo = std::max((zlo - z) / eta, 0.0);
-  const double ds = scatter_distance(ss, std::min(rout - rin, zhi - zlo), u0, 1e-12);
+  const double ds = scatter_distance(ss, std::min(rout - rin, zhi - zlo), u0, 1e-12, cap);
   double sb = s_rin;
   if (s_rout < sb) sb = s_rout;
   if (s_zlo < sb) sb = s_zlo;
@@ -991,6 +991,437 @@ long long orc_comb_with_xi(void* h, long long Nmax, const double* xi, double* di
   B = nbk;
   for (int c = 0; c < nc; ++c) disc[c] = ecen[c] - after[c];
   return (long long)B.size();
+}
+
+}  // extern "C"
+
+/* =====================================================================================
+ * Multigroup (MG_IMC/MG_IMC2D.py)
+ * =================================================================================== */
+namespace {
+
+/* Planck fraction F(x) = (15/pi^4) * int_0^x t^3/(e^t - 1) dt: Bernoulli power series for
+ * x < 1, exponential series sum_k e^{-kx}(x^3/k + 3x^2/k^2 + 6x/k^3 + 6/k^4) above (the
+ * standard expansions of the incomplete Planck integral; Widger & Woodall, Bull. Amer.
+ * Meteor. Soc. 57 (1976) 1217).  Stands in for the external planck_integrals module
+ * (MG_IMC/MG_IMC2D.py:62) whose group fractions the step normalises anyway. */
+double planck_F(double x) {
+  const double c = 15.0 / (PI * PI * PI * PI);
+  if (!(x > 0.0)) return 0.0;
+  if (x < 1.0) {
+    /* t^3/(e^t-1) = sum_n B_n t^(n+2)/n!; integrate term by term */
+    static const double B[] = {1.0, -0.5, 1.0 / 6.0, 0.0, -1.0 / 30.0, 0.0, 1.0 / 42.0, 0.0, -1.0 / 30.0, 0.0,
+                               5.0 / 66.0, 0.0, -691.0 / 2730.0, 0.0, 7.0 / 6.0, 0.0, -3617.0 / 510.0, 0.0,
+                               43867.0 / 798.0, 0.0, -174611.0 / 330.0};
+    double sum = 0.0, xp = x * x * x, fact = 1.0;
+    for (int n = 0; n <= 20; ++n) {
+      if (n > 0) fact *= n;
+      if (B[n] != 0.0) sum += B[n] * xp / ((n + 3) * fact);
+      xp *= x;
+    }
+    return c * sum;
+  }
+  double tail = 0.0;
+  const int K = (int)(2.0 + 40.0 / x);
+  for (int k = K; k >= 1; --k) {
+    const double kx = k * x, ik = 1.0 / k;
+    tail += std::exp(-kx) * ik * (x * x * x + ik * (3.0 * x * x + ik * (6.0 * x + ik * 6.0)));
+  }
+  return 1.0 - c * tail;
+}
+
+/* normalised group fractions b*_g of the Planck spectrum at T (sum = 1 unless T <= 0) */
+void planck_fractions(const double* edges, int G, double T, double* b) {
+  double tot = 0.0;
+  for (int g = 0; g < G; ++g) {
+    const double f = (T > 0.0) ? planck_F(edges[g + 1] / T) - planck_F(edges[g] / T) : 0.0;
+    b[g] = f > 0.0 ? f : 0.0;
+    tot += b[g];
+  }
+  for (int g = 0; g < G; ++g) b[g] = tot > 0.0 ? b[g] / tot : 0.0;
+}
+
+/* mixture-of-Gammas CDF over n = 1..200 with weights 1/n^4 (MG_IMC/MG_IMC2D.py:105-107) */
+struct MixCdf {
+  double cdf[200];
+  MixCdf() {
+    double tot = 0.0;
+    for (int n = 1; n <= 200; ++n) { const double d = (double)n; tot += 1.0 / (d * d * d * d); }
+    double run = 0.0;
+    for (int n = 1; n <= 200; ++n) { const double d = (double)n; run += 1.0 / (d * d * d * d); cdf[n - 1] = run / tot; }
+  }
+};
+const MixCdf& mixcdf() { static MixCdf m; return m; }
+
+/* group of a photon sampled from the Planck spectrum at T (MG_IMC/MG_IMC2D.py:202-254):
+ * n from the 1/n^4 mixture, x = (sum of four Exp(1)) / n, energy T*x, group by edges */
+int planck_group(double T, const double* edges, int G, double un, double u1, double u2, double u3, double u4) {
+  if (!(T > 0.0)) return 0;
+  const MixCdf& m = mixcdf();
+  double ns = 200.0;
+  for (int i = 0; i < 200; ++i) if (un <= m.cdf[i]) { ns = (double)(i + 1); break; }
+  const double x = (-std::log(u1) - std::log(u2) - std::log(u3) - std::log(u4)) / ns;
+  const double f = T * x;
+  if (f < edges[0]) return 0;
+  if (f >= edges[G]) return G - 1;
+  for (int g = 0; g < G; ++g) if (f >= edges[g] && f < edges[g + 1]) return g;
+  return G - 1;
+}
+
+/* canonical prefix sum of n values (inclusive): 1024 contiguous segments summed in order,
+ * segment offsets added in order — the order the CUDA path uses */
+void canon_prefix(const double* x, long long n, double* out) {
+  const long long per = (n + 1023) / 1024;
+  std::vector<double> seg(1024, 0.0);
+  for (int t = 0; t < 1024; ++t) {
+    const long long lo = std::min((long long)t * per, n), hi = std::min(lo + per, n);
+    double s = 0.0;
+    for (long long i = lo; i < hi; ++i) s += x[i];
+    seg[t] = s;
+  }
+  double off = 0.0;
+  for (int t = 0; t < 1024; ++t) {
+    const long long lo = std::min((long long)t * per, n), hi = std::min(lo + per, n);
+    double run = off;
+    for (long long i = lo; i < hi; ++i) { run += x[i]; out[i] = run; }
+    off += seg[t];
+  }
+}
+
+/* first index with cdf[i] > x (np.searchsorted side='right'), clamped */
+int search_right(const double* cdf, int n, double x) {
+  int lo = 0, hi = n;
+  while (lo < hi) { const int mid = (lo + hi) >> 1; if (cdf[mid] <= x) lo = mid + 1; else hi = mid; }
+  return std::min(lo, n - 1);
+}
+/* first index with cdf[i] >= x */
+int search_left(const double* cdf, int n, double x) {
+  int lo = 0, hi = n;
+  while (lo < hi) { const int mid = (lo + hi) >> 1; if (cdf[mid] < x) lo = mid + 1; else hi = mid; }
+  return std::min(lo, n - 1);
+}
+
+}  // namespace
+
+extern "C" {
+
+double orc_planck_F(double x) { return planck_F(x); }
+void orc_planck_fractions(const double* edges, int G, double T, double* b) { planck_fractions(edges, G, T, b); }
+int orc_planck_group(double T, const double* edges, int G, const double* u) {
+  return planck_group(T, edges, G, u[0], u[1], u[2], u[3], u[4]);
+}
+
+typedef struct {
+  uint32_t step;
+  double dt, theta;
+  const double* T;          /* [c] */
+  const double* sigma;      /* [g][c] true absorption opacity */
+  const double* cv;         /* [c] */
+  long long Ntarget, Nboundary, Nsource;
+  const double* source;     /* [g][c] power density or NULL */
+  const double* face_T[4];
+  int reflect[4];
+  long long max_events;
+  const double* emission_fractions;  /* [g] or NULL */
+  const double* group_edges;         /* [G+1] */
+  double T_emit_floor;
+  int nthreads;
+  int sources_only;
+} orc_mg_in;
+
+typedef struct {
+  double* dep; double* si;         /* [g][c] */
+  double* emitted;                 /* [c] */
+  double* sigma_a; double* sigma_s;/* [g][c] */
+  double* bnd_by_group;            /* [g] */
+  double* esc_by_group;            /* [g] */
+  double boundary_emission, source_emission, emission_total;
+  double bnd_by_side[4];
+  double escaped[4];
+  long long stats[S_N];
+  long long n_transported;
+  double weight_floor;
+} orc_mg_out;
+
+/* multigroup initial census, MG_IMC/MG_IMC2D.py:992-1097: N particles of equal weight
+ * E/N, cell ~ a Tr^4 V, position uniform in the cell, isotropic, time 0, group from the
+ * Planck spectrum at the local Tr.  Draws: k, blocks 0-2, step 0, TAG_IC. */
+long long orc_init_ic_mg(void* h, long long N, const double* Tr, const double* edges, double T_emit_floor) {
+  Oracle* o = (Oracle*)h;
+  Problem& P = o->P;
+  Bank& B = o->B;
+  B.resize(0);
+  const int nc = ncells(P), G = P.ng;
+  std::vector<double> E(nc), cdf(nc);
+  for (int c = 0; c < nc; ++c) {
+    E[c] = A_RAD * pow4(Tr[c]) * P.vol[c];
+    if (T_emit_floor > 0 && Tr[c] < T_emit_floor) E[c] = 0;
+  }
+  canon_prefix(E.data(), nc, cdf.data());
+  const double Et = cdf[nc - 1];
+  if (N <= 0 || !(Et > 0)) return 0;
+  const double wgt = Et / (double)N;
+  for (long long k = 0; k < N; ++k) {
+    Draw4 a = draw(P.seed, (uint32_t)k, 0, 0, oracle::TAG_IC);
+    Draw4 b = draw(P.seed, (uint32_t)k, 1, 0, oracle::TAG_IC);
+    Draw4 d = draw(P.seed, (uint32_t)k, 2, 0, oracle::TAG_IC);
+    const int c = search_right(cdf.data(), nc, a.u[0] * Et);
+    const int i = c % P.nx, j = c / P.nx;
+    const double e1a = P.e1[i], e1b = P.e1[i + 1], e2a = P.e2[j], e2b = P.e2[j + 1];
+    double p1, p2 = e2a + a.u[2] * (e2b - e2a), d1, d2;
+    if (P.geom == G_RZ) p1 = std::sqrt(e1a * e1a + a.u[1] * (e1b * e1b - e1a * e1a));
+    else p1 = e1a + a.u[1] * (e1b - e1a);
+    iso_dir(P.geom, a.u[3], b.u[0], d1, d2);
+    const int g = planck_group(Tr[c], edges, G, b.u[1], b.u[2], b.u[3], d.u[0], d.u[1]);
+    B.push(wgt, d1, d2, 0.0, p1, p2, c, g);
+  }
+  return (long long)B.size();
+}
+
+int orc_step_transport_mg(void* h, const orc_mg_in* in, orc_mg_out* out) {
+  Oracle* o = (Oracle*)h;
+  Problem& P = o->P;
+  Bank& B = o->B;
+  const int nc = ncells(P), G = P.ng;
+  const double* edges = in->group_edges;
+  /* Fleck factor with the Planck-mean opacity, MG_IMC/MG_IMC2D.py:1703-1719 */
+  std::vector<double> bstar((size_t)G * nc), sa((size_t)G * nc), ss((size_t)G * nc), b(G);
+  for (int c = 0; c < nc; ++c) {
+    planck_fractions(edges, G, in->T[c], b.data());
+    double sp = 0.0;
+    for (int g = 0; g < G; ++g) { bstar[(size_t)g * nc + c] = b[g]; sp += in->sigma[(size_t)g * nc + c] * b[g]; }
+    const double T = in->T[c];
+    const double beta = 4.0 * A_RAD * pow3(T) / in->cv[c];
+    double f = 1.0 / (1.0 + in->theta * beta * sp * C_LIGHT * in->dt);
+    f = std::min(1.0, std::max(0.0, f));
+    for (int g = 0; g < G; ++g) {
+      const size_t q = (size_t)g * nc + c;
+      ss[q] = in->sigma[q] * (1.0 - f);
+      sa[q] = in->sigma[q] * f;
+    }
+  }
+  std::copy(sa.begin(), sa.end(), out->sigma_a);
+  std::copy(ss.begin(), ss.end(), out->sigma_s);
+  for (int g = 0; g < G; ++g) { out->bnd_by_group[g] = 0; out->esc_by_group[g] = 0; }
+  for (int q = 0; q < 4; ++q) { out->bnd_by_side[q] = 0; out->escaped[q] = 0; }
+
+  /* ---- boundary: the gray face sampling plus a Planck group at the face cell's T ---- */
+  double bnd_total = 0.0;
+  for (int side = 0; side < 4; ++side) {
+    const double* Tf = in->face_T[side];
+    if (!Tf || in->Nboundary <= 0) continue;
+    const bool along2 = side < 2;
+    const int nf = along2 ? P.ny : P.nx;
+    std::vector<double> Ef(nf), cdf(nf);
+    double Et = 0;
+    for (int q = 0; q < nf; ++q) {
+      double area;
+      if (P.geom == G_XY) area = along2 ? (P.e2[q + 1] - P.e2[q]) : (P.e1[q + 1] - P.e1[q]);
+      else if (along2) { const double R = side == 0 ? P.e1[0] : P.e1[P.nx]; area = 2.0 * PI * R * (P.e2[q + 1] - P.e2[q]); }
+      else area = PI * (P.e1[q + 1] * P.e1[q + 1] - P.e1[q] * P.e1[q]);
+      const double T = Tf[q];
+      Ef[q] = (T > 0) ? A_RAD * C_LIGHT * T * T * T * T / 4.0 * area * in->dt : 0.0;
+      Et += Ef[q];
+      cdf[q] = Et;
+    }
+    if (!(Et > 0)) continue;
+    const long long n = in->Nboundary;
+    const double wgt = Et / (double)n;
+    for (long long k = 0; k < n; ++k) {
+      Draw4 a = draw(P.seed, (uint32_t)k, 0, in->step, oracle::TAG_BOUNDARY | side);
+      Draw4 bb = draw(P.seed, (uint32_t)k, 1, in->step, oracle::TAG_BOUNDARY | side);
+      Draw4 d = draw(P.seed, (uint32_t)k, 2, in->step, oracle::TAG_BOUNDARY | side);
+      int q = (int)(std::lower_bound(cdf.begin(), cdf.end(), a.u[0] * Et) - cdf.begin());
+      q = std::min(q, nf - 1);
+      while (Ef[q] <= 0 && q > 0) --q;
+      const double mu_n = std::sqrt(a.u[2]);
+      const double t = bb.u[0] * in->dt;
+      double p1, p2, d1, d2;
+      int i, j;
+      if (P.geom == G_XY) {
+        const double mu_t = std::sqrt(std::max(0.0, 1.0 - mu_n * mu_n));
+        const double ct = mu_t * std::cos(2.0 * PI * a.u[3]);
+        if (along2) {
+          j = q; i = side == 0 ? 0 : P.nx - 1;
+          p1 = side == 0 ? P.e1[0] : P.e1[P.nx];
+          p2 = P.e2[q] + a.u[1] * (P.e2[q + 1] - P.e2[q]);
+          d1 = side == 0 ? mu_n : -mu_n; d2 = ct;
+        } else {
+          i = q; j = side == 2 ? 0 : P.ny - 1;
+          p2 = side == 2 ? P.e2[0] : P.e2[P.ny];
+          p1 = P.e1[q] + a.u[1] * (P.e1[q + 1] - P.e1[q]);
+          d2 = side == 2 ? mu_n : -mu_n; d1 = ct;
+        }
+      } else {
+        if (along2) {
+          j = q; i = side == 0 ? 0 : P.nx - 1;
+          p1 = side == 0 ? P.e1[0] : P.e1[P.nx];
+          p2 = P.e2[q] + a.u[1] * (P.e2[q + 1] - P.e2[q]);
+          d1 = side == 0 ? mu_n : -mu_n; d2 = 2.0 * a.u[3] - 1.0;
+        } else {
+          i = q; j = side == 2 ? 0 : P.ny - 1;
+          const double r0 = P.e1[q], r1 = P.e1[q + 1];
+          p1 = std::sqrt(r0 * r0 + a.u[1] * (r1 * r1 - r0 * r0));
+          p2 = side == 2 ? P.e2[0] : P.e2[P.ny];
+          d2 = side == 2 ? mu_n : -mu_n; d1 = std::cos(2.0 * PI * a.u[3]);
+        }
+      }
+      const int g = planck_group(Tf[q], edges, G, bb.u[1], bb.u[2], bb.u[3], d.u[0], d.u[1]);
+      B.push(wgt, d1, d2, t, p1, p2, i + P.nx * j, g);
+      out->bnd_by_group[g] += wgt;
+      out->bnd_by_side[side] += wgt;
+      bnd_total += wgt;
+    }
+  }
+  out->boundary_emission = bnd_total;
+
+  /* ---- categorical volume sources: cell ~ sum_g E_gc, group ~ E_gc, equal weights ----
+   * (fixed source MG_IMC/MG_IMC2D.py:1098-1170; emission :1866-1943) */
+  auto categorical = [&](const std::vector<double>& Egc, long long N, uint32_t tag) -> double {
+    std::vector<double> Ec(nc, 0.0), cdf(nc);
+    for (int c = 0; c < nc; ++c) { double s2 = 0.0; for (int g = 0; g < G; ++g) s2 += Egc[(size_t)g * nc + c]; Ec[c] = s2; }
+    canon_prefix(Ec.data(), nc, cdf.data());
+    const double Et = cdf[nc - 1];
+    if (!(Et > 0) || N <= 0) return 0.0;
+    const double wgt = Et / (double)N;
+    std::vector<double> gc(G);
+    for (long long k = 0; k < N; ++k) {
+      Draw4 a = draw(P.seed, (uint32_t)k, 0, in->step, tag);
+      Draw4 bb = draw(P.seed, (uint32_t)k, 1, in->step, tag);
+      const int c = search_right(cdf.data(), nc, a.u[0] * Et);
+      double run = 0.0;
+      for (int g = 0; g < G; ++g) { run += Egc[(size_t)g * nc + c]; gc[g] = run; }
+      const int g = search_left(gc.data(), G, a.u[1] * run);
+      const int i = c % P.nx, j = c / P.nx;
+      const double e1a = P.e1[i], e1b = P.e1[i + 1], e2a = P.e2[j], e2b = P.e2[j + 1];
+      double p1 = P.geom == G_RZ ? std::sqrt(e1a * e1a + a.u[2] * (e1b * e1b - e1a * e1a)) : e1a + a.u[2] * (e1b - e1a);
+      const double p2 = e2a + a.u[3] * (e2b - e2a);
+      double d1, d2;
+      iso_dir(P.geom, bb.u[0], bb.u[1], d1, d2);
+      B.push(wgt, d1, d2, bb.u[2] * in->dt, p1, p2, c, g);
+    }
+    return wgt * (double)N;
+  };
+  out->source_emission = 0.0;
+  if (in->source && in->Nsource > 0) {
+    std::vector<double> Sgc((size_t)G * nc);
+    for (int g = 0; g < G; ++g)
+      for (int c = 0; c < nc; ++c) Sgc[(size_t)g * nc + c] = in->source[(size_t)g * nc + c] * P.vol[c] * in->dt;
+    out->source_emission = categorical(Sgc, in->Nsource, oracle::TAG_SOURCE);
+  }
+  std::vector<double> Egc((size_t)G * nc, 0.0);
+  for (int c = 0; c < nc; ++c) {
+    const double T = in->T[c];
+    if (in->T_emit_floor > 0 && T < in->T_emit_floor) continue;
+    const double aT4 = A_RAD * C_LIGHT * pow4(T) * in->dt * P.vol[c];
+    for (int g = 0; g < G; ++g) {
+      const size_t q = (size_t)g * nc + c;
+      const double bg = in->emission_fractions ? in->emission_fractions[g] : bstar[q];
+      Egc[q] = sa[q] * bg * aT4;
+    }
+  }
+  double Eemit = 0.0;
+  for (int c = 0; c < nc; ++c) { out->emitted[c] = 0.0; for (int g = 0; g < G; ++g) out->emitted[c] += Egc[(size_t)g * nc + c]; Eemit += out->emitted[c]; }
+  out->emission_total = 0.0;
+  if (in->Ntarget > 0) {
+    const double issued = categorical(Egc, in->Ntarget, oracle::TAG_EMISSION);
+    /* matter loses E_c scaled so the total is exactly the issued particle energy */
+    const double scale = Eemit > 0 ? issued / Eemit : 0.0;
+    for (int c = 0; c < nc; ++c) out->emitted[c] *= scale;
+    out->emission_total = issued;
+  } else {
+    for (int c = 0; c < nc; ++c) out->emitted[c] = 0.0;
+  }
+  if (in->sources_only) return 0;
+
+  /* ---- transport, MG_IMC/MG_IMC2D.py:774-989 ---- */
+  const long long N = (long long)B.size();
+  double wsum = 0;
+  for (long long k = 0; k < N; ++k) wsum += B.w[k];
+  const double floor_w = 1e-10 * wsum / (double)std::max(N, 1LL);
+  out->weight_floor = floor_w;
+  out->n_transported = N;
+  int nth = in->nthreads > 0 ? in->nthreads : 1;
+#ifndef _OPENMP
+  nth = 1;
+#endif
+  const size_t ncg = (size_t)nc * G;
+  std::vector<std::vector<KSum>> dep_t(nth, std::vector<KSum>(ncg)), si_t(nth, std::vector<KSum>(ncg));
+  std::vector<std::vector<long long>> st_t(nth, std::vector<long long>(S_N, 0));
+  std::vector<std::vector<KSum>> esc_t(nth, std::vector<KSum>(4 + G));
+  const double dt = in->dt;
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nth)
+  for (long long k = 0; k < N; ++k) {
+    int tid = 0;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+#endif
+    KSum* dep = dep_t[tid].data();
+    KSum* si = si_t[tid].data();
+    long long* st = st_t[tid].data();
+    KSum* esc = esc_t[tid].data();
+    double w = B.w[k], d1 = B.d1[k], d2 = B.d2[k], p1 = B.p1[k], p2 = B.p2[k];
+    int c = B.cell[k];
+    const int g = B.grp[k];
+    if (!(w > floor_w)) continue;  /* reference: skipped without an event */
+    double dcen = (dt - B.t[k]) * C_LIGHT;
+    uint32_t ev = 0;
+    while (dcen > 0) {
+      if (in->max_events > 0 && (long long)ev >= in->max_events) { st[S_CAP]++; break; }
+      int i = c % P.nx, j = c / P.nx;
+      const size_t q = (size_t)g * nc + c;
+      Draw4 r = draw(P.seed, (uint32_t)k, ev, in->step, oracle::TAG_TRANSPORT);
+      ++ev;
+      st[S_EVENTS]++;
+      /* MG events: no effective-scatter cap (MG_IMC/MG_IMC2D.py:601-604) */
+      EventOut e;
+      if (P.geom == G_XY) e = event_xy(w, d1, d2, p1, p2, P.e1[i], P.e1[i + 1], P.e2[j], P.e2[j + 1], sa[q], ss[q], dcen, r.u[0], r.u[1], r.u[2], false);
+      else e = event_rz(w, d1, d2, p1, p2, P.e1[i], P.e1[i + 1], P.e2[j], P.e2[j + 1], sa[q], ss[q], dcen, r.u[0], r.u[1], r.u[2], false);
+      if (e.evt == EV_BOUNDARY) st[S_BOUNDARY]++; else if (e.evt == EV_SCATTER) st[S_SCATTER]++; else st[S_CENSUS]++;
+      if (sa[q] > 1e-12) {
+        dep[q].add(e.dep / P.vol[c]);
+        si[q].add(e.dep_i / (dt * P.vol[c]));
+      } else {
+        si[q].add(w * (dcen - e.dcen) / (dt * P.vol[c]));
+        e.w = w;  /* no absorption below the threshold */
+      }
+      w = e.w; d1 = e.d1; d2 = e.d2; p1 = e.p1; p2 = e.p2; dcen = e.dcen;
+      if (e.cross != X_NONE) {
+        if (e.cross == X_IP) ++i; else if (e.cross == X_IM) --i; else if (e.cross == X_JP) ++j; else --j;
+        int side = -1;
+        if (i < 0) side = 0; else if (i >= P.nx) side = 1; else if (j < 0) side = 2; else if (j >= P.ny) side = 3;
+        if (side >= 0) {
+          if (in->reflect[side]) {
+            /* the reference does not reset the index after a -dir1 reflection
+             * (MG_IMC/MG_IMC2D.py:916-919): here the particle stays in cell 0 */
+            if (side < 2) { d1 = -d1; i = side == 0 ? 0 : P.nx - 1; }
+            else { d2 = -d2; j = side == 2 ? 0 : P.ny - 1; }
+            st[S_REFLECT]++;
+          } else {
+            esc[side].add(w); esc[4 + g].add(w); st[S_ESCAPE]++;
+            w = 0; dcen = 0;
+          }
+        }
+        if (w > 0) c = i + P.nx * j;
+      }
+      /* MG_IMC/MG_IMC2D.py:858-860: the next event's floor test stops the history; an
+       * escape set dcen = 0 and a weight that underflowed to 0 is at the floor too */
+      if (dcen > 0 && w <= floor_w) { st[S_FLOOR]++; break; }
+    }
+    B.w[k] = w; B.d1[k] = d1; B.d2[k] = d2; B.p1[k] = p1; B.p2[k] = p2; B.cell[k] = c;
+  }
+  for (size_t q = 0; q < ncg; ++q) {
+    KSum d, s2;
+    for (int t = 0; t < nth; ++t) { d.add(dep_t[t][q].value()); s2.add(si_t[t][q].value()); }
+    out->dep[q] = d.value(); out->si[q] = s2.value();
+  }
+  for (int s2 = 0; s2 < S_N; ++s2) { out->stats[s2] = 0; for (int t = 0; t < nth; ++t) out->stats[s2] += st_t[t][s2]; }
+  for (int q = 0; q < 4 + G; ++q) {
+    KSum x;
+    for (int t = 0; t < nth; ++t) x.add(esc_t[t][q].value());
+    if (q < 4) out->escaped[q] = x.value(); else out->esc_by_group[q - 4] = x.value();
+  }
+  return 0;
 }
 
 }  // extern "C"

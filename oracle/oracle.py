@@ -42,6 +42,27 @@ class StepOut(ctypes.Structure):
     ]
 
 
+class MgIn(ctypes.Structure):
+    _fields_ = [
+        ("step", c_uint32), ("dt", c_double), ("theta", c_double),
+        ("T", c_void_p), ("sigma", c_void_p), ("cv", c_void_p),
+        ("Ntarget", c_longlong), ("Nboundary", c_longlong), ("Nsource", c_longlong),
+        ("source", c_void_p), ("face_T", c_void_p * 4), ("reflect", c_int * 4),
+        ("max_events", c_longlong), ("emission_fractions", c_void_p), ("group_edges", c_void_p),
+        ("T_emit_floor", c_double), ("nthreads", c_int), ("sources_only", c_int),
+    ]
+
+
+class MgOut(ctypes.Structure):
+    _fields_ = [
+        ("dep", c_void_p), ("si", c_void_p), ("emitted", c_void_p), ("sigma_a", c_void_p), ("sigma_s", c_void_p),
+        ("bnd_by_group", c_void_p), ("esc_by_group", c_void_p),
+        ("boundary_emission", c_double), ("source_emission", c_double), ("emission_total", c_double),
+        ("bnd_by_side", c_double * 4), ("escaped", c_double * 4), ("stats", c_longlong * S_N),
+        ("n_transported", c_longlong), ("weight_floor", c_double),
+    ]
+
+
 _lib = None
 
 
@@ -65,6 +86,15 @@ def load():
         lib.orc_comb_with_xi.restype = c_longlong
         lib.orc_comb_with_xi.argtypes = [c_void_p, c_longlong, c_void_p, c_void_p]
         lib.orc_event.argtypes = [c_int, c_void_p, c_void_p]
+        lib.orc_init_ic_mg.restype = c_longlong
+        lib.orc_init_ic_mg.argtypes = [c_void_p, c_longlong, c_void_p, c_void_p, c_double]
+        lib.orc_step_transport_mg.restype = c_int
+        lib.orc_step_transport_mg.argtypes = [c_void_p, POINTER(MgIn), POINTER(MgOut)]
+        lib.orc_planck_F.restype = c_double
+        lib.orc_planck_F.argtypes = [c_double]
+        lib.orc_planck_fractions.argtypes = [c_void_p, c_int, c_double, c_void_p]
+        lib.orc_planck_group.restype = c_int
+        lib.orc_planck_group.argtypes = [c_double, c_void_p, c_int, c_void_p]
         lib.orc_philox.argtypes = [c_void_p, c_void_p, c_void_p]
         for f in ("orc_slab_linear", "orc_sphere_cdf", "orc_rz_r_cdf"):
             getattr(lib, f).restype = c_double
@@ -106,6 +136,7 @@ class Oracle:
         self.nx, self.ny = len(self.e1) - 1, len(self.e2) - 1
         self.nc = self.nx * self.ny
         self.vol = np.ascontiguousarray(volumes_flat, dtype=np.float64).reshape(-1)
+        self.ng = int(n_groups)
         self.h = self.lib.orc_create(GEOM[geometry], self.nx, self.ny, n_groups, _p(self.e1), _p(self.e2),
                                      _p(self.vol), int(seed) & 0xFFFFFFFFFFFFFFFF)
 
@@ -178,8 +209,63 @@ class Oracle:
         out["weight_floor"] = so.weight_floor
         return out
 
+    # ---------------- multigroup ----------------
+    def init_ic_mg(self, tr_flat, N, group_edges, t_emit_floor=0.0) -> int:
+        tr = np.ascontiguousarray(tr_flat, dtype=np.float64)
+        ge = np.ascontiguousarray(group_edges, dtype=np.float64)
+        return int(self.lib.orc_init_ic_mg(self.h, int(N), _p(tr), _p(ge), float(t_emit_floor)))
+
+    def transport_mg(self, T, sigma_gc, cv, source_gc, step, dt, theta, Ntarget, Nboundary, Nsource, face_T,
+                     reflect, group_edges, max_events=0, emission_fractions=None, t_emit_floor=0.0, nthreads=None,
+                     sources_only=False) -> dict:
+        keep = []
+
+        def arr(x):
+            if x is None:
+                return None
+            a = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+            keep.append(a)
+            return _p(a)
+
+        G = len(group_edges) - 1
+        mi = MgIn()
+        mi.step = int(step) & 0xFFFFFFFF
+        mi.dt, mi.theta = float(dt), float(theta)
+        mi.T, mi.sigma, mi.cv = arr(T), arr(sigma_gc), arr(cv)
+        mi.Ntarget, mi.Nboundary, mi.Nsource = int(Ntarget), int(Nboundary), int(Nsource)
+        mi.source = arr(source_gc)
+        for q in range(4):
+            mi.face_T[q] = arr(face_T[q]) if q < len(face_T) else None
+            mi.reflect[q] = int(bool(reflect[q])) if q < len(reflect) else 0
+        mi.max_events = int(max_events)
+        mi.emission_fractions = arr(emission_fractions)
+        mi.group_edges = arr(group_edges)
+        mi.T_emit_floor = float(t_emit_floor)
+        mi.nthreads = int(nthreads or os.cpu_count() or 1)
+        mi.sources_only = int(bool(sources_only))
+        ncg = self.nc * G
+        out = {k: np.zeros(ncg) for k in ("dep", "si", "sigma_a", "sigma_s")}
+        out["emitted"] = np.zeros(self.nc)
+        out["bnd_by_group"] = np.zeros(G)
+        out["esc_by_group"] = np.zeros(G)
+        mo = MgOut()
+        for k in ("dep", "si", "emitted", "sigma_a", "sigma_s", "bnd_by_group", "esc_by_group"):
+            setattr(mo, k, _p(out[k]))
+        st = self.lib.orc_step_transport_mg(self.h, ctypes.byref(mi), ctypes.byref(mo))
+        if st != 0:
+            raise AssertionError("invalid multigroup material state")
+        out["boundary_emission"] = mo.boundary_emission
+        out["source_emission"] = mo.source_emission
+        out["emission_total"] = mo.emission_total
+        out["bnd_by_side"] = np.array(mo.bnd_by_side[:])
+        out["escaped"] = np.array(mo.escaped[:])
+        out["stats"] = np.array(mo.stats[:], dtype=np.int64)
+        out["n_transported"] = mo.n_transported
+        out["weight_floor"] = mo.weight_floor
+        return out
+
     def comb(self, Nmax, step, per_group=False) -> np.ndarray:
-        disc = np.zeros(self.nc)
+        disc = np.zeros(self.nc * (self.ng if per_group else 1))
         self.lib.orc_comb(self.h, int(Nmax), int(step) & 0xFFFFFFFF, int(per_group), _p(disc))
         return disc
 

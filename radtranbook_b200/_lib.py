@@ -60,6 +60,7 @@ class ImcStepParams(ctypes.Structure):
         ("rz_linear_source", c_int32), ("mg_reference_rules", c_int32),
         ("t_emit_floor", c_double),
         ("block_size", c_int32), ("blocks_per_sm", c_int32), ("chunk", c_int32), ("reserved", c_int32),
+        ("emission_fractions", c_void_p),
     ]
 
 
@@ -67,6 +68,7 @@ class ImcTallies(ctypes.Structure):
     _fields_ = [
         ("dep", c_void_p), ("si", c_void_p), ("emitted", c_void_p), ("sigma_a", c_void_p),
         ("sigma_s", c_void_p), ("escaped", c_void_p), ("stats", c_void_p),
+        ("escaped_group", c_void_p), ("boundary_group", c_void_p),
     ]
 
 

@@ -339,3 +339,214 @@ cudaError_t imc_launch_canon_sum_eV(const double* e, const double* vol, int nc, 
   k_canon_eV<<<1, NT, 0, s>>>(e, vol, nc, out);
   return cudaGetLastError();
 }
+
+// =====================================================================================
+// Multigroup planning (MG_IMC/MG_IMC2D.py:1703-1943): Planck group fractions, Fleck factor
+// with the Planck-mean opacity, categorical emission / fixed-source tables.
+// =====================================================================================
+namespace {
+
+// Planck fraction F(x) = (15/pi^4) int_0^x t^3/(e^t-1) dt: Bernoulli series below x = 1,
+// exponential series above (Widger & Woodall 1976).  Same expansion as the oracle.
+__device__ double planck_F(double x) {
+  const double c = 15.0 / (PI * PI * PI * PI);
+  if (!(x > 0.0)) return 0.0;
+  if (x < 1.0) {
+    const double B[21] = {1.0, -0.5, 1.0 / 6.0, 0.0, -1.0 / 30.0, 0.0, 1.0 / 42.0, 0.0, -1.0 / 30.0, 0.0,
+                          5.0 / 66.0, 0.0, -691.0 / 2730.0, 0.0, 7.0 / 6.0, 0.0, -3617.0 / 510.0, 0.0,
+                          43867.0 / 798.0, 0.0, -174611.0 / 330.0};
+    double sum = 0.0, xp = x * x * x, fact = 1.0;
+    for (int n = 0; n <= 20; ++n) {
+      if (n > 0) fact *= n;
+      if (B[n] != 0.0) sum += B[n] * xp / ((n + 3) * fact);
+      xp *= x;
+    }
+    return c * sum;
+  }
+  double tail = 0.0;
+  const int K = (int)(2.0 + 40.0 / x);
+  for (int k = K; k >= 1; --k) {
+    const double kx = k * x, ik = 1.0 / k;
+    tail += exp(-kx) * ik * (x * x * x + ik * (3.0 * x * x + ik * (6.0 * x + ik * 6.0)));
+  }
+  return 1.0 - c * tail;
+}
+
+// canonical inclusive prefix sum of n values (the oracle's canon_prefix order)
+__device__ void block_canon_prefix(const double* x, int n, double* out, double* sh) {
+  const int t = threadIdx.x;
+  const int per = (n + NT - 1) / NT;
+  const int lo = min(t * per, n), hi = min(lo + per, n);
+  double s = 0.0;
+  for (int i = lo; i < hi; ++i) s += x[i];
+  sh[t] = s;
+  __syncthreads();
+  if (t == 0) {
+    double off = 0.0;
+    for (int q = 0; q < NT; ++q) { const double v = sh[q]; sh[q] = off; off += v; }
+  }
+  __syncthreads();
+  double run = sh[t];
+  for (int i = lo; i < hi; ++i) { run += x[i]; out[i] = run; }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(NT) k_plan_mg(PlanMgArgs a) {
+  __shared__ double sh[NT];
+  const int t = threadIdx.x;
+  const int nc = a.nc, G = a.ng;
+  for (int q = t; q <= a.nx; q += NT) a.e1f[q] = (float)a.e1[q];
+  for (int q = t; q <= a.ny; q += NT) a.e2f[q] = (float)a.e2[q];
+  if (t == 0) {
+    // mixture-of-Gammas CDF over n = 1..200 with weights 1/n^4 (MG_IMC/MG_IMC2D.py:105-107)
+    double tot = 0.0;
+    for (int n = 1; n <= 200; ++n) { const double d = (double)n; tot += 1.0 / (d * d * d * d); }
+    double run = 0.0;
+    for (int n = 1; n <= 200; ++n) { const double d = (double)n; run += 1.0 / (d * d * d * d); a.mixcdf[n - 1] = run / tot; }
+  }
+  // ---- per cell: Planck fractions, Planck-mean opacity, Fleck, emission by group ----
+  for (int c = t; c < nc; c += NT) {
+    const double T = a.T[c];
+    if (!isfinite(T) || !(a.cv[c] > 0.0)) atomicOr(&a.sum->flags, (int)IMC_FLAG_NONFINITE);
+    double* gc = a.Egc + (size_t)c * G;  // scratch: fractions, then cumulative emission
+    double tot = 0.0;
+    for (int g = 0; g < G; ++g) {
+      const double f = (T > 0.0) ? planck_F(a.gedges[g + 1] / T) - planck_F(a.gedges[g] / T) : 0.0;
+      gc[g] = f > 0.0 ? f : 0.0;
+      tot += gc[g];
+    }
+    double sp = 0.0;
+    for (int g = 0; g < G; ++g) {
+      gc[g] = tot > 0.0 ? gc[g] / tot : 0.0;
+      sp += a.sigma[(size_t)g * nc + c] * gc[g];
+    }
+    const double beta = 4.0 * A_RAD * pow3(T) / a.cv[c];
+    double f = 1.0 / (1.0 + a.theta * beta * sp * C_LIGHT * a.dt);
+    f = fmin(1.0, fmax(0.0, f));
+    const double aT4 = (a.t_emit_floor > 0.0 && T < a.t_emit_floor) ? 0.0
+                                                                      : A_RAD * C_LIGHT * pow4(T) * a.dt * a.vol[c];
+    double run = 0.0;
+    for (int g = 0; g < G; ++g) {
+      const size_t q = (size_t)g * nc + c;
+      const double ss = a.sigma[q] * (1.0 - f);
+      const double sa = a.sigma[q] * f;
+      a.sa[q] = sa; a.ss[q] = ss;
+      a.sass[q] = make_float2((float)sa, (float)ss);
+      a.cellf[q] = make_double2(1.0 / a.vol[c], sa > 1e-12 ? 1.0 / (sa * a.vol[c] * a.dt) : -1.0 / (a.vol[c] * a.dt));
+      const double bg = a.emission_fractions ? a.emission_fractions[g] : gc[g];
+      run += sa * bg * aT4;
+      gc[g] = run;  // cumulative over groups
+    }
+    a.Ec[c] = run;
+  }
+  __syncthreads();
+  block_canon_prefix(a.Ec, nc, a.cdf, sh);
+  const double Eemit = a.cdf[nc - 1];
+  long long n_emit = 0;
+  double issued = 0.0;
+  if (a.n_target > 0 && Eemit > 0.0) {
+    n_emit = a.n_target;
+    const float w32 = (float)(Eemit / (double)n_emit);
+    issued = (double)n_emit * (double)w32;
+  }
+  const double scale = Eemit > 0.0 ? issued / Eemit : 0.0;
+  for (int c = t; c < nc; c += NT) a.emitted[c] = a.Ec[c] * scale;
+
+  // ---- fixed source [g][c] (MG_IMC/MG_IMC2D.py:1098-1170) ----
+  long long n_src = 0;
+  double e_src = 0.0;
+  if (a.source && a.n_source > 0) {
+    for (int c = t; c < nc; c += NT) {
+      double run = 0.0;
+      for (int g = 0; g < G; ++g) {
+        run += a.source[(size_t)g * nc + c] * a.vol[c] * a.dt;
+        a.Sgc[(size_t)c * G + g] = run;
+      }
+      a.Sc[c] = run;
+    }
+    __syncthreads();
+    block_canon_prefix(a.Sc, nc, a.Scdf, sh);
+    const double St = a.Scdf[nc - 1];
+    if (St > 0.0) {
+      n_src = a.n_source;
+      e_src = (double)n_src * (double)(float)(St / (double)n_src);
+    }
+  }
+
+  // ---- boundary faces (as gray) ----
+  if (t < 4) {
+    const int side = t;
+    a.sum->n_side[side] = 0;
+    a.sum->e_side[side] = 0.0;
+    const double* Tf = a.face_T[side];
+    if (Tf && a.n_boundary > 0) {
+      const bool along2 = side < 2;
+      const int nf = along2 ? a.ny : a.nx;
+      double* Ef = a.face + (size_t)(side * 2 + 0) * a.nf;
+      double* cdf = a.face + (size_t)(side * 2 + 1) * a.nf;
+      double Et = 0.0;
+      for (int q = 0; q < nf; ++q) {
+        double area;
+        if (a.geom == G_XY) area = along2 ? (a.e2[q + 1] - a.e2[q]) : (a.e1[q + 1] - a.e1[q]);
+        else if (along2) { const double R = side == 0 ? a.e1[0] : a.e1[a.nx]; area = 2.0 * PI * R * (a.e2[q + 1] - a.e2[q]); }
+        else area = PI * (a.e1[q + 1] * a.e1[q + 1] - a.e1[q] * a.e1[q]);
+        const double T = Tf[q];
+        Ef[q] = (T > 0.0) ? A_RAD * C_LIGHT * T * T * T * T / 4.0 * area * a.dt : 0.0;
+        Et += Ef[q];
+        cdf[q] = Et;
+      }
+      if (Et > 0.0) {
+        a.sum->n_side[side] = a.n_boundary;
+        a.sum->e_side[side] = (double)a.n_boundary * (double)(float)(Et / (double)a.n_boundary);
+      }
+    }
+  }
+  __syncthreads();
+  if (t == 0) {
+    long long base = a.sum->n_census;
+    for (int q = 0; q < 4; ++q) { a.sum->base_side[q] = base; base += a.sum->n_side[q]; }
+    a.sum->n_source = n_src; a.sum->base_source = base; base += n_src;
+    a.sum->n_emission = n_emit; a.sum->base_emission = base; base += n_emit;
+    a.sum->n_bank = base;
+    a.sum->source_emission = e_src;
+    a.sum->emission_total = issued;
+  }
+}
+
+// multigroup initial census plan: cell CDF of a Tr^4 V, N particles of weight E/N
+__global__ void __launch_bounds__(NT) k_ic_plan_mg(IcMgArgs a) {
+  __shared__ double sh[NT];
+  const int t = threadIdx.x;
+  if (t == 0) {
+    double tot = 0.0;
+    for (int n = 1; n <= 200; ++n) { const double d = (double)n; tot += 1.0 / (d * d * d * d); }
+    double run = 0.0;
+    for (int n = 1; n <= 200; ++n) { const double d = (double)n; run += 1.0 / (d * d * d * d); a.mixcdf[n - 1] = run / tot; }
+  }
+  for (int c = t; c < a.nc; c += NT) {
+    double e = A_RAD * pow4(a.tr[c]) * a.vol[c];
+    if (a.t_emit_floor > 0.0 && a.tr[c] < a.t_emit_floor) e = 0.0;
+    a.E[c] = e;
+  }
+  __syncthreads();
+  block_canon_prefix(a.E, a.nc, a.cdf, sh);
+  if (t == 0) {
+    const double Et = a.cdf[a.nc - 1];
+    const long long n = (a.n_target > 0 && Et > 0.0) ? a.n_target : 0;
+    a.sum->n_emission = n; a.sum->base_emission = 0; a.sum->n_bank = n;
+  }
+}
+
+}  // namespace
+
+cudaError_t imc_launch_plan_mg(const PlanMgArgs& a, cudaStream_t s) {
+  ++g_imc_launches;
+  k_plan_mg<<<1, NT, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t imc_launch_ic_plan_mg(const IcMgArgs& a, cudaStream_t s) {
+  ++g_imc_launches;
+  k_ic_plan_mg<<<1, NT, 0, s>>>(a);
+  return cudaGetLastError();
+}

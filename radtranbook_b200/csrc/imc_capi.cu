@@ -59,12 +59,14 @@ imc_status check_mesh(const imc_mesh* m) {
   if (m->nx <= 0 || m->ny <= 0) return IMC_ERR_BAD_GEOMETRY;
   const bool oned = m->geometry == IMC_GEOM_SLAB || m->geometry == IMC_GEOM_SPHERE;
   if (oned && m->ny != 1) return IMC_ERR_BAD_GEOMETRY;
-  if (m->n_groups != 1) return IMC_ERR_INVALID_ARG;  // multigroup tracking: not in this build
+  if (m->n_groups < 1) return IMC_ERR_INVALID_ARG;
+  if (m->n_groups > 1 && (oned || !m->group_edges)) return IMC_ERR_INVALID_ARG;  // MG: xy / rz
   return IMC_OK;
 }
 
-bool bank_ok(const imc_bank* b, bool two_d) {
+bool bank_ok(const imc_bank* b, bool two_d, bool mg = false) {
   if (!b || !b->pos1 || !b->dir1 || !b->weight || !b->time || !b->cell) return false;
+  if (mg && !b->group) return false;
   if (two_d && (!b->pos2 || !b->dir2)) return false;
   return b->size >= 0 && b->capacity >= b->size && b->capacity < (1LL << 31);
 }
@@ -90,10 +92,13 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   imc_status st = check_mesh(mesh);
   if (st != IMC_OK) return st;
   const bool two_d = mesh->geometry >= IMC_GEOM_XY;
+  const int ng = mesh->n_groups;
+  const bool mg = ng > 1;
   if (!mat || !mat->temperature || !mat->sigma || !mat->cv || !par || !tal || !sum) return IMC_ERR_INVALID_ARG;
   if (!tal->dep || !tal->si || !tal->emitted || !tal->sigma_a || !tal->sigma_s || !tal->escaped || !tal->stats)
     return IMC_ERR_INVALID_ARG;
-  if (!bank_ok(bank, two_d) || !workspace) return IMC_ERR_INVALID_ARG;
+  if (mg && (!tal->escaped_group || !tal->boundary_group)) return IMC_ERR_INVALID_ARG;
+  if (!bank_ok(bank, two_d, mg) || !workspace) return IMC_ERR_INVALID_ARG;
   if (!(par->dt > 0.0) || par->n_target < 0 || par->n_boundary < 0 || par->n_source < 0) return IMC_ERR_INVALID_ARG;
   const long long bound = source_bound(mesh, par);
   const long long n_upper = bank->size + bound;
@@ -127,7 +132,31 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   pa.emitted = tal->emitted;
   pa.face = ws_ptr<double>(workspace, L.face); pa.nf = std::max(mesh->nx, mesh->ny);
   pa.sum = sum;
-  IMC_CUDA(imc_launch_plan(pa, s));
+  PlanMgArgs pm{};
+  if (!mg) {
+    IMC_CUDA(imc_launch_plan(pa, s));
+  } else {
+    IMC_CUDA(cudaMemsetAsync(tal->boundary_group, 0, sizeof(double) * ng, s));
+    IMC_CUDA(cudaMemsetAsync(tal->escaped_group, 0, sizeof(double) * ng, s));
+    pm.geom = mesh->geometry; pm.nx = mesh->nx; pm.ny = mesh->ny; pm.nc = nc; pm.ng = ng;
+    pm.e1 = mesh->edges1; pm.e2 = mesh->edges2; pm.vol = mesh->volume;
+    pm.T = mat->temperature; pm.sigma = mat->sigma; pm.cv = mat->cv; pm.source = mat->source;
+    pm.gedges = mesh->group_edges; pm.emission_fractions = par->emission_fractions;
+    pm.dt = par->dt; pm.theta = par->theta;
+    pm.n_target = par->n_target; pm.n_source = par->n_source; pm.n_boundary = par->n_boundary;
+    for (int q = 0; q < 4; ++q) pm.face_T[q] = par->face_T[q];
+    pm.t_emit_floor = par->t_emit_floor;
+    pm.sa = tal->sigma_a; pm.ss = tal->sigma_s; pm.sass = pa.sass; pm.cellf = pa.cellf;
+    pm.e1f = pa.e1f; pm.e2f = pa.e2f;
+    pm.Egc = ws_ptr<double>(workspace, L.mg_gcdf); pm.Ec = ws_ptr<double>(workspace, L.mg_ec);
+    pm.cdf = ws_ptr<double>(workspace, L.mg_cdf);
+    pm.Sgc = ws_ptr<double>(workspace, L.mg_sgcdf); pm.Sc = ws_ptr<double>(workspace, L.mg_sc);
+    pm.Scdf = ws_ptr<double>(workspace, L.mg_scdf);
+    pm.emitted = tal->emitted; pm.face = pa.face; pm.nf = pa.nf;
+    pm.mixcdf = ws_ptr<double>(workspace, L.mixcdf);
+    pm.sum = sum;
+    IMC_CUDA(imc_launch_plan_mg(pm, s));
+  }
 
   // ---- sources, appended in the reference's order: census | boundary | fixed | emission ----
   PhaseEvents& pe = phase_events();
@@ -144,6 +173,8 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     ba.dt = par->dt; ba.seed = par->seed; ba.step = par->step;
     ba.p1 = bank->pos1; ba.p2 = p2; ba.d1 = bank->dir1; ba.d2 = d2; ba.wb = bank->weight;
     ba.t = bank->time; ba.cell = bank->cell; ba.group = bank->group;
+    ba.ng = ng; ba.faceT = par->face_T[side]; ba.gedges = mesh->group_edges;
+    ba.mixcdf = ws_ptr<double>(workspace, L.mixcdf); ba.boundary_group = tal->boundary_group;
     IMC_CUDA(imc_launch_fill_boundary(ba, s));
   }
   auto fill = [&](const int64_t* d_n, const int64_t* d_base, long long n_bound, const long long* off,
@@ -158,21 +189,37 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     fa.t = bank->time; fa.cell = bank->cell; fa.group = bank->group;
     return imc_launch_fill_volume(fa, s);
   };
+  auto fill_mg = [&](const int64_t* d_n, const int64_t* d_base, long long n_bound, const double* cdf,
+                     const double* gcdf, uint32_t tag) -> cudaError_t {
+    FillMgArgs fm{};
+    fm.geom = mesh->geometry; fm.nx = mesh->nx; fm.ny = mesh->ny; fm.nc = nc; fm.ng = ng;
+    fm.e1 = mesh->edges1; fm.e2 = mesh->edges2; fm.cdf = cdf; fm.gcdf = gcdf; fm.tr = nullptr;
+    fm.gedges = mesh->group_edges; fm.mixcdf = ws_ptr<double>(workspace, L.mixcdf);
+    fm.d_n = d_n; fm.d_base = d_base; fm.n_bound = n_bound;
+    fm.time_scale = par->dt; fm.seed = par->seed; fm.step = par->step; fm.tag = tag;
+    fm.p1 = bank->pos1; fm.p2 = p2; fm.d1 = bank->dir1; fm.d2 = d2; fm.wb = bank->weight;
+    fm.t = bank->time; fm.cell = bank->cell; fm.group = bank->group;
+    return imc_launch_fill_mg(fm, s);
+  };
   const bool rzlin = mesh->geometry == IMC_GEOM_RZ && par->rz_linear_source;
-  if (mat->source && par->n_source > 0)
+  if (mg) {
+    if (mat->source && par->n_source > 0)
+      IMC_CUDA(fill_mg(&sum->n_source, &sum->base_source, par->n_source, pm.Scdf, pm.Sgc, imcdev::TAG_SOURCE));
+    if (par->n_target > 0)
+      IMC_CUDA(fill_mg(&sum->n_emission, &sum->base_emission, par->n_target, pm.cdf, pm.Egc, imcdev::TAG_EMISSION));
+  } else if (mat->source && par->n_source > 0)
     IMC_CUDA(fill(&sum->n_source, &sum->base_source, par->n_source + nc, pa.src_off, pa.src_w,
                   rzlin ? pa.tilt : nullptr, rzlin ? 3 : 0, imcdev::TAG_SOURCE));
   int ekind = 0;
   if (mesh->geometry == IMC_GEOM_SLAB) ekind = 1;
   else if (mesh->geometry == IMC_GEOM_SPHERE) ekind = 2;
   else if (rzlin) ekind = 3;
-  if (par->n_target > 0)
+  if (!mg && par->n_target > 0)
     IMC_CUDA(fill(&sum->n_emission, &sum->base_emission, par->n_target + nc, pa.emit_off, pa.emit_w,
                   ekind ? pa.tilt : nullptr, ekind, imcdev::TAG_EMISSION));
 
   // ---- tracking ----
   if (pe.ok) IMC_CUDA(cudaEventRecord(pe.e[1], s));
-  const int ng = 1;
   IMC_CUDA(cudaMemsetAsync(tal->dep, 0, sizeof(double) * nc * ng, s));
   IMC_CUDA(cudaMemsetAsync(tal->si, 0, sizeof(double) * nc * ng, s));
   IMC_CUDA(cudaMemsetAsync(tal->escaped, 0, sizeof(double) * 4, s));
@@ -197,10 +244,11 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   ta.seed = par->seed; ta.step = par->step;
   ta.chunk = par->chunk > 0 ? par->chunk : 64;
   ta.group_edges = mesh->group_edges;
+  ta.escaped_group = tal->escaped_group;
   const int block = par->block_size > 0 ? par->block_size : 256;
   const int bps = par->blocks_per_sm > 0 ? par->blocks_per_sm : 3;
   // reserved: bit 0 = stage the cell table in shared memory, bit 1 = prefetch the next draw
-  const bool smem_cells = (par->reserved & 1) ? true : (nc <= 4096);
+  const bool smem_cells = (par->reserved & 1) ? true : ((long long)nc * ng <= 4096);
   const bool prefetch = (par->reserved & 2) != 0;
   IMC_CUDA(imc_launch_track(ta, mesh->geometry, block, sm_count() * bps, smem_cells, prefetch, s));
   if (pe.ok) { IMC_CUDA(cudaEventRecord(pe.e[2], s)); pe.recorded = true; }
@@ -270,6 +318,11 @@ WsLayout imc_ws_layout(const imc_mesh* m, int64_t capacity) {
   L.src_n = take(8 * nc); L.src_off = take(8 * (nc + 1)); L.src_w = take(4 * nc);
   L.src_QV = take(8 * nc); L.src_issued = take(8 * nc);
   L.face = take(8 * 4 * 2 * nf);
+  if (ng > 1) {
+    L.mg_gcdf = take(8 * ncg); L.mg_ec = take(8 * nc); L.mg_cdf = take(8 * nc);
+    L.mg_sgcdf = take(8 * ncg); L.mg_sc = take(8 * nc); L.mg_scdf = take(8 * nc);
+  }
+  L.mixcdf = take(8 * 200);
   L.ecen = take(8 * ncg); L.ew = take(8 * ncg); L.ncopy = take(8 * ncg);
   L.cnt = take(4 * cap); L.blk = take(8 * ((cap + 1023) / 1024 + 2));
   L.total = o;
@@ -329,6 +382,29 @@ imc_status imc_init_census(const imc_mesh* mesh, const double* tr, int64_t n_tar
   if (bound > bank->capacity) { if (n_out) *n_out = bound; return IMC_ERR_BANK_OVERFLOW; }
   imc_step_summary* sum = internal_summary(workspace, L);
   IMC_CUDA(cudaMemsetAsync(sum, 0, sizeof(imc_step_summary), s));
+  if (mesh->n_groups > 1) {
+    if (!bank->group) return IMC_ERR_INVALID_ARG;
+    IcMgArgs im{};
+    im.nc = nc; im.vol = mesh->volume; im.tr = tr; im.n_target = n_target; im.t_emit_floor = t_emit_floor;
+    im.E = ws_ptr<double>(workspace, L.mg_ec); im.cdf = ws_ptr<double>(workspace, L.mg_cdf);
+    im.mixcdf = ws_ptr<double>(workspace, L.mixcdf); im.sum = sum;
+    IMC_CUDA(imc_launch_ic_plan_mg(im, s));
+    FillMgArgs fm{};
+    fm.geom = mesh->geometry; fm.nx = mesh->nx; fm.ny = mesh->ny; fm.nc = nc; fm.ng = mesh->n_groups;
+    fm.e1 = mesh->edges1; fm.e2 = mesh->edges2; fm.cdf = im.cdf; fm.gcdf = nullptr; fm.tr = tr;
+    fm.gedges = mesh->group_edges; fm.mixcdf = im.mixcdf;
+    fm.d_n = &sum->n_emission; fm.d_base = &sum->base_emission; fm.n_bound = n_target;
+    fm.time_scale = 0.0; fm.seed = seed; fm.step = 0; fm.tag = imcdev::TAG_IC;
+    fm.p1 = bank->pos1; fm.p2 = bank->pos2; fm.d1 = bank->dir1; fm.d2 = bank->dir2; fm.wb = bank->weight;
+    fm.t = bank->time; fm.cell = bank->cell; fm.group = bank->group;
+    IMC_CUDA(imc_launch_fill_mg(fm, s));
+    long long n = 0;
+    IMC_CUDA(cudaMemcpyAsync(&n, &sum->n_emission, sizeof(n), cudaMemcpyDeviceToHost, s));
+    IMC_CUDA(cudaStreamSynchronize(s));
+    bank->size = n;
+    if (n_out) *n_out = n;
+    return IMC_OK;
+  }
   IcArgs ia{};
   ia.geom = mesh->geometry; ia.nx = mesh->nx; ia.ny = mesh->ny; ia.nc = nc;
   ia.e1 = mesh->edges1; ia.e2 = mesh->edges2; ia.vol = mesh->volume; ia.tr = tr;
@@ -398,7 +474,7 @@ imc_status imc_material_update(const imc_mesh* mesh, const imc_tallies* tal, dou
   if (st != IMC_OK) return st;
   if (!tal || !tal->dep || !tal->si || !tal->emitted || !e || !tr) return IMC_ERR_INVALID_ARG;
   MatArgs ma{};
-  ma.nc = mesh->nx * mesh->ny; ma.ng = 1; ma.vol = mesh->volume;
+  ma.nc = mesh->nx * mesh->ny; ma.ng = mesh->n_groups; ma.vol = mesh->volume;
   ma.dep = tal->dep; ma.si = tal->si; ma.emitted = tal->emitted; ma.e = e; ma.tr = tr;
   IMC_CUDA(imc_launch_material(ma, (cudaStream_t)stream));
   return IMC_OK;

@@ -147,6 +147,22 @@ __device__ __forceinline__ void warp_tally1(bool flush, int key, double va, doub
   __syncwarp();
 }
 
+// Group of a photon sampled from the Planck spectrum at T (mixture of Gammas,
+// MG_IMC/MG_IMC2D.py:202-254): n from the 1/n^4 mixture CDF, x = (four Exp(1)) / n,
+// energy T*x located in the group edges.
+__device__ __forceinline__ int planck_group(double T, const double* edges, int G, const double* mixcdf, double un,
+                                            double u1, double u2, double u3, double u4) {
+  if (!(T > 0.0)) return 0;
+  double ns = 200.0;
+  for (int i = 0; i < 200; ++i) if (un <= mixcdf[i]) { ns = (double)(i + 1); break; }
+  const double x = (-log(u1) - log(u2) - log(u3) - log(u4)) / ns;
+  const double f = T * x;
+  if (f < edges[0]) return 0;
+  if (f >= edges[G]) return G - 1;
+  for (int g = 0; g < G; ++g) if (f >= edges[g] && f < edges[g + 1]) return g;
+  return G - 1;
+}
+
 __device__ __forceinline__ double warp_sum_d(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);

@@ -38,6 +38,7 @@ struct TrackArgs {
   uint32_t step;
   int chunk;
   const double* group_edges; // MG
+  double* escaped_group;     // MG: [ng]
 };
 
 cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool smem_cells, bool prefetch,
@@ -57,6 +58,7 @@ struct WsLayout {
   size_t tilt;                // double [4*nc] per-cell tilt constants
   size_t src_n, src_off, src_w, src_QV, src_issued;  // fixed source
   size_t face;                // double [4][2][nf] per-side face energies and CDF
+  size_t mg_gcdf, mg_ec, mg_cdf, mg_sgcdf, mg_sc, mg_scdf, mixcdf;  // multigroup tables
   size_t summary;             // imc_step_summary used by the synchronous wrappers
   size_t queue;               // uint64 ticket counter
   size_t ecen, ew, ncopy;     // comb: double [nb], double [nb], long long [nb]
@@ -156,6 +158,8 @@ struct BndArgs {
   double dt;
   uint64_t seed; uint32_t step;
   float* p1; float* p2; float* d1; float* d2; float* wb; float* t; int* cell; int* group;
+  // multigroup: Planck group at the face cell's temperature
+  int ng; const double* faceT; const double* gedges; const double* mixcdf; double* boundary_group;
 };
 cudaError_t imc_launch_fill_boundary(const BndArgs& a, cudaStream_t s);
 
@@ -184,3 +188,51 @@ cudaError_t imc_launch_comb_scatter(const CombArgs& a, cudaStream_t s);
 cudaError_t imc_launch_philox(const uint32_t* ctr, uint32_t k0, uint32_t k1, uint32_t* out, long long n, cudaStream_t s);
 
 extern unsigned long long g_imc_launches;
+
+// ---------------------------------------------------------------------------------
+// Multigroup planning and sources
+// ---------------------------------------------------------------------------------
+struct PlanMgArgs {
+  int geom, nx, ny, nc, ng;
+  const double* e1; const double* e2; const double* vol;
+  const double* T; const double* sigma; const double* cv; const double* source;  // sigma, source [g][c]
+  const double* gedges; const double* emission_fractions;
+  double dt, theta;
+  long long n_target, n_source, n_boundary;
+  const double* face_T[4];
+  double t_emit_floor;
+  double* sa; double* ss; float2* sass; double2* cellf;  // [g][c]
+  float* e1f; float* e2f;
+  double* Egc; double* Ec; double* cdf;       // emission: [c][g] cumulative, [c], [c] canonical prefix
+  double* Sgc; double* Sc; double* Scdf;      // fixed source, same shapes
+  double* emitted;                            // [c]
+  double* face; int nf;
+  double* mixcdf;                             // [200]
+  imc_step_summary* sum;
+};
+cudaError_t imc_launch_plan_mg(const PlanMgArgs& a, cudaStream_t s);
+
+struct IcMgArgs {
+  int nc;
+  const double* vol; const double* tr;
+  long long n_target; double t_emit_floor;
+  double* E; double* cdf; double* mixcdf;
+  imc_step_summary* sum;
+};
+cudaError_t imc_launch_ic_plan_mg(const IcMgArgs& a, cudaStream_t s);
+
+// categorical (cell ~ total, group ~ per-cell cumulative) multigroup source fill; the IC
+// variant samples the group from the Planck spectrum at tr[c] instead
+struct FillMgArgs {
+  int geom, nx, ny, nc, ng;
+  const double* e1; const double* e2;
+  const double* cdf;           // [c] canonical inclusive prefix of cell totals
+  const double* gcdf;          // [c][g] cumulative over groups (NULL: Planck group at tr)
+  const double* tr;            // IC: [c]
+  const double* gedges; const double* mixcdf;
+  const int64_t* d_n; const int64_t* d_base; long long n_bound;
+  double time_scale;
+  uint64_t seed; uint32_t step; uint32_t tag;
+  float* p1; float* p2; float* d1; float* d2; float* wb; float* t; int* cell; int* group;
+};
+cudaError_t imc_launch_fill_mg(const FillMgArgs& a, cudaStream_t s);

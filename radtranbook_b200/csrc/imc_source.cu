@@ -209,7 +209,62 @@ __global__ void k_fill_boundary(BndArgs a) {
     a.wb[b] = wq;
     a.t[b] = (float)t;
     a.cell[b] = i + a.nx * j;
-    if (a.group) a.group[b] = 0;
+    if (a.group) {
+      int g = 0;
+      if (a.ng > 1) {
+        const U4 rd = draw(a.seed, (uint32_t)k, 2, a.step, TAG_BOUNDARY | (uint32_t)a.side);
+        g = planck_group(a.faceT[q], a.gedges, a.ng, a.mixcdf, u01d(rb.y), u01d(rb.z), u01d(rb.w), u01d(rd.x),
+                         u01d(rd.y));
+        atomicAdd(a.boundary_group + g, (double)wq);
+      }
+      a.group[b] = g;
+    }
+  }
+}
+
+// multigroup categorical sources (MG_IMC/MG_IMC2D.py:1098-1170, 1866-1943) and the MG
+// initial census (:992-1097): cell ~ canonical CDF over cells, group ~ the cell's cumulative
+// group emission (or the Planck spectrum at tr for the IC), equal weights, uniform position.
+__global__ void k_fill_mg(FillMgArgs a) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long n = *a.d_n, base = *a.d_base;
+  if (n <= 0) return;
+  const double total = a.cdf[a.nc - 1];
+  const float wq = (float)(total / (double)n);
+  const bool ic = a.gcdf == nullptr;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+    const U4 ra = draw(a.seed, (uint32_t)k, 0, a.step, a.tag);
+    const U4 rb = draw(a.seed, (uint32_t)k, 1, a.step, a.tag);
+    const double x = u01d(ra.x) * total;
+    int lo = 0, hi = a.nc;  // first c with cdf[c] > x
+    while (lo < hi) { const int mid = (lo + hi) >> 1; if (a.cdf[mid] <= x) lo = mid + 1; else hi = mid; }
+    const int c = min(lo, a.nc - 1);
+    const int i = c % a.nx, j = c / a.nx;
+    const double e1a = a.e1[i], e1b = a.e1[i + 1], e2a = a.e2[j], e2b = a.e2[j + 1];
+    int g;
+    double up1, up2, ua, ub, ut;
+    if (!ic) {
+      const double* gc = a.gcdf + (size_t)c * a.ng;
+      const double y = u01d(ra.y) * gc[a.ng - 1];
+      g = a.ng - 1;
+      for (int q = 0; q < a.ng; ++q) if (gc[q] >= y) { g = q; break; }
+      up1 = u01d(ra.z); up2 = u01d(ra.w); ua = u01d(rb.x); ub = u01d(rb.y); ut = u01d(rb.z);
+    } else {
+      const U4 rd = draw(a.seed, (uint32_t)k, 2, a.step, a.tag);
+      up1 = u01d(ra.y); up2 = u01d(ra.z); ua = u01d(ra.w); ub = u01d(rb.x); ut = 0.0;
+      g = planck_group(a.tr[c], a.gedges, a.ng, a.mixcdf, u01d(rb.y), u01d(rb.z), u01d(rb.w), u01d(rd.x), u01d(rd.y));
+    }
+    double p1 = (a.geom == G_RZ) ? sqrt(e1a * e1a + up1 * (e1b * e1b - e1a * e1a)) : e1a + up1 * (e1b - e1a);
+    const double p2 = e2a + up2 * (e2b - e2a);
+    double d1, d2;
+    iso_dir(a.geom, ua, ub, d1, d2);
+    const long long b = base + k;
+    a.p1[b] = (float)p1; a.p2[b] = (float)p2;
+    a.d1[b] = (float)d1; a.d2[b] = (float)d2;
+    a.wb[b] = wq;
+    a.t[b] = (float)(ut * a.time_scale);
+    a.cell[b] = c;
+    a.group[b] = g;
   }
 }
 
@@ -248,6 +303,13 @@ cudaError_t imc_launch_fill_boundary(const BndArgs& a, cudaStream_t s) {
   if (a.n_bound <= 0) return cudaSuccess;
   ++g_imc_launches;
   k_fill_boundary<<<grid_for(a.n_bound, 256), 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t imc_launch_fill_mg(const FillMgArgs& a, cudaStream_t s) {
+  if (a.n_bound <= 0) return cudaSuccess;
+  ++g_imc_launches;
+  k_fill_mg<<<grid_for(a.n_bound, 256), 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 

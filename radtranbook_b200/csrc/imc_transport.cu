@@ -25,7 +25,10 @@ namespace {
 // Block-level counters for rare events (shared-memory atomics keep them out of registers).
 enum : int { B_CENSUS = 0, B_FLOOR, B_REFLECT, B_CAP, B_ESCAPE, B_N };
 
-template <int GEOM, bool SMEM_CELLS, bool PREFETCH>
+// MG: multigroup rules of MG_IMC/MG_IMC2D.py:580-989 (group-indexed tables, no effective-
+// scatter cap, no absorption for sigma_a <= 1e-12, the weight floor ends a history after its
+// event is committed, escaped energy also by group).
+template <int GEOM, bool SMEM_CELLS, bool PREFETCH, bool MG>
 __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ unsigned blk_cnt[B_N];
@@ -38,7 +41,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   for (int q = threadIdx.x; q <= a.nx; q += blockDim.x) E1[q] = a.e1[q];
   for (int q = threadIdx.x; q <= a.ny; q += blockDim.x) E2[q] = a.e2[q];
   if (SMEM_CELLS)
-    for (int q = threadIdx.x; q < a.nc; q += blockDim.x) CS[q] = a.sass[q];
+    for (int q = threadIdx.x; q < a.nc * a.ng; q += blockDim.x) CS[q] = a.sass[q];
   if (threadIdx.x < B_N) blk_cnt[threadIdx.x] = 0u;
   if (threadIdx.x < 4) blk_esc[threadIdx.x] = 0.0;
   __syncthreads();
@@ -57,7 +60,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   uint32_t pid = 0, ev = 0;
   U4 rnext{0u, 0u, 0u, 0u};  // PREFETCH: the next event's draw, computed one event ahead
   float x = 0, y = 0, u = 0, v = 0, w = 0, dcen = 0;
-  int ci = 0, cj = 0;
+  int ci = 0, cj = 0, grp = 0;
   double acc_lost = 0.0, acc_wd = 0.0;  // energy removed / w*s in the current cell
   unsigned s_bd = 0, s_sc = 0;          // per-event counters (census/cap counted at finish)
 
@@ -93,8 +96,9 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
         pid = chunk_next + rank;
         w = a.w[pid];
         dcen = (a.dt - a.t[pid]) * c_light;
-        if (w > 0.f && dcen > 0.f) {
+        if ((MG ? w > weight_floor : w > 0.f) && dcen > 0.f) {
           x = a.p1[pid]; u = a.d1[pid];
+          if (MG) grp = a.group[pid];
           if (GEOM == G_XY || GEOM == G_RZ) { y = a.p2[pid]; v = a.d2[pid]; }
           const int c = a.cell[pid];
           cj = c / a.nx; ci = c - cj * a.nx;
@@ -113,9 +117,10 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
     double f_lost = 0.0, f_wd = 0.0;
     if (has) {
       const int c = ci + a.nx * cj;
+      const int cq = MG ? c + a.nc * grp : c;  // (group, cell) table / tally index
       float sa, ss;
-      if (SMEM_CELLS) { const float2 q = CS[c]; sa = q.x; ss = q.y; }
-      else { const float2 q = __ldg(a.sass + c); sa = q.x; ss = q.y; }
+      if (SMEM_CELLS) { const float2 q = CS[cq]; sa = q.x; ss = q.y; }
+      else { const float2 q = __ldg(a.sass + cq); sa = q.x; ss = q.y; }
       bool finished = false, frozen = false;
       if (ev >= (uint32_t)a.max_events) {
         // events-per-history cap (IMC/IMC2D.py:974-977): stops, weight stays in census
@@ -178,7 +183,8 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
         // short series, so the logarithm is evaluated only when it can win.
         float ds = BIGF;
         {
-          const float sig = (ss * L > 10000.0f) ? 10000.0f / L : (ss > ss_thr ? ss : 0.f);
+          const bool capped = !MG && ss * L > 10000.0f;
+          const float sig = capped ? 10000.0f / L : (ss > ss_thr ? ss : 0.f);
           if (sig > 0.f) {
             const float s_other = fminf(sb, dcen);
             const double t = (double)sig * (double)s_other;
@@ -187,7 +193,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
               const double thr = 1.0 - t * (1.0 - t * (0.5 - t * (1.0 / 6.0)));
               may = u01d(r.x) > thr;
             }
-            if (may) ds = (ss * L > 10000.0f) ? neglog_u(r.x) * (L * 1e-4f) : __fdividef(neglog_u(r.x), ss);
+            if (may) ds = capped ? neglog_u(r.x) * (L * 1e-4f) : __fdividef(neglog_u(r.x), ss);
           }
         }
         d = sb; evt = EV_BOUNDARY;
@@ -249,14 +255,14 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
           xn = rn;
         }
         // implicit capture; the energy removed is the exact difference of the FP32 weights
-        const float wn = w * __expf(-sa * d);
+        const float wn = (MG && !(sa > 1e-12f)) ? w : w * __expf(-sa * d);
         acc_lost += (double)w - (double)wn;
         acc_wd += (double)(w * d);
         dcen -= d;
         if (evt == EV_BOUNDARY) ++s_bd; else if (evt == EV_SCATTER) ++s_sc;
         else atomicAdd(&blk_cnt[B_CENSUS], 1u);
 
-        if (GEOM == G_XY || GEOM == G_RZ) {
+        if (!MG && (GEOM == G_XY || GEOM == G_RZ)) {
           if (wn <= weight_floor) {
             // IMC/IMC2D.py:1043-1047: history stops in place keeping its weight
             atomicAdd(&blk_cnt[B_FLOOR], 1u);
@@ -269,7 +275,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
           w = wn; x = xn; y = yn; u = un; v = vn;
           if (cross != X_NONE) {
             // leaving the cell: flush the accumulators for the old cell
-            flush = true; flush_cell = c; f_lost = acc_lost; f_wd = acc_wd;
+            flush = true; flush_cell = cq; f_lost = acc_lost; f_wd = acc_wd;
             acc_lost = 0.0; acc_wd = 0.0;
             int ni = ci, nj = cj;
             if (cross == X_IP) ++ni; else if (cross == X_IM) --ni; else if (cross == X_JP) ++nj; else --nj;
@@ -282,6 +288,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
                 atomicAdd(&blk_cnt[B_REFLECT], 1u);
               } else {
                 atomicAdd(&blk_esc[side], (double)w);
+                if (MG) atomicAdd(a.escaped_group + grp, (double)w);
                 atomicAdd(&blk_cnt[B_ESCAPE], 1u);
                 w = 0.f;
                 finished = true;
@@ -303,6 +310,11 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
               w = 0.f;
               finished = true;
             }
+          } else if (MG && !finished && dcen > 0.f && w <= weight_floor) {
+            // MG_IMC/MG_IMC2D.py:858-860: the next event would stop at the floor (a weight
+            // that underflowed to 0 included)
+            atomicAdd(&blk_cnt[B_FLOOR], 1u);
+            finished = true;
           } else if (!finished && !(w > 0.f)) {
             w = 0.f;
             finished = true;
@@ -315,7 +327,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
         // ended by crossing has already queued the old cell and holds nothing new: a 1-D
         // weight-floor kill after a crossing deposits directly.)
         if (!flush && (acc_lost != 0.0 || acc_wd != 0.0)) {
-          flush = true; flush_cell = c; f_lost = acc_lost; f_wd = acc_wd;
+          flush = true; flush_cell = cq; f_lost = acc_lost; f_wd = acc_wd;
         }
         acc_lost = 0.0; acc_wd = 0.0;
         a.w[pid] = w;
@@ -360,34 +372,41 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   if (threadIdx.x < 4 && blk_esc[threadIdx.x] != 0.0) atomicAdd(a.escaped + threadIdx.x, blk_esc[threadIdx.x]);
 }
 
-template <int GEOM, bool SM, bool PF>
+template <int GEOM, bool SM, bool PF, bool MG>
 cudaError_t launch_one(const TrackArgs& a, int block, int grid, cudaStream_t s) {
   const int nwarps = block / 32;
   size_t sh = nwarps * sizeof(WarpStage) + sizeof(float) * (a.nx + a.ny + 4);
-  if (SM) sh += sizeof(float2) * a.nc;
+  if (SM) sh += sizeof(float2) * a.nc * a.ng;
   if (sh > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_track<GEOM, SM, PF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+    cudaError_t e = cudaFuncSetAttribute(k_track<GEOM, SM, PF, MG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
     if (e != cudaSuccess) return e;
   }
-  k_track<GEOM, SM, PF><<<grid, block, sh, s>>>(a);
+  k_track<GEOM, SM, PF, MG><<<grid, block, sh, s>>>(a);
   return cudaGetLastError();
 }
 
-template <int GEOM>
+template <int GEOM, bool MG>
 cudaError_t launch_geom(const TrackArgs& a, int block, int grid, bool sm, bool pf, cudaStream_t s) {
-  if (sm) return pf ? launch_one<GEOM, true, true>(a, block, grid, s) : launch_one<GEOM, true, false>(a, block, grid, s);
-  return pf ? launch_one<GEOM, false, true>(a, block, grid, s) : launch_one<GEOM, false, false>(a, block, grid, s);
+  if (sm) return pf ? launch_one<GEOM, true, true, MG>(a, block, grid, s) : launch_one<GEOM, true, false, MG>(a, block, grid, s);
+  return pf ? launch_one<GEOM, false, true, MG>(a, block, grid, s) : launch_one<GEOM, false, false, MG>(a, block, grid, s);
 }
 
 }  // namespace
 
 cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool sm, bool pf, cudaStream_t s) {
   ++g_imc_launches;
+  if (a.ng > 1) {  // multigroup: 2-D geometries (MG_IMC/MG_IMC2D.py)
+    switch (geom) {
+      case G_XY: return launch_geom<G_XY, true>(a, block, grid, sm, pf, s);
+      case G_RZ: return launch_geom<G_RZ, true>(a, block, grid, sm, pf, s);
+      default: return cudaErrorInvalidValue;
+    }
+  }
   switch (geom) {
-    case G_SLAB: return launch_geom<G_SLAB>(a, block, grid, sm, pf, s);
-    case G_SPHERE: return launch_geom<G_SPHERE>(a, block, grid, sm, pf, s);
-    case G_XY: return launch_geom<G_XY>(a, block, grid, sm, pf, s);
-    case G_RZ: return launch_geom<G_RZ>(a, block, grid, sm, pf, s);
+    case G_SLAB: return launch_geom<G_SLAB, false>(a, block, grid, sm, pf, s);
+    case G_SPHERE: return launch_geom<G_SPHERE, false>(a, block, grid, sm, pf, s);
+    case G_XY: return launch_geom<G_XY, false>(a, block, grid, sm, pf, s);
+    case G_RZ: return launch_geom<G_RZ, false>(a, block, grid, sm, pf, s);
     default: return cudaErrorInvalidValue;
   }
 }

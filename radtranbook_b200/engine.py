@@ -92,7 +92,7 @@ class Engine:
     """One IMC mesh on one device.  Cell arrays are flat, c = i + nx*j (float64)."""
 
     def __init__(self, geometry: str, edges1, edges2, volumes, seed: int = 0x5EED0001, n_groups: int = 1,
-                 capacity: int = 1 << 16, device: torch.device | None = None):
+                 capacity: int = 1 << 16, device: torch.device | None = None, group_edges=None):
         self.lib = _lib.load()
         self.device = device or require_cuda()
         if geometry not in _lib.GEOM:
@@ -112,7 +112,16 @@ class Engine:
         self.vol = torch.as_tensor(np.asarray(volumes, dtype=np.float64).reshape(-1), **f64)
         if self.vol.numel() != self.nc:
             raise ValueError("volumes must have nx*ny entries")
-        self.cmesh = ImcMesh(self.gcode, self.nx, self.ny, n_groups, _ptr(self.e1), _ptr(self.e2), _ptr(self.vol), None)
+        self.gedges = None
+        if n_groups > 1:
+            if group_edges is None or len(group_edges) != n_groups + 1:
+                raise ValueError("multigroup needs n_groups + 1 group edges")
+            self.gedges = torch.as_tensor(np.asarray(group_edges, dtype=np.float64), **f64)
+        self.cmesh = ImcMesh(self.gcode, self.nx, self.ny, n_groups, _ptr(self.e1), _ptr(self.e2), _ptr(self.vol),
+                             _ptr(self.gedges))
+        self.escaped_group = torch.zeros(n_groups, **f64) if n_groups > 1 else None
+        self.boundary_group = torch.zeros(n_groups, **f64) if n_groups > 1 else None
+        self.emission_fractions = None  # optional device tensor [g]
         ncg = self.nc * n_groups
         self.dep = torch.zeros(ncg, **f64)
         self.si = torch.zeros(ncg, **f64)
@@ -123,7 +132,8 @@ class Engine:
         self.stats = torch.zeros(_lib.STAT_N, dtype=torch.int64, device=dev)
         self.disc = torch.zeros(ncg, **f64)
         self.ctal = ImcTallies(_ptr(self.dep), _ptr(self.si), _ptr(self.emitted), _ptr(self.sigma_a),
-                               _ptr(self.sigma_s), _ptr(self.escaped), _ptr(self.stats))
+                               _ptr(self.sigma_s), _ptr(self.escaped), _ptr(self.stats),
+                               _ptr(self.escaped_group), _ptr(self.boundary_group))
         # device step summary (sizes, energies, statistics) and its pinned host copy; the
         # asynchronous step writes its statistics and escaped energy straight into it
         nsum = ctypes.sizeof(ImcStepSummary)
@@ -133,7 +143,8 @@ class Engine:
         base = self.summary_dev.data_ptr()
         self.ctal_async = ImcTallies(_ptr(self.dep), _ptr(self.si), _ptr(self.emitted), _ptr(self.sigma_a),
                                      _ptr(self.sigma_s), base + ImcStepSummary.escaped.offset,
-                                     base + ImcStepSummary.stats.offset)
+                                     base + ImcStepSummary.stats.offset, _ptr(self.escaped_group),
+                                     _ptr(self.boundary_group))
         self._census_dev_valid = False
         self._upper = 0
         mg = n_groups > 1
@@ -261,6 +272,7 @@ class Engine:
         par.blocks_per_sm = int(self.launch["blocks_per_sm"])
         par.chunk = int(self.launch["chunk"])
         par.reserved = int(bool(self.launch.get("smem_cells", 0))) | (int(bool(self.launch.get("prefetch", 0))) << 1)
+        par.emission_fractions = _ptr(self.emission_fractions)
         return par
 
     def _set_census_count(self, n: int) -> None:

@@ -1,0 +1,365 @@
+"""Drop-in for the reference's MG_IMC/MG_IMC2D.py multigroup time-step API (geometry 'xy'
+or 'rz'; a 1-D slab is 'xy' with one cell in y), on the B200 engine.
+
+Same entry points, argument names, defaults, return values and info keys as
+MG_IMC/MG_IMC2D.py:1409 (init_simulation), :1635 (step) and :2125 (run_simulation).
+Group Planck fractions come from the engine's own incomplete-Planck-integral series (the
+reference imports them from an external `planck_integrals` extension, or splits energy
+equally across groups without it, MG_IMC/MG_IMC2D.py:60-94).
+Differences from the reference, all deliberate:
+  - Philox random streams keyed by `seed`;
+  - right/top face sources start inside the last cell (the reference places them at index
+    nx / ny, where they are lost at once, MG_IMC/MG_IMC2D.py:424-441 with :840-852);
+  - a reflection at the -x (-r) face puts the particle back in cell 0 (the reference keeps
+    index -1 and loses it on the next event, MG_IMC/MG_IMC2D.py:916-919);
+  - material emission removes from each cell its nominal emission energy scaled so the total
+    equals the issued particle energy exactly (FP32 weights);
+  - info['ledger'] adds the FP64 energy-balance closure.
+"""
+from __future__ import annotations
+
+import time as _time
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._gray import GrayState, _host_copy, average_tallies, face_temperatures
+from .engine import A_RAD, C_LIGHT, Engine
+from .materials import evaluate
+
+__c = 29.98
+__a = 0.01372
+
+
+def _cell_volumes(edges1, edges2, geometry):
+    if geometry == "xy":
+        return np.diff(edges1)[:, None] * np.diff(edges2)[None, :]
+    if geometry == "rz":
+        return np.pi * (edges1[1:] ** 2 - edges1[:-1] ** 2)[:, None] * np.diff(edges2)[None, :]
+    raise ValueError(f"Unknown geometry: {geometry}")
+
+
+def planck_fractions(energy_edges, T) -> np.ndarray:
+    """Normalised group fractions b*_g(T) on the host, shape (G,) + T.shape (used for the
+    particle-budget estimate of Ntotal); the device computes the same series per cell."""
+    e = np.asarray(energy_edges, dtype=np.float64)
+    T = np.asarray(T, dtype=np.float64)
+
+    def F(x):
+        x = np.asarray(x, dtype=np.float64)
+        out = np.zeros_like(x)
+        c = 15.0 / np.pi ** 4
+        small = (x > 0) & (x < 1.0)
+        xs = x[small]
+        B = [1.0, -0.5, 1 / 6, 0, -1 / 30, 0, 1 / 42, 0, -1 / 30, 0, 5 / 66, 0, -691 / 2730, 0, 7 / 6, 0,
+             -3617 / 510, 0, 43867 / 798, 0, -174611 / 330]
+        acc = np.zeros_like(xs)
+        fact = 1.0
+        for n in range(21):
+            if n > 0:
+                fact *= n
+            if B[n]:
+                acc += B[n] * xs ** (n + 3) / ((n + 3) * fact)
+        out[small] = c * acc
+        big = x >= 1.0
+        xb = x[big]
+        tail = np.zeros_like(xb)
+        for k in range(42, 0, -1):
+            ik = 1.0 / k
+            tail += np.exp(-k * xb) * ik * (xb ** 3 + ik * (3 * xb ** 2 + ik * (6 * xb + ik * 6)))
+        out[big] = 1.0 - c * tail
+        return out
+
+    with np.errstate(divide="ignore", invalid="ignore"):
+        Tpos = np.where(T > 0, T, 1.0)
+        f = np.stack([F(e[g + 1] / Tpos) - F(e[g] / Tpos) for g in range(len(e) - 1)])
+    f = np.clip(f, 0.0, None)
+    tot = f.sum(axis=0)
+    return np.where(tot > 0, f / np.where(tot > 0, tot, 1.0), 0.0)
+
+
+class SimulationState2DMG(GrayState):
+    """Multigroup state: the gray fields plus groups and radiation energy by group."""
+
+    _PARTICLE_2D = dict(GrayState._PARTICLE_2D)
+
+    def __getattr__(self, name):
+        if name == "groups":
+            return object.__getattribute__(self, "_engine").bank.view("group").cpu().numpy().astype(np.int32)
+        return super().__getattr__(name)
+
+
+def init_simulation(Ntarget, Tinit, Tr_init, edges1, edges2, energy_edges, eos, inv_eos, Ntarget_ic=None,
+                    T_emit_floor=0.0, geometry="xy", seed=0x5EED0001):
+    e1 = np.asarray(edges1, dtype=np.float64)
+    e2 = np.asarray(edges2, dtype=np.float64)
+    G = len(energy_edges) - 1
+    vol = _cell_volumes(e1, e2, geometry)
+    eng = Engine(geometry, e1, e2, np.ascontiguousarray(vol.T).reshape(-1), seed=seed, n_groups=G,
+                 group_edges=energy_edges, capacity=4 * int(Ntarget) + 1024)
+    dev = eng.device
+    nx, ny = len(e1) - 1, len(e2) - 1
+    state = SimulationState2DMG(eng, 2, (nx, ny), torch.zeros(eng.nc, dtype=torch.float64, device=dev),
+                                torch.zeros(eng.nc, dtype=torch.float64, device=dev),
+                                torch.zeros(eng.nc, dtype=torch.float64, device=dev), 0.0, 0.0, 0)
+    Tg = torch.as_tensor(np.asarray(Tinit, dtype=np.float64), device=dev)
+    e = evaluate(eos, Tg, lambda: np.asarray(Tinit, dtype=np.float64), Tg)
+    state._e.copy_(state.flat(e))
+    state._T.copy_(state.flat(Tg))
+    back = evaluate(inv_eos, state.grid(state._e), lambda: state.grid(state._e).cpu().numpy(), Tg)
+    assert torch.allclose(back, Tg), "Inverse EOS failed"
+    N_ic = Ntarget if Ntarget_ic is None else Ntarget_ic
+    tr = state.flat(torch.as_tensor(np.asarray(Tr_init, dtype=np.float64), device=dev))
+    eng.init_census(tr, int(N_ic), T_emit_floor)
+    rad = _rad_by_group(eng)
+    object.__setattr__(state, "_rad_group", rad)
+    state.__dict__["radiation_energy_by_group"] = rad.view(G, ny, nx).transpose(1, 2).cpu().numpy().copy()
+    state.__dict__["radiation_energy_by_group_postcomb"] = None
+    state._Tr.copy_(torch.pow(rad.sum(0) / A_RAD, 0.25))
+    radiation, internal = eng.energy_totals(state._e)
+    state.previous_total_energy = internal + radiation
+    state.refresh_host()
+    return state
+
+
+def _rad_by_group(eng: Engine) -> torch.Tensor:
+    """Census radiation energy density by (group, cell) from the bank's weights, (G, nc)."""
+    G, nc = eng.ng, eng.nc
+    acc = torch.zeros(G * nc, dtype=torch.float64, device=eng.device)
+    if eng.bank.size:
+        w = eng.bank.view("weight").double()
+        live = w > 0
+        idx = (eng.bank.view("cell").long() + nc * eng.bank.view("group").long())[live]
+        acc.index_add_(0, idx, w[live])
+    return acc.view(G, nc) / eng.vol.view(1, nc)
+
+
+def _boundary_energy_estimate(geometry, e1, e2, Tb, dt, bsf) -> float:
+    """Analytic boundary emission for the Ntotal split (MG_IMC/MG_IMC2D.py:1546-1632)."""
+    E = 0.0
+    names = ("left", "right", "bottom", "top") if geometry == "xy" else ("rmin", "rmax", "zmin", "zmax")
+    for q, side in enumerate(names):
+        if q < 2:
+            centers, widths = 0.5 * (e2[:-1] + e2[1:]), np.diff(e2)
+            X = e1[0] if q == 0 else e1[-1]
+            area = widths if geometry == "xy" else 2.0 * np.pi * X * widths
+            Ts = np.array([bsf(X, c, side) for c in centers]) if bsf is not None else np.full(len(centers), Tb[q])
+        else:
+            centers = 0.5 * (e1[:-1] + e1[1:])
+            Y = e2[0] if q == 2 else e2[-1]
+            area = np.diff(e1) if geometry == "xy" else np.pi * (e1[1:] ** 2 - e1[:-1] ** 2)
+            Ts = np.array([bsf(c, Y, side) for c in centers]) if bsf is not None else np.full(len(centers), Tb[q])
+        Ts = np.where(Ts > 0, Ts, 0.0)
+        E += float(np.sum(__a * __c * Ts ** 4 / 4.0 * area * dt))
+    return E
+
+
+def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges2, energy_edges, sigma_a_funcs,
+         inv_eos, cv, source, reflect=(False, False, False, False), theta=1.0, use_scalar_intensity_Tr=True,
+         conserve_comb_energy=False, geometry="xy", max_events_per_particle=1_000_000, boundary_source_func=None,
+         emission_fractions=None, Ntotal=0, Ntotal_T_floor=0.0, particle_budget_fmin=0.1, T_emit_floor=0.0,
+         Nmax_growth=0, Nmax_final=None, _timing=False, _allreduce=None):
+    if geometry not in ("xy", "rz"):
+        raise ValueError(f"Unknown geometry: {geometry}")
+    t_step_start = _time.perf_counter()
+    eng: Engine = state._engine
+    G, nc = eng.ng, eng.nc
+    like = state.grid(state._T)
+    host_T = lambda: state.temperature  # noqa: E731
+    sig = torch.stack([state.flat(evaluate(f, like, host_T, like)) for f in sigma_a_funcs])  # (G, nc)
+    cvv = state.flat(evaluate(cv, like, host_T, like))
+    if emission_fractions is not None:
+        eng.emission_fractions = torch.as_tensor(np.asarray(emission_fractions, dtype=np.float64), device=eng.device)
+    else:
+        eng.emission_fractions = None
+    src = None
+    if Nsource > 0 and source is not None:
+        s = np.asarray(source, dtype=np.float64)
+        if s.ndim == 0:
+            s = np.broadcast_to(s, like.shape)
+        if s.ndim == 2:  # gray source goes to the lowest group (MG_IMC/MG_IMC2D.py:1111-1118)
+            s3 = np.zeros((G,) + s.shape)
+            s3[0] = s
+            s = s3
+        if s.max() > 0:
+            src = torch.stack([state.flat(torch.as_tensor(s[g], device=eng.device)) for g in range(G)]).reshape(-1)
+    e1, e2 = np.asarray(edges1, dtype=np.float64), np.asarray(edges2, dtype=np.float64)
+    E_bc_est = E_mat_est = float("nan")
+    if Ntotal > 0:
+        Tb = [T_boundary[q](state.time) if callable(T_boundary[q]) else T_boundary[q] for q in range(4)]
+        E_bc_est = _boundary_energy_estimate(geometry, e1, e2, Tb, dt, boundary_source_func)
+        T = state.temperature
+        sig_h = sig.view(G, *reversed(like.shape)).transpose(1, 2).cpu().numpy()
+        b = planck_fractions(energy_edges, T)
+        sP = np.sum(sig_h * b, axis=0)
+        beta = 4.0 * __a * T ** 3 / np.broadcast_to(np.asarray(cv(T) if not getattr(cv, "_imc_device", False)
+                                                                 else state.grid(cvv).cpu().numpy()), T.shape)
+        f = np.clip(1.0 / (1.0 + theta * beta * sP * __c * dt), 0.0, 1.0)
+        vol = _cell_volumes(e1, e2, geometry)
+        ce = np.sum(sig_h * f * b, axis=0) * __a * __c * T ** 4 * dt * vol
+        if Ntotal_T_floor > 0.0:
+            ce = np.where(T > Ntotal_T_floor, ce, 0.0)
+        E_mat_est = float(np.sum(ce))
+        tot = E_bc_est + E_mat_est
+        frac_bc = E_bc_est / tot if tot > 0 else 0.5
+        fmin = float(np.clip(particle_budget_fmin, 0.0, 0.5))
+        frac_bc = float(np.clip(frac_bc, fmin, 1.0 - fmin))
+        Nboundary = int(round(Ntotal * frac_bc))
+        Ntarget = Ntotal - Nboundary
+    cache = state.__dict__.setdefault("_face_cache", {})
+    faces = face_temperatures(2, geometry, T_boundary, state.time, e1, e2, boundary_source_func, eng.device, cache)
+    refl = tuple(reflect) + (False,) * (4 - len(reflect))
+    t_eval = _time.perf_counter()
+    eng.transport_async(state._T, sig.reshape(-1).contiguous(), cvv, src, state.count, dt, theta, Ntarget, Nboundary,
+                        Nsource, faces, refl, max_events=max_events_per_particle, rz_linear_source=False,
+                        t_emit_floor=T_emit_floor)
+    world = 1
+    if _allreduce is not None:
+        world = _allreduce.get_world_size()
+        average_tallies(_allreduce, eng)
+    eng.material_update(state._e, state._Tr)
+    rad_pre = (eng.si.view(G, nc) / C_LIGHT).clone()  # radiation energy density by group (path length)
+    eng.comb_async(Nmax, state.count, state._e, per_group=True)
+    if conserve_comb_energy:
+        state._e.add_(eng.disc.view(G, nc).sum(0) / eng.vol)
+    Tn = evaluate(inv_eos, state.grid(state._e), lambda: _host_copy(state.grid(state._e)), like)
+    state._T.copy_(state.flat(Tn))
+    try:
+        sm = eng.fetch(state.host_copies())
+    except _lib.ImcError as ex:
+        if ex.status == 3:
+            raise AssertionError("non-finite or non-positive material state") from ex
+        raise
+    if not use_scalar_intensity_Tr:
+        pre = eng.spare
+        acc = torch.zeros(G * nc, dtype=torch.float64, device=eng.device)
+        w = pre.view("weight").double()
+        live = w > 0
+        acc.index_add_(0, (pre.view("cell").long() + nc * pre.view("group").long())[live], w[live])
+        rad_pre = acc.view(G, nc) / eng.vol.view(1, nc)
+        state._Tr.copy_(torch.pow(rad_pre.sum(0) / A_RAD, 0.25))
+        state.refresh_host()
+    else:
+        state.take_host_copies()
+    rad_post = _rad_by_group(eng)
+    internal = float(sm.internal_energy)
+    rad = float(sm.comb_after)
+    comb_disc = float(sm.comb_before) - rad
+    if conserve_comb_energy:
+        internal += comb_disc
+    boundary_emission = float(sum(sm.e_side))
+    boundary_loss = float(sum(sm.escaped))
+    if _allreduce is not None and world > 1:
+        t = torch.tensor([rad, comb_disc, boundary_loss], dtype=torch.float64, device=eng.device)
+        _allreduce.all_reduce(t)
+        rad, comb_disc, boundary_loss = (float(x) / world for x in t.cpu())
+    total = internal + rad
+    dE = total - state.previous_total_energy
+    residual = dE - boundary_emission + boundary_loss - float(sm.source_emission)
+    closure = residual + (0.0 if conserve_comb_energy else comb_disc)
+    state.time = state.time + dt
+    state.previous_total_energy = total
+    state.count += 1
+
+    def grid3(x):  # (G, nc) -> (G, nx, ny)
+        nx, ny = state._shape
+        return x.view(G, ny, nx).transpose(1, 2).cpu().numpy().copy()
+
+    rad_group_pre = grid3(rad_pre)
+    rad_group_post = grid3(rad_post)
+    object.__setattr__(state, "_rad_group", rad_pre)
+    state.__dict__["radiation_energy_by_group"] = rad_group_pre
+    state.__dict__["radiation_energy_by_group_postcomb"] = rad_group_post
+    stats = np.array(sm.stats[:], dtype=np.int64)
+    bnd_group = eng.boundary_group.cpu().numpy().copy()
+    esc_group = eng.escaped_group.cpu().numpy().copy()
+    ms_src, ms_tr = eng.phase_times()
+    t_end = _time.perf_counter()
+    n_tr = int(sm.n_bank)
+    ev = int(stats[_lib.STAT_EVENTS])
+    info = {
+        "time": state.time,
+        "temperature": state.temperature,
+        "radiation_temperature": state.radiation_temperature,
+        "radiation_energy_by_group": rad_group_pre,
+        "radiation_energy_by_group_postcomb": rad_group_post,
+        "N_particles": int(eng.bank.size),
+        "N_boundary": Nboundary,
+        "N_target": Ntarget,
+        "particle_budget_fmin": float(np.clip(particle_budget_fmin, 0.0, 0.5)),
+        "E_boundary_est": E_bc_est,
+        "E_material_est": E_mat_est,
+        "total_energy": total,
+        "total_internal_energy": internal,
+        "total_radiation_energy": rad,
+        "boundary_emission": boundary_emission,
+        "boundary_emission_by_group": bnd_group,
+        "boundary_emission_by_side": np.array(sm.e_side[:]),
+        "boundary_loss": boundary_loss,
+        "boundary_outgoing": boundary_loss,
+        "boundary_outgoing_by_group": esc_group,
+        "boundary_outgoing_by_side": np.array(sm.escaped[:]),
+        "source_emission": float(sm.source_emission),
+        "incoming_energy_total": boundary_emission + float(sm.source_emission),
+        "outgoing_energy_total": boundary_loss,
+        "dE_system": dE,
+        "energy_expected_dE": boundary_emission + float(sm.source_emission) - boundary_loss,
+        "energy_residual": residual,
+        "energy_loss": residual,
+        "Nmax_next": (min(Nmax + Nmax_growth, Nmax_final) if Nmax_final is not None else Nmax + Nmax_growth)
+        if Nmax_growth > 0 else Nmax,
+        "ledger": {"comb_discrepancy": comb_disc, "closure": closure,
+                   "relative_closure": closure / max(abs(total), 1e-300),
+                   "emission": float(sm.emission_total),
+                   "weight_floor": 1e-10 * float(sm.weight_sum) / max(n_tr, 1)},
+        "profiling": {
+            "phase_times_s": {
+                "sampling": (t_eval - t_step_start) + ms_src * 1e-3,
+                "transport": ms_tr * 1e-3,
+                "postprocess": max(t_end - t_eval - (ms_src + ms_tr) * 1e-3, 0.0),
+                "total": t_end - t_step_start,
+            },
+            "transport_events": {
+                "total": ev,
+                "boundary_crossings": int(stats[_lib.STAT_BOUNDARY]),
+                "absorption_continue_events": int(stats[_lib.STAT_SCATTER]),
+                "census_events": int(stats[_lib.STAT_CENSUS]),
+                "absorption_capture_events": 0,
+                "weight_floor_kills": int(stats[_lib.STAT_FLOOR]),
+                "reflections": int(stats[_lib.STAT_REFLECT]),
+                "event_cap_hits": int(stats[_lib.STAT_CAP]),
+                "avg_events_per_particle": ev / max(n_tr, 1),
+                "n_particles_transported": n_tr,
+            },
+        },
+    }
+    return state, info
+
+
+def run_simulation(Ntarget, Nboundary, Nsource, Nmax, Tinit, Tr_init, T_boundary, dt, edges1, edges2, energy_edges,
+                   sigma_a_funcs, eos, inv_eos, cv, source, final_time, reflect=(False, False, False, False),
+                   output_freq=1, theta=1.0, use_scalar_intensity_Tr=True, Ntarget_ic=None,
+                   conserve_comb_energy=False, geometry="xy", max_events_per_particle=1_000_000,
+                   emission_fractions=None, T_emit_floor=0.0, Nmax_growth=0, Nmax_final=None, seed=0x5EED0001):
+    state = init_simulation(Ntarget, Tinit, Tr_init, edges1, edges2, energy_edges, eos, inv_eos,
+                            Ntarget_ic=Ntarget_ic, T_emit_floor=T_emit_floor, geometry=geometry, seed=seed)
+    history = []
+    while state.time < final_time - 1e-15:
+        step_dt = min(dt, final_time - state.time)
+        state, info = step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, step_dt, edges1, edges2,
+                           energy_edges, sigma_a_funcs, inv_eos, cv, source, reflect=reflect, theta=theta,
+                           use_scalar_intensity_Tr=use_scalar_intensity_Tr, conserve_comb_energy=conserve_comb_energy,
+                           geometry=geometry, max_events_per_particle=max_events_per_particle,
+                           emission_fractions=emission_fractions, T_emit_floor=T_emit_floor,
+                           Nmax_growth=Nmax_growth, Nmax_final=Nmax_final)
+        Nmax = info["Nmax_next"]
+        if (state.count - 1) % output_freq == 0 or (final_time - state.time) < 1e-12:
+            history.append(info)
+    return history, state
+
+
+def tune(state, grid=None, repeats=2):
+    from ._gray import tune as _tune
+
+    return _tune(state, grid=grid, repeats=repeats)

@@ -13,7 +13,9 @@ RADTRANBOOK_REF); the fixtures it writes are small .npz files committed with thi
                  IMC/IMC2D.py:1293 _solve_r_linear_cdf
   sources.npz    per-cell counts and weights of IMC/IMC1D.py:251 emitted_particles and
                  IMC/IMC2D.py:1326 _sample_source_rz_linear (the deterministic part of sampling)
-  stats_*.npz    multi-seed statistics of whole reference steps (IMC1D.step, IMC2D.step):
+  planck.npz     MG_IMC/MG_IMC2D.py:202 Planck (mixture-of-Gammas) group sampler, with its draws
+  stats_*.npz    multi-seed statistics of whole reference steps (IMC1D.step, IMC2D.step,
+                 MG_IMC2D.step with planck_shim/ standing in for the external planck_integrals):
                  per-cell mean and standard error of material and radiation temperature
 
 The reference's random numbers cannot be reproduced by a different generator, so whole-step
@@ -267,6 +269,62 @@ def run_stats_rz(IMC2D, seeds=16, steps=3):
                 Tr_se=Trs.std(0, ddof=1) / np.sqrt(seeds), seeds=seeds, steps=steps, nr=nr, nz=nz)
 
 
+MG = dict(nx=40, L=0.5, G=10, cv=0.3, T0=0.001, dt=0.005, steps=3, Ntarget=4000, Nboundary=2000, Nmax=12000)
+
+
+def mg_setup():
+    edges = np.logspace(-4, np.log10(20.0), MG["G"] + 1)
+    nu = 0.5 * (edges[:-1] + edges[1:])
+    funcs = [(lambda T, n=n: np.clip(10.0 * n ** -3 * np.power(T, -0.5), 1e-2, 1e6)) for n in nu]
+    return edges, nu, funcs
+
+
+def load_reference_mg():
+    sys.path.insert(0, os.path.join(HERE, "planck_shim"))
+    sys.path.insert(0, os.path.join(REF, "MG_IMC"))
+    import MG_IMC2D  # noqa: E402
+    assert MG_IMC2D._PLANCK_AVAILABLE, "planck_integrals stand-in not found"
+    return MG_IMC2D
+
+
+def gen_planck_sampler(MG_IMC2D, n=3000, seed=17):
+    _, seed_np, _, draw_np = nb_helpers()
+    rng = np.random.default_rng(seed)
+    edges = np.logspace(-4, np.log10(20.0), 11)
+    rows, res = [], []
+    for q in range(40):
+        T = 10 ** rng.uniform(-3, 0.5)
+        seed_np(300 + q)
+        u = draw_np(5 * 50).reshape(50, 5)
+        seed_np(300 + q)
+        _, g = MG_IMC2D._sample_planck_spectrum_mixture_of_gammas_jit(50, T, edges[:-1], edges[1:],
+                                                                       MG_IMC2D._PLANCK_MIXTURE_CDF)
+        for k in range(50):
+            rows.append([T] + list(u[k])); res.append(g[k])
+    return dict(planck_in=np.array(rows), planck_group=np.array(res), planck_edges=edges)
+
+
+def run_stats_mg(MG_IMC2D, seeds=16):
+    edges, nu, funcs = mg_setup()
+    nx = MG["nx"]
+    x_e = np.linspace(0, MG["L"], nx + 1); y_e = np.array([0.0, 1.0])
+    cv = MG["cv"]
+    seed_py, seed_np, _, _ = nb_helpers()
+    Ts, Trs = [], []
+    for s in range(seeds):
+        np.random.seed(s); random.seed(s); seed_py(s); seed_np(s)
+        st = MG_IMC2D.init_simulation(MG["Ntarget"], np.full((nx, 1), MG["T0"]), np.full((nx, 1), MG["T0"]), x_e, y_e,
+                                      edges, lambda T: cv * T, lambda e: e / cv, geometry="xy")
+        for _ in range(MG["steps"]):
+            st, info = MG_IMC2D.step(st, MG["Ntarget"], MG["Nboundary"], 0, MG["Nmax"], (1.0, 0.0, 0.0, 0.0), MG["dt"],
+                                     x_e, y_e, edges, funcs, lambda e: e / cv, lambda T: cv + 0 * T,
+                                     np.zeros((nx, 1)), reflect=(False, False, True, True), geometry="xy")
+        Ts.append(st.temperature[:, 0].copy()); Trs.append(st.radiation_temperature[:, 0].copy())
+    Ts, Trs = np.array(Ts), np.array(Trs)
+    return dict(T_mean=Ts.mean(0), T_se=Ts.std(0, ddof=1) / np.sqrt(seeds), Tr_mean=Trs.mean(0),
+                Tr_se=Trs.std(0, ddof=1) / np.sqrt(seeds), seeds=seeds, **MG)
+
+
 def main():
     t0 = time.time()
     IMC1D, IMC2D = load_reference()
@@ -292,6 +350,15 @@ def main():
             s2 = run_stats_rz(IMC2D)
         np.savez_compressed(os.path.join(HERE, "stats_rz.npz"), **s2)
         print(f"rz statistics written ({time.time() - t0:.1f} s)")
+    MG_IMC2D = load_reference_mg()
+    with contextlib.redirect_stdout(io.StringIO()):
+        pl = gen_planck_sampler(MG_IMC2D)
+    np.savez_compressed(os.path.join(HERE, "planck.npz"), **pl)
+    if "--no-stats" not in sys.argv and "--no-mg-stats" not in sys.argv:
+        with contextlib.redirect_stdout(io.StringIO()):
+            s3 = run_stats_mg(MG_IMC2D)
+        np.savez_compressed(os.path.join(HERE, "stats_mg.npz"), **s3)
+        print(f"multigroup statistics written ({time.time() - t0:.1f} s)")
 
 
 if __name__ == "__main__":
