@@ -197,6 +197,27 @@ IMC_API imc_status imc_comb(const imc_mesh* mesh, const imc_bank* in, imc_bank* 
                     void* workspace, size_t workspace_bytes, imc_comb_report* report,
                     void* stream);
 
+/* imc_comb without a workspace argument.  No reference counterpart: the reference combs
+ * NumPy arrays and has no device scratch to provide.
+ *
+ * For callers that cannot allocate device memory, e.g. a C or Fortran host that links only
+ * this library and the CUDA runtime and owns no device allocator, or code that must not
+ * change the device's memory map.  Scratch is a fixed array of IMC_NOALLOC_SCRATCH_BYTES
+ * compiled into the library, one per device; this call allocates and frees nothing.
+ *   - Limit: imc_workspace_bytes(mesh, in->size) must be <= IMC_NOALLOC_SCRATCH_BYTES
+ *     (8 MiB; e.g. a 60 x 210 gray mesh with up to about 1.5 million entries in `in`).
+ *     Larger inputs return IMC_ERR_WORKSPACE without launching anything.
+ *   - The first call on a device, made with that device current, looks up the array's
+ *     device address; make that first call before any stream capture.
+ *   - The array is shared by every call on the device: calls that overlap in time (other
+ *     host threads, or work still running on another stream) race on it.
+ * Inputs, outputs and report are those of imc_comb; the stream is synchronised. */
+#define IMC_NOALLOC_SCRATCH_BYTES ((size_t)8 << 20)
+IMC_API imc_status imc_comb_noalloc(const imc_mesh* mesh, const imc_bank* in, imc_bank* out,
+                                    int64_t n_max, uint64_t seed, uint32_t step,
+                                    int32_t per_group, double* disc,
+                                    imc_comb_report* report, void* stream);
+
 /* Asynchronous forms.  Nothing is synchronised and no size is returned to the host:
  * imc_step_transport_async reads summary->n_census (set it to the bank's live size),
  * requires bank->capacity >= n_census + imc_source_bound(...), and writes the source

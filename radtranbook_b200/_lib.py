@@ -114,6 +114,8 @@ SIGNATURES = {
     "imc_material_update": (c_int, [POINTER(ImcMesh), POINTER(ImcTallies), c_void_p, c_void_p, c_void_p]),
     "imc_comb": (c_int, [POINTER(ImcMesh), POINTER(ImcBank), POINTER(ImcBank), c_int64, c_uint64, c_uint32,
                          c_int32, c_void_p, c_void_p, c_size_t, POINTER(ImcCombReport), c_void_p]),
+    "imc_comb_noalloc": (c_int, [POINTER(ImcMesh), POINTER(ImcBank), POINTER(ImcBank), c_int64, c_uint64,
+                                 c_uint32, c_int32, c_void_p, POINTER(ImcCombReport), c_void_p]),
     "imc_source_bound": (c_int64, [POINTER(ImcMesh), POINTER(ImcStepParams)]),
     "imc_step_transport_async": (c_int, [POINTER(ImcMesh), POINTER(ImcMaterial), POINTER(ImcStepParams),
                                          POINTER(ImcBank), POINTER(ImcTallies), c_void_p, c_size_t, c_void_p,

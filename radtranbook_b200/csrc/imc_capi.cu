@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cstddef>
 #include <cstring>
+#include <mutex>
 #include "imc_device.cuh"
 #include "imc_internal.h"
 
@@ -329,6 +330,37 @@ WsLayout imc_ws_layout(const imc_mesh* m, int64_t capacity) {
   return L;
 }
 
+// ---- library-owned comb scratch (imc_comb_noalloc) ----
+// A caller that owns no device allocator cannot provide a workspace, so this entry point
+// carves its scratch from a fixed array linked into the library.  The array is a module
+// global: the runtime creates one per device when the module is loaded there, which
+// happens at the latest on the first cudaGetSymbolAddress with that device current.
+namespace {
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[IMC_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of this device's scratch array, looked up once per device.
+imc_status noalloc_scratch(void** ptr) {
+  int dev = -1;
+  IMC_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return IMC_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    IMC_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    if (!p) return IMC_ERR_CUDA;
+    g_noalloc_ptr[dev] = p;
+  }
+  *ptr = g_noalloc_ptr[dev];
+  return IMC_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 size_t imc_workspace_bytes(const imc_mesh* mesh, int64_t bank_capacity) {
@@ -503,6 +535,42 @@ imc_status imc_comb(const imc_mesh* mesh, const imc_bank* in, imc_bank* out, int
   IMC_CUDA(cudaMemsetAsync(&sum->flags, 0, sizeof(int), s));
   IMC_CUDA(cudaMemcpyAsync(&sum->n_bank, &n_in, sizeof(n_in), cudaMemcpyHostToDevice, s));
   st = comb_async(mesh, in, out, n_max, seed, step, per_group, disc, nullptr, workspace, workspace_bytes, sum, s);
+  if (st != IMC_OK) return st;
+  imc_step_summary h;
+  IMC_CUDA(cudaMemcpyAsync(&h, sum, sizeof(h), cudaMemcpyDeviceToHost, s));
+  IMC_CUDA(cudaStreamSynchronize(s));
+  report->required_capacity = h.n_out;
+  report->energy_before = h.comb_before;
+  report->energy_after = h.comb_after;
+  if (h.flags & IMC_FLAG_COMB_OVERFLOW) return IMC_ERR_BANK_OVERFLOW;
+  out->size = h.n_out;
+  report->n_out = h.n_out;
+  return IMC_OK;
+}
+
+imc_status imc_comb_noalloc(const imc_mesh* mesh, const imc_bank* in, imc_bank* out, int64_t n_max,
+                            uint64_t seed, uint32_t step, int32_t per_group, double* disc,
+                            imc_comb_report* report, void* stream) {
+  if (!report || !mesh || !in || !out) return IMC_ERR_INVALID_ARG;
+  std::memset(report, 0, sizeof(*report));
+  imc_status st = check_mesh(mesh);
+  if (st != IMC_OK) return st;
+  if (in->size < 0) return IMC_ERR_INVALID_ARG;
+  const WsLayout L = imc_ws_layout(mesh, in->size);
+  if (L.total > IMC_NOALLOC_SCRATCH_BYTES) return IMC_ERR_WORKSPACE;
+  void* scratch = nullptr;
+  st = noalloc_scratch(&scratch);
+  if (st != IMC_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  report->n_in = in->size;
+  // The array outlives every call: clear the whole summary (flags, counters, energies) so
+  // nothing from an earlier call is read.  The comb clears its own bin accumulators.
+  imc_step_summary* sum = internal_summary(scratch, L);
+  IMC_CUDA(cudaMemsetAsync(sum, 0, sizeof(*sum), s));
+  long long n_in = in->size;
+  IMC_CUDA(cudaMemcpyAsync(&sum->n_bank, &n_in, sizeof(n_in), cudaMemcpyHostToDevice, s));
+  st = comb_async(mesh, in, out, n_max, seed, step, per_group, disc, nullptr, scratch, IMC_NOALLOC_SCRATCH_BYTES,
+                  sum, s);
   if (st != IMC_OK) return st;
   imc_step_summary h;
   IMC_CUDA(cudaMemcpyAsync(&h, sum, sizeof(h), cudaMemcpyDeviceToHost, s));
