@@ -257,6 +257,99 @@ IMC_API int imc_last_cuda_error(void);
 /* number of kernels this library launched since load (diagnostic) */
 IMC_API unsigned long long imc_kernel_launches(void);
 
+/* ------------------------------------------------------------------------------------
+ * Batched independent 1-D gray slab problems.
+ *
+ * Replaces a host loop of IMC/IMC1D.py:908 step(..., geometry='slab') over independent
+ * problems.  Instance k is a slab of nc_k cells with
+ *   sigma_a(T) = opacity_a[k] * T^opacity_p[k], constant cv[k] (e = cv T),
+ *   boundary temperature face_T[2k + side] on the left (side 0) / right (side 1) face
+ *   (<= 0: no source), reflect bit mask (bit 0 left, bit 1 right),
+ *   n_target[k] emission and n_boundary[k] boundary particles per source face per step,
+ *   comb target n_max[k] and Philox key seed[k].
+ * Instance k's particles draw the same random numbers, in the same bank order, as a
+ * single-problem run of imc_step_transport / imc_comb with seed[k] (census | left face |
+ * right face | emission), so each instance reproduces that run.
+ *
+ * One imc_batch_step is a fixed sequence of kernels over all instances: sources, the
+ * persistent tracking kernel (one work queue over every instance's histories), the fused
+ * material + Fleck update, the per-cell comb and a per-instance energy ledger.  It reads
+ * every count from device memory, synchronises nothing and allocates nothing, so the
+ * caller may capture it in a CUDA graph and replay the graph once per step.
+ * ------------------------------------------------------------------------------------ */
+typedef struct imc_batch {
+  int32_t n_inst;               /* K */
+  int32_t n_cells;              /* sum of nc_k */
+  int64_t n_slots;              /* bank slots per bank = slot_off[K] (host copy) */
+  int64_t max_new;              /* host bound: sum over k of the new particles of one step,
+                                   sides_k * n_boundary[k] + n_target[k] + nc_k */
+  double dt, theta;
+  const int32_t* cell_off;      /* [K+1] instance k owns cells [cell_off[k], cell_off[k+1]) */
+  const double* edges;          /* [n_cells + K] instance k's nc_k+1 edges start at cell_off[k]+k */
+  const int64_t* slot_off;      /* [K+1] bank slots of instance k */
+  const uint64_t* seed;         /* [K] */
+  const int64_t* n_target;      /* [K] */
+  const int64_t* n_boundary;    /* [K] */
+  const int64_t* n_max;         /* [K] */
+  const double* face_T;         /* [2K] */
+  const int32_t* reflect;       /* [K] */
+  const double* opacity_a;      /* [K] */
+  const double* opacity_p;      /* [K] */
+  const double* cv;             /* [K] */
+} imc_batch;
+
+/* per-instance energy ledger of the last step (FP64), ledger[k * IMC_BL_N + field] */
+enum {
+  IMC_BL_TOTAL = 0,      /* internal + radiation after the comb */
+  IMC_BL_PREV = 1,       /* the same at the start of the step */
+  IMC_BL_INTERNAL = 2,
+  IMC_BL_RADIATION = 3,  /* census energy after the comb */
+  IMC_BL_BOUNDARY = 4,   /* boundary energy issued */
+  IMC_BL_ESCAPED = 5,
+  IMC_BL_EMISSION = 6,   /* emission energy issued */
+  IMC_BL_COMB_DISC = 7,  /* census energy before - after the comb */
+  IMC_BL_CLOSURE = 8,    /* TOTAL - PREV - BOUNDARY + ESCAPED + COMB_DISC */
+  IMC_BL_MAX_REL = 9,    /* max over steps of |CLOSURE| / TOTAL */
+  IMC_BL_EVENTS = 10,    /* track segments of this instance, accumulated over steps */
+  IMC_BL_N = 11
+};
+
+typedef struct imc_batch_state {   /* device memory, caller-owned */
+  imc_bank bank[2];             /* 1-D banks (pos1, dir1, weight, time, cell), n_slots each */
+  int32_t* sel;                 /* [1] the bank that holds the census */
+  uint32_t* step;               /* [1] step index (Philox counter word 2) */
+  int64_t* n_census;            /* [K] census entries of instance k, at its first slot */
+  double* T;                    /* [n_cells] material temperature */
+  double* e;                    /* [n_cells] internal energy density */
+  double* tr;                   /* [n_cells] radiation temperature */
+  double* dep;                  /* [n_cells] deposition of the last step */
+  double* si;                   /* [n_cells] path-length intensity of the last step */
+  double* emitted;              /* [n_cells] emission issued in the last step */
+  double* ledger;               /* [K * IMC_BL_N] */
+  unsigned long long* stats;    /* [IMC_STAT_N], accumulated over steps */
+  int32_t* flags;               /* [1] IMC_FLAG_* (sticky; the caller clears it) */
+} imc_batch_state;
+
+typedef struct imc_batch_launch {  /* tracking kernel shape; 0 = default */
+  int32_t block_size;
+  int32_t blocks_per_sm;
+  int32_t chunk;                /* histories per work-queue ticket (at most) */
+  int32_t refill_min;           /* idle lanes a warp waits for before it refills (1..32) */
+} imc_batch_launch;
+
+IMC_API size_t imc_batch_workspace_bytes(const imc_batch* b);
+/* T = T0, e = cv T0, equilibrium initial census of n_target[k] particles at Tr0
+ * (IMC/IMC1D.py:220-248), ledger PREV, step = 0, sel = 0, stats and flags cleared, and
+ * the Fleck tables of the first step.  Synchronises the stream. */
+IMC_API imc_status imc_batch_init(const imc_batch* b, imc_batch_state* s, const double* T0,
+                                  const double* Tr0, void* workspace, size_t workspace_bytes,
+                                  void* stream);
+/* One time step of every instance, asynchronous (see above).  Errors found on the device
+ * (non-finite material state, a bank slot overflow) set bits in *s->flags. */
+IMC_API imc_status imc_batch_step(const imc_batch* b, imc_batch_state* s,
+                                  const imc_batch_launch* launch, void* workspace,
+                                  size_t workspace_bytes, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

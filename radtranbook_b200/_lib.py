@@ -104,6 +104,29 @@ class ImcStepSummary(ctypes.Structure):
 
 
 # name -> (restype, argtypes); every symbol declared in include/imcb200.h
+# batched 1-D slab problems
+(BL_TOTAL, BL_PREV, BL_INTERNAL, BL_RADIATION, BL_BOUNDARY, BL_ESCAPED, BL_EMISSION, BL_COMB_DISC, BL_CLOSURE,
+ BL_MAX_REL, BL_EVENTS, BL_N) = range(12)
+
+
+class ImcBatch(ctypes.Structure):
+    _fields_ = [("n_inst", c_int32), ("n_cells", c_int32), ("n_slots", c_int64), ("max_new", c_int64),
+                ("dt", c_double), ("theta", c_double),
+                ("cell_off", c_void_p), ("edges", c_void_p), ("slot_off", c_void_p), ("seed", c_void_p),
+                ("n_target", c_void_p), ("n_boundary", c_void_p), ("n_max", c_void_p), ("face_T", c_void_p),
+                ("reflect", c_void_p), ("opacity_a", c_void_p), ("opacity_p", c_void_p), ("cv", c_void_p)]
+
+
+class ImcBatchState(ctypes.Structure):
+    _fields_ = [("bank", ImcBank * 2), ("sel", c_void_p), ("step", c_void_p), ("n_census", c_void_p),
+                ("T", c_void_p), ("e", c_void_p), ("tr", c_void_p), ("dep", c_void_p), ("si", c_void_p),
+                ("emitted", c_void_p), ("ledger", c_void_p), ("stats", c_void_p), ("flags", c_void_p)]
+
+
+class ImcBatchLaunch(ctypes.Structure):
+    _fields_ = [("block_size", c_int32), ("blocks_per_sm", c_int32), ("chunk", c_int32), ("refill_min", c_int32)]
+
+
 SIGNATURES = {
     "imc_workspace_bytes": (c_size_t, [POINTER(ImcMesh), c_int64]),
     "imc_init_census": (c_int, [POINTER(ImcMesh), c_void_p, c_int64, c_double, c_uint64, POINTER(ImcBank),
@@ -116,6 +139,11 @@ SIGNATURES = {
                          c_int32, c_void_p, c_void_p, c_size_t, POINTER(ImcCombReport), c_void_p]),
     "imc_comb_noalloc": (c_int, [POINTER(ImcMesh), POINTER(ImcBank), POINTER(ImcBank), c_int64, c_uint64,
                                  c_uint32, c_int32, c_void_p, POINTER(ImcCombReport), c_void_p]),
+    "imc_batch_workspace_bytes": (c_size_t, [POINTER(ImcBatch)]),
+    "imc_batch_init": (c_int, [POINTER(ImcBatch), POINTER(ImcBatchState), c_void_p, c_void_p, c_void_p, c_size_t,
+                               c_void_p]),
+    "imc_batch_step": (c_int, [POINTER(ImcBatch), POINTER(ImcBatchState), POINTER(ImcBatchLaunch), c_void_p, c_size_t,
+                               c_void_p]),
     "imc_source_bound": (c_int64, [POINTER(ImcMesh), POINTER(ImcStepParams)]),
     "imc_step_transport_async": (c_int, [POINTER(ImcMesh), POINTER(ImcMaterial), POINTER(ImcStepParams),
                                          POINTER(ImcBank), POINTER(ImcTallies), c_void_p, c_size_t, c_void_p,

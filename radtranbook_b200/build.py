@@ -18,9 +18,10 @@ LIB = HERE / "libimcb200.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden"]
-PER_FILE = {"imc_bookkeeping.cu": ["-fmad=false"]}
-SOURCES = ["imc_capi.cu", "imc_bookkeeping.cu", "imc_source.cu", "imc_transport.cu", "imc_comb.cu"]
-HEADERS = ["imc_device.cuh", "imc_internal.h"]
+PER_FILE = {"imc_bookkeeping.cu": ["-fmad=false"], "imc_batch_plan.cu": ["-fmad=false"]}
+SOURCES = ["imc_capi.cu", "imc_bookkeeping.cu", "imc_source.cu", "imc_transport.cu", "imc_comb.cu",
+           "imc_batch.cu", "imc_batch_plan.cu"]
+HEADERS = ["imc_device.cuh", "imc_internal.h", "imc_block.cuh", "imc_sample.cuh", "imc_batch.h"]
 
 
 def nvcc() -> str:

@@ -1,0 +1,80 @@
+// imc_block.cuh — single-block FP64 building blocks shared by the per-problem planning
+// kernels (one 1024-thread block per problem): the canonical summation order, the count
+// scan and the volume-source plan.  Files that include this are compiled without FMA
+// contraction, so the numbers match the CPU oracle's (canon_sum, ceil counts) exactly.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace imcblk {
+
+constexpr int NT = 1024;
+
+__device__ __forceinline__ double pow4(double T) { const double t2 = T * T; return t2 * t2; }
+__device__ __forceinline__ double pow3(double T) { return T * T * T; }
+
+// 1024 strided partial sums, then a halving tree (the oracle's canon_sum).
+__device__ inline double block_canon_sum(const double* x, long long n, double* red) {
+  const int t = threadIdx.x;
+  double s = 0.0;
+  for (long long i = t; i < n; i += NT) s += x[i];
+  red[t] = s;
+  __syncthreads();
+  for (int h = NT / 2; h >= 1; h >>= 1) {
+    if (t < h) red[t] += red[t + h];
+    __syncthreads();
+  }
+  const double r = red[0];
+  __syncthreads();
+  return r;
+}
+
+// Exclusive scan of per-order-position counts n[0..m) into off[0..m]; returns the total.
+__device__ inline long long block_scan_counts(const long long* n, long long* off, int m, long long* sh) {
+  const int t = threadIdx.x;
+  const int per = (m + NT - 1) / NT;
+  const int lo = min(t * per, m), hi = min(lo + per, m);
+  long long s = 0;
+  for (int o = lo; o < hi; ++o) s += n[o];
+  sh[t] = s;
+  __syncthreads();
+  // Hillis-Steele inclusive scan of the 1024 thread totals
+  for (int d = 1; d < NT; d <<= 1) {
+    const long long v = (t >= d) ? sh[t - d] : 0;
+    __syncthreads();
+    sh[t] += v;
+    __syncthreads();
+  }
+  long long run = sh[t] - s;  // exclusive
+  for (int o = lo; o < hi; ++o) { off[o] = run; run += n[o]; }
+  const long long total = sh[NT - 1];
+  if (t == 0) off[m] = total;
+  __syncthreads();
+  return total;
+}
+
+// order position o = i*ny + j (the reference's i-outer, j-inner source loops)
+__device__ __forceinline__ int order_to_cell(int o, int nx, int ny) {
+  const int i = o / ny, j = o - (o / ny) * ny;
+  return i + nx * j;
+}
+
+// Volume-source counts (ceil(N QV_c / Q), in source order), per-cell weights and the
+// energy actually issued per cell (n_c times the FP32 weight, exact in FP64).
+__device__ inline long long plan_volume(const double* QV, long long N, int nx, int ny, int nc, long long* cnt,
+                                 long long* off, float* w, double* issued, double* red, long long* sh) {
+  const double Qt = block_canon_sum(QV, nc, red);
+  for (int o = threadIdx.x; o < nc; o += NT) {
+    const int c = order_to_cell(o, nx, ny);
+    long long n = 0;
+    if (Qt > 0.0 && N > 0) n = (long long)ceil((double)N * QV[c] / Qt);
+    cnt[o] = n;
+    const float wc = n > 0 ? (float)(QV[c] / (double)n) : 0.f;
+    w[c] = wc;
+    issued[c] = (double)n * (double)wc;
+  }
+  __syncthreads();
+  return block_scan_counts(cnt, off, nc, sh);
+}
+
+}  // namespace imcblk

@@ -303,6 +303,8 @@ imc_step_summary* internal_summary(void* workspace, const WsLayout& L) {
 
 }  // namespace
 
+void imc_note_cuda_error(int e) { g_last_cuda = e; }
+
 WsLayout imc_ws_layout(const imc_mesh* m, int64_t capacity) {
   WsLayout L{};
   size_t o = 0;
