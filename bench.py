@@ -174,6 +174,7 @@ def _gpu_steps(p, state, steps, use_device, dist=None):
     cv = p["cv_dev"] if use_device else p["cv_host"]
     inv = p["inv_eos_dev"] if use_device else p["inv_eos_host"]
     seg = hist = 0
+    info = None
     for _ in range(steps):
         state, info = imc2d.step(state, p["Ntarget"], p["Nboundary"], 0, p["Nmax"], p["T_boundary"], p["dt"],
                                  p["edges1"], p["edges2"], sig, inv, cv, p["source"], reflect=p["reflect"],
@@ -182,7 +183,11 @@ def _gpu_steps(p, state, steps, use_device, dist=None):
         te = info["profiling"]["transport_events"]
         seg += te["total"]
         hist += te["n_particles_transported"]
+        CLOSURE[0] = max(CLOSURE[0], abs(info["ledger"]["relative_closure"]))
     return state, seg, hist, info
+
+
+CLOSURE = [0.0]  # worst |energy closure| / total energy over the steps run
 
 
 def run_ours(args, rank: int, world: int):
@@ -225,6 +230,7 @@ def run_ours(args, rank: int, world: int):
     s0 = torch.cuda.Event(enable_timing=True)
     s1 = torch.cuda.Event(enable_timing=True)
     launches0 = lib.imc_kernel_launches()
+    CLOSURE[0] = 0.0
     track_ms = []
     segs_per_step = []
     clocks = ClockSampler(dev.index)
@@ -312,6 +318,7 @@ def run_ours(args, rank: int, world: int):
         "segments_per_step": seg_all / args.steps,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
+        "energy_closure_max_rel": CLOSURE[0],
         "roofline": roof,
         "cpu_baseline": cpu,
         "clocks": clocks.summary(),

@@ -159,6 +159,7 @@ __global__ void __launch_bounds__(256) k_btrack(BatchArgs a) {
   int k = 0, cb = 0, eb = 0, nc = 0, rmask = 0, ci = 0;
   uint64_t seed = 0;
   float wfloor = 0.f, x = 0.f, u = 0.f, w = 0.f, dcen = 0.f;
+  double inv_q = 0.0;  // the instance's fixed-point energy quantum, inverted
   double acc_lost = 0.0, acc_wd = 0.0;
   unsigned s_bd = 0, s_sc = 0;
 
@@ -195,7 +196,9 @@ __global__ void __launch_bounds__(256) k_btrack(BatchArgs a) {
             cb = a.cell_off[k]; nc = a.cell_off[k + 1] - cb; eb = cb + k;
             rmask = a.reflect[k]; seed = a.seed[k];
             const long long nb = a.n_bank[k];
-            wfloor = (float)(1e-10 * a.wsum[k] / (double)(nb > 0 ? nb : 1));
+            const double W = a.wsum[k];
+            wfloor = (float)(1e-10 * W / (double)(nb > 0 ? nb : 1));
+            inv_q = fx_inv_quantum(W);
             ev = 0;
             has = true;
           }
@@ -264,7 +267,7 @@ __global__ void __launch_bounds__(256) k_btrack(BatchArgs a) {
               ni = side == 0 ? 0 : nc - 1;
               atomicAdd(&blk_cnt[B_REFLECT], 1u);
             } else {
-              atomicAdd(a.esc + 2 * k + side, (double)w);
+              atomicAdd(a.esc_fx + 2 * k + side, fx_units((double)w, inv_q));
               atomicAdd(&blk_cnt[B_ESCAPE], 1u);
               w = 0.f;
               finished = true;
@@ -279,7 +282,7 @@ __global__ void __launch_bounds__(256) k_btrack(BatchArgs a) {
           const int c2 = cb + ci;
           const double2 cf = __ldg(a.cellf + c2);
           const double rem = (double)w;
-          atomicAdd(a.dep + c2, rem * cf.x);
+          atomicAdd(a.dep_fx + c2, fx_units(rem, inv_q));
           if (cf.y > 0.0) atomicAdd(a.si + c2, rem * cf.y);
           w = 0.f;
           finished = true;
@@ -297,13 +300,14 @@ __global__ void __launch_bounds__(256) k_btrack(BatchArgs a) {
         has = false;
       }
     }
-    double vd = 0.0, vs = 0.0;
+    unsigned long long ud = 0ull;
+    double vs = 0.0;
     if (flush) {
       const double2 cf = __ldg(a.cellf + flush_cell);
-      vd = f_lost * cf.x;
+      ud = fx_units(f_lost, inv_q);  // lanes of one cell share its instance's quantum
       vs = cf.y > 0.0 ? f_lost * cf.y : -f_wd * cf.y;
     }
-    warp_tally2(flush, flush_cell, vd, vs, a.dep, a.si, st);
+    warp_tally_fx(flush, flush_cell, ud, vs, a.dep_fx, a.si, st);
   }
 
   const unsigned long long t_bd = warp_sum_u(s_bd), t_sc = warp_sum_u(s_sc);
@@ -571,7 +575,7 @@ inline size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
 
 struct BatchLayout {
   size_t cell_inst, ef, vol, sass, cellf, emit_E, emit_n, emit_off, emit_w, tilt, ecen, ew, ncopy;
-  size_t n_side, w_side, n_bank, n_new, census_cap, live_pref, new_pref, inst_pref, copies_d, wsum, esc;
+  size_t n_side, w_side, n_bank, n_new, census_cap, live_pref, new_pref, inst_pref, copies_d, wsum, esc_fx, dep_fx;
   size_t comb_after, e_side, e_emit, comb_before, cnt, blk, queue, total;
   long long max_tiles;
 };
@@ -588,7 +592,7 @@ BatchLayout batch_layout(const imc_batch* b) {
   L.ecen = take(8 * nc); L.ew = take(8 * nc); L.ncopy = take(8 * nc);
   L.n_side = take(8 * 2 * K); L.w_side = take(4 * 2 * K); L.n_bank = take(8 * K); L.n_new = take(8 * K);
   L.census_cap = take(8 * K); L.live_pref = take(8 * (K + 1)); L.new_pref = take(8 * (K + 1));
-  L.inst_pref = take(8 * (K + 1)); L.copies_d = take(8 * K); L.wsum = take(8 * K); L.esc = take(8 * 2 * K);
+  L.inst_pref = take(8 * (K + 1)); L.copies_d = take(8 * K); L.wsum = take(8 * K); L.esc_fx = take(8 * 2 * K); L.dep_fx = take(8 * nc);
   L.comb_after = take(8 * K); L.e_side = take(8 * 2 * K); L.e_emit = take(8 * K); L.comb_before = take(8 * K);
   L.cnt = take(4 * ns); L.blk = take(8 * ((size_t)L.max_tiles + 1)); L.queue = take(8);
   L.total = o;
@@ -621,7 +625,8 @@ BatchArgs make_args(const imc_batch* b, const imc_batch_state* s, void* ws, cons
   a.n_bank = wp<long long>(ws, L.n_bank); a.n_new = wp<long long>(ws, L.n_new);
   a.census_cap = wp<long long>(ws, L.census_cap); a.live_pref = wp<long long>(ws, L.live_pref);
   a.new_pref = wp<long long>(ws, L.new_pref); a.inst_pref = wp<long long>(ws, L.inst_pref);
-  a.copies_d = wp<double>(ws, L.copies_d); a.wsum = wp<double>(ws, L.wsum); a.esc = wp<double>(ws, L.esc);
+  a.copies_d = wp<double>(ws, L.copies_d); a.wsum = wp<double>(ws, L.wsum);
+  a.esc_fx = wp<unsigned long long>(ws, L.esc_fx); a.dep_fx = wp<unsigned long long>(ws, L.dep_fx);
   a.comb_after = wp<double>(ws, L.comb_after); a.e_side = wp<double>(ws, L.e_side);
   a.e_emit = wp<double>(ws, L.e_emit); a.comb_before = wp<double>(ws, L.comb_before);
   a.cnt = wp<int>(ws, L.cnt); a.blk = wp<long long>(ws, L.blk); a.queue = wp<unsigned long long>(ws, L.queue);

@@ -45,7 +45,8 @@ struct BatchArgs {
   long long* inst_pref;  // [K+1] exclusive prefix of comb copies per instance
   double* copies_d;      // [K] comb copies per instance (exact in FP64)
   double* wsum;          // [K]
-  double* esc;           // [2K]
+  unsigned long long* esc_fx;  // [2K] escaped energy, fixed point (units of wsum * 2^-60)
+  unsigned long long* dep_fx;  // [n_cells] deposited energy, fixed point
   double* comb_after;    // [K]
   double* e_side;        // [2K]
   double* e_emit;        // [K]

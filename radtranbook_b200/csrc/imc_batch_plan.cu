@@ -60,7 +60,10 @@ __global__ void k_bmaterial_fleck(BatchArgs a, int update) {
   const double cv = a.cv[k];
   double T;
   if (update) {
-    const double e = a.e[c] + a.dep[c] - a.emitted[c] / V;
+    // deposition of the step from its fixed-point sum (units of wsum * 2^-60)
+    const double dep = fx_energy(a.dep_fx[c], a.wsum[k]) * (1.0 / V);  // as the single-problem finalize
+    a.dep[c] = dep;
+    const double e = a.e[c] + dep - a.emitted[c] / V;
     a.e[c] = e;
     const double x = a.si[c] / A_RAD / C_LIGHT;
     a.tr[c] = x > 0.0 ? sqrt(sqrt(x)) : 0.0;
@@ -93,7 +96,7 @@ __global__ void __launch_bounds__(NT) k_bplan(BatchArgs a) {
   const double* e1 = a.edges + cb + k;
   const double* T = a.T + cb;
   for (int c = t; c < nc; c += NT) {
-    a.dep[cb + c] = 0.0; a.si[cb + c] = 0.0; a.ecen[cb + c] = 0.0; a.ncopy[cb + c] = 0.0;
+    a.dep_fx[cb + c] = 0ull; a.si[cb + c] = 0.0; a.ecen[cb + c] = 0.0; a.ncopy[cb + c] = 0.0;
   }
   const long long n_emit = plan_volume(a.emit_E + cb, a.n_target[k], nc, 1, nc, a.emit_n + cb,
                                        a.emit_off + cb + k, a.emit_w + cb, a.emitted + cb, red, sh);
@@ -127,7 +130,7 @@ __global__ void __launch_bounds__(NT) k_bplan(BatchArgs a) {
       }
     }
     a.n_side[2 * k + side] = n; a.w_side[2 * k + side] = wq; a.e_side[2 * k + side] = e;
-    a.esc[2 * k + side] = 0.0;
+    a.esc_fx[2 * k + side] = 0ull;
   }
   __syncthreads();
   if (t == 0) {
@@ -238,7 +241,7 @@ __global__ void __launch_bounds__(NT) k_bledger(BatchArgs a, int init) {
       L[IMC_BL_INTERNAL] = internal; L[IMC_BL_RADIATION] = rad;
     } else {
       const double prev = L[IMC_BL_TOTAL];
-      const double escaped = a.esc[2 * k] + a.esc[2 * k + 1];
+      const double escaped = fx_energy(a.esc_fx[2 * k] + a.esc_fx[2 * k + 1], a.wsum[k]);
       const double disc = a.comb_before[k] - a.comb_after[k];
       const double closure = total - prev - L[IMC_BL_BOUNDARY] + escaped + disc;
       L[IMC_BL_PREV] = prev; L[IMC_BL_TOTAL] = total;

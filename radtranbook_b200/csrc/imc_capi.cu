@@ -221,9 +221,11 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
 
   // ---- tracking ----
   if (pe.ok) IMC_CUDA(cudaEventRecord(pe.e[1], s));
-  IMC_CUDA(cudaMemsetAsync(tal->dep, 0, sizeof(double) * nc * ng, s));
+  unsigned long long* dep_fx = ws_ptr<unsigned long long>(workspace, L.dep_fx);
+  unsigned long long* esc_fx = ws_ptr<unsigned long long>(workspace, L.esc_fx);
+  IMC_CUDA(cudaMemsetAsync(dep_fx, 0, sizeof(unsigned long long) * nc * ng, s));
+  IMC_CUDA(cudaMemsetAsync(esc_fx, 0, sizeof(unsigned long long) * (4 + ng), s));
   IMC_CUDA(cudaMemsetAsync(tal->si, 0, sizeof(double) * nc * ng, s));
-  IMC_CUDA(cudaMemsetAsync(tal->escaped, 0, sizeof(double) * 4, s));
   IMC_CUDA(cudaMemsetAsync(tal->stats, 0, sizeof(unsigned long long) * IMC_STAT_N, s));
   unsigned long long* queue = ws_ptr<unsigned long long>(workspace, L.queue);
   IMC_CUDA(cudaMemsetAsync(queue, 0, 8, s));
@@ -246,6 +248,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   ta.chunk = par->chunk > 0 ? par->chunk : 64;
   ta.group_edges = mesh->group_edges;
   ta.escaped_group = tal->escaped_group;
+  ta.dep_fx = dep_fx; ta.esc_fx = esc_fx;
   const int block = par->block_size > 0 ? par->block_size : 256;
   const int bps = par->blocks_per_sm > 0 ? par->blocks_per_sm : 3;
   // reserved: bit 0 = stage the cell table in shared memory, bit 1 = prefetch the next draw
@@ -253,6 +256,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   const bool prefetch = (par->reserved & 2) != 0;
   IMC_CUDA(imc_launch_track(ta, mesh->geometry, block, sm_count() * bps, smem_cells, prefetch, s));
   if (pe.ok) { IMC_CUDA(cudaEventRecord(pe.e[2], s)); pe.recorded = true; }
+  IMC_CUDA(imc_launch_tally_finalize(ta, s));
   return IMC_OK;
 }
 
@@ -315,7 +319,7 @@ WsLayout imc_ws_layout(const imc_mesh* m, int64_t capacity) {
   auto take = [&](size_t bytes) { const size_t r = o; o += al256(bytes); return r; };
   L.summary = take(sizeof(imc_step_summary)); L.queue = take(8);
   L.e1f = take(4 * (nx + 1)); L.e2f = take(4 * (ny + 1));
-  L.sass = take(8 * ncg); L.cellf = take(16 * nc);
+  L.sass = take(8 * ncg); L.cellf = take(16 * ncg);
   L.emit_E = take(8 * ncg); L.emit_n = take(8 * nc); L.emit_off = take(8 * (nc + 1)); L.emit_w = take(4 * nc);
   L.tilt = take(8 * 4 * nc);
   L.src_n = take(8 * nc); L.src_off = take(8 * (nc + 1)); L.src_w = take(4 * nc);
@@ -328,6 +332,7 @@ WsLayout imc_ws_layout(const imc_mesh* m, int64_t capacity) {
   L.mixcdf = take(8 * 200);
   L.ecen = take(8 * ncg); L.ew = take(8 * ncg); L.ncopy = take(8 * ncg);
   L.cnt = take(4 * cap); L.blk = take(8 * ((cap + 1023) / 1024 + 2));
+  L.dep_fx = take(8 * ncg); L.esc_fx = take(8 * (4 + ng));
   L.total = o;
   return L;
 }

@@ -147,6 +147,48 @@ __device__ __forceinline__ void warp_tally1(bool flush, int key, double va, doub
   __syncwarp();
 }
 
+// ---- energy tallies in 64-bit fixed point ----
+// Deposited and escaped energy are summed as integers in units of q = W * 2^-60, W the
+// total weight tracked in the step (an upper bound of every such sum, so no total exceeds
+// 2^60 units).  Integer adds are exact and independent of order: each deposit is rounded
+// once, by at most q/2, however many adds a cell receives, which keeps the step's energy
+// balance far inside 1e-12 where FP64 atomics would drift with the square root of the
+// number of adds.
+constexpr double FX_ONE = 1152921504606846976.0;  // 2^60
+__device__ __forceinline__ double fx_inv_quantum(double wsum) { return wsum > 0.0 ? FX_ONE / wsum : 0.0; }
+__device__ __forceinline__ unsigned long long fx_units(double e, double inv_q) { return __double2ull_rn(e * inv_q); }
+__device__ __forceinline__ double fx_energy(unsigned long long u, double wsum) { return (double)u * (wsum / FX_ONE); }
+
+// warp_tally2 with the first tally in fixed point
+__device__ __forceinline__ void warp_tally_fx(bool flush, int key, unsigned long long ua, double vb,
+                                              unsigned long long* __restrict__ ta, double* __restrict__ tb,
+                                              WarpStage* st) {
+  const unsigned fm = __ballot_sync(FULL, flush);
+  if (fm == 0u) return;
+  const int lane = threadIdx.x & 31;
+  const unsigned peers = __match_any_sync(FULL, flush ? key : -1 - lane);
+  if (__all_sync(FULL, !flush || __popc(peers) == 1)) {
+    if (flush) { if (ua) atomicAdd(ta + key, ua); atomicAdd(tb + key, vb); }
+    return;
+  }
+  unsigned long long* sa_u = reinterpret_cast<unsigned long long*>(st->a);
+  sa_u[lane] = ua; st->b[lane] = vb;
+  __syncwarp();
+  if (flush && (__ffs(peers) - 1) == lane) {
+    unsigned long long su = 0ull;
+    double sb = 0.0;
+    unsigned m = peers;
+    while (m) {
+      const int l = __ffs(m) - 1;
+      m &= m - 1;
+      su += sa_u[l]; sb += st->b[l];
+    }
+    if (su) atomicAdd(ta + key, su);
+    atomicAdd(tb + key, sb);
+  }
+  __syncwarp();
+}
+
 // Group of a photon sampled from the Planck spectrum at T (mixture of Gammas,
 // MG_IMC/MG_IMC2D.py:202-254): n from the 1/n^4 mixture CDF, x = (four Exp(1)) / n,
 // energy T*x located in the group edges.

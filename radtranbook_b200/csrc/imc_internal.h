@@ -18,7 +18,7 @@ struct TrackArgs {
   const float* e1;           // nx+1 edges (FP32 copy)
   const float* e2;           // ny+1
   const float2* sass;        // [g][c] (Fleck absorption, effective scatter), FP32
-  const double2* cellf;      // [c] (1/V, 1/(sigma_a V dt) or -1/(V dt))
+  const double2* cellf;      // [g][c] (1/V, 1/(sigma_a V dt) or -1/(V dt))
   double* dep;               // [g][c]
   double* si;                // [g][c]
   double* escaped;           // [4 + ng]
@@ -39,10 +39,14 @@ struct TrackArgs {
   int chunk;
   const double* group_edges; // MG
   double* escaped_group;     // MG: [ng]
+  unsigned long long* dep_fx; // [g][c] deposited energy, fixed point (zeroed before launch)
+  unsigned long long* esc_fx; // [4 + ng] escaped energy by side, then by group (MG)
 };
 
 cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool smem_cells, bool prefetch,
                              cudaStream_t s);
+// dep = fixed-point deposition / V, escaped (and escaped_group) from their fixed-point sums
+cudaError_t imc_launch_tally_finalize(const TrackArgs& a, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------
 // Workspace layout (byte offsets into the caller's workspace, 256-aligned pieces)
@@ -50,7 +54,7 @@ cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, 
 struct WsLayout {
   size_t e1f, e2f;            // float edges
   size_t sass;                // float2 [ncg]
-  size_t cellf;               // double2 [nc]
+  size_t cellf;               // double2 [ncg]
   size_t emit_E;              // double [ncg]  emission energy per (group,) cell
   size_t emit_n;              // int64 [nc]    emission count per cell (order position)
   size_t emit_off;            // int64 [nc+1]  exclusive offsets in source order
@@ -64,6 +68,7 @@ struct WsLayout {
   size_t ecen, ew, ncopy;     // comb: double [nb], double [nb], long long [nb]
   size_t cnt;                 // int32 [cap]    comb copies per entry
   size_t blk;                 // int64 [nblk+1] comb block totals / offsets
+  size_t dep_fx, esc_fx;      // uint64 [ncg], [4 + ng] fixed-point energy tallies
   size_t total;
 };
 

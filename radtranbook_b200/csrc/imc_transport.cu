@@ -32,7 +32,7 @@ template <int GEOM, bool SMEM_CELLS, bool PREFETCH, bool MG>
 __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ unsigned blk_cnt[B_N];
-  __shared__ double blk_esc[4];
+  __shared__ unsigned long long blk_esc[4];
   WarpStage* stages = reinterpret_cast<WarpStage*>(smem);
   const int nwarps = blockDim.x >> 5;
   float* E1 = reinterpret_cast<float*>(stages + nwarps);
@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   if (SMEM_CELLS)
     for (int q = threadIdx.x; q < a.nc * a.ng; q += blockDim.x) CS[q] = a.sass[q];
   if (threadIdx.x < B_N) blk_cnt[threadIdx.x] = 0u;
-  if (threadIdx.x < 4) blk_esc[threadIdx.x] = 0.0;
+  if (threadIdx.x < 4) blk_esc[threadIdx.x] = 0ull;
   __syncthreads();
 
   const int lane = threadIdx.x & 31;
@@ -67,6 +67,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   const float c_light = (float)C_LIGHT;
   // weight floor, IMC/IMC1D.py:1007 / IMC/IMC2D.py:1771
   const float weight_floor = (float)(1e-10 * (*a.wsum) / (double)(n > 0 ? n : 1));
+  const double inv_q = fx_inv_quantum(*a.wsum);  // fixed-point energy tallies
   const float ss_thr = (GEOM == G_SLAB || GEOM == G_SPHERE) ? 1e-10f : 1e-12f;
 
   for (;;) {
@@ -287,8 +288,9 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
                 else { v = -v; nj = side == 2 ? 0 : a.ny - 1; }
                 atomicAdd(&blk_cnt[B_REFLECT], 1u);
               } else {
-                atomicAdd(&blk_esc[side], (double)w);
-                if (MG) atomicAdd(a.escaped_group + grp, (double)w);
+                const unsigned long long uw = fx_units((double)w, inv_q);
+                atomicAdd(&blk_esc[side], uw);
+                if (MG) atomicAdd(a.esc_fx + 4 + grp, uw);
                 atomicAdd(&blk_cnt[B_ESCAPE], 1u);
                 w = 0.f;
                 finished = true;
@@ -305,7 +307,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
               const int c2 = ci + a.nx * cj;
               const double2 cf = __ldg(a.cellf + c2);
               const double rem = (double)w;
-              atomicAdd(a.dep + c2, rem * cf.x);
+              atomicAdd(a.dep_fx + c2, fx_units(rem, inv_q));
               if (cf.y > 0.0) atomicAdd(a.si + c2, rem * cf.y);
               w = 0.f;
               finished = true;
@@ -343,13 +345,14 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
     // ---------------- converged tally flush ----------------
     // cellf[c] = (1/V, si factor): si factor > 0 is 1/(sigma_a V dt); < 0 is -1/(V dt),
     // meaning the cell's sigma_a is below the threshold and w*s is the estimator.
-    double vd = 0.0, vs = 0.0;
+    unsigned long long ud = 0ull;
+    double vs = 0.0;
     if (flush) {
       const double2 cf = __ldg(a.cellf + flush_cell);
-      vd = f_lost * cf.x;
+      ud = fx_units(f_lost, inv_q);
       vs = cf.y > 0.0 ? f_lost * cf.y : -f_wd * cf.y;
     }
-    warp_tally2(flush, flush_cell, vd, vs, a.dep, a.si, st);
+    warp_tally_fx(flush, flush_cell, ud, vs, a.dep_fx, a.si, st);
   }
 
   // ---------------- statistics ----------------
@@ -369,7 +372,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
     if (cap) atomicAdd(a.stats + S_CAP, cap);
     if (blk_cnt[B_ESCAPE]) atomicAdd(a.stats + S_ESCAPE, (unsigned long long)blk_cnt[B_ESCAPE]);
   }
-  if (threadIdx.x < 4 && blk_esc[threadIdx.x] != 0.0) atomicAdd(a.escaped + threadIdx.x, blk_esc[threadIdx.x]);
+  if (threadIdx.x < 4 && blk_esc[threadIdx.x] != 0ull) atomicAdd(a.esc_fx + threadIdx.x, blk_esc[threadIdx.x]);
 }
 
 template <int GEOM, bool SM, bool PF, bool MG>
@@ -391,7 +394,25 @@ cudaError_t launch_geom(const TrackArgs& a, int block, int grid, bool sm, bool p
   return pf ? launch_one<GEOM, false, true, MG>(a, block, grid, s) : launch_one<GEOM, false, false, MG>(a, block, grid, s);
 }
 
+// Fixed-point tallies to the FP64 outputs: deposition per unit volume per (group, cell),
+// escaped energy per side and (MG) per group.
+__global__ void k_tally_finalize(TrackArgs a) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  const double W = *a.wsum;
+  const int ncg = a.nc * a.ng;
+  if (q < ncg) a.dep[q] = fx_energy(a.dep_fx[q], W) * a.cellf[q].x;
+  else if (q < ncg + 4) a.escaped[q - ncg] = fx_energy(a.esc_fx[q - ncg], W);
+  else if (q < ncg + 4 + a.ng && a.ng > 1) a.escaped_group[q - ncg - 4] = fx_energy(a.esc_fx[q - ncg], W);
+}
+
 }  // namespace
+
+cudaError_t imc_launch_tally_finalize(const TrackArgs& a, cudaStream_t s) {
+  ++g_imc_launches;
+  const int n = a.nc * a.ng + 4 + a.ng;
+  k_tally_finalize<<<(n + 255) / 256, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
 
 cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool sm, bool pf, cudaStream_t s) {
   ++g_imc_launches;
