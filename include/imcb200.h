@@ -197,6 +197,24 @@ IMC_API imc_status imc_comb(const imc_mesh* mesh, const imc_bank* in, imc_bank* 
                     void* workspace, size_t workspace_bytes, imc_comb_report* report,
                     void* stream);
 
+/* Vector-Jacobian product of one step's deposition tally with respect to the per-cell
+ * opacity mat->sigma, 2-D gray (xy or rz):
+ *   grad[c] += sum_c' cotangent[c'] * d dep[c'] / d sigma[c].
+ * The arguments are those of the forward imc_step_transport call, with `bank` holding the
+ * same census entries (its first bank->size entries) as before the forward call.  The
+ * step's source particles are regenerated from the same Philox streams and every history
+ * is tracked twice from its counter (no path is stored): once for its total cotangent-
+ * weighted score, once to accumulate the path-length derivative of implicit capture and
+ * the likelihood-ratio derivative of effective scattering, chained through the Fleck
+ * factor (d sigma_a / d sigma = f^2, d sigma_s / d sigma = 1 - f^2).  The bank entries
+ * after bank->size and the tallies' sigma_a / sigma_s / emitted are used as scratch; the
+ * census entries and bank->size are unchanged.  Synchronises the stream.
+ * No reference counterpart: the reference has no derivative of its tallies. */
+IMC_API imc_status imc_adjoint_vjp(const imc_mesh* mesh, const imc_material* mat,
+                                   const imc_step_params* par, imc_bank* bank,
+                                   const double* cotangent, double* grad, imc_tallies* tal,
+                                   void* workspace, size_t workspace_bytes, void* stream);
+
 /* imc_comb without a workspace argument.  No reference counterpart: the reference combs
  * NumPy arrays and has no device scratch to provide.
  *

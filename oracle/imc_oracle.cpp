@@ -52,6 +52,7 @@ enum { S_EVENTS = 0, S_BOUNDARY, S_SCATTER, S_CENSUS, S_CAPTURE, S_FLOOR, S_REFL
 
 struct EventOut {
   double w, d1, d2, p1, p2, dep, dep_i, dcen;
+  double s;  /* path length of the event */
   int cross, evt;
 };
 
@@ -169,7 +170,7 @@ EventOut event_xy(double w, double ux, double uy, double x, double y, double xl,
   const double lost = w - wn;
   o.dep = lost;
   o.dep_i = (sa > 1e-12) ? lost / sa : w * s;
-  o.w = wn; o.d1 = uxn; o.d2 = uyn; o.p1 = xn; o.p2 = yn; o.dcen = dcen - s;
+  o.w = wn; o.d1 = uxn; o.d2 = uyn; o.p1 = xn; o.p2 = yn; o.dcen = dcen - s; o.s = s;
   o.cross = cross; o.evt = evt;
   return o;
 }
@@ -238,7 +239,7 @@ EventOut event_rz(double w, double mu, double eta, double r, double z, double ri
   const double lost = w - wn;
   o.dep = lost;
   o.dep_i = (sa > 1e-12) ? lost / sa : w * s;
-  o.w = wn; o.d1 = mun; o.d2 = etan; o.p1 = rn; o.p2 = zn; o.dcen = dcen - s;
+  o.w = wn; o.d1 = mun; o.d2 = etan; o.p1 = rn; o.p2 = zn; o.dcen = dcen - s; o.s = s;
   o.cross = cross; o.evt = evt;
   return o;
 }
@@ -899,6 +900,120 @@ int orc_step_transport(void* h, const orc_step_in* in, orc_step_out* out) {
   }
   for (int t = 0; t < nth; ++t)
     for (int s = 0; s < S_N; ++s) out->stats[s] += st_t[t][s];
+  return 0;
+}
+
+/* Vector-Jacobian product of the deposition tally with respect to the per-cell opacity
+ * (2-D gray), in FP64: the estimator of the GPU adjoint kernel restated on the same
+ * histories.  Per history, a first replay gives its cotangent-weighted score
+ * L = sum_i a_i d_i (a = cot / V, d = deposit of event i); a second replay accumulates
+ * per cell visit gp = sum s_k (a_k w_{k+1} + L_{<=k} - L) (implicit capture, path fixed)
+ * and, where the scatter distance depends on sigma_s (not capped, sigma_s > 1e-12),
+ * gs1 = sum (L - L_{<k}) s_k, gs2 = sum over scatters of (L - L_{<k}) (likelihood ratio),
+ * and adds f^2 gp + (1 - f^2)(gs2 / sigma_s - gs1) to grad[cell] (f = sigma_a / sigma, the
+ * Fleck factor).  The bank holds the step's census and sources (orc_step_transport with
+ * sources_only) and is not modified.  History rules as orc_step_transport (2-D). */
+int orc_adjoint_vjp(void* h, const orc_step_in* in, const double* cot, double* grad) {
+  Oracle* o = (Oracle*)h;
+  Problem& P = o->P;
+  Bank& B = o->B;
+  if (P.geom != G_XY && P.geom != G_RZ) return 2;
+  const int nc = ncells(P);
+  std::vector<double> sa, ss;
+  fleck(P, in, sa, ss);
+  const long long N = (long long)B.size();
+  double wsum = 0;
+  for (long long k = 0; k < N; ++k) wsum += B.w[k];
+  const double floor_w = 1e-10 * wsum / (double)std::max(N, 1LL);
+  int nth = in->nthreads > 0 ? in->nthreads : 1;
+#ifndef _OPENMP
+  nth = 1;
+#endif
+  std::vector<std::vector<KSum>> g_t(nth, std::vector<KSum>(nc));
+  const double dt = in->dt;
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nth)
+  for (long long k = 0; k < N; ++k) {
+    int tid = 0;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+#endif
+    KSum* g = g_t[tid].data();
+    if (!(B.w[k] > 0) || !((dt - B.t[k]) * C_LIGHT > 0)) continue;
+    auto replay = [&](int phase, double Ltot) -> double {
+      double w = B.w[k], d1 = B.d1[k], d2 = B.d2[k], p1 = B.p1[k], p2 = B.p2[k];
+      int c = B.cell[k];
+      double dcen = (dt - B.t[k]) * C_LIGHT;
+      uint32_t ev = 0;
+      double L = 0.0, Lc = 0.0, gp = 0.0, gs1 = 0.0, gs2 = 0.0;
+      auto flush = [&](int cell) {
+        if (phase == 1 && (gp != 0.0 || gs1 != 0.0 || gs2 != 0.0)) {
+          const double sig = in->sigma[cell];
+          const double f = sig > 0 ? sa[cell] / sig : 1.0;
+          double val = f * f * gp;
+          if (ss[cell] > 0 && (gs1 != 0.0 || gs2 != 0.0)) val += (1.0 - f * f) * (gs2 / ss[cell] - gs1);
+          g[cell].add(val);
+        }
+        gp = gs1 = gs2 = 0.0;
+      };
+      while (dcen > 0) {
+        int i = c % P.nx, j = c / P.nx;
+        if (in->max_events > 0 && (long long)ev >= in->max_events) break;
+        Draw4 r = draw(P.seed, (uint32_t)k, ev, in->step, oracle::TAG_TRANSPORT);
+        ++ev;
+        const double xl = P.e1[i], xr = P.e1[i + 1], yl = P.e2[j], yr = P.e2[j + 1];
+        EventOut e = P.geom == G_XY
+                         ? event_xy(w, d1, d2, p1, p2, xl, xr, yl, yr, sa[c], ss[c], dcen, r.u[0], r.u[1], r.u[2])
+                         : event_rz(w, d1, d2, p1, p2, xl, xr, yl, yr, sa[c], ss[c], dcen, r.u[0], r.u[1], r.u[2]);
+        const double Lcell = std::min(xr - xl, yr - yl);
+        const bool scores = !(ss[c] * Lcell > 10000.0) && ss[c] > 1e-12;
+        const double ac = cot[c] / P.vol[c];
+        const double dd = w - e.w;
+        if (phase == 0) {
+          L += ac * dd;
+        } else {
+          const double Lprev = Lc;
+          Lc += ac * dd;
+          gp += e.s * (ac * e.w + Lc - Ltot);
+          if (scores) {
+            const double R = Ltot - Lprev;
+            gs1 += R * e.s;
+            if (e.evt == EV_SCATTER) gs2 += R;
+          }
+        }
+        dcen = e.dcen;
+        w = e.w;
+        if (w <= floor_w) break; /* 2-D floor: the history stops */
+        d1 = e.d1; d2 = e.d2; p1 = e.p1; p2 = e.p2;
+        if (e.cross != X_NONE) {
+          flush(c);
+          if (e.cross == X_IP) ++i; else if (e.cross == X_IM) --i;
+          else if (e.cross == X_JP) ++j; else --j;
+          int side = -1;
+          if (i < 0) side = 0; else if (i >= P.nx) side = 1; else if (j < 0) side = 2; else if (j >= P.ny) side = 3;
+          if (side >= 0) {
+            if (in->reflect[side]) {
+              if (side < 2) { d1 = -d1; i = side == 0 ? 0 : P.nx - 1; }
+              else { d2 = -d2; j = side == 2 ? 0 : P.ny - 1; }
+            } else {
+              w = 0; dcen = 0;
+              break;
+            }
+          }
+          c = i + P.nx * j;
+        }
+        if (w <= 1e-300) break;
+      }
+      flush(c);
+      return L;
+    };
+    const double Ltot = replay(0, 0.0);
+    replay(1, Ltot);
+  }
+  for (int c = 0; c < nc; ++c) {
+    KSum x;
+    for (int t = 0; t < nth; ++t) x.add(g_t[t][c].value());
+    grad[c] = x.value();
+  }
   return 0;
 }
 

@@ -81,6 +81,8 @@ def load():
         lib.orc_init_ic.argtypes = [c_void_p, c_longlong, c_void_p, c_double]
         lib.orc_step_transport.restype = c_int
         lib.orc_step_transport.argtypes = [c_void_p, POINTER(StepIn), POINTER(StepOut)]
+        lib.orc_adjoint_vjp.restype = c_int
+        lib.orc_adjoint_vjp.argtypes = [c_void_p, POINTER(StepIn), c_void_p, c_void_p]
         lib.orc_comb.restype = c_longlong
         lib.orc_comb.argtypes = [c_void_p, c_longlong, c_uint32, c_int, c_void_p]
         lib.orc_comb_with_xi.restype = c_longlong
@@ -208,6 +210,31 @@ class Oracle:
         out["n_transported"] = so.n_transported
         out["weight_floor"] = so.weight_floor
         return out
+
+    def adjoint_vjp(self, T, sigma, cv, step, dt, theta, reflect, cotangent, max_events=0, nthreads=None):
+        """d(cot . dep)/d sigma on the current bank (census + the step's sources, e.g. after
+        transport(..., sources_only=True)), FP64; the bank is not modified."""
+        keep = []
+
+        def arr(x):
+            a = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+            keep.append(a)
+            return _p(a)
+
+        si = StepIn()
+        si.step = int(step) & 0xFFFFFFFF
+        si.dt, si.theta = float(dt), float(theta)
+        si.T, si.sigma, si.cv = arr(T), arr(sigma), arr(cv)
+        for q in range(4):
+            si.face_T[q] = None
+            si.reflect[q] = int(bool(reflect[q])) if q < len(reflect) else 0
+        si.max_events = int(max_events)
+        si.nthreads = int(nthreads or os.cpu_count() or 1)
+        grad = np.zeros(self.nc)
+        st = self.lib.orc_adjoint_vjp(self.h, ctypes.byref(si), arr(cotangent), _p(grad))
+        if st != 0:
+            raise ValueError("the adjoint covers 2-D gray geometries (xy, rz)")
+        return grad
 
     # ---------------- multigroup ----------------
     def init_ic_mg(self, tr_flat, N, group_edges, t_emit_floor=0.0) -> int:

@@ -139,6 +139,8 @@ SIGNATURES = {
                          c_int32, c_void_p, c_void_p, c_size_t, POINTER(ImcCombReport), c_void_p]),
     "imc_comb_noalloc": (c_int, [POINTER(ImcMesh), POINTER(ImcBank), POINTER(ImcBank), c_int64, c_uint64,
                                  c_uint32, c_int32, c_void_p, POINTER(ImcCombReport), c_void_p]),
+    "imc_adjoint_vjp": (c_int, [POINTER(ImcMesh), POINTER(ImcMaterial), POINTER(ImcStepParams), POINTER(ImcBank),
+                                c_void_p, c_void_p, POINTER(ImcTallies), c_void_p, c_size_t, c_void_p]),
     "imc_batch_workspace_bytes": (c_size_t, [POINTER(ImcBatch)]),
     "imc_batch_init": (c_int, [POINTER(ImcBatch), POINTER(ImcBatchState), c_void_p, c_void_p, c_void_p, c_size_t,
                                c_void_p]),

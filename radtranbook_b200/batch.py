@@ -27,32 +27,9 @@ import torch
 
 from . import _lib
 from .engine import require_cuda
+from .rng import philox4x32_10, u01 as _u01
 
 TAG_INSTANCE = 0x70000000  # Philox stream of per-instance keys and parameters
-
-
-# --------------------------------------------------------------------------- Philox (host)
-def philox4x32_10(ctr: np.ndarray, key: int) -> np.ndarray:
-    """Philox-4x32-10 of counters ctr[(n, 4) uint32] under a 64-bit key (host, vectorised).
-    The same function as the device generator (Salmon et al., SC'11)."""
-    c = np.asarray(ctr, dtype=np.uint64).reshape(-1, 4).copy()
-    k0, k1 = np.uint64(key & 0xFFFFFFFF), np.uint64((key >> 32) & 0xFFFFFFFF)
-    m32 = np.uint64(0xFFFFFFFF)
-    M0, M1 = np.uint64(0xD2511F53), np.uint64(0xCD9E8D57)
-    for r in range(10):
-        if r:
-            k0 = (k0 + np.uint64(0x9E3779B9)) & m32
-            k1 = (k1 + np.uint64(0xBB67AE85)) & m32
-        p0 = M0 * c[:, 0]
-        p1 = M1 * c[:, 2]
-        hi0, lo0 = p0 >> np.uint64(32), p0 & m32
-        hi1, lo1 = p1 >> np.uint64(32), p1 & m32
-        c = np.stack([hi1 ^ c[:, 1] ^ k0, lo1, hi0 ^ c[:, 3] ^ k1, lo0], axis=1)
-    return c.astype(np.uint32)
-
-
-def _u01(x: np.ndarray) -> np.ndarray:
-    return (((x.astype(np.uint64) >> np.uint64(9)) << np.uint64(1)) | np.uint64(1)).astype(np.float64) * 2.0 ** -24
 
 
 # --------------------------------------------------------------------------- problem

@@ -20,7 +20,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden"]
 PER_FILE = {"imc_bookkeeping.cu": ["-fmad=false"], "imc_batch_plan.cu": ["-fmad=false"]}
 SOURCES = ["imc_capi.cu", "imc_bookkeeping.cu", "imc_source.cu", "imc_transport.cu", "imc_comb.cu",
-           "imc_batch.cu", "imc_batch_plan.cu"]
+           "imc_batch.cu", "imc_batch_plan.cu", "imc_adjoint.cu"]
 HEADERS = ["imc_device.cuh", "imc_internal.h", "imc_block.cuh", "imc_sample.cuh", "imc_batch.h"]
 
 

@@ -87,9 +87,11 @@ inline void set_bank(float*& p2, float*& d2, const imc_bank* b, bool two_d) {
   d2 = two_d ? b->dir2 : nullptr;
 }
 
+// adj != NULL: the sources are made as for the forward step, then the adjoint kernel
+// replays the histories instead of tracking them (bank and tallies are not written).
 imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const imc_step_params* par,
                            imc_bank* bank, imc_tallies* tal, void* workspace, size_t workspace_bytes,
-                           imc_step_summary* sum, cudaStream_t s) {
+                           imc_step_summary* sum, cudaStream_t s, const AdjointArgs* adj = nullptr) {
   imc_status st = check_mesh(mesh);
   if (st != IMC_OK) return st;
   const bool two_d = mesh->geometry >= IMC_GEOM_XY;
@@ -254,6 +256,13 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   // reserved: bit 0 = stage the cell table in shared memory, bit 1 = prefetch the next draw
   const bool smem_cells = (par->reserved & 1) ? true : ((long long)nc * ng <= 4096);
   const bool prefetch = (par->reserved & 2) != 0;
+  if (adj) {
+    AdjointArgs A = *adj;
+    A.t = ta; A.sa64 = tal->sigma_a; A.ss64 = tal->sigma_s; A.sig64 = mat->sigma;
+    IMC_CUDA(imc_launch_adjoint(A, mesh->geometry, block, sm_count() * bps, s));
+    if (pe.ok) { IMC_CUDA(cudaEventRecord(pe.e[2], s)); pe.recorded = true; }
+    return IMC_OK;
+  }
   IMC_CUDA(imc_launch_track(ta, mesh->geometry, block, sm_count() * bps, smem_cells, prefetch, s));
   if (pe.ok) { IMC_CUDA(cudaEventRecord(pe.e[2], s)); pe.recorded = true; }
   IMC_CUDA(imc_launch_tally_finalize(ta, s));
@@ -505,6 +514,31 @@ imc_status imc_step_transport(const imc_mesh* mesh, const imc_material* mat, con
   bank->size = h.n_bank;
   if (h.flags & IMC_FLAG_NONFINITE) return IMC_ERR_NONFINITE;
   if (h.flags & IMC_FLAG_EVENT_CAP) return IMC_ERR_EVENT_CAP;
+  return IMC_OK;
+}
+
+imc_status imc_adjoint_vjp(const imc_mesh* mesh, const imc_material* mat, const imc_step_params* par,
+                           imc_bank* bank, const double* cotangent, double* grad, imc_tallies* tal, void* workspace,
+                           size_t workspace_bytes, void* stream) {
+  if (!mesh || !par || !bank || !cotangent || !grad) return IMC_ERR_INVALID_ARG;
+  imc_status st = check_mesh(mesh);
+  if (st != IMC_OK) return st;
+  if ((mesh->geometry != IMC_GEOM_XY && mesh->geometry != IMC_GEOM_RZ) || mesh->n_groups != 1)
+    return IMC_ERR_BAD_GEOMETRY;
+  const WsLayout L = imc_ws_layout(mesh, bank->capacity);
+  if (!workspace || workspace_bytes < L.total) return IMC_ERR_WORKSPACE;
+  cudaStream_t s = (cudaStream_t)stream;
+  imc_step_summary* sum = internal_summary(workspace, L);
+  long long n_census = bank->size;
+  IMC_CUDA(cudaMemcpyAsync(&sum->n_census, &n_census, sizeof(n_census), cudaMemcpyHostToDevice, s));
+  AdjointArgs A{};
+  A.cot = cotangent; A.grad = grad;
+  st = transport_async(mesh, mat, par, bank, tal, workspace, workspace_bytes, sum, s, &A);
+  if (st != IMC_OK) return st;
+  int flags = 0;
+  IMC_CUDA(cudaMemcpyAsync(&flags, &sum->flags, sizeof(int), cudaMemcpyDeviceToHost, s));
+  IMC_CUDA(cudaStreamSynchronize(s));
+  if (flags & IMC_FLAG_NONFINITE) return IMC_ERR_NONFINITE;
   return IMC_OK;
 }
 

@@ -48,6 +48,19 @@ cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, 
 // dep = fixed-point deposition / V, escaped (and escaped_group) from their fixed-point sums
 cudaError_t imc_launch_tally_finalize(const TrackArgs& a, cudaStream_t s);
 
+// Adjoint tracking (imc_adjoint.cu): the step's histories replayed from their Philox
+// counters, accumulating the vector-Jacobian product of the deposition tally with respect
+// to the per-cell opacity.
+struct AdjointArgs {
+  TrackArgs t;            // the forward step's tracking arguments (tallies unused)
+  const double* cot;      // [c] cotangent of the deposition tally (per unit volume)
+  double* grad;           // [c] += d(cot . dep) / d sigma
+  const double* sa64;     // [c] Fleck absorption opacity (FP64)
+  const double* ss64;     // [c] effective scatter opacity (FP64)
+  const double* sig64;    // [c] opacity sigma
+};
+cudaError_t imc_launch_adjoint(const AdjointArgs& a, int geom, int block, int grid, cudaStream_t s);
+
 // ---------------------------------------------------------------------------------
 // Workspace layout (byte offsets into the caller's workspace, 256-aligned pieces)
 // ---------------------------------------------------------------------------------

@@ -1,5 +1,5 @@
-"""Host-side checks of the batched slab engine (no GPU): the host Philox against the
-oracle's, the uneven 256-instance batch's parameter ranges and determinism, the bank slot
+"""Host-side checks of the batched slab engine (no GPU): the host Philox (rng.py) against
+the oracle's, the uneven 256-instance batch's parameter ranges and determinism, the bank slot
 plan, and the ledger field numbering against include/imcb200.h."""
 import pathlib
 import re
@@ -7,7 +7,7 @@ import re
 import numpy as np
 
 from oracle import oracle as O
-from radtranbook_b200 import _lib, batch
+from radtranbook_b200 import _lib, batch, rng as host_rng
 
 ROOT = pathlib.Path(__file__).resolve().parents[1]
 
@@ -16,7 +16,7 @@ def test_host_philox_matches_oracle():
     rng = np.random.default_rng(3)
     ctr = rng.integers(0, 2 ** 32, size=(64, 4), dtype=np.uint64).astype(np.uint32)
     key = (0x1234567, 0x89ABCDEF)
-    got = batch.philox4x32_10(ctr, key[0] | (key[1] << 32))
+    got = host_rng.philox4x32_10(ctr, key[0] | (key[1] << 32))
     for q in range(len(ctr)):
         np.testing.assert_array_equal(got[q], O.philox(ctr[q], key))
 
