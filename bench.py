@@ -37,6 +37,10 @@ sys.path.insert(0, ROOT)
 METRIC = "IMC track-segments/s and FOM=1/(rel.var*time) on 1 B200: plain vs batched/adjoint"
 UNIT = "track-segments/s"
 B_SEG_2D = 72  # bytes per 2-D gray segment: 36-byte record loaded + stored
+# DRAM bytes the tracking kernel actually moves per segment on this workload: ncu
+# dram__bytes_read.sum + dram__bytes_write.sum of one full-size launch (401.4 MB for
+# 66.79 M segments); the histories stay in registers across their events.
+DRAM_B_PER_SEG_MEASURED = 401.441024e6 / 66791775
 
 
 def measured_peaks():
@@ -190,6 +194,166 @@ def _gpu_steps(p, state, steps, use_device, dist=None):
 CLOSURE = [0.0]  # worst |energy closure| / total energy over the steps run
 
 
+def _fom(x_runs: np.ndarray, t_runs: list) -> dict:
+    """FOM = 1 / (R^2 T): R^2 = mean over the region of interest (cells whose mean tally
+    exceeds 1e-3 of the largest) of Var_s(X_c) / mean_s(X_c)^2 across independent seeds,
+    T = mean wall time of one run."""
+    m = x_runs.mean(0)
+    roi = m > 1e-3 * m.max()
+    r2 = float(np.mean(x_runs[:, roi].var(0, ddof=1) / m[roi] ** 2))
+    t = float(np.mean(t_runs))
+    return {"fom": 1.0 / (r2 * t), "rel_var": r2, "rel_err": float(np.sqrt(r2)), "seconds_per_run": t,
+            "seeds": int(x_runs.shape[0]), "roi_cells": int(roi.sum())}
+
+
+def fom_gpu(p, steps: int, seeds: int, launch: dict | None) -> dict:
+    """Crooked pipe, `steps` drop-in steps per seed (device material callables), last-step
+    deposition per cell as the tally; run wall time by CUDA events around the steps."""
+    import torch
+
+    from radtranbook_b200 import imc2d
+
+    xs, ts = [], []
+    for s in range(seeds):
+        st = imc2d.init_simulation(p["Ntarget"], p["Tinit"], p["Tr_init"], p["edges1"], p["edges2"], p["eos_dev"],
+                                   p["inv_eos_dev"], geometry="rz", seed=0xF0E00000 + s)
+        if launch:
+            st._engine.launch.update(launch)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        st, _, _, _ = _gpu_steps(p, st, steps, True)
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1) * 1e-3)
+        xs.append(st._engine.dep[: st._engine.nc].double().cpu().numpy().copy())
+    out = _fom(np.array(xs), ts)
+    out["particles_per_step"] = p["Ntarget"] + p["Nboundary"]
+    out["steps"] = steps
+    return out
+
+
+def fom_cpu(scale: float, steps: int, seeds: int, nthreads: int) -> dict:
+    """The same FOM for the FP64 CPU oracle at `scale` x the particle counts (the FOM is
+    nearly independent of the particle count: R^2 ~ 1/N, T ~ N)."""
+    from oracle import oracle as O
+    from radtranbook_b200 import problems
+
+    p = problems.crooked_pipe(scale=scale)
+    e1, e2 = p["edges1"], p["edges2"]
+    vol = O.flat2d(np.pi * (e1[1:] ** 2 - e1[:-1] ** 2)[:, None] * np.diff(e2)[None, :])
+    rc = 0.5 * (e1[:-1] + e1[1:])
+    face = [None, None, np.where(rc < 0.5, 0.5, 0.0), None]
+    kw = dict(Ntarget=p["Ntarget"], Nboundary=p["Nboundary"], Nsource=0, Nmax=p["Nmax"], face_T=face, dt=p["dt"],
+              sigma_a_func=p["sigma_host"], inv_eos=p["inv_eos_host"], cv=p["cv_host"], reflect=p["reflect"],
+              max_events=1_000_000)
+    xs, ts = [], []
+    for s in range(seeds):
+        run = O.OracleGray("rz", e1, e2, vol, 0xC0E00000 + s, p["Ntarget"], p["Tinit"], p["Tr_init"], p["eos_host"],
+                           p["inv_eos_host"], nthreads=nthreads)
+        t0 = time.perf_counter()
+        r = None
+        for _ in range(steps):
+            r = run.step(**kw)
+        ts.append(time.perf_counter() - t0)
+        xs.append(np.asarray(r["dep"], dtype=np.float64).copy())
+    out = _fom(np.array(xs), ts)
+    out["particles_per_step"] = p["Ntarget"] + p["Nboundary"]
+    out["steps"] = steps
+    out["cores"] = nthreads
+    return out
+
+
+def form_batched(steps: int, tune: bool) -> dict:
+    """Uneven 256-instance slab batch: the batched engine (one CUDA graph per step) and the
+    plain form (the single-problem drop-in, one instance after the other) on the same
+    histories (each instance draws identical Philox streams in both forms)."""
+    import torch
+
+    from radtranbook_b200 import _lib, batch
+
+    spec = batch.uneven_slab_batch()
+    eng = batch.BatchEngine(spec)
+    eng.init()
+    tuned = None
+    if tune:
+        tuned = batch.tune(eng, grid={"block_size": (256,), "blocks_per_sm": (4, 8), "chunk": (1024, 4096),
+                                      "refill_min": (1, 8)})
+        eng.init()  # tuning replays the first step from the initial state; start over
+    eng.capture()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    eng.step(steps)
+    e1.record()
+    torch.cuda.synchronize()
+    eng.check()
+    tb = e0.elapsed_time(e1) * 1e-3
+    ev_b = eng.total_events()
+    L = eng.ledger()
+    t0 = time.perf_counter()
+    pl = batch.run_plain(spec, steps, launch=None)
+    torch.cuda.synchronize()
+    tp = time.perf_counter() - t0
+    return {"workload": "uneven_slab_batch_256", "steps": steps, "instances": spec.K,
+            "particles_per_step": int((spec.n_target + spec.n_boundary).sum()),
+            "batched_segments_per_s": ev_b / tb, "plain_segments_per_s": pl["events"] / tp,
+            "speedup": (ev_b / tb) / (pl["events"] / tp), "same_histories": bool(ev_b == pl["events"]),
+            "batched_s": tb, "plain_s": tp, "energy_closure_max_rel": float(L[:, _lib.BL_MAX_REL].max()),
+            "launch": dict(eng.launch), "autotune": None if tuned is None else
+            {"best_ms": tuned["best_ms"], "worst_ms": tuned["worst_ms"], "candidates": len(tuned["trials"])}}
+
+
+def form_adjoint(repeats: int = 3, fd_cells: int = 64) -> dict:
+    """128 x 128 random-opacity XY step (4e6 histories): forward and VJP device time, and
+    the VJP against central differences with common random numbers on random cells."""
+    import torch
+
+    from radtranbook_b200 import adjoint
+
+    prob, sigma_np = adjoint.opacity_field_problem()
+    sig = torch.as_tensor(sigma_np, device=prob.device)
+    cot = torch.as_tensor(adjoint.unit_cotangent(prob.nc), device=prob.device)
+    prob.forward(sig)
+    prob.vjp(sig, cot)
+    fw, bw = [], []
+    for _ in range(repeats):
+        prob.forward(sig)
+        fw.append(prob.forward_ms)
+    segs = int(prob.engine.host_stats()[0][0])
+    for _ in range(repeats):
+        g = prob.vjp(sig, cot)
+        bw.append(prob.backward_ms)
+    rng = np.random.default_rng(0xFDC)
+    cells = rng.choice(prob.nc, fd_cells, replace=False)
+    fd = adjoint.fd_check(prob, sig, cot, cells, rel=1e-3)
+    ga = g.cpu().numpy()[cells]
+    sig_cells = np.abs(fd) > 1e-3 * np.abs(fd).max()
+    rel = np.abs(ga - fd) / np.maximum(np.abs(fd), 1e-300)
+    return {"workload": "random_opacity_xy_128x128", "histories": prob.setup.n_boundary,
+            "forward_ms": float(np.median(fw)), "backward_ms": float(np.median(bw)),
+            "backward_over_forward": float(np.median(bw) / np.median(fw)), "segments_per_forward": segs,
+            "fd_cells": fd_cells, "fd_rel_err_vector": float(np.linalg.norm(ga - fd) / np.linalg.norm(fd)),
+            "fd_significant_cells": int(sig_cells.sum()),
+            "fd_max_rel_err_significant": float(rel[sig_cells].max()) if sig_cells.any() else None}
+
+
+def max_time_and_totals(dist, ms: float, counts: list, device) -> tuple:
+    """Whole-job figures of a timed region: the slowest rank's device time (ms) and the
+    sum over ranks of each count (segments, histories)."""
+    if dist is None:
+        return float(ms), [float(c) for c in counts]
+    import torch
+
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    tot = torch.tensor([float(c) for c in counts], dtype=torch.float64, device=device)
+    dist.all_reduce(tot)
+    return float(t.item()), [float(x) for x in tot.cpu()]
+
+
 def run_ours(args, rank: int, world: int):
     import torch
 
@@ -248,17 +412,7 @@ def run_ours(args, rank: int, world: int):
         barrier()
         clocks.mark_end()
     launches = lib.imc_kernel_launches() - launches0
-    ms = s0.elapsed_time(s1)
-    tmax = ms
-    if dist is not None:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tmax = float(t.item())
-        tot = torch.tensor([float(seg), float(hist)], device=dev, dtype=torch.float64)
-        dist.all_reduce(tot)
-        seg_all, hist_all = float(tot[0]), float(tot[1])
-    else:
-        seg_all, hist_all = float(seg), float(hist)
+    tmax, (seg_all, hist_all) = max_time_and_totals(dist, s0.elapsed_time(s1), [seg, hist], dev)
     value = seg_all / (tmax * 1e-3)
 
     # ---------------- end to end through the drop-in API with host callables ----------------
@@ -274,14 +428,7 @@ def run_ours(args, rank: int, world: int):
     state2, seg2, hist2, _ = _gpu_steps(p, state2, args.steps, False, dist)
     e1.record()
     barrier()
-    ms2 = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([ms2], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms2 = float(t.item())
-        t2 = torch.tensor([float(seg2)], device=dev, dtype=torch.float64)
-        dist.all_reduce(t2)
-        seg2 = float(t2.item())
+    ms2, (seg2,) = max_time_and_totals(dist, e0.elapsed_time(e1), [seg2], dev)
     h2d = (_lib.TRANSFER["h2d"] - tr0["h2d"]) / args.steps
     d2h = (_lib.TRANSFER["d2h"] - tr0["d2h"]) / args.steps
     e2e = seg2 / (ms2 * 1e-3)
@@ -294,7 +441,9 @@ def run_ours(args, rank: int, world: int):
     t_launch = float(np.mean(track_ms)) * 1e-3
     achieved = B_SEG_2D * seg_per_launch / t_launch / 1e9
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": None, "kernel": "k_track<RZ>", "peak_source": peak_kind,
+            "traffic": DRAM_B_PER_SEG_MEASURED * seg_per_launch, "kernel": "k_track<RZ>", "peak_source": peak_kind,
+            "traffic_source": "ncu dram bytes of one full-size k_track launch (6.01 B/segment), scaled to the "
+                              "segments per launch of this run",
             "segments_per_launch": seg_per_launch, "bytes_per_segment_algorithmic": B_SEG_2D,
             "track_ms_per_launch": t_launch * 1e3}
     cpu = None
@@ -303,6 +452,14 @@ def run_ours(args, rank: int, world: int):
         cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
                "sample": f"crooked pipe, {args.cpu_scale:g} x particles, 1 warm-up + {args.cpu_steps} timed steps, "
                          f"FP64 C++ oracle, OpenMP ({dtc:.1f} s)", "histories_per_s": h}
+    forms = fom = None
+    if world == 1 and not args.no_forms:
+        forms = {"batched": form_batched(args.batch_steps, not args.no_tune), "adjoint": form_adjoint()}
+    if world == 1 and not args.no_fom:
+        fom = {"gpu": fom_gpu(p, args.fom_steps, args.fom_seeds, dict(eng.launch))}
+        if not args.no_cpu_baseline:
+            fom["cpu"] = fom_cpu(args.fom_cpu_scale, args.fom_steps, args.fom_cpu_seeds, os.cpu_count() or 1)
+            fom["gpu_over_cpu"] = fom["gpu"]["fom"] / fom["cpu"]["fom"]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": tmax / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -322,6 +479,8 @@ def run_ours(args, rank: int, world: int):
         "roofline": roof,
         "cpu_baseline": cpu,
         "clocks": clocks.summary(),
+        "fom": fom,
+        "forms": forms,
     }
     print(json.dumps(line), flush=True)
 
@@ -338,6 +497,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--tune-log", default=None, help="write the autotuner's trials to this JSON file")
+    ap.add_argument("--no-forms", action="store_true", help="skip the batched and adjoint forms")
+    ap.add_argument("--batch-steps", type=int, default=4)
+    ap.add_argument("--no-fom", action="store_true")
+    ap.add_argument("--fom-seeds", type=int, default=32)
+    ap.add_argument("--fom-steps", type=int, default=100)
+    ap.add_argument("--fom-cpu-seeds", type=int, default=8)
+    ap.add_argument("--fom-cpu-scale", type=float, default=0.01)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -111,17 +111,36 @@ def _host_copy(t: torch.Tensor) -> np.ndarray:
     return a
 
 
-def average_tallies(dist, eng: Engine) -> None:
-    """Mean over ranks of [dep | si | escaped] with one all-reduce (the only exchange)."""
+def allreduce_mean(dist, tensors: list) -> None:
+    """Replace every tensor by its mean over the ranks, with one all-reduce of their
+    concatenation (the replicas' only data exchange)."""
     world = dist.get_world_size()
     if world == 1:
         return
-    n1, n2 = eng.dep.numel(), eng.si.numel()
-    buf = torch.cat([eng.dep, eng.si])
+    sizes = [t.numel() for t in tensors]
+    buf = torch.cat([t.reshape(-1) for t in tensors])
     dist.all_reduce(buf)
     buf /= world
-    eng.dep.copy_(buf[:n1])
-    eng.si.copy_(buf[n1:n1 + n2])
+    o = 0
+    for t, n in zip(tensors, sizes):
+        t.copy_(buf[o:o + n].view_as(t))
+        o += n
+
+
+def replica_mean(dist, values: list, device) -> list:
+    """Mean over the ranks of a few FP64 scalars (one all-reduce)."""
+    world = dist.get_world_size()
+    if world == 1:
+        return [float(v) for v in values]
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t)
+    return [float(x) / world for x in t.cpu()]
+
+
+def average_tallies(dist, eng: Engine) -> None:
+    """Mean over ranks of the deposition and intensity tallies, before the material update,
+    so every replica applies the same material state."""
+    allreduce_mean(dist, [eng.dep, eng.si])
 
 
 def face_temperatures(dim: int, geometry: str, T_boundary, time_now: float, e1: np.ndarray, e2: np.ndarray,
@@ -231,9 +250,7 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
     if conserve_comb_energy:
         internal += comb_disc
     if allreduce is not None and world > 1:
-        t = torch.tensor([rad, comb_disc, boundary_loss], dtype=torch.float64, device=eng.device)
-        allreduce.all_reduce(t)
-        rad, comb_disc, boundary_loss = (float(x) / world for x in t.cpu())
+        rad, comb_disc, boundary_loss = replica_mean(allreduce, [rad, comb_disc, boundary_loss], eng.device)
     if not use_scalar_intensity_Tr:
         state.refresh_host()
     else:

@@ -24,7 +24,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._gray import GrayState, _host_copy, average_tallies, face_temperatures
+from ._gray import GrayState, _host_copy, average_tallies, face_temperatures, replica_mean
 from .engine import A_RAD, C_LIGHT, Engine
 from .materials import evaluate
 
@@ -251,9 +251,7 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
     boundary_emission = float(sum(sm.e_side))
     boundary_loss = float(sum(sm.escaped))
     if _allreduce is not None and world > 1:
-        t = torch.tensor([rad, comb_disc, boundary_loss], dtype=torch.float64, device=eng.device)
-        _allreduce.all_reduce(t)
-        rad, comb_disc, boundary_loss = (float(x) / world for x in t.cpu())
+        rad, comb_disc, boundary_loss = replica_mean(_allreduce, [rad, comb_disc, boundary_loss], eng.device)
     total = internal + rad
     dE = total - state.previous_total_energy
     residual = dE - boundary_emission + boundary_loss - float(sm.source_emission)
