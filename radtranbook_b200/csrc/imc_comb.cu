@@ -22,14 +22,22 @@ __device__ __forceinline__ int bin_of(const CombArgs& a, long long k) {
   return a.per_group ? a.cell[k] + a.nc * a.group[k] : a.cell[k];
 }
 
+constexpr int ECH = 4096;       // consecutive entries per k_comb_ecen block
+constexpr int EBINS = 1024;     // shared-memory bins per block
+
+// Each block sums a contiguous run of ECH entries into its shared bins (warp groups first),
+// then adds one value per distinct bin to ecen.
 __global__ void __launch_bounds__(256) k_comb_ecen(CombArgs a) {
+  __shared__ BlockBins<EBINS> t;
   __shared__ WarpStage stages[8];
   WarpStage* st = stages + (threadIdx.x >> 5);
-  const long long stride = (long long)gridDim.x * blockDim.x;
+  bins_init(t);
+  __syncthreads();
   const long long n_in = *a.d_n_in;
+  const long long base = (long long)blockIdx.x * ECH;
   // block-uniform trip count keeps every warp converged for the aggregated reduction
-  for (long long base = (long long)blockIdx.x * blockDim.x; base < n_in; base += stride) {
-    const long long k = base + threadIdx.x;
+  for (int i = 0; i < ECH; i += 256) {
+    const long long k = base + i + threadIdx.x;
     bool live = false;
     int b = 0;
     double w = 0.0;
@@ -37,13 +45,18 @@ __global__ void __launch_bounds__(256) k_comb_ecen(CombArgs a) {
       const float wf = a.w[k];
       if (wf > 0.f) { live = true; b = bin_of(a, k); w = (double)wf; }
     }
-    warp_tally1(live, b, w, a.ecen, st);
+    warp_bins_add(live, b, w, t, a.ecen, st);
   }
+  __syncthreads();
+  bins_flush(t, a.ecen);
 }
 
 __global__ void __launch_bounds__(CB) k_comb_count(CombArgs a) {
   __shared__ long long sh[CB / 32];
   __shared__ WarpStage stages[CB / 32];
+  __shared__ BlockBins<CB> t;
+  bins_init(t);
+  __syncthreads();
   const long long k = (long long)blockIdx.x * CB + threadIdx.x;
   const long long n_in = *a.d_n_in;
   int n = 0, b = 0;
@@ -59,11 +72,12 @@ __global__ void __launch_bounds__(CB) k_comb_count(CombArgs a) {
     }
     a.cnt[k] = n;
   }
-  // copies per bin: warp-aggregated (the bank is largely grouped by cell)
-  warp_tally1(n > 0, b, (double)n, a.ncopy, stages + (threadIdx.x >> 5));
+  // copies per bin: aggregated per warp, then per block (the bank is largely grouped by cell)
+  warp_bins_add(n > 0, b, (double)n, t, a.ncopy, stages + (threadIdx.x >> 5));
   const unsigned ws = __reduce_add_sync(FULL, (unsigned)n);
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = ws;
   __syncthreads();
+  bins_flush(t, a.ncopy);
   if (threadIdx.x < 32) {
     unsigned long long v = sh[threadIdx.x];
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
@@ -148,18 +162,12 @@ __global__ void k_comb_disc(CombArgs a) {
   if ((threadIdx.x & 31) == 0 && after != 0.0) atomicAdd(&a.sum->comb_after, after);
 }
 
-int grid_for(long long n, int block) {
-  long long g = (n + block - 1) / block;
-  if (g > 148LL * 16) g = 148LL * 16;
-  return (int)(g < 1 ? 1 : g);
-}
-
 }  // namespace
 
 cudaError_t imc_launch_comb_ecen(const CombArgs& a, cudaStream_t s) {
   if (a.n_bound <= 0) return cudaSuccess;
   ++g_imc_launches;
-  k_comb_ecen<<<grid_for(a.n_bound, 256), 256, 0, s>>>(a);
+  k_comb_ecen<<<(unsigned)((a.n_bound + ECH - 1) / ECH), 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -147,6 +147,62 @@ __device__ __forceinline__ void warp_tally1(bool flush, int key, double va, doub
   __syncwarp();
 }
 
+// ---- block-aggregated per-bin sums ----
+// The census of a step piles up in a few cells (the hottest radiation), so even after
+// per-warp aggregation thousands of FP64 atomics land on each of those addresses and
+// serialise in the L2.  A block first sums its (bin, value) pairs in a shared-memory hash
+// table (per-warp groups add once), then flushes one global atomic per distinct bin.
+// Probing is bounded: a bin that finds no slot in BINS_PROBES tries adds to global memory.
+constexpr int BINS_PROBES = 8;
+template <int S>
+struct BlockBins {
+  int key[S];
+  double val[S];
+};
+
+template <int S>
+__device__ __forceinline__ void bins_init(BlockBins<S>& t) {
+  for (int i = threadIdx.x; i < S; i += blockDim.x) { t.key[i] = -1; t.val[i] = 0.0; }
+}
+
+template <int S>
+__device__ __forceinline__ void bins_add(BlockBins<S>& t, int bin, double v, double* __restrict__ global) {
+  const unsigned h = ((unsigned)bin * 2654435761u) >> 8;
+#pragma unroll 1
+  for (int p = 0; p < BINS_PROBES; ++p) {
+    const int s = (int)((h + (unsigned)p) & (unsigned)(S - 1));
+    const int old = atomicCAS(&t.key[s], -1, bin);
+    if (old == -1 || old == bin) { atomicAdd(&t.val[s], v); return; }
+  }
+  atomicAdd(global + bin, v);
+}
+
+// warp_tally1 whose group sums go into the block's table (every lane calls it, converged)
+template <int S>
+__device__ __forceinline__ void warp_bins_add(bool flush, int key, double v, BlockBins<S>& t,
+                                              double* __restrict__ global, WarpStage* st) {
+  const unsigned fm = __ballot_sync(FULL, flush);
+  if (fm == 0u) return;
+  const int lane = threadIdx.x & 31;
+  const unsigned peers = __match_any_sync(FULL, flush ? key : -1 - lane);
+  st->a[lane] = v;
+  __syncwarp();
+  if (flush && (__ffs(peers) - 1) == lane) {
+    double s = 0.0;
+    unsigned m = peers;
+    while (m) { const int l = __ffs(m) - 1; m &= m - 1; s += st->a[l]; }
+    bins_add(t, key, s, global);
+  }
+  __syncwarp();
+}
+
+// after a __syncthreads(): one global atomic per occupied slot
+template <int S>
+__device__ __forceinline__ void bins_flush(BlockBins<S>& t, double* __restrict__ global) {
+  for (int i = threadIdx.x; i < S; i += blockDim.x)
+    if (t.key[i] >= 0) atomicAdd(global + t.key[i], t.val[i]);
+}
+
 // ---- energy tallies in 64-bit fixed point ----
 // Deposited and escaped energy are summed as integers in units of q = W * 2^-60, W the
 // total weight tracked in the step (an upper bound of every such sum, so no total exceeds
