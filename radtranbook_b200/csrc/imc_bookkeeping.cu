@@ -12,6 +12,7 @@
 //   IC             IMC/IMC1D.py:220-248, 535-575; IMC/IMC2D.py:1110-1188
 //   material       IMC/IMC1D.py:1021-1035; IMC/IMC2D.py:1801-1810
 //   comb targets   IMC/IMC1D.py:786-799; IMC/IMC2D.py:1461-1468
+#include <algorithm>
 #include <cmath>
 #include "imc_block.cuh"
 #include "imc_device.cuh"
@@ -25,18 +26,17 @@ constexpr double PI = 3.14159265358979323846;
 using imcblk::NT;
 using namespace imcblk;
 
-__global__ void __launch_bounds__(NT) k_plan(PlanArgs a) {
-  __shared__ double red[NT];
-  __shared__ long long sh[NT];
-  const int t = threadIdx.x;
-  const int nc = a.nc;
-  for (int q = t; q <= a.nx; q += NT) a.e1f[q] = (float)a.e1[q];
-  for (int q = t; q <= a.ny; q += NT) a.e2f[q] = (float)a.e2[q];
+// Per-cell part of the plan, one thread per cell: Fleck factor, absorption / effective
+// scatter tables, emission energy, linear tilt constants, FP32 edges.
+__global__ void k_plan_cells(PlanArgs a) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c <= a.nx) a.e1f[c] = (float)a.e1[c];
+  if (c <= a.ny) a.e2f[c] = (float)a.e2[c];
+  if (c >= a.nc) return;
   const bool oned = (a.geom == G_SLAB || a.geom == G_SPHERE);
-
   // ---- Fleck factor and emission energy per cell (gray) ----
   const double sa_thr = oned ? 1e-10 : 1e-12;  // IMC/IMC1D.py:117, IMC/IMC2D.py:917
-  for (int c = t; c < nc; c += NT) {
+  {
     const double T = a.T[c];
     if (!isfinite(T) || (oned && !(T > 0.0)) || !isfinite(a.sigma[c]) || !(a.cv[c] > 0.0))
       atomicOr(&a.sum->flags, (int)IMC_FLAG_NONFINITE);
@@ -53,15 +53,8 @@ __global__ void __launch_bounds__(NT) k_plan(PlanArgs a) {
     if (a.t_emit_floor > 0.0 && T < a.t_emit_floor) E = 0.0;
     a.emit_E[c] = E;
   }
-  __syncthreads();
-
-  // ---- emission counts / weights / offsets ----
-  const long long n_emit = plan_volume(a.emit_E, a.n_target, a.nx, a.ny, nc, a.emit_n, a.emit_off,
-                                       a.emit_w, a.emitted, red, sh);
-  const double e_emit = block_canon_sum(a.emitted, nc, red);
-
   // ---- tilt constants (emission; fixed-source RZ tilt uses the same T) ----
-  for (int c = t; c < nc; c += NT) {
+  {
     const int i = c % a.nx, j = c / a.nx;
     double* tl = a.tilt + 4 * c;
     tl[0] = tl[1] = tl[2] = tl[3] = 0.0;
@@ -113,7 +106,19 @@ __global__ void __launch_bounds__(NT) k_plan(PlanArgs a) {
       tl[0] = ar; tl[1] = Mloc; tl[2] = Pn;
     }
   }
-  __syncthreads();
+}
+
+__global__ void __launch_bounds__(NT) k_plan(PlanArgs a) {
+  __shared__ double red[NT];
+  __shared__ long long sh[NT];
+  const int t = threadIdx.x;
+  const int nc = a.nc;
+  const bool oned = (a.geom == G_SLAB || a.geom == G_SPHERE);
+
+  // ---- emission counts / weights / offsets ----
+  const long long n_emit = plan_volume(a.emit_E, a.n_target, a.nx, a.ny, nc, a.emit_n, a.emit_off,
+                                       a.emit_w, a.emitted, red, sh);
+  const double e_emit = block_canon_sum(a.emitted, nc, red);
 
   // ---- fixed source (reference: only when max(source) > 0) ----
   long long n_src = 0;
@@ -250,7 +255,8 @@ __global__ void __launch_bounds__(NT) k_canon_eV(const double* e, const double* 
 }  // namespace
 
 cudaError_t imc_launch_plan(const PlanArgs& a, cudaStream_t s) {
-  ++g_imc_launches;
+  g_imc_launches += 2;
+  k_plan_cells<<<(std::max(a.nc, std::max(a.nx, a.ny) + 1) + 255) / 256, 256, 0, s>>>(a);
   k_plan<<<1, NT, 0, s>>>(a);
   return cudaGetLastError();
 }
