@@ -6,7 +6,8 @@
 //   3. n_k      = floor(w_k / ew[b] + xi_k), xi from Philox (k, 0, step, TAG_COMB);
 //      per-block totals                                                       k_comb_count
 //   4. exclusive scan of block totals                                         k_comb_scan
-//   5. copies written in bank order (block-local scan + block offset)         k_comb_scatter
+//   5. copies written in bank order (block-local scan + block offset; one
+//      thread per copy)                                                       k_comb_scatter
 //   6. disc[b] = ecen - (copies in b) * FP32(ew)                              k_comb_disc
 // Order of the output bank = order of the input bank, so the result is deterministic.
 #include "imc_device.cuh"
@@ -113,13 +114,18 @@ __global__ void __launch_bounds__(1024) k_comb_scan(long long* blk, long long nb
   }
 }
 
+// One thread per output copy: the tile's copy counts are scanned in shared memory, each
+// thread finds the entry of its copy by a binary search there and gathers the entry's fields
+// (cached: a tile's entries are few), so the output stores are contiguous across the warp.
 __global__ void __launch_bounds__(CB) k_comb_scatter(CombArgs a) {
+  __shared__ int incl[CB];
   __shared__ int sh[CB / 32];
-  const long long k = (long long)blockIdx.x * CB + threadIdx.x;
+  const long long tile0 = (long long)blockIdx.x * CB;
+  const long long k = tile0 + threadIdx.x;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const long long n_in = *a.d_n_in;
   const int n = (k < n_in) ? a.cnt[k] : 0;
-  // block-exclusive scan of n
+  // block-inclusive scan of the copy counts
   int x = n;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) { const int y = __shfl_up_sync(FULL, x, o); if (lane >= o) x += y; }
@@ -132,22 +138,22 @@ __global__ void __launch_bounds__(CB) k_comb_scatter(CombArgs a) {
     sh[lane] = v;
   }
   __syncthreads();
-  const long long start = a.blk[blockIdx.x] + (wid ? sh[wid - 1] : 0) + (x - n);
-  if (n > 0) {
-    const int b = bin_of(a, k);
-    const float wq = (float)a.ew[b];
-    const float p1 = a.p1[k], p2 = a.p2 ? a.p2[k] : 0.f, d1 = a.d1[k], d2 = a.d2 ? a.d2[k] : 0.f;
-    const int c = a.cell[k];
-    const int g = a.group ? a.group[k] : 0;
-    for (int q = 0; q < n; ++q) {
-      const long long o = start + q;
-      if (o >= a.out_capacity) break;  // overflow: flagged by the scan, caller regrows
-      a.op1[o] = p1; a.od1[o] = d1;
-      if (a.op2) a.op2[o] = p2;
-      if (a.od2) a.od2[o] = d2;
-      a.ow[o] = wq; a.ot[o] = 0.f; a.ocell[o] = c;
-      if (a.ogroup) a.ogroup[o] = g;
-    }
+  incl[threadIdx.x] = x + (wid ? sh[wid - 1] : 0);
+  __syncthreads();
+  const int total = incl[CB - 1];
+  const long long out0 = a.blk[blockIdx.x];
+  for (int o = threadIdx.x; o < total; o += CB) {
+    const long long dst = out0 + o;
+    if (dst >= a.out_capacity) break;  // overflow: flagged by the scan, caller regrows
+    int lo = 0, hi = CB - 1;  // the entry j with incl[j-1] <= o < incl[j]
+    while (lo < hi) { const int mid = (lo + hi) >> 1; if (incl[mid] > o) hi = mid; else lo = mid + 1; }
+    const long long src = tile0 + lo;
+    const int b = bin_of(a, src);
+    a.op1[dst] = a.p1[src]; a.od1[dst] = a.d1[src];
+    if (a.op2) a.op2[dst] = a.p2[src];
+    if (a.od2) a.od2[dst] = a.d2[src];
+    a.ow[dst] = (float)a.ew[b]; a.ot[dst] = 0.f; a.ocell[dst] = a.cell[src];
+    if (a.ogroup) a.ogroup[dst] = a.group[src];
   }
 }
 
