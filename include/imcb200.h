@@ -9,16 +9,18 @@
  *                            sigma_a_func, inv_eos, cv, source, reflect, theta, ...)
  *   IMC/IMC2D.py:1591   step(state, ..., edges1, edges2, ..., geometry='xy'|'rz', ...)
  *   MG_IMC/MG_IMC2D.py:1635  step(state, ..., energy_edges, sigma_a_funcs, ...)
+ *   MG_IMC/MG_IMC1D.py:917   step(state, ..., mesh, energy_edges, sigma_a_funcs, ...)
  *
  *   imc_step_transport  = reference lines from the Fleck factor through the transport
  *                         kernel (IMC/IMC1D.py:932-1017, IMC/IMC2D.py:1646-1797,
- *                         MG_IMC/MG_IMC2D.py:1703-1976)
+ *                         MG_IMC/MG_IMC2D.py:1703-1976, MG_IMC/MG_IMC1D.py:941-1140)
  *   imc_material_update = internal_energy += dep - emitted / V; Tr from the path-length
  *                         intensity (IMC/IMC1D.py:1021-1035, IMC/IMC2D.py:1801-1810)
  *   imc_comb            = the stochastic comb (IMC/IMC1D.py:770-828, IMC/IMC2D.py:1448-1511,
- *                         MG_IMC/MG_IMC2D.py:1314-1378)
+ *                         MG_IMC/MG_IMC2D.py:1314-1378, MG_IMC/MG_IMC1D.py:746-847)
  *   imc_init_census     = the equilibrium initial census of init_simulation
- *                         (IMC/IMC1D.py:220-248,535-575; IMC/IMC2D.py:1110-1188)
+ *                         (IMC/IMC1D.py:220-248,535-575; IMC/IMC2D.py:1110-1188;
+ *                         MG_IMC/MG_IMC1D.py:514-566)
  *
  * Conventions
  *   - Every pointer in a struct is DEVICE memory, caller-owned.  The library never
@@ -71,7 +73,9 @@ enum {
 typedef struct imc_mesh {
   int32_t geometry;        /* IMC_GEOM_* */
   int32_t nx, ny;          /* cells per direction; ny = 1 in 1-D */
-  int32_t n_groups;        /* 1 = gray */
+  int32_t n_groups;        /* 1 = gray; > 1 with xy / rz: MG_IMC2D rules; with the
+                              sphere: MG_IMC1D rules (stratified (group, cell) sources,
+                              scatter cap, weight floor 1e-14 * sum / n) */
   const double* edges1;    /* nx+1 (x | r) */
   const double* edges2;    /* ny+1 (y | z); 1-D: {0, 1} */
   const double* volume;    /* nx*ny cell volumes (1-D slab: dx; sphere: 4/3 pi dr^3) */
@@ -95,7 +99,7 @@ typedef struct imc_material {   /* per-cell state at the start of the step (FP64
   const double* temperature;    /* T (keV), [c] */
   const double* sigma;          /* true absorption opacity (1/cm), [g][c] */
   const double* cv;             /* rho c_v (GJ/cm^3/keV), [c] */
-  const double* source;         /* fixed source power density, [c], or NULL */
+  const double* source;         /* fixed source power density, [c] (MG: [g][c]), or NULL */
 } imc_material;
 
 typedef struct imc_step_params {
@@ -108,14 +112,16 @@ typedef struct imc_step_params {
                                    (sides 0/1: ny entries, 2/3: nx entries; 1-D: 1) */
   int64_t max_events;           /* events per history cap (2-D reference); <= 0: none */
   int32_t rz_linear_source;     /* RZ emission with the linear r/z tilt */
-  int32_t mg_reference_rules;   /* unused, must be 0: with n_groups > 1 the MG_IMC2D event
-                                   rules (no scatter cap) always apply */
+  int32_t mg_reference_rules;   /* unused, must be 0: the multigroup event rules follow the
+                                   geometry (MG_IMC2D in xy / rz, MG_IMC1D on the sphere) */
   double t_emit_floor;
   int32_t block_size;           /* tracking launch shape; 0 = tuned default */
   int32_t blocks_per_sm;
   int32_t chunk;                /* histories claimed per warp ticket (guided: at most this) */
   int32_t reserved;             /* bit 0: shared-memory cell table; bit 1: draw prefetch */
   const double* emission_fractions; /* MG: [g] fixed emission spectrum, or NULL = Planck */
+  int64_t n_boundary_side[4];   /* > 0: boundary particles on that side instead of n_boundary
+                                   (per-side budgets, MG_IMC/MG_IMC1D.py:1000-1040) */
 } imc_step_params;
 
 typedef struct imc_tallies {    /* device outputs, overwritten by each step */
@@ -161,7 +167,8 @@ typedef struct imc_step_summary {
   int32_t pad;
   double e_side[4];             /* issued boundary energy per side (GJ) */
   double source_emission, emission_total;
-  double weight_sum;            /* sum of tracked weights; floor = 1e-10 * sum / n_bank */
+  double weight_sum;            /* sum of tracked weights; floor = 1e-10 * sum / n_bank
+                                   (MG sphere: 1e-14) */
   double comb_before, comb_after;
   double internal_energy;       /* sum_c e[c] V[c] after imc_comb_async */
   unsigned long long stats[IMC_STAT_N];
@@ -172,7 +179,8 @@ typedef struct imc_step_summary {
 IMC_API size_t imc_workspace_bytes(const imc_mesh* mesh, int64_t bank_capacity);
 
 /* Equilibrium initial census at radiation temperature tr[c] into an empty bank.
- * (IMC/IMC1D.py:220-248, IMC/IMC2D.py:1110-1188, MG_IMC/MG_IMC2D.py:992-1235) */
+ * (IMC/IMC1D.py:220-248, IMC/IMC2D.py:1110-1188, MG_IMC/MG_IMC2D.py:992-1235,
+ * MG_IMC/MG_IMC1D.py:514-566) */
 IMC_API imc_status imc_init_census(const imc_mesh* mesh, const double* tr, int64_t n_target,
                            double t_emit_floor, uint64_t seed, imc_bank* bank, void* workspace,
                            size_t workspace_bytes, int64_t* n_out, void* stream);
@@ -191,7 +199,14 @@ IMC_API imc_status imc_material_update(const imc_mesh* mesh, const imc_tallies* 
                                double* tr, void* stream);
 
 /* Stochastic comb of bank `in` into bank `out` (census times reset to 0).
- * per_group != 0 combs per (cell, group) bin (MG).  disc[bin] = energy before - after. */
+ * per_group is a set of flags: IMC_COMB_PER_GROUP combs per (cell, group) bin (MG);
+ * IMC_COMB_CONSERVE_RADIATION gives every copy in a bin the bin's pre-comb energy divided
+ * by its copy count (MG_IMC/MG_IMC1D.py:808-820, conserve_comb_energy='radiation').
+ * n_max > 0 combs to n_max; n_max == 0 only drops dead entries (every live entry copied
+ * once with its weight); n_max < 0 combs to |n_max| when at least |n_max| entries are
+ * alive, else only drops dead entries (MG_IMC/MG_IMC1D.py:1194-1200).
+ * disc[bin] = energy before - after. */
+enum { IMC_COMB_PER_GROUP = 1, IMC_COMB_CONSERVE_RADIATION = 2 };
 IMC_API imc_status imc_comb(const imc_mesh* mesh, const imc_bank* in, imc_bank* out, int64_t n_max,
                     uint64_t seed, uint32_t step, int32_t per_group, double* disc,
                     void* workspace, size_t workspace_bytes, imc_comb_report* report,

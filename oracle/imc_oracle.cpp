@@ -15,6 +15,8 @@
  *   multigroup xy/rz MG_IMC/MG_IMC2D.py:202-254 (Planck sampler), 580-771 (events),
  *                    774-989 (history loop), 1237-1267 (emission groups),
  *                    1270-1378 (comb), 1635-2122 (step)
+ *   multigroup 1-D sphere  MG_IMC/MG_IMC1D.py:276-461 (events, history loop), 514-743
+ *                    (IC and sources), 746-847 (comb), 917-1140 (step)
  * It differs from the reference in exactly one way on purpose: random numbers come
  * from Philox-4x32-10 streams keyed by (seed) with counter (index, block, step, tag),
  * the same streams the CUDA path draws, so the two can be compared history by history.
@@ -1023,24 +1025,33 @@ int orc_adjoint_vjp(void* h, const orc_step_in* in, const double* cot, double* g
  *   ew = ecen/desired; copies = floor(w/ew + xi), each of weight ew, in bank order.
  * xi: Philox (pre-comb index k, block 0, step, TAG_COMB).  Sets census times to 0.
  * disc (per bin) = ecen - ecen_after.  Returns the new bank size. */
-long long orc_comb(void* h, long long Nmax, uint32_t step, int per_group, double* disc) {
+/* Stochastic comb.  flags: bit 0 = bins per (cell, group), bit 1 = each bin's copies share
+ * the bin's pre-comb energy equally (MG_IMC/MG_IMC1D.py:808-820, conserve_comb_energy =
+ * 'radiation').  Nmax > 0 combs to Nmax; Nmax == 0 only drops dead entries; Nmax < 0 combs
+ * to |Nmax| when at least |Nmax| entries are alive, else only drops dead entries
+ * (MG_IMC/MG_IMC1D.py:1194-1200).  Surviving entries start the next step at t = 0. */
+long long orc_comb(void* h, long long Nmax, uint32_t step, int flags, double* disc) {
   Oracle* o = (Oracle*)h;
   Problem& P = o->P;
   Bank& B = o->B;
   const int nc = ncells(P);
+  const bool per_group = (flags & 1) != 0, conserve_rad = (flags & 2) != 0;
   const int nb = per_group ? nc * P.ng : nc;
   std::vector<double> ecen(nb, 0.0), ew(nb, 0.0);
   std::vector<long long> ncopy(nb, 0);
   const long long N = (long long)B.size();
   auto bin = [&](long long k) { return per_group ? B.cell[k] + nc * B.grp[k] : B.cell[k]; };
+  long long live = 0;
   {
     std::vector<KSum> acc(nb);
-    for (long long k = 0; k < N; ++k) if (B.w[k] > 0) acc[bin(k)].add(B.w[k]);
+    for (long long k = 0; k < N; ++k) if (B.w[k] > 0) { acc[bin(k)].add(B.w[k]); ++live; }
     for (int b = 0; b < nb; ++b) ecen[b] = acc[b].value();
   }
   double E = 0;
   for (int b = 0; b < nb; ++b) E += ecen[b];
-  if (!(E > 0)) {
+  const bool compact_only = Nmax == 0 || (Nmax < 0 && live < -Nmax);
+  if (Nmax < 0) Nmax = -Nmax;
+  if (!(E > 0) || compact_only) {
     Bank nbk;
     for (long long k = 0; k < N; ++k)
       if (B.w[k] > 0) nbk.push(B.w[k], B.d1[k], B.d2[k], 0.0, B.p1[k], B.p2[k], B.cell[k], B.grp[k]);
@@ -1055,19 +1066,26 @@ long long orc_comb(void* h, long long Nmax, uint32_t step, int per_group, double
     }
   }
   Bank nbk;
+  std::vector<long long> nk(N, 0);
   for (long long k = 0; k < N; ++k) {
     if (!(B.w[k] > 0)) continue;
     const int b = bin(k);
     if (!(ew[b] > 0)) continue;
     Draw4 r = draw(P.seed, (uint32_t)k, 0, step, oracle::TAG_COMB);
-    const long long n = (long long)std::floor(B.w[k] / ew[b] + r.u[0]);
-    for (long long q = 0; q < n; ++q)
-      nbk.push(ew[b], B.d1[k], B.d2[k], 0.0, B.p1[k], B.p2[k], B.cell[k], B.grp[k]);
-    if (n > 0) ncopy[b] += n;
+    nk[k] = (long long)std::floor(B.w[k] / ew[b] + r.u[0]);
+    if (nk[k] > 0) ncopy[b] += nk[k];
+  }
+  std::vector<double> wout(ew);
+  if (conserve_rad)
+    for (int b = 0; b < nb; ++b) wout[b] = ncopy[b] > 0 ? ecen[b] / (double)ncopy[b] : 0.0;
+  for (long long k = 0; k < N; ++k) {
+    const int b = nk[k] > 0 ? bin(k) : 0;
+    for (long long q = 0; q < nk[k]; ++q)
+      nbk.push(wout[b], B.d1[k], B.d2[k], 0.0, B.p1[k], B.p2[k], B.cell[k], B.grp[k]);
   }
   B = nbk;
-  /* energy after the comb in bin b is exactly ncopy * ew (identical copies) */
-  for (int b = 0; b < nb; ++b) disc[b] = ecen[b] - (double)ncopy[b] * ew[b];
+  /* energy after the comb in bin b is exactly ncopy * (copy weight): identical copies */
+  for (int b = 0; b < nb; ++b) disc[b] = ecen[b] - (double)ncopy[b] * wout[b];
   return (long long)B.size();
 }
 
@@ -1108,6 +1126,44 @@ long long orc_comb_with_xi(void* h, long long Nmax, const double* xi, double* di
   return (long long)B.size();
 }
 
+/* per-(cell, group) comb with caller-supplied uniforms (one per live entry, pre-comb
+ * order), for the pin against MG_IMC/MG_IMC1D.py:746-847 _comb_mg_1d; bit 1 of flags
+ * shares each bin's energy equally among its copies ('radiation') */
+long long orc_comb_mg_with_xi(void* h, long long Nmax, const double* xi, int flags, double* disc) {
+  Oracle* o = (Oracle*)h;
+  Problem& P = o->P;
+  Bank& B = o->B;
+  const int nc = ncells(P), nb = nc * P.ng;
+  std::vector<double> ecen(nb, 0.0), ew(nb, 0.0), wout(nb, 0.0);
+  std::vector<long long> ncopy(nb, 0);
+  const long long N = (long long)B.size();
+  for (long long k = 0; k < N; ++k) if (B.w[k] > 0) ecen[B.cell[k] + nc * B.grp[k]] += B.w[k];
+  double E = 0;
+  for (int b = 0; b < nb; ++b) E += ecen[b];
+  for (int b = 0; b < nb; ++b)
+    if (ecen[b] > 0) ew[b] = ecen[b] / std::max(1.0, std::nearbyint((double)Nmax * ecen[b] / E));
+  std::vector<long long> nk(N, 0);
+  long long live = 0;
+  for (long long k = 0; k < N; ++k) {
+    if (!(B.w[k] > 0)) continue;
+    const double x = xi[live++];
+    const int b = B.cell[k] + nc * B.grp[k];
+    if (!(ew[b] > 0)) continue;
+    nk[k] = (long long)std::floor(B.w[k] / ew[b] + x);
+    ncopy[b] += nk[k];
+  }
+  for (int b = 0; b < nb; ++b) wout[b] = (flags & 2) ? (ncopy[b] > 0 ? ecen[b] / (double)ncopy[b] : 0.0) : ew[b];
+  Bank nbk;
+  for (long long k = 0; k < N; ++k) {
+    const int b = B.cell[k] + nc * B.grp[k];
+    for (long long q = 0; q < nk[k]; ++q)
+      nbk.push(wout[b], B.d1[k], B.d2[k], B.t[k], B.p1[k], B.p2[k], B.cell[k], B.grp[k]);
+  }
+  B = nbk;
+  for (int b = 0; b < nb; ++b) disc[b] = ecen[b] - (double)ncopy[b] * wout[b];
+  return (long long)B.size();
+}
+
 }  // extern "C"
 
 /* =====================================================================================
@@ -1120,6 +1176,17 @@ namespace {
  * standard expansions of the incomplete Planck integral; Widger & Woodall, Bull. Amer.
  * Meteor. Soc. 57 (1976) 1217).  Stands in for the external planck_integrals module
  * (MG_IMC/MG_IMC2D.py:62) whose group fractions the step normalises anyway. */
+/* sum_k e^{-kx}(x^3/k + 3x^2/k^2 + 6x/k^3 + 6/k^4) = (pi^4/15)(1 - F(x)), for x >= 1 */
+double planck_tail(double x) {
+  double tail = 0.0;
+  const int K = (int)(2.0 + 40.0 / x);
+  for (int k = K; k >= 1; --k) {
+    const double kx = k * x, ik = 1.0 / k;
+    tail += std::exp(-kx) * ik * (x * x * x + ik * (3.0 * x * x + ik * (6.0 * x + ik * 6.0)));
+  }
+  return tail;
+}
+
 double planck_F(double x) {
   const double c = 15.0 / (PI * PI * PI * PI);
   if (!(x > 0.0)) return 0.0;
@@ -1136,20 +1203,22 @@ double planck_F(double x) {
     }
     return c * sum;
   }
-  double tail = 0.0;
-  const int K = (int)(2.0 + 40.0 / x);
-  for (int k = K; k >= 1; --k) {
-    const double kx = k * x, ik = 1.0 / k;
-    tail += std::exp(-kx) * ik * (x * x * x + ik * (3.0 * x * x + ik * (6.0 * x + ik * 6.0)));
-  }
-  return 1.0 - c * tail;
+  return 1.0 - c * planck_tail(x);
+}
+
+/* F(x1) - F(x0); above x = 1 as a difference of tails, which keeps its relative precision
+ * far into the Wien tail (1 - F cancels to 0 there) */
+double planck_frac(double x0, double x1) {
+  if (!(x1 > x0)) return 0.0;
+  if (x0 >= 1.0) return 15.0 / (PI * PI * PI * PI) * (planck_tail(x0) - planck_tail(x1));
+  return planck_F(x1) - planck_F(x0);
 }
 
 /* normalised group fractions b*_g of the Planck spectrum at T (sum = 1 unless T <= 0) */
 void planck_fractions(const double* edges, int G, double T, double* b) {
   double tot = 0.0;
   for (int g = 0; g < G; ++g) {
-    const double f = (T > 0.0) ? planck_F(edges[g + 1] / T) - planck_F(edges[g] / T) : 0.0;
+    const double f = (T > 0.0) ? planck_frac(edges[g] / T, edges[g + 1] / T) : 0.0;
     b[g] = f > 0.0 ? f : 0.0;
     tot += b[g];
   }
@@ -1170,14 +1239,17 @@ const MixCdf& mixcdf() { static MixCdf m; return m; }
 
 /* group of a photon sampled from the Planck spectrum at T (MG_IMC/MG_IMC2D.py:202-254):
  * n from the 1/n^4 mixture, x = (sum of four Exp(1)) / n, energy T*x, group by edges */
-int planck_group(double T, const double* edges, int G, double un, double u1, double u2, double u3, double u4) {
+int planck_group(double T, const double* edges, int G, double un, double u1, double u2, double u3, double u4,
+                 bool below_to_last = false) {
   if (!(T > 0.0)) return 0;
   const MixCdf& m = mixcdf();
   double ns = 200.0;
   for (int i = 0; i < 200; ++i) if (un <= m.cdf[i]) { ns = (double)(i + 1); break; }
   const double x = (-std::log(u1) - std::log(u2) - std::log(u3) - std::log(u4)) / ns;
   const double f = T * x;
-  if (f < edges[0]) return 0;
+  /* MG_IMC/MG_IMC1D.py:180-186 assigns an energy below the lowest edge to the last group;
+   * MG_IMC/MG_IMC2D.py:242-243 to the first.  Each module's rule is kept. */
+  if (f < edges[0]) return below_to_last ? G - 1 : 0;
   if (f >= edges[G]) return G - 1;
   for (int g = 0; g < G; ++g) if (f >= edges[g] && f < edges[g + 1]) return g;
   return G - 1;
@@ -1224,6 +1296,9 @@ double orc_planck_F(double x) { return planck_F(x); }
 void orc_planck_fractions(const double* edges, int G, double T, double* b) { planck_fractions(edges, G, T, b); }
 int orc_planck_group(double T, const double* edges, int G, const double* u) {
   return planck_group(T, edges, G, u[0], u[1], u[2], u[3], u[4]);
+}
+int orc_planck_group_mg1d(double T, const double* edges, int G, const double* u) {
+  return planck_group(T, edges, G, u[0], u[1], u[2], u[3], u[4], true);
 }
 
 typedef struct {
@@ -1524,6 +1599,271 @@ int orc_step_transport_mg(void* h, const orc_mg_in* in, orc_mg_out* out) {
       if (dcen > 0 && w <= floor_w) { st[S_FLOOR]++; break; }
     }
     B.w[k] = w; B.d1[k] = d1; B.d2[k] = d2; B.p1[k] = p1; B.p2[k] = p2; B.cell[k] = c;
+  }
+  for (size_t q = 0; q < ncg; ++q) {
+    KSum d, s2;
+    for (int t = 0; t < nth; ++t) { d.add(dep_t[t][q].value()); s2.add(si_t[t][q].value()); }
+    out->dep[q] = d.value(); out->si[q] = s2.value();
+  }
+  for (int s2 = 0; s2 < S_N; ++s2) { out->stats[s2] = 0; for (int t = 0; t < nth; ++t) out->stats[s2] += st_t[t][s2]; }
+  for (int q = 0; q < 4 + G; ++q) {
+    KSum x;
+    for (int t = 0; t < nth; ++t) x.add(esc_t[t][q].value());
+    if (q < 4) out->escaped[q] = x.value(); else out->esc_by_group[q - 4] = x.value();
+  }
+  return 0;
+}
+
+}  // extern "C"
+
+/* =====================================================================================
+ * Multigroup 1-D sphere (MG_IMC/MG_IMC1D.py)
+ *
+ * Sources are stratified per (group, cell) bin, bins in the reference's g-outer / i-inner
+ * order: n_b = max(1, round(N E_b / E)) for emitting bins (fixed source: round, no
+ * minimum), weight E_b / n_b, radius uniform in the shell's volume, mu ~ U(-1, 1).
+ * Tracking is the gray spherical event with group-indexed opacities, the sigma_s*dr > 1e4
+ * cap, a weight floor of 1e-14 * sum(w) / N and the floor kill after every event.
+ * Draws per particle k of a source: blocks 0 (radius, -, direction, -) and 1 (time, then
+ * the Planck group sampler's five uniforms with block 2 for the IC).
+ * =================================================================================== */
+namespace {
+
+/* stratified (group, cell) counts; minimum one per positive bin when min1 */
+long long strat_counts(const std::vector<double>& E, long long N, bool min1, std::vector<long long>& n) {
+  const long long nb = (long long)E.size();
+  n.assign(nb, 0);
+  const double Et = canon_sum(E.data(), nb);
+  if (N <= 0 || !(Et > 0)) return 0;
+  long long tot = 0;
+  for (long long b = 0; b < nb; ++b) {
+    if (!(E[b] > 0)) continue;
+    const double r = std::nearbyint((double)N * E[b] / Et);
+    n[b] = min1 ? std::max(1LL, (long long)r) : std::max(0LL, (long long)r);
+    tot += n[b];
+  }
+  return tot;
+}
+
+/* append the particles of stratified bins (b = g*nc + c); returns the energy issued */
+double strat_fill(const Problem& P, const std::vector<double>& E, const std::vector<long long>& n, double dt,
+                  uint32_t step, uint32_t tag, Bank& B) {
+  const int nc = ncells(P);
+  double total = 0.0;
+  uint32_t k = 0;
+  for (size_t b = 0; b < E.size(); ++b) {
+    if (n[b] <= 0) continue;
+    const int g = (int)(b / nc), c = (int)(b % nc);
+    const double wgt = E[b] / (double)n[b];
+    const double r0 = P.e1[c], r1 = P.e1[c + 1];
+    for (long long q = 0; q < n[b]; ++q, ++k) {
+      Draw4 r = draw(P.seed, k, 0, step, tag);
+      Draw4 s = draw(P.seed, k, 1, step, tag);
+      double p1 = std::cbrt(r0 * r0 * r0 + (r1 * r1 * r1 - r0 * r0 * r0) * r.u[0]);
+      p1 = std::min(std::max(p1, r0), r1);
+      B.push(wgt, 2.0 * r.u[2] - 1.0, 0.0, s.u[0] * dt, p1, 0.0, c, g);
+      total += wgt;
+    }
+  }
+  return total;
+}
+
+}  // namespace
+
+extern "C" {
+
+/* initial census, MG_IMC/MG_IMC1D.py:514-566: per shell max(1, round(N E_i / E)) particles
+ * of weight E_i / n_i (E_i = a Tr^4 V, zero below T_emit_floor), group from the Planck
+ * spectrum at the shell's Tr.  Draws: k, blocks 0-2, step 0, TAG_IC. */
+long long orc_init_ic_mg1d(void* h, long long N, const double* Tr, const double* edges, double T_emit_floor) {
+  Oracle* o = (Oracle*)h;
+  Problem& P = o->P;
+  Bank& B = o->B;
+  B.resize(0);
+  const int nc = ncells(P), G = P.ng;
+  std::vector<double> E(nc);
+  for (int c = 0; c < nc; ++c) {
+    E[c] = A_RAD * pow4(Tr[c]) * P.vol[c];
+    if (T_emit_floor > 0 && Tr[c] < T_emit_floor) E[c] = 0;
+  }
+  std::vector<long long> n;
+  strat_counts(E, N, true, n);
+  uint32_t k = 0;
+  for (int c = 0; c < nc; ++c) {
+    if (n[c] <= 0) continue;
+    const double wgt = E[c] / (double)n[c];
+    const double r0 = P.e1[c], r1 = P.e1[c + 1];
+    for (long long q = 0; q < n[c]; ++q, ++k) {
+      Draw4 r = draw(P.seed, k, 0, 0, oracle::TAG_IC);
+      Draw4 s = draw(P.seed, k, 1, 0, oracle::TAG_IC);
+      Draw4 d = draw(P.seed, k, 2, 0, oracle::TAG_IC);
+      double p1 = std::cbrt(r0 * r0 * r0 + (r1 * r1 * r1 - r0 * r0 * r0) * r.u[0]);
+      p1 = std::min(std::max(p1, r0), r1);
+      const int g = planck_group(Tr[c], edges, G, s.u[1], s.u[2], s.u[3], d.u[0], d.u[1], true);
+      B.push(wgt, 2.0 * r.u[2] - 1.0, 0.0, 0.0, p1, 0.0, c, g);
+    }
+  }
+  return (long long)B.size();
+}
+
+/* one MG_IMC1D step up to the material update (MG_IMC/MG_IMC1D.py:917-1140):
+ * Fleck with the Planck-mean opacity, boundary (inner, outer) | fixed source | emission,
+ * then transport (MG_IMC/MG_IMC1D.py:367-461).  source is [g][c] (a gray source is
+ * placed in group 0 by the caller, as the reference does). */
+int orc_step_transport_mg1d(void* h, const orc_mg_in* in, orc_mg_out* out) {
+  Oracle* o = (Oracle*)h;
+  Problem& P = o->P;
+  Bank& B = o->B;
+  if (P.geom != G_SPHERE) return 2;
+  const int nc = ncells(P), G = P.ng;
+  const size_t ncg = (size_t)nc * G;
+  const double* edges = in->group_edges;
+  std::vector<double> bstar(ncg), sa(ncg), ss(ncg), b(G);
+  for (int c = 0; c < nc; ++c) {
+    planck_fractions(edges, G, in->T[c], b.data());
+    double sp = 0.0;
+    for (int g = 0; g < G; ++g) { bstar[(size_t)g * nc + c] = b[g]; sp += in->sigma[(size_t)g * nc + c] * b[g]; }
+    const double T = in->T[c];
+    const double beta = 4.0 * A_RAD * pow3(T) / in->cv[c];
+    double f = 1.0 / (1.0 + in->theta * beta * sp * C_LIGHT * in->dt);
+    f = std::min(1.0, std::max(0.0, f));
+    for (int g = 0; g < G; ++g) {
+      const size_t q = (size_t)g * nc + c;
+      sa[q] = in->sigma[q] * f;
+      ss[q] = in->sigma[q] * (1.0 - f);
+    }
+  }
+  std::copy(sa.begin(), sa.end(), out->sigma_a);
+  std::copy(ss.begin(), ss.end(), out->sigma_s);
+  for (int g = 0; g < G; ++g) { out->bnd_by_group[g] = 0; out->esc_by_group[g] = 0; }
+  for (int q = 0; q < 4; ++q) { out->bnd_by_side[q] = 0; out->escaped[q] = 0; }
+
+  /* ---- boundary, MG_IMC/MG_IMC1D.py:653-676: a c T^4 / 4 * 4 pi R^2 * dt on the inner
+   * (outward) and outer (inward) sphere, half-Lambertian, Planck group at the face T ---- */
+  double bnd_total = 0.0;
+  for (int side = 0; side < 2; ++side) {
+    const double* Tf = in->face_T[side];
+    if (!Tf || in->Nboundary <= 0) continue;
+    const double R = side == 0 ? P.e1[0] : P.e1[P.nx];
+    const double T = Tf[0];
+    const double Et = (T > 0) ? A_RAD * C_LIGHT * T * T * T * T / 4.0 * (4.0 * PI * R * R) * in->dt : 0.0;
+    if (!(Et > 0)) continue;
+    const long long n = in->Nboundary;
+    const double wgt = Et / (double)n;
+    for (long long k = 0; k < n; ++k) {
+      Draw4 a = draw(P.seed, (uint32_t)k, 0, in->step, oracle::TAG_BOUNDARY | side);
+      Draw4 bb = draw(P.seed, (uint32_t)k, 1, in->step, oracle::TAG_BOUNDARY | side);
+      Draw4 d = draw(P.seed, (uint32_t)k, 2, in->step, oracle::TAG_BOUNDARY | side);
+      const double mu_n = std::sqrt(a.u[2]);
+      const int g = planck_group(T, edges, G, bb.u[1], bb.u[2], bb.u[3], d.u[0], d.u[1], true);
+      B.push(wgt, side == 0 ? mu_n : -mu_n, 0.0, bb.u[0] * in->dt, R, 0.0, side == 0 ? 0 : P.nx - 1, g);
+      out->bnd_by_group[g] += wgt;
+      out->bnd_by_side[side] += wgt;
+      bnd_total += wgt;
+    }
+  }
+  out->boundary_emission = bnd_total;
+
+  /* ---- fixed source, MG_IMC/MG_IMC1D.py:679-743 (only when max(source) > 0) ---- */
+  out->source_emission = 0.0;
+  if (in->source && in->Nsource > 0) {
+    double smax = 0.0;
+    for (size_t q = 0; q < ncg; ++q) smax = std::max(smax, in->source[q]);
+    if (smax > 0) {
+      std::vector<double> QV(ncg);
+      for (int g = 0; g < G; ++g)
+        for (int c = 0; c < nc; ++c) QV[(size_t)g * nc + c] = in->source[(size_t)g * nc + c] * P.vol[c] * in->dt;
+      std::vector<long long> n;
+      strat_counts(QV, in->Nsource, false, n);
+      out->source_emission = strat_fill(P, QV, n, in->dt, in->step, oracle::TAG_SOURCE, B);
+    }
+  }
+
+  /* ---- emission, MG_IMC/MG_IMC1D.py:569-650 ---- */
+  std::vector<double> Egc(ncg, 0.0);
+  for (int c = 0; c < nc; ++c) {
+    const double T = in->T[c];
+    if (in->T_emit_floor > 0 && T < in->T_emit_floor) continue;
+    for (int g = 0; g < G; ++g) {
+      const size_t q = (size_t)g * nc + c;
+      Egc[q] = A_RAD * C_LIGHT * pow4(T) * sa[q] * bstar[q] * in->dt * P.vol[c];
+    }
+  }
+  for (int c = 0; c < nc; ++c) out->emitted[c] = 0.0;
+  out->emission_total = 0.0;
+  if (in->Ntarget > 0) {
+    std::vector<long long> n;
+    strat_counts(Egc, in->Ntarget, true, n);
+    const size_t n0 = B.size();
+    out->emission_total = strat_fill(P, Egc, n, in->dt, in->step, oracle::TAG_EMISSION, B);
+    std::vector<KSum> em(nc);
+    for (size_t k = n0; k < B.size(); ++k) em[B.cell[k]].add(B.w[k]);
+    for (int c = 0; c < nc; ++c) out->emitted[c] = em[c].value();
+  }
+  if (in->sources_only) return 0;
+
+  /* ---- transport, MG_IMC/MG_IMC1D.py:367-461; weight floor :1127 ---- */
+  const long long N = (long long)B.size();
+  double wsum = 0;
+  for (long long k = 0; k < N; ++k) wsum += B.w[k];
+  const double floor_w = 1e-14 * wsum / (double)std::max(N, 1LL);
+  out->weight_floor = floor_w;
+  out->n_transported = N;
+  int nth = in->nthreads > 0 ? in->nthreads : 1;
+#ifndef _OPENMP
+  nth = 1;
+#endif
+  std::vector<std::vector<KSum>> dep_t(nth, std::vector<KSum>(ncg)), si_t(nth, std::vector<KSum>(ncg));
+  std::vector<std::vector<long long>> st_t(nth, std::vector<long long>(S_N, 0));
+  std::vector<std::vector<KSum>> esc_t(nth, std::vector<KSum>(4 + G));
+  const double dt = in->dt;
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nth)
+  for (long long k = 0; k < N; ++k) {
+    int tid = 0;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+#endif
+    KSum* dep = dep_t[tid].data();
+    KSum* si = si_t[tid].data();
+    long long* st = st_t[tid].data();
+    KSum* esc = esc_t[tid].data();
+    double w = B.w[k], mu = B.d1[k], r = B.p1[k];
+    int c = B.cell[k];
+    const int g = B.grp[k];
+    /* a zero-weight entry carries nothing (the reference moves it without effect) */
+    if (!(w > 0)) continue;
+    double dcen = (dt - B.t[k]) * C_LIGHT;
+    uint32_t ev = 0;
+    while (dcen > 0) {
+      const size_t q = (size_t)g * nc + c;
+      Draw4 u = draw(P.seed, (uint32_t)k, ev, in->step, oracle::TAG_TRANSPORT);
+      ++ev;
+      st[S_EVENTS]++;
+      EventOut e = event_sphere(w, mu, r, P.e1[c], P.e1[c + 1], sa[q], ss[q], dcen, u.u[0], u.u[1]);
+      if (e.evt == EV_BOUNDARY) st[S_BOUNDARY]++; else if (e.evt == EV_SCATTER) st[S_SCATTER]++; else st[S_CENSUS]++;
+      dep[q].add(e.dep);
+      si[q].add(e.dep_i / dt);
+      w = e.w; mu = e.d1; r = e.p1; dcen = e.dcen;
+      bool escaped = false;
+      if (e.cross != X_NONE) {
+        int i = c + (e.cross == X_IP ? 1 : -1);
+        const int side = i < 0 ? 0 : (i >= P.nx ? 1 : -1);
+        if (side >= 0) {
+          if (in->reflect[side]) { mu = -mu; i = side == 0 ? 0 : P.nx - 1; st[S_REFLECT]++; }
+          else { esc[side].add(w); esc[4 + g].add(w); st[S_ESCAPE]++; w = 0; dcen = 0; escaped = true; }
+        }
+        if (!escaped) c = i;
+      }
+      if (!escaped && w < floor_w) {
+        /* MG_IMC/MG_IMC1D.py:439-452: kill, the remainder deposited in the current shell */
+        const size_t q2 = (size_t)g * nc + c;
+        st[S_FLOOR]++;
+        dep[q2].add(w / P.vol[c]);
+        if (sa[q2] > 1e-10) si[q2].add(w / dt / sa[q2] / P.vol[c]);
+        w = 0; dcen = 0;
+      }
+    }
+    B.w[k] = w; B.d1[k] = mu; B.p1[k] = r; B.cell[k] = c;
   }
   for (size_t q = 0; q < ncg; ++q) {
     KSum d, s2;

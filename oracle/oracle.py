@@ -92,11 +92,19 @@ def load():
         lib.orc_init_ic_mg.argtypes = [c_void_p, c_longlong, c_void_p, c_void_p, c_double]
         lib.orc_step_transport_mg.restype = c_int
         lib.orc_step_transport_mg.argtypes = [c_void_p, POINTER(MgIn), POINTER(MgOut)]
+        lib.orc_init_ic_mg1d.restype = c_longlong
+        lib.orc_init_ic_mg1d.argtypes = [c_void_p, c_longlong, c_void_p, c_void_p, c_double]
+        lib.orc_step_transport_mg1d.restype = c_int
+        lib.orc_step_transport_mg1d.argtypes = [c_void_p, POINTER(MgIn), POINTER(MgOut)]
+        lib.orc_comb_mg_with_xi.restype = c_longlong
+        lib.orc_comb_mg_with_xi.argtypes = [c_void_p, c_longlong, c_void_p, c_int, c_void_p]
         lib.orc_planck_F.restype = c_double
         lib.orc_planck_F.argtypes = [c_double]
         lib.orc_planck_fractions.argtypes = [c_void_p, c_int, c_double, c_void_p]
         lib.orc_planck_group.restype = c_int
         lib.orc_planck_group.argtypes = [c_double, c_void_p, c_int, c_void_p]
+        lib.orc_planck_group_mg1d.restype = c_int
+        lib.orc_planck_group_mg1d.argtypes = [c_double, c_void_p, c_int, c_void_p]
         lib.orc_philox.argtypes = [c_void_p, c_void_p, c_void_p]
         for f in ("orc_slab_linear", "orc_sphere_cdf", "orc_rz_r_cdf"):
             getattr(lib, f).restype = c_double
@@ -242,9 +250,19 @@ class Oracle:
         ge = np.ascontiguousarray(group_edges, dtype=np.float64)
         return int(self.lib.orc_init_ic_mg(self.h, int(N), _p(tr), _p(ge), float(t_emit_floor)))
 
+    def init_ic_mg1d(self, tr_flat, N, group_edges, t_emit_floor=0.0) -> int:
+        """MG_IMC1D initial census (stratified per shell, Planck group at the shell's Tr)."""
+        tr = np.ascontiguousarray(tr_flat, dtype=np.float64)
+        ge = np.ascontiguousarray(group_edges, dtype=np.float64)
+        return int(self.lib.orc_init_ic_mg1d(self.h, int(N), _p(tr), _p(ge), float(t_emit_floor)))
+
+    def transport_mg1d(self, *args, **kw) -> dict:
+        """One MG_IMC1D step up to the material update (same arguments as transport_mg)."""
+        return self.transport_mg(*args, _entry="orc_step_transport_mg1d", **kw)
+
     def transport_mg(self, T, sigma_gc, cv, source_gc, step, dt, theta, Ntarget, Nboundary, Nsource, face_T,
                      reflect, group_edges, max_events=0, emission_fractions=None, t_emit_floor=0.0, nthreads=None,
-                     sources_only=False) -> dict:
+                     sources_only=False, _entry="orc_step_transport_mg") -> dict:
         keep = []
 
         def arr(x):
@@ -278,7 +296,7 @@ class Oracle:
         mo = MgOut()
         for k in ("dep", "si", "emitted", "sigma_a", "sigma_s", "bnd_by_group", "esc_by_group"):
             setattr(mo, k, _p(out[k]))
-        st = self.lib.orc_step_transport_mg(self.h, ctypes.byref(mi), ctypes.byref(mo))
+        st = getattr(self.lib, _entry)(self.h, ctypes.byref(mi), ctypes.byref(mo))
         if st != 0:
             raise AssertionError("invalid multigroup material state")
         out["boundary_emission"] = mo.boundary_emission
@@ -291,9 +309,18 @@ class Oracle:
         out["weight_floor"] = mo.weight_floor
         return out
 
-    def comb(self, Nmax, step, per_group=False) -> np.ndarray:
+    def comb(self, Nmax, step, per_group=False, conserve_radiation=False) -> np.ndarray:
+        """Nmax > 0 combs to Nmax; 0 only drops dead entries; < 0 combs to |Nmax| once at
+        least |Nmax| entries are alive.  Returns the per-bin discrepancy (before - after)."""
         disc = np.zeros(self.nc * (self.ng if per_group else 1))
-        self.lib.orc_comb(self.h, int(Nmax), int(step) & 0xFFFFFFFF, int(per_group), _p(disc))
+        flags = int(bool(per_group)) | (2 if conserve_radiation else 0)
+        self.lib.orc_comb(self.h, int(Nmax), int(step) & 0xFFFFFFFF, flags, _p(disc))
+        return disc
+
+    def comb_mg_with_xi(self, Nmax, xi, conserve_radiation=False) -> np.ndarray:
+        disc = np.zeros(self.nc * self.ng)
+        x = np.ascontiguousarray(xi, dtype=np.float64)
+        self.lib.orc_comb_mg_with_xi(self.h, int(Nmax), _p(x), 2 if conserve_radiation else 0, _p(disc))
         return disc
 
     def comb_with_xi(self, Nmax, xi) -> np.ndarray:

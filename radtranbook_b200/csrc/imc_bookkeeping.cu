@@ -11,7 +11,8 @@
 //   boundary       IMC/IMC1D.py:319-329, 744-763; IMC/IMC2D.py:157-489
 //   IC             IMC/IMC1D.py:220-248, 535-575; IMC/IMC2D.py:1110-1188
 //   material       IMC/IMC1D.py:1021-1035; IMC/IMC2D.py:1801-1810
-//   comb targets   IMC/IMC1D.py:786-799; IMC/IMC2D.py:1461-1468
+//   comb targets   IMC/IMC1D.py:786-799; IMC/IMC2D.py:1461-1468; MG_IMC/MG_IMC1D.py:1194-1200
+//   multigroup     MG_IMC/MG_IMC2D.py:1703-1943 (xy, rz); MG_IMC/MG_IMC1D.py:941-1120 (sphere)
 #include <algorithm>
 #include <cmath>
 #include "imc_block.cuh"
@@ -147,7 +148,8 @@ __global__ void __launch_bounds__(NT) k_plan(PlanArgs a) {
     a.sum->n_side[side] = 0;
     a.sum->e_side[side] = 0.0;
     const double* Tf = a.face_T[side];
-    if (Tf && a.n_boundary > 0 && !(oned && side >= 2)) {
+    const long long nbs = a.n_side[side];
+    if (Tf && nbs > 0 && !(oned && side >= 2)) {
       const bool along2 = side < 2;
       const int nf = oned ? 1 : (along2 ? a.ny : a.nx);
       double* Ef = a.face + (size_t)(side * 2 + 0) * a.nf;
@@ -170,9 +172,9 @@ __global__ void __launch_bounds__(NT) k_plan(PlanArgs a) {
         cdf[q] = Et;
       }
       if (Et > 0.0) {
-        a.sum->n_side[side] = a.n_boundary;
-        const float wq = (float)(Et / (double)a.n_boundary);
-        a.sum->e_side[side] = (double)a.n_boundary * (double)wq;
+        a.sum->n_side[side] = nbs;
+        const float wq = (float)(Et / (double)nbs);
+        a.sum->e_side[side] = (double)nbs * (double)wq;
       }
     }
   }
@@ -208,7 +210,8 @@ __global__ void __launch_bounds__(NT) k_ic_plan(IcArgs a) {
     const int c = order_to_cell(o, a.nx, a.ny);
     long long n = 0;
     if (N > 0) {
-      if (oned) n = Et > 0.0 ? (long long)ceil(E[c] / Et * (double)N) : 0;
+      if (a.rule == 2) n = (Et > 0.0 && E[c] > 0.0) ? max(1LL, (long long)rint((double)N * E[c] / Et)) : 0;
+      else if (oned) n = Et > 0.0 ? (long long)ceil(E[c] / Et * (double)N) : 0;
       else n = max(1LL, (long long)ceil((double)N * E[c] / fmax(Et, 1e-300)));
     }
     a.n[o] = n;
@@ -232,6 +235,9 @@ __global__ void k_material(MatArgs a) {
 __global__ void __launch_bounds__(NT) k_comb_plan(CombPlanArgs a) {
   __shared__ double red[NT];
   const double E = block_canon_sum(a.ecen, a.nb, red);
+  // MG_IMC/MG_IMC1D.py:1194-1200: Nmax = 0 never combs; Nmax < 0 combs once |Nmax| entries live
+  const bool compact = a.force_compact || (a.threshold > 0 && (long long)*a.n_live < a.threshold);
+  if (threadIdx.x == 0) *a.mode = compact ? 1 : 0;
   for (int b = threadIdx.x; b < a.nb; b += NT) {
     const double ec = a.ecen[b];
     double ew = 0.0;
@@ -289,6 +295,17 @@ namespace {
 
 // Planck fraction F(x) = (15/pi^4) int_0^x t^3/(e^t-1) dt: Bernoulli series below x = 1,
 // exponential series above (Widger & Woodall 1976).  Same expansion as the oracle.
+// sum_k e^{-kx}(x^3/k + 3x^2/k^2 + 6x/k^3 + 6/k^4) = (pi^4/15)(1 - F(x)), for x >= 1
+__device__ double planck_tail(double x) {
+  double tail = 0.0;
+  const int K = (int)(2.0 + 40.0 / x);
+  for (int k = K; k >= 1; --k) {
+    const double kx = k * x, ik = 1.0 / k;
+    tail += exp(-kx) * ik * (x * x * x + ik * (3.0 * x * x + ik * (6.0 * x + ik * 6.0)));
+  }
+  return tail;
+}
+
 __device__ double planck_F(double x) {
   const double c = 15.0 / (PI * PI * PI * PI);
   if (!(x > 0.0)) return 0.0;
@@ -304,13 +321,15 @@ __device__ double planck_F(double x) {
     }
     return c * sum;
   }
-  double tail = 0.0;
-  const int K = (int)(2.0 + 40.0 / x);
-  for (int k = K; k >= 1; --k) {
-    const double kx = k * x, ik = 1.0 / k;
-    tail += exp(-kx) * ik * (x * x * x + ik * (3.0 * x * x + ik * (6.0 * x + ik * 6.0)));
-  }
-  return 1.0 - c * tail;
+  return 1.0 - c * planck_tail(x);
+}
+
+// F(x1) - F(x0); above x = 1 as a difference of tails, which keeps its relative precision
+// far into the Wien tail (1 - F cancels to 0 there)
+__device__ double planck_frac(double x0, double x1) {
+  if (!(x1 > x0)) return 0.0;
+  if (x0 >= 1.0) return 15.0 / (PI * PI * PI * PI) * (planck_tail(x0) - planck_tail(x1));
+  return planck_F(x1) - planck_F(x0);
 }
 
 // canonical inclusive prefix sum of n values (the oracle's canon_prefix order)
@@ -352,7 +371,7 @@ __global__ void __launch_bounds__(NT) k_plan_mg(PlanMgArgs a) {
     double* gc = a.Egc + (size_t)c * G;  // scratch: fractions, then cumulative emission
     double tot = 0.0;
     for (int g = 0; g < G; ++g) {
-      const double f = (T > 0.0) ? planck_F(a.gedges[g + 1] / T) - planck_F(a.gedges[g] / T) : 0.0;
+      const double f = (T > 0.0) ? planck_frac(a.gedges[g] / T, a.gedges[g + 1] / T) : 0.0;
       gc[g] = f > 0.0 ? f : 0.0;
       tot += gc[g];
     }
@@ -420,7 +439,8 @@ __global__ void __launch_bounds__(NT) k_plan_mg(PlanMgArgs a) {
     a.sum->n_side[side] = 0;
     a.sum->e_side[side] = 0.0;
     const double* Tf = a.face_T[side];
-    if (Tf && a.n_boundary > 0) {
+    const long long nbs = a.n_side[side];
+    if (Tf && nbs > 0) {
       const bool along2 = side < 2;
       const int nf = along2 ? a.ny : a.nx;
       double* Ef = a.face + (size_t)(side * 2 + 0) * a.nf;
@@ -437,8 +457,8 @@ __global__ void __launch_bounds__(NT) k_plan_mg(PlanMgArgs a) {
         cdf[q] = Et;
       }
       if (Et > 0.0) {
-        a.sum->n_side[side] = a.n_boundary;
-        a.sum->e_side[side] = (double)a.n_boundary * (double)(float)(Et / (double)a.n_boundary);
+        a.sum->n_side[side] = nbs;
+        a.sum->e_side[side] = (double)nbs * (double)(float)(Et / (double)nbs);
       }
     }
   }
@@ -451,6 +471,132 @@ __global__ void __launch_bounds__(NT) k_plan_mg(PlanMgArgs a) {
     a.sum->n_bank = base;
     a.sum->source_emission = e_src;
     a.sum->emission_total = issued;
+  }
+}
+
+// Multigroup 1-D sphere planning (MG_IMC/MG_IMC1D.py:941-1120): Planck fractions, Fleck
+// factor with the Planck-mean opacity, emission E_gc = a c T^4 sigma_a,g b*_g dt V per
+// (group, cell) bin b = g*nc + c with stratified counts max(1, round(N E_b / E)) (fixed
+// source: round, no minimum), inner / outer sphere boundary faces.
+__global__ void __launch_bounds__(NT) k_plan_mg1d(PlanMgArgs a) {
+  __shared__ double red[NT];
+  __shared__ long long sh[NT];
+  const int t = threadIdx.x;
+  const int nc = a.nc, G = a.ng, ncg = nc * G;
+  for (int q = t; q <= a.nx; q += NT) a.e1f[q] = (float)a.e1[q];
+  for (int q = t; q <= a.ny; q += NT) a.e2f[q] = (float)a.e2[q];
+  if (t == 0) {
+    double tot = 0.0;
+    for (int n = 1; n <= 200; ++n) { const double d = (double)n; tot += 1.0 / (d * d * d * d); }
+    double run = 0.0;
+    for (int n = 1; n <= 200; ++n) { const double d = (double)n; run += 1.0 / (d * d * d * d); a.mixcdf[n - 1] = run / tot; }
+  }
+  for (int c = t; c < nc; c += NT) {
+    const double T = a.T[c];
+    if (!isfinite(T) || !(a.cv[c] > 0.0)) atomicOr(&a.sum->flags, (int)IMC_FLAG_NONFINITE);
+    double* b = a.Egc + (size_t)c * G;  // scratch: Planck fractions of this cell
+    double tot = 0.0;
+    for (int g = 0; g < G; ++g) {
+      const double f = (T > 0.0) ? planck_frac(a.gedges[g] / T, a.gedges[g + 1] / T) : 0.0;
+      b[g] = f > 0.0 ? f : 0.0;
+      tot += b[g];
+    }
+    double sp = 0.0;
+    for (int g = 0; g < G; ++g) {
+      b[g] = tot > 0.0 ? b[g] / tot : 0.0;
+      sp += a.sigma[(size_t)g * nc + c] * b[g];
+    }
+    const double beta = 4.0 * A_RAD * pow3(T) / a.cv[c];
+    double f = 1.0 / (1.0 + a.theta * beta * sp * C_LIGHT * a.dt);
+    f = fmin(1.0, fmax(0.0, f));
+    const bool cold = a.t_emit_floor > 0.0 && T < a.t_emit_floor;
+    for (int g = 0; g < G; ++g) {
+      const size_t q = (size_t)g * nc + c;
+      const double sa = a.sigma[q] * f;
+      const double ss = a.sigma[q] * (1.0 - f);
+      a.sa[q] = sa; a.ss[q] = ss;
+      a.sass[q] = make_float2((float)sa, (float)ss);
+      // MG_IMC/MG_IMC1D.py:346-350: path-length estimator below sigma_a = 1e-10
+      a.cellf[q] = make_double2(1.0 / a.vol[c], sa > 1e-10 ? 1.0 / (sa * a.vol[c] * a.dt) : -1.0 / (a.vol[c] * a.dt));
+      a.emit_E[q] = cold ? 0.0 : A_RAD * C_LIGHT * pow4(T) * sa * b[g] * a.dt * a.vol[c];
+    }
+  }
+  __syncthreads();
+  // ---- emission: stratified counts, FP32 weights, energy issued per bin and per cell ----
+  const double Et = block_canon_sum(a.emit_E, ncg, red);
+  for (int q = t; q < ncg; q += NT) {
+    const double E = a.emit_E[q];
+    long long n = 0;
+    if (a.n_target > 0 && Et > 0.0 && E > 0.0) n = max(1LL, (long long)rint((double)a.n_target * E / Et));
+    const float w = n > 0 ? (float)(E / (double)n) : 0.f;
+    a.emit_n[q] = n; a.emit_w[q] = w; a.emit_issued[q] = (double)n * (double)w;
+  }
+  __syncthreads();
+  const long long n_emit = block_scan_counts(a.emit_n, a.emit_off, ncg, sh);
+  const double e_emit = block_canon_sum(a.emit_issued, ncg, red);
+  for (int c = t; c < nc; c += NT) {
+    double e = 0.0;
+    for (int g = 0; g < G; ++g) e += a.emit_issued[(size_t)g * nc + c];
+    a.emitted[c] = e;
+  }
+  // ---- fixed source [g][c] (MG_IMC/MG_IMC1D.py:679-743; only when max(source) > 0) ----
+  long long n_src = 0;
+  double e_src = 0.0;
+  if (a.source && a.n_source > 0) {
+    double smax = 0.0;
+    for (int q = t; q < ncg; q += NT) {
+      smax = fmax(smax, a.source[q]);
+      a.src_QV[q] = a.source[q] * a.vol[q % nc] * a.dt;
+    }
+    red[t] = smax;
+    __syncthreads();
+    for (int h = NT / 2; h >= 1; h >>= 1) { if (t < h) red[t] = fmax(red[t], red[t + h]); __syncthreads(); }
+    const bool any = red[0] > 0.0;
+    __syncthreads();
+    if (any) {
+      const double Qt = block_canon_sum(a.src_QV, ncg, red);
+      for (int q = t; q < ncg; q += NT) {
+        const double Q = a.src_QV[q];
+        long long n = 0;
+        if (Qt > 0.0 && Q > 0.0) n = max(0LL, (long long)rint((double)a.n_source * Q / Qt));
+        const float w = n > 0 ? (float)(Q / (double)n) : 0.f;
+        a.src_n[q] = n; a.src_w[q] = w; a.src_issued[q] = (double)n * (double)w;
+      }
+      __syncthreads();
+      n_src = block_scan_counts(a.src_n, a.src_off, ncg, sh);
+      e_src = block_canon_sum(a.src_issued, ncg, red);
+    }
+  }
+  // ---- boundary: a c T^4 / 4 * 4 pi R^2 * dt on the inner and outer sphere ----
+  if (t < 4) {
+    const int side = t;
+    a.sum->n_side[side] = 0;
+    a.sum->e_side[side] = 0.0;
+    const double* Tf = a.face_T[side];
+    const long long nbs = a.n_side[side];
+    if (side < 2 && Tf && nbs > 0) {
+      double* Ef = a.face + (size_t)(side * 2 + 0) * a.nf;
+      double* cdf = a.face + (size_t)(side * 2 + 1) * a.nf;
+      const double R = side == 0 ? a.e1[0] : a.e1[a.nx];
+      const double T = Tf[0];
+      const double E = (T > 0.0) ? A_RAD * C_LIGHT * T * T * T * T / 4.0 * (4.0 * PI * R * R) * a.dt : 0.0;
+      Ef[0] = E;
+      cdf[0] = E;
+      if (E > 0.0) {
+        a.sum->n_side[side] = nbs;
+        a.sum->e_side[side] = (double)nbs * (double)(float)(E / (double)nbs);
+      }
+    }
+  }
+  __syncthreads();
+  if (t == 0) {
+    long long base = a.sum->n_census;
+    for (int q = 0; q < 4; ++q) { a.sum->base_side[q] = base; base += a.sum->n_side[q]; }
+    a.sum->n_source = n_src; a.sum->base_source = base; base += n_src;
+    a.sum->n_emission = n_emit; a.sum->base_emission = base; base += n_emit;
+    a.sum->n_bank = base;
+    a.sum->source_emission = e_src;
+    a.sum->emission_total = e_emit;
   }
 }
 
@@ -483,6 +629,12 @@ __global__ void __launch_bounds__(NT) k_ic_plan_mg(IcMgArgs a) {
 cudaError_t imc_launch_plan_mg(const PlanMgArgs& a, cudaStream_t s) {
   ++g_imc_launches;
   k_plan_mg<<<1, NT, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t imc_launch_plan_mg1d(const PlanMgArgs& a, cudaStream_t s) {
+  ++g_imc_launches;
+  k_plan_mg1d<<<1, NT, 0, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -61,7 +61,8 @@ imc_status check_mesh(const imc_mesh* m) {
   const bool oned = m->geometry == IMC_GEOM_SLAB || m->geometry == IMC_GEOM_SPHERE;
   if (oned && m->ny != 1) return IMC_ERR_BAD_GEOMETRY;
   if (m->n_groups < 1) return IMC_ERR_INVALID_ARG;
-  if (m->n_groups > 1 && (oned || !m->group_edges)) return IMC_ERR_INVALID_ARG;  // MG: xy / rz
+  // multigroup: xy / rz (MG_IMC2D) and the 1-D sphere (MG_IMC1D)
+  if (m->n_groups > 1 && (m->geometry == IMC_GEOM_SLAB || !m->group_edges)) return IMC_ERR_INVALID_ARG;
   return IMC_OK;
 }
 
@@ -72,13 +73,20 @@ bool bank_ok(const imc_bank* b, bool two_d, bool mg = false) {
   return b->size >= 0 && b->capacity >= b->size && b->capacity < (1LL << 31);
 }
 
+inline bool mg_sphere(const imc_mesh* m) { return m->n_groups > 1 && m->geometry == IMC_GEOM_SPHERE; }
+
+inline long long side_count(const imc_step_params* p, int q) {
+  return p->n_boundary_side[q] > 0 ? p->n_boundary_side[q] : p->n_boundary;
+}
+
 long long source_bound(const imc_mesh* m, const imc_step_params* p) {
-  const long long nc = (long long)m->nx * m->ny;
+  // ceil adds at most one per cell; MG 1-D: round (+1/2) and the minimum of one per bin
+  const long long nb = (long long)m->nx * m->ny * (mg_sphere(m) ? m->n_groups : 1);
   long long b = 0;
   for (int q = 0; q < 4; ++q)
-    if (p->face_T[q] && p->n_boundary > 0) b += p->n_boundary;
-  if (p->n_target > 0) b += p->n_target + nc;   // ceil adds at most one per cell
-  if (p->n_source > 0) b += p->n_source + nc;
+    if (p->face_T[q] && side_count(p, q) > 0) b += side_count(p, q);
+  if (p->n_target > 0) b += p->n_target + nb;
+  if (p->n_source > 0) b += p->n_source + nb;
   return b;
 }
 
@@ -97,12 +105,14 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   const bool two_d = mesh->geometry >= IMC_GEOM_XY;
   const int ng = mesh->n_groups;
   const bool mg = ng > 1;
+  const bool mg1 = mg_sphere(mesh);  // MG_IMC1D: stratified (group, cell) sources
   if (!mat || !mat->temperature || !mat->sigma || !mat->cv || !par || !tal || !sum) return IMC_ERR_INVALID_ARG;
   if (!tal->dep || !tal->si || !tal->emitted || !tal->sigma_a || !tal->sigma_s || !tal->escaped || !tal->stats)
     return IMC_ERR_INVALID_ARG;
   if (mg && (!tal->escaped_group || !tal->boundary_group)) return IMC_ERR_INVALID_ARG;
   if (!bank_ok(bank, two_d, mg) || !workspace) return IMC_ERR_INVALID_ARG;
   if (!(par->dt > 0.0) || par->n_target < 0 || par->n_boundary < 0 || par->n_source < 0) return IMC_ERR_INVALID_ARG;
+  for (int q = 0; q < 4; ++q) if (par->n_boundary_side[q] < 0) return IMC_ERR_INVALID_ARG;
   const long long bound = source_bound(mesh, par);
   const long long n_upper = bank->size + bound;
   if (n_upper > bank->capacity) return IMC_ERR_BANK_OVERFLOW;
@@ -121,6 +131,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   pa.T = mat->temperature; pa.sigma = mat->sigma; pa.cv = mat->cv; pa.source = mat->source;
   pa.dt = par->dt; pa.theta = par->theta;
   pa.n_target = par->n_target; pa.n_source = par->n_source; pa.n_boundary = par->n_boundary;
+  for (int q = 0; q < 4; ++q) pa.n_side[q] = side_count(par, q);
   for (int q = 0; q < 4; ++q) pa.face_T[q] = par->face_T[q];
   pa.rz_linear = par->rz_linear_source; pa.t_emit_floor = par->t_emit_floor;
   pa.sa = tal->sigma_a; pa.ss = tal->sigma_s;
@@ -138,6 +149,29 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   PlanMgArgs pm{};
   if (!mg) {
     IMC_CUDA(imc_launch_plan(pa, s));
+  } else if (mg1) {
+    IMC_CUDA(cudaMemsetAsync(tal->boundary_group, 0, sizeof(double) * ng, s));
+    IMC_CUDA(cudaMemsetAsync(tal->escaped_group, 0, sizeof(double) * ng, s));
+    pm.geom = mesh->geometry; pm.nx = mesh->nx; pm.ny = mesh->ny; pm.nc = nc; pm.ng = ng;
+    pm.e1 = mesh->edges1; pm.e2 = mesh->edges2; pm.vol = mesh->volume;
+    pm.T = mat->temperature; pm.sigma = mat->sigma; pm.cv = mat->cv; pm.source = mat->source;
+    pm.gedges = mesh->group_edges;
+    pm.dt = par->dt; pm.theta = par->theta;
+    pm.n_target = par->n_target; pm.n_source = par->n_source; pm.n_boundary = par->n_boundary;
+    for (int q = 0; q < 4; ++q) pm.n_side[q] = side_count(par, q);
+    for (int q = 0; q < 4; ++q) pm.face_T[q] = par->face_T[q];
+    pm.t_emit_floor = par->t_emit_floor;
+    pm.sa = tal->sigma_a; pm.ss = tal->sigma_s; pm.sass = pa.sass; pm.cellf = pa.cellf;
+    pm.e1f = pa.e1f; pm.e2f = pa.e2f;
+    pm.Egc = ws_ptr<double>(workspace, L.mg_gcdf);
+    pm.emitted = tal->emitted; pm.face = pa.face; pm.nf = pa.nf;
+    pm.mixcdf = ws_ptr<double>(workspace, L.mixcdf);
+    pm.emit_E = pa.emit_E; pm.emit_n = pa.emit_n; pm.emit_off = pa.emit_off; pm.emit_w = pa.emit_w;
+    pm.emit_issued = ws_ptr<double>(workspace, L.emit_issued);
+    pm.src_QV = pa.src_QV; pm.src_n = pa.src_n; pm.src_off = pa.src_off; pm.src_w = pa.src_w;
+    pm.src_issued = pa.src_issued;
+    pm.sum = sum;
+    IMC_CUDA(imc_launch_plan_mg1d(pm, s));
   } else {
     IMC_CUDA(cudaMemsetAsync(tal->boundary_group, 0, sizeof(double) * ng, s));
     IMC_CUDA(cudaMemsetAsync(tal->escaped_group, 0, sizeof(double) * ng, s));
@@ -147,6 +181,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     pm.gedges = mesh->group_edges; pm.emission_fractions = par->emission_fractions;
     pm.dt = par->dt; pm.theta = par->theta;
     pm.n_target = par->n_target; pm.n_source = par->n_source; pm.n_boundary = par->n_boundary;
+    for (int q = 0; q < 4; ++q) pm.n_side[q] = side_count(par, q);
     for (int q = 0; q < 4; ++q) pm.face_T[q] = par->face_T[q];
     pm.t_emit_floor = par->t_emit_floor;
     pm.sa = tal->sigma_a; pm.ss = tal->sigma_s; pm.sass = pa.sass; pm.cellf = pa.cellf;
@@ -167,23 +202,26 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   float *p2, *d2;
   set_bank(p2, d2, bank, two_d);
   for (int side = 0; side < 4; ++side) {
-    if (!par->face_T[side] || par->n_boundary <= 0) continue;
+    if (!par->face_T[side] || side_count(par, side) <= 0) continue;
     BndArgs ba{};
     ba.geom = mesh->geometry; ba.nx = mesh->nx; ba.ny = mesh->ny; ba.side = side; ba.nf = pa.nf;
     ba.e1 = mesh->edges1; ba.e2 = mesh->edges2;
     ba.face = pa.face + (size_t)side * 2 * pa.nf;
-    ba.d_n = &sum->n_side[side]; ba.d_base = &sum->base_side[side]; ba.n_bound = par->n_boundary;
+    ba.d_n = &sum->n_side[side]; ba.d_base = &sum->base_side[side]; ba.n_bound = side_count(par, side);
     ba.dt = par->dt; ba.seed = par->seed; ba.step = par->step;
     ba.p1 = bank->pos1; ba.p2 = p2; ba.d1 = bank->dir1; ba.d2 = d2; ba.wb = bank->weight;
     ba.t = bank->time; ba.cell = bank->cell; ba.group = bank->group;
     ba.ng = ng; ba.faceT = par->face_T[side]; ba.gedges = mesh->group_edges;
     ba.mixcdf = ws_ptr<double>(workspace, L.mixcdf); ba.boundary_group = tal->boundary_group;
+    ba.below_last = mg1 ? 1 : 0;
     IMC_CUDA(imc_launch_fill_boundary(ba, s));
   }
+  const int nbins = mg1 ? nc * ng : nc;  // source order positions (MG 1-D: (group, cell) bins)
   auto fill = [&](const int64_t* d_n, const int64_t* d_base, long long n_bound, const long long* off,
                   const float* w, const double* tilt, int kind, uint32_t tag) -> cudaError_t {
     FillArgs fa{};
     fa.geom = mesh->geometry; fa.nx = mesh->nx; fa.ny = mesh->ny; fa.nc = nc;
+    fa.nbins = nbins; fa.bins_by_group = mg1 ? 1 : 0;
     fa.e1 = mesh->edges1; fa.e2 = mesh->edges2; fa.T = mat->temperature;
     fa.d_n = d_n; fa.d_base = d_base; fa.n_bound = n_bound;
     fa.off = off; fa.w = w; fa.tilt = tilt; fa.tilt_kind = kind;
@@ -205,7 +243,14 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     return imc_launch_fill_mg(fm, s);
   };
   const bool rzlin = mesh->geometry == IMC_GEOM_RZ && par->rz_linear_source;
-  if (mg) {
+  if (mg1) {
+    if (mat->source && par->n_source > 0)
+      IMC_CUDA(fill(&sum->n_source, &sum->base_source, par->n_source + nbins, pa.src_off, pa.src_w, nullptr, 0,
+                    imcdev::TAG_SOURCE));
+    if (par->n_target > 0)
+      IMC_CUDA(fill(&sum->n_emission, &sum->base_emission, par->n_target + nbins, pa.emit_off, pa.emit_w, nullptr, 0,
+                    imcdev::TAG_EMISSION));
+  } else if (mg) {
     if (mat->source && par->n_source > 0)
       IMC_CUDA(fill_mg(&sum->n_source, &sum->base_source, par->n_source, pm.Scdf, pm.Sgc, imcdev::TAG_SOURCE));
     if (par->n_target > 0)
@@ -241,6 +286,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   ta.cell = bank->cell; ta.group = bank->group;
   ta.n_dev = &sum->n_bank; ta.wsum = &sum->weight_sum; ta.queue = queue; ta.flags = &sum->flags;
   ta.dt = (float)par->dt;
+  ta.floor_coef = mg1 ? 1e-14 : 1e-10;
   int rm = 0;
   for (int q = 0; q < 4; ++q) if (par->reflect[q]) rm |= 1 << q;
   ta.reflect_mask = rm;
@@ -277,14 +323,18 @@ imc_status comb_async(const imc_mesh* mesh, const imc_bank* in, imc_bank* out, i
   const bool two_d = mesh->geometry >= IMC_GEOM_XY;
   if (!bank_ok(in, two_d) || !bank_ok(out, two_d) || !disc || !workspace || !sum) return IMC_ERR_INVALID_ARG;
   if (in->pos1 == out->pos1 || in->weight == out->weight) return IMC_ERR_INVALID_ARG;
-  if (per_group && (!in->group || !out->group)) return IMC_ERR_INVALID_ARG;
+  const bool by_group = (per_group & IMC_COMB_PER_GROUP) != 0;
+  if (by_group && (!in->group || !out->group)) return IMC_ERR_INVALID_ARG;
   const WsLayout L = imc_ws_layout(mesh, in->size);
   if (workspace_bytes < L.total) return IMC_ERR_WORKSPACE;
   const int nc = mesh->nx * mesh->ny;
-  const int nb = per_group ? nc * mesh->n_groups : nc;
+  const int nb = by_group ? nc * mesh->n_groups : nc;
 
   CombArgs ca{};
-  ca.nc = nc; ca.nb = nb; ca.per_group = per_group;
+  ca.nc = nc; ca.nb = nb; ca.per_group = by_group ? 1 : 0;
+  ca.conserve_rad = (per_group & IMC_COMB_CONSERVE_RADIATION) ? 1 : 0;
+  ca.mode = ws_ptr<int>(workspace, L.comb_mode);
+  ca.n_live = ws_ptr<unsigned long long>(workspace, L.comb_mode + 8);
   ca.d_n_in = &sum->n_bank; ca.n_bound = in->size; ca.out_capacity = out->capacity;
   ca.w = in->weight; ca.cell = in->cell; ca.group = in->group;
   ca.p1 = in->pos1; ca.p2 = two_d ? in->pos2 : nullptr; ca.d1 = in->dir1; ca.d2 = two_d ? in->dir2 : nullptr;
@@ -300,9 +350,16 @@ imc_status comb_async(const imc_mesh* mesh, const imc_bank* in, imc_bank* out, i
   IMC_CUDA(cudaMemsetAsync(ca.ecen, 0, sizeof(double) * nb, s));
   IMC_CUDA(cudaMemsetAsync(ca.ncopy, 0, sizeof(double) * nb, s));
   IMC_CUDA(cudaMemsetAsync(&sum->comb_after, 0, sizeof(double), s));
+  IMC_CUDA(cudaMemsetAsync(ca.mode, 0, 16, s));
   IMC_CUDA(imc_launch_comb_ecen(ca, s));
   CombPlanArgs cp{};
-  cp.nb = nb; cp.n_max = n_max; cp.ecen = ca.ecen; cp.ew = ca.ew; cp.sum = sum;
+  cp.nb = nb; cp.ecen = ca.ecen; cp.ew = ca.ew; cp.sum = sum;
+  // n_max > 0: comb to n_max; 0: keep every live entry; < 0: comb to |n_max| once at least
+  // |n_max| entries are alive (MG_IMC/MG_IMC1D.py:1194-1200)
+  cp.n_max = n_max < 0 ? -n_max : n_max;
+  cp.threshold = n_max < 0 ? -n_max : 0;
+  cp.force_compact = n_max == 0 ? 1 : 0;
+  cp.n_live = ca.n_live; cp.mode = ca.mode;
   IMC_CUDA(imc_launch_comb_plan(cp, s));
   IMC_CUDA(imc_launch_comb_count(ca, s));
   IMC_CUDA(imc_launch_comb_scatter(ca, s));
@@ -329,10 +386,11 @@ WsLayout imc_ws_layout(const imc_mesh* m, int64_t capacity) {
   L.summary = take(sizeof(imc_step_summary)); L.queue = take(8);
   L.e1f = take(4 * (nx + 1)); L.e2f = take(4 * (ny + 1));
   L.sass = take(8 * ncg); L.cellf = take(16 * ncg);
-  L.emit_E = take(8 * ncg); L.emit_n = take(8 * nc); L.emit_off = take(8 * (nc + 1)); L.emit_w = take(4 * nc);
+  L.emit_E = take(8 * ncg); L.emit_n = take(8 * ncg); L.emit_off = take(8 * (ncg + 1)); L.emit_w = take(4 * ncg);
+  L.emit_issued = take(8 * ncg);
   L.tilt = take(8 * 4 * nc);
-  L.src_n = take(8 * nc); L.src_off = take(8 * (nc + 1)); L.src_w = take(4 * nc);
-  L.src_QV = take(8 * nc); L.src_issued = take(8 * nc);
+  L.src_n = take(8 * ncg); L.src_off = take(8 * (ncg + 1)); L.src_w = take(4 * ncg);
+  L.src_QV = take(8 * ncg); L.src_issued = take(8 * ncg);
   L.face = take(8 * 4 * 2 * nf);
   if (ng > 1) {
     L.mg_gcdf = take(8 * ncg); L.mg_ec = take(8 * nc); L.mg_cdf = take(8 * nc);
@@ -341,6 +399,7 @@ WsLayout imc_ws_layout(const imc_mesh* m, int64_t capacity) {
   L.mixcdf = take(8 * 200);
   L.ecen = take(8 * ncg); L.ew = take(8 * ncg); L.ncopy = take(8 * ncg);
   L.cnt = take(4 * cap); L.blk = take(8 * ((cap + 1023) / 1024 + 2));
+  L.comb_mode = take(16);
   L.dep_fx = take(8 * ncg); L.esc_fx = take(8 * (4 + ng));
   L.total = o;
   return L;
@@ -430,7 +489,8 @@ imc_status imc_init_census(const imc_mesh* mesh, const double* tr, int64_t n_tar
   if (bound > bank->capacity) { if (n_out) *n_out = bound; return IMC_ERR_BANK_OVERFLOW; }
   imc_step_summary* sum = internal_summary(workspace, L);
   IMC_CUDA(cudaMemsetAsync(sum, 0, sizeof(imc_step_summary), s));
-  if (mesh->n_groups > 1) {
+  const bool mg1 = mg_sphere(mesh);
+  if (mesh->n_groups > 1 && !mg1) {
     if (!bank->group) return IMC_ERR_INVALID_ARG;
     IcMgArgs im{};
     im.nc = nc; im.vol = mesh->volume; im.tr = tr; im.n_target = n_target; im.t_emit_floor = t_emit_floor;
@@ -453,8 +513,19 @@ imc_status imc_init_census(const imc_mesh* mesh, const double* tr, int64_t n_tar
     if (n_out) *n_out = n;
     return IMC_OK;
   }
+  if (mg1) {
+    if (!bank->group || !mesh->group_edges) return IMC_ERR_INVALID_ARG;
+    // the Planck group sampler's mixture table (MG_IMC/MG_IMC1D.py:105-107)
+    double mix[200];
+    double tot = 0.0, run = 0.0;
+    for (int n = 1; n <= 200; ++n) { const double d = (double)n; tot += 1.0 / (d * d * d * d); }
+    for (int n = 1; n <= 200; ++n) { const double d = (double)n; run += 1.0 / (d * d * d * d); mix[n - 1] = run / tot; }
+    IMC_CUDA(cudaMemcpyAsync(ws_ptr<double>(workspace, L.mixcdf), mix, sizeof(mix), cudaMemcpyHostToDevice, s));
+    IMC_CUDA(cudaStreamSynchronize(s));  // mix is a stack array
+  }
   IcArgs ia{};
   ia.geom = mesh->geometry; ia.nx = mesh->nx; ia.ny = mesh->ny; ia.nc = nc;
+  ia.rule = mg1 ? 2 : (two_d ? 1 : 0);
   ia.e1 = mesh->edges1; ia.e2 = mesh->edges2; ia.vol = mesh->volume; ia.tr = tr;
   ia.n_target = n_target; ia.t_emit_floor = t_emit_floor;
   ia.n = ws_ptr<long long>(workspace, L.emit_n); ia.off = ws_ptr<long long>(workspace, L.emit_off);
@@ -467,6 +538,11 @@ imc_status imc_init_census(const imc_mesh* mesh, const double* tr, int64_t n_tar
   fa.d_n = &sum->n_emission; fa.d_base = &sum->base_emission; fa.n_bound = bound;
   fa.off = ia.off; fa.w = ia.w; fa.tilt = nullptr; fa.tilt_kind = 0;
   fa.time_scale = 0.0; fa.seed = seed; fa.step = 0; fa.tag = imcdev::TAG_IC;
+  fa.nbins = nc; fa.bins_by_group = 0;
+  if (mg1) {
+    fa.tr = tr; fa.gedges = mesh->group_edges; fa.mixcdf = ws_ptr<double>(workspace, L.mixcdf);
+    fa.ng = mesh->n_groups;
+  }
   set_bank(fa.p2, fa.d2, bank, two_d);
   fa.p1 = bank->pos1; fa.d1 = bank->dir1;
   fa.wb = bank->weight; fa.t = bank->time; fa.cell = bank->cell; fa.group = bank->group;
@@ -509,7 +585,7 @@ imc_status imc_step_transport(const imc_mesh* mesh, const imc_material* mat, con
   report->n_boundary = nb; report->n_source = h.n_source; report->n_emission = h.n_emission;
   report->source_emission = h.source_emission; report->emission_total = h.emission_total;
   report->n_transported = h.n_bank;
-  report->weight_floor = 1e-10 * h.weight_sum / (double)std::max<long long>(h.n_bank, 1);
+  report->weight_floor = (mg_sphere(mesh) ? 1e-14 : 1e-10) * h.weight_sum / (double)std::max<long long>(h.n_bank, 1);
   imc_phase_times(&report->ms_sources, &report->ms_transport);
   bank->size = h.n_bank;
   if (h.flags & IMC_FLAG_NONFINITE) return IMC_ERR_NONFINITE;

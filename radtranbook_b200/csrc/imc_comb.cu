@@ -10,6 +10,9 @@
 //      thread per copy)                                                       k_comb_scatter
 //   6. disc[b] = ecen - (copies in b) * FP32(ew)                              k_comb_disc
 // Order of the output bank = order of the input bank, so the result is deterministic.
+// Modes (MG_IMC/MG_IMC1D.py:1187-1200, 808-820): when the comb plan decides not to comb
+// (Nmax = 0, or fewer live entries than a threshold) every live entry is copied once with its
+// weight (disc = 0); with conserve_rad each bin's copies share its pre-comb energy equally.
 #include "imc_device.cuh"
 #include "imc_internal.h"
 
@@ -21,6 +24,13 @@ constexpr int CB = 1024;  // comb block
 
 __device__ __forceinline__ int bin_of(const CombArgs& a, long long k) {
   return a.per_group ? a.cell[k] + a.nc * a.group[k] : a.cell[k];
+}
+
+// weight of every copy in bin b: the comb weight, or the bin's energy shared equally
+__device__ __forceinline__ float copy_weight(const CombArgs& a, int b) {
+  if (!a.conserve_rad) return (float)a.ew[b];
+  const double n = a.ncopy[b];
+  return n > 0.0 ? (float)(a.ecen[b] / n) : 0.f;
 }
 
 constexpr int ECH = 4096;       // consecutive entries per k_comb_ecen block
@@ -37,6 +47,7 @@ __global__ void __launch_bounds__(256) k_comb_ecen(CombArgs a) {
   const long long n_in = *a.d_n_in;
   const long long base = (long long)blockIdx.x * ECH;
   // block-uniform trip count keeps every warp converged for the aggregated reduction
+  unsigned n_live = 0;
   for (int i = 0; i < ECH; i += 256) {
     const long long k = base + i + threadIdx.x;
     bool live = false;
@@ -46,8 +57,11 @@ __global__ void __launch_bounds__(256) k_comb_ecen(CombArgs a) {
       const float wf = a.w[k];
       if (wf > 0.f) { live = true; b = bin_of(a, k); w = (double)wf; }
     }
+    n_live += live ? 1u : 0u;
     warp_bins_add(live, b, w, t, a.ecen, st);
   }
+  n_live = __reduce_add_sync(FULL, n_live);
+  if ((threadIdx.x & 31) == 0 && n_live) atomicAdd(a.n_live, (unsigned long long)n_live);
   __syncthreads();
   bins_flush(t, a.ecen);
 }
@@ -60,13 +74,16 @@ __global__ void __launch_bounds__(CB) k_comb_count(CombArgs a) {
   __syncthreads();
   const long long k = (long long)blockIdx.x * CB + threadIdx.x;
   const long long n_in = *a.d_n_in;
+  const bool compact = *a.mode != 0;
   int n = 0, b = 0;
   if (k < n_in) {
     const float wf = a.w[k];
     if (wf > 0.f) {
       b = bin_of(a, k);
       const double ew = a.ew[b];
-      if (ew > 0.0) {
+      if (compact) {
+        n = 1;
+      } else if (ew > 0.0) {
         const U4 r = draw(a.seed, (uint32_t)k, 0, a.step, TAG_COMB);
         n = (int)floor((double)wf / ew + u01d(r.x));
       }
@@ -142,6 +159,7 @@ __global__ void __launch_bounds__(CB) k_comb_scatter(CombArgs a) {
   __syncthreads();
   const int total = incl[CB - 1];
   const long long out0 = a.blk[blockIdx.x];
+  const bool compact = *a.mode != 0;
   for (int o = threadIdx.x; o < total; o += CB) {
     const long long dst = out0 + o;
     if (dst >= a.out_capacity) break;  // overflow: flagged by the scan, caller regrows
@@ -152,7 +170,8 @@ __global__ void __launch_bounds__(CB) k_comb_scatter(CombArgs a) {
     a.op1[dst] = a.p1[src]; a.od1[dst] = a.d1[src];
     if (a.op2) a.op2[dst] = a.p2[src];
     if (a.od2) a.od2[dst] = a.d2[src];
-    a.ow[dst] = (float)a.ew[b]; a.ot[dst] = 0.f; a.ocell[dst] = a.cell[src];
+    a.ow[dst] = compact ? a.w[src] : copy_weight(a, b);
+    a.ot[dst] = 0.f; a.ocell[dst] = a.cell[src];
     if (a.ogroup) a.ogroup[dst] = a.group[src];
   }
 }
@@ -161,7 +180,8 @@ __global__ void k_comb_disc(CombArgs a) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   double after = 0.0;
   if (b < a.nb) {
-    after = a.ncopy[b] * (double)(float)a.ew[b];
+    // compact only: every live entry kept with its weight, nothing is lost
+    after = *a.mode != 0 ? a.ecen[b] : a.ncopy[b] * (double)copy_weight(a, b);
     a.disc[b] = a.ecen[b] - after;
   }
   after = warp_sum_d(after);

@@ -248,14 +248,16 @@ __device__ __forceinline__ void warp_tally_fx(bool flush, int key, unsigned long
 // Group of a photon sampled from the Planck spectrum at T (mixture of Gammas,
 // MG_IMC/MG_IMC2D.py:202-254): n from the 1/n^4 mixture CDF, x = (four Exp(1)) / n,
 // energy T*x located in the group edges.
+// below_last: an energy below the lowest edge goes to the last group (MG_IMC/MG_IMC1D.py:180-186);
+// otherwise to the first (MG_IMC/MG_IMC2D.py:242-243)
 __device__ __forceinline__ int planck_group(double T, const double* edges, int G, const double* mixcdf, double un,
-                                            double u1, double u2, double u3, double u4) {
+                                            double u1, double u2, double u3, double u4, bool below_last = false) {
   if (!(T > 0.0)) return 0;
   double ns = 200.0;
   for (int i = 0; i < 200; ++i) if (un <= mixcdf[i]) { ns = (double)(i + 1); break; }
   const double x = (-log(u1) - log(u2) - log(u3) - log(u4)) / ns;
   const double f = T * x;
-  if (f < edges[0]) return 0;
+  if (f < edges[0]) return below_last ? G - 1 : 0;
   if (f >= edges[G]) return G - 1;
   for (int g = 0; g < G; ++g) if (f >= edges[g] && f < edges[g + 1]) return g;
   return G - 1;

@@ -27,7 +27,8 @@ struct TrackArgs {
   int* cell;
   int* group;
   const int64_t* n_dev;      // bank entries to track (device)
-  const double* wsum;        // sum of their weights (device): floor = 1e-10 * wsum / n
+  const double* wsum;        // sum of their weights (device): floor = floor_coef * wsum / n
+  double floor_coef;         // 1e-10 (IMC1D, IMC2D, MG_IMC2D); 1e-14 (MG_IMC1D)
   unsigned long long* queue; // ticket counter (zeroed before launch)
   int* flags;                // IMC_FLAG_* (device)
   float dt;
@@ -69,11 +70,12 @@ struct WsLayout {
   size_t sass;                // float2 [ncg]
   size_t cellf;               // double2 [ncg]
   size_t emit_E;              // double [ncg]  emission energy per (group,) cell
-  size_t emit_n;              // int64 [nc]    emission count per cell (order position)
-  size_t emit_off;            // int64 [nc+1]  exclusive offsets in source order
-  size_t emit_w;              // float [nc]
+  size_t emit_n;              // int64 [ncg]   emission count per order position (MG 1-D: per bin)
+  size_t emit_off;            // int64 [ncg+1] exclusive offsets in source order
+  size_t emit_w;              // float [ncg]
+  size_t emit_issued;         // double [ncg]  MG 1-D: energy issued per bin
   size_t tilt;                // double [4*nc] per-cell tilt constants
-  size_t src_n, src_off, src_w, src_QV, src_issued;  // fixed source
+  size_t src_n, src_off, src_w, src_QV, src_issued;  // fixed source ([ncg] / [ncg+1])
   size_t face;                // double [4][2][nf] per-side face energies and CDF
   size_t mg_gcdf, mg_ec, mg_cdf, mg_sgcdf, mg_sc, mg_scdf, mixcdf;  // multigroup tables
   size_t summary;             // imc_step_summary used by the synchronous wrappers
@@ -81,6 +83,7 @@ struct WsLayout {
   size_t ecen, ew, ncopy;     // comb: double [nb], double [nb], long long [nb]
   size_t cnt;                 // int32 [cap]    comb copies per entry
   size_t blk;                 // int64 [nblk+1] comb block totals / offsets
+  size_t comb_mode;           // int32 mode + uint64 live-entry count (comb)
   size_t dep_fx, esc_fx;      // uint64 [ncg], [4 + ng] fixed-point energy tallies
   size_t total;
 };
@@ -100,6 +103,7 @@ struct PlanArgs {
   const double* T; const double* sigma; const double* cv; const double* source;
   double dt, theta;
   long long n_target, n_source, n_boundary;
+  long long n_side[4];             // boundary particles per side (n_boundary unless overridden)
   const double* face_T[4];
   int rz_linear;
   double t_emit_floor;
@@ -119,6 +123,8 @@ cudaError_t imc_launch_plan(const PlanArgs& a, cudaStream_t s);
 
 struct IcArgs {
   int geom, nx, ny, nc;
+  int rule;                        // counts: 0 ceil(N E/Et) (IMC1D), 1 max(1, ceil) (IMC2D),
+                                   // 2 max(1, round) for E > 0 (MG_IMC1D)
   const double* e1; const double* e2; const double* vol;
   const double* tr;
   long long n_target;
@@ -138,6 +144,10 @@ cudaError_t imc_launch_material(const MatArgs& a, cudaStream_t s);
 struct CombPlanArgs {
   int nb;
   long long n_max;
+  long long threshold;             // > 0: comb only when at least this many entries are alive
+  int force_compact;               // 1: no comb, only drop dead entries
+  const unsigned long long* n_live;
+  int* mode;                       // out: 0 comb, 1 compact only
   const double* ecen;
   double* ew;
   imc_step_summary* sum;
@@ -156,13 +166,17 @@ struct FillArgs {
   const int64_t* d_n;          // particles to write (device)
   const int64_t* d_base;       // first bank index (device)
   long long n_bound;           // host upper bound of *d_n (grid sizing)
-  const long long* off;        // [nc+1] offsets in source order
-  const float* w;              // [nc] per-cell weight
+  int nbins;                   // order positions in off (nc; bins_by_group: ng*nc)
+  int bins_by_group;           // 1: bin b = g*nc + c carries group g (MG 1-D sources)
+  const long long* off;        // [nbins+1] offsets in source order
+  const float* w;              // [nc] per-cell weight ([nbins] when bins_by_group)
   const double* tilt;          // [4*nc] or NULL
   int tilt_kind;               // 0 none, 1 slab linear-T, 2 sphere linear-T^4, 3 rz linear
   double time_scale;           // birth time = u * time_scale (dt; 0 for the IC)
   uint64_t seed; uint32_t step; uint32_t tag;
   float* p1; float* p2; float* d1; float* d2; float* wb; float* t; int* cell; int* group;
+  // MG 1-D initial census: group from the Planck spectrum at tr[c] (NULL otherwise)
+  const double* tr; const double* gedges; const double* mixcdf; int ng;
 };
 cudaError_t imc_launch_fill_volume(const FillArgs& a, cudaStream_t s);
 
@@ -178,6 +192,7 @@ struct BndArgs {
   float* p1; float* p2; float* d1; float* d2; float* wb; float* t; int* cell; int* group;
   // multigroup: Planck group at the face cell's temperature
   int ng; const double* faceT; const double* gedges; const double* mixcdf; double* boundary_group;
+  int below_last;              // MG 1-D: an energy below the lowest edge goes to the last group
 };
 cudaError_t imc_launch_fill_boundary(const BndArgs& a, cudaStream_t s);
 
@@ -188,6 +203,9 @@ cudaError_t imc_launch_wsum(const float* w, const int64_t* d_n, long long n_boun
 // ---------------------------------------------------------------------------------
 struct CombArgs {
   int nc, nb, per_group;
+  int conserve_rad;            // copies in bin b weigh ecen[b] / ncopy[b] (bin energy kept)
+  int* mode;                   // set by the comb plan: 0 comb, 1 compact only (copy live entries)
+  unsigned long long* n_live;  // live entries (counted by k_comb_ecen; zeroed before)
   const int64_t* d_n_in;       // entries to comb (device)
   long long n_bound;           // host upper bound of *d_n_in (grid sizing)
   long long out_capacity;
@@ -217,6 +235,7 @@ struct PlanMgArgs {
   const double* gedges; const double* emission_fractions;
   double dt, theta;
   long long n_target, n_source, n_boundary;
+  long long n_side[4];             // boundary particles per side
   const double* face_T[4];
   double t_emit_floor;
   double* sa; double* ss; float2* sass; double2* cellf;  // [g][c]
@@ -227,8 +246,12 @@ struct PlanMgArgs {
   double* face; int nf;
   double* mixcdf;                             // [200]
   imc_step_summary* sum;
+  // 1-D sphere (MG_IMC1D): stratified (group, cell) bins b = g*nc + c
+  double* emit_E; long long* emit_n; long long* emit_off; float* emit_w; double* emit_issued;
+  double* src_QV; long long* src_n; long long* src_off; float* src_w; double* src_issued;
 };
 cudaError_t imc_launch_plan_mg(const PlanMgArgs& a, cudaStream_t s);
+cudaError_t imc_launch_plan_mg1d(const PlanMgArgs& a, cudaStream_t s);
 
 struct IcMgArgs {
   int nc;

@@ -6,8 +6,9 @@
 // Sampling math is FP64 (Newton-bisection CDF inversions included) and stored as FP32.
 //
 //   volume sources  IMC/IMC1D.py:203-316 (slab emission, linear-T tilt, fixed source),
-//                   IMC/IMC1D.py:578-741 (sphere), IMC/IMC2D.py:1191-1445 (xy, rz)
-//   initial census  IMC/IMC1D.py:220-248, 535-575; IMC/IMC2D.py:1110-1188
+//                   IMC/IMC1D.py:578-741 (sphere), IMC/IMC2D.py:1191-1445 (xy, rz),
+//                   MG_IMC/MG_IMC1D.py:569-743 (sphere, stratified per (group, cell))
+//   initial census  IMC/IMC1D.py:220-248, 535-575; IMC/IMC2D.py:1110-1188; MG_IMC/MG_IMC1D.py:514-566
 //   boundary        IMC/IMC1D.py:319-329, 744-763; IMC/IMC2D.py:157-489
 // Random numbers: Philox (particle index within this source, block 0/1, step, tag).
 #include <cmath>
@@ -25,10 +26,12 @@ __global__ void k_fill_volume(FillArgs a) {
   const long long n = *a.d_n, base = *a.d_base;
   for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
     // order position o with off[o] <= k < off[o+1]
-    int lo = 0, hi = a.nc;  // search in off[0..nc]
+    int lo = 0, hi = a.nbins;  // search in off[0..nbins]
     while (lo < hi) { const int mid = (lo + hi) >> 1; if (a.off[mid + 1] <= k) lo = mid + 1; else hi = mid; }
     const int o = lo;
-    const int i = o / a.ny, j = o - i * a.ny;
+    const int g = a.bins_by_group ? o / a.nc : 0;  // MG 1-D bins b = g*nc + c
+    const int oc = o - g * a.nc;
+    const int i = oc / a.ny, j = oc - i * a.ny;
     const int c = i + a.nx * j;
     const U4 r = draw(a.seed, (uint32_t)k, 0, a.step, a.tag);
     const U4 s = draw(a.seed, (uint32_t)k, 1, a.step, a.tag);
@@ -73,10 +76,17 @@ __global__ void k_fill_volume(FillArgs a) {
     a.p1[b] = (float)p1; a.d1[b] = (float)d1;
     if (a.p2) a.p2[b] = (float)p2;
     if (a.d2) a.d2[b] = (float)d2;
-    a.wb[b] = a.w[c];
+    a.wb[b] = a.w[a.bins_by_group ? o : c];
     a.t[b] = (float)(s0 * a.time_scale);
     a.cell[b] = c;
-    if (a.group) a.group[b] = 0;
+    if (a.group) {
+      int gb = g;
+      if (a.tr) {  // MG 1-D initial census: Planck group at the cell's Tr (MG_IMC/MG_IMC1D.py:557-560)
+        const U4 d = draw(a.seed, (uint32_t)k, 2, a.step, a.tag);
+        gb = planck_group(a.tr[c], a.gedges, a.ng, a.mixcdf, s1, u01d(s.z), u01d(s.w), u01d(d.x), u01d(d.y), true);
+      }
+      a.group[b] = gb;
+    }
   }
 }
 
@@ -151,7 +161,7 @@ __global__ void k_fill_boundary(BndArgs a) {
       if (a.ng > 1) {
         const U4 rd = draw(a.seed, (uint32_t)k, 2, a.step, TAG_BOUNDARY | (uint32_t)a.side);
         g = planck_group(a.faceT[q], a.gedges, a.ng, a.mixcdf, u01d(rb.y), u01d(rb.z), u01d(rb.w), u01d(rd.x),
-                         u01d(rd.y));
+                         u01d(rd.y), a.below_last != 0);
         atomicAdd(a.boundary_group + g, (double)wq);
       }
       a.group[b] = g;

@@ -4,6 +4,7 @@
 //   slab   IMC/IMC1D.py:75-130 (move_particle), 133-200 (move_particles)
 //   sphere IMC/IMC1D.py:336-436, 439-532
 //   xy/rz  IMC/IMC2D.py:711-935 (events), 938-1107 (history loop)
+//   multigroup  MG_IMC/MG_IMC2D.py:580-989 (xy, rz), MG_IMC/MG_IMC1D.py:276-461 (sphere)
 //
 // Execution model: a persistent grid (blocks_per_sm x SMs).  Each warp claims a chunk of
 // bank indices with one atomic ticket and keeps 32 histories in registers.  Every loop
@@ -25,14 +26,18 @@ namespace {
 // Block-level counters for rare events (shared-memory atomics keep them out of registers).
 enum : int { B_CENSUS = 0, B_FLOOR, B_REFLECT, B_CAP, B_ESCAPE, B_N };
 
-// MG: multigroup rules of MG_IMC/MG_IMC2D.py:580-989 (group-indexed tables, no effective-
-// scatter cap, no absorption for sigma_a <= 1e-12, the weight floor ends a history after its
-// event is committed, escaped energy also by group).
+// MG: group-indexed tables and tallies, escaped energy also by group.  In 2-D the rules of
+// MG_IMC/MG_IMC2D.py:580-989 (no effective-scatter cap, no absorption for sigma_a <= 1e-12,
+// the weight floor ends a history after its event is committed); on the 1-D sphere those of
+// MG_IMC/MG_IMC1D.py:276-461, which are the gray spherical ones (cap, floor kill with local
+// deposit) with the floor coefficient 1e-14.
 template <int GEOM, bool SMEM_CELLS, bool PREFETCH, bool MG>
 __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ unsigned blk_cnt[B_N];
   __shared__ unsigned long long blk_esc[4];
+  constexpr bool ONED = GEOM == G_SLAB || GEOM == G_SPHERE;
+  constexpr bool MG2 = MG && !ONED;  // MG_IMC2D history rules
   WarpStage* stages = reinterpret_cast<WarpStage*>(smem);
   const int nwarps = blockDim.x >> 5;
   float* E1 = reinterpret_cast<float*>(stages + nwarps);
@@ -65,8 +70,8 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   unsigned s_bd = 0, s_sc = 0;          // per-event counters (census/cap counted at finish)
 
   const float c_light = (float)C_LIGHT;
-  // weight floor, IMC/IMC1D.py:1007 / IMC/IMC2D.py:1771
-  const float weight_floor = (float)(1e-10 * (*a.wsum) / (double)(n > 0 ? n : 1));
+  // weight floor, IMC/IMC1D.py:1007 / IMC/IMC2D.py:1771 (1e-10); MG_IMC/MG_IMC1D.py:1127 (1e-14)
+  const float weight_floor = (float)(a.floor_coef * (*a.wsum) / (double)(n > 0 ? n : 1));
   const double inv_q = fx_inv_quantum(*a.wsum);  // fixed-point energy tallies
   const float ss_thr = (GEOM == G_SLAB || GEOM == G_SPHERE) ? 1e-10f : 1e-12f;
 
@@ -97,7 +102,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
         pid = chunk_next + rank;
         w = a.w[pid];
         dcen = (a.dt - a.t[pid]) * c_light;
-        if ((MG ? w > weight_floor : w > 0.f) && dcen > 0.f) {
+        if ((MG2 ? w > weight_floor : w > 0.f) && dcen > 0.f) {
           x = a.p1[pid]; u = a.d1[pid];
           if (MG) grp = a.group[pid];
           if (GEOM == G_XY || GEOM == G_RZ) { y = a.p2[pid]; v = a.d2[pid]; }
@@ -184,7 +189,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
         // short series, so the logarithm is evaluated only when it can win.
         float ds = BIGF;
         {
-          const bool capped = !MG && ss * L > 10000.0f;
+          const bool capped = !MG2 && ss * L > 10000.0f;
           const float sig = capped ? 10000.0f / L : (ss > ss_thr ? ss : 0.f);
           if (sig > 0.f) {
             const float s_other = fminf(sb, dcen);
@@ -256,7 +261,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
           xn = rn;
         }
         // implicit capture; the energy removed is the exact difference of the FP32 weights
-        const float wn = (MG && !(sa > 1e-12f)) ? w : w * __expf(-sa * d);
+        const float wn = (MG2 && !(sa > 1e-12f)) ? w : w * __expf(-sa * d);
         acc_lost += (double)w - (double)wn;
         acc_wd += (double)(w * d);
         dcen -= d;
@@ -304,7 +309,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
               // IMC/IMC1D.py:188-195: kill and deposit the remainder in the current cell
               // (every cell, including the two edge cells the reference skips)
               atomicAdd(&blk_cnt[B_FLOOR], 1u);
-              const int c2 = ci + a.nx * cj;
+              const int c2 = ci + a.nx * cj + (MG ? a.nc * grp : 0);
               const double2 cf = __ldg(a.cellf + c2);
               const double rem = (double)w;
               atomicAdd(a.dep_fx + c2, fx_units(rem, inv_q));
@@ -312,7 +317,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
               w = 0.f;
               finished = true;
             }
-          } else if (MG && !finished && dcen > 0.f && w <= weight_floor) {
+          } else if (MG2 && !finished && dcen > 0.f && w <= weight_floor) {
             // MG_IMC/MG_IMC2D.py:858-860: the next event would stop at the floor (a weight
             // that underflowed to 0 included)
             atomicAdd(&blk_cnt[B_FLOOR], 1u);
@@ -416,8 +421,9 @@ cudaError_t imc_launch_tally_finalize(const TrackArgs& a, cudaStream_t s) {
 
 cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool sm, bool pf, cudaStream_t s) {
   ++g_imc_launches;
-  if (a.ng > 1) {  // multigroup: 2-D geometries (MG_IMC/MG_IMC2D.py)
+  if (a.ng > 1) {  // multigroup: 2-D (MG_IMC/MG_IMC2D.py) and the 1-D sphere (MG_IMC/MG_IMC1D.py)
     switch (geom) {
+      case G_SPHERE: return launch_geom<G_SPHERE, true>(a, block, grid, sm, pf, s);
       case G_XY: return launch_geom<G_XY, true>(a, block, grid, sm, pf, s);
       case G_RZ: return launch_geom<G_RZ, true>(a, block, grid, sm, pf, s);
       default: return cudaErrorInvalidValue;

@@ -26,6 +26,10 @@ def _ptr(t: torch.Tensor | None) -> int | None:
     return None if t is None else t.data_ptr()
 
 
+def _comb_flags(per_group: bool, conserve_radiation: bool) -> int:
+    return (_lib.COMB_PER_GROUP if per_group else 0) | (_lib.COMB_CONSERVE_RADIATION if conserve_radiation else 0)
+
+
 def require_cuda() -> torch.device:
     if not torch.cuda.is_available():
         raise RuntimeError("radtranbook_b200 needs a CUDA device (B200, sm_100a); none is available")
@@ -219,18 +223,22 @@ class Engine:
         _lib.check("imc_material_update", self.lib.imc_material_update(
             ctypes.byref(self.cmesh), ctypes.byref(self.ctal), _ptr(e), _ptr(tr), self._stream()))
 
-    def comb(self, n_max: int, step: int, per_group: bool = False) -> ImcCombReport:
+    def comb(self, n_max: int, step: int, per_group: bool = False, conserve_radiation: bool = False) -> ImcCombReport:
+        """Comb the bank (n_max > 0: to n_max; 0: drop dead entries only; < 0: to |n_max| once
+        at least |n_max| entries are alive)."""
         rep = ImcCombReport()
         src = self.bank
         dst = self.spare
         dst.size = 0
-        dst.ensure(int(n_max) + 2 * self.nc * self.ng + 1024)
+        # n_max <= 0 keeps at most every input entry (a threshold comb makes <= the live count)
+        dst.ensure((int(n_max) if n_max > 0 else src.size) + 2 * self.nc * self.ng + 1024)
+        flags = _comb_flags(per_group, conserve_radiation)
         cin = src.c()
 
         def run(cb):
             wsp, wsn = self._ws(max(src.size, 1))
             return self.lib.imc_comb(ctypes.byref(self.cmesh), ctypes.byref(cin), ctypes.byref(cb), int(n_max),
-                                     self.seed, int(step) & 0xFFFFFFFF, int(per_group), _ptr(self.disc), wsp, wsn,
+                                     self.seed, int(step) & 0xFFFFFFFF, flags, _ptr(self.disc), wsp, wsn,
                                      ctypes.byref(rep), self._stream())
 
         cb = self._call_bank("imc_comb", run, dst, lambda: rep.required_capacity)
@@ -256,7 +264,7 @@ class Engine:
     # One step = transport_async -> material_update -> (caller's inv_eos) -> comb_async ->
     # fetch(): a single device->host copy of the summary and one stream synchronisation.
     def _params(self, step, dt, theta, n_target, n_boundary, n_source, face_T, reflect, max_events,
-                rz_linear_source, t_emit_floor) -> ImcStepParams:
+                rz_linear_source, t_emit_floor, n_boundary_side=None) -> ImcStepParams:
         par = ImcStepParams()
         par.seed = self.seed
         par.step = int(step) & 0xFFFFFFFF
@@ -273,6 +281,8 @@ class Engine:
         par.chunk = int(self.launch["chunk"])
         par.reserved = int(bool(self.launch.get("smem_cells", 0))) | (int(bool(self.launch.get("prefetch", 0))) << 1)
         par.emission_fractions = _ptr(self.emission_fractions)
+        for q, n in enumerate(n_boundary_side or ()):
+            par.n_boundary_side[q] = int(n)
         return par
 
     def _set_census_count(self, n: int) -> None:
@@ -280,17 +290,17 @@ class Engine:
         self._census_dev_valid = True
 
     def transport_async(self, T, sigma, cv, source, step, dt, theta, n_target, n_boundary, n_source, face_T,
-                        reflect, max_events=0, rz_linear_source=True, t_emit_floor=0.0) -> int:
+                        reflect, max_events=0, rz_linear_source=True, t_emit_floor=0.0, n_boundary_side=None) -> int:
         """Sources + tracking without a host synchronisation.  Returns the host upper bound
         of the tracked bank size (the true size is in the device summary)."""
         if not self._census_dev_valid:
             self._set_census_count(self.bank.size)
         self._last_transport = ((T, sigma, cv, source, step, dt, theta, n_target, n_boundary, n_source, face_T,
                                  reflect), dict(max_events=max_events, rz_linear_source=rz_linear_source,
-                                                t_emit_floor=t_emit_floor))
+                                                t_emit_floor=t_emit_floor, n_boundary_side=n_boundary_side))
         self._mat = ImcMaterial(_ptr(T), _ptr(sigma), _ptr(cv), _ptr(source))
         self._par = self._params(step, dt, theta, n_target, n_boundary, n_source, face_T, reflect, max_events,
-                                 rz_linear_source, t_emit_floor)
+                                 rz_linear_source, t_emit_floor, n_boundary_side)
         bound = int(self.lib.imc_source_bound(ctypes.byref(self.cmesh), ctypes.byref(self._par)))
         self.bank.ensure(self.bank.size + bound)
         wsp, wsn = self._ws(self.bank.capacity)
@@ -303,20 +313,23 @@ class Engine:
         self._upper = self.bank.size + bound
         return self._upper
 
-    def comb_async(self, n_max: int, step: int, e: torch.Tensor | None, per_group: bool = False) -> None:
+    def comb_async(self, n_max: int, step: int, e: torch.Tensor | None, per_group: bool = False,
+                   conserve_radiation: bool = False) -> None:
+        """Queue the comb (n_max semantics as comb()); fetch() completes it."""
         self.spare.size = 0
-        self.spare.ensure(int(1.15 * n_max) + 2 * self.nc * self.ng + 4096)
-        self._comb_args = (int(n_max), int(step), e, per_group)
+        want = int(1.15 * n_max) if n_max > 0 else self._upper
+        self.spare.ensure(want + 2 * self.nc * self.ng + 4096)
+        self._comb_args = (int(n_max), int(step), e, _comb_flags(per_group, conserve_radiation))
         self._launch_comb()
 
     def _launch_comb(self) -> None:
-        n_max, step, e, per_group = self._comb_args
+        n_max, step, e, flags = self._comb_args
         cin = self.bank.c()
         cin.size = self._upper
         cout = self.spare.c()
         wsp, wsn = self._ws(max(self._upper, self.bank.capacity))
         st = self.lib.imc_comb_async(ctypes.byref(self.cmesh), ctypes.byref(cin), ctypes.byref(cout), n_max,
-                                     self.seed, step & 0xFFFFFFFF, int(per_group), _ptr(self.disc), _ptr(e),
+                                     self.seed, step & 0xFFFFFFFF, flags, _ptr(self.disc), _ptr(e),
                                      wsp, wsn, self.summary_dev.data_ptr(), self._stream())
         _lib.check("imc_comb_async", st)
 

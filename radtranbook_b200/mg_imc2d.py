@@ -63,17 +63,27 @@ def planck_fractions(energy_edges, T) -> np.ndarray:
                 acc += B[n] * xs ** (n + 3) / ((n + 3) * fact)
         out[small] = c * acc
         big = x >= 1.0
-        xb = x[big]
-        tail = np.zeros_like(xb)
-        for k in range(42, 0, -1):
-            ik = 1.0 / k
-            tail += np.exp(-k * xb) * ik * (xb ** 3 + ik * (3 * xb ** 2 + ik * (6 * xb + ik * 6)))
-        out[big] = 1.0 - c * tail
+        out[big] = 1.0 - c * tail(x[big])
         return out
 
-    with np.errstate(divide="ignore", invalid="ignore"):
+    def tail(x):
+        t = np.zeros_like(x)
+        for k in range(42, 0, -1):
+            ik = 1.0 / k
+            t += np.exp(-k * x) * ik * (x ** 3 + ik * (3 * x ** 2 + ik * (6 * x + ik * 6)))
+        return t
+
+    def frac(x0, x1):
+        # above x = 1 as a difference of tails (1 - F cancels to 0 deep in the Wien tail)
+        x0, x1 = np.broadcast_arrays(np.asarray(x0, dtype=np.float64), np.asarray(x1, dtype=np.float64))
+        hi = x0 >= 1.0
+        out = F(x1) - F(x0)
+        out[hi] = 15.0 / np.pi ** 4 * (tail(x0[hi]) - tail(x1[hi]))
+        return out
+
+    with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
         Tpos = np.where(T > 0, T, 1.0)
-        f = np.stack([F(e[g + 1] / Tpos) - F(e[g] / Tpos) for g in range(len(e) - 1)])
+        f = np.stack([frac(e[g] / Tpos, e[g + 1] / Tpos) for g in range(len(e) - 1)])
     f = np.clip(f, 0.0, None)
     tot = f.sum(axis=0)
     return np.where(tot > 0, f / np.where(tot > 0, tot, 1.0), 0.0)

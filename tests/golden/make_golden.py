@@ -14,8 +14,12 @@ RADTRANBOOK_REF); the fixtures it writes are small .npz files committed with thi
   sources.npz    per-cell counts and weights of IMC/IMC1D.py:251 emitted_particles and
                  IMC/IMC2D.py:1326 _sample_source_rz_linear (the deterministic part of sampling)
   planck.npz     MG_IMC/MG_IMC2D.py:202 Planck (mixture-of-Gammas) group sampler, with its draws
+  mg1d.npz       MG_IMC/MG_IMC1D.py pins: stratified emission / IC / fixed-source counts and
+                 weights, the per-(cell, group) comb in both energy modes, the spherical event
+                 and the Planck sampler, with their draws
   stats_*.npz    multi-seed statistics of whole reference steps (IMC1D.step, IMC2D.step,
-                 MG_IMC2D.step with planck_shim/ standing in for the external planck_integrals):
+                 MG_IMC2D.step and MG_IMC1D.step with planck_shim/ standing in for the
+                 external planck_integrals):
                  per-cell mean and standard error of material and radiation temperature
 
 The reference's random numbers cannot be reproduced by a different generator, so whole-step
@@ -325,7 +329,153 @@ def run_stats_mg(MG_IMC2D, seeds=16):
                 Tr_se=Trs.std(0, ddof=1) / np.sqrt(seeds), seeds=seeds, **MG)
 
 
+MG1 = dict(I=30, R=1.0, G=4, cv=0.2, T0=0.05, Tb=1.0, dt=0.01, steps=4, Ntarget=3000, Nboundary=3000, Nmax=8000)
+
+
+def mg1d_setup():
+    edges = np.logspace(-2, np.log10(20.0), MG1["G"] + 1)
+    nu = 0.5 * (edges[:-1] + edges[1:])
+    funcs = [(lambda T, n=n: np.clip(2.0 * n ** -3 * np.power(T, -0.5), 0.1, 1e4)) for n in nu]
+    return edges, nu, funcs
+
+
+def load_reference_mg1d():
+    sys.path.insert(0, os.path.join(HERE, "planck_shim"))
+    sys.path.insert(0, os.path.join(REF, "MG_IMC"))
+    import MG_IMC1D  # noqa: E402
+    assert MG_IMC1D._PLANCK_AVAILABLE, "planck_integrals stand-in not found"
+    return MG_IMC1D
+
+
+def gen_mg1d_pins(M, seed=23):
+    """MG_IMC/MG_IMC1D.py pins: stratified emission / IC / fixed-source counts and weights
+    (:514-743), the per-(cell, group) comb (:746-847) with its uniforms, the spherical event
+    (:276-364) and the Planck sampler (:144-195) with their draws."""
+    seed_py, seed_np, draw_py, draw_np = nb_helpers()
+    rng = np.random.default_rng(seed)
+    I, G = 20, 4
+    edges = np.logspace(-2, np.log10(20.0), G + 1)
+    out = {"edges": edges}
+    meshes, Ts, sas, Ns, dts, cnt_e, w_e, emit = [], [], [], [], [], [], [], []
+    srcs, cnt_s, w_s, Ns_s, cnt_ic, w_ic, Ns_ic = [], [], [], [], [], [], []
+    for q in range(8):
+        e = np.concatenate([[0.0], np.cumsum(10 ** rng.uniform(-2, -0.5, I))])
+        mesh = np.stack([e[:-1], e[1:]], axis=1)
+        T = 10 ** rng.uniform(-1.5, 0.3, I)
+        saf = 10 ** rng.uniform(-1, 3, (G, I))
+        N = int(rng.integers(500, 5000)); dt = float(10 ** rng.uniform(-3, -1))
+        np.random.seed(q)
+        w, mu, t, r, c, g, ebg = M._emitted_particles_spherical_mg(N, T, dt, mesh, saf, edges)
+        b = c + g.astype(np.int64) * I
+        cnt = np.bincount(b, minlength=G * I)
+        wb = np.zeros(G * I); wb[b] = w
+        meshes.append(e); Ts.append(T); sas.append(saf); Ns.append(N); dts.append(dt)
+        cnt_e.append(cnt); w_e.append(wb); emit.append(ebg)
+        src = 10 ** rng.uniform(-2, 1, (G, I)) * (rng.uniform(size=(G, I)) > 0.3)
+        Nsrc = int(rng.integers(200, 3000))
+        w, mu, t, r, c, g = M._sample_source_spherical_mg(Nsrc, src, dt, mesh, edges, T)
+        b = c + g.astype(np.int64) * I
+        cnt = np.bincount(b, minlength=G * I)
+        wb = np.zeros(G * I); wb[b] = w
+        srcs.append(src); Ns_s.append(Nsrc); cnt_s.append(cnt); w_s.append(wb)
+        Nic = int(rng.integers(500, 5000))
+        Tr = T * (rng.uniform(size=I) > 0.2)
+        w, mu, t, r, c, g = M._equilibrium_sample_spherical_mg(Nic, Tr, mesh, edges)
+        cnt = np.bincount(c, minlength=I)
+        wb = np.zeros(I); wb[c] = w
+        Ns_ic.append(Nic); cnt_ic.append(cnt); w_ic.append(wb)
+        Ts[-1] = T
+        out.setdefault("ic_Tr", []).append(Tr)
+    out.update(mesh=np.array(meshes), T=np.array(Ts), saf=np.array(sas), N=np.array(Ns), dt=np.array(dts),
+               emit_counts=np.array(cnt_e), emit_w=np.array(w_e), emit_by_group=np.array(emit),
+               src=np.array(srcs), src_N=np.array(Ns_s), src_counts=np.array(cnt_s), src_w=np.array(w_s),
+               ic_N=np.array(Ns_ic), ic_counts=np.array(cnt_ic), ic_w=np.array(w_ic))
+    out["ic_Tr"] = np.array(out["ic_Tr"])
+    # ---- comb, both energy modes ----
+    for mode in ("none", "radiation"):
+        n = 3000
+        w = 10 ** rng.uniform(-3, 0, n) * (rng.uniform(size=n) > 0.1)
+        c = rng.integers(0, I, n); g = rng.integers(0, G, n).astype(np.int32)
+        mu = rng.uniform(-1, 1, n); t = rng.uniform(0, 0.01, n); r = rng.uniform(0, 1, n)
+        nmax = 2500
+        np.random.seed(77)
+        xi = np.random.random(int(np.sum(w > 0)))
+        np.random.seed(77)
+        nw, nc, ng, nm, nt, npos, disc = M._comb_mg_1d(w, c, g, mu, t, r, nmax, I, G,
+                                                        conserve_rad_energy=(mode == "radiation"))
+        out.update({f"comb_{mode}_in": np.stack([w, c, g, mu, t, r], axis=1), f"comb_{mode}_xi": xi,
+                    f"comb_{mode}_out": np.stack([nw, nc, ng, nm, npos], axis=1), f"comb_{mode}_disc": disc})
+    out["comb_nmax"] = 2500
+    # ---- spherical event of MG_IMC1D ----
+    rows, draws, res = [], [], []
+    for q in range(300):
+        r0 = rng.choice([0.0, 10 ** rng.uniform(-2, 0)], p=[0.2, 0.8]); dr = 10 ** rng.uniform(-3, -1); r1 = r0 + dr
+        x = r0 + dr * rng.uniform(0.01, 0.99)
+        mu = rng.uniform(-1, 1)
+        w = 10 ** rng.uniform(-3, 1)
+        sa = 0.0 if rng.uniform() < 0.2 else float(10 ** rng.uniform(-3, 7))
+        ss = 0.0 if rng.uniform() < 0.2 else float(10 ** rng.uniform(-3, 7))
+        dcen = 10 ** rng.uniform(-4, 0)
+        seed_py(7000 + q); rr = draw_py(4)
+        seed_py(7000 + q)
+        o = M._move_particle_spherical(w, mu, x, r0, r1, sa, ss, dcen)
+        rows.append([w, mu, 0, x, 0, r0, r1, 0, 1, sa, ss, dcen]); draws.append(rr)
+        res.append([o[0], o[1], 0, o[2], 0, o[4], o[5], o[6], {1: 1, -1: 2, 0: 0}[o[3]], {1: 1, 2: 2, 3: 0}[o[7]]])
+    out["ev_in"], out["ev_r"], out["ev_out"] = np.array(rows), np.array(draws), np.array(res)
+    # ---- Planck sampler of MG_IMC1D ----
+    prow, pres = [], []
+    for q in range(30):
+        T = 10 ** rng.uniform(-2, 0.5)
+        seed_np(400 + q)
+        u = draw_np(5 * 40).reshape(40, 5)
+        seed_np(400 + q)
+        _, gg = M._sample_planck_spectrum_mg_jit(40, T, edges[:-1], edges[1:], M._PLANCK_MIXTURE_CDF)
+        for k in range(40):
+            prow.append([T] + list(u[k])); pres.append(gg[k])
+    out["planck_in"], out["planck_group"] = np.array(prow), np.array(pres)
+    return out
+
+
+def run_stats_mg1d(M, seeds=32):
+    edges, nu, funcs = mg1d_setup()
+    I, R, cv = MG1["I"], MG1["R"], MG1["cv"]
+    e = np.linspace(0, R, I + 1)
+    mesh = np.stack([e[:-1], e[1:]], axis=1)
+    seed_py, seed_np, _, _ = nb_helpers()
+    Ts, Trs = [], []
+    for s in range(seeds):
+        np.random.seed(s); random.seed(s); seed_py(s); seed_np(s)
+        st = M.init_simulation(MG1["Ntarget"], np.full(I, MG1["T0"]), np.full(I, MG1["T0"]), mesh, edges,
+                               lambda T: cv * T, lambda u: u / cv)
+        for _ in range(MG1["steps"]):
+            st, info = M.step(st, MG1["Ntarget"], MG1["Nboundary"], 0, MG1["Nmax"], (0.0, MG1["Tb"]), MG1["dt"], mesh,
+                              edges, funcs, lambda u: u / cv, lambda T: cv + 0 * T, np.zeros(I))
+        Ts.append(st.temperature.copy()); Trs.append(st.radiation_temperature.copy())
+    Ts, Trs = np.array(Ts), np.array(Trs)
+    return dict(T_mean=Ts.mean(0), T_se=Ts.std(0, ddof=1) / np.sqrt(seeds), Tr_mean=Trs.mean(0),
+                Tr_se=Trs.std(0, ddof=1) / np.sqrt(seeds), seeds=seeds, **MG1)
+
+
+def main_mg1d():
+    import contextlib
+    import io
+
+    t0 = time.time()
+    M = load_reference_mg1d()
+    with contextlib.redirect_stdout(io.StringIO()):
+        pins = gen_mg1d_pins(M)
+    np.savez_compressed(os.path.join(HERE, "mg1d.npz"), **pins)
+    print(f"MG 1-D pins written ({time.time() - t0:.1f} s)")
+    if "--no-stats" not in sys.argv:
+        with contextlib.redirect_stdout(io.StringIO()):
+            st = run_stats_mg1d(M)
+        np.savez_compressed(os.path.join(HERE, "stats_mg1d.npz"), **st)
+        print(f"MG 1-D statistics written ({time.time() - t0:.1f} s)")
+
+
 def main():
+    if "--mg1d-only" in sys.argv:
+        return main_mg1d()
     t0 = time.time()
     IMC1D, IMC2D = load_reference()
     import contextlib
@@ -359,6 +509,7 @@ def main():
             s3 = run_stats_mg(MG_IMC2D)
         np.savez_compressed(os.path.join(HERE, "stats_mg.npz"), **s3)
         print(f"multigroup statistics written ({time.time() - t0:.1f} s)")
+    main_mg1d()
 
 
 if __name__ == "__main__":
