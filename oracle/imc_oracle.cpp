@@ -324,6 +324,26 @@ inline void iso_dir(int geom, double ua, double ub, double& d1, double& d2) {
   }
 }
 
+/* Carter-Forest absorption (IMC/IMC1D_CarterForest.py:146-194, :678-709;
+ * IMC/IMC2D_CarterForest.py:189-210, :318-340), for an event whose absorption distance won
+ * (EV_SCATTER of the flight run with sigma_s := sigma_a and no implicit capture, which also
+ * drew the new isotropic direction).  rate = c sigma_a beta, 0 when beta or sigma_a <=
+ * 1e-15.  Re-emission after a delay ~ Exp(rate) when it falls inside the step (e.dcen becomes
+ * the distance left after the delay); otherwise capture (returns true).  Without a rate the
+ * 1-D modules redirect the photon and the 2-D module captures it.  The stiff fast path
+ * (threshold > 0) captures with probability exp(-rate t_left), else redirects at once. */
+bool cf_absorb(bool oned, double rate, double fastpath, double ud, EventOut& e) {
+  const double tr = e.dcen / C_LIGHT;
+  if (!(rate > 0)) return !oned;
+  if (fastpath > 0 && tr > 1e-14 && rate * tr > fastpath) return ud < std::exp(-rate * tr);
+  const double delay = -std::log(std::max(ud, 1e-15)) / rate;
+  if (oned ? (tr > 1e-14 && delay < tr) : (delay < tr - 1e-15)) {
+    e.dcen = std::max(0.0, (tr - delay) * C_LIGHT);
+    return false;
+  }
+  return true;
+}
+
 }  // namespace
 
 /* ======================================================================================
@@ -343,6 +363,28 @@ void orc_event(int geom, const double* in, double* out) {
   }
   out[0] = o.w; out[1] = o.d1; out[2] = o.d2; out[3] = o.p1; out[4] = o.p2;
   out[5] = o.dep; out[6] = o.dep_i; out[7] = o.dcen; out[8] = o.cross; out[9] = o.evt;
+}
+
+/* one Carter-Forest event (pins): in = w d1 d2 p1 p2 lo1 hi1 lo2 hi2 sigma_a rate dcen
+ * fastpath u0 u1 u2 u3 (u0 distance; 1-D: u1 direction, u2 delay; 2-D: u1 u2 direction, u3
+ * delay); out = w d1 d2 p1 p2 dep_w dep_i dcen cross evt (0 census, 1 boundary,
+ * 2 absorbed and continuing, 4 captured).  dep_i is w*s (1-D: per unit length / volume). */
+void orc_event_cf(int geom, const double* in, double* out) {
+  EventOut e;
+  const bool oned = geom == G_SLAB || geom == G_SPHERE;
+  switch (geom) {
+    case G_SLAB: e = event_slab(in[0], in[1], in[3], in[5], in[6], 0.0, in[9], in[11], in[13], in[14]); break;
+    case G_SPHERE: e = event_sphere(in[0], in[1], in[3], in[5], in[6], 0.0, in[9], in[11], in[13], in[14]); break;
+    case G_XY: e = event_xy(in[0], in[1], in[2], in[3], in[4], in[5], in[6], in[7], in[8], 0.0, in[9], in[11], in[13], in[14], in[15]); break;
+    default: e = event_rz(in[0], in[1], in[2], in[3], in[4], in[5], in[6], in[7], in[8], 0.0, in[9], in[11], in[13], in[14], in[15]); break;
+  }
+  int evt = e.evt == EV_SCATTER ? 2 : e.evt;
+  double dep_w = 0.0, w = e.w;
+  if (e.evt == EV_SCATTER && cf_absorb(oned, in[10], in[12], oned ? in[15] : in[16], e)) {
+    evt = 4; dep_w = w; w = 0.0; e.dcen = 0.0;
+  }
+  out[0] = w; out[1] = e.d1; out[2] = e.d2; out[3] = e.p1; out[4] = e.p2;
+  out[5] = dep_w; out[6] = e.dep_i; out[7] = e.dcen; out[8] = e.cross; out[9] = evt;
 }
 
 void orc_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
@@ -457,6 +499,8 @@ typedef struct {
   double T_emit_floor;
   int nthreads;
   int sources_only;       /* 1: Fleck + sources appended, no transport (pins) */
+  int method;             /* 0 Fleck-Cummings, 1 Carter-Forest */
+  double cf_fastpath;     /* Carter-Forest stiff fast path threshold (0 = off) */
 } orc_step_in;
 
 typedef struct {
@@ -630,7 +674,9 @@ double rz_r_cdf(double r0, double r1, double a, double M, double xi) {
  * slab: IMC/IMC1D.py:251-316; sphere :629-741; xy IMC/IMC2D.py:1191-1238;
  * rz uniform :1241-1290, rz linear :1326-1445. */
 double volume_source(const Problem& P, const std::vector<double>& QV, const double* T, long long N,
-                     double dt, uint32_t step, uint32_t tag, bool tilt, bool rz_linear, Bank& B) {
+                     double dt, uint32_t step, uint32_t tag, bool tilt, bool rz_linear, Bank& B,
+                     bool min1_round = false, const std::vector<double>* cf_rate = nullptr,
+                     double cf_thr = 0.0) {
   const int nc = ncells(P);
   const double Qt = canon_sum(QV.data(), nc);
   if (!(Qt > 0) || N <= 0) return 0;
@@ -684,7 +730,10 @@ double volume_source(const Problem& P, const std::vector<double>& QV, const doub
   double total = 0;
   uint32_t k = 0;
   for (int c : order) {
-    const long long n = (long long)std::ceil((double)N * QV[c] / Qt);
+    /* Carter-Forest 1-D emission (IMC/IMC1D_CarterForest.py:499, :932): max(1, round) in
+     * every cell, a zero-energy cell included */
+    const long long n = min1_round ? std::max(1LL, (long long)std::nearbyint((double)N * QV[c] / Qt))
+                                   : (long long)std::ceil((double)N * QV[c] / Qt);
     if (n <= 0) continue;
     const double wgt = QV[c] / (double)n;
     const int i = c % P.nx, j = c / P.nx;
@@ -733,7 +782,14 @@ double volume_source(const Problem& P, const std::vector<double>& QV, const doub
       p1 = std::min(std::max(p1, a), b);
       p2 = is1d(P) ? 0.0 : std::min(std::max(p2, lo), hi);
       iso_dir(P.geom, r.u[2], r.u[3], d1, d2);
-      const double t = s.u[0] * dt;  /* reference 1-D fixed source uses U(0,1): fixed to U(0,dt) */
+      double t = s.u[0] * dt;  /* reference 1-D fixed source uses U(0,1): fixed to U(0,dt) */
+      if (cf_rate) {
+        /* Carter-Forest emission time, density ~ exp(-rate t) on [0, dt]
+         * (IMC/IMC1D_CarterForest.py:529-536, IMC/IMC2D_CarterForest.py:51-56):
+         * t = -ln(1 - xi (1 - e^{-rate dt})) / rate, written with log1p / expm1 */
+        const double rt = (*cf_rate)[c];
+        if (rt > cf_thr) t = -std::log1p(s.u[0] * std::expm1(-rt * dt)) / rt;
+      }
       B.push(wgt, d1, d2, t, p1, p2, c, 0);
       total += wgt;
     }
@@ -754,6 +810,23 @@ int orc_step_transport(void* h, const orc_step_in* in, orc_step_out* out) {
   fleck(P, in, sa, ss);
   for (int c = 0; c < nc; ++c)
     if (!(in->T[c] > 0) && is1d(P)) return 1; /* IMC/IMC1D.py:264 asserts T > 0 */
+  /* Carter-Forest (IMC/IMC1D_CarterForest.py:1151-1244, IMC/IMC2D_CarterForest.py:909-1045):
+   * no Fleck factor, sigma_a is the true opacity, no effective scatter; beta = 4aT^3/cv
+   * (2-D: T floored at 1e-12) sets the re-emission rate c sigma_a beta, which is zero when
+   * beta or sigma_a <= 1e-15 (no re-emission) */
+  const bool cf = in->method == 1;
+  std::vector<double> rate_e(nc, 0.0), rate_re(nc, 0.0), beta_c(nc, 0.0);
+  if (cf) {
+    for (int c = 0; c < nc; ++c) {
+      const double Tm = is1d(P) ? in->T[c] : std::max(in->T[c], 1e-12);
+      const double beta = 4.0 * A_RAD * pow3(Tm) / in->cv[c];
+      beta_c[c] = beta;
+      sa[c] = in->sigma[c];
+      ss[c] = 0.0;
+      rate_e[c] = C_LIGHT * in->sigma[c] * beta;
+      rate_re[c] = (beta > 1e-15 && in->sigma[c] > 1e-15) ? rate_e[c] : 0.0;
+    }
+  }
   if (out->sigma_a) std::copy(sa.begin(), sa.end(), out->sigma_a);
   if (out->sigma_s) std::copy(ss.begin(), ss.end(), out->sigma_s);
 
@@ -774,6 +847,15 @@ int orc_step_transport(void* h, const orc_step_in* in, orc_step_out* out) {
   std::vector<double> E(nc);
   for (int c = 0; c < nc; ++c) {
     E[c] = A_RAD * C_LIGHT * pow4(std::max(in->T[c], 0.0)) * sa[c] * in->dt * P.vol[c];
+    if (cf) {
+      /* a T^4 (1 - e^{-rate dt}) / beta V (IMC/IMC1D_CarterForest.py:485-494,
+       * IMC/IMC2D_CarterForest.py:877-883), 1 - e^{-x} without cancellation */
+      const double T4 = pow4(std::max(in->T[c], 0.0));
+      const double beta = beta_c[c];
+      const bool decays = is1d(P) ? rate_e[c] > 1e-10 : (rate_e[c] > 1e-12 && beta > 1e-15);
+      E[c] = decays ? A_RAD * T4 * -std::expm1(-rate_e[c] * in->dt) / beta * P.vol[c]
+                    : A_RAD * T4 * C_LIGHT * in->sigma[c] * in->dt * P.vol[c];
+    }
     if (in->T_emit_floor > 0 && in->T[c] < in->T_emit_floor) E[c] = 0;
     out->emitted[c] = 0;
   }
@@ -781,7 +863,8 @@ int orc_step_transport(void* h, const orc_step_in* in, orc_step_out* out) {
     const size_t n0 = B.size();
     if (in->Ntarget > 0)
       volume_source(P, E, in->T, in->Ntarget, in->dt, in->step, oracle::TAG_EMISSION, true,
-                    (P.geom == G_RZ) && in->rz_linear_source, B);
+                    (P.geom == G_RZ) && in->rz_linear_source, B, cf && is1d(P), cf ? &rate_e : nullptr,
+                    is1d(P) ? 1e-10 : 1e-12);
     /* matter loses exactly the energy carried by the issued emission particles */
     std::vector<KSum> em(nc);
     for (size_t k = n0; k < B.size(); ++k) em[B.cell[k]].add(B.w[k]);
@@ -820,34 +903,49 @@ int orc_step_transport(void* h, const orc_step_in* in, orc_step_out* out) {
     KSum* esc = esc_t[tid].data();
     double w = B.w[k], d1 = B.d1[k], d2 = B.d2[k], p1 = B.p1[k], p2 = B.p2[k];
     int c = B.cell[k];
-    if (!(w > 0)) continue;
+    /* Carter-Forest: an entry at or below the floor is not moved and stays in census
+     * (IMC/IMC2D_CarterForest.py:381; the 1-D module deletes it, :320-322) */
+    if (!(w > 0) || (cf && !(w > floor_w))) continue;
     double dcen = (dt - B.t[k]) * C_LIGHT;
     uint32_t ev = 0;
     bool frozen = false;
     while (dcen > 0) {
       int i = c % P.nx, j = c / P.nx;
       st[S_EVENTS]++;
-      if (!oned && in->max_events > 0 && (long long)ev >= in->max_events) {
+      if ((cf || !oned) && in->max_events > 0 && (long long)ev >= in->max_events) {
         /* IMC/IMC2D.py:974-977: cap hit, particle stays in census with its weight */
         st[S_CAP]++;
         break;
       }
       Draw4 r = draw(P.seed, (uint32_t)k, ev, in->step, oracle::TAG_TRANSPORT);
       ++ev;
+      /* Carter-Forest: the absorption distance is the capped "scatter" distance of sigma_a
+       * and nothing is captured along the flight (weights change only at a capture) */
+      const double sa_e = cf ? 0.0 : sa[c], ss_e = cf ? sa[c] : ss[c];
       EventOut e;
       switch (P.geom) {
-        case G_SLAB: e = event_slab(w, d1, p1, P.e1[i], P.e1[i + 1], sa[c], ss[c], dcen, r.u[0], r.u[1]); break;
-        case G_SPHERE: e = event_sphere(w, d1, p1, P.e1[i], P.e1[i + 1], sa[c], ss[c], dcen, r.u[0], r.u[1]); break;
-        case G_XY: e = event_xy(w, d1, d2, p1, p2, P.e1[i], P.e1[i + 1], P.e2[j], P.e2[j + 1], sa[c], ss[c], dcen, r.u[0], r.u[1], r.u[2]); break;
-        default: e = event_rz(w, d1, d2, p1, p2, P.e1[i], P.e1[i + 1], P.e2[j], P.e2[j + 1], sa[c], ss[c], dcen, r.u[0], r.u[1], r.u[2]); break;
+        case G_SLAB: e = event_slab(w, d1, p1, P.e1[i], P.e1[i + 1], sa_e, ss_e, dcen, r.u[0], r.u[1]); break;
+        case G_SPHERE: e = event_sphere(w, d1, p1, P.e1[i], P.e1[i + 1], sa_e, ss_e, dcen, r.u[0], r.u[1]); break;
+        case G_XY: e = event_xy(w, d1, d2, p1, p2, P.e1[i], P.e1[i + 1], P.e2[j], P.e2[j + 1], sa_e, ss_e, dcen, r.u[0], r.u[1], r.u[2]); break;
+        default: e = event_rz(w, d1, d2, p1, p2, P.e1[i], P.e1[i + 1], P.e2[j], P.e2[j + 1], sa_e, ss_e, dcen, r.u[0], r.u[1], r.u[2]); break;
       }
+      const bool captured = cf && e.evt == EV_SCATTER && cf_absorb(oned, rate_re[c], in->cf_fastpath,
+                                                                   oned ? r.u[2] : r.u[3], e);
       if (e.evt == EV_BOUNDARY) st[S_BOUNDARY]++;
+      else if (captured) st[S_CAPTURE]++;
       else if (e.evt == EV_SCATTER) st[S_SCATTER]++;
       else st[S_CENSUS]++;
       if (oned) { dep[c].add(e.dep); si[c].add(e.dep_i / dt); }
       else { dep[c].add(e.dep / P.vol[c]); si[c].add(e.dep_i / (dt * P.vol[c])); }
       dcen = e.dcen;
-      if (!oned) {
+      if (captured) {
+        dep[c].add(w / P.vol[c]);
+        w = 0; dcen = 0;
+        break;
+      }
+      if (cf) {
+        w = e.w;
+      } else if (!oned) {
         /* IMC/IMC2D.py:1042-1047: at/below the floor the history stops in place,
          * keeping its weight (position and cell from before the event) */
         w = e.w;
@@ -873,7 +971,7 @@ int orc_step_transport(void* h, const orc_step_in* in, orc_step_out* out) {
         }
         if (!escaped) c = i + P.nx * j;
       }
-      if (oned && !escaped && w < floor_w) {
+      if (oned && !cf && !escaped && w < floor_w) {
         /* IMC/IMC1D.py:188-195; the reference deposits only for interior cells and loses
          * the energy in the two edge cells: here every cell gets it (ledger closes). */
         st[S_FLOOR]++;

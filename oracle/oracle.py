@@ -30,7 +30,7 @@ class StepIn(ctypes.Structure):
         ("Ntarget", c_longlong), ("Nboundary", c_longlong), ("Nsource", c_longlong),
         ("source", c_void_p), ("face_T", c_void_p * 4), ("reflect", c_int * 4),
         ("max_events", c_longlong), ("rz_linear_source", c_int), ("T_emit_floor", c_double),
-        ("nthreads", c_int), ("sources_only", c_int),
+        ("nthreads", c_int), ("sources_only", c_int), ("method", c_int), ("cf_fastpath", c_double),
     ]
 
 
@@ -88,6 +88,7 @@ def load():
         lib.orc_comb_with_xi.restype = c_longlong
         lib.orc_comb_with_xi.argtypes = [c_void_p, c_longlong, c_void_p, c_void_p]
         lib.orc_event.argtypes = [c_int, c_void_p, c_void_p]
+        lib.orc_event_cf.argtypes = [c_int, c_void_p, c_void_p]
         lib.orc_init_ic_mg.restype = c_longlong
         lib.orc_init_ic_mg.argtypes = [c_void_p, c_longlong, c_void_p, c_void_p, c_double]
         lib.orc_step_transport_mg.restype = c_int
@@ -137,6 +138,16 @@ def event(geometry: str, inp) -> np.ndarray:
     return out
 
 
+def event_cf(geometry: str, inp) -> np.ndarray:
+    """One Carter-Forest event.  inp = (w d1 d2 p1 p2 lo1 hi1 lo2 hi2 sigma_a rate dcen
+    fastpath u0 u1 u2 u3); returns (w d1 d2 p1 p2 dep_w dep_i dcen crossed evt)."""
+    lib = load()
+    a = np.ascontiguousarray(inp, dtype=np.float64)
+    out = np.zeros(10)
+    lib.orc_event_cf(GEOM[geometry], _p(a), _p(out))
+    return out
+
+
 class Oracle:
     def __init__(self, geometry: str, edges1, edges2, volumes_flat, seed: int, n_groups: int = 1):
         self.lib = load()
@@ -181,7 +192,9 @@ class Oracle:
         self.lib.orc_set_bank(self.h, len(arrs[0]), *[_p(a) for a in arrs], _p(c), _p(g))
 
     def transport(self, T, sigma, cv, source, step, dt, theta, Ntarget, Nboundary, Nsource, face_T, reflect,
-                  max_events=0, rz_linear_source=True, t_emit_floor=0.0, nthreads=None, sources_only=False) -> dict:
+                  max_events=0, rz_linear_source=True, t_emit_floor=0.0, nthreads=None, sources_only=False,
+                  method="fc", cf_fastpath=0.0) -> dict:
+        """Sources + transport of one step; method 'fc' (Fleck-Cummings) or 'cf' (Carter-Forest)."""
         keep = []
 
         def arr(x):
@@ -205,6 +218,8 @@ class Oracle:
         si.T_emit_floor = float(t_emit_floor)
         si.nthreads = int(nthreads or os.cpu_count() or 1)
         si.sources_only = int(bool(sources_only))
+        si.method = {"fc": 0, "cf": 1}[method]
+        si.cf_fastpath = float(cf_fastpath)
         out = {k: np.zeros(self.nc) for k in ("dep", "si", "emitted", "sigma_a", "sigma_s")}
         so = StepOut()
         so.dep, so.si, so.emitted, so.sigma_a, so.sigma_s = (_p(out[k]) for k in ("dep", "si", "emitted", "sigma_a", "sigma_s"))
@@ -364,14 +379,14 @@ class OracleGray:
 
     def step(self, Ntarget, Nboundary, Nsource, Nmax, face_T, dt, sigma_a_func, inv_eos, cv, source=None,
              reflect=(False, False, False, False), theta=1.0, conserve_comb_energy=False, max_events=0,
-             rz_linear_source=True):
+             rz_linear_source=True, method="fc", cf_fastpath=0.0):
         Tg = self.grid(self.T)
         sigma = flat2d(np.broadcast_to(sigma_a_func(Tg), Tg.shape))
         cvv = flat2d(np.broadcast_to(cv(Tg), Tg.shape))
         src = None if source is None else flat2d(source)
         r = self.o.transport(self.T, sigma, cvv, src, self.count, dt, theta, Ntarget, Nboundary, Nsource, face_T,
                              reflect, max_events=max_events, rz_linear_source=rz_linear_source,
-                             nthreads=self.nthreads)
+                             nthreads=self.nthreads, method=method, cf_fastpath=cf_fastpath)
         self.e = self.e + r["dep"] - r["emitted"] / self.o.vol
         self.T = flat2d(inv_eos(self.grid(self.e)))
         self.Tr = np.sqrt(np.sqrt(np.maximum(r["si"], 0) / A_RAD / C_LIGHT))

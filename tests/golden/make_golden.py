@@ -14,12 +14,15 @@ RADTRANBOOK_REF); the fixtures it writes are small .npz files committed with thi
   sources.npz    per-cell counts and weights of IMC/IMC1D.py:251 emitted_particles and
                  IMC/IMC2D.py:1326 _sample_source_rz_linear (the deterministic part of sampling)
   planck.npz     MG_IMC/MG_IMC2D.py:202 Planck (mixture-of-Gammas) group sampler, with its draws
+  cf.npz         Carter-Forest pins: the four event functions of IMC/IMC1D_CarterForest.py and
+                 IMC/IMC2D_CarterForest.py with their draws, and the emission samplers' counts,
+                 weights and energies
   mg1d.npz       MG_IMC/MG_IMC1D.py pins: stratified emission / IC / fixed-source counts and
                  weights, the per-(cell, group) comb in both energy modes, the spherical event
                  and the Planck sampler, with their draws
   stats_*.npz    multi-seed statistics of whole reference steps (IMC1D.step, IMC2D.step,
                  MG_IMC2D.step and MG_IMC1D.step with planck_shim/ standing in for the
-                 external planck_integrals):
+                 external planck_integrals; IMC1D_CarterForest.step, IMC2D_CarterForest.step):
                  per-cell mean and standard error of material and radiation temperature
 
 The reference's random numbers cannot be reproduced by a different generator, so whole-step
@@ -473,9 +476,177 @@ def main_mg1d():
         print(f"MG 1-D statistics written ({time.time() - t0:.1f} s)")
 
 
+def load_reference_cf():
+    sys.path.insert(0, os.path.join(REF, "IMC"))
+    import IMC1D_CarterForest as CF1  # noqa: E402
+    import IMC2D_CarterForest as CF2  # noqa: E402
+    return CF1, CF2
+
+
+def gen_cf_pins(CF1, CF2, n=300, seed=29):
+    """Carter-Forest pins: the four event functions (IMC/IMC1D_CarterForest.py:63 move_particle_cf,
+    :614 move_particle_spherical_cf, IMC/IMC2D_CarterForest.py:102 _move_particle_xy_cf_jit,
+    :216 _move_particle_rz_cf_jit) with the draws they consumed, and the emission samplers'
+    per-cell counts, weights and energies (:442 emitted_particles, :889
+    emitted_particles_spherical, IMC/IMC2D_CarterForest.py:876 _sample_internal_emission_cf)."""
+    seed_py, seed_np, draw_py, _ = nb_helpers()
+    rng = np.random.default_rng(seed)
+    out = {}
+
+    def sig():
+        k = rng.integers(0, 5)
+        return 0.0 if k == 0 else float(10 ** rng.uniform(-3, 7))
+
+    def bet():
+        return 1e-17 if rng.uniform() < 0.15 else float(10 ** rng.uniform(-4, 1))
+
+    def fpath():
+        return float(10 ** rng.uniform(-1, 1)) if rng.uniform() < 0.2 else 0.0
+
+    rows, draws, res = [], [], []
+    for q in range(n):  # slab
+        xl = rng.uniform(0, 1); dx = 10 ** rng.uniform(-3, -1); xr = xl + dx
+        x = xl + dx * rng.uniform(0.02, 0.98); mu = rng.uniform(-1, 1)
+        w = 10 ** rng.uniform(-3, 1); sa = sig(); b = bet(); dcen = 10 ** rng.uniform(-4, 0); fp = fpath()
+        seed_py(11000 + q); r = draw_py(6); seed_py(11000 + q)
+        o = CF1.move_particle_cf(w, mu, x, 0.0, xl, xr, sa, b, dcen, fp)
+        rows.append([w, mu, 0, x, 0, xl, xr, 0, 1, sa, b, dcen, fp]); draws.append(r)
+        res.append([o[0], o[1], 0, o[2], 0, o[5], o[6], o[7], {1: 1, -1: 2, 0: 0}[o[4]], {1: 1, 2: 2, 3: 0, 4: 4}[o[8]]])
+    out["slab_in"], out["slab_r"], out["slab_out"] = np.array(rows), np.array(draws), np.array(res)
+    rows, draws, res = [], [], []
+    for q in range(n):  # sphere
+        r0 = rng.choice([0.0, 10 ** rng.uniform(-2, 0)], p=[0.2, 0.8]); dr = 10 ** rng.uniform(-3, -1); r1 = r0 + dr
+        x = r0 + dr * rng.uniform(0.02, 0.98); mu = rng.uniform(-1, 1)
+        w = 10 ** rng.uniform(-3, 1); sa = sig(); b = bet(); dcen = 10 ** rng.uniform(-4, 0); fp = fpath()
+        seed_py(12000 + q); r = draw_py(6); seed_py(12000 + q)
+        o = CF1.move_particle_spherical_cf(w, mu, x, 0.0, r0, r1, sa, b, dcen, fp)
+        rows.append([w, mu, 0, x, 0, r0, r1, 0, 1, sa, b, dcen, fp]); draws.append(r)
+        res.append([o[0], o[1], 0, o[2], 0, o[5], o[6], o[7], {1: 1, -1: 2, 0: 0}[o[4]], {1: 1, 2: 2, 3: 0, 4: 4}[o[8]]])
+    out["sphere_in"], out["sphere_r"], out["sphere_out"] = np.array(rows), np.array(draws), np.array(res)
+    for geo in ("xy", "rz"):
+        rows, draws, res = [], [], []
+        e1 = np.concatenate([[0.0], np.cumsum(10 ** rng.uniform(-2, -0.5, 12))])
+        e2 = np.concatenate([[0.0], np.cumsum(10 ** rng.uniform(-2, -0.5, 12))])
+        for q in range(n):
+            i = int(rng.integers(0, 12)); j = int(rng.integers(0, 12))
+            a1, b1, a2, b2 = e1[i], e1[i + 1], e2[j], e2[j + 1]
+            p1 = a1 + (b1 - a1) * rng.uniform(0.02, 0.98); p2 = a2 + (b2 - a2) * rng.uniform(0.02, 0.98)
+            if geo == "xy":
+                uz = rng.uniform(-1, 1); ph = rng.uniform(0, 2 * np.pi); rxy = np.sqrt(1 - uz * uz)
+                d1, d2 = rxy * np.cos(ph), rxy * np.sin(ph)
+            else:
+                d1, d2 = rng.uniform(-1, 1), rng.uniform(-1, 1)
+            w = 10 ** rng.uniform(-3, 1); sa = sig(); b = bet(); dcen = 10 ** rng.uniform(-4, 0); fp = fpath()
+            seed_py(13000 + q); r = draw_py(6); seed_py(13000 + q)
+            fn = CF2._move_particle_xy_cf_jit if geo == "xy" else CF2._move_particle_rz_cf_jit
+            o = fn(w, d1, d2, p1, p2, i, j, e1, e2, sa, b, dcen, 0.0, fp)
+            rows.append([w, d1, d2, p1, p2, a1, b1, a2, b2, sa, b, dcen, fp]); draws.append(r)
+            # (w, d1, d2, p1, p2, time, crossed, dep_w, dep_i, dcen, evt)
+            res.append([o[0], o[1], o[2], o[3], o[4], o[7], o[8], o[9], o[6], o[10]])
+        out[f"{geo}_in"], out[f"{geo}_r"], out[f"{geo}_out"] = np.array(rows), np.array(draws), np.array(res)
+    # ---- emission samplers ----
+    I = 25
+    for geo in ("slab", "spherical"):
+        Ts, sas, cvs, Ns, cnts, ws, Es = [], [], [], [], [], [], []
+        for q in range(6):
+            T = 10 ** rng.uniform(-1.5, 0.3, I); sa = 10 ** rng.uniform(-1, 3, I); cv = 10 ** rng.uniform(-2, 0, I)
+            beta = 4.0 * 0.01372 * T ** 3 / cv
+            N = int(rng.integers(500, 5000)); dt = 0.01
+            e = np.linspace(0.0, 1.0, I + 1)
+            mesh = np.stack([e[:-1], e[1:]], axis=1)
+            seed_np(500 + q); seed_py(500 + q)
+            fn = CF1.emitted_particles if geo == "slab" else CF1.emitted_particles_spherical
+            w, mu, t, x, c, E = fn(N, T, dt, mesh, sa, beta)
+            cnt = np.bincount(c, minlength=I); wc = np.zeros(I); wc[c] = w
+            Ts.append(T); sas.append(sa); cvs.append(cv); Ns.append(N); cnts.append(cnt); ws.append(wc); Es.append(E)
+        out.update({f"em_{geo}_T": np.array(Ts), f"em_{geo}_sa": np.array(sas), f"em_{geo}_cv": np.array(cvs),
+                    f"em_{geo}_N": np.array(Ns), f"em_{geo}_counts": np.array(cnts), f"em_{geo}_w": np.array(ws),
+                    f"em_{geo}_E": np.array(Es)})
+    nx, ny = 10, 8
+    e1 = np.linspace(0, 1, nx + 1); e2 = np.linspace(0, 2, ny + 1)
+    vol = np.diff(e1)[:, None] * np.diff(e2)[None, :]
+    Ts, sas, cvs, Ns, cnts, ws, Es = [], [], [], [], [], [], []
+    for q in range(6):
+        T = 10 ** rng.uniform(-1.5, 0.3, (nx, ny)); sa = 10 ** rng.uniform(-1, 3, (nx, ny))
+        cv = 10 ** rng.uniform(-2, 0, (nx, ny))
+        beta = 4.0 * 0.01372 * np.maximum(T, 1e-12) ** 3 / cv
+        N = int(rng.integers(500, 5000))
+        seed_np(600 + q); seed_py(600 + q)
+        smp, E = CF2._sample_internal_emission_cf(N, T, 0.01, e1, e2, vol, sa, beta, "xy", False)
+        w, d1, d2, t, p1, p2, ci, cj = smp
+        flat = ci + nx * cj
+        cnt = np.bincount(flat, minlength=nx * ny); wc = np.zeros(nx * ny); wc[flat] = w
+        Ts.append(T); sas.append(sa); cvs.append(cv); Ns.append(N); cnts.append(cnt); ws.append(wc); Es.append(E)
+    out.update(em_xy_T=np.array(Ts), em_xy_sa=np.array(sas), em_xy_cv=np.array(cvs), em_xy_N=np.array(Ns),
+               em_xy_counts=np.array(cnts), em_xy_w=np.array(ws), em_xy_E=np.array(Es))
+    return out
+
+
+CFX = dict(nx=30, ny=3, L=0.3, cv=0.3, T0=0.05, dt=0.01, steps=3, Ntarget=3000, Nboundary=3000, Nmax=12000)
+
+
+def run_stats_cf(CF1, CF2, seeds=32):
+    """Carter-Forest whole steps: a slab Marshak wave (sigma = 100 T^-3, 10 steps) through
+    IMC1D_CarterForest.step, and a 30 x 3 XY Marshak wave through IMC2D_CarterForest.step."""
+    seed_py, seed_np, _, _ = nb_helpers()
+    I = 100
+    mesh = np.array([[i * 0.002, (i + 1) * 0.002] for i in range(I)])
+    cv = 0.3
+    Ts, Trs = [], []
+    for s in range(seeds):
+        np.random.seed(s); random.seed(s); seed_py(s); seed_np(s)
+        st = CF1.init_simulation(2000, np.full(I, 0.001), np.full(I, 0.001), mesh, lambda T: cv * T, lambda e: e / cv)
+        for _ in range(10):
+            st, info = CF1.step(st, 2000, 2000, 0, 8000, (1.0, 0.0), 0.01, mesh, lambda T: 100.0 * T ** -3,
+                                lambda e: e / cv, lambda T: cv + 0 * T, np.zeros(I))
+        Ts.append(st.temperature.copy()); Trs.append(st.radiation_temperature.copy())
+    Ts, Trs = np.array(Ts), np.array(Trs)
+    slab = dict(T_mean=Ts.mean(0), T_se=Ts.std(0, ddof=1) / np.sqrt(seeds), Tr_mean=Trs.mean(0),
+                Tr_se=Trs.std(0, ddof=1) / np.sqrt(seeds), seeds=seeds, steps=10, A=100.0)
+    nx, ny = CFX["nx"], CFX["ny"]
+    x_e = np.linspace(0, CFX["L"], nx + 1); y_e = np.linspace(0, 0.1, ny + 1)
+    cvx = CFX["cv"]
+    Ts, Trs = [], []
+    for s in range(seeds):
+        np.random.seed(s); random.seed(s); seed_py(s); seed_np(s)
+        st = CF2.init_simulation(CFX["Ntarget"], np.full((nx, ny), CFX["T0"]), np.full((nx, ny), CFX["T0"]), x_e, y_e,
+                                 lambda T: cvx * T, lambda e: e / cvx, geometry="xy")
+        for _ in range(CFX["steps"]):
+            st, info = CF2.step(st, CFX["Ntarget"], CFX["Nboundary"], 0, CFX["Nmax"], (1.0, 0.0, 0.0, 0.0), CFX["dt"],
+                                x_e, y_e, lambda T: 1.0 * np.maximum(T, 1e-3) ** -3, lambda e: e / cvx,
+                                lambda T: cvx + 0 * T, np.zeros((nx, ny)), reflect=(False, False, True, True),
+                                geometry="xy")
+        Ts.append(st.temperature.copy()); Trs.append(st.radiation_temperature.copy())
+    Ts, Trs = np.array(Ts), np.array(Trs)
+    xy = dict(T_mean=Ts.mean(0), T_se=Ts.std(0, ddof=1) / np.sqrt(seeds), Tr_mean=Trs.mean(0),
+              Tr_se=Trs.std(0, ddof=1) / np.sqrt(seeds), seeds=seeds, **CFX)
+    return slab, xy
+
+
+def main_cf():
+    import contextlib
+    import io
+
+    t0 = time.time()
+    load_reference()
+    CF1, CF2 = load_reference_cf()
+    with contextlib.redirect_stdout(io.StringIO()):
+        pins = gen_cf_pins(CF1, CF2)
+    np.savez_compressed(os.path.join(HERE, "cf.npz"), **pins)
+    print(f"Carter-Forest pins written ({time.time() - t0:.1f} s)")
+    if "--no-stats" not in sys.argv:
+        with contextlib.redirect_stdout(io.StringIO()):
+            slab, xy = run_stats_cf(CF1, CF2)
+        np.savez_compressed(os.path.join(HERE, "stats_cf_slab.npz"), **slab)
+        np.savez_compressed(os.path.join(HERE, "stats_cf_xy.npz"), **xy)
+        print(f"Carter-Forest statistics written ({time.time() - t0:.1f} s)")
+
+
 def main():
     if "--mg1d-only" in sys.argv:
         return main_mg1d()
+    if "--cf-only" in sys.argv:
+        return main_cf()
     t0 = time.time()
     IMC1D, IMC2D = load_reference()
     import contextlib
@@ -510,6 +681,7 @@ def main():
         np.savez_compressed(os.path.join(HERE, "stats_mg.npz"), **s3)
         print(f"multigroup statistics written ({time.time() - t0:.1f} s)")
     main_mg1d()
+    main_cf()
 
 
 if __name__ == "__main__":
