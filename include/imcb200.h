@@ -122,7 +122,18 @@ typedef struct imc_step_params {
   const double* emission_fractions; /* MG: [g] fixed emission spectrum, or NULL = Planck */
   int64_t n_boundary_side[4];   /* > 0: boundary particles on that side instead of n_boundary
                                    (per-side budgets, MG_IMC/MG_IMC1D.py:1000-1040) */
+  int32_t method;               /* IMC_METHOD_FLECK_CUMMINGS or IMC_METHOD_CARTER_FOREST (gray) */
+  int32_t pad_method;
+  double cf_fastpath;           /* Carter-Forest stiff fast path: when rate * t_left exceeds it,
+                                   capture with probability exp(-rate t_left) (0 = off) */
 } imc_step_params;
+
+/* Carter-Forest (IMC/IMC1D_CarterForest.py, IMC/IMC2D_CarterForest.py): no Fleck factor;
+ * sigma_a is the true opacity and there is no effective scatter; emission a T^4 (1 - e^{-k dt})
+ * / beta V per cell (k = c sigma_a beta, beta = 4 a T^3 / cv) with birth times of density
+ * ~ e^{-k t}; an absorbed photon is re-emitted isotropically after a delay ~ Exp(k) when that
+ * falls inside the step and is captured (its weight deposited) otherwise. */
+enum { IMC_METHOD_FLECK_CUMMINGS = 0, IMC_METHOD_CARTER_FOREST = 1 };
 
 typedef struct imc_tallies {    /* device outputs, overwritten by each step */
   double* dep;                  /* [g][c] energy deposited per unit volume */

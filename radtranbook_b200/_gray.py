@@ -185,9 +185,10 @@ def face_temperatures(dim: int, geometry: str, T_boundary, time_now: float, e1: 
 def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, sigma_a_func, inv_eos, cv,
               source, reflect, theta, use_scalar_intensity_Tr, conserve_comb_energy, T_emit_floor=0.0,
               rz_linear_source=True, max_events=0, boundary_source_func=None, geometry="slab",
-              allreduce=None):
-    """One time step.  With device material callables the host synchronises once, at the
-    end (sizes, energies and statistics come back in one device summary).
+              allreduce=None, method="fc", cf_fastpath=0.0):
+    """One time step (method 'fc' Fleck-Cummings, 'cf' Carter-Forest).  With device material
+    callables the host synchronises once, at the end (sizes, energies and statistics come
+    back in one device summary).
 
     allreduce: a torch.distributed module when each rank runs an independent replica of the
     problem (its own Philox key and full particle counts); the per-cell tallies and escaped
@@ -214,7 +215,9 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
     refl = tuple(reflect) + (False,) * (4 - len(reflect))
     t_eval = _time.perf_counter()
     eng.transport_async(state._T, sigma, cvv, src, state.count, dt, theta, Ntarget, Nboundary, Nsource, faces,
-                        refl, max_events=max_events, rz_linear_source=rz_linear_source, t_emit_floor=T_emit_floor)
+                        refl, max_events=max_events, rz_linear_source=rz_linear_source, t_emit_floor=T_emit_floor,
+                        method=_lib.METHOD_CARTER_FOREST if method == "cf" else _lib.METHOD_FLECK_CUMMINGS,
+                        cf_fastpath=cf_fastpath)
     world = 1
     if allreduce is not None:
         world = allreduce.get_world_size()
@@ -305,7 +308,12 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
         },
     }
     te = info["profiling"]["transport_events"]
-    if dim == 1:
+    if method == "cf":
+        # IMC/IMC1D_CarterForest.py:1359-1372 and IMC/IMC2D_CarterForest.py:1141-1152 keys
+        te["absorption_continue_events"] = int(stats[_lib.STAT_SCATTER])
+        te["absorption_capture_events"] = int(stats[_lib.STAT_CAPTURE])
+        te["event_cap_hits"] = int(stats[_lib.STAT_CAP])
+    elif dim == 1:
         te["scatter_events"] = int(stats[_lib.STAT_SCATTER])
     else:
         te["absorption_continue_events"] = int(stats[_lib.STAT_SCATTER])

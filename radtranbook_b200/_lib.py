@@ -29,6 +29,7 @@ STATUS = {
 OK, BANK_OVERFLOW = 0, 1
 
 COMB_PER_GROUP, COMB_CONSERVE_RADIATION = 1, 2  # imc_comb flags
+METHOD_FLECK_CUMMINGS, METHOD_CARTER_FOREST = 0, 1  # imc_step_params.method
 
 STAT_EVENTS, STAT_BOUNDARY, STAT_SCATTER, STAT_CENSUS, STAT_CAPTURE, STAT_FLOOR, STAT_REFLECT, STAT_CAP, STAT_ESCAPE, STAT_N = range(10)
 
@@ -64,6 +65,7 @@ class ImcStepParams(ctypes.Structure):
         ("block_size", c_int32), ("blocks_per_sm", c_int32), ("chunk", c_int32), ("reserved", c_int32),
         ("emission_fractions", c_void_p),
         ("n_boundary_side", c_int64 * 4),
+        ("method", c_int32), ("pad_method", c_int32), ("cf_fastpath", c_double),
     ]
 
 

@@ -59,15 +59,18 @@ __device__ __forceinline__ int order_to_cell(int o, int nx, int ny) {
   return i + nx * j;
 }
 
-// Volume-source counts (ceil(N QV_c / Q), in source order), per-cell weights and the
-// energy actually issued per cell (n_c times the FP32 weight, exact in FP64).
+// Volume-source counts (ceil(N QV_c / Q), in source order; min1_round: max(1, round), the
+// Carter-Forest 1-D emission rule), per-cell weights and the energy actually issued per
+// cell (n_c times the FP32 weight, exact in FP64).
 __device__ inline long long plan_volume(const double* QV, long long N, int nx, int ny, int nc, long long* cnt,
-                                 long long* off, float* w, double* issued, double* red, long long* sh) {
+                                 long long* off, float* w, double* issued, double* red, long long* sh,
+                                 bool min1_round = false) {
   const double Qt = block_canon_sum(QV, nc, red);
   for (int o = threadIdx.x; o < nc; o += NT) {
     const int c = order_to_cell(o, nx, ny);
     long long n = 0;
-    if (Qt > 0.0 && N > 0) n = (long long)ceil((double)N * QV[c] / Qt);
+    if (Qt > 0.0 && N > 0)
+      n = min1_round ? max(1LL, (long long)rint((double)N * QV[c] / Qt)) : (long long)ceil((double)N * QV[c] / Qt);
     cnt[o] = n;
     const float wc = n > 0 ? (float)(QV[c] / (double)n) : 0.f;
     w[c] = wc;

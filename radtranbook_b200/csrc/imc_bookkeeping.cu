@@ -51,6 +51,23 @@ __global__ void k_plan_cells(PlanArgs a) {
     const double iv = 1.0 / a.vol[c];
     a.cellf[c] = make_double2(iv, sa > sa_thr ? 1.0 / (sa * a.vol[c] * a.dt) : -1.0 / (a.vol[c] * a.dt));
     double E = A_RAD * C_LIGHT * pow4(fmax(T, 0.0)) * sa * a.dt * a.vol[c];
+    if (a.method == IMC_METHOD_CARTER_FOREST) {
+      // Carter-Forest (IMC/IMC1D_CarterForest.py:1181-1185, 485-494; IMC/IMC2D_CarterForest.py:
+      // 947-948, 877-883): true opacity, no effective scatter (the tracking kernel samples the
+      // absorption distance from the scatter slot), path-length intensity only, emission
+      // a T^4 (1 - e^{-k dt}) / beta V with k = c sigma beta
+      const double sig = a.sigma[c];
+      const double Tm = oned ? T : fmax(T, 1e-12);
+      const double beta = 4.0 * A_RAD * pow3(Tm) / a.cv[c];
+      const double rate = C_LIGHT * sig * beta;
+      a.sa[c] = sig; a.ss[c] = 0.0;
+      a.sass[c] = make_float2(0.f, (float)sig);
+      a.cellf[c] = make_double2(iv, -1.0 / (a.vol[c] * a.dt));
+      a.cf_rate[c] = (beta > 1e-15 && sig > 1e-15) ? (float)rate : 0.f;
+      const double T4 = pow4(fmax(T, 0.0));
+      const bool decays = oned ? rate > 1e-10 : (rate > 1e-12 && beta > 1e-15);
+      E = decays ? A_RAD * T4 * -expm1(-rate * a.dt) / beta * a.vol[c] : A_RAD * T4 * C_LIGHT * sig * a.dt * a.vol[c];
+    }
     if (a.t_emit_floor > 0.0 && T < a.t_emit_floor) E = 0.0;
     a.emit_E[c] = E;
   }
@@ -106,6 +123,10 @@ __global__ void k_plan_cells(PlanArgs a) {
       const double Pn = (q0 + q1 > 0.0) ? q0 / (q0 + q1) : 0.5;
       tl[0] = ar; tl[1] = Mloc; tl[2] = Pn;
     }
+    if (a.method == IMC_METHOD_CARTER_FOREST) {
+      const double Tm = oned ? a.T[c] : fmax(a.T[c], 1e-12);
+      tl[3] = C_LIGHT * a.sigma[c] * (4.0 * A_RAD * pow3(Tm) / a.cv[c]);  // birth-time rate
+    }
   }
 }
 
@@ -117,8 +138,11 @@ __global__ void __launch_bounds__(NT) k_plan(PlanArgs a) {
   const bool oned = (a.geom == G_SLAB || a.geom == G_SPHERE);
 
   // ---- emission counts / weights / offsets ----
+  // Carter-Forest 1-D emission counts are max(1, round) in every cell
+  // (IMC/IMC1D_CarterForest.py:499, :932); otherwise ceil
+  const bool cf1 = a.method == IMC_METHOD_CARTER_FOREST && oned;
   const long long n_emit = plan_volume(a.emit_E, a.n_target, a.nx, a.ny, nc, a.emit_n, a.emit_off,
-                                       a.emit_w, a.emitted, red, sh);
+                                       a.emit_w, a.emitted, red, sh, cf1);
   const double e_emit = block_canon_sum(a.emitted, nc, red);
 
   // ---- fixed source (reference: only when max(source) > 0) ----

@@ -113,6 +113,9 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   if (!bank_ok(bank, two_d, mg) || !workspace) return IMC_ERR_INVALID_ARG;
   if (!(par->dt > 0.0) || par->n_target < 0 || par->n_boundary < 0 || par->n_source < 0) return IMC_ERR_INVALID_ARG;
   for (int q = 0; q < 4; ++q) if (par->n_boundary_side[q] < 0) return IMC_ERR_INVALID_ARG;
+  const bool cf = par->method == IMC_METHOD_CARTER_FOREST;
+  if (par->method != IMC_METHOD_FLECK_CUMMINGS && !cf) return IMC_ERR_INVALID_ARG;
+  if (cf && (mg || adj)) return IMC_ERR_INVALID_ARG;  // Carter-Forest: gray forward steps
   const long long bound = source_bound(mesh, par);
   const long long n_upper = bank->size + bound;
   if (n_upper > bank->capacity) return IMC_ERR_BANK_OVERFLOW;
@@ -134,6 +137,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   for (int q = 0; q < 4; ++q) pa.n_side[q] = side_count(par, q);
   for (int q = 0; q < 4; ++q) pa.face_T[q] = par->face_T[q];
   pa.rz_linear = par->rz_linear_source; pa.t_emit_floor = par->t_emit_floor;
+  pa.method = par->method; pa.cf_rate = ws_ptr<float>(workspace, L.cf_rate);
   pa.sa = tal->sigma_a; pa.ss = tal->sigma_s;
   pa.sass = ws_ptr<float2>(workspace, L.sass); pa.cellf = ws_ptr<double2>(workspace, L.cellf);
   pa.e1f = ws_ptr<float>(workspace, L.e1f); pa.e2f = ws_ptr<float>(workspace, L.e2f);
@@ -217,6 +221,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     IMC_CUDA(imc_launch_fill_boundary(ba, s));
   }
   const int nbins = mg1 ? nc * ng : nc;  // source order positions (MG 1-D: (group, cell) bins)
+  bool cf_times = false;
   auto fill = [&](const int64_t* d_n, const int64_t* d_base, long long n_bound, const long long* off,
                   const float* w, const double* tilt, int kind, uint32_t tag) -> cudaError_t {
     FillArgs fa{};
@@ -228,6 +233,10 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     fa.time_scale = par->dt; fa.seed = par->seed; fa.step = par->step; fa.tag = tag;
     fa.p1 = bank->pos1; fa.p2 = p2; fa.d1 = bank->dir1; fa.d2 = d2; fa.wb = bank->weight;
     fa.t = bank->time; fa.cell = bank->cell; fa.group = bank->group;
+    if (cf_times) {
+      fa.cf_rate4 = pa.tilt + 3;
+      fa.cf_thr = (mesh->geometry == IMC_GEOM_SLAB || mesh->geometry == IMC_GEOM_SPHERE) ? 1e-10 : 1e-12;
+    }
     return imc_launch_fill_volume(fa, s);
   };
   auto fill_mg = [&](const int64_t* d_n, const int64_t* d_base, long long n_bound, const double* cdf,
@@ -262,9 +271,12 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   if (mesh->geometry == IMC_GEOM_SLAB) ekind = 1;
   else if (mesh->geometry == IMC_GEOM_SPHERE) ekind = 2;
   else if (rzlin) ekind = 3;
-  if (!mg && par->n_target > 0)
+  if (!mg && par->n_target > 0) {
+    cf_times = cf;  // Carter-Forest birth times for the emission only
     IMC_CUDA(fill(&sum->n_emission, &sum->base_emission, par->n_target + nc, pa.emit_off, pa.emit_w,
                   ekind ? pa.tilt : nullptr, ekind, imcdev::TAG_EMISSION));
+    cf_times = false;
+  }
 
   // ---- tracking ----
   if (pe.ok) IMC_CUDA(cudaEventRecord(pe.e[1], s));
@@ -287,6 +299,8 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   ta.n_dev = &sum->n_bank; ta.wsum = &sum->weight_sum; ta.queue = queue; ta.flags = &sum->flags;
   ta.dt = (float)par->dt;
   ta.floor_coef = mg1 ? 1e-14 : 1e-10;
+  ta.cf_rate = cf ? pa.cf_rate : nullptr;
+  ta.cf_fastpath = (float)par->cf_fastpath;
   int rm = 0;
   for (int q = 0; q < 4; ++q) if (par->reflect[q]) rm |= 1 << q;
   ta.reflect_mask = rm;
@@ -401,6 +415,7 @@ WsLayout imc_ws_layout(const imc_mesh* m, int64_t capacity) {
   L.cnt = take(4 * cap); L.blk = take(8 * ((cap + 1023) / 1024 + 2));
   L.comb_mode = take(16);
   L.dep_fx = take(8 * ncg); L.esc_fx = take(8 * (4 + ng));
+  L.cf_rate = take(4 * nc);
   L.total = o;
   return L;
 }

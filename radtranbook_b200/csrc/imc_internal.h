@@ -42,6 +42,8 @@ struct TrackArgs {
   double* escaped_group;     // MG: [ng]
   unsigned long long* dep_fx; // [g][c] deposited energy, fixed point (zeroed before launch)
   unsigned long long* esc_fx; // [4 + ng] escaped energy by side, then by group (MG)
+  const float* cf_rate;      // Carter-Forest: [c] re-emission rate c sigma_a beta (0: none), else NULL
+  float cf_fastpath;         // Carter-Forest stiff fast-path threshold (0 = off)
 };
 
 cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool smem_cells, bool prefetch,
@@ -85,6 +87,7 @@ struct WsLayout {
   size_t blk;                 // int64 [nblk+1] comb block totals / offsets
   size_t comb_mode;           // int32 mode + uint64 live-entry count (comb)
   size_t dep_fx, esc_fx;      // uint64 [ncg], [4 + ng] fixed-point energy tallies
+  size_t cf_rate;             // float [nc] Carter-Forest re-emission rate
   size_t total;
 };
 
@@ -107,6 +110,8 @@ struct PlanArgs {
   const double* face_T[4];
   int rz_linear;
   double t_emit_floor;
+  int method;                      // IMC_METHOD_*
+  float* cf_rate;                  // Carter-Forest: [c] re-emission rate (tilt[4c+3]: emission rate)
   // outputs
   double* sa; double* ss;          // FP64 [ncg]
   float2* sass;                    // FP32 [ncg]
@@ -177,6 +182,9 @@ struct FillArgs {
   float* p1; float* p2; float* d1; float* d2; float* wb; float* t; int* cell; int* group;
   // MG 1-D initial census: group from the Planck spectrum at tr[c] (NULL otherwise)
   const double* tr; const double* gedges; const double* mixcdf; int ng;
+  // Carter-Forest emission: birth time of density ~ exp(-k t) on [0, dt], k = cf_rate4[4c]
+  // when k > cf_thr (else uniform); NULL otherwise
+  const double* cf_rate4; double cf_thr;
 };
 cudaError_t imc_launch_fill_volume(const FillArgs& a, cudaStream_t s);
 

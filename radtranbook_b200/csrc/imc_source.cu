@@ -77,7 +77,14 @@ __global__ void k_fill_volume(FillArgs a) {
     if (a.p2) a.p2[b] = (float)p2;
     if (a.d2) a.d2[b] = (float)d2;
     a.wb[b] = a.w[a.bins_by_group ? o : c];
-    a.t[b] = (float)(s0 * a.time_scale);
+    double tb = s0 * a.time_scale;
+    if (a.cf_rate4) {
+      // Carter-Forest birth time, density ~ exp(-k t) on [0, dt]: t = -ln(1 - xi (1 - e^{-k dt})) / k
+      // (IMC/IMC1D_CarterForest.py:529-536, IMC/IMC2D_CarterForest.py:51-56)
+      const double k = a.cf_rate4[4 * c];
+      if (k > a.cf_thr) tb = -log1p(s0 * expm1(-k * a.time_scale)) / k;
+    }
+    a.t[b] = (float)tb;
     a.cell[b] = c;
     if (a.group) {
       int gb = g;

@@ -24,14 +24,20 @@ using namespace imcdev;
 namespace {
 
 // Block-level counters for rare events (shared-memory atomics keep them out of registers).
-enum : int { B_CENSUS = 0, B_FLOOR, B_REFLECT, B_CAP, B_ESCAPE, B_N };
+enum : int { B_CENSUS = 0, B_FLOOR, B_REFLECT, B_CAP, B_ESCAPE, B_CAPTURE, B_N };
 
 // MG: group-indexed tables and tallies, escaped energy also by group.  In 2-D the rules of
 // MG_IMC/MG_IMC2D.py:580-989 (no effective-scatter cap, no absorption for sigma_a <= 1e-12,
 // the weight floor ends a history after its event is committed); on the 1-D sphere those of
 // MG_IMC/MG_IMC1D.py:276-461, which are the gray spherical ones (cap, floor kill with local
 // deposit) with the floor coefficient 1e-14.
-template <int GEOM, bool SMEM_CELLS, bool PREFETCH, bool MG>
+// CF: Carter-Forest (IMC/IMC1D_CarterForest.py:63-331, 614-820; IMC/IMC2D_CarterForest.py:
+// 102-508).  The table holds (0, sigma_a): the flight samples the absorption distance in the
+// scatter slot (same threshold and cap) and captures nothing on the way; at an absorption the
+// photon is re-emitted in the new direction the event drew after a delay ~ Exp(cf_rate) if that
+// falls inside the step, else captured (its weight deposited).  Histories at or below the
+// weight floor are not moved (they stay in census).
+template <int GEOM, bool SMEM_CELLS, bool PREFETCH, bool MG, bool CF>
 __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ unsigned blk_cnt[B_N];
@@ -102,7 +108,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
         pid = chunk_next + rank;
         w = a.w[pid];
         dcen = (a.dt - a.t[pid]) * c_light;
-        if ((MG2 ? w > weight_floor : w > 0.f) && dcen > 0.f) {
+        if ((MG2 || CF ? w > weight_floor : w > 0.f) && dcen > 0.f) {
           x = a.p1[pid]; u = a.d1[pid];
           if (MG) grp = a.group[pid];
           if (GEOM == G_XY || GEOM == G_RZ) { y = a.p2[pid]; v = a.d2[pid]; }
@@ -265,10 +271,29 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
         acc_lost += (double)w - (double)wn;
         acc_wd += (double)(w * d);
         dcen -= d;
-        if (evt == EV_BOUNDARY) ++s_bd; else if (evt == EV_SCATTER) ++s_sc;
+        bool captured = false;
+        if (CF && evt == EV_SCATTER) {
+          // absorption (IMC/IMC1D_CarterForest.py:146-194, IMC/IMC2D_CarterForest.py:189-210)
+          const float rate = __ldg(a.cf_rate + c);
+          const float tr = dcen / c_light;  // time left after the flight
+          const uint32_t ub = ONED ? r.z : r.w;
+          if (!(rate > 0.f)) {
+            captured = !ONED;  // no re-emission: 1-D redirects, 2-D captures
+          } else if (a.cf_fastpath > 0.f && tr > 1e-14f && rate * tr > a.cf_fastpath) {
+            captured = u01f(ub) < __expf(-rate * tr);
+          } else {
+            const float delay = __fdividef(neglog_u(ub), rate);
+            if (ONED ? (tr > 1e-14f && delay < tr) : (delay < tr - 1e-15f)) dcen = fmaxf(0.f, (tr - delay) * c_light);
+            else captured = true;
+          }
+          if (captured) acc_lost += (double)w;
+        }
+        if (evt == EV_BOUNDARY) ++s_bd;
+        else if (captured) atomicAdd(&blk_cnt[B_CAPTURE], 1u);
+        else if (evt == EV_SCATTER) ++s_sc;
         else atomicAdd(&blk_cnt[B_CENSUS], 1u);
 
-        if (!MG && (GEOM == G_XY || GEOM == G_RZ)) {
+        if (!MG && !CF && (GEOM == G_XY || GEOM == G_RZ)) {
           if (wn <= weight_floor) {
             // IMC/IMC2D.py:1043-1047: history stops in place keeping its weight
             atomicAdd(&blk_cnt[B_FLOOR], 1u);
@@ -278,7 +303,8 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
           }
         }
         if (!frozen) {
-          w = wn; x = xn; y = yn; u = un; v = vn;
+          w = captured ? 0.f : wn; x = xn; y = yn; u = un; v = vn;
+          if (CF && captured) finished = true;
           if (cross != X_NONE) {
             // leaving the cell: flush the accumulators for the old cell
             flush = true; flush_cell = cq; f_lost = acc_lost; f_wd = acc_wd;
@@ -305,7 +331,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
             ci = ni; cj = nj;
           }
           if (GEOM == G_SLAB || GEOM == G_SPHERE) {
-            if (!finished && w < weight_floor) {
+            if (!CF && !finished && w < weight_floor) {
               // IMC/IMC1D.py:188-195: kill and deposit the remainder in the current cell
               // (every cell, including the two edge cells the reference skips)
               atomicAdd(&blk_cnt[B_FLOOR], 1u);
@@ -369,9 +395,10 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    const unsigned long long cen = blk_cnt[B_CENSUS], cap = blk_cnt[B_CAP];
+    const unsigned long long cen = blk_cnt[B_CENSUS], cap = blk_cnt[B_CAP], capt = blk_cnt[B_CAPTURE];
     if (cen) atomicAdd(a.stats + S_CENSUS, cen);
-    if (cen + cap) atomicAdd(a.stats + S_EVENTS, cen + cap);
+    if (capt) atomicAdd(a.stats + S_CAPTURE, capt);
+    if (cen + cap + capt) atomicAdd(a.stats + S_EVENTS, cen + cap + capt);
     if (blk_cnt[B_FLOOR]) atomicAdd(a.stats + S_FLOOR, (unsigned long long)blk_cnt[B_FLOOR]);
     if (blk_cnt[B_REFLECT]) atomicAdd(a.stats + S_REFLECT, (unsigned long long)blk_cnt[B_REFLECT]);
     if (cap) atomicAdd(a.stats + S_CAP, cap);
@@ -380,23 +407,23 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   if (threadIdx.x < 4 && blk_esc[threadIdx.x] != 0ull) atomicAdd(a.esc_fx + threadIdx.x, blk_esc[threadIdx.x]);
 }
 
-template <int GEOM, bool SM, bool PF, bool MG>
+template <int GEOM, bool SM, bool PF, bool MG, bool CF>
 cudaError_t launch_one(const TrackArgs& a, int block, int grid, cudaStream_t s) {
   const int nwarps = block / 32;
   size_t sh = nwarps * sizeof(WarpStage) + sizeof(float) * (a.nx + a.ny + 4);
   if (SM) sh += sizeof(float2) * a.nc * a.ng;
   if (sh > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_track<GEOM, SM, PF, MG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+    cudaError_t e = cudaFuncSetAttribute(k_track<GEOM, SM, PF, MG, CF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
     if (e != cudaSuccess) return e;
   }
-  k_track<GEOM, SM, PF, MG><<<grid, block, sh, s>>>(a);
+  k_track<GEOM, SM, PF, MG, CF><<<grid, block, sh, s>>>(a);
   return cudaGetLastError();
 }
 
-template <int GEOM, bool MG>
+template <int GEOM, bool MG, bool CF = false>
 cudaError_t launch_geom(const TrackArgs& a, int block, int grid, bool sm, bool pf, cudaStream_t s) {
-  if (sm) return pf ? launch_one<GEOM, true, true, MG>(a, block, grid, s) : launch_one<GEOM, true, false, MG>(a, block, grid, s);
-  return pf ? launch_one<GEOM, false, true, MG>(a, block, grid, s) : launch_one<GEOM, false, false, MG>(a, block, grid, s);
+  if (sm) return pf ? launch_one<GEOM, true, true, MG, CF>(a, block, grid, s) : launch_one<GEOM, true, false, MG, CF>(a, block, grid, s);
+  return pf ? launch_one<GEOM, false, true, MG, CF>(a, block, grid, s) : launch_one<GEOM, false, false, MG, CF>(a, block, grid, s);
 }
 
 // Fixed-point tallies to the FP64 outputs: deposition per unit volume per (group, cell),
@@ -426,6 +453,15 @@ cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, 
       case G_SPHERE: return launch_geom<G_SPHERE, true>(a, block, grid, sm, pf, s);
       case G_XY: return launch_geom<G_XY, true>(a, block, grid, sm, pf, s);
       case G_RZ: return launch_geom<G_RZ, true>(a, block, grid, sm, pf, s);
+      default: return cudaErrorInvalidValue;
+    }
+  }
+  if (a.cf_rate) {  // Carter-Forest, gray
+    switch (geom) {
+      case G_SLAB: return launch_geom<G_SLAB, false, true>(a, block, grid, sm, pf, s);
+      case G_SPHERE: return launch_geom<G_SPHERE, false, true>(a, block, grid, sm, pf, s);
+      case G_XY: return launch_geom<G_XY, false, true>(a, block, grid, sm, pf, s);
+      case G_RZ: return launch_geom<G_RZ, false, true>(a, block, grid, sm, pf, s);
       default: return cudaErrorInvalidValue;
     }
   }

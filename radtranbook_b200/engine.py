@@ -199,10 +199,10 @@ class Engine:
     def transport(self, T: torch.Tensor, sigma: torch.Tensor, cv: torch.Tensor, source: torch.Tensor | None,
                   step: int, dt: float, theta: float, n_target: int, n_boundary: int, n_source: int,
                   face_T: list, reflect, max_events: int = 0, rz_linear_source: bool = True,
-                  t_emit_floor: float = 0.0) -> StepResult:
+                  t_emit_floor: float = 0.0, method: int = 0, cf_fastpath: float = 0.0) -> StepResult:
         mat = ImcMaterial(_ptr(T), _ptr(sigma), _ptr(cv), _ptr(source))
         par = self._params(step, dt, theta, n_target, n_boundary, n_source, face_T, reflect, max_events,
-                           rz_linear_source, t_emit_floor)
+                           rz_linear_source, t_emit_floor, method=method, cf_fastpath=cf_fastpath)
         rep = ImcStepReport()
         # sources add at most n_target + n_source + ncell (ceil) + 4 * n_boundary entries
         self.bank.ensure(self.bank.size + int(n_target) + int(n_source) + 2 * self.nc + 4 * int(n_boundary) + 16)
@@ -264,7 +264,7 @@ class Engine:
     # One step = transport_async -> material_update -> (caller's inv_eos) -> comb_async ->
     # fetch(): a single device->host copy of the summary and one stream synchronisation.
     def _params(self, step, dt, theta, n_target, n_boundary, n_source, face_T, reflect, max_events,
-                rz_linear_source, t_emit_floor, n_boundary_side=None) -> ImcStepParams:
+                rz_linear_source, t_emit_floor, n_boundary_side=None, method=0, cf_fastpath=0.0) -> ImcStepParams:
         par = ImcStepParams()
         par.seed = self.seed
         par.step = int(step) & 0xFFFFFFFF
@@ -283,6 +283,8 @@ class Engine:
         par.emission_fractions = _ptr(self.emission_fractions)
         for q, n in enumerate(n_boundary_side or ()):
             par.n_boundary_side[q] = int(n)
+        par.method = int(method)
+        par.cf_fastpath = float(cf_fastpath)
         return par
 
     def _set_census_count(self, n: int) -> None:
@@ -290,17 +292,19 @@ class Engine:
         self._census_dev_valid = True
 
     def transport_async(self, T, sigma, cv, source, step, dt, theta, n_target, n_boundary, n_source, face_T,
-                        reflect, max_events=0, rz_linear_source=True, t_emit_floor=0.0, n_boundary_side=None) -> int:
+                        reflect, max_events=0, rz_linear_source=True, t_emit_floor=0.0, n_boundary_side=None,
+                        method=0, cf_fastpath=0.0) -> int:
         """Sources + tracking without a host synchronisation.  Returns the host upper bound
         of the tracked bank size (the true size is in the device summary)."""
         if not self._census_dev_valid:
             self._set_census_count(self.bank.size)
         self._last_transport = ((T, sigma, cv, source, step, dt, theta, n_target, n_boundary, n_source, face_T,
                                  reflect), dict(max_events=max_events, rz_linear_source=rz_linear_source,
-                                                t_emit_floor=t_emit_floor, n_boundary_side=n_boundary_side))
+                                                t_emit_floor=t_emit_floor, n_boundary_side=n_boundary_side,
+                                                method=method, cf_fastpath=cf_fastpath))
         self._mat = ImcMaterial(_ptr(T), _ptr(sigma), _ptr(cv), _ptr(source))
         self._par = self._params(step, dt, theta, n_target, n_boundary, n_source, face_T, reflect, max_events,
-                                 rz_linear_source, t_emit_floor, n_boundary_side)
+                                 rz_linear_source, t_emit_floor, n_boundary_side, method, cf_fastpath)
         bound = int(self.lib.imc_source_bound(ctypes.byref(self.cmesh), ctypes.byref(self._par)))
         self.bank.ensure(self.bank.size + bound)
         wsp, wsn = self._ws(self.bank.capacity)
