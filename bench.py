@@ -340,6 +340,47 @@ def form_adjoint(repeats: int = 3, fd_cells: int = 64) -> dict:
             "fd_max_rel_err_significant": float(rel[sig_cells].max()) if sig_cells.any() else None}
 
 
+def form_carter_forest(steps: int = 10, warmup: int = 2) -> dict:
+    """The headline crooked-pipe step with Carter-Forest transport (IMC/IMC2D_CarterForest.py
+    semantics): true absorption with delayed re-emission instead of the Fleck factor, same
+    sources, mesh and particle counts; device material callables, CUDA-event timing."""
+    import torch
+
+    from radtranbook_b200 import imc2d_cf, problems
+
+    p = problems.crooked_pipe(scale=1.0)
+    st = imc2d_cf.init_simulation(p["Ntarget"], p["Tinit"], p["Tinit"], p["edges1"], p["edges2"], p["eos_dev"],
+                                  p["inv_eos_dev"], geometry="rz", seed=0xCF0D)
+
+    def run(n, st):
+        seg = capt = reem = 0
+        worst = 0.0
+        for _ in range(n):
+            st, info = imc2d_cf.step(st, p["Ntarget"], p["Nboundary"], 0, p["Nmax"], p["T_boundary"], p["dt"],
+                                     p["edges1"], p["edges2"], p["sigma_dev"], p["inv_eos_dev"], p["cv_dev"],
+                                     p["source"], reflect=p["reflect"], geometry="rz",
+                                     boundary_source_func=p["boundary_source_func"])
+            te = info["profiling"]["transport_events"]
+            seg += te["total"]
+            capt += te["absorption_capture_events"]
+            reem += te["absorption_continue_events"]
+            worst = max(worst, abs(info["ledger"]["relative_closure"]))
+        return st, seg, capt, reem, worst
+
+    st, _, _, _, _ = run(warmup, st)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    st, seg, capt, reem, worst = run(steps, st)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return {"workload": "crooked_pipe_rz_60x210, Carter-Forest", "steps": steps, "segments_per_s": seg / (ms * 1e-3),
+            "ms_per_step": ms / steps, "segments_per_step": seg / steps, "captures_per_step": capt / steps,
+            "reemissions_per_step": reem / steps, "energy_closure_max_rel": worst}
+
+
 def max_time_and_totals(dist, ms: float, counts: list, device) -> tuple:
     """Whole-job figures of a timed region: the slowest rank's device time (ms) and the
     sum over ranks of each count (segments, histories)."""
@@ -454,7 +495,9 @@ def run_ours(args, rank: int, world: int):
                          f"FP64 C++ oracle, OpenMP ({dtc:.1f} s)", "histories_per_s": h}
     forms = fom = None
     if world == 1 and not args.no_forms:
-        forms = {"batched": form_batched(args.batch_steps, not args.no_tune), "adjoint": form_adjoint()}
+        forms = {"batched": form_batched(args.batch_steps, not args.no_tune), "adjoint": form_adjoint(),
+                 "carter_forest": form_carter_forest()}
+        forms["carter_forest"]["over_fleck_cummings"] = forms["carter_forest"]["segments_per_s"] / value
     if world == 1 and not args.no_fom:
         fom = {"gpu": fom_gpu(p, args.fom_steps, args.fom_seeds, dict(eng.launch))}
         if not args.no_cpu_baseline:

@@ -162,6 +162,11 @@ __global__ void __launch_bounds__(256) k_btrack(BatchArgs a) {
   double inv_q = 0.0;  // the instance's fixed-point energy quantum, inverted
   double acc_lost = 0.0, acc_wd = 0.0;
   unsigned s_bd = 0, s_sc = 0;
+  // events of finished histories, summed per lane while they belong to one instance (a
+  // warp's claims are contiguous runs of one instance's entries) and added to the
+  // instance's ledger when the instance changes: one atomic per run, not per history
+  unsigned long long ev_acc = 0ull;
+  int ev_k = 0;
 
   for (;;) {
     unsigned need = __ballot_sync(FULL, !has);
@@ -296,7 +301,12 @@ __global__ void __launch_bounds__(256) k_btrack(BatchArgs a) {
         acc_lost = 0.0; acc_wd = 0.0;
         B.w[pid] = w;
         if (w > 0.f) { B.p1[pid] = x; B.d1[pid] = u; B.cell[pid] = ci; }
-        atomicAdd(a.ledger + (size_t)k * IMC_BL_N + IMC_BL_EVENTS, (double)ev);
+        if (k != ev_k) {
+          if (ev_acc) atomicAdd(a.ledger + (size_t)ev_k * IMC_BL_N + IMC_BL_EVENTS, (double)ev_acc);
+          ev_k = k;
+          ev_acc = 0ull;
+        }
+        ev_acc += ev;
         has = false;
       }
     }
@@ -310,6 +320,7 @@ __global__ void __launch_bounds__(256) k_btrack(BatchArgs a) {
     warp_tally_fx(flush, flush_cell, ud, vs, a.dep_fx, a.si, st);
   }
 
+  if (ev_acc) atomicAdd(a.ledger + (size_t)ev_k * IMC_BL_N + IMC_BL_EVENTS, (double)ev_acc);
   const unsigned long long t_bd = warp_sum_u(s_bd), t_sc = warp_sum_u(s_sc);
   if (lane == 0) {
     if (t_bd) atomicAdd(a.stats + S_BOUNDARY, t_bd);
@@ -434,9 +445,13 @@ __global__ void __launch_bounds__(1024) k_bcomb_scan(BatchArgs a) {
   scan(a.inst_pref, a.K);
 }
 
-// copies written in entry order into the instance's slots of the other bank
+// Copies written in entry order into the instance's slots of the other bank, one thread per
+// output copy: the tile's copy counts are scanned in shared memory and each thread finds the
+// entry of its copy by a binary search there, so the stores are contiguous across the warp
+// however many copies a single entry makes (the census piles up in a few hot entries).
 __global__ void __launch_bounds__(BATCH_TILE) k_bcomb_scatter(BatchArgs a) {
   extern __shared__ long long pref[];
+  __shared__ int incl[BATCH_TILE];
   __shared__ int sh[BATCH_TILE / 32];
   load_pref(pref, a.live_pref, a.K);
   const int sel = *a.sel;
@@ -446,7 +461,8 @@ __global__ void __launch_bounds__(BATCH_TILE) k_bcomb_scatter(BatchArgs a) {
   const long long total = pref[a.K];
   const long long ntiles = (total + BATCH_TILE - 1) / BATCH_TILE;
   for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const long long q = tile * BATCH_TILE + threadIdx.x;
+    const long long tile0 = tile * BATCH_TILE;
+    const long long q = tile0 + threadIdx.x;
     const int n = (q < total) ? a.cnt[q] : 0;
     int x = n;
 #pragma unroll
@@ -460,22 +476,24 @@ __global__ void __launch_bounds__(BATCH_TILE) k_bcomb_scatter(BatchArgs a) {
       sh[lane] = v;
     }
     __syncthreads();
-    if (n > 0) {
-      const long long start = a.blk[tile] + (wid ? sh[wid - 1] : 0) + (x - n);
-      const int k = find_inst(pref, a.K, q);
-      const long long pid = a.slot_off[k] + (q - pref[k]);
-      const long long within = start - a.inst_pref[k];
-      const long long cap = a.census_cap[k];
-      const int c = B.cell[pid];
-      const float wq = (float)a.ew[a.cell_off[k] + c];
-      const float p1 = B.p1[pid], d1 = B.d1[pid];
-      for (int r = 0; r < n; ++r) {
-        if (within + r >= cap) break;  // flagged by the scan
-        const long long o = a.slot_off[k] + within + r;
-        O.p1[o] = p1; O.d1[o] = d1; O.w[o] = wq; O.t[o] = 0.f; O.cell[o] = c;
-      }
-    }
+    incl[threadIdx.x] = x + (wid ? sh[wid - 1] : 0);
     __syncthreads();
+    const int tot = incl[BATCH_TILE - 1];
+    const long long out0 = a.blk[tile];
+    for (int o = threadIdx.x; o < tot; o += BATCH_TILE) {
+      int lo = 0, hi = BATCH_TILE - 1;  // the entry j with incl[j-1] <= o < incl[j]
+      while (lo < hi) { const int mid = (lo + hi) >> 1; if (incl[mid] > o) hi = mid; else lo = mid + 1; }
+      const long long src = tile0 + lo;
+      const int k = find_inst(pref, a.K, src);
+      const long long within = out0 + o - a.inst_pref[k];
+      if (within >= a.census_cap[k]) continue;  // overflow: flagged by the scan
+      const long long pid = a.slot_off[k] + (src - pref[k]);
+      const int c = B.cell[pid];
+      const long long dst = a.slot_off[k] + within;
+      O.p1[dst] = B.p1[pid]; O.d1[dst] = B.d1[pid];
+      O.w[dst] = (float)a.ew[a.cell_off[k] + c]; O.t[dst] = 0.f; O.cell[dst] = c;
+    }
+    __syncthreads();  // incl and sh are reused by the next tile
   }
 }
 

@@ -209,3 +209,26 @@ def test_cf_xy_matches_reference_statistically():
     roi = ref["T_mean"] > 1.5 * T0
     SP.compare_means(Ts.mean(0), Ts.std(0, ddof=1) / np.sqrt(seeds), ref["T_mean"], ref["T_se"], roi)
     SP.compare_means(Trs.mean(0), Trs.std(0, ddof=1) / np.sqrt(seeds), ref["Tr_mean"], ref["Tr_se"], roi)
+
+
+def _equilibrium(cv, T0, Tr0):
+    """cv T + a T^4 = cv T0 + a Tr0^4 (the closed cell's conserved energy density)."""
+    from scipy.optimize import brentq
+
+    E = cv * T0 + A * Tr0 ** 4
+    return brentq(lambda T: cv * T + A * T ** 4 - E, 0.0, 10.0)
+
+
+def test_cf_zero_d_equilibrates_to_exact_temperature():
+    """IMC/test_simple_equilibration.py set-up (one reflecting cell, sigma = 100, cv = 0.01,
+    T = 0.4, Tr = 1.0, dt = 0.01): after 5 steps the material sits at the exact equilibrium
+    (the reference prints ~0.88 keV; the exact value is 0.894)."""
+    Teq = _equilibrium(0.01, 0.4, 1.0)
+    e = np.array([0.0, 0.1])
+    run = O.OracleGray("slab", e, [0.0, 1.0], np.diff(e), 11, 20000, np.array([0.4]), np.array([1.0]),
+                       lambda T: 0.01 * T, lambda u: u / 0.01, nthreads=2)
+    for _ in range(5):
+        r = run.step(20000, 0, 0, 20000, [None, None], 0.01, lambda T: 100.0 + 0 * T, lambda u: u / 0.01,
+                     lambda T: np.full_like(T, 0.01), reflect=(True, True), conserve_comb_energy=True, method="cf")
+        assert abs(r["closure"]) < 1e-12 * r["total_energy"]
+    assert abs(run.T[0] - Teq) < 0.01 * Teq, (run.T[0], Teq)

@@ -163,3 +163,22 @@ def test_cf_xy_dropin_matches_reference_statistically(cuda):
     roi = ref["T_mean"] > 1.5 * T0
     SP.compare_means(Ts.mean(0), Ts.std(0, ddof=1) / np.sqrt(seeds), ref["T_mean"], ref["T_se"], roi)
     SP.compare_means(Trs.mean(0), Trs.std(0, ddof=1) / np.sqrt(seeds), ref["Tr_mean"], ref["Tr_se"], roi)
+
+
+def test_cf_zero_d_equilibrates_to_exact_temperature(cuda):
+    """IMC/test_simple_equilibration.py set-up through the drop-in: the closed cell reaches
+    cv T + a T^4 = cv T0 + a Tr0^4 (0.894 keV) within 1 %."""
+    from scipy.optimize import brentq
+
+    from radtranbook_b200 import imc1d_cf
+
+    Teq = brentq(lambda T: 0.01 * T + 0.01372 * T ** 4 - (0.01 * 0.4 + 0.01372), 0.0, 10.0)
+    mesh = np.array([[0.0, 0.1]])
+    st = imc1d_cf.init_simulation(20000, np.array([0.4]), np.array([1.0]), mesh, lambda T: 0.01 * T,
+                                  lambda u: u / 0.01)
+    for _ in range(5):
+        st, info = imc1d_cf.step(st, 20000, 0, 0, 20000, (0.0, 0.0), 0.01, mesh, lambda T: 100.0 + 0 * T,
+                                 lambda u: u / 0.01, lambda T: 0.01 + 0 * T, np.zeros(1), reflect=(True, True),
+                                 use_scalar_intensity_Tr=False, conserve_comb_energy=True)
+        assert abs(info["ledger"]["relative_closure"]) < 1e-12
+    assert abs(st.temperature[0] - Teq) < 0.01 * Teq, (st.temperature[0], Teq)
