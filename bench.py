@@ -381,6 +381,49 @@ def form_carter_forest(steps: int = 10, warmup: int = 2) -> dict:
             "reemissions_per_step": reem / steps, "energy_closure_max_rel": worst}
 
 
+def form_device_loop(steps: int = 20) -> dict:
+    """The same crooked-pipe steps run eagerly (drop-in step: one host synchronisation per
+    step) and as the device-resident loop (one captured two-step graph replayed, dt and Philox
+    step read from device memory): full size and a 1/100 launch-bound size."""
+    import torch
+
+    from radtranbook_b200 import driver, imc2d, problems
+
+    out = {}
+    for tag, scale, nr, nz in (("full", 1.0, 60, 210), ("small", 0.01, 30, 105)):
+        p = problems.crooked_pipe(scale=scale, nr=nr, nz=nz)
+
+        def init():
+            return imc2d.init_simulation(p["Ntarget"], p["Tinit"], p["Tr_init"], p["edges1"], p["edges2"],
+                                         p["eos_dev"], p["inv_eos_dev"], geometry="rz", seed=0xD1)
+
+        st = init()
+        st, _, _, _ = _gpu_steps(p, st, 3, True)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        st, seg_e, _, _ = _gpu_steps(p, st, steps, True)
+        e1.record()
+        torch.cuda.synchronize()
+        ms_e = e0.elapsed_time(e1) / steps
+        st2 = init()
+        st2, _, _, _ = _gpu_steps(p, st2, 3, True)
+        loop = driver.DeviceLoop(st2, Ntarget=p["Ntarget"], Nboundary=p["Nboundary"], Nsource=0, Nmax=p["Nmax"],
+                                 T_boundary=p["T_boundary"], sigma_a_func=p["sigma_dev"], inv_eos=p["inv_eos_dev"],
+                                 cv=p["cv_dev"], source=p["source"], reflect=p["reflect"], geometry="rz",
+                                 max_events=1_000_000, boundary_source_func=p["boundary_source_func"])
+        loop.run([p["dt"]] * steps)  # capture and a first run outside the timing
+        res = loop.run([p["dt"]] * steps)
+        ms_g = res["device_ms"] / steps
+        seg_g = sum(s["transport_events"]["total"] for s in res["steps"])
+        out[tag] = {"particles_per_step": p["Ntarget"] + p["Nboundary"], "eager_ms_per_step": ms_e,
+                    "device_loop_ms_per_step": ms_g, "speedup": ms_e / ms_g,
+                    "eager_segments_per_s": seg_e / (ms_e * steps * 1e-3),
+                    "device_loop_segments_per_s": seg_g / (ms_g * steps * 1e-3),
+                    "max_relative_closure": res["max_relative_closure"]}
+    return out
+
+
 def max_time_and_totals(dist, ms: float, counts: list, device) -> tuple:
     """Whole-job figures of a timed region: the slowest rank's device time (ms) and the
     sum over ranks of each count (segments, histories)."""
@@ -496,7 +539,7 @@ def run_ours(args, rank: int, world: int):
     forms = fom = None
     if world == 1 and not args.no_forms:
         forms = {"batched": form_batched(args.batch_steps, not args.no_tune), "adjoint": form_adjoint(),
-                 "carter_forest": form_carter_forest()}
+                 "carter_forest": form_carter_forest(), "device_loop": form_device_loop()}
         forms["carter_forest"]["over_fleck_cummings"] = forms["carter_forest"]["segments_per_s"] / value
     if world == 1 and not args.no_fom:
         fom = {"gpu": fom_gpu(p, args.fom_steps, args.fom_seeds, dict(eng.launch))}

@@ -126,6 +126,10 @@ typedef struct imc_step_params {
   int32_t pad_method;
   double cf_fastpath;           /* Carter-Forest stiff fast path: when rate * t_left exceeds it,
                                    capture with probability exp(-rate t_left) (0 = off) */
+  const uint32_t* step_dev;     /* DEVICE pointer or NULL: when set, every kernel of the step reads
+                                   the Philox step counter from it at run time instead of `step` */
+  const double* dt_dev;         /* DEVICE pointer or NULL: likewise for dt.  With both set, a
+                                   captured step is replayed (CUDA graph) for any step and dt. */
 } imc_step_params;
 
 /* Carter-Forest (IMC/IMC1D_CarterForest.py, IMC/IMC2D_CarterForest.py): no Fleck factor;
@@ -282,6 +286,14 @@ IMC_API imc_status imc_comb_async(const imc_mesh* mesh, const imc_bank* in, imc_
                                   double* disc, const double* e, void* workspace,
                                   size_t workspace_bytes, imc_step_summary* summary,
                                   void* stream);
+/* imc_comb_async with the Philox step counter read from device memory when the comb runs
+ * (step_dev, a DEVICE pointer), so a captured comb can be replayed for every step.  No
+ * reference counterpart (the reference time loop runs on the host). */
+IMC_API imc_status imc_comb_async_dev(const imc_mesh* mesh, const imc_bank* in, imc_bank* out,
+                                      int64_t n_max, uint64_t seed, const uint32_t* step_dev,
+                                      int32_t per_group, double* disc, const double* e,
+                                      void* workspace, size_t workspace_bytes,
+                                      imc_step_summary* summary, void* stream);
 /* Device time (ms) of the source fill and of tracking in this host thread's last
  * imc_step_transport[_async]; valid once that work has completed. */
 IMC_API imc_status imc_phase_times(float* ms_sources, float* ms_transport);

@@ -66,6 +66,7 @@ class ImcStepParams(ctypes.Structure):
         ("emission_fractions", c_void_p),
         ("n_boundary_side", c_int64 * 4),
         ("method", c_int32), ("pad_method", c_int32), ("cf_fastpath", c_double),
+        ("step_dev", c_void_p), ("dt_dev", c_void_p),
     ]
 
 
@@ -157,6 +158,8 @@ SIGNATURES = {
                                          c_void_p]),
     "imc_comb_async": (c_int, [POINTER(ImcMesh), POINTER(ImcBank), POINTER(ImcBank), c_int64, c_uint64, c_uint32,
                                c_int32, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p, c_void_p]),
+    "imc_comb_async_dev": (c_int, [POINTER(ImcMesh), POINTER(ImcBank), POINTER(ImcBank), c_int64, c_uint64,
+                                   c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p, c_void_p]),
     "imc_phase_times": (c_int, [POINTER(ctypes.c_float), POINTER(ctypes.c_float)]),
     "imc_energy_totals": (c_int, [POINTER(ImcMesh), POINTER(ImcBank), c_void_p, POINTER(c_double),
                                   POINTER(c_double), c_void_p, c_size_t, c_void_p]),

@@ -30,6 +30,7 @@ using namespace imcblk;
 // Per-cell part of the plan, one thread per cell: Fleck factor, absorption / effective
 // scatter tables, emission energy, linear tilt constants, FP32 edges.
 __global__ void k_plan_cells(PlanArgs a) {
+  const double dt = a.dt_dev ? *a.dt_dev : a.dt;  // device-resident step length (graph replay)
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c <= a.nx) a.e1f[c] = (float)a.e1[c];
   if (c <= a.ny) a.e2f[c] = (float)a.e2[c];
@@ -42,15 +43,15 @@ __global__ void k_plan_cells(PlanArgs a) {
     if (!isfinite(T) || (oned && !(T > 0.0)) || !isfinite(a.sigma[c]) || !(a.cv[c] > 0.0))
       atomicOr(&a.sum->flags, (int)IMC_FLAG_NONFINITE);
     const double beta = 4.0 * A_RAD * pow3(T) / a.cv[c];
-    double f = 1.0 / (1.0 + a.theta * beta * a.sigma[c] * C_LIGHT * a.dt);
+    double f = 1.0 / (1.0 + a.theta * beta * a.sigma[c] * C_LIGHT * dt);
     f = fmin(1.0, fmax(0.0, f));
     const double ss = a.sigma[c] * (1.0 - f);
     const double sa = a.sigma[c] * f;
     a.sa[c] = sa; a.ss[c] = ss;
     a.sass[c] = make_float2((float)sa, (float)ss);
     const double iv = 1.0 / a.vol[c];
-    a.cellf[c] = make_double2(iv, sa > sa_thr ? 1.0 / (sa * a.vol[c] * a.dt) : -1.0 / (a.vol[c] * a.dt));
-    double E = A_RAD * C_LIGHT * pow4(fmax(T, 0.0)) * sa * a.dt * a.vol[c];
+    a.cellf[c] = make_double2(iv, sa > sa_thr ? 1.0 / (sa * a.vol[c] * dt) : -1.0 / (a.vol[c] * dt));
+    double E = A_RAD * C_LIGHT * pow4(fmax(T, 0.0)) * sa * dt * a.vol[c];
     if (a.method == IMC_METHOD_CARTER_FOREST) {
       // Carter-Forest (IMC/IMC1D_CarterForest.py:1181-1185, 485-494; IMC/IMC2D_CarterForest.py:
       // 947-948, 877-883): true opacity, no effective scatter (the tracking kernel samples the
@@ -62,11 +63,11 @@ __global__ void k_plan_cells(PlanArgs a) {
       const double rate = C_LIGHT * sig * beta;
       a.sa[c] = sig; a.ss[c] = 0.0;
       a.sass[c] = make_float2(0.f, (float)sig);
-      a.cellf[c] = make_double2(iv, -1.0 / (a.vol[c] * a.dt));
+      a.cellf[c] = make_double2(iv, -1.0 / (a.vol[c] * dt));
       a.cf_rate[c] = (beta > 1e-15 && sig > 1e-15) ? (float)rate : 0.f;
       const double T4 = pow4(fmax(T, 0.0));
       const bool decays = oned ? rate > 1e-10 : (rate > 1e-12 && beta > 1e-15);
-      E = decays ? A_RAD * T4 * -expm1(-rate * a.dt) / beta * a.vol[c] : A_RAD * T4 * C_LIGHT * sig * a.dt * a.vol[c];
+      E = decays ? A_RAD * T4 * -expm1(-rate * dt) / beta * a.vol[c] : A_RAD * T4 * C_LIGHT * sig * dt * a.vol[c];
     }
     if (a.t_emit_floor > 0.0 && T < a.t_emit_floor) E = 0.0;
     a.emit_E[c] = E;
@@ -131,6 +132,7 @@ __global__ void k_plan_cells(PlanArgs a) {
 }
 
 __global__ void __launch_bounds__(NT) k_plan(PlanArgs a) {
+  const double dt = a.dt_dev ? *a.dt_dev : a.dt;  // device-resident step length (graph replay)
   __shared__ double red[NT];
   __shared__ long long sh[NT];
   const int t = threadIdx.x;
@@ -152,7 +154,7 @@ __global__ void __launch_bounds__(NT) k_plan(PlanArgs a) {
     double smax = 0.0;
     for (int c = t; c < nc; c += NT) {
       smax = fmax(smax, a.source[c]);
-      a.src_QV[c] = a.source[c] * a.dt * a.vol[c];
+      a.src_QV[c] = a.source[c] * dt * a.vol[c];
     }
     red[t] = smax;
     __syncthreads();
@@ -191,7 +193,7 @@ __global__ void __launch_bounds__(NT) k_plan(PlanArgs a) {
           else area = PI * (a.e1[q + 1] * a.e1[q + 1] - a.e1[q] * a.e1[q]);
         }
         const double T = Tf[q];
-        Ef[q] = (T > 0.0) ? A_RAD * C_LIGHT * T * T * T * T / 4.0 * area * a.dt : 0.0;
+        Ef[q] = (T > 0.0) ? A_RAD * C_LIGHT * T * T * T * T / 4.0 * area * dt : 0.0;
         Et += Ef[q];
         cdf[q] = Et;
       }
@@ -376,6 +378,7 @@ __device__ void block_canon_prefix(const double* x, int n, double* out, double* 
 }
 
 __global__ void __launch_bounds__(NT) k_plan_mg(PlanMgArgs a) {
+  const double dt = a.dt_dev ? *a.dt_dev : a.dt;  // device-resident step length (graph replay)
   __shared__ double sh[NT];
   const int t = threadIdx.x;
   const int nc = a.nc, G = a.ng;
@@ -405,10 +408,10 @@ __global__ void __launch_bounds__(NT) k_plan_mg(PlanMgArgs a) {
       sp += a.sigma[(size_t)g * nc + c] * gc[g];
     }
     const double beta = 4.0 * A_RAD * pow3(T) / a.cv[c];
-    double f = 1.0 / (1.0 + a.theta * beta * sp * C_LIGHT * a.dt);
+    double f = 1.0 / (1.0 + a.theta * beta * sp * C_LIGHT * dt);
     f = fmin(1.0, fmax(0.0, f));
     const double aT4 = (a.t_emit_floor > 0.0 && T < a.t_emit_floor) ? 0.0
-                                                                      : A_RAD * C_LIGHT * pow4(T) * a.dt * a.vol[c];
+                                                                      : A_RAD * C_LIGHT * pow4(T) * dt * a.vol[c];
     double run = 0.0;
     for (int g = 0; g < G; ++g) {
       const size_t q = (size_t)g * nc + c;
@@ -416,7 +419,7 @@ __global__ void __launch_bounds__(NT) k_plan_mg(PlanMgArgs a) {
       const double sa = a.sigma[q] * f;
       a.sa[q] = sa; a.ss[q] = ss;
       a.sass[q] = make_float2((float)sa, (float)ss);
-      a.cellf[q] = make_double2(1.0 / a.vol[c], sa > 1e-12 ? 1.0 / (sa * a.vol[c] * a.dt) : -1.0 / (a.vol[c] * a.dt));
+      a.cellf[q] = make_double2(1.0 / a.vol[c], sa > 1e-12 ? 1.0 / (sa * a.vol[c] * dt) : -1.0 / (a.vol[c] * dt));
       const double bg = a.emission_fractions ? a.emission_fractions[g] : gc[g];
       run += sa * bg * aT4;
       gc[g] = run;  // cumulative over groups
@@ -443,7 +446,7 @@ __global__ void __launch_bounds__(NT) k_plan_mg(PlanMgArgs a) {
     for (int c = t; c < nc; c += NT) {
       double run = 0.0;
       for (int g = 0; g < G; ++g) {
-        run += a.source[(size_t)g * nc + c] * a.vol[c] * a.dt;
+        run += a.source[(size_t)g * nc + c] * a.vol[c] * dt;
         a.Sgc[(size_t)c * G + g] = run;
       }
       a.Sc[c] = run;
@@ -476,7 +479,7 @@ __global__ void __launch_bounds__(NT) k_plan_mg(PlanMgArgs a) {
         else if (along2) { const double R = side == 0 ? a.e1[0] : a.e1[a.nx]; area = 2.0 * PI * R * (a.e2[q + 1] - a.e2[q]); }
         else area = PI * (a.e1[q + 1] * a.e1[q + 1] - a.e1[q] * a.e1[q]);
         const double T = Tf[q];
-        Ef[q] = (T > 0.0) ? A_RAD * C_LIGHT * T * T * T * T / 4.0 * area * a.dt : 0.0;
+        Ef[q] = (T > 0.0) ? A_RAD * C_LIGHT * T * T * T * T / 4.0 * area * dt : 0.0;
         Et += Ef[q];
         cdf[q] = Et;
       }
@@ -503,6 +506,7 @@ __global__ void __launch_bounds__(NT) k_plan_mg(PlanMgArgs a) {
 // (group, cell) bin b = g*nc + c with stratified counts max(1, round(N E_b / E)) (fixed
 // source: round, no minimum), inner / outer sphere boundary faces.
 __global__ void __launch_bounds__(NT) k_plan_mg1d(PlanMgArgs a) {
+  const double dt = a.dt_dev ? *a.dt_dev : a.dt;  // device-resident step length (graph replay)
   __shared__ double red[NT];
   __shared__ long long sh[NT];
   const int t = threadIdx.x;
@@ -531,7 +535,7 @@ __global__ void __launch_bounds__(NT) k_plan_mg1d(PlanMgArgs a) {
       sp += a.sigma[(size_t)g * nc + c] * b[g];
     }
     const double beta = 4.0 * A_RAD * pow3(T) / a.cv[c];
-    double f = 1.0 / (1.0 + a.theta * beta * sp * C_LIGHT * a.dt);
+    double f = 1.0 / (1.0 + a.theta * beta * sp * C_LIGHT * dt);
     f = fmin(1.0, fmax(0.0, f));
     const bool cold = a.t_emit_floor > 0.0 && T < a.t_emit_floor;
     for (int g = 0; g < G; ++g) {
@@ -541,8 +545,8 @@ __global__ void __launch_bounds__(NT) k_plan_mg1d(PlanMgArgs a) {
       a.sa[q] = sa; a.ss[q] = ss;
       a.sass[q] = make_float2((float)sa, (float)ss);
       // MG_IMC/MG_IMC1D.py:346-350: path-length estimator below sigma_a = 1e-10
-      a.cellf[q] = make_double2(1.0 / a.vol[c], sa > 1e-10 ? 1.0 / (sa * a.vol[c] * a.dt) : -1.0 / (a.vol[c] * a.dt));
-      a.emit_E[q] = cold ? 0.0 : A_RAD * C_LIGHT * pow4(T) * sa * b[g] * a.dt * a.vol[c];
+      a.cellf[q] = make_double2(1.0 / a.vol[c], sa > 1e-10 ? 1.0 / (sa * a.vol[c] * dt) : -1.0 / (a.vol[c] * dt));
+      a.emit_E[q] = cold ? 0.0 : A_RAD * C_LIGHT * pow4(T) * sa * b[g] * dt * a.vol[c];
     }
   }
   __syncthreads();
@@ -570,7 +574,7 @@ __global__ void __launch_bounds__(NT) k_plan_mg1d(PlanMgArgs a) {
     double smax = 0.0;
     for (int q = t; q < ncg; q += NT) {
       smax = fmax(smax, a.source[q]);
-      a.src_QV[q] = a.source[q] * a.vol[q % nc] * a.dt;
+      a.src_QV[q] = a.source[q] * a.vol[q % nc] * dt;
     }
     red[t] = smax;
     __syncthreads();
@@ -603,7 +607,7 @@ __global__ void __launch_bounds__(NT) k_plan_mg1d(PlanMgArgs a) {
       double* cdf = a.face + (size_t)(side * 2 + 1) * a.nf;
       const double R = side == 0 ? a.e1[0] : a.e1[a.nx];
       const double T = Tf[0];
-      const double E = (T > 0.0) ? A_RAD * C_LIGHT * T * T * T * T / 4.0 * (4.0 * PI * R * R) * a.dt : 0.0;
+      const double E = (T > 0.0) ? A_RAD * C_LIGHT * T * T * T * T / 4.0 * (4.0 * PI * R * R) * dt : 0.0;
       Ef[0] = E;
       cdf[0] = E;
       if (E > 0.0) {

@@ -33,9 +33,10 @@ inline size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
 struct PhaseEvents {
   cudaEvent_t e[3] = {nullptr, nullptr, nullptr};
   bool ok = false, recorded = false;
-  PhaseEvents() {
-    ok = true;
-    for (auto& x : e) ok = ok && cudaEventCreate(&x) == cudaSuccess;
+  explicit PhaseEvents(bool create = true) {
+    ok = create;
+    if (create)
+      for (auto& x : e) ok = ok && cudaEventCreate(&x) == cudaSuccess;
   }
 };
 PhaseEvents& phase_events() {
@@ -138,6 +139,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   for (int q = 0; q < 4; ++q) pa.face_T[q] = par->face_T[q];
   pa.rz_linear = par->rz_linear_source; pa.t_emit_floor = par->t_emit_floor;
   pa.method = par->method; pa.cf_rate = ws_ptr<float>(workspace, L.cf_rate);
+  pa.dt_dev = par->dt_dev;
   pa.sa = tal->sigma_a; pa.ss = tal->sigma_s;
   pa.sass = ws_ptr<float2>(workspace, L.sass); pa.cellf = ws_ptr<double2>(workspace, L.cellf);
   pa.e1f = ws_ptr<float>(workspace, L.e1f); pa.e2f = ws_ptr<float>(workspace, L.e2f);
@@ -175,6 +177,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     pm.src_QV = pa.src_QV; pm.src_n = pa.src_n; pm.src_off = pa.src_off; pm.src_w = pa.src_w;
     pm.src_issued = pa.src_issued;
     pm.sum = sum;
+    pm.dt_dev = par->dt_dev;
     IMC_CUDA(imc_launch_plan_mg1d(pm, s));
   } else {
     IMC_CUDA(cudaMemsetAsync(tal->boundary_group, 0, sizeof(double) * ng, s));
@@ -197,11 +200,17 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     pm.emitted = tal->emitted; pm.face = pa.face; pm.nf = pa.nf;
     pm.mixcdf = ws_ptr<double>(workspace, L.mixcdf);
     pm.sum = sum;
+    pm.dt_dev = par->dt_dev;
     IMC_CUDA(imc_launch_plan_mg(pm, s));
   }
 
   // ---- sources, appended in the reference's order: census | boundary | fixed | emission ----
-  PhaseEvents& pe = phase_events();
+  // (the phase-timing events are left out of a stream capture)
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  IMC_CUDA(cudaStreamIsCapturing(s, &capture));
+  PhaseEvents& pe_all = phase_events();
+  PhaseEvents pe_off(false);
+  PhaseEvents& pe = capture == cudaStreamCaptureStatusNone ? pe_all : pe_off;
   if (pe.ok) IMC_CUDA(cudaEventRecord(pe.e[0], s));
   float *p2, *d2;
   set_bank(p2, d2, bank, two_d);
@@ -218,6 +227,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     ba.ng = ng; ba.faceT = par->face_T[side]; ba.gedges = mesh->group_edges;
     ba.mixcdf = ws_ptr<double>(workspace, L.mixcdf); ba.boundary_group = tal->boundary_group;
     ba.below_last = mg1 ? 1 : 0;
+    ba.dt_dev = par->dt_dev; ba.step_dev = par->step_dev;
     IMC_CUDA(imc_launch_fill_boundary(ba, s));
   }
   const int nbins = mg1 ? nc * ng : nc;  // source order positions (MG 1-D: (group, cell) bins)
@@ -227,6 +237,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     FillArgs fa{};
     fa.geom = mesh->geometry; fa.nx = mesh->nx; fa.ny = mesh->ny; fa.nc = nc;
     fa.nbins = nbins; fa.bins_by_group = mg1 ? 1 : 0;
+    fa.time_scale_dev = par->dt_dev; fa.step_dev = par->step_dev;
     fa.e1 = mesh->edges1; fa.e2 = mesh->edges2; fa.T = mat->temperature;
     fa.d_n = d_n; fa.d_base = d_base; fa.n_bound = n_bound;
     fa.off = off; fa.w = w; fa.tilt = tilt; fa.tilt_kind = kind;
@@ -249,6 +260,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     fm.time_scale = par->dt; fm.seed = par->seed; fm.step = par->step; fm.tag = tag;
     fm.p1 = bank->pos1; fm.p2 = p2; fm.d1 = bank->dir1; fm.d2 = d2; fm.wb = bank->weight;
     fm.t = bank->time; fm.cell = bank->cell; fm.group = bank->group;
+    fm.time_scale_dev = par->dt_dev; fm.step_dev = par->step_dev;
     return imc_launch_fill_mg(fm, s);
   };
   const bool rzlin = mesh->geometry == IMC_GEOM_RZ && par->rz_linear_source;
@@ -301,6 +313,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   ta.floor_coef = mg1 ? 1e-14 : 1e-10;
   ta.cf_rate = cf ? pa.cf_rate : nullptr;
   ta.cf_fastpath = (float)par->cf_fastpath;
+  ta.dt_dev = par->dt_dev; ta.step_dev = par->step_dev;
   int rm = 0;
   for (int q = 0; q < 4; ++q) if (par->reflect[q]) rm |= 1 << q;
   ta.reflect_mask = rm;
@@ -331,7 +344,8 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
 
 imc_status comb_async(const imc_mesh* mesh, const imc_bank* in, imc_bank* out, int64_t n_max, uint64_t seed,
                       uint32_t step, int32_t per_group, double* disc, const double* e, void* workspace,
-                      size_t workspace_bytes, imc_step_summary* sum, cudaStream_t s) {
+                      size_t workspace_bytes, imc_step_summary* sum, cudaStream_t s,
+                      const uint32_t* step_dev = nullptr) {
   imc_status st = check_mesh(mesh);
   if (st != IMC_OK) return st;
   const bool two_d = mesh->geometry >= IMC_GEOM_XY;
@@ -355,7 +369,7 @@ imc_status comb_async(const imc_mesh* mesh, const imc_bank* in, imc_bank* out, i
   ca.ecen = ws_ptr<double>(workspace, L.ecen); ca.ew = ws_ptr<double>(workspace, L.ew);
   ca.ncopy = ws_ptr<double>(workspace, L.ncopy); ca.cnt = ws_ptr<int>(workspace, L.cnt);
   ca.blk = ws_ptr<long long>(workspace, L.blk);
-  ca.seed = seed; ca.step = step;
+  ca.seed = seed; ca.step = step; ca.step_dev = step_dev;
   ca.op1 = out->pos1; ca.op2 = two_d ? out->pos2 : nullptr; ca.od1 = out->dir1; ca.od2 = two_d ? out->dir2 : nullptr;
   ca.ow = out->weight; ca.ot = out->time; ca.ocell = out->cell; ca.ogroup = out->group;
   ca.disc = disc;
@@ -649,6 +663,15 @@ imc_status imc_comb_async(const imc_mesh* mesh, const imc_bank* in, imc_bank* ou
                           size_t workspace_bytes, imc_step_summary* summary, void* stream) {
   return comb_async(mesh, in, out, n_max, seed, step, per_group, disc, e, workspace, workspace_bytes, summary,
                     (cudaStream_t)stream);
+}
+
+imc_status imc_comb_async_dev(const imc_mesh* mesh, const imc_bank* in, imc_bank* out, int64_t n_max,
+                              uint64_t seed, const uint32_t* step_dev, int32_t per_group, double* disc,
+                              const double* e, void* workspace, size_t workspace_bytes, imc_step_summary* summary,
+                              void* stream) {
+  if (!step_dev) return IMC_ERR_INVALID_ARG;
+  return comb_async(mesh, in, out, n_max, seed, 0u, per_group, disc, e, workspace, workspace_bytes, summary,
+                    (cudaStream_t)stream, step_dev);
 }
 
 imc_status imc_comb(const imc_mesh* mesh, const imc_bank* in, imc_bank* out, int64_t n_max, uint64_t seed,

@@ -67,6 +67,7 @@ __global__ void __launch_bounds__(256) k_comb_ecen(CombArgs a) {
 }
 
 __global__ void __launch_bounds__(CB) k_comb_count(CombArgs a) {
+  const uint32_t step = a.step_dev ? *a.step_dev : a.step;  // graph replay
   __shared__ long long sh[CB / 32];
   __shared__ WarpStage stages[CB / 32];
   __shared__ BlockBins<CB> t;
@@ -84,7 +85,7 @@ __global__ void __launch_bounds__(CB) k_comb_count(CombArgs a) {
       if (compact) {
         n = 1;
       } else if (ew > 0.0) {
-        const U4 r = draw(a.seed, (uint32_t)k, 0, a.step, TAG_COMB);
+        const U4 r = draw(a.seed, (uint32_t)k, 0, step, TAG_COMB);
         n = (int)floor((double)wf / ew + u01d(r.x));
       }
     }

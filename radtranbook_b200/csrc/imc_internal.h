@@ -44,6 +44,8 @@ struct TrackArgs {
   unsigned long long* esc_fx; // [4 + ng] escaped energy by side, then by group (MG)
   const float* cf_rate;      // Carter-Forest: [c] re-emission rate c sigma_a beta (0: none), else NULL
   float cf_fastpath;         // Carter-Forest stiff fast-path threshold (0 = off)
+  const double* dt_dev;      // non-NULL: the step length is read from device memory (graph replay)
+  const uint32_t* step_dev;  // non-NULL: the Philox step counter is read from device memory
 };
 
 cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool smem_cells, bool prefetch,
@@ -112,6 +114,7 @@ struct PlanArgs {
   double t_emit_floor;
   int method;                      // IMC_METHOD_*
   float* cf_rate;                  // Carter-Forest: [c] re-emission rate (tilt[4c+3]: emission rate)
+  const double* dt_dev;            // non-NULL: dt read from device memory (graph replay)
   // outputs
   double* sa; double* ss;          // FP64 [ncg]
   float2* sass;                    // FP32 [ncg]
@@ -185,6 +188,7 @@ struct FillArgs {
   // Carter-Forest emission: birth time of density ~ exp(-k t) on [0, dt], k = cf_rate4[4c]
   // when k > cf_thr (else uniform); NULL otherwise
   const double* cf_rate4; double cf_thr;
+  const double* time_scale_dev; const uint32_t* step_dev;  // non-NULL: read from device memory
 };
 cudaError_t imc_launch_fill_volume(const FillArgs& a, cudaStream_t s);
 
@@ -201,6 +205,7 @@ struct BndArgs {
   // multigroup: Planck group at the face cell's temperature
   int ng; const double* faceT; const double* gedges; const double* mixcdf; double* boundary_group;
   int below_last;              // MG 1-D: an energy below the lowest edge goes to the last group
+  const double* dt_dev; const uint32_t* step_dev;  // non-NULL: read from device memory
 };
 cudaError_t imc_launch_fill_boundary(const BndArgs& a, cudaStream_t s);
 
@@ -213,6 +218,7 @@ struct CombArgs {
   int nc, nb, per_group;
   int conserve_rad;            // copies in bin b weigh ecen[b] / ncopy[b] (bin energy kept)
   int* mode;                   // set by the comb plan: 0 comb, 1 compact only (copy live entries)
+  const uint32_t* step_dev;    // non-NULL: the Philox step counter is read from device memory
   unsigned long long* n_live;  // live entries (counted by k_comb_ecen; zeroed before)
   const int64_t* d_n_in;       // entries to comb (device)
   long long n_bound;           // host upper bound of *d_n_in (grid sizing)
@@ -257,6 +263,7 @@ struct PlanMgArgs {
   // 1-D sphere (MG_IMC1D): stratified (group, cell) bins b = g*nc + c
   double* emit_E; long long* emit_n; long long* emit_off; float* emit_w; double* emit_issued;
   double* src_QV; long long* src_n; long long* src_off; float* src_w; double* src_issued;
+  const double* dt_dev;            // non-NULL: dt read from device memory (graph replay)
 };
 cudaError_t imc_launch_plan_mg(const PlanMgArgs& a, cudaStream_t s);
 cudaError_t imc_launch_plan_mg1d(const PlanMgArgs& a, cudaStream_t s);
@@ -283,5 +290,6 @@ struct FillMgArgs {
   double time_scale;
   uint64_t seed; uint32_t step; uint32_t tag;
   float* p1; float* p2; float* d1; float* d2; float* wb; float* t; int* cell; int* group;
+  const double* time_scale_dev; const uint32_t* step_dev;  // non-NULL: read from device memory
 };
 cudaError_t imc_launch_fill_mg(const FillMgArgs& a, cudaStream_t s);

@@ -22,6 +22,8 @@ using namespace imcsample;
 namespace {
 
 __global__ void k_fill_volume(FillArgs a) {
+  const double time_scale = a.time_scale_dev ? *a.time_scale_dev : a.time_scale;  // graph replay
+  const uint32_t step = a.step_dev ? *a.step_dev : a.step;
   const long long stride = (long long)gridDim.x * blockDim.x;
   const long long n = *a.d_n, base = *a.d_base;
   for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
@@ -33,8 +35,8 @@ __global__ void k_fill_volume(FillArgs a) {
     const int oc = o - g * a.nc;
     const int i = oc / a.ny, j = oc - i * a.ny;
     const int c = i + a.nx * j;
-    const U4 r = draw(a.seed, (uint32_t)k, 0, a.step, a.tag);
-    const U4 s = draw(a.seed, (uint32_t)k, 1, a.step, a.tag);
+    const U4 r = draw(a.seed, (uint32_t)k, 0, step, a.tag);
+    const U4 s = draw(a.seed, (uint32_t)k, 1, step, a.tag);
     const double u0 = u01d(r.x), u1 = u01d(r.y), u2 = u01d(r.z), u3 = u01d(r.w);
     const double s0 = u01d(s.x), s1 = u01d(s.y);
     const double ea = a.e1[i], eb = a.e1[i + 1];
@@ -77,19 +79,19 @@ __global__ void k_fill_volume(FillArgs a) {
     if (a.p2) a.p2[b] = (float)p2;
     if (a.d2) a.d2[b] = (float)d2;
     a.wb[b] = a.w[a.bins_by_group ? o : c];
-    double tb = s0 * a.time_scale;
+    double tb = s0 * time_scale;
     if (a.cf_rate4) {
       // Carter-Forest birth time, density ~ exp(-k t) on [0, dt]: t = -ln(1 - xi (1 - e^{-k dt})) / k
       // (IMC/IMC1D_CarterForest.py:529-536, IMC/IMC2D_CarterForest.py:51-56)
       const double k = a.cf_rate4[4 * c];
-      if (k > a.cf_thr) tb = -log1p(s0 * expm1(-k * a.time_scale)) / k;
+      if (k > a.cf_thr) tb = -log1p(s0 * expm1(-k * time_scale)) / k;
     }
     a.t[b] = (float)tb;
     a.cell[b] = c;
     if (a.group) {
       int gb = g;
       if (a.tr) {  // MG 1-D initial census: Planck group at the cell's Tr (MG_IMC/MG_IMC1D.py:557-560)
-        const U4 d = draw(a.seed, (uint32_t)k, 2, a.step, a.tag);
+        const U4 d = draw(a.seed, (uint32_t)k, 2, step, a.tag);
         gb = planck_group(a.tr[c], a.gedges, a.ng, a.mixcdf, s1, u01d(s.z), u01d(s.w), u01d(d.x), u01d(d.y), true);
       }
       a.group[b] = gb;
@@ -98,6 +100,8 @@ __global__ void k_fill_volume(FillArgs a) {
 }
 
 __global__ void k_fill_boundary(BndArgs a) {
+  const double dt = a.dt_dev ? *a.dt_dev : a.dt;  // graph replay
+  const uint32_t step = a.step_dev ? *a.step_dev : a.step;
   const long long stride = (long long)gridDim.x * blockDim.x;
   const bool oned = (a.geom == G_SLAB || a.geom == G_SPHERE);
   const bool along2 = a.side < 2;
@@ -109,8 +113,8 @@ __global__ void k_fill_boundary(BndArgs a) {
   const double total = cdf[nf - 1];
   const float wq = (float)(total / (double)n);
   for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
-    const U4 ra = draw(a.seed, (uint32_t)k, 0, a.step, TAG_BOUNDARY | (uint32_t)a.side);
-    const U4 rb = draw(a.seed, (uint32_t)k, 1, a.step, TAG_BOUNDARY | (uint32_t)a.side);
+    const U4 ra = draw(a.seed, (uint32_t)k, 0, step, TAG_BOUNDARY | (uint32_t)a.side);
+    const U4 rb = draw(a.seed, (uint32_t)k, 1, step, TAG_BOUNDARY | (uint32_t)a.side);
     const double ua0 = u01d(ra.x), ua1 = u01d(ra.y), ua2 = u01d(ra.z), ua3 = u01d(ra.w);
     const double x = ua0 * total;
     int lo = 0, hi = nf;  // lower_bound(cdf, x)
@@ -118,7 +122,7 @@ __global__ void k_fill_boundary(BndArgs a) {
     int q = min(lo, nf - 1);
     while (q > 0 && Ef[q] <= 0.0) --q;
     const double mu_n = sqrt(ua2);
-    const double t = u01d(rb.x) * a.dt;
+    const double t = u01d(rb.x) * dt;
     double p1, p2 = 0.0, d1, d2 = 0.0;
     int i, j = 0;
     const int side = a.side;
@@ -166,7 +170,7 @@ __global__ void k_fill_boundary(BndArgs a) {
     if (a.group) {
       int g = 0;
       if (a.ng > 1) {
-        const U4 rd = draw(a.seed, (uint32_t)k, 2, a.step, TAG_BOUNDARY | (uint32_t)a.side);
+        const U4 rd = draw(a.seed, (uint32_t)k, 2, step, TAG_BOUNDARY | (uint32_t)a.side);
         g = planck_group(a.faceT[q], a.gedges, a.ng, a.mixcdf, u01d(rb.y), u01d(rb.z), u01d(rb.w), u01d(rd.x),
                          u01d(rd.y), a.below_last != 0);
         atomicAdd(a.boundary_group + g, (double)wq);
@@ -180,6 +184,8 @@ __global__ void k_fill_boundary(BndArgs a) {
 // initial census (:992-1097): cell ~ canonical CDF over cells, group ~ the cell's cumulative
 // group emission (or the Planck spectrum at tr for the IC), equal weights, uniform position.
 __global__ void k_fill_mg(FillMgArgs a) {
+  const double time_scale = a.time_scale_dev ? *a.time_scale_dev : a.time_scale;  // graph replay
+  const uint32_t step = a.step_dev ? *a.step_dev : a.step;
   const long long stride = (long long)gridDim.x * blockDim.x;
   const long long n = *a.d_n, base = *a.d_base;
   if (n <= 0) return;
@@ -187,8 +193,8 @@ __global__ void k_fill_mg(FillMgArgs a) {
   const float wq = (float)(total / (double)n);
   const bool ic = a.gcdf == nullptr;
   for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
-    const U4 ra = draw(a.seed, (uint32_t)k, 0, a.step, a.tag);
-    const U4 rb = draw(a.seed, (uint32_t)k, 1, a.step, a.tag);
+    const U4 ra = draw(a.seed, (uint32_t)k, 0, step, a.tag);
+    const U4 rb = draw(a.seed, (uint32_t)k, 1, step, a.tag);
     const double x = u01d(ra.x) * total;
     int lo = 0, hi = a.nc;  // first c with cdf[c] > x
     while (lo < hi) { const int mid = (lo + hi) >> 1; if (a.cdf[mid] <= x) lo = mid + 1; else hi = mid; }
@@ -204,7 +210,7 @@ __global__ void k_fill_mg(FillMgArgs a) {
       for (int q = 0; q < a.ng; ++q) if (gc[q] >= y) { g = q; break; }
       up1 = u01d(ra.z); up2 = u01d(ra.w); ua = u01d(rb.x); ub = u01d(rb.y); ut = u01d(rb.z);
     } else {
-      const U4 rd = draw(a.seed, (uint32_t)k, 2, a.step, a.tag);
+      const U4 rd = draw(a.seed, (uint32_t)k, 2, step, a.tag);
       up1 = u01d(ra.y); up2 = u01d(ra.z); ua = u01d(ra.w); ub = u01d(rb.x); ut = 0.0;
       g = planck_group(a.tr[c], a.gedges, a.ng, a.mixcdf, u01d(rb.y), u01d(rb.z), u01d(rb.w), u01d(rd.x), u01d(rd.y));
     }
@@ -216,7 +222,7 @@ __global__ void k_fill_mg(FillMgArgs a) {
     a.p1[b] = (float)p1; a.p2[b] = (float)p2;
     a.d1[b] = (float)d1; a.d2[b] = (float)d2;
     a.wb[b] = wq;
-    a.t[b] = (float)(ut * a.time_scale);
+    a.t[b] = (float)(ut * time_scale);
     a.cell[b] = c;
     a.group[b] = g;
   }

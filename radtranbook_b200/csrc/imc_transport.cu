@@ -39,6 +39,8 @@ enum : int { B_CENSUS = 0, B_FLOOR, B_REFLECT, B_CAP, B_ESCAPE, B_CAPTURE, B_N }
 // weight floor are not moved (they stay in census).
 template <int GEOM, bool SMEM_CELLS, bool PREFETCH, bool MG, bool CF>
 __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
+  const float dtk = a.dt_dev ? (float)*a.dt_dev : a.dt;  // graph replay: step length and Philox
+  const uint32_t stepk = a.step_dev ? *a.step_dev : a.step;  // step counter from device memory
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ unsigned blk_cnt[B_N];
   __shared__ unsigned long long blk_esc[4];
@@ -107,7 +109,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
       if (!has && rank < avail) {
         pid = chunk_next + rank;
         w = a.w[pid];
-        dcen = (a.dt - a.t[pid]) * c_light;
+        dcen = (dtk - a.t[pid]) * c_light;
         if ((MG2 || CF ? w > weight_floor : w > 0.f) && dcen > 0.f) {
           x = a.p1[pid]; u = a.d1[pid];
           if (MG) grp = a.group[pid];
@@ -115,7 +117,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
           const int c = a.cell[pid];
           cj = c / a.nx; ci = c - cj * a.nx;
           ev = 0;
-          if (PREFETCH) rnext = draw(a.seed, pid, 0u, a.step, TAG_TRANSPORT);
+          if (PREFETCH) rnext = draw(a.seed, pid, 0u, stepk, TAG_TRANSPORT);
           has = true;
         }
       }
@@ -145,9 +147,9 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
           // this event's numbers were drawn during the previous event; draw the next now so
           // its dependent multiply chain overlaps this event's geometry
           r = rnext;
-          rnext = draw(a.seed, pid, ev + 1u, a.step, TAG_TRANSPORT);
+          rnext = draw(a.seed, pid, ev + 1u, stepk, TAG_TRANSPORT);
         } else {
-          r = draw(a.seed, pid, ev, a.step, TAG_TRANSPORT);
+          r = draw(a.seed, pid, ev, stepk, TAG_TRANSPORT);
         }
         ++ev;
         float d, sb, L, xn = x, yn = y, un = u, vn = v;

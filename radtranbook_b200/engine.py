@@ -264,7 +264,8 @@ class Engine:
     # One step = transport_async -> material_update -> (caller's inv_eos) -> comb_async ->
     # fetch(): a single device->host copy of the summary and one stream synchronisation.
     def _params(self, step, dt, theta, n_target, n_boundary, n_source, face_T, reflect, max_events,
-                rz_linear_source, t_emit_floor, n_boundary_side=None, method=0, cf_fastpath=0.0) -> ImcStepParams:
+                rz_linear_source, t_emit_floor, n_boundary_side=None, method=0, cf_fastpath=0.0,
+                step_dev=None, dt_dev=None) -> ImcStepParams:
         par = ImcStepParams()
         par.seed = self.seed
         par.step = int(step) & 0xFFFFFFFF
@@ -285,6 +286,8 @@ class Engine:
             par.n_boundary_side[q] = int(n)
         par.method = int(method)
         par.cf_fastpath = float(cf_fastpath)
+        par.step_dev = _ptr(step_dev)
+        par.dt_dev = _ptr(dt_dev)
         return par
 
     def _set_census_count(self, n: int) -> None:
@@ -293,9 +296,11 @@ class Engine:
 
     def transport_async(self, T, sigma, cv, source, step, dt, theta, n_target, n_boundary, n_source, face_T,
                         reflect, max_events=0, rz_linear_source=True, t_emit_floor=0.0, n_boundary_side=None,
-                        method=0, cf_fastpath=0.0) -> int:
+                        method=0, cf_fastpath=0.0, step_dev=None, dt_dev=None) -> int:
         """Sources + tracking without a host synchronisation.  Returns the host upper bound
-        of the tracked bank size (the true size is in the device summary)."""
+        of the tracked bank size (the true size is in the device summary).  step_dev / dt_dev:
+        device scalars (int32 / float64) the kernels read the step counter and dt from, for a
+        captured step replayed with new values."""
         if not self._census_dev_valid:
             self._set_census_count(self.bank.size)
         self._last_transport = ((T, sigma, cv, source, step, dt, theta, n_target, n_boundary, n_source, face_T,
@@ -304,7 +309,8 @@ class Engine:
                                                 method=method, cf_fastpath=cf_fastpath))
         self._mat = ImcMaterial(_ptr(T), _ptr(sigma), _ptr(cv), _ptr(source))
         self._par = self._params(step, dt, theta, n_target, n_boundary, n_source, face_T, reflect, max_events,
-                                 rz_linear_source, t_emit_floor, n_boundary_side, method, cf_fastpath)
+                                 rz_linear_source, t_emit_floor, n_boundary_side, method, cf_fastpath,
+                                 step_dev, dt_dev)
         bound = int(self.lib.imc_source_bound(ctypes.byref(self.cmesh), ctypes.byref(self._par)))
         self.bank.ensure(self.bank.size + bound)
         wsp, wsn = self._ws(self.bank.capacity)
@@ -318,20 +324,32 @@ class Engine:
         return self._upper
 
     def comb_async(self, n_max: int, step: int, e: torch.Tensor | None, per_group: bool = False,
-                   conserve_radiation: bool = False) -> None:
-        """Queue the comb (n_max semantics as comb()); fetch() completes it."""
+                   conserve_radiation: bool = False, step_dev: torch.Tensor | None = None,
+                   out_capacity: int | None = None) -> None:
+        """Queue the comb (n_max semantics as comb()); fetch() completes it.  step_dev: device
+        step counter (graph replay); out_capacity: cap the combed census below the spare bank's
+        capacity (a larger one is flagged as an overflow and the census is emptied)."""
         self.spare.size = 0
         want = int(1.15 * n_max) if n_max > 0 else self._upper
         self.spare.ensure(want + 2 * self.nc * self.ng + 4096)
-        self._comb_args = (int(n_max), int(step), e, _comb_flags(per_group, conserve_radiation))
+        self._comb_args = (int(n_max), int(step), e, _comb_flags(per_group, conserve_radiation), step_dev,
+                           out_capacity)
         self._launch_comb()
 
     def _launch_comb(self) -> None:
-        n_max, step, e, flags = self._comb_args
+        n_max, step, e, flags, step_dev, out_capacity = self._comb_args
         cin = self.bank.c()
         cin.size = self._upper
         cout = self.spare.c()
+        if out_capacity is not None:
+            cout.capacity = min(int(out_capacity), cout.capacity)
         wsp, wsn = self._ws(max(self._upper, self.bank.capacity))
+        if step_dev is not None:
+            st = self.lib.imc_comb_async_dev(ctypes.byref(self.cmesh), ctypes.byref(cin), ctypes.byref(cout), n_max,
+                                             self.seed, step_dev.data_ptr(), flags, _ptr(self.disc), _ptr(e),
+                                             wsp, wsn, self.summary_dev.data_ptr(), self._stream())
+            _lib.check("imc_comb_async_dev", st)
+            return
         st = self.lib.imc_comb_async(ctypes.byref(self.cmesh), ctypes.byref(cin), ctypes.byref(cout), n_max,
                                      self.seed, step & 0xFFFFFFFF, flags, _ptr(self.disc), _ptr(e),
                                      wsp, wsn, self.summary_dev.data_ptr(), self._stream())
