@@ -37,6 +37,7 @@ sys.path.insert(0, ROOT)
 METRIC = "IMC track-segments/s and FOM=1/(rel.var*time) on 1 B200: plain vs batched/adjoint"
 UNIT = "track-segments/s"
 B_SEG_2D = 72  # bytes per 2-D gray segment: 36-byte record loaded + stored
+B_SEG_2D_MG = 80  # 2-D multigroup: the 36-byte record plus the group index, loaded + stored
 # DRAM bytes the tracking kernel actually moves per segment on this workload: ncu
 # dram__bytes_read.sum + dram__bytes_write.sum of one full-size launch (401.4 MB for
 # 66.79 M segments); the histories stay in registers across their events.
@@ -424,6 +425,59 @@ def form_device_loop(steps: int = 20) -> dict:
     return out
 
 
+def form_mg_crooked_pipe(steps: int = 12, warmup: int = 3) -> dict:
+    """The multigroup crooked pipe (MG_IMC/problems/crooked_pipe_multigroup_imc.py, 10 groups,
+    60 x 210 RZ, 'standard' preset: 200k emission + 200k surface-source particles per step,
+    Nmax 1e6 growing by 5e4 per step) through the mg_imc2d drop-in step with device
+    callables, dt from 1e-4 ns growing by 1.1; CUDA-event timing of whole steps."""
+    import torch
+
+    from radtranbook_b200 import mg_imc2d, problems
+
+    p = problems.mg_crooked_pipe(mode="standard")
+    e1, e2, ge = p["edges1"], p["edges2"], p["energy_edges"]
+    st = mg_imc2d.init_simulation(p["Ntarget"], p["Tinit"], p["Tr_init"], e1, e2, ge, p["eos_dev"], p["inv_eos_dev"],
+                                  T_emit_floor=p["T_emit_floor"], geometry="rz", seed=0x36C9)
+    state = {"dt": p["dt_initial"], "k": 0}
+
+    def run(n, st):
+        seg = hist = 0
+        worst = 0.0
+        for _ in range(n):
+            Nmax = min(p["Nmax"] + state["k"] * p["Nmax_growth"], p["Nmax_final"])
+            st, info = mg_imc2d.step(st, p["Ntarget"], p["Nboundary"], 0, Nmax, p["T_boundary"], state["dt"], e1,
+                                     e2, ge, p["sigma_dev"], p["inv_eos_dev"], p["cv_dev"], p["source"],
+                                     reflect=p["reflect"], geometry="rz",
+                                     boundary_source_func=p["boundary_source_func"], T_emit_floor=p["T_emit_floor"])
+            te = info["profiling"]["transport_events"]
+            seg += te["total"]
+            hist += te["n_particles_transported"]
+            track.append(info["profiling"]["phase_times_s"]["transport"] * 1e3)
+            worst = max(worst, abs(info["ledger"]["relative_closure"]))
+            state["dt"] = min(state["dt"] * p["dt_growth"], p["dt_max"])
+            state["k"] += 1
+        return st, seg, hist, worst, info
+
+    track = []
+    st, _, _, _, _ = run(warmup, st)
+    track.clear()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1_ = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    st, seg, hist, worst, info = run(steps, st)
+    e1_.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1_)
+    peak, _ = measured_peaks()
+    return {"workload": "mg_crooked_pipe_rz_60x210_10g_standard", "steps": steps, "warmup": warmup,
+            "segments_per_s": seg / (ms * 1e-3), "histories_per_s": hist / (ms * 1e-3), "ms_per_step": ms / steps,
+            "segments_per_step": seg / steps, "census_after": int(info["N_particles"]), "time_ns": float(st.time),
+            "transport_ms_per_step": float(np.mean(track)),
+            "step_roofline_frac": B_SEG_2D_MG * seg / (ms * 1e-3) / 1e9 / peak,
+            "bytes_per_segment_algorithmic": B_SEG_2D_MG, "energy_closure_max_rel": worst}
+
+
 def max_time_and_totals(dist, ms: float, counts: list, device) -> tuple:
     """Whole-job figures of a timed region: the slowest rank's device time (ms) and the
     sum over ranks of each count (segments, histories)."""
@@ -539,7 +593,8 @@ def run_ours(args, rank: int, world: int):
     forms = fom = None
     if world == 1 and not args.no_forms:
         forms = {"batched": form_batched(args.batch_steps, not args.no_tune), "adjoint": form_adjoint(),
-                 "carter_forest": form_carter_forest(), "device_loop": form_device_loop()}
+                 "carter_forest": form_carter_forest(), "device_loop": form_device_loop(),
+                 "mg_crooked_pipe": form_mg_crooked_pipe()}
         forms["carter_forest"]["over_fleck_cummings"] = forms["carter_forest"]["segments_per_s"] / value
     if world == 1 and not args.no_fom:
         fom = {"gpu": fom_gpu(p, args.fom_steps, args.fom_seeds, dict(eng.launch))}

@@ -11,6 +11,8 @@ problem can be run through the drop-in API, the device engine or the CPU oracle.
                  cv 0.001; wall sigma 2000, cv 0.5; 0.5 keV on z=0 for r<0.5; reflect r=0;
                  T0 = 0.05 keV; dt 0.01 ns x 100; 2e6 source particles per step split 2:1
                  emission:boundary, Nmax 6.67e6 (IMC/CrookedPipe2D.py geometry)
+  mg_crooked_pipe  2-D RZ multigroup crooked pipe (MG_IMC/problems/crooked_pipe_multigroup_imc.py
+                 with its command-line defaults; see the function)
 """
 from __future__ import annotations
 
@@ -104,6 +106,79 @@ def crooked_pipe(scale: float = 1.0, nr: int = 60, nz: int = 210) -> dict:
         Ntarget=n_src - n_bnd, Nboundary=n_bnd, Nsource=0, Nmax=int(round(6.67e6 * scale)),
         T_boundary=(0.0, 0.0, 0.0, 0.0), reflect=(True, False, False, False), boundary_source_func=bsf,
         dt=0.01, n_steps=100, source=np.zeros((nr, nz)), thin=thin,
+        fiducials={"r=0,z=0.25": (0.0, 0.25), "r=0,z=2.75": (0.0, 2.75), "r=1.25,z=3.5": (1.25, 3.5),
+                   "r=0,z=4.25": (0.0, 4.25), "r=0,z=6.75": (0.0, 6.75)},
+    )
+
+
+def mg_crooked_pipe_thick(r: np.ndarray, z: np.ndarray) -> np.ndarray:
+    """Wall (optically thick) map of the multigroup crooked pipe, at cell centres
+    (MG_IMC/problems/crooked_pipe_multigroup_imc.py:185-208)."""
+    thin = (((r < 0.5) & ((z < 3.0) | (z > 4.0))) | ((r < 1.5) & (z > 2.5) & (z < 3.0))
+            | ((r < 1.5) & (z > 4.0) & (z < 4.5)) | ((r >= 1.0) & (r < 1.5) & (z > 2.5) & (z < 4.5)))
+    return ~thin
+
+
+def mg_crooked_pipe(n_groups: int = 10, nr: int = 60, nz: int = 210, mode: str = "standard",
+                    bc_T: float = 0.5) -> dict:
+    """The multigroup crooked pipe of MG_IMC/problems/crooked_pipe_multigroup_imc.py with its
+    command-line defaults: r in [0,2] x z in [0,7] cm, wall density 2, pipe density 0.1 g/cm^3,
+    e = 0.05 rho T, sigma_g(T) = sqrt(sigma(T, E_g) sigma(T, E_g+1)) with
+    sigma(T, E) = min(10 rho max(T, 0.01)^-1/2 E^-3, 1e14), groups log-spaced on [0.01, 10] keV,
+    T0 = 0.05 keV, a 0.5 keV blackbody surface source on z = 0 for r < 0.5, reflecting axis,
+    emission only from cells above 0.075 keV, dt from 1e-4 ns growing by 1.1 to 0.01 ns, and the
+    driver's particle presets ('quick' 20k + 20k per step, Nmax 1e5 + 1e4 per step to 5e5;
+    'standard' 200k + 200k, Nmax 1e6 + 5e4 per step to 5e6)."""
+    r_edges = np.linspace(0.0, 2.0, nr + 1)
+    z_edges = np.linspace(0.0, 7.0, nz + 1)
+    rc = 0.5 * (r_edges[:-1] + r_edges[1:])
+    zc = 0.5 * (z_edges[:-1] + z_edges[1:])
+    R, Z = np.meshgrid(rc, zc, indexing="ij")
+    rho = np.where(mg_crooked_pipe_thick(R, Z), 2.0, 0.1)
+    cvg = 0.05 * rho
+    edges = np.logspace(np.log10(1e-2), np.log10(10.0), n_groups + 1)
+    cache = {}
+
+    def dev(a, T):
+        key = (id(a), T.device)
+        if key not in cache:
+            cache[key] = torch.as_tensor(a, dtype=torch.float64, device=T.device)
+        return cache[key]
+
+    def opacity(g):
+        lo, hi = float(edges[g]), float(edges[g + 1])
+
+        def host(T):
+            Ts = np.maximum(T, 1e-2) ** -0.5
+            return np.sqrt(np.minimum(10.0 * rho * Ts * lo ** -3, 1e14) * np.minimum(10.0 * rho * Ts * hi ** -3, 1e14))
+
+        @device_callable
+        def device(T):
+            Ts = torch.pow(torch.clamp(T, min=1e-2), -0.5)
+            rh = dev(rho, T)
+            return torch.sqrt(torch.clamp(10.0 * rh * Ts * lo ** -3, max=1e14)
+                              * torch.clamp(10.0 * rh * Ts * hi ** -3, max=1e14))
+        return host, device
+
+    ops = [opacity(g) for g in range(n_groups)]
+    presets = {"quick": (20_000, 20_000, 100_000, 10_000, 500_000),
+               "standard": (200_000, 200_000, 1_000_000, 50_000, 5_000_000)}
+    nt, nb, nmax, ngrow, nfin = presets[mode]
+
+    def bsf(r, z, side):
+        return bc_T if (side == "zmin" and r < 0.5) else 0.0
+
+    return dict(
+        name=f"2-D RZ multigroup crooked pipe ({nr}x{nz}, {n_groups} groups)",
+        geometry="rz", dim=2, edges1=r_edges, edges2=z_edges, energy_edges=edges, rho=rho,
+        Tinit=np.full((nr, nz), 0.05), Tr_init=np.full((nr, nz), 0.05),
+        sigma_host=[h for h, _ in ops], sigma_dev=[d for _, d in ops],
+        cv_host=lambda T: cvg.copy(), cv_dev=device_callable(lambda T: dev(cvg, T)),
+        eos_host=lambda T: cvg * T, inv_eos_host=lambda e: e / cvg,
+        eos_dev=device_callable(lambda T: dev(cvg, T) * T), inv_eos_dev=device_callable(lambda e: e / dev(cvg, e)),
+        Ntarget=nt, Nboundary=nb, Nsource=0, Nmax=nmax, Nmax_growth=ngrow, Nmax_final=nfin,
+        T_boundary=(0.0, 0.0, 0.0, 0.0), reflect=(True, False, False, False), boundary_source_func=bsf,
+        T_emit_floor=0.075, dt_initial=1e-4, dt_max=0.01, dt_growth=1.1, source=np.zeros((nr, nz)),
         fiducials={"r=0,z=0.25": (0.0, 0.25), "r=0,z=2.75": (0.0, 2.75), "r=1.25,z=3.5": (1.25, 3.5),
                    "r=0,z=4.25": (0.0, 4.25), "r=0,z=6.75": (0.0, 6.75)},
     )
