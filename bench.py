@@ -429,15 +429,21 @@ def form_mg_crooked_pipe(steps: int = 12, warmup: int = 3) -> dict:
     """The multigroup crooked pipe (MG_IMC/problems/crooked_pipe_multigroup_imc.py, 10 groups,
     60 x 210 RZ, 'standard' preset: 200k emission + 200k surface-source particles per step,
     Nmax 1e6 growing by 5e4 per step) through the mg_imc2d drop-in step with device
-    callables, dt from 1e-4 ns growing by 1.1; CUDA-event timing of whole steps."""
+    callables, dt from 1e-4 ns growing by 1.1; CUDA-event timing of whole steps.  The same
+    steps (same dt and Nmax sequence, from the same state) are also run as the device-resident
+    loop (one replayed graph, radtranbook_b200.driver.DeviceLoop)."""
     import torch
 
-    from radtranbook_b200 import mg_imc2d, problems
+    from radtranbook_b200 import driver, mg_imc2d, problems
 
     p = problems.mg_crooked_pipe(mode="standard")
     e1, e2, ge = p["edges1"], p["edges2"], p["energy_edges"]
-    st = mg_imc2d.init_simulation(p["Ntarget"], p["Tinit"], p["Tr_init"], e1, e2, ge, p["eos_dev"], p["inv_eos_dev"],
-                                  T_emit_floor=p["T_emit_floor"], geometry="rz", seed=0x36C9)
+
+    def init():
+        return mg_imc2d.init_simulation(p["Ntarget"], p["Tinit"], p["Tr_init"], e1, e2, ge, p["eos_dev"],
+                                        p["inv_eos_dev"], T_emit_floor=p["T_emit_floor"], geometry="rz", seed=0x36C9)
+
+    st = init()
     state = {"dt": p["dt_initial"], "k": 0}
 
     def run(n, st):
@@ -454,13 +460,15 @@ def form_mg_crooked_pipe(steps: int = 12, warmup: int = 3) -> dict:
             hist += te["n_particles_transported"]
             track.append(info["profiling"]["phase_times_s"]["transport"] * 1e3)
             worst = max(worst, abs(info["ledger"]["relative_closure"]))
+            used.append(state["dt"])
             state["dt"] = min(state["dt"] * p["dt_growth"], p["dt_max"])
             state["k"] += 1
         return st, seg, hist, worst, info
 
-    track = []
+    track, used = [], []
     st, _, _, _, _ = run(warmup, st)
     track.clear()
+    del used[:]
     e0 = torch.cuda.Event(enable_timing=True)
     e1_ = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
@@ -470,12 +478,30 @@ def form_mg_crooked_pipe(steps: int = 12, warmup: int = 3) -> dict:
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1_)
     peak, _ = measured_peaks()
+    dts = list(used)
+    # the same steps as the device-resident loop
+    st2 = init()
+    state.update(dt=p["dt_initial"], k=0)
+    st2, _, _, _, _ = run(warmup, st2)
+    loop = driver.DeviceLoop(st2, Ntarget=p["Ntarget"], Nboundary=p["Nboundary"], Nsource=0,
+                             Nmax=p["Nmax"] + warmup * p["Nmax_growth"], T_boundary=p["T_boundary"],
+                             sigma_a_func=p["sigma_dev"], inv_eos=p["inv_eos_dev"], cv=p["cv_dev"],
+                             reflect=p["reflect"], geometry="rz", max_events=1_000_000,
+                             boundary_source_func=p["boundary_source_func"], T_emit_floor=p["T_emit_floor"],
+                             Nmax_growth=p["Nmax_growth"], Nmax_final=p["Nmax_final"])
+    res = loop.run(dts)
+    seg_g = sum(s["transport_events"]["total"] for s in res["steps"])
+    loop_ms = res["device_ms"] / steps
     return {"workload": "mg_crooked_pipe_rz_60x210_10g_standard", "steps": steps, "warmup": warmup,
             "segments_per_s": seg / (ms * 1e-3), "histories_per_s": hist / (ms * 1e-3), "ms_per_step": ms / steps,
             "segments_per_step": seg / steps, "census_after": int(info["N_particles"]), "time_ns": float(st.time),
             "transport_ms_per_step": float(np.mean(track)),
             "step_roofline_frac": B_SEG_2D_MG * seg / (ms * 1e-3) / 1e9 / peak,
-            "bytes_per_segment_algorithmic": B_SEG_2D_MG, "energy_closure_max_rel": worst}
+            "bytes_per_segment_algorithmic": B_SEG_2D_MG, "energy_closure_max_rel": worst,
+            "device_loop": {"ms_per_step": loop_ms, "speedup_over_eager": (ms / steps) / loop_ms,
+                            "segments_per_s": seg_g / (loop_ms * steps * 1e-3),
+                            "same_census_as_eager": int(res["steps"][-1]["N_particles"]) == int(info["N_particles"]),
+                            "max_relative_closure": res["max_relative_closure"]}}
 
 
 def max_time_and_totals(dist, ms: float, counts: list, device) -> tuple:

@@ -287,13 +287,24 @@ IMC_API imc_status imc_comb_async(const imc_mesh* mesh, const imc_bank* in, imc_
                                   size_t workspace_bytes, imc_step_summary* summary,
                                   void* stream);
 /* imc_comb_async with the Philox step counter read from device memory when the comb runs
- * (step_dev, a DEVICE pointer), so a captured comb can be replayed for every step.  No
- * reference counterpart (the reference time loop runs on the host). */
+ * (step_dev, a DEVICE pointer), so a captured comb can be replayed for every step; when
+ * n_max_dev (DEVICE, nullable) is given, the comb target is read from it too (a growing
+ * Nmax, MG_IMC/MG_IMC2D.py:2067-2120 'Nmax_next'), and n_max only selects the mode (> 0).
+ * No reference counterpart (the reference time loop runs on the host). */
 IMC_API imc_status imc_comb_async_dev(const imc_mesh* mesh, const imc_bank* in, imc_bank* out,
-                                      int64_t n_max, uint64_t seed, const uint32_t* step_dev,
-                                      int32_t per_group, double* disc, const double* e,
-                                      void* workspace, size_t workspace_bytes,
+                                      int64_t n_max, const int64_t* n_max_dev, uint64_t seed,
+                                      const uint32_t* step_dev, int32_t per_group, double* disc,
+                                      const double* e, void* workspace, size_t workspace_bytes,
                                       imc_step_summary* summary, void* stream);
+/* Energy (sum of live FP32 weights, FP64) per bin of a bank: per (group, cell) bin
+ * g*nc + c when per_group is set (needs bank->group), else per cell; out[bins] is
+ * overwritten.  The entry count is read from device memory when the kernel runs (n_dev, a
+ * DEVICE pointer, e.g. the summary's n_out after imc_comb_async; counts above bank->capacity
+ * are clipped to it), so it can follow a queued comb without a host synchronisation.  Divided
+ * by the cell volumes this is MG_IMC2D's post-comb radiation_energy_by_group
+ * (MG_IMC/MG_IMC2D.py:2017-2025). */
+IMC_API imc_status imc_bank_energy_by_bin(const imc_mesh* mesh, const imc_bank* bank, const int64_t* n_dev,
+                                          int32_t per_group, double* out, void* stream);
 /* Device time (ms) of the source fill and of tracking in this host thread's last
  * imc_step_transport[_async]; valid once that work has completed. */
 IMC_API imc_status imc_phase_times(float* ms_sources, float* ms_transport);

@@ -158,8 +158,10 @@ SIGNATURES = {
                                          c_void_p]),
     "imc_comb_async": (c_int, [POINTER(ImcMesh), POINTER(ImcBank), POINTER(ImcBank), c_int64, c_uint64, c_uint32,
                                c_int32, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p, c_void_p]),
-    "imc_comb_async_dev": (c_int, [POINTER(ImcMesh), POINTER(ImcBank), POINTER(ImcBank), c_int64, c_uint64,
-                                   c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p, c_void_p]),
+    "imc_comb_async_dev": (c_int, [POINTER(ImcMesh), POINTER(ImcBank), POINTER(ImcBank), c_int64, c_void_p,
+                                   c_uint64, c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p, c_void_p]),
+    "imc_bank_energy_by_bin": (c_int, [POINTER(ImcMesh), POINTER(ImcBank), c_void_p, c_int32, c_void_p,
+                                       c_void_p]),
     "imc_phase_times": (c_int, [POINTER(ctypes.c_float), POINTER(ctypes.c_float)]),
     "imc_energy_totals": (c_int, [POINTER(ImcMesh), POINTER(ImcBank), c_void_p, POINTER(c_double),
                                   POINTER(c_double), c_void_p, c_size_t, c_void_p]),

@@ -264,10 +264,11 @@ __global__ void __launch_bounds__(NT) k_comb_plan(CombPlanArgs a) {
   // MG_IMC/MG_IMC1D.py:1194-1200: Nmax = 0 never combs; Nmax < 0 combs once |Nmax| entries live
   const bool compact = a.force_compact || (a.threshold > 0 && (long long)*a.n_live < a.threshold);
   if (threadIdx.x == 0) *a.mode = compact ? 1 : 0;
+  const long long n_max = a.n_max_dev ? (long long)*a.n_max_dev : a.n_max;
   for (int b = threadIdx.x; b < a.nb; b += NT) {
     const double ec = a.ecen[b];
     double ew = 0.0;
-    if (E > 0.0 && ec > 0.0) ew = ec / fmax(1.0, rint((double)a.n_max * ec / E));
+    if (E > 0.0 && ec > 0.0) ew = ec / fmax(1.0, rint((double)n_max * ec / E));
     a.ew[b] = ew;
   }
   if (threadIdx.x == 0) a.sum->comb_before = E;
@@ -377,14 +378,15 @@ __device__ void block_canon_prefix(const double* x, int n, double* out, double* 
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(NT) k_plan_mg(PlanMgArgs a) {
+// Per-cell part of the 2-D multigroup plan, one thread per cell over a wide grid (each cell's
+// numbers depend on that cell alone, so the result is the single-block loop's).
+__global__ void k_plan_mg_cells(PlanMgArgs a) {
   const double dt = a.dt_dev ? *a.dt_dev : a.dt;  // device-resident step length (graph replay)
-  __shared__ double sh[NT];
-  const int t = threadIdx.x;
   const int nc = a.nc, G = a.ng;
-  for (int q = t; q <= a.nx; q += NT) a.e1f[q] = (float)a.e1[q];
-  for (int q = t; q <= a.ny; q += NT) a.e2f[q] = (float)a.e2[q];
-  if (t == 0) {
+  const int t0 = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  for (int q = t0; q <= a.nx; q += stride) a.e1f[q] = (float)a.e1[q];
+  for (int q = t0; q <= a.ny; q += stride) a.e2f[q] = (float)a.e2[q];
+  if (t0 == 0) {
     // mixture-of-Gammas CDF over n = 1..200 with weights 1/n^4 (MG_IMC/MG_IMC2D.py:105-107)
     double tot = 0.0;
     for (int n = 1; n <= 200; ++n) { const double d = (double)n; tot += 1.0 / (d * d * d * d); }
@@ -392,7 +394,7 @@ __global__ void __launch_bounds__(NT) k_plan_mg(PlanMgArgs a) {
     for (int n = 1; n <= 200; ++n) { const double d = (double)n; run += 1.0 / (d * d * d * d); a.mixcdf[n - 1] = run / tot; }
   }
   // ---- per cell: Planck fractions, Planck-mean opacity, Fleck, emission by group ----
-  for (int c = t; c < nc; c += NT) {
+  for (int c = t0; c < nc; c += stride) {
     const double T = a.T[c];
     if (!isfinite(T) || !(a.cv[c] > 0.0)) atomicOr(&a.sum->flags, (int)IMC_FLAG_NONFINITE);
     double* gc = a.Egc + (size_t)c * G;  // scratch: fractions, then cumulative emission
@@ -426,7 +428,25 @@ __global__ void __launch_bounds__(NT) k_plan_mg(PlanMgArgs a) {
     }
     a.Ec[c] = run;
   }
-  __syncthreads();
+  // fixed source [g][c] (MG_IMC/MG_IMC2D.py:1098-1170): per-cell cumulative over groups
+  if (a.source && a.n_source > 0) {
+    for (int c = t0; c < nc; c += stride) {
+      double run = 0.0;
+      for (int g = 0; g < G; ++g) {
+        run += a.source[(size_t)g * nc + c] * a.vol[c] * dt;
+        a.Sgc[(size_t)c * G + g] = run;
+      }
+      a.Sc[c] = run;
+    }
+  }
+}
+
+// Single-block part: canonical prefix sums and totals, counts, boundary faces, bank layout.
+__global__ void __launch_bounds__(NT) k_plan_mg(PlanMgArgs a) {
+  const double dt = a.dt_dev ? *a.dt_dev : a.dt;  // device-resident step length (graph replay)
+  __shared__ double sh[NT];
+  const int t = threadIdx.x;
+  const int nc = a.nc;
   block_canon_prefix(a.Ec, nc, a.cdf, sh);
   const double Eemit = a.cdf[nc - 1];
   long long n_emit = 0;
@@ -443,15 +463,6 @@ __global__ void __launch_bounds__(NT) k_plan_mg(PlanMgArgs a) {
   long long n_src = 0;
   double e_src = 0.0;
   if (a.source && a.n_source > 0) {
-    for (int c = t; c < nc; c += NT) {
-      double run = 0.0;
-      for (int g = 0; g < G; ++g) {
-        run += a.source[(size_t)g * nc + c] * a.vol[c] * dt;
-        a.Sgc[(size_t)c * G + g] = run;
-      }
-      a.Sc[c] = run;
-    }
-    __syncthreads();
     block_canon_prefix(a.Sc, nc, a.Scdf, sh);
     const double St = a.Scdf[nc - 1];
     if (St > 0.0) {
@@ -655,7 +666,9 @@ __global__ void __launch_bounds__(NT) k_ic_plan_mg(IcMgArgs a) {
 }  // namespace
 
 cudaError_t imc_launch_plan_mg(const PlanMgArgs& a, cudaStream_t s) {
-  ++g_imc_launches;
+  g_imc_launches += 2;
+  const int n = std::max(a.nc, std::max(a.nx, a.ny) + 1);
+  k_plan_mg_cells<<<(n + 255) / 256, 256, 0, s>>>(a);
   k_plan_mg<<<1, NT, 0, s>>>(a);
   return cudaGetLastError();
 }

@@ -345,7 +345,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
 imc_status comb_async(const imc_mesh* mesh, const imc_bank* in, imc_bank* out, int64_t n_max, uint64_t seed,
                       uint32_t step, int32_t per_group, double* disc, const double* e, void* workspace,
                       size_t workspace_bytes, imc_step_summary* sum, cudaStream_t s,
-                      const uint32_t* step_dev = nullptr) {
+                      const uint32_t* step_dev = nullptr, const int64_t* n_max_dev = nullptr) {
   imc_status st = check_mesh(mesh);
   if (st != IMC_OK) return st;
   const bool two_d = mesh->geometry >= IMC_GEOM_XY;
@@ -385,6 +385,7 @@ imc_status comb_async(const imc_mesh* mesh, const imc_bank* in, imc_bank* out, i
   // n_max > 0: comb to n_max; 0: keep every live entry; < 0: comb to |n_max| once at least
   // |n_max| entries are alive (MG_IMC/MG_IMC1D.py:1194-1200)
   cp.n_max = n_max < 0 ? -n_max : n_max;
+  cp.n_max_dev = n_max > 0 ? n_max_dev : nullptr;
   cp.threshold = n_max < 0 ? -n_max : 0;
   cp.force_compact = n_max == 0 ? 1 : 0;
   cp.n_live = ca.n_live; cp.mode = ca.mode;
@@ -666,12 +667,31 @@ imc_status imc_comb_async(const imc_mesh* mesh, const imc_bank* in, imc_bank* ou
 }
 
 imc_status imc_comb_async_dev(const imc_mesh* mesh, const imc_bank* in, imc_bank* out, int64_t n_max,
-                              uint64_t seed, const uint32_t* step_dev, int32_t per_group, double* disc,
-                              const double* e, void* workspace, size_t workspace_bytes, imc_step_summary* summary,
-                              void* stream) {
+                              const int64_t* n_max_dev, uint64_t seed, const uint32_t* step_dev, int32_t per_group,
+                              double* disc, const double* e, void* workspace, size_t workspace_bytes,
+                              imc_step_summary* summary, void* stream) {
   if (!step_dev) return IMC_ERR_INVALID_ARG;
   return comb_async(mesh, in, out, n_max, seed, 0u, per_group, disc, e, workspace, workspace_bytes, summary,
-                    (cudaStream_t)stream, step_dev);
+                    (cudaStream_t)stream, step_dev, n_max_dev);
+}
+
+imc_status imc_bank_energy_by_bin(const imc_mesh* mesh, const imc_bank* bank, const int64_t* n_dev,
+                                  int32_t per_group, double* out, void* stream) {
+  imc_status st = check_mesh(mesh);
+  if (st != IMC_OK) return st;
+  if (!bank || !bank->weight || !bank->cell || !n_dev || !out || bank->capacity < 0) return IMC_ERR_INVALID_ARG;
+  if (per_group && !bank->group) return IMC_ERR_INVALID_ARG;
+  const cudaStream_t s = (cudaStream_t)stream;
+  const int nc = mesh->nx * mesh->ny;
+  const int nb = per_group ? nc * std::max(1, mesh->n_groups) : nc;
+  IMC_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * nb, s));
+  CombArgs ca{};
+  ca.nc = nc; ca.nb = nb; ca.per_group = per_group ? 1 : 0;
+  ca.w = bank->weight; ca.cell = bank->cell; ca.group = bank->group;
+  ca.d_n_in = n_dev; ca.n_bound = bank->capacity;
+  ca.ecen = out;
+  IMC_CUDA(imc_launch_comb_ecen(ca, s));
+  return IMC_OK;
 }
 
 imc_status imc_comb(const imc_mesh* mesh, const imc_bank* in, imc_bank* out, int64_t n_max, uint64_t seed,

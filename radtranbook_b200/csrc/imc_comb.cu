@@ -44,7 +44,7 @@ __global__ void __launch_bounds__(256) k_comb_ecen(CombArgs a) {
   WarpStage* st = stages + (threadIdx.x >> 5);
   bins_init(t);
   __syncthreads();
-  const long long n_in = *a.d_n_in;
+  const long long n_in = min((long long)*a.d_n_in, (long long)a.n_bound);  // a count above the bound is never read
   const long long base = (long long)blockIdx.x * ECH;
   // block-uniform trip count keeps every warp converged for the aggregated reduction
   unsigned n_live = 0;
@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(256) k_comb_ecen(CombArgs a) {
     warp_bins_add(live, b, w, t, a.ecen, st);
   }
   n_live = __reduce_add_sync(FULL, n_live);
-  if ((threadIdx.x & 31) == 0 && n_live) atomicAdd(a.n_live, (unsigned long long)n_live);
+  if ((threadIdx.x & 31) == 0 && n_live && a.n_live) atomicAdd(a.n_live, (unsigned long long)n_live);
   __syncthreads();
   bins_flush(t, a.ecen);
 }

@@ -78,8 +78,13 @@ __device__ __forceinline__ float slab_face(float x, float mu, float xl, float xr
 }
 
 // ---- sphere / cylinder: cancellation-free roots of l^2 + 2 r mu l + (r^2 - R^2) = 0 ----
+// sqrt(x) = x * x^(-1/2): one hardware reciprocal square root and a multiply (a few ulp,
+// against the ~10-instruction correctly rounded sqrtf); 0 for x <= 0.  Tracking is FP32
+// with statistical tolerances, and every kernel that replays a history uses the same form.
+__device__ __forceinline__ float sqrt_nn(float x) { return x > 0.f ? x * rsqrtf(x) : 0.f; }
+
 __device__ __forceinline__ float outer_root(float r, float mu, float R, float b2) {
-  const float q = sqrtf(fmaxf(fmaf(R, R, -b2), 0.f));
+  const float q = sqrt_nn(fmaf(R, R, -b2));
   float l = (mu >= 0.f) ? __fdividef((R - r) * (R + r), fmaxf(fmaf(r, mu, q), 1e-30f)) : q - r * mu;
   return fmaxf(l, 0.f);
 }
@@ -87,7 +92,7 @@ __device__ __forceinline__ float inner_root(float r, float mu, float R, float b2
   if (!(R > 0.f) || !(mu < 0.f)) return BIGF;
   const float disc = fmaf(R, R, -b2);
   if (!(disc > 0.f)) return BIGF;
-  const float l = __fdividef((r - R) * (r + R), sqrtf(disc) - r * mu);
+  const float l = __fdividef((r - R) * (r + R), disc * rsqrtf(disc) - r * mu);
   return fmaxf(l, 0.f);
 }
 

@@ -152,6 +152,7 @@ cudaError_t imc_launch_material(const MatArgs& a, cudaStream_t s);
 struct CombPlanArgs {
   int nb;
   long long n_max;
+  const int64_t* n_max_dev;        // when set, the comb target (read at run time)
   long long threshold;             // > 0: comb only when at least this many entries are alive
   int force_compact;               // 1: no comb, only drop dead entries
   const unsigned long long* n_live;

@@ -99,7 +99,19 @@ __global__ void k_fill_volume(FillArgs a) {
   }
 }
 
+// Boundary energy by group: every particle of a face has the same FP32 weight wq, so the
+// tally is (count of the group) x wq.  Counts go to shared memory per block (groups below
+// kBndGroups) and each block adds count x wq once per group: exact and order-independent
+// (every partial sum is an integer multiple of wq below 2^29 wq), and free of the contention
+// of one FP64 atomic per particle on a handful of addresses.
+constexpr int kBndGroups = 256;
+
 __global__ void k_fill_boundary(BndArgs a) {
+  __shared__ unsigned s_gcnt[kBndGroups];
+  const bool tally_groups = a.group && a.ng > 1;
+  if (tally_groups)
+    for (int g = threadIdx.x; g < kBndGroups; g += blockDim.x) s_gcnt[g] = 0u;
+  __syncthreads();
   const double dt = a.dt_dev ? *a.dt_dev : a.dt;  // graph replay
   const uint32_t step = a.step_dev ? *a.step_dev : a.step;
   const long long stride = (long long)gridDim.x * blockDim.x;
@@ -109,7 +121,7 @@ __global__ void k_fill_boundary(BndArgs a) {
   const double* Ef = a.face;
   const double* cdf = a.face + a.nf;
   const long long n = *a.d_n, base = *a.d_base;
-  if (n <= 0) return;
+  if (n <= 0) return;  // uniform across the grid: no block passes the barrier below alone
   const double total = cdf[nf - 1];
   const float wq = (float)(total / (double)n);
   for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
@@ -173,10 +185,16 @@ __global__ void k_fill_boundary(BndArgs a) {
         const U4 rd = draw(a.seed, (uint32_t)k, 2, step, TAG_BOUNDARY | (uint32_t)a.side);
         g = planck_group(a.faceT[q], a.gedges, a.ng, a.mixcdf, u01d(rb.y), u01d(rb.z), u01d(rb.w), u01d(rd.x),
                          u01d(rd.y), a.below_last != 0);
-        atomicAdd(a.boundary_group + g, (double)wq);
+        if (g < kBndGroups) atomicAdd(&s_gcnt[g], 1u);
+        else atomicAdd(a.boundary_group + g, (double)wq);
       }
       a.group[b] = g;
     }
+  }
+  if (tally_groups) {
+    __syncthreads();
+    for (int g = threadIdx.x; g < min(a.ng, kBndGroups); g += blockDim.x)
+      if (s_gcnt[g]) atomicAdd(a.boundary_group + g, (double)s_gcnt[g] * (double)wq);
   }
 }
 

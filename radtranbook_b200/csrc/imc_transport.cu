@@ -180,9 +180,9 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
           L = fminf(rout - rin, zhi - zlo);
           const float sin2 = (1.f - v) * (1.f + v);
           if (sin2 >= 1e-15f) {
-            st_ = sqrtf(sin2);
+            const float ist = rsqrtf(sin2);
+            st_ = sin2 * ist;
             const float b2 = x * x * ((1.f - u) * (1.f + u));
-            const float ist = __frcp_rn(st_);
             s_rout = outer_root(x, u, rout, b2) * ist;
             const float li = inner_root(x, u, rin, b2);
             if (li < BIGF) s_rin = li * ist;
@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
         } else if (GEOM == G_SPHERE) {
           const float r0 = E1[ci], r1 = E1[ci + 1];
           const float ax = fmaf(u, d, x);
-          float rn = sqrtf(fmaf(ax, ax, d * d * ((1.f - u) * (1.f + u))));
+          float rn = sqrt_nn(fmaf(ax, ax, d * d * ((1.f - u) * (1.f + u))));
           float mun = rn > 1e-15f ? (x * u + d) / rn : 1.f;
           if (evt == EV_BOUNDARY) {
             if (dout <= din) { rn = r1; mun = (x * u + d) / r1; cross = X_IP; }
@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
           } else {
             if (evt == EV_SCATTER) {
               const float uz = fmaf(2.f, u01f(r.y), -1.f);
-              const float rxy = sqrtf(fmaxf(0.f, (1.f - uz) * (1.f + uz)));
+              const float rxy = sqrt_nn((1.f - uz) * (1.f + uz));
               float sp, cp;
               sincospif(2.f * u01f(r.z), &sp, &cp);
               un = rxy * cp; vn = rxy * sp;
@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
           const float rin = E1[ci], rout = E1[ci + 1], zlo = E2[cj], zhi = E2[cj + 1];
           const float l = d * st_;
           const float ax = fmaf(u, l, x);
-          float rn = sqrtf(fmaf(ax, ax, l * l * ((1.f - u) * (1.f + u))));
+          float rn = sqrt_nn(fmaf(ax, ax, l * l * ((1.f - u) * (1.f + u))));
           yn = fmaf(d, v, y);
           if (rn > 1e-15f && l > 0.f) un = fminf(1.f, fmaxf(-1.f, __fdividef(fmaf(x, u, l), rn)));
           if (evt == EV_BOUNDARY) {

@@ -15,10 +15,18 @@ replayed n/2 times (a one-step graph finishes an odd count); one synchronisation
 brings the histories back, and the FP64 energy ledger of every step is rebuilt from the
 stored summaries exactly as the eager step builds it.
 
-Requirements: gray states (imc1d, imc2d, imc1d_cf, imc2d_cf), device material callables,
+Multigroup states (mg_imc2d; MG_IMC/problems/crooked_pipe_multigroup_imc.py's loop) take a
+list of per-group opacity callables, comb per (group, cell) and may grow Nmax every step
+(Nmax_growth up to Nmax_final, read by the comb from a device schedule); the loop also keeps
+the radiation energy by group (path-length estimate, MG_IMC2D's radiation_energy_by_group)
+at the fiducial cells every step and over the mesh at output steps.
+
+Requirements: gray (imc1d, imc2d, imc1d_cf, imc2d_cf) or 2-D multigroup states, device
+material callables, fixed particle counts (no Ntotal split: it needs host estimates),
 time-independent boundary temperatures (the graph holds fixed face tables), and a census
-bound: the comb's output is capped at census_margin * Nmax (+ slack); a step that would exceed
-it is flagged (its census is emptied, so nothing is written out of bounds) and run() raises.
+bound: the comb's output is capped at census_margin * max Nmax (+ slack); a step that would
+exceed it is flagged (its census is emptied, so nothing is written out of bounds) and run()
+raises.
 """
 from __future__ import annotations
 
@@ -29,6 +37,7 @@ import torch
 
 from . import _lib
 from ._gray import face_temperatures
+from .engine import C_LIGHT
 from .materials import evaluate, is_device
 
 
@@ -65,26 +74,39 @@ def _no_host():
 
 
 class DeviceLoop:
-    """Run many drop-in steps of one gray state as a replayed CUDA graph (see the module
-    docstring).  The keyword arguments are those of the drop-in step (IMC2D.step names);
-    fiducial_cells: reference-layout cell indices ((i, j) in 2-D, i in 1-D) whose T and Tr are
-    recorded after every step."""
+    """Run many drop-in steps of one state as a replayed CUDA graph (see the module
+    docstring).  The keyword arguments are those of the drop-in step (IMC2D.step and
+    MG_IMC2D.step names; sigma_a_func is the list of per-group callables for a multigroup
+    state); fiducial_cells: reference-layout cell indices ((i, j) in 2-D, i in 1-D) whose T and
+    Tr are recorded after every step."""
 
     def __init__(self, state, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary, sigma_a_func, inv_eos, cv,
                  source=None, reflect=(False, False, False, False), theta=1.0, conserve_comb_energy=False,
                  rz_linear_source=True, max_events=0, boundary_source_func=None, geometry="xy", method="fc",
-                 cf_fastpath=0.0, T_emit_floor=0.0, fiducial_cells=(), census_margin=1.25):
-        for f in (sigma_a_func, inv_eos, cv):
+                 cf_fastpath=0.0, T_emit_floor=0.0, fiducial_cells=(), census_margin=1.25, Nmax_growth=0,
+                 Nmax_final=None):
+        self.state = state
+        eng = state._engine
+        self.eng = eng
+        dev = eng.device
+        self.mg = eng.ng > 1
+        funcs = list(sigma_a_func) if self.mg else [sigma_a_func]
+        if self.mg and (len(funcs) != eng.ng or state._dim != 2):
+            raise ValueError("a multigroup device loop needs a 2-D state and one opacity callable per group")
+        for f in (*funcs, inv_eos, cv):
             if not is_device(f):
                 _no_host()
         if any(callable(t) for t in T_boundary):
             raise ValueError("the device loop needs time-independent boundary temperatures")
         if int(Nmax) <= 0:
             raise ValueError("the device loop combs to Nmax > 0 every step")
-        self.state = state
-        eng = state._engine
-        self.eng = eng
-        dev = eng.device
+        self.sigma_funcs = funcs
+        self.nmax = (int(Nmax), int(Nmax_growth), int(Nmax_final) if Nmax_final is not None else None)
+        self.nmax_top = max(int(Nmax), int(Nmax_final)) if (Nmax_growth and Nmax_final is not None) else int(Nmax)
+        if Nmax_growth and Nmax_final is None:
+            raise ValueError("Nmax_growth needs Nmax_final (the census bound)")
+        if self.mg:
+            rz_linear_source = False  # MG_IMC2D samples emission uniformly in the cell
         self.kw = dict(Ntarget=int(Ntarget), Nboundary=int(Nboundary), Nsource=int(Nsource), Nmax=int(Nmax),
                        theta=float(theta), max_events=int(max_events), rz_linear_source=bool(rz_linear_source),
                        method=_lib.METHOD_CARTER_FOREST if method == "cf" else _lib.METHOD_FLECK_CUMMINGS,
@@ -106,9 +128,13 @@ class DeviceLoop:
         else:
             fid = [int(i) for i in fiducial_cells]
         self.fid = torch.as_tensor(np.asarray(fid, dtype=np.int64), device=dev)
-        self.cap_census = int(census_margin * Nmax) + 2 * eng.nc * eng.ng + 4096
+        self.cap_census = int(census_margin * self.nmax_top) + 2 * eng.nc * eng.ng + 4096
         self.step_dev = torch.zeros(1, dtype=torch.int32, device=dev)
         self.dt_dev = torch.zeros(1, dtype=torch.float64, device=dev)
+        self.nmax_dev = torch.zeros(1, dtype=torch.int64, device=dev)
+        self.k_done = 0  # steps run so far (the Nmax schedule continues across run() calls)
+        if self.mg:
+            self.rad_last = torch.zeros(eng.ng * eng.nc, dtype=torch.float64, device=dev)
         self.k_dev = torch.zeros(1, dtype=torch.int64, device=dev)
         self._cap = (0, -1)   # (steps, outputs) the history buffers hold
         self._graphs = {}     # (id of the bank holding the census, steps per graph) -> graph
@@ -119,8 +145,10 @@ class DeviceLoop:
         # prologue: this step's dt and Philox step counter
         torch.index_select(self.dt_sched, 0, self.k_dev, out=self.dt_dev)
         torch.index_select(self.step_sched, 0, self.k_dev, out=self.step_dev)
+        torch.index_select(self.nmax_sched, 0, self.k_dev, out=self.nmax_dev)
         like = st.grid(st._T)
-        sigma = st.flat(evaluate(self.sigma_a_func, like, _no_host, like))
+        sigma = torch.cat([st.flat(evaluate(f, like, _no_host, like)).reshape(-1) for f in self.sigma_funcs]) \
+            if self.mg else st.flat(evaluate(self.sigma_funcs[0], like, _no_host, like))
         cvv = st.flat(evaluate(self.cv, like, _no_host, like))
         # the host-side step and dt are placeholders: the kernels read step_dev / dt_dev
         eng.transport_async(st._T, sigma, cvv, self.src, 0, 1.0, kw["theta"], kw["Ntarget"], kw["Nboundary"],
@@ -129,9 +157,15 @@ class DeviceLoop:
                             method=kw["method"], cf_fastpath=kw["cf_fastpath"], step_dev=self.step_dev,
                             dt_dev=self.dt_dev)
         eng.material_update(st._e, st._Tr)
-        eng.comb_async(kw["Nmax"], 0, st._e, step_dev=self.step_dev, out_capacity=self.cap_census)
+        if self.mg:
+            self.rad_last.copy_(eng.si)
+            if self.fid.numel():
+                at_fid = eng.si.view(eng.ng, eng.nc).index_select(1, self.fid)
+                self.hist_Eg.index_copy_(0, self.k_dev, at_fid.view(1, -1))
+        eng.comb_async(self.nmax_top, 0, st._e, per_group=self.mg, step_dev=self.step_dev,
+                       out_capacity=self.cap_census, n_max_dev=self.nmax_dev)
         if self.conserve:
-            st._e.add_(eng.disc[: eng.nc] / eng.vol)
+            st._e.add_((eng.disc.view(eng.ng, eng.nc).sum(0) if self.mg else eng.disc[: eng.nc]) / eng.vol)
         Tn = evaluate(self.inv_eos, st.grid(st._e), _no_host, like)
         st._T.copy_(st.flat(Tn))
         # epilogue: summary, fiducial temperatures, output snapshots
@@ -142,6 +176,8 @@ class DeviceLoop:
         slot = torch.index_select(self.out_slot, 0, self.k_dev)
         self.snap_T.index_copy_(0, slot, st._T.view(1, -1))
         self.snap_Tr.index_copy_(0, slot, st._Tr.view(1, -1))
+        if self.mg:
+            self.snap_Eg.index_copy_(0, slot, self.rad_last.view(1, -1))
         self.k_dev.add_(1)
         # the comb wrote the next census into the spare bank: swap (sizes stay upper bounds)
         eng.spare.size = self.cap_census
@@ -171,6 +207,7 @@ class DeviceLoop:
         dev = self.eng.device
         self.dt_sched = torch.zeros(n, dtype=torch.float64, device=dev)
         self.step_sched = torch.zeros(n, dtype=torch.int32, device=dev)
+        self.nmax_sched = torch.zeros(n, dtype=torch.int64, device=dev)
         self.out_slot = torch.full((n,), n_out, dtype=torch.int64, device=dev)
         self.hist_sum = torch.zeros((n, ctypes.sizeof(_lib.ImcStepSummary)), dtype=torch.uint8, device=dev)
         nf = max(int(self.fid.numel()), 1)
@@ -178,6 +215,10 @@ class DeviceLoop:
         self.hist_Tr = torch.zeros((n, nf), dtype=torch.float64, device=dev)
         self.snap_T = torch.zeros((n_out + 1, self.eng.nc), dtype=torch.float64, device=dev)
         self.snap_Tr = torch.zeros_like(self.snap_T)
+        if self.mg:
+            ncg = self.eng.ng * self.eng.nc
+            self.hist_Eg = torch.zeros((n, self.eng.ng * nf), dtype=torch.float64, device=dev)
+            self.snap_Eg = torch.zeros((n_out + 1, ncg), dtype=torch.float64, device=dev)
         self._cap = (n, n_out)
         self._graphs = {}
 
@@ -198,6 +239,7 @@ class DeviceLoop:
         self._buffers(n, len(labels))
         self.dt_sched[:n].copy_(torch.as_tensor(np.asarray(dts, dtype=np.float64)))
         self.step_sched[:n].copy_(torch.arange(st.count, st.count + n, dtype=torch.int32))
+        self.nmax_sched[:n].copy_(torch.as_tensor(self._nmax_schedule(n), dtype=torch.int64))
         slots = np.full(n, self._cap[1], dtype=np.int64)  # the last row collects non-output steps
         for q, k in enumerate(outs):
             slots[int(k)] = q
@@ -205,14 +247,15 @@ class DeviceLoop:
         # size everything for the census bound before capture (no allocation in the graph)
         bound = int(eng.lib.imc_source_bound(ctypes.byref(eng.cmesh), ctypes.byref(eng._params(
             0, 1.0, 1.0, self.kw["Ntarget"], self.kw["Nboundary"], self.kw["Nsource"], self.faces, self.refl, 0,
-            True, 0.0))))
+            self.kw["rz_linear_source"], 0.0))))
         for b in (eng.bank, eng.spare):
             b.ensure(self.cap_census + bound)
         eng._ws(max(eng.bank.capacity, eng.spare.capacity))
         # evaluate the material callables once outside the capture (they may build device
         # tables on first use, which a capture cannot do)
         like = st.grid(st._T)
-        evaluate(self.sigma_a_func, like, _no_host, like)
+        for f in self.sigma_funcs:
+            evaluate(f, like, _no_host, like)
         evaluate(self.cv, like, _no_host, like)
         evaluate(self.inv_eos, st.grid(st._e), _no_host, like)
         eng._set_census_count(eng.bank.size)
@@ -232,6 +275,13 @@ class DeviceLoop:
         out = self._finish(dts, outs, labels)
         out["device_ms"] = e0.elapsed_time(e1)
         return out
+
+    def _nmax_schedule(self, n: int) -> list:
+        """Comb targets of the next n steps (MG_IMC2D 'Nmax_next': + Nmax_growth per step, capped
+        at Nmax_final)."""
+        n0, growth, final = self.nmax
+        out = [n0 + (self.k_done + k) * growth if growth else n0 for k in range(n)]
+        return [min(x, final) for x in out] if (growth and final is not None) else out
 
     def _finish(self, dts, outs, labels) -> dict:
         st, eng = self.state, self.eng
@@ -267,6 +317,7 @@ class DeviceLoop:
                                                "n_particles_transported": int(sm.n_bank)}})
             prev = total
         st.count += len(dts)
+        self.k_done += len(dts)
         st.previous_total_energy = prev
         eng.bank.size = int(steps[-1]["N_particles"])
         eng.spare.size = 0
@@ -279,8 +330,23 @@ class DeviceLoop:
         sT, sTr = self.snap_T.cpu(), self.snap_Tr.cpu()
         for q, label in enumerate(labels):
             snaps[label] = (st.grid(sT[q]).numpy().copy(), st.grid(sTr[q]).numpy().copy())
-        return {"times": times, "steps": steps, "fiducial_T": fid_T, "fiducial_Tr": fid_Tr, "snapshots": snaps,
-                "max_relative_closure": worst}
+        out = {"times": times, "steps": steps, "fiducial_T": fid_T, "fiducial_Tr": fid_Tr, "snapshots": snaps,
+               "max_relative_closure": worst}
+        if self.mg:
+            G, nf = eng.ng, int(self.fid.numel())
+            nx, ny = st._shape
+
+            def grid3(x):  # (G * nc) -> (G, nx, ny), energy density (si / c)
+                return (x.view(G, ny, nx).transpose(1, 2) / C_LIGHT).cpu().numpy().copy()
+
+            out["fiducial_Erad_by_group"] = self.hist_Eg[:n].cpu().numpy().reshape(n, G, -1)[:, :, :nf] / C_LIGHT
+            sE = self.snap_Eg
+            out["snapshots_Erad_by_group"] = {label: grid3(sE[q]) for q, label in enumerate(labels)}
+            object.__setattr__(st, "_rad_group", (self.rad_last / C_LIGHT).view(G, -1).clone())
+            st.__dict__["radiation_energy_by_group"] = grid3(self.rad_last)
+            st.__dict__["radiation_energy_by_group_postcomb"] = None
+            out["Nmax_next"] = self._nmax_schedule(1)[0]
+        return out
 
 
 def crooked_pipe_run(state, problem: dict, output_times, dt_initial=0.001, dt_max=10.0, growth=1.1,
@@ -310,3 +376,36 @@ def crooked_pipe_run(state, problem: dict, output_times, dt_initial=0.001, dt_ma
         fid[lbl] = [float(T0[i, j])] + list(res["fiducial_T"][:, q])
         fid_rad[lbl] = [float(Tr0[i, j])] + list(res["fiducial_Tr"][:, q])
     return times, fid, fid_rad, res["snapshots"], res
+
+
+def mg_crooked_pipe_run(state, problem: dict, output_times, fiducial_points=None, census_margin=1.25):
+    """The time loop of MG_IMC/problems/crooked_pipe_multigroup_imc.py on the device: dt from
+    the problem's dt_initial growing by dt_growth to dt_max and landing on the output times,
+    Nmax growing by Nmax_growth per step to Nmax_final, fiducial T / Tr / radiation spectra every
+    step, and T, Tr and the radiation energy by group at the output times.  problem: a
+    radtranbook_b200.problems.mg_crooked_pipe dict; state: its mg_imc2d state.  Returns
+    (times, fiducial_data, fiducial_data_rad, snapshots, result); snapshots[t] = (T, Tr, Erad_g)."""
+    e1, e2 = problem["edges1"], problem["edges2"]
+    rc, zc = 0.5 * (e1[:-1] + e1[1:]), 0.5 * (e2[:-1] + e2[1:])
+    pts = fiducial_points if fiducial_points is not None else problem["fiducials"]
+    cells = {lbl: (int(np.argmin(np.abs(rc - r))), int(np.argmin(np.abs(zc - z)))) for lbl, (r, z) in pts.items()}
+    sched, _ = adaptive_schedule(state.time, list(output_times), problem["dt_initial"], problem["dt_max"],
+                                 problem["dt_growth"])
+    loop = DeviceLoop(state, Ntarget=problem["Ntarget"], Nboundary=problem["Nboundary"], Nsource=0,
+                      Nmax=problem["Nmax"], T_boundary=problem["T_boundary"], sigma_a_func=problem["sigma_dev"],
+                      inv_eos=problem["inv_eos_dev"], cv=problem["cv_dev"], reflect=problem["reflect"],
+                      geometry="rz", max_events=1_000_000, boundary_source_func=problem["boundary_source_func"],
+                      T_emit_floor=problem["T_emit_floor"], fiducial_cells=list(cells.values()),
+                      census_margin=census_margin, Nmax_growth=problem["Nmax_growth"],
+                      Nmax_final=problem["Nmax_final"])
+    outputs = {k: tout for k, (_, tout) in enumerate(sched) if tout is not None}
+    T0, Tr0 = state.temperature.copy(), state.radiation_temperature.copy()
+    t_start = state.time
+    res = loop.run([dt for dt, _ in sched], outputs)
+    times = [t_start] + res["times"]
+    fid, fid_rad = {}, {}
+    for q, (lbl, (i, j)) in enumerate(cells.items()):
+        fid[lbl] = [float(T0[i, j])] + list(res["fiducial_T"][:, q])
+        fid_rad[lbl] = [float(Tr0[i, j])] + list(res["fiducial_Tr"][:, q])
+    snaps = {t: (T, Tr, res["snapshots_Erad_by_group"][t]) for t, (T, Tr) in res["snapshots"].items()}
+    return times, fid, fid_rad, snaps, res

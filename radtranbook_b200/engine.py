@@ -325,19 +325,23 @@ class Engine:
 
     def comb_async(self, n_max: int, step: int, e: torch.Tensor | None, per_group: bool = False,
                    conserve_radiation: bool = False, step_dev: torch.Tensor | None = None,
-                   out_capacity: int | None = None) -> None:
+                   out_capacity: int | None = None, n_max_dev: torch.Tensor | None = None) -> None:
         """Queue the comb (n_max semantics as comb()); fetch() completes it.  step_dev: device
-        step counter (graph replay); out_capacity: cap the combed census below the spare bank's
-        capacity (a larger one is flagged as an overflow and the census is emptied)."""
+        step counter (graph replay); n_max_dev: device int64 comb target read when the comb runs
+        (with step_dev; n_max > 0 then sizes the spare bank); out_capacity: cap the combed census
+        below the spare bank's capacity (a larger one is flagged as an overflow and the census
+        is emptied)."""
         self.spare.size = 0
         want = int(1.15 * n_max) if n_max > 0 else self._upper
         self.spare.ensure(want + 2 * self.nc * self.ng + 4096)
+        if n_max_dev is not None and (step_dev is None or n_max <= 0):
+            raise ValueError("n_max_dev needs step_dev and n_max > 0")
         self._comb_args = (int(n_max), int(step), e, _comb_flags(per_group, conserve_radiation), step_dev,
-                           out_capacity)
+                           out_capacity, n_max_dev)
         self._launch_comb()
 
     def _launch_comb(self) -> None:
-        n_max, step, e, flags, step_dev, out_capacity = self._comb_args
+        n_max, step, e, flags, step_dev, out_capacity, n_max_dev = self._comb_args
         cin = self.bank.c()
         cin.size = self._upper
         cout = self.spare.c()
@@ -346,7 +350,8 @@ class Engine:
         wsp, wsn = self._ws(max(self._upper, self.bank.capacity))
         if step_dev is not None:
             st = self.lib.imc_comb_async_dev(ctypes.byref(self.cmesh), ctypes.byref(cin), ctypes.byref(cout), n_max,
-                                             self.seed, step_dev.data_ptr(), flags, _ptr(self.disc), _ptr(e),
+                                             None if n_max_dev is None else n_max_dev.data_ptr(), self.seed,
+                                             step_dev.data_ptr(), flags, _ptr(self.disc), _ptr(e),
                                              wsp, wsn, self.summary_dev.data_ptr(), self._stream())
             _lib.check("imc_comb_async_dev", st)
             return
@@ -354,6 +359,18 @@ class Engine:
                                      self.seed, step & 0xFFFFFFFF, flags, _ptr(self.disc), _ptr(e),
                                      wsp, wsn, self.summary_dev.data_ptr(), self._stream())
         _lib.check("imc_comb_async", st)
+
+    def census_energy_async(self, out: torch.Tensor, per_group: bool = True) -> None:
+        """Queue, after comb_async, the energy per bin ((group, cell), or cell) of the comb's
+        output (the next census) into out; the entry count is read on the device.  A comb that
+        fetch() has to repeat (overflow) makes this stale: fetch() then sets comb_repeated."""
+        cb = self.spare.c()
+        cb.size = cb.capacity
+        off = ImcStepSummary.n_out.offset
+        st = self.lib.imc_bank_energy_by_bin(ctypes.byref(self.cmesh), ctypes.byref(cb),
+                                            self.summary_dev.data_ptr() + off, int(bool(per_group)), _ptr(out),
+                                            self._stream())
+        _lib.check("imc_bank_energy_by_bin", st)
 
     def fetch(self, host_copies=()) -> ImcStepSummary:
         """Copy the summary (and any (device, pinned host) pairs) to the host and synchronise.
@@ -366,6 +383,7 @@ class Engine:
         stream.synchronize()
         _lib.TRANSFER["d2h"] += self.summary_host.numel()
         sm = self.summary
+        self.comb_repeated = False
         if sm.flags & _lib.FLAG_NONFINITE:
             raise _lib.ImcError("imc_step_transport_async", 3)
         if sm.flags & _lib.FLAG_EVENT_CAP:
@@ -375,6 +393,7 @@ class Engine:
             off = ImcStepSummary.flags.offset
             self.summary_dev[off:off + 4].zero_()
             self._launch_comb()
+            self.comb_repeated = True
             self.summary_host.copy_(self.summary_dev, non_blocking=True)
             stream.synchronize()
             if sm.flags & _lib.FLAG_COMB_OVERFLOW:

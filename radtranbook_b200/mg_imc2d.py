@@ -145,6 +145,19 @@ def _rad_by_group(eng: Engine) -> torch.Tensor:
     return acc.view(G, nc) / eng.vol.view(1, nc)
 
 
+def _group_buffers(state, eng: Engine) -> dict:
+    """Device buffer for the post-comb energy by group and pinned host buffers for the
+    end-of-step copies of the by-group fields (allocated once per state)."""
+    hb = state.__dict__.get("_mg_hbuf")
+    if hb is None:
+        n = eng.ng * eng.nc
+        hb = {"post_dev": torch.zeros(n, dtype=torch.float64, device=eng.device)}
+        for k, m in (("pre", n), ("post", n), ("bnd", eng.ng), ("esc", eng.ng)):
+            hb[k] = torch.zeros(m, dtype=torch.float64, pin_memory=True)
+        object.__setattr__(state, "_mg_hbuf", hb)
+    return hb
+
+
 def _boundary_energy_estimate(geometry, e1, e2, Tb, dt, bsf) -> float:
     """Analytic boundary emission for the Ntotal split (MG_IMC/MG_IMC2D.py:1546-1632)."""
     E = 0.0
@@ -229,14 +242,19 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
         world = _allreduce.get_world_size()
         average_tallies(_allreduce, eng)
     eng.material_update(state._e, state._Tr)
-    rad_pre = (eng.si.view(G, nc) / C_LIGHT).clone()  # radiation energy density by group (path length)
+    rad_pre = eng.si.view(G, nc) / C_LIGHT  # radiation energy density by group (path length)
     eng.comb_async(Nmax, state.count, state._e, per_group=True)
+    hb = _group_buffers(state, eng)
+    eng.census_energy_async(hb["post_dev"], per_group=True)  # post-comb energy by (group, cell)
+    hb["post_dev"].view(G, nc).div_(eng.vol.view(1, nc))
     if conserve_comb_energy:
         state._e.add_(eng.disc.view(G, nc).sum(0) / eng.vol)
     Tn = evaluate(inv_eos, state.grid(state._e), lambda: _host_copy(state.grid(state._e)), like)
     state._T.copy_(state.flat(Tn))
+    group_copies = [(rad_pre.reshape(-1), hb["pre"]), (hb["post_dev"], hb["post"]),
+                    (eng.boundary_group, hb["bnd"]), (eng.escaped_group, hb["esc"])]
     try:
-        sm = eng.fetch(state.host_copies())
+        sm = eng.fetch(state.host_copies() + group_copies)
     except _lib.ImcError as ex:
         if ex.status == 3:
             raise AssertionError("non-finite or non-positive material state") from ex
@@ -252,7 +270,8 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
         state.refresh_host()
     else:
         state.take_host_copies()
-    rad_post = _rad_by_group(eng)
+    if eng.comb_repeated:  # the comb ran again after an overflow: rebuild from the new census
+        hb["post"].copy_(_rad_by_group(eng).reshape(-1))
     internal = float(sm.internal_energy)
     rad = float(sm.comb_after)
     comb_disc = float(sm.comb_before) - rad
@@ -270,18 +289,21 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
     state.previous_total_energy = total
     state.count += 1
 
-    def grid3(x):  # (G, nc) -> (G, nx, ny)
+    def grid3(h):  # pinned host (G * nc) -> (G, nx, ny)
         nx, ny = state._shape
-        return x.view(G, ny, nx).transpose(1, 2).cpu().numpy().copy()
+        return h.numpy().reshape(G, ny, nx).transpose(0, 2, 1).copy()
 
-    rad_group_pre = grid3(rad_pre)
-    rad_group_post = grid3(rad_post)
+    if not use_scalar_intensity_Tr:
+        hb["pre"].copy_(rad_pre.reshape(-1))
+    rad_group_pre = grid3(hb["pre"])
+    rad_group_post = grid3(hb["post"])
+    _lib.TRANSFER["d2h"] += 8 * (2 * G * nc + 2 * G)
     object.__setattr__(state, "_rad_group", rad_pre)
     state.__dict__["radiation_energy_by_group"] = rad_group_pre
     state.__dict__["radiation_energy_by_group_postcomb"] = rad_group_post
     stats = np.array(sm.stats[:], dtype=np.int64)
-    bnd_group = eng.boundary_group.cpu().numpy().copy()
-    esc_group = eng.escaped_group.cpu().numpy().copy()
+    bnd_group = hb["bnd"].numpy().copy()
+    esc_group = hb["esc"].numpy().copy()
     ms_src, ms_tr = eng.phase_times()
     t_end = _time.perf_counter()
     n_tr = int(sm.n_bank)

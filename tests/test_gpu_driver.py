@@ -89,3 +89,70 @@ def test_slab_device_loop(cuda):
     res = loop.run([mp["dt"]] * 3)
     np.testing.assert_allclose(st_b.temperature, st_a.temperature, rtol=1e-12, atol=0)
     assert res["steps"][-1]["N_particles"] == info["N_particles"] and res["device_ms"] > 0
+
+
+def test_mg_device_loop_matches_eager_steps(cuda):
+    """Multigroup crooked pipe (coarse mesh, 'quick' counts): the replayed graph with the
+    growing Nmax and per-group comb against eager mg_imc2d steps."""
+    from radtranbook_b200 import mg_imc2d
+
+    p = problems.mg_crooked_pipe(nr=30, nz=105, mode="quick")
+    e1, e2, ge = p["edges1"], p["edges2"], p["energy_edges"]
+    sched, _ = driver.adaptive_schedule(0.0, [4e-4, 1e-3], p["dt_initial"], p["dt_max"], 1.5)
+    dts = [dt for dt, _ in sched][:7]
+    assert len(dts) >= 6
+
+    def init():
+        return mg_imc2d.init_simulation(p["Ntarget"], p["Tinit"], p["Tr_init"], e1, e2, ge, p["eos_dev"],
+                                        p["inv_eos_dev"], T_emit_floor=p["T_emit_floor"], geometry="rz", seed=31)
+
+    a = init()
+    eager = []
+    for k, dt in enumerate(dts):
+        Nmax = min(p["Nmax"] + k * p["Nmax_growth"], p["Nmax_final"])
+        a, info = mg_imc2d.step(a, p["Ntarget"], p["Nboundary"], 0, Nmax, p["T_boundary"], dt, e1, e2, ge,
+                                p["sigma_dev"], p["inv_eos_dev"], p["cv_dev"], p["source"], reflect=p["reflect"],
+                                geometry="rz", boundary_source_func=p["boundary_source_func"],
+                                T_emit_floor=p["T_emit_floor"])
+        eager.append((info, a.temperature.copy()))
+    b = init()
+    cells = [(0, 2), (3, 10), (12, 40)]
+    loop = driver.DeviceLoop(b, Ntarget=p["Ntarget"], Nboundary=p["Nboundary"], Nsource=0, Nmax=p["Nmax"],
+                             T_boundary=p["T_boundary"], sigma_a_func=p["sigma_dev"], inv_eos=p["inv_eos_dev"],
+                             cv=p["cv_dev"], reflect=p["reflect"], geometry="rz", max_events=1_000_000,
+                             boundary_source_func=p["boundary_source_func"], T_emit_floor=p["T_emit_floor"],
+                             fiducial_cells=cells, Nmax_growth=p["Nmax_growth"], Nmax_final=p["Nmax_final"])
+    res = loop.run(dts[:4], {1: "after-2"})
+    res2 = loop.run(dts[4:])  # the Nmax schedule continues across calls
+    assert res["max_relative_closure"] < 1e-12 and res2["max_relative_closure"] < 1e-12
+    steps = res["steps"] + res2["steps"]
+    fid_Eg = np.concatenate([res["fiducial_Erad_by_group"], res2["fiducial_Erad_by_group"]])
+    for k, (info, T) in enumerate(eager):
+        assert steps[k]["N_particles"] == info["N_particles"], k
+        np.testing.assert_allclose(steps[k]["total_energy"], info["total_energy"], rtol=1e-12)
+        Eg = info["radiation_energy_by_group"]
+        np.testing.assert_allclose(fid_Eg[k], np.stack([Eg[:, i, j] for i, j in cells], axis=1), rtol=1e-12,
+                                   atol=1e-300)
+    np.testing.assert_allclose(b.temperature, a.temperature, rtol=1e-12, atol=0)
+    np.testing.assert_allclose(b.radiation_energy_by_group, a.radiation_energy_by_group, rtol=1e-12, atol=1e-300)
+    np.testing.assert_allclose(res["snapshots_Erad_by_group"]["after-2"], eager[1][0]["radiation_energy_by_group"],
+                               rtol=1e-12, atol=1e-300)
+    assert res2["Nmax_next"] == min(p["Nmax"] + len(dts) * p["Nmax_growth"], p["Nmax_final"])
+    assert b.count == a.count
+
+
+def test_mg_crooked_pipe_driver_hits_output_times(cuda):
+    from radtranbook_b200 import mg_imc2d
+
+    p = problems.mg_crooked_pipe(nr=30, nz=105, mode="quick")
+    st = mg_imc2d.init_simulation(p["Ntarget"], p["Tinit"], p["Tr_init"], p["edges1"], p["edges2"],
+                                  p["energy_edges"], p["eos_dev"], p["inv_eos_dev"], T_emit_floor=p["T_emit_floor"],
+                                  geometry="rz", seed=8)
+    times, fid, fid_rad, snaps, res = driver.mg_crooked_pipe_run(st, p, [5e-4, 2e-3])
+    assert set(snaps) == {5e-4, 2e-3}
+    assert any(abs(t - 5e-4) < 1e-12 for t in times) and abs(times[-1] - 2e-3) < 1e-12
+    assert all(len(v) == len(times) for v in fid.values()) and len(fid) == 5
+    assert res["max_relative_closure"] < 1e-12
+    T, Tr, Eg = snaps[2e-3]
+    np.testing.assert_allclose(T, st.temperature, rtol=0)
+    assert Eg.shape == (10, 30, 105) and (Eg >= 0).all() and Eg[:, :3, :3].sum() > 0
