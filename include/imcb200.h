@@ -118,7 +118,7 @@ typedef struct imc_step_params {
   int32_t block_size;           /* tracking launch shape; 0 = tuned default */
   int32_t blocks_per_sm;
   int32_t chunk;                /* histories claimed per warp ticket (guided: at most this) */
-  int32_t reserved;             /* bit 0: shared-memory cell table; bit 1: draw prefetch */
+  int32_t reserved;             /* bit 0: shared-memory cell table (other bits ignored) */
   const double* emission_fractions; /* MG: [g] fixed emission spectrum, or NULL = Planck */
   int64_t n_boundary_side[4];   /* > 0: boundary particles on that side instead of n_boundary
                                    (per-side budgets, MG_IMC/MG_IMC1D.py:1000-1040) */

@@ -6,8 +6,6 @@ ticket and refill finished lanes at every event boundary.  Its speed depends on:
   blocks_per_sm  resident blocks requested per SM (grid = blocks_per_sm x SMs)
   chunk          histories claimed per warp ticket (refill cadence / bank tile)
   smem_cells     stage the per-cell (sigma_a, sigma_s) table in shared memory
-  prefetch       draw the next event's Philox numbers one event ahead (more registers,
-                 more instruction-level parallelism)
 The tuner replays the engine's last transport on a snapshot of the census bank for every
 candidate (the Philox streams make each trial the identical work), times the tracking
 phase with CUDA events, restores the census and installs the fastest shape.
@@ -25,7 +23,6 @@ DEFAULT_GRID = {
     "blocks_per_sm": (4, 8),
     "chunk": (512, 1024, 2048, 4096, 8192),
     "smem_cells": (0, 1),
-    "prefetch": (0, 1),
 }
 
 

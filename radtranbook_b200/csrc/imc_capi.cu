@@ -326,9 +326,8 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   ta.dep_fx = dep_fx; ta.esc_fx = esc_fx;
   const int block = par->block_size > 0 ? par->block_size : 256;
   const int bps = par->blocks_per_sm > 0 ? par->blocks_per_sm : 3;
-  // reserved: bit 0 = stage the cell table in shared memory, bit 1 = prefetch the next draw
+  // reserved: bit 0 = stage the cell table in shared memory
   const bool smem_cells = (par->reserved & 1) ? true : ((long long)nc * ng <= 4096);
-  const bool prefetch = (par->reserved & 2) != 0;
   if (adj) {
     AdjointArgs A = *adj;
     A.t = ta; A.sa64 = tal->sigma_a; A.ss64 = tal->sigma_s; A.sig64 = mat->sigma;
@@ -336,7 +335,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     if (pe.ok) { IMC_CUDA(cudaEventRecord(pe.e[2], s)); pe.recorded = true; }
     return IMC_OK;
   }
-  IMC_CUDA(imc_launch_track(ta, mesh->geometry, block, sm_count() * bps, smem_cells, prefetch, s));
+  IMC_CUDA(imc_launch_track(ta, mesh->geometry, block, sm_count() * bps, smem_cells, s));
   if (pe.ok) { IMC_CUDA(cudaEventRecord(pe.e[2], s)); pe.recorded = true; }
   IMC_CUDA(imc_launch_tally_finalize(ta, s));
   return IMC_OK;

@@ -48,8 +48,7 @@ struct TrackArgs {
   const uint32_t* step_dev;  // non-NULL: the Philox step counter is read from device memory
 };
 
-cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool smem_cells, bool prefetch,
-                             cudaStream_t s);
+cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool smem_cells, cudaStream_t s);
 // dep = fixed-point deposition / V, escaped (and escaped_group) from their fixed-point sums
 cudaError_t imc_launch_tally_finalize(const TrackArgs& a, cudaStream_t s);
 

@@ -37,7 +37,7 @@ enum : int { B_CENSUS = 0, B_FLOOR, B_REFLECT, B_CAP, B_ESCAPE, B_CAPTURE, B_N }
 // photon is re-emitted in the new direction the event drew after a delay ~ Exp(cf_rate) if that
 // falls inside the step, else captured (its weight deposited).  Histories at or below the
 // weight floor are not moved (they stay in census).
-template <int GEOM, bool SMEM_CELLS, bool PREFETCH, bool MG, bool CF>
+template <int GEOM, bool SMEM_CELLS, bool MG, bool CF>
 __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   const float dtk = a.dt_dev ? (float)*a.dt_dev : a.dt;  // graph replay: step length and Philox
   const uint32_t stepk = a.step_dev ? *a.step_dev : a.step;  // step counter from device memory
@@ -71,9 +71,12 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   // lane state
   bool has = false;
   uint32_t pid = 0, ev = 0;
-  U4 rnext{0u, 0u, 0u, 0u};  // PREFETCH: the next event's draw, computed one event ahead
   float x = 0, y = 0, u = 0, v = 0, w = 0, dcen = 0;
   int ci = 0, cj = 0, grp = 0;
+  // (sigma_a, sigma_s) of the current (group, cell), loaded as soon as the cell is known (at
+  // refill, after a crossing) so the load overlaps the tally flush and refill of the loop end
+  float2 tab = make_float2(0.f, 0.f);
+  auto table = [&](int cq) { return SMEM_CELLS ? CS[cq] : __ldg(a.sass + cq); };
   double acc_lost = 0.0, acc_wd = 0.0;  // energy removed / w*s in the current cell
   unsigned s_bd = 0, s_sc = 0;          // per-event counters (census/cap counted at finish)
 
@@ -116,8 +119,8 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
           if (GEOM == G_XY || GEOM == G_RZ) { y = a.p2[pid]; v = a.d2[pid]; }
           const int c = a.cell[pid];
           cj = c / a.nx; ci = c - cj * a.nx;
+          tab = table(MG ? c + a.nc * grp : c);
           ev = 0;
-          if (PREFETCH) rnext = draw(a.seed, pid, 0u, stepk, TAG_TRANSPORT);
           has = true;
         }
       }
@@ -132,9 +135,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
     if (has) {
       const int c = ci + a.nx * cj;
       const int cq = MG ? c + a.nc * grp : c;  // (group, cell) table / tally index
-      float sa, ss;
-      if (SMEM_CELLS) { const float2 q = CS[cq]; sa = q.x; ss = q.y; }
-      else { const float2 q = __ldg(a.sass + cq); sa = q.x; ss = q.y; }
+      const float sa = tab.x, ss = tab.y;
       bool finished = false, frozen = false;
       if (ev >= (uint32_t)a.max_events) {
         // events-per-history cap (IMC/IMC2D.py:974-977): stops, weight stays in census
@@ -142,15 +143,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
         if (!a.cap_is_reference) atomicOr(a.flags, (int)IMC_FLAG_EVENT_CAP);
         finished = true;
       } else {
-        U4 r;
-        if (PREFETCH) {
-          // this event's numbers were drawn during the previous event; draw the next now so
-          // its dependent multiply chain overlaps this event's geometry
-          r = rnext;
-          rnext = draw(a.seed, pid, ev + 1u, stepk, TAG_TRANSPORT);
-        } else {
-          r = draw(a.seed, pid, ev, stepk, TAG_TRANSPORT);
-        }
+        const U4 r = draw(a.seed, pid, ev, stepk, TAG_TRANSPORT);
         ++ev;
         float d, sb, L, xn = x, yn = y, un = u, vn = v;
         int evt, cross = X_NONE;
@@ -331,6 +324,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
               }
             }
             ci = ni; cj = nj;
+            if (!finished) tab = table(MG ? ci + a.nx * cj + a.nc * grp : ci + a.nx * cj);
           }
           if (GEOM == G_SLAB || GEOM == G_SPHERE) {
             if (!CF && !finished && w < weight_floor) {
@@ -409,23 +403,22 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   if (threadIdx.x < 4 && blk_esc[threadIdx.x] != 0ull) atomicAdd(a.esc_fx + threadIdx.x, blk_esc[threadIdx.x]);
 }
 
-template <int GEOM, bool SM, bool PF, bool MG, bool CF>
+template <int GEOM, bool SM, bool MG, bool CF>
 cudaError_t launch_one(const TrackArgs& a, int block, int grid, cudaStream_t s) {
   const int nwarps = block / 32;
   size_t sh = nwarps * sizeof(WarpStage) + sizeof(float) * (a.nx + a.ny + 4);
   if (SM) sh += sizeof(float2) * a.nc * a.ng;
   if (sh > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_track<GEOM, SM, PF, MG, CF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+    cudaError_t e = cudaFuncSetAttribute(k_track<GEOM, SM, MG, CF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
     if (e != cudaSuccess) return e;
   }
-  k_track<GEOM, SM, PF, MG, CF><<<grid, block, sh, s>>>(a);
+  k_track<GEOM, SM, MG, CF><<<grid, block, sh, s>>>(a);
   return cudaGetLastError();
 }
 
 template <int GEOM, bool MG, bool CF = false>
-cudaError_t launch_geom(const TrackArgs& a, int block, int grid, bool sm, bool pf, cudaStream_t s) {
-  if (sm) return pf ? launch_one<GEOM, true, true, MG, CF>(a, block, grid, s) : launch_one<GEOM, true, false, MG, CF>(a, block, grid, s);
-  return pf ? launch_one<GEOM, false, true, MG, CF>(a, block, grid, s) : launch_one<GEOM, false, false, MG, CF>(a, block, grid, s);
+cudaError_t launch_geom(const TrackArgs& a, int block, int grid, bool sm, cudaStream_t s) {
+  return sm ? launch_one<GEOM, true, MG, CF>(a, block, grid, s) : launch_one<GEOM, false, MG, CF>(a, block, grid, s);
 }
 
 // Fixed-point tallies to the FP64 outputs: deposition per unit volume per (group, cell),
@@ -448,30 +441,30 @@ cudaError_t imc_launch_tally_finalize(const TrackArgs& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool sm, bool pf, cudaStream_t s) {
+cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool sm, cudaStream_t s) {
   ++g_imc_launches;
   if (a.ng > 1) {  // multigroup: 2-D (MG_IMC/MG_IMC2D.py) and the 1-D sphere (MG_IMC/MG_IMC1D.py)
     switch (geom) {
-      case G_SPHERE: return launch_geom<G_SPHERE, true>(a, block, grid, sm, pf, s);
-      case G_XY: return launch_geom<G_XY, true>(a, block, grid, sm, pf, s);
-      case G_RZ: return launch_geom<G_RZ, true>(a, block, grid, sm, pf, s);
+      case G_SPHERE: return launch_geom<G_SPHERE, true>(a, block, grid, sm, s);
+      case G_XY: return launch_geom<G_XY, true>(a, block, grid, sm, s);
+      case G_RZ: return launch_geom<G_RZ, true>(a, block, grid, sm, s);
       default: return cudaErrorInvalidValue;
     }
   }
   if (a.cf_rate) {  // Carter-Forest, gray
     switch (geom) {
-      case G_SLAB: return launch_geom<G_SLAB, false, true>(a, block, grid, sm, pf, s);
-      case G_SPHERE: return launch_geom<G_SPHERE, false, true>(a, block, grid, sm, pf, s);
-      case G_XY: return launch_geom<G_XY, false, true>(a, block, grid, sm, pf, s);
-      case G_RZ: return launch_geom<G_RZ, false, true>(a, block, grid, sm, pf, s);
+      case G_SLAB: return launch_geom<G_SLAB, false, true>(a, block, grid, sm, s);
+      case G_SPHERE: return launch_geom<G_SPHERE, false, true>(a, block, grid, sm, s);
+      case G_XY: return launch_geom<G_XY, false, true>(a, block, grid, sm, s);
+      case G_RZ: return launch_geom<G_RZ, false, true>(a, block, grid, sm, s);
       default: return cudaErrorInvalidValue;
     }
   }
   switch (geom) {
-    case G_SLAB: return launch_geom<G_SLAB, false>(a, block, grid, sm, pf, s);
-    case G_SPHERE: return launch_geom<G_SPHERE, false>(a, block, grid, sm, pf, s);
-    case G_XY: return launch_geom<G_XY, false>(a, block, grid, sm, pf, s);
-    case G_RZ: return launch_geom<G_RZ, false>(a, block, grid, sm, pf, s);
+    case G_SLAB: return launch_geom<G_SLAB, false>(a, block, grid, sm, s);
+    case G_SPHERE: return launch_geom<G_SPHERE, false>(a, block, grid, sm, s);
+    case G_XY: return launch_geom<G_XY, false>(a, block, grid, sm, s);
+    case G_RZ: return launch_geom<G_RZ, false>(a, block, grid, sm, s);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -155,7 +155,7 @@ class Engine:
         self.bank = Bank(capacity, dev, mg)
         self.spare = Bank(capacity, dev, mg)
         self.ws = torch.empty(0, dtype=torch.uint8, device=dev)
-        self.launch = dict(block_size=256, blocks_per_sm=4, chunk=512, smem_cells=0, prefetch=0)
+        self.launch = dict(block_size=256, blocks_per_sm=4, chunk=512, smem_cells=0)
         self._last_transport = None
 
     # ------------------------------------------------------------------ helpers
@@ -280,7 +280,7 @@ class Engine:
         par.block_size = int(self.launch["block_size"])
         par.blocks_per_sm = int(self.launch["blocks_per_sm"])
         par.chunk = int(self.launch["chunk"])
-        par.reserved = int(bool(self.launch.get("smem_cells", 0))) | (int(bool(self.launch.get("prefetch", 0))) << 1)
+        par.reserved = int(bool(self.launch.get("smem_cells", 0)))
         par.emission_fractions = _ptr(self.emission_fractions)
         for q, n in enumerate(n_boundary_side or ()):
             par.n_boundary_side[q] = int(n)
