@@ -548,7 +548,13 @@ def run_ours(args, rank: int, world: int):
     state, _, _, _ = _gpu_steps(p, state, args.warmup, True, dist)
     eng = state._engine
     tuned = None
-    if not args.no_tune:
+    if args.launch:
+        # a fixed launch shape (block, blocks per SM, chunk, smem cells), e.g. the tuner's choice
+        b, bps, ch, sm = (int(x) for x in args.launch.split(","))
+        eng.launch.update(block_size=b, blocks_per_sm=bps, chunk=ch, smem_cells=sm)
+        launch_shape = dict(eng.launch)
+        tuned = {"best_ms": None, "worst_ms": None, "trials": [], "fixed": args.launch}
+    elif not args.no_tune:
         tuned = imc2d.tune(state)
         launch_shape = dict(eng.launch)
         if args.tune_log:
@@ -663,6 +669,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--launch", default=None,
+                    help="fixed tracking launch shape 'block,blocks_per_sm,chunk,smem_cells' instead of tuning")
     ap.add_argument("--tune-log", default=None, help="write the autotuner's trials to this JSON file")
     ap.add_argument("--no-forms", action="store_true", help="skip the batched and adjoint forms")
     ap.add_argument("--batch-steps", type=int, default=4)
