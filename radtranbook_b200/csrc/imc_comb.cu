@@ -79,8 +79,9 @@ __global__ void __launch_bounds__(CB) k_comb_count(CombArgs a) {
   int n = 0, b = 0;
   if (k < n_in) {
     const float wf = a.w[k];
+    const int bk = bin_of(a, k);  // loaded with the weight (k < n_in: in bounds)
     if (wf > 0.f) {
-      b = bin_of(a, k);
+      b = bk;
       const double ew = a.ew[b];
       if (compact) {
         n = 1;

@@ -21,14 +21,29 @@ using namespace imcsample;
 
 namespace {
 
+// Offsets sampled into shared memory for the first levels of the particle -> bin search.
+constexpr int kOffSamples = 1024;
+
 __global__ void k_fill_volume(FillArgs a) {
   const double time_scale = a.time_scale_dev ? *a.time_scale_dev : a.time_scale;  // graph replay
   const uint32_t step = a.step_dev ? *a.step_dev : a.step;
   const long long stride = (long long)gridDim.x * blockDim.x;
   const long long n = *a.d_n, base = *a.d_base;
+  // s_off[q] = off[min((q + 1) * span, nbins)]: the search for the bin of particle k (the
+  // smallest o with off[o + 1] > k) first finds its span of `span` bins in shared memory,
+  // then bisects the span in global memory.
+  __shared__ long long s_off[kOffSamples];
+  const int nbins = a.nbins;
+  if (nbins <= 0) return;  // uniform across the grid
+  const int span = (nbins + kOffSamples - 1) / kOffSamples;
+  const int m = (nbins + span - 1) / span;
+  for (int q = threadIdx.x; q < m; q += blockDim.x) s_off[q] = a.off[min((q + 1) * span, nbins)];
+  __syncthreads();
   for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
-    // order position o with off[o] <= k < off[o+1]
-    int lo = 0, hi = a.nbins;  // search in off[0..nbins]
+    // order position o with off[o] <= k < off[o+1] (k < n = off[nbins], so o < nbins)
+    int qlo = 0, qhi = m - 1;
+    while (qlo < qhi) { const int mid = (qlo + qhi) >> 1; if (s_off[mid] > k) qhi = mid; else qlo = mid + 1; }
+    int lo = qlo * span, hi = min(lo + span, nbins) - 1;
     while (lo < hi) { const int mid = (lo + hi) >> 1; if (a.off[mid + 1] <= k) lo = mid + 1; else hi = mid; }
     const int o = lo;
     const int g = a.bins_by_group ? o / a.nc : 0;  // MG 1-D bins b = g*nc + c
