@@ -38,7 +38,7 @@ import torch
 from . import _lib
 from ._gray import face_temperatures
 from .engine import C_LIGHT
-from .materials import evaluate, is_device
+from .materials import GroupedOpacity, evaluate, evaluate_groups, is_device
 
 
 def adaptive_schedule(t0: float, output_times, dt_initial: float, dt_max: float, growth: float, saved=()):
@@ -90,7 +90,8 @@ class DeviceLoop:
         self.eng = eng
         dev = eng.device
         self.mg = eng.ng > 1
-        funcs = list(sigma_a_func) if self.mg else [sigma_a_func]
+        funcs = (sigma_a_func if isinstance(sigma_a_func, GroupedOpacity) else list(sigma_a_func)) if self.mg \
+            else [sigma_a_func]
         if self.mg and (len(funcs) != eng.ng or state._dim != 2):
             raise ValueError("a multigroup device loop needs a 2-D state and one opacity callable per group")
         for f in (*funcs, inv_eos, cv):
@@ -147,7 +148,7 @@ class DeviceLoop:
         torch.index_select(self.step_sched, 0, self.k_dev, out=self.step_dev)
         torch.index_select(self.nmax_sched, 0, self.k_dev, out=self.nmax_dev)
         like = st.grid(st._T)
-        sigma = torch.cat([st.flat(evaluate(f, like, _no_host, like)).reshape(-1) for f in self.sigma_funcs]) \
+        sigma = evaluate_groups(self.sigma_funcs, like, _no_host, like).transpose(1, 2).reshape(-1) \
             if self.mg else st.flat(evaluate(self.sigma_funcs[0], like, _no_host, like))
         cvv = st.flat(evaluate(self.cv, like, _no_host, like))
         # the host-side step and dt are placeholders: the kernels read step_dev / dt_dev
@@ -254,6 +255,8 @@ class DeviceLoop:
         # evaluate the material callables once outside the capture (they may build device
         # tables on first use, which a capture cannot do)
         like = st.grid(st._T)
+        if self.mg:
+            evaluate_groups(self.sigma_funcs, like, _no_host, like)
         for f in self.sigma_funcs:
             evaluate(f, like, _no_host, like)
         evaluate(self.cv, like, _no_host, like)

@@ -90,3 +90,23 @@ class LinearEOS:
         self.eos = device_callable(lambda T: self.cv(T) * T)
         self.inv_eos = device_callable(lambda e: e / self.cv(e))
         self.cv_func = self.cv
+
+
+class GroupedOpacity(list):
+    """The per-group opacity callables of a multigroup problem (a list, as MG_IMC2D.step
+    takes) together with one device function that evaluates every group at once:
+    all_groups(T) -> (G, *T.shape).  The multigroup steps call all_groups (one fused
+    expression instead of G small ones); iterating gives the per-group callables, which
+    must compute the same numbers."""
+
+    def __init__(self, funcs, all_groups):
+        super().__init__(funcs)
+        self.all_groups = all_groups
+
+
+def evaluate_groups(funcs, T_dev: torch.Tensor, T_host_fn, like: torch.Tensor) -> torch.Tensor:
+    """Every group's opacity on the temperature field, (G, *like.shape) float64 on the device."""
+    if isinstance(funcs, GroupedOpacity):
+        out = funcs.all_groups(T_dev)
+        return torch.broadcast_to(out.to(like.device, torch.float64), (len(funcs),) + tuple(like.shape))
+    return torch.stack([evaluate(f, T_dev, T_host_fn, like) for f in funcs])

@@ -28,7 +28,7 @@ import torch
 from . import _lib
 from ._gray import GrayState, _host_copy, average_tallies, face_temperatures, replica_mean
 from .engine import A_RAD, C_LIGHT, Engine
-from .materials import evaluate
+from .materials import evaluate, evaluate_groups
 from .mg_imc2d import planck_fractions
 
 __c = 29.98
@@ -142,7 +142,7 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, mesh, energy_
     mode = _comb_mode(conserve_comb_energy)
     like = state._T
     host_T = lambda: state.temperature  # noqa: E731
-    sig = torch.stack([evaluate(f, like, host_T, like) for f in sigma_a_funcs])  # (G, I)
+    sig = evaluate_groups(sigma_a_funcs, like, host_T, like)  # (G, I)
     cvv = evaluate(cv, like, host_T, like)
     Tb = [T_boundary[q](state.time) if callable(T_boundary[q]) else T_boundary[q] for q in range(2)]
     n_side = None

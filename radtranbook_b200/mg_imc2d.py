@@ -26,7 +26,7 @@ import torch
 from . import _lib
 from ._gray import GrayState, _host_copy, average_tallies, face_temperatures, replica_mean
 from .engine import A_RAD, C_LIGHT, Engine
-from .materials import evaluate
+from .materials import evaluate, evaluate_groups
 
 __c = 29.98
 __a = 0.01372
@@ -190,7 +190,7 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
     G, nc = eng.ng, eng.nc
     like = state.grid(state._T)
     host_T = lambda: state.temperature  # noqa: E731
-    sig = torch.stack([state.flat(evaluate(f, like, host_T, like)) for f in sigma_a_funcs])  # (G, nc)
+    sig = evaluate_groups(sigma_a_funcs, like, host_T, like).transpose(1, 2).reshape(G, -1)  # (G, nc), flat order
     cvv = state.flat(evaluate(cv, like, host_T, like))
     if emission_fractions is not None:
         eng.emission_fractions = torch.as_tensor(np.asarray(emission_fractions, dtype=np.float64), device=eng.device)

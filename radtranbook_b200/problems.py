@@ -19,7 +19,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from .materials import device_callable
+from .materials import GroupedOpacity, device_callable
 
 
 def marshak_slab(scale: float = 1.0) -> dict:
@@ -161,6 +161,16 @@ def mg_crooked_pipe(n_groups: int = 10, nr: int = 60, nz: int = 210, mode: str =
         return host, device
 
     ops = [opacity(g) for g in range(n_groups)]
+    inv3 = [(float(edges[g]) ** -3, float(edges[g + 1]) ** -3) for g in range(n_groups)]
+
+    def all_groups(T):  # every group in one expression, the same arithmetic as each callable
+        key = ("inv3", T.device)
+        if key not in cache:
+            t = torch.tensor(inv3, dtype=torch.float64, device=T.device)
+            cache[key] = (t[:, 0].view(-1, 1, 1).contiguous(), t[:, 1].view(-1, 1, 1).contiguous())
+        lo3, hi3 = cache[key]
+        s = 10.0 * dev(rho, T) * torch.pow(torch.clamp(T, min=1e-2), -0.5)
+        return torch.sqrt(torch.clamp(s * lo3, max=1e14) * torch.clamp(s * hi3, max=1e14))
     presets = {"quick": (20_000, 20_000, 100_000, 10_000, 500_000),
                "standard": (200_000, 200_000, 1_000_000, 50_000, 5_000_000)}
     nt, nb, nmax, ngrow, nfin = presets[mode]
@@ -172,7 +182,7 @@ def mg_crooked_pipe(n_groups: int = 10, nr: int = 60, nz: int = 210, mode: str =
         name=f"2-D RZ multigroup crooked pipe ({nr}x{nz}, {n_groups} groups)",
         geometry="rz", dim=2, edges1=r_edges, edges2=z_edges, energy_edges=edges, rho=rho,
         Tinit=np.full((nr, nz), 0.05), Tr_init=np.full((nr, nz), 0.05),
-        sigma_host=[h for h, _ in ops], sigma_dev=[d for _, d in ops],
+        sigma_host=[h for h, _ in ops], sigma_dev=GroupedOpacity([d for _, d in ops], all_groups),
         cv_host=lambda T: cvg.copy(), cv_dev=device_callable(lambda T: dev(cvg, T)),
         eos_host=lambda T: cvg * T, inv_eos_host=lambda e: e / cvg,
         eos_dev=device_callable(lambda T: dev(cvg, T) * T), inv_eos_dev=device_callable(lambda e: e / dev(cvg, e)),
