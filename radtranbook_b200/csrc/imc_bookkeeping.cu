@@ -258,20 +258,25 @@ __global__ void k_material(MatArgs a) {
   a.tr[c] = x > 0.0 ? sqrt(sqrt(x)) : 0.0;
 }
 
+// Single block: the canonical total of the census energy and the comb mode.
 __global__ void __launch_bounds__(NT) k_comb_plan(CombPlanArgs a) {
   __shared__ double red[NT];
   const double E = block_canon_sum(a.ecen, a.nb, red);
   // MG_IMC/MG_IMC1D.py:1194-1200: Nmax = 0 never combs; Nmax < 0 combs once |Nmax| entries live
   const bool compact = a.force_compact || (a.threshold > 0 && (long long)*a.n_live < a.threshold);
-  if (threadIdx.x == 0) *a.mode = compact ? 1 : 0;
+  if (threadIdx.x == 0) { *a.mode = compact ? 1 : 0; a.sum->comb_before = E; }
+}
+
+// Wide: the comb weight of every bin, ecen / max(1, rint(Nmax ecen / E)).
+__global__ void k_comb_weights(CombPlanArgs a) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= a.nb) return;
+  const double E = a.sum->comb_before;
   const long long n_max = a.n_max_dev ? (long long)*a.n_max_dev : a.n_max;
-  for (int b = threadIdx.x; b < a.nb; b += NT) {
-    const double ec = a.ecen[b];
-    double ew = 0.0;
-    if (E > 0.0 && ec > 0.0) ew = ec / fmax(1.0, rint((double)n_max * ec / E));
-    a.ew[b] = ew;
-  }
-  if (threadIdx.x == 0) a.sum->comb_before = E;
+  const double ec = a.ecen[b];
+  double ew = 0.0;
+  if (E > 0.0 && ec > 0.0) ew = ec / fmax(1.0, rint((double)n_max * ec / E));
+  a.ew[b] = ew;
 }
 
 __global__ void __launch_bounds__(NT) k_canon_eV(const double* e, const double* vol, int nc, double* out) {
@@ -304,8 +309,9 @@ cudaError_t imc_launch_material(const MatArgs& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 cudaError_t imc_launch_comb_plan(const CombPlanArgs& a, cudaStream_t s) {
-  ++g_imc_launches;
+  g_imc_launches += 2;
   k_comb_plan<<<1, NT, 0, s>>>(a);
+  if (a.nb > 0) k_comb_weights<<<(a.nb + 255) / 256, 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 cudaError_t imc_launch_canon_sum_eV(const double* e, const double* vol, int nc, double* out, cudaStream_t s) {
@@ -333,30 +339,41 @@ __device__ double planck_tail(double x) {
   return tail;
 }
 
-__device__ double planck_F(double x) {
-  const double c = 15.0 / (PI * PI * PI * PI);
-  if (!(x > 0.0)) return 0.0;
-  if (x < 1.0) {
-    const double B[21] = {1.0, -0.5, 1.0 / 6.0, 0.0, -1.0 / 30.0, 0.0, 1.0 / 42.0, 0.0, -1.0 / 30.0, 0.0,
-                          5.0 / 66.0, 0.0, -691.0 / 2730.0, 0.0, 7.0 / 6.0, 0.0, -3617.0 / 510.0, 0.0,
-                          43867.0 / 798.0, 0.0, -174611.0 / 330.0};
-    double sum = 0.0, xp = x * x * x, fact = 1.0;
-    for (int n = 0; n <= 20; ++n) {
-      if (n > 0) fact *= n;
-      if (B[n] != 0.0) sum += B[n] * xp / ((n + 3) * fact);
-      xp *= x;
-    }
-    return c * sum;
+// Bernoulli series of (pi^4/15) F(x) for 0 < x < 1
+__device__ double planck_series(double x) {
+  const double B[21] = {1.0, -0.5, 1.0 / 6.0, 0.0, -1.0 / 30.0, 0.0, 1.0 / 42.0, 0.0, -1.0 / 30.0, 0.0,
+                        5.0 / 66.0, 0.0, -691.0 / 2730.0, 0.0, 7.0 / 6.0, 0.0, -3617.0 / 510.0, 0.0,
+                        43867.0 / 798.0, 0.0, -174611.0 / 330.0};
+  double sum = 0.0, xp = x * x * x, fact = 1.0;
+  for (int n = 0; n <= 20; ++n) {
+    if (n > 0) fact *= n;
+    if (B[n] != 0.0) sum += B[n] * xp / ((n + 3) * fact);
+    xp *= x;
   }
-  return 1.0 - c * planck_tail(x);
+  return sum;
+}
+
+// One group edge x = E/T with its series (0 < x < 1) or tail (x >= 1) value, evaluated once
+// and shared by the two groups the edge bounds.
+struct PlanckEdge { double x, s; };
+
+__device__ PlanckEdge planck_edge(double x) {
+  if (!(x > 0.0)) return PlanckEdge{x, 0.0};
+  return PlanckEdge{x, x < 1.0 ? planck_series(x) : planck_tail(x)};
+}
+
+__device__ double planck_F(const PlanckEdge& e) {
+  const double c = 15.0 / (PI * PI * PI * PI);
+  if (!(e.x > 0.0)) return 0.0;
+  return e.x < 1.0 ? c * e.s : 1.0 - c * e.s;
 }
 
 // F(x1) - F(x0); above x = 1 as a difference of tails, which keeps its relative precision
 // far into the Wien tail (1 - F cancels to 0 there)
-__device__ double planck_frac(double x0, double x1) {
-  if (!(x1 > x0)) return 0.0;
-  if (x0 >= 1.0) return 15.0 / (PI * PI * PI * PI) * (planck_tail(x0) - planck_tail(x1));
-  return planck_F(x1) - planck_F(x0);
+__device__ double planck_frac(const PlanckEdge& e0, const PlanckEdge& e1) {
+  if (!(e1.x > e0.x)) return 0.0;
+  if (e0.x >= 1.0) return 15.0 / (PI * PI * PI * PI) * (e0.s - e1.s);
+  return planck_F(e1) - planck_F(e0);
 }
 
 // canonical inclusive prefix sum of n values (the oracle's canon_prefix order)
@@ -399,8 +416,11 @@ __global__ void k_plan_mg_cells(PlanMgArgs a) {
     if (!isfinite(T) || !(a.cv[c] > 0.0)) atomicOr(&a.sum->flags, (int)IMC_FLAG_NONFINITE);
     double* gc = a.Egc + (size_t)c * G;  // scratch: fractions, then cumulative emission
     double tot = 0.0;
+    PlanckEdge lo = planck_edge(T > 0.0 ? a.gedges[0] / T : 0.0);
     for (int g = 0; g < G; ++g) {
-      const double f = (T > 0.0) ? planck_frac(a.gedges[g] / T, a.gedges[g + 1] / T) : 0.0;
+      const PlanckEdge hi = planck_edge(T > 0.0 ? a.gedges[g + 1] / T : 0.0);
+      const double f = (T > 0.0) ? planck_frac(lo, hi) : 0.0;
+      lo = hi;
       gc[g] = f > 0.0 ? f : 0.0;
       tot += gc[g];
     }
@@ -535,8 +555,11 @@ __global__ void __launch_bounds__(NT) k_plan_mg1d(PlanMgArgs a) {
     if (!isfinite(T) || !(a.cv[c] > 0.0)) atomicOr(&a.sum->flags, (int)IMC_FLAG_NONFINITE);
     double* b = a.Egc + (size_t)c * G;  // scratch: Planck fractions of this cell
     double tot = 0.0;
+    PlanckEdge lo = planck_edge(T > 0.0 ? a.gedges[0] / T : 0.0);
     for (int g = 0; g < G; ++g) {
-      const double f = (T > 0.0) ? planck_frac(a.gedges[g] / T, a.gedges[g + 1] / T) : 0.0;
+      const PlanckEdge hi = planck_edge(T > 0.0 ? a.gedges[g + 1] / T : 0.0);
+      const double f = (T > 0.0) ? planck_frac(lo, hi) : 0.0;
+      lo = hi;
       b[g] = f > 0.0 ? f : 0.0;
       tot += b[g];
     }
