@@ -14,7 +14,7 @@ import torch
 
 from . import _lib
 from .engine import A_RAD, C_LIGHT, Engine
-from .materials import evaluate
+from .materials import evaluate, is_device
 
 
 class GrayState:
@@ -103,6 +103,17 @@ class GrayState:
             self._host.pop(name, None)
             return
         object.__setattr__(self, name, value)
+
+
+def _pinned(state, key: str, n: int) -> torch.Tensor:
+    """A pinned host buffer of n doubles kept on the state (allocated once)."""
+    bufs = state.__dict__.get("_pinned")
+    if bufs is None:
+        bufs = {}
+        object.__setattr__(state, "_pinned", bufs)
+    if key not in bufs or bufs[key].numel() != n:
+        bufs[key] = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    return bufs[key]
 
 
 def _host_copy(t: torch.Tensor) -> np.ndarray:
@@ -224,12 +235,26 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
         average_tallies(allreduce, eng)
 
     # material update: e += dep - emitted/V ; Tr from the path-length intensity.  The comb
-    # does not need T, so it is queued first and a host inv_eos overlaps it on the GPU.
+    # does not need T: with a host inv_eos (and the comb discrepancy not booked into e), e is
+    # copied out before the comb is queued, so the host evaluation overlaps the comb.
     eng.material_update(state._e, state._Tr)
+    e_ready = None
+    if not conserve_comb_energy and not is_device(inv_eos):
+        e_pin = _pinned(state, "e_mid", eng.nc)
+        e_pin.copy_(state._e, non_blocking=True)
+        e_ready = torch.cuda.Event()
+        e_ready.record()
     eng.comb_async(Nmax, state.count, state._e)
     if conserve_comb_energy:
         state._e.add_(eng.disc[: eng.nc] / eng.vol)
-    Tn = evaluate(inv_eos, state.grid(state._e), lambda: _host_copy(state.grid(state._e)), like)
+    if e_ready is not None:
+        def e_host():
+            e_ready.synchronize()
+            _lib.TRANSFER["d2h"] += e_pin.numel() * 8
+            return e_pin.numpy().copy() if state._dim == 1 else e_pin.numpy().reshape(state._shape[1], state._shape[0]).T
+        Tn = evaluate(inv_eos, state.grid(state._e), e_host, like)
+    else:
+        Tn = evaluate(inv_eos, state.grid(state._e), lambda: _host_copy(state.grid(state._e)), like)
     state._T.copy_(state.flat(Tn))
     try:
         sm = eng.fetch(state.host_copies())
