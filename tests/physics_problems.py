@@ -64,3 +64,36 @@ def zero_d_exact(p, times):
     sol = solve_ivp(rhs, [0.0, times[-1] * (1 + 1e-12)], [A_RAD * p["Tr0"] ** 4, cv * p["T0"]], t_eval=times,
                     rtol=1e-10, atol=1e-14)
     return sol.y[1] / cv, (sol.y[0] / A_RAD) ** 0.25
+
+
+def zero_d_mg_exact(edges, sigmas, cv, T0, Tr0, times):
+    """0-D multigroup exchange: dE_g/dt = c sigma_g (a T^4 b_g(T) - E_g), cv dT/dt = -sum_g of
+    the same, with b_g the normalised Planck fractions over the groups (as the MG step emits)
+    and E_g(0) = a Tr0^4 b_g(Tr0).  Returns T(t), Tr(t) = (sum_g E_g / a)^(1/4)."""
+    from scipy.integrate import solve_ivp
+
+    from radtranbook_b200.mg_imc2d import planck_fractions
+
+    sig = np.asarray(sigmas, dtype=np.float64)
+    G = len(sig)
+
+    def rhs(t, y):
+        T = y[G] / cv
+        b = planck_fractions(edges, np.array([T])).reshape(G)
+        ex = C_LIGHT * sig * (A_RAD * T ** 4 * b - y[:G])
+        return np.concatenate([ex, [-ex.sum()]])
+
+    b0 = planck_fractions(edges, np.array([Tr0])).reshape(G)
+    y0 = np.concatenate([A_RAD * Tr0 ** 4 * b0, [cv * T0]])
+    sol = solve_ivp(rhs, [0.0, times[-1] * (1 + 1e-12)], y0, t_eval=times, rtol=1e-9, atol=1e-14, method="LSODA")
+    return sol.y[G] / cv, (np.clip(sol.y[:G].sum(0), 0.0, None) / A_RAD) ** 0.25
+
+
+def marshak_self_similar(x, t, T_bc=1.0, cv=0.3, sigma_coef=300.0):
+    """Self-similar Marshak wave for sigma = sigma_coef T^-3, e = cv T (IMC/MarshakWave2D.py:
+    187-209; profile constants xi_max = 1.11305, omega = 0.05989)."""
+    xi_max, omega = 1.11305, 0.05989
+    K = 8.0 * A_RAD * C_LIGHT / (7.0 * 3.0 * sigma_coef * T_bc ** -3 * cv)
+    xi = np.asarray(x) / np.sqrt(K * max(float(t), 1e-30))
+    return np.where(xi < xi_max, T_bc * np.power(np.maximum((1.0 - xi / xi_max) * (1.0 + omega * xi / xi_max), 1e-30),
+                                                  1.0 / 6.0), 0.0)

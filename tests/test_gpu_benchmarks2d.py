@@ -1,0 +1,140 @@
+"""Known-answer checks of the reference's own validation scripts, run through the drop-in API
+on the GPU.
+
+  - Multigroup gray limit (MG_IMC/problems/test_0D_multigroup_compare.py set-up: one closed
+    cell, sigma = 1 in every group of [0.1, 0.5, 1, 2, 5, 10] keV, cv = 0.01, T0 = 0.4,
+    Tr0 = 1.0): the MG step against the gray step and the gray exchange ODE.
+  - Multigroup infinite medium (MG_IMC/problems/compare_infinite_medium_imc_vs_scipy.py
+    idea: the deterministic 0-D multigroup exchange solved by scipy): eight groups with
+    group-dependent opacities, T and Tr against the ODE at every step.
+  - Cartesian directional symmetry and the self-similar Marshak wave
+    (IMC/MarshakWave2D.py:212-283: sigma = 300 T^-3, cv = 0.3, 60 x 60 cells on 0.2 cm, a
+    1 keV source on the left face or on the bottom face, dt = 0.01 ns to 1 ns): the
+    transverse means of the two runs against each other and against the self-similar profile.
+  - RZ planar limit (IMC/MarshakWave2D.py:286-340: a thin annulus at r = 10 cm driven from
+    z = 0) against the 1-D slab step on the same z mesh.
+
+Tolerances are the Monte Carlo noise of these particle counts with margin, written per test.
+"""
+import numpy as np
+import pytest
+
+from tests import physics_problems as PP
+
+pytestmark = pytest.mark.gpu
+
+A_RAD = PP.A_RAD
+
+
+def _rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def _mg_zero_d(edges, sigmas, steps, dt=0.002, cv=0.01, T0=0.4, Tr0=1.0, N=20000, seed=0x0DD0):
+    from radtranbook_b200 import mg_imc2d
+
+    e1, e2 = np.array([0.0, 0.1]), np.array([0.0, 1.0])
+    fns = [(lambda T, s=s: s + 0.0 * T) for s in sigmas]
+    st = mg_imc2d.init_simulation(N, np.full((1, 1), T0), np.full((1, 1), Tr0), e1, e2, edges, lambda T: cv * T,
+                                  lambda u: u / cv, geometry="xy", seed=seed)
+    T, Tr = [], []
+    for _ in range(steps):
+        st, info = mg_imc2d.step(st, N, 0, 0, 2 * N, (0.0,) * 4, dt, e1, e2, edges, fns, lambda u: u / cv,
+                                 lambda T: cv + 0.0 * T, np.zeros((1, 1)), reflect=(True,) * 4)
+        assert abs(info["ledger"]["relative_closure"]) < 1e-12
+        T.append(float(st.temperature[0, 0]))
+        Tr.append(float(st.radiation_temperature[0, 0]))
+    return np.array(T), np.array(Tr)
+
+
+def test_multigroup_gray_limit(cuda):
+    from radtranbook_b200 import imc1d
+
+    edges = np.array([0.1, 0.5, 1.0, 2.0, 5.0, 10.0])
+    steps, dt = 60, 0.002
+    Tm, Trm = _mg_zero_d(edges, [1.0] * 5, steps, dt)
+    p = PP.zero_d(dt=dt, t_final=steps * dt)
+    mesh = np.stack([p["edges"][:-1], p["edges"][1:]], 1)
+    st = imc1d.init_simulation(20000, np.array([p["T0"]]), np.array([p["Tr0"]]), mesh, p["eos"], p["inv_eos"],
+                               seed=0x0DD1)
+    Tg = []
+    for _ in range(steps):
+        st, info = imc1d.step(st, 20000, 0, 0, 40000, (0.0, 0.0), dt, mesh, p["sigma"], p["inv_eos"], p["cvf"],
+                              np.zeros(1), reflect=(True, True))
+        Tg.append(float(st.temperature[0]))
+    Tex, Trex = PP.zero_d_exact(p, dt * np.arange(1, steps + 1))
+    e_mg = float(np.max(np.abs(Tm - Tex) / Tex))
+    e_gray = float(np.max(np.abs(np.array(Tg) - Tex) / Tex))
+    e_tr = float(np.max(np.abs(Trm - Trex) / Trex))
+    print(f"gray limit: MG vs ODE {e_mg:.2e}, gray vs ODE {e_gray:.2e}, MG Tr vs ODE {e_tr:.2e}, "
+          f"MG vs gray {np.max(np.abs(Tm - np.array(Tg)) / np.array(Tg)):.2e}")
+    assert e_mg < 0.02 and e_gray < 0.02 and e_tr < 0.02
+
+
+def test_multigroup_infinite_medium_matches_ode(cuda):
+    edges = np.logspace(-2, np.log10(20.0), 9)
+    nu = np.sqrt(edges[:-1] * edges[1:])
+    sig = np.clip(0.5 / nu, 0.2, 2.0)
+    steps, dt = 60, 0.002
+    Tm, Trm = _mg_zero_d(edges, sig, steps, dt, seed=0x0DD2)
+    Tex, Trex = PP.zero_d_mg_exact(edges, sig, 0.01, 0.4, 1.0, dt * np.arange(1, steps + 1))
+    eT = float(np.max(np.abs(Tm - Tex) / Tex))
+    eTr = float(np.max(np.abs(Trm - Trex) / Trex))
+    print(f"MG infinite medium: T vs ODE {eT:.2e}, Tr vs ODE {eTr:.2e}")
+    assert eT < 0.03 and eTr < 0.03
+
+
+def _marshak_2d(geometry, e1, e2, Tbc, reflect, Ntarget, Nboundary, Nmax, steps, dt=0.01, seed=0x2D2D):
+    from radtranbook_b200 import imc2d
+
+    nx, ny = len(e1) - 1, len(e2) - 1
+    st = imc2d.init_simulation(Ntarget, np.full((nx, ny), 1e-4), np.full((nx, ny), 1e-4), e1, e2,
+                               lambda T: 0.3 * T, lambda u: u / 0.3, geometry=geometry, seed=seed)
+    for _ in range(steps):
+        st, info = imc2d.step(st, Ntarget, Nboundary, 0, Nmax, Tbc, dt, e1, e2,
+                              lambda T: 300.0 * np.maximum(T, 1e-4) ** -3, lambda u: u / 0.3,
+                              lambda T: 0.3 + 0.0 * T, np.zeros((nx, ny)), reflect=reflect, geometry=geometry,
+                              max_events_per_particle=100)
+        assert abs(info["ledger"]["relative_closure"]) < 1e-12
+    return st.temperature.copy()
+
+
+def test_xy_directional_symmetry_and_self_similar_profile(cuda):
+    n, L, steps = 60, 0.2, 100
+    e = np.linspace(0.0, L, n + 1)
+    Tx = _marshak_2d("xy", e, e, (1.0, 0.0, 0.0, 0.0), (False, True, True, True), 20000, 12000, 80000, steps)
+    Ty = _marshak_2d("xy", e, e, (0.0, 0.0, 1.0, 0.0), (True, True, False, True), 20000, 12000, 80000, steps,
+                     seed=0x2D2E)
+    px, py = Tx.mean(axis=1), Ty.mean(axis=0)
+    xc = 0.5 * (e[:-1] + e[1:])
+    Tss = PP.marshak_self_similar(xc, steps * 0.01)
+    bulk = Tss > 0.3
+    e_sym = _rel_l2(px, py)
+    e_ss = _rel_l2(px[bulk], Tss[bulk])
+    front = lambda p: float(np.interp(0.5, p[::-1], xc[::-1]))  # noqa: E731  where T falls through 0.5 keV
+    print(f"xy symmetry rel-L2 {e_sym:.2e}; x-run vs self-similar (T_ss > 0.3) {e_ss:.2e}; "
+          f"front(0.5 keV) x {front(px):.4f} y {front(py):.4f} self-similar {front(Tss):.4f}")
+    assert e_sym < 0.05
+    assert e_ss < 0.10
+    assert abs(front(px) - front(Tss)) < 0.15 * front(Tss)
+
+
+def test_rz_planar_limit_matches_slab(cuda):
+    from radtranbook_b200 import imc1d
+
+    nz, Lz, steps = 60, 0.2, 100
+    z = np.linspace(0.0, Lz, nz + 1)
+    r = np.linspace(10.0, 10.2, 11)
+    Trz = _marshak_2d("rz", r, z, (0.0, 0.0, 1.0, 0.0), (True, True, False, True), 24000, 12000, 120000, steps)
+    pz = Trz.mean(axis=0)
+    mesh = np.stack([z[:-1], z[1:]], 1)
+    st = imc1d.init_simulation(24000, np.full(nz, 1e-4), np.full(nz, 1e-4), mesh, lambda T: 0.3 * T,
+                               lambda u: u / 0.3, seed=0x1D1D)
+    for _ in range(steps):
+        st, info = imc1d.step(st, 24000, 12000, 0, 120000, (1.0, 0.0), 0.01, mesh,
+                              lambda T: 300.0 * np.maximum(T, 1e-4) ** -3, lambda u: u / 0.3,
+                              lambda T: 0.3 + 0.0 * T, np.zeros(nz), reflect=(False, True))
+    p1 = st.temperature.copy()
+    e_pl = _rel_l2(pz, p1)
+    print(f"rz planar limit rel-L2 {e_pl:.2e}")
+    assert e_pl < 0.05
