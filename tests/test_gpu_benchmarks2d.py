@@ -68,7 +68,8 @@ def test_multigroup_gray_limit(cuda):
     e_tr = float(np.max(np.abs(Trm - Trex) / Trex))
     print(f"gray limit: MG vs ODE {e_mg:.2e}, gray vs ODE {e_gray:.2e}, MG Tr vs ODE {e_tr:.2e}, "
           f"MG vs gray {np.max(np.abs(Tm - np.array(Tg)) / np.array(Tg)):.2e}")
-    assert e_mg < 0.02 and e_gray < 0.02 and e_tr < 0.02
+    assert e_mg < 0.02 and e_gray < 0.02 and e_tr < 0.02  # measured 0.9 %, 0.8 %, 0.7 %
+    assert np.max(np.abs(Tm - np.array(Tg)) / np.array(Tg)) < 0.01  # measured 0.12 %
 
 
 def test_multigroup_infinite_medium_matches_ode(cuda):
@@ -81,7 +82,7 @@ def test_multigroup_infinite_medium_matches_ode(cuda):
     eT = float(np.max(np.abs(Tm - Tex) / Tex))
     eTr = float(np.max(np.abs(Trm - Trex) / Trex))
     print(f"MG infinite medium: T vs ODE {eT:.2e}, Tr vs ODE {eTr:.2e}")
-    assert eT < 0.03 and eTr < 0.03
+    assert eT < 0.015 and eTr < 0.015  # measured 0.5 %, 0.2 %
 
 
 def _marshak_2d(geometry, e1, e2, Tbc, reflect, Ntarget, Nboundary, Nmax, steps, dt=0.01, seed=0x2D2D):
@@ -114,8 +115,8 @@ def test_xy_directional_symmetry_and_self_similar_profile(cuda):
     front = lambda p: float(np.interp(0.5, p[::-1], xc[::-1]))  # noqa: E731  where T falls through 0.5 keV
     print(f"xy symmetry rel-L2 {e_sym:.2e}; x-run vs self-similar (T_ss > 0.3) {e_ss:.2e}; "
           f"front(0.5 keV) x {front(px):.4f} y {front(py):.4f} self-similar {front(Tss):.4f}")
-    assert e_sym < 0.05
-    assert e_ss < 0.10
+    assert e_sym < 0.02  # measured 0.55 %
+    assert e_ss < 0.12  # measured 8 %: the self-similar profile is the diffusion limit
     assert abs(front(px) - front(Tss)) < 0.15 * front(Tss)
 
 
@@ -137,4 +138,4 @@ def test_rz_planar_limit_matches_slab(cuda):
     p1 = st.temperature.copy()
     e_pl = _rel_l2(pz, p1)
     print(f"rz planar limit rel-L2 {e_pl:.2e}")
-    assert e_pl < 0.05
+    assert e_pl < 0.04  # measured 1.9 %
