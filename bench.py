@@ -648,6 +648,8 @@ def run_ours(args, rank: int, world: int):
                    "autotune": None if tuned is None else {"best_ms": tuned["best_ms"], "worst_ms": tuned["worst_ms"],
                                                            "candidates": len(tuned["trials"])}},
         "histories_per_s": hist_all / (tmax * 1e-3),
+        # histories against HBM / (2 x 36-byte record + 28-byte source fill) per history
+        "histories_roofline_frac": hist_all / (tmax * 1e-3) * (2 * 36 + 28) / (peak * 1e9),
         "segments_per_step": seg_all / args.steps,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
