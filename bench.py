@@ -678,6 +678,9 @@ def main():
                     help="fixed tracking launch shape 'block,blocks_per_sm,chunk,smem_cells' instead of tuning")
     ap.add_argument("--tune-log", default=None, help="write the autotuner's trials to this JSON file")
     ap.add_argument("--no-forms", action="store_true", help="skip the batched and adjoint forms")
+    ap.add_argument("--only-form", default=None,
+                    choices=["batched", "adjoint", "carter_forest", "device_loop", "mg_crooked_pipe"],
+                    help="run one further form alone on GPU 0 and print its JSON (no headline line)")
     ap.add_argument("--batch-steps", type=int, default=4)
     ap.add_argument("--no-fom", action="store_true")
     ap.add_argument("--fom-seeds", type=int, default=32)
@@ -689,6 +692,15 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.only_form:
+        import torch
+
+        torch.cuda.set_device(0)
+        fn = {"batched": lambda: form_batched(args.batch_steps, not args.no_tune), "adjoint": form_adjoint,
+              "carter_forest": form_carter_forest, "device_loop": form_device_loop,
+              "mg_crooked_pipe": form_mg_crooked_pipe}[args.only_form]
+        print(json.dumps({"form": args.only_form, **fn()}), flush=True)
         return
     if world > 1:
         import datetime
