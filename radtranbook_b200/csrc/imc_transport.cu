@@ -85,6 +85,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   const float weight_floor = (float)(a.floor_coef * (*a.wsum) / (double)(n > 0 ? n : 1));
   const double inv_q = fx_inv_quantum(*a.wsum);  // fixed-point energy tallies
   const float ss_thr = (GEOM == G_SLAB || GEOM == G_SPHERE) ? 1e-10f : 1e-12f;
+  const float inv_nx = 1.0f / (float)a.nx;  // cell -> (i, j) at refill without an integer divide
 
   for (;;) {
     // ---------------- refill idle lanes from the warp's chunk ----------------
@@ -118,7 +119,11 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
           if (MG) grp = a.group[pid];
           if (GEOM == G_XY || GEOM == G_RZ) { y = a.p2[pid]; v = a.d2[pid]; }
           const int c = a.cell[pid];
-          cj = c / a.nx; ci = c - cj * a.nx;
+          // j from a float estimate, corrected to the exact quotient (the estimate is off by
+          // at most one for any int c)
+          cj = __float2int_rd(((float)c + 0.5f) * inv_nx);
+          ci = c - cj * a.nx;
+          if (ci < 0) { --cj; ci += a.nx; } else if (ci >= a.nx) { ++cj; ci -= a.nx; }
           tab = table(MG ? c + a.nc * grp : c);
           ev = 0;
           has = true;
