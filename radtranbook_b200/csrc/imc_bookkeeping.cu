@@ -536,21 +536,21 @@ __global__ void __launch_bounds__(NT) k_plan_mg(PlanMgArgs a) {
 // factor with the Planck-mean opacity, emission E_gc = a c T^4 sigma_a,g b*_g dt V per
 // (group, cell) bin b = g*nc + c with stratified counts max(1, round(N E_b / E)) (fixed
 // source: round, no minimum), inner / outer sphere boundary faces.
-__global__ void __launch_bounds__(NT) k_plan_mg1d(PlanMgArgs a) {
+// Per-shell part of the sphere plan, one thread per shell over a wide grid (each shell's
+// numbers depend on that shell alone, so the result is the single-block loop's).
+__global__ void k_plan_mg1d_cells(PlanMgArgs a) {
   const double dt = a.dt_dev ? *a.dt_dev : a.dt;  // device-resident step length (graph replay)
-  __shared__ double red[NT];
-  __shared__ long long sh[NT];
-  const int t = threadIdx.x;
-  const int nc = a.nc, G = a.ng, ncg = nc * G;
-  for (int q = t; q <= a.nx; q += NT) a.e1f[q] = (float)a.e1[q];
-  for (int q = t; q <= a.ny; q += NT) a.e2f[q] = (float)a.e2[q];
-  if (t == 0) {
+  const int nc = a.nc, G = a.ng;
+  const int t0 = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  for (int q = t0; q <= a.nx; q += stride) a.e1f[q] = (float)a.e1[q];
+  for (int q = t0; q <= a.ny; q += stride) a.e2f[q] = (float)a.e2[q];
+  if (t0 == 0) {
     double tot = 0.0;
     for (int n = 1; n <= 200; ++n) { const double d = (double)n; tot += 1.0 / (d * d * d * d); }
     double run = 0.0;
     for (int n = 1; n <= 200; ++n) { const double d = (double)n; run += 1.0 / (d * d * d * d); a.mixcdf[n - 1] = run / tot; }
   }
-  for (int c = t; c < nc; c += NT) {
+  for (int c = t0; c < nc; c += stride) {
     const double T = a.T[c];
     if (!isfinite(T) || !(a.cv[c] > 0.0)) atomicOr(&a.sum->flags, (int)IMC_FLAG_NONFINITE);
     double* b = a.Egc + (size_t)c * G;  // scratch: Planck fractions of this cell
@@ -583,7 +583,16 @@ __global__ void __launch_bounds__(NT) k_plan_mg1d(PlanMgArgs a) {
       a.emit_E[q] = cold ? 0.0 : A_RAD * C_LIGHT * pow4(T) * sa * b[g] * dt * a.vol[c];
     }
   }
-  __syncthreads();
+}
+
+// Single-block part of the sphere plan: canonical totals, stratified counts and scans,
+// fixed source, boundary faces, bank layout.
+__global__ void __launch_bounds__(NT) k_plan_mg1d(PlanMgArgs a) {
+  const double dt = a.dt_dev ? *a.dt_dev : a.dt;  // device-resident step length (graph replay)
+  __shared__ double red[NT];
+  __shared__ long long sh[NT];
+  const int t = threadIdx.x;
+  const int nc = a.nc, G = a.ng, ncg = nc * G;
   // ---- emission: stratified counts, FP32 weights, energy issued per bin and per cell ----
   const double Et = block_canon_sum(a.emit_E, ncg, red);
   for (int q = t; q < ncg; q += NT) {
@@ -697,7 +706,9 @@ cudaError_t imc_launch_plan_mg(const PlanMgArgs& a, cudaStream_t s) {
 }
 
 cudaError_t imc_launch_plan_mg1d(const PlanMgArgs& a, cudaStream_t s) {
-  ++g_imc_launches;
+  g_imc_launches += 2;
+  const int n = std::max(a.nc, std::max(a.nx, a.ny) + 1);
+  k_plan_mg1d_cells<<<(n + 255) / 256, 256, 0, s>>>(a);
   k_plan_mg1d<<<1, NT, 0, s>>>(a);
   return cudaGetLastError();
 }
