@@ -58,7 +58,8 @@ typedef enum imc_status {
   IMC_ERR_TIMEOUT = 5,         /* a bounded device wait gave up */
   IMC_ERR_CUDA = 6,            /* CUDA runtime error (see imc_last_cuda_error) */
   IMC_ERR_INVALID_ARG = 7,
-  IMC_ERR_WORKSPACE = 8        /* workspace too small */
+  IMC_ERR_WORKSPACE = 8,       /* workspace too small */
+  IMC_ERR_BOUNDS = 9           /* bounds-checked build only: an index or weight out of range */
 } imc_status;
 
 enum { IMC_GEOM_SLAB = 0, IMC_GEOM_SPHERE = 1, IMC_GEOM_XY = 2, IMC_GEOM_RZ = 3 };
@@ -169,7 +170,12 @@ typedef struct imc_comb_report {
 /* Device-resident summary of one step, written by the asynchronous calls (the caller
  * allocates it in device memory and copies it to the host once per step).  Bank sizes
  * live here between the phases, so no phase needs the host to know them. */
-enum { IMC_FLAG_EVENT_CAP = 1, IMC_FLAG_NONFINITE = 2, IMC_FLAG_COMB_OVERFLOW = 4 };
+/* IMC_FLAG_BOUNDS is set only by the bounds-checked build of this library
+ * (libimcb200_checked.so: every source compiled with IMC_CHECKED): a tracking or comb kernel
+ * met a cell, group or bin index outside the mesh, or a non-finite particle weight; it
+ * skipped that access and the host call reports IMC_ERR_BOUNDS.  No reference counterpart
+ * (the reference asserts particle-in-cell in its event loop, IMC/IMC1D.py:98-113). */
+enum { IMC_FLAG_EVENT_CAP = 1, IMC_FLAG_NONFINITE = 2, IMC_FLAG_COMB_OVERFLOW = 4, IMC_FLAG_BOUNDS = 8 };
 typedef struct imc_step_summary {
   int64_t n_census;             /* bank entries before the sources (set by the caller) */
   int64_t n_side[4];            /* boundary particles per side */

@@ -7,11 +7,13 @@ device call is made, the call raises.
 from __future__ import annotations
 
 import ctypes
+import os
 import pathlib
 from ctypes import POINTER, c_double, c_int, c_int32, c_int64, c_uint32, c_uint64, c_ulonglong, c_void_p, c_size_t, c_char_p
 
 HERE = pathlib.Path(__file__).resolve().parent
-LIB_PATH = HERE / "libimcb200.so"
+# IMCB200_CHECKED=1 selects the bounds-checked build (radtranbook_b200/build.py)
+LIB_PATH = HERE / ("libimcb200_checked.so" if os.environ.get("IMCB200_CHECKED") == "1" else "libimcb200.so")
 
 GEOM = {"slab": 0, "spherical": 1, "xy": 2, "rz": 3}
 
@@ -25,6 +27,7 @@ STATUS = {
     6: "IMC_ERR_CUDA",
     7: "IMC_ERR_INVALID_ARG",
     8: "IMC_ERR_WORKSPACE",
+    9: "IMC_ERR_BOUNDS",
 }
 OK, BANK_OVERFLOW = 0, 1
 
@@ -95,7 +98,7 @@ class ImcCombReport(ctypes.Structure):
     ]
 
 
-FLAG_EVENT_CAP, FLAG_NONFINITE, FLAG_COMB_OVERFLOW = 1, 2, 4
+FLAG_EVENT_CAP, FLAG_NONFINITE, FLAG_COMB_OVERFLOW, FLAG_BOUNDS = 1, 2, 4, 8
 
 
 class ImcStepSummary(ctypes.Structure):

@@ -488,6 +488,7 @@ const char* imc_status_str(imc_status s) {
     case IMC_ERR_CUDA: return "CUDA runtime error";
     case IMC_ERR_INVALID_ARG: return "invalid argument";
     case IMC_ERR_WORKSPACE: return "workspace too small";
+    case IMC_ERR_BOUNDS: return "bounds check failed (an index or weight out of range)";
   }
   return "unknown status";
 }
@@ -617,6 +618,7 @@ imc_status imc_step_transport(const imc_mesh* mesh, const imc_material* mat, con
   report->weight_floor = (mg_sphere(mesh) ? 1e-14 : 1e-10) * h.weight_sum / (double)std::max<long long>(h.n_bank, 1);
   imc_phase_times(&report->ms_sources, &report->ms_transport);
   bank->size = h.n_bank;
+  if (h.flags & IMC_FLAG_BOUNDS) return IMC_ERR_BOUNDS;
   if (h.flags & IMC_FLAG_NONFINITE) return IMC_ERR_NONFINITE;
   if (h.flags & IMC_FLAG_EVENT_CAP) return IMC_ERR_EVENT_CAP;
   return IMC_OK;
@@ -643,6 +645,7 @@ imc_status imc_adjoint_vjp(const imc_mesh* mesh, const imc_material* mat, const 
   int flags = 0;
   IMC_CUDA(cudaMemcpyAsync(&flags, &sum->flags, sizeof(int), cudaMemcpyDeviceToHost, s));
   IMC_CUDA(cudaStreamSynchronize(s));
+  if (flags & IMC_FLAG_BOUNDS) return IMC_ERR_BOUNDS;
   if (flags & IMC_FLAG_NONFINITE) return IMC_ERR_NONFINITE;
   return IMC_OK;
 }
@@ -716,6 +719,7 @@ imc_status imc_comb(const imc_mesh* mesh, const imc_bank* in, imc_bank* out, int
   report->required_capacity = h.n_out;
   report->energy_before = h.comb_before;
   report->energy_after = h.comb_after;
+  if (h.flags & IMC_FLAG_BOUNDS) return IMC_ERR_BOUNDS;
   if (h.flags & IMC_FLAG_COMB_OVERFLOW) return IMC_ERR_BANK_OVERFLOW;
   out->size = h.n_out;
   report->n_out = h.n_out;
@@ -752,6 +756,7 @@ imc_status imc_comb_noalloc(const imc_mesh* mesh, const imc_bank* in, imc_bank* 
   report->required_capacity = h.n_out;
   report->energy_before = h.comb_before;
   report->energy_after = h.comb_after;
+  if (h.flags & IMC_FLAG_BOUNDS) return IMC_ERR_BOUNDS;
   if (h.flags & IMC_FLAG_COMB_OVERFLOW) return IMC_ERR_BANK_OVERFLOW;
   out->size = h.n_out;
   report->n_out = h.n_out;

@@ -26,6 +26,18 @@ __device__ __forceinline__ int bin_of(const CombArgs& a, long long k) {
   return a.per_group ? a.cell[k] + a.nc * a.group[k] : a.cell[k];
 }
 
+// Bounds-checked build: a bin outside [0, nb) is reported and its entry treated as dead.
+__device__ __forceinline__ bool bin_ok(const CombArgs& a, int b) {
+#ifdef IMC_CHECKED
+  if (b >= 0 && b < a.nb) return true;
+  if (a.sum) atomicOr(&a.sum->flags, (int)IMC_FLAG_BOUNDS);
+  return false;
+#else
+  (void)a; (void)b;
+  return true;
+#endif
+}
+
 // weight of every copy in bin b: the comb weight, or the bin's energy shared equally
 __device__ __forceinline__ float copy_weight(const CombArgs& a, int b) {
   if (!a.conserve_rad) return (float)a.ew[b];
@@ -55,7 +67,7 @@ __global__ void __launch_bounds__(256) k_comb_ecen(CombArgs a) {
     double w = 0.0;
     if (k < n_in) {
       const float wf = a.w[k];
-      if (wf > 0.f) { live = true; b = bin_of(a, k); w = (double)wf; }
+      if (wf > 0.f) { b = bin_of(a, k); live = bin_ok(a, b); w = live ? (double)wf : 0.0; if (!live) b = 0; }
     }
     n_live += live ? 1u : 0u;
     warp_bins_add(live, b, w, t, a.ecen, st);
@@ -80,7 +92,7 @@ __global__ void __launch_bounds__(CB) k_comb_count(CombArgs a) {
   if (k < n_in) {
     const float wf = a.w[k];
     const int bk = bin_of(a, k);  // loaded with the weight (k < n_in: in bounds)
-    if (wf > 0.f) {
+    if (wf > 0.f && bin_ok(a, bk)) {
       b = bk;
       const double ew = a.ew[b];
       if (compact) {

@@ -119,20 +119,36 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
           if (MG) grp = a.group[pid];
           if (GEOM == G_XY || GEOM == G_RZ) { y = a.p2[pid]; v = a.d2[pid]; }
           const int c = a.cell[pid];
-          // j from a float estimate, corrected to the exact quotient (the estimate is off by
-          // at most one for any int c)
-          cj = __float2int_rd(((float)c + 0.5f) * inv_nx);
-          ci = c - cj * a.nx;
-          if (ci < 0) { --cj; ci += a.nx; } else if (ci >= a.nx) { ++cj; ci -= a.nx; }
-          tab = table(MG ? c + a.nc * grp : c);
-          ev = 0;
-          has = true;
+#ifdef IMC_CHECKED
+          // bounds-checked build: an entry outside the mesh (or group range), or with a
+          // non-finite weight, is reported and left untouched
+          if (c < 0 || c >= a.nc || (MG && (grp < 0 || grp >= a.ng)) || !isfinite(w)) {
+            atomicOr(a.flags, (int)IMC_FLAG_BOUNDS);
+          } else
+#endif
+          {
+            // j from a float estimate, corrected to the exact quotient (the estimate is off
+            // by at most one for any int c)
+            cj = __float2int_rd(((float)c + 0.5f) * inv_nx);
+            ci = c - cj * a.nx;
+            if (ci < 0) { --cj; ci += a.nx; } else if (ci >= a.nx) { ++cj; ci -= a.nx; }
+            tab = table(MG ? c + a.nc * grp : c);
+            ev = 0;
+            has = true;
+          }
         }
       }
       chunk_next += min((uint32_t)__popc(need), avail);
       need = __ballot_sync(FULL, !has);
     }
     if (!__any_sync(FULL, has)) break;
+#ifdef IMC_CHECKED
+    if (has && (ci < 0 || ci >= a.nx || cj < 0 || cj >= a.ny || !isfinite(w) || !isfinite(x) || !isfinite(dcen))) {
+      atomicOr(a.flags, (int)IMC_FLAG_BOUNDS);
+      acc_lost = 0.0; acc_wd = 0.0;  // nothing is tallied at an invalid index
+      has = false;
+    }
+#endif
 
     bool flush = false;
     int flush_cell = 0;

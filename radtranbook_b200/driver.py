@@ -294,6 +294,8 @@ class DeviceLoop:
         worst = 0.0
         for k, dt in enumerate(dts):
             sm = _lib.ImcStepSummary.from_buffer_copy(raw[k].tobytes())
+            if sm.flags & _lib.FLAG_BOUNDS:
+                raise _lib.ImcError("device loop: bounds check", 9)
             if sm.flags & _lib.FLAG_COMB_OVERFLOW:
                 raise _lib.ImcError("device loop: census above census_margin * Nmax", _lib.BANK_OVERFLOW)
             if sm.flags & _lib.FLAG_NONFINITE:

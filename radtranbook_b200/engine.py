@@ -384,6 +384,8 @@ class Engine:
         _lib.TRANSFER["d2h"] += self.summary_host.numel()
         sm = self.summary
         self.comb_repeated = False
+        if sm.flags & _lib.FLAG_BOUNDS:
+            raise _lib.ImcError("bounds check", 9)
         if sm.flags & _lib.FLAG_NONFINITE:
             raise _lib.ImcError("imc_step_transport_async", 3)
         if sm.flags & _lib.FLAG_EVENT_CAP:
