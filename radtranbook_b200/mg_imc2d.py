@@ -251,7 +251,13 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
         state._e.add_(eng.disc.view(G, nc).sum(0) / eng.vol)
     Tn = evaluate(inv_eos, state.grid(state._e), lambda: _host_copy(state.grid(state._e)), like)
     state._T.copy_(state.flat(Tn))
-    group_copies = [(rad_pre.reshape(-1), hb["pre"]), (hb["post_dev"], hb["post"]),
+    nx, ny = state._shape
+
+    def to_grid3(x):  # device (G, nc) in flat cell order -> (G, nx, ny) C order, flattened
+        return x.reshape(G, ny, nx).transpose(1, 2).reshape(-1)
+
+    # the (G, nx, ny) transposes run on the device, so the host only copies contiguous arrays
+    group_copies = [(to_grid3(rad_pre), hb["pre"]), (to_grid3(hb["post_dev"]), hb["post"]),
                     (eng.boundary_group, hb["bnd"]), (eng.escaped_group, hb["esc"])]
     try:
         sm = eng.fetch(state.host_copies() + group_copies)
@@ -271,7 +277,7 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
     else:
         state.take_host_copies()
     if eng.comb_repeated:  # the comb ran again after an overflow: rebuild from the new census
-        hb["post"].copy_(_rad_by_group(eng).reshape(-1))
+        hb["post"].copy_(to_grid3(_rad_by_group(eng)))
     internal = float(sm.internal_energy)
     rad = float(sm.comb_after)
     comb_disc = float(sm.comb_before) - rad
@@ -289,12 +295,11 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
     state.previous_total_energy = total
     state.count += 1
 
-    def grid3(h):  # pinned host (G * nc) -> (G, nx, ny)
-        nx, ny = state._shape
-        return h.numpy().reshape(G, ny, nx).transpose(0, 2, 1).copy()
+    def grid3(h):  # pinned host buffer, already (G, nx, ny) -> an array of its own
+        return h.numpy().reshape(G, nx, ny).copy()
 
     if not use_scalar_intensity_Tr:
-        hb["pre"].copy_(rad_pre.reshape(-1))
+        hb["pre"].copy_(to_grid3(rad_pre))
     rad_group_pre = grid3(hb["pre"])
     rad_group_post = grid3(hb["post"])
     _lib.TRANSFER["d2h"] += 8 * (2 * G * nc + 2 * G)
