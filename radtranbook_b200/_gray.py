@@ -210,8 +210,10 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
     dim = state._dim
     like = state.grid(state._T)
     host_T = lambda: state.temperature  # noqa: E731
-    sigma = state.flat(evaluate(sigma_a_func, like, host_T, like))
-    cvv = state.flat(evaluate(cv, like, host_T, like))
+    # host callables' results go up by asynchronous copies from pinned buffers of the state
+    # (refilled only next step, after this step's end-of-step synchronisation)
+    sigma = state.flat(evaluate(sigma_a_func, like, host_T, like, stage=_pinned(state, "sigma", eng.nc)))
+    cvv = state.flat(evaluate(cv, like, host_T, like, stage=_pinned(state, "cv", eng.nc)))
     src = None
     if Nsource > 0 and source is not None:
         src_t = source.double() if isinstance(source, torch.Tensor) else torch.as_tensor(
@@ -252,7 +254,7 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
             e_ready.synchronize()
             _lib.TRANSFER["d2h"] += e_pin.numel() * 8
             return e_pin.numpy().copy() if state._dim == 1 else e_pin.numpy().reshape(state._shape[1], state._shape[0]).T
-        Tn = evaluate(inv_eos, state.grid(state._e), e_host, like)
+        Tn = evaluate(inv_eos, state.grid(state._e), e_host, like, stage=_pinned(state, "T_new", eng.nc))
     else:
         Tn = evaluate(inv_eos, state.grid(state._e), lambda: _host_copy(state.grid(state._e)), like)
     state._T.copy_(state.flat(Tn))

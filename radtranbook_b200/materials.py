@@ -27,11 +27,14 @@ def is_device(fn) -> bool:
     return bool(getattr(fn, "_imc_device", False))
 
 
-def evaluate(fn, T_dev: torch.Tensor, T_host_fn, like: torch.Tensor) -> torch.Tensor:
+def evaluate(fn, T_dev: torch.Tensor, T_host_fn, like: torch.Tensor, stage: torch.Tensor | None = None) -> torch.Tensor:
     """Evaluate a material callable on the temperature field.
 
     T_dev: device tensor in the reference's array shape.  T_host_fn: zero-argument
     function returning the same field as a NumPy array (called only for host callables).
+    stage: optional pinned host buffer (>= like.numel() doubles) for a host callable's
+    result, which then goes to the device by an asynchronous copy (the caller must not
+    refill the buffer before the stream has passed that copy).
     Returns a float64 device tensor broadcast to `like`'s shape.
     """
     if is_device(fn):
@@ -40,6 +43,12 @@ def evaluate(fn, T_dev: torch.Tensor, T_host_fn, like: torch.Tensor) -> torch.Te
             out = torch.as_tensor(np.asarray(out, dtype=np.float64), device=like.device)
         return torch.broadcast_to(out.to(like.device, torch.float64), like.shape)
     out = fn(T_host_fn())
+    if stage is not None:
+        n = like.numel()
+        host = stage[:n].view(tuple(like.shape))
+        np.copyto(host.numpy(), np.broadcast_to(np.asarray(out, dtype=np.float64), tuple(like.shape)))
+        TRANSFER["h2d"] += n * 8
+        return host.to(like.device, non_blocking=True)
     arr = np.array(np.broadcast_to(np.asarray(out, dtype=np.float64), tuple(like.shape)), order="C", copy=True)
     TRANSFER["h2d"] += arr.nbytes
     return torch.as_tensor(arr, device=like.device)
