@@ -113,9 +113,14 @@ class GroupedOpacity(list):
         self.all_groups = all_groups
 
 
-def evaluate_groups(funcs, T_dev: torch.Tensor, T_host_fn, like: torch.Tensor) -> torch.Tensor:
-    """Every group's opacity on the temperature field, (G, *like.shape) float64 on the device."""
+def evaluate_groups(funcs, T_dev: torch.Tensor, T_host_fn, like: torch.Tensor,
+                    stage: torch.Tensor | None = None) -> torch.Tensor:
+    """Every group's opacity on the temperature field, (G, *like.shape) float64 on the device.
+    stage: optional pinned host buffer of G x like.numel() doubles for host callables (see
+    evaluate)."""
     if isinstance(funcs, GroupedOpacity):
         out = funcs.all_groups(T_dev)
         return torch.broadcast_to(out.to(like.device, torch.float64), (len(funcs),) + tuple(like.shape))
-    return torch.stack([evaluate(f, T_dev, T_host_fn, like) for f in funcs])
+    n = like.numel()
+    return torch.stack([evaluate(f, T_dev, T_host_fn, like, stage=None if stage is None else stage[g * n:(g + 1) * n])
+                        for g, f in enumerate(funcs)])
