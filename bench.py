@@ -507,6 +507,27 @@ def form_mg_crooked_pipe(steps: int = 12, warmup: int = 3) -> dict:
                             "max_relative_closure": res["max_relative_closure"]}}
 
 
+def form_mg_crooked_pipe_run(output_times=(1.0, 5.0, 10.0)) -> dict:
+    """The multigroup crooked pipe driven by driver.mg_crooked_pipe_run to the last output time
+    ('standard' preset, adaptive dt from 1e-4 ns by 1.1 to 0.01 ns, Nmax growing to 5e6):
+    device time, steps, census, worst closure and the fiducial temperatures at each output."""
+    from radtranbook_b200 import driver, mg_imc2d, problems
+
+    p = problems.mg_crooked_pipe(mode="standard")
+    st = mg_imc2d.init_simulation(p["Ntarget"], p["Tinit"], p["Tr_init"], p["edges1"], p["edges2"],
+                                  p["energy_edges"], p["eos_dev"], p["inv_eos_dev"], T_emit_floor=p["T_emit_floor"],
+                                  geometry="rz", seed=0x36CA)
+    times, fid, fid_rad, snaps, res = driver.mg_crooked_pipe_run(st, p, list(output_times))
+    idx = {t: int(np.argmin(np.abs(np.array(times) - t))) for t in output_times}
+    seg = sum(s["transport_events"]["total"] for s in res["steps"])
+    return {"workload": "mg_crooked_pipe_rz_60x210_10g_standard, device loop to %g ns" % max(output_times),
+            "steps": len(res["steps"]), "device_s": res["device_ms"] * 1e-3,
+            "segments_per_s": seg / (res["device_ms"] * 1e-3), "census_final": res["steps"][-1]["N_particles"],
+            "max_relative_closure": res["max_relative_closure"],
+            "fiducial_T": {lbl: {str(t): fid[lbl][i] for t, i in idx.items()} for lbl in fid},
+            "fiducial_Tr": {lbl: {str(t): fid_rad[lbl][i] for t, i in idx.items()} for lbl in fid_rad}}
+
+
 def max_time_and_totals(dist, ms: float, counts: list, device) -> tuple:
     """Whole-job figures of a timed region: the slowest rank's device time (ms) and the
     sum over ranks of each count (segments, histories)."""
@@ -679,7 +700,8 @@ def main():
     ap.add_argument("--tune-log", default=None, help="write the autotuner's trials to this JSON file")
     ap.add_argument("--no-forms", action="store_true", help="skip the batched and adjoint forms")
     ap.add_argument("--only-form", default=None,
-                    choices=["batched", "adjoint", "carter_forest", "device_loop", "mg_crooked_pipe"],
+                    choices=["batched", "adjoint", "carter_forest", "device_loop", "mg_crooked_pipe",
+                             "mg_crooked_pipe_run"],
                     help="run one further form alone on GPU 0 and print its JSON (no headline line)")
     ap.add_argument("--batch-steps", type=int, default=4)
     ap.add_argument("--no-fom", action="store_true")
@@ -699,7 +721,7 @@ def main():
         torch.cuda.set_device(0)
         fn = {"batched": lambda: form_batched(args.batch_steps, not args.no_tune), "adjoint": form_adjoint,
               "carter_forest": form_carter_forest, "device_loop": form_device_loop,
-              "mg_crooked_pipe": form_mg_crooked_pipe}[args.only_form]
+              "mg_crooked_pipe": form_mg_crooked_pipe, "mg_crooked_pipe_run": form_mg_crooked_pipe_run}[args.only_form]
         print(json.dumps({"form": args.only_form, **fn()}), flush=True)
         return
     if world > 1:
