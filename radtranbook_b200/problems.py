@@ -13,6 +13,9 @@ problem can be run through the drop-in API, the device engine or the CPU oracle.
                  emission:boundary, Nmax 6.67e6 (IMC/CrookedPipe2D.py geometry)
   mg_crooked_pipe  2-D RZ multigroup crooked pipe (MG_IMC/problems/crooked_pipe_multigroup_imc.py
                  with its command-line defaults; see the function)
+  marshak_mg     multigroup Marshak wave, 200 cells x 10 groups, 1e6 particles per step, on the
+                 2-D multigroup step (MG_IMC/problems/test_marshak_wave_multigroup_powerlaw.py
+                 set-up with sigma_g clamped to [1e-2, 1e6]; see the function)
 """
 from __future__ import annotations
 
@@ -191,4 +194,50 @@ def mg_crooked_pipe(n_groups: int = 10, nr: int = 60, nz: int = 210, mode: str =
         T_emit_floor=0.075, dt_initial=1e-4, dt_max=0.01, dt_growth=1.1, source=np.zeros((nr, nz)),
         fiducials={"r=0,z=0.25": (0.0, 0.25), "r=0,z=2.75": (0.0, 2.75), "r=1.25,z=3.5": (1.25, 3.5),
                    "r=0,z=4.25": (0.0, 4.25), "r=0,z=6.75": (0.0, 6.75)},
+    )
+
+
+def marshak_mg(scale: float = 1.0) -> dict:
+    """1-D multigroup Marshak wave run through the 2-D multigroup step (MG_IMC2D on an XY strip,
+    reflecting in y): slab 0.5 cm in 200 cells, 10 groups with edges log-spaced on [1e-4, 20]
+    keV, sigma_g(T) = clamp(10 nu_g^-3 T^-1/2, 1e-2, 1e6) with nu_g the arithmetic group
+    midpoint, cv = 0.3, a 1 keV source on the left face, T0 = 0.001 keV, dt = 0.005 ns,
+    1e6 particles per step split 2:1 between emission and the boundary, Nmax 1.33e6."""
+    nx = 200
+    e1 = np.linspace(0.0, 0.5, nx + 1)
+    e2 = np.array([0.0, 1.0])
+    edges = np.logspace(-4, np.log10(20.0), 11)
+    nu = 0.5 * (edges[:-1] + edges[1:])
+    cv_val = 0.3
+
+    def one(g):
+        k = 10.0 * nu[g] ** -3
+
+        def host(T):
+            return np.clip(k * np.power(T, -0.5), 1e-2, 1e6)
+
+        @device_callable
+        def dev(T):
+            return torch.clamp(k * torch.pow(T, -0.5), min=1e-2, max=1e6)
+        return host, dev
+
+    ops = [one(g) for g in range(10)]
+    kt = {}
+
+    def all_groups(T):  # every group in one expression, the same arithmetic as each callable
+        if T.device not in kt:
+            kt[T.device] = torch.tensor(10.0 * nu ** -3, dtype=torch.float64, device=T.device).view(-1, 1, 1)
+        return torch.clamp(kt[T.device] * torch.pow(T, -0.5), min=1e-2, max=1e6)
+
+    return dict(
+        name="multigroup Marshak wave (200 cells, 10 groups) on the 2-D multigroup step",
+        geometry="xy", dim=2, edges1=e1, edges2=e2, energy_edges=edges,
+        Tinit=np.full((nx, 1), 0.001), Tr_init=np.full((nx, 1), 0.001),
+        sigma_host=[h for h, _ in ops], sigma_dev=GroupedOpacity([d for _, d in ops], all_groups),
+        cv_host=lambda T: np.full_like(T, cv_val), cv_dev=device_callable(lambda T: torch.full_like(T, cv_val)),
+        eos_host=lambda T: cv_val * T, inv_eos_host=lambda e: e / cv_val,
+        eos_dev=device_callable(lambda T: cv_val * T), inv_eos_dev=device_callable(lambda e: e / cv_val),
+        Ntarget=int(666667 * scale), Nboundary=int(333333 * scale), Nsource=0, Nmax=int(1330000 * scale),
+        T_boundary=(1.0, 0.0, 0.0, 0.0), reflect=(False, False, True, True), dt=0.005, n_steps=200,
+        source=np.zeros((nx, 1)),
     )
