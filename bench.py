@@ -507,6 +507,55 @@ def form_mg_crooked_pipe(steps: int = 12, warmup: int = 3) -> dict:
                             "max_relative_closure": res["max_relative_closure"]}}
 
 
+def form_other_configs(steps: int = 20, warmup: int = 5) -> dict:
+    """The other two single-problem workloads at full size through the drop-in steps with device
+    callables (CUDA-event timing of whole steps): the slab Marshak wave (20k + 20k particles
+    per step, 100 cells) and the multigroup Marshak wave (1e6 particles per step, 200 cells x
+    10 groups, problems.marshak_mg)."""
+    import torch
+
+    from radtranbook_b200 import imc1d, mg_imc2d, problems
+
+    out = {}
+    p = problems.marshak_slab()
+    st = imc1d.init_simulation(p["Ntarget"], p["Tinit"], p["Tr_init"], p["mesh"], p["eos_dev"], p["inv_eos_dev"],
+                               seed=0xC0F1)
+
+    def slab(st, n):
+        seg = 0
+        for _ in range(n):
+            st, info = imc1d.step(st, p["Ntarget"], p["Nboundary"], 0, p["Nmax"], p["T_boundary"], p["dt"],
+                                  p["mesh"], p["sigma_dev"], p["inv_eos_dev"], p["cv_dev"], p["source"])
+            seg += info["profiling"]["transport_events"]["total"]
+        return st, seg
+
+    q = problems.marshak_mg()
+    sm = mg_imc2d.init_simulation(q["Ntarget"], q["Tinit"], q["Tr_init"], q["edges1"], q["edges2"],
+                                  q["energy_edges"], q["eos_dev"], q["inv_eos_dev"], geometry="xy", seed=0xC0F3)
+
+    def mg(sm, n):
+        seg = 0
+        for _ in range(n):
+            sm, info = mg_imc2d.step(sm, q["Ntarget"], q["Nboundary"], 0, q["Nmax"], q["T_boundary"], q["dt"],
+                                     q["edges1"], q["edges2"], q["energy_edges"], q["sigma_dev"], q["inv_eos_dev"],
+                                     q["cv_dev"], q["source"], reflect=q["reflect"], geometry="xy")
+            seg += info["profiling"]["transport_events"]["total"]
+        return sm, seg
+
+    for tag, fn, s0 in (("slab_marshak_100_cells", slab, st), ("mg_marshak_200x10", mg, sm)):
+        s0, _ = fn(s0, warmup)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        s0, seg = fn(s0, steps)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out[tag] = {"steps": steps, "after_warmup_steps": warmup, "ms_per_step": ms / steps,
+                    "segments_per_step": seg / steps, "segments_per_s": seg / (ms * 1e-3)}
+    return out
+
+
 def form_mg_crooked_pipe_run(output_times=(1.0, 5.0, 10.0)) -> dict:
     """The multigroup crooked pipe driven by driver.mg_crooked_pipe_run to the last output time
     ('standard' preset, adaptive dt from 1e-4 ns by 1.1 to 0.01 ns, Nmax growing to 5e6):
@@ -650,7 +699,7 @@ def run_ours(args, rank: int, world: int):
     if world == 1 and not args.no_forms:
         forms = {"batched": form_batched(args.batch_steps, not args.no_tune), "adjoint": form_adjoint(),
                  "carter_forest": form_carter_forest(), "device_loop": form_device_loop(launch=dict(eng.launch)),
-                 "mg_crooked_pipe": form_mg_crooked_pipe()}
+                 "mg_crooked_pipe": form_mg_crooked_pipe(), "other_configs": form_other_configs()}
         forms["carter_forest"]["over_fleck_cummings"] = forms["carter_forest"]["segments_per_s"] / value
     if world == 1 and not args.no_fom:
         fom = {"gpu": fom_gpu(p, args.fom_steps, args.fom_seeds, dict(eng.launch))}
@@ -701,7 +750,7 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="skip the batched and adjoint forms")
     ap.add_argument("--only-form", default=None,
                     choices=["batched", "adjoint", "carter_forest", "device_loop", "mg_crooked_pipe",
-                             "mg_crooked_pipe_run"],
+                             "mg_crooked_pipe_run", "other_configs"],
                     help="run one further form alone on GPU 0 and print its JSON (no headline line)")
     ap.add_argument("--batch-steps", type=int, default=4)
     ap.add_argument("--no-fom", action="store_true")
@@ -721,7 +770,8 @@ def main():
         torch.cuda.set_device(0)
         fn = {"batched": lambda: form_batched(args.batch_steps, not args.no_tune), "adjoint": form_adjoint,
               "carter_forest": form_carter_forest, "device_loop": form_device_loop,
-              "mg_crooked_pipe": form_mg_crooked_pipe, "mg_crooked_pipe_run": form_mg_crooked_pipe_run}[args.only_form]
+              "mg_crooked_pipe": form_mg_crooked_pipe, "mg_crooked_pipe_run": form_mg_crooked_pipe_run,
+              "other_configs": form_other_configs}[args.only_form]
         print(json.dumps({"form": args.only_form, **fn()}), flush=True)
         return
     if world > 1:
