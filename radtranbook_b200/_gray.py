@@ -116,6 +116,19 @@ def _pinned(state, key: str, n: int) -> torch.Tensor:
     return bufs[key]
 
 
+def _staged(state, key: str, n: int) -> dict:
+    """A pinned host buffer and its device twin (n doubles each) kept on the state: the
+    stage / stage_dev pair of materials.evaluate, so a host callable's result reaches the
+    device without a device allocation per step."""
+    devs = state.__dict__.get("_stage_dev")
+    if devs is None:
+        devs = {}
+        object.__setattr__(state, "_stage_dev", devs)
+    if key not in devs or devs[key].numel() != n:
+        devs[key] = torch.empty(n, dtype=torch.float64, device=state._engine.device)
+    return {"stage": _pinned(state, key, n), "stage_dev": devs[key]}
+
+
 def _host_copy(t: torch.Tensor) -> np.ndarray:
     a = t.cpu().numpy()
     _lib.TRANSFER["d2h"] += a.nbytes
@@ -212,8 +225,8 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
     host_T = lambda: state.temperature  # noqa: E731
     # host callables' results go up by asynchronous copies from pinned buffers of the state
     # (refilled only next step, after this step's end-of-step synchronisation)
-    sigma = state.flat(evaluate(sigma_a_func, like, host_T, like, stage=_pinned(state, "sigma", eng.nc)))
-    cvv = state.flat(evaluate(cv, like, host_T, like, stage=_pinned(state, "cv", eng.nc)))
+    sigma = state.flat(evaluate(sigma_a_func, like, host_T, like, **_staged(state, "sigma", eng.nc)))
+    cvv = state.flat(evaluate(cv, like, host_T, like, **_staged(state, "cv", eng.nc)))
     src = None
     if Nsource > 0 and source is not None:
         src_t = source.double() if isinstance(source, torch.Tensor) else torch.as_tensor(
@@ -254,7 +267,7 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
             e_ready.synchronize()
             _lib.TRANSFER["d2h"] += e_pin.numel() * 8
             return e_pin.numpy().copy() if state._dim == 1 else e_pin.numpy().reshape(state._shape[1], state._shape[0]).T
-        Tn = evaluate(inv_eos, state.grid(state._e), e_host, like, stage=_pinned(state, "T_new", eng.nc))
+        Tn = evaluate(inv_eos, state.grid(state._e), e_host, like, **_staged(state, "T_new", eng.nc))
     else:
         Tn = evaluate(inv_eos, state.grid(state._e), lambda: _host_copy(state.grid(state._e)), like)
     state._T.copy_(state.flat(Tn))

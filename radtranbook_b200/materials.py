@@ -27,14 +27,17 @@ def is_device(fn) -> bool:
     return bool(getattr(fn, "_imc_device", False))
 
 
-def evaluate(fn, T_dev: torch.Tensor, T_host_fn, like: torch.Tensor, stage: torch.Tensor | None = None) -> torch.Tensor:
+def evaluate(fn, T_dev: torch.Tensor, T_host_fn, like: torch.Tensor, stage: torch.Tensor | None = None,
+             stage_dev: torch.Tensor | None = None) -> torch.Tensor:
     """Evaluate a material callable on the temperature field.
 
     T_dev: device tensor in the reference's array shape.  T_host_fn: zero-argument
     function returning the same field as a NumPy array (called only for host callables).
     stage: optional pinned host buffer (>= like.numel() doubles) for a host callable's
     result, which then goes to the device by an asynchronous copy (the caller must not
-    refill the buffer before the stream has passed that copy).
+    refill the buffer before the stream has passed that copy); stage_dev: optional device
+    buffer of the same size that receives it (no allocation per call; the result is a view of
+    it, valid until the buffer's next use).
     Returns a float64 device tensor broadcast to `like`'s shape.
     """
     if is_device(fn):
@@ -48,6 +51,10 @@ def evaluate(fn, T_dev: torch.Tensor, T_host_fn, like: torch.Tensor, stage: torc
         host = stage[:n].view(tuple(like.shape))
         np.copyto(host.numpy(), np.broadcast_to(np.asarray(out, dtype=np.float64), tuple(like.shape)))
         TRANSFER["h2d"] += n * 8
+        if stage_dev is not None:
+            out_dev = stage_dev[:n].view(tuple(like.shape))
+            out_dev.copy_(host, non_blocking=True)
+            return out_dev
         return host.to(like.device, non_blocking=True)
     arr = np.array(np.broadcast_to(np.asarray(out, dtype=np.float64), tuple(like.shape)), order="C", copy=True)
     TRANSFER["h2d"] += arr.nbytes
@@ -114,7 +121,7 @@ class GroupedOpacity(list):
 
 
 def evaluate_groups(funcs, T_dev: torch.Tensor, T_host_fn, like: torch.Tensor,
-                    stage: torch.Tensor | None = None) -> torch.Tensor:
+                    stage: torch.Tensor | None = None, stage_dev: torch.Tensor | None = None) -> torch.Tensor:
     """Every group's opacity on the temperature field, (G, *like.shape) float64 on the device.
     stage: optional pinned host buffer of G x like.numel() doubles for host callables (see
     evaluate)."""
@@ -122,5 +129,6 @@ def evaluate_groups(funcs, T_dev: torch.Tensor, T_host_fn, like: torch.Tensor,
         out = funcs.all_groups(T_dev)
         return torch.broadcast_to(out.to(like.device, torch.float64), (len(funcs),) + tuple(like.shape))
     n = like.numel()
-    return torch.stack([evaluate(f, T_dev, T_host_fn, like, stage=None if stage is None else stage[g * n:(g + 1) * n])
+    return torch.stack([evaluate(f, T_dev, T_host_fn, like, stage=None if stage is None else stage[g * n:(g + 1) * n],
+                                 stage_dev=None if stage_dev is None else stage_dev[g * n:(g + 1) * n])
                         for g, f in enumerate(funcs)])

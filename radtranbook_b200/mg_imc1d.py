@@ -26,7 +26,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._gray import GrayState, _host_copy, _pinned, average_tallies, face_temperatures, replica_mean
+from ._gray import GrayState, _host_copy, _staged, average_tallies, face_temperatures, replica_mean
 from .engine import A_RAD, C_LIGHT, Engine
 from .materials import evaluate, evaluate_groups
 from .mg_imc2d import planck_fractions
@@ -143,8 +143,8 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, mesh, energy_
     like = state._T
     host_T = lambda: state.temperature  # noqa: E731
     # host callables' results go up by asynchronous copies from pinned buffers of the state
-    sig = evaluate_groups(sigma_a_funcs, like, host_T, like, stage=_pinned(state, "sigma_g", G * I))  # (G, I)
-    cvv = evaluate(cv, like, host_T, like, stage=_pinned(state, "cv", I))
+    sig = evaluate_groups(sigma_a_funcs, like, host_T, like, **_staged(state, "sigma_g", G * I))  # (G, I)
+    cvv = evaluate(cv, like, host_T, like, **_staged(state, "cv", I))
     Tb = [T_boundary[q](state.time) if callable(T_boundary[q]) else T_boundary[q] for q in range(2)]
     n_side = None
     if particle_budget_fmin > 0.0:
@@ -181,7 +181,7 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, mesh, energy_
     eng.comb_async(Nmax, state.count, state._e, per_group=True, conserve_radiation=(mode == "radiation"))
     if mode == "material":
         state._e.add_(eng.disc.view(G, I).sum(0) / eng.vol)
-    Tn = evaluate(inv_eos, state._e, lambda: _host_copy(state._e), like, stage=_pinned(state, "T_new", I))
+    Tn = evaluate(inv_eos, state._e, lambda: _host_copy(state._e), like, **_staged(state, "T_new", I))
     state._T.copy_(Tn.reshape(-1))
     try:
         sm = eng.fetch(state.host_copies())

@@ -24,7 +24,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._gray import GrayState, _host_copy, _pinned, average_tallies, face_temperatures, replica_mean
+from ._gray import GrayState, _host_copy, _staged, average_tallies, face_temperatures, replica_mean
 from .engine import A_RAD, C_LIGHT, Engine
 from .materials import evaluate, evaluate_groups
 
@@ -192,8 +192,8 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
     host_T = lambda: state.temperature  # noqa: E731
     # host callables' results go up by asynchronous copies from pinned buffers of the state
     sig = evaluate_groups(sigma_a_funcs, like, host_T, like,
-                          stage=_pinned(state, "sigma_g", G * nc)).transpose(1, 2).reshape(G, -1)  # (G, nc)
-    cvv = state.flat(evaluate(cv, like, host_T, like, stage=_pinned(state, "cv", nc)))
+                          **_staged(state, "sigma_g", G * nc)).transpose(1, 2).reshape(G, -1)  # (G, nc)
+    cvv = state.flat(evaluate(cv, like, host_T, like, **_staged(state, "cv", nc)))
     if emission_fractions is not None:
         eng.emission_fractions = torch.as_tensor(np.asarray(emission_fractions, dtype=np.float64), device=eng.device)
     else:
@@ -252,7 +252,7 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
     if conserve_comb_energy:
         state._e.add_(eng.disc.view(G, nc).sum(0) / eng.vol)
     Tn = evaluate(inv_eos, state.grid(state._e), lambda: _host_copy(state.grid(state._e)), like,
-                  stage=_pinned(state, "T_new", nc))
+                  **_staged(state, "T_new", nc))
     state._T.copy_(state.flat(Tn))
     nx, ny = state._shape
 
