@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(CB) k_comb_count(CombArgs a) {
   bins_init(t);
   __syncthreads();
   const long long k = (long long)blockIdx.x * CB + threadIdx.x;
-  const long long n_in = *a.d_n_in;
+  const long long n_in = min((long long)*a.d_n_in, (long long)a.n_bound);  // the grid covers n_bound entries
   const bool compact = *a.mode != 0;
   int n = 0, b = 0;
   if (k < n_in) {
@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(CB) k_comb_scatter(CombArgs a) {
   const long long tile0 = (long long)blockIdx.x * CB;
   const long long k = tile0 + threadIdx.x;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const long long n_in = *a.d_n_in;
+  const long long n_in = min((long long)*a.d_n_in, (long long)a.n_bound);
   const int n = (k < n_in) ? a.cnt[k] : 0;
   // block-inclusive scan of the copy counts
   int x = n;

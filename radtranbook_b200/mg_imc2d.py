@@ -380,19 +380,34 @@ def run_simulation(Ntarget, Nboundary, Nsource, Nmax, Tinit, Tr_init, T_boundary
                    output_freq=1, theta=1.0, use_scalar_intensity_Tr=True, Ntarget_ic=None,
                    conserve_comb_energy=False, geometry="xy", max_events_per_particle=1_000_000,
                    emission_fractions=None, T_emit_floor=0.0, Nmax_growth=0, Nmax_final=None, seed=0x5EED0001):
+    """The time loop of MG_IMC/MG_IMC2D.py:2125-2259: steps of min(dt, time left) until
+    final_time (within max(1e-15, 1e-12 max(final_time, 1))); every output_freq-th step and the
+    last one append the step's info, with 'cumulative_energy_residual' and
+    'net_boundary_energy' added, to the history.  Returns (history, state)."""
     state = init_simulation(Ntarget, Tinit, Tr_init, edges1, edges2, energy_edges, eos, inv_eos,
                             Ntarget_ic=Ntarget_ic, T_emit_floor=T_emit_floor, geometry=geometry, seed=seed)
     history = []
-    while state.time < final_time - 1e-15:
-        step_dt = min(dt, final_time - state.time)
+    t = 0.0
+    step_count = 0
+    cumulative_residual = 0.0
+    time_tol = max(1e-15, 1e-12 * max(final_time, 1.0))
+    while t < final_time - time_tol:
+        step_dt = min(dt, final_time - t)
+        if step_dt <= time_tol:
+            break
         state, info = step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, step_dt, edges1, edges2,
                            energy_edges, sigma_a_funcs, inv_eos, cv, source, reflect=reflect, theta=theta,
                            use_scalar_intensity_Tr=use_scalar_intensity_Tr, conserve_comb_energy=conserve_comb_energy,
                            geometry=geometry, max_events_per_particle=max_events_per_particle,
                            emission_fractions=emission_fractions, T_emit_floor=T_emit_floor,
                            Nmax_growth=Nmax_growth, Nmax_final=Nmax_final)
+        t = state.time
         Nmax = info["Nmax_next"]
-        if (state.count - 1) % output_freq == 0 or (final_time - state.time) < 1e-12:
+        step_count += 1
+        cumulative_residual += info["energy_residual"]
+        if step_count % output_freq == 0 or (final_time - t) < time_tol:
+            info["cumulative_energy_residual"] = cumulative_residual
+            info["net_boundary_energy"] = info["boundary_emission"] - info["boundary_outgoing"]
             history.append(info)
     return history, state
 

@@ -1,7 +1,7 @@
 """Generate the golden fixtures under tests/golden/ from the reference itself.
 
-Run in a container that has the reference checkout (default /root/reference, override with
-RADTRANBOOK_REF); the fixtures it writes are small .npz files committed with this script.
+Run where a reference checkout exists, with its path in the RADTRANBOOK_REF environment
+variable (required); the fixtures it writes are small .npz files committed with this script.
 
   events.npz     the reference's own jitted event functions (IMC/IMC1D.py:75 move_particle,
                  :336 move_particle_spherical, IMC/IMC2D.py:739 _move_particle_xy_jit,
@@ -24,6 +24,10 @@ RADTRANBOOK_REF); the fixtures it writes are small .npz files committed with thi
                  MG_IMC2D.step and MG_IMC1D.step with planck_shim/ standing in for the
                  external planck_integrals; IMC1D_CarterForest.step, IMC2D_CarterForest.step):
                  per-cell mean and standard error of material and radiation temperature
+                 (--stats-only: the slab, RZ and multigroup ones, 32 seeds x 10 steps)
+  loops.json     the run_simulation loops of the six step modules on small problems (output
+                 times, history shapes, info-history times and key trees) and the info key
+                 tree of one step() of each module (--loops-only)
 
 The reference's random numbers cannot be reproduced by a different generator, so whole-step
 parity is statistical; the event, comb and sampler fixtures pin the arithmetic exactly.
@@ -38,7 +42,7 @@ import types
 
 import numpy as np
 
-REF = os.environ.get("RADTRANBOOK_REF", "/root/reference")
+REF = os.environ.get("RADTRANBOOK_REF", "")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -227,7 +231,7 @@ def gen_sources(IMC1D, IMC2D, seed=13):
     return out
 
 
-def run_stats_slab(IMC1D, seeds=32, steps=5):
+def run_stats_slab(IMC1D, seeds=32, steps=10):
     I = 100
     mesh = np.array([[i * 0.002, (i + 1) * 0.002] for i in range(I)])
     cv = 0.3
@@ -250,7 +254,7 @@ def run_stats_slab(IMC1D, seeds=32, steps=5):
                 NMax=8000, dt=0.01)
 
 
-def run_stats_rz(IMC2D, seeds=16, steps=3):
+def run_stats_rz(IMC2D, seeds=32, steps=10):
     nr, nz = 30, 105
     r_e = np.linspace(0, 2, nr + 1); z_e = np.linspace(0, 7, nz + 1)
     rc = 0.5 * (r_e[:-1] + r_e[1:]); zc = 0.5 * (z_e[:-1] + z_e[1:])
@@ -276,7 +280,7 @@ def run_stats_rz(IMC2D, seeds=16, steps=3):
                 Tr_se=Trs.std(0, ddof=1) / np.sqrt(seeds), seeds=seeds, steps=steps, nr=nr, nz=nz)
 
 
-MG = dict(nx=40, L=0.5, G=10, cv=0.3, T0=0.001, dt=0.005, steps=3, Ntarget=4000, Nboundary=2000, Nmax=12000)
+MG = dict(nx=40, L=0.5, G=10, cv=0.3, T0=0.001, dt=0.005, steps=10, Ntarget=4000, Nboundary=2000, Nmax=12000)
 
 
 def mg_setup():
@@ -311,7 +315,7 @@ def gen_planck_sampler(MG_IMC2D, n=3000, seed=17):
     return dict(planck_in=np.array(rows), planck_group=np.array(res), planck_edges=edges)
 
 
-def run_stats_mg(MG_IMC2D, seeds=16):
+def run_stats_mg(MG_IMC2D, seeds=32):
     edges, nu, funcs = mg_setup()
     nx = MG["nx"]
     x_e = np.linspace(0, MG["L"], nx + 1); y_e = np.array([0.0, 1.0])
@@ -642,11 +646,143 @@ def main_cf():
         print(f"Carter-Forest statistics written ({time.time() - t0:.1f} s)")
 
 
+def key_tree(d):
+    """Nested key structure of an info dict: {key: subtree or None}."""
+    return {k: (key_tree(v) if isinstance(v, dict) else None) for k, v in d.items()}
+
+
+# small problems for the time-loop fixtures: final_time is not a multiple of dt, so every loop
+# ends with a short step, and output_freq = 3 exercises the output cadence
+LOOP = dict(dt=0.01, final_time=0.075, output_freq=3, N=300, Nmax=1000, T0=0.01, cv=0.3)
+
+
+def gen_loops():
+    """The reference's run_simulation loops (IMC/IMC1D.py:1127, IMC/IMC2D.py:1900,
+    MG_IMC/MG_IMC2D.py:2125, MG_IMC/MG_IMC1D.py:1312, IMC/IMC1D_CarterForest.py:1381,
+    IMC/IMC2D_CarterForest.py:1162) on small problems: output times, history shapes and, for
+    the loops that return info dicts, their times and key trees; plus the info key tree of one
+    step() of every module."""
+    IMC1D, IMC2D = load_reference()
+    MG2 = load_reference_mg()
+    MG1 = load_reference_mg1d()
+    CF1, CF2 = load_reference_cf()
+    L = LOOP
+    cv, N, Nmax, dt, tf, of = L["cv"], L["N"], L["Nmax"], L["dt"], L["final_time"], L["output_freq"]
+    eos, inv = (lambda T: cv * T), (lambda e: e / cv)
+    cvf = lambda T: cv + 0 * T  # noqa: E731
+    sig = lambda T: 10.0 + 0 * T  # noqa: E731
+    I = 10
+    mesh = np.array([[i * 0.01, (i + 1) * 0.01] for i in range(I)])
+    x_e, y_e = np.linspace(0, 0.06, 7), np.linspace(0, 0.05, 6)
+    r_e, z_e = np.linspace(0, 0.06, 7), np.linspace(0, 0.05, 6)
+    m_e, m_y = np.linspace(0, 0.06, 7), np.array([0.0, 1.0])
+    gedges = np.array([1e-2, 0.3, 2.0, 20.0])
+    gsig = [lambda T, k=k: (5.0 + 0 * T) * k for k in (1.0, 2.0, 4.0)]
+    out = {"problem": L}
+    T1 = np.full(I, L["T0"])
+
+    def hist(times, Tr, T):
+        return {"times": [float(t) for t in times], "Tr_shape": list(np.shape(Tr)), "T_shape": list(np.shape(T))}
+
+    seed_py, seed_np, _, _ = nb_helpers()
+
+    def seed(s):
+        np.random.seed(s); random.seed(s); seed_py(s); seed_np(s)
+
+    seed(1)
+    out["imc1d"] = hist(*IMC1D.run_simulation(N, N, 0, Nmax, T1, T1, (1.0, 0.0), dt, mesh, sig, eos, inv, cvf,
+                                              np.zeros(I), tf, output_freq=of))
+    st = IMC1D.init_simulation(N, T1, T1, mesh, eos, inv)
+    _, info = IMC1D.step(st, N, N, 0, Nmax, (1.0, 0.0), dt, mesh, sig, inv, cvf, np.zeros(I))
+    out["imc1d"]["info_keys"] = key_tree(info)
+    for geo, e1, e2 in (("xy", x_e, y_e), ("rz", r_e, z_e)):
+        T2 = np.full((len(e1) - 1, len(e2) - 1), L["T0"])
+        seed(2)
+        out[f"imc2d_{geo}"] = hist(*IMC2D.run_simulation(N, N, 0, Nmax, T2, T2, (1.0, 0.0, 0.0, 0.0), dt, e1, e2, sig,
+                                                         eos, inv, cvf, np.zeros_like(T2), tf, output_freq=of,
+                                                         geometry=geo))
+        st = IMC2D.init_simulation(N, T2, T2, e1, e2, eos, inv, geometry=geo)
+        _, info = IMC2D.step(st, N, N, 0, Nmax, (1.0, 0.0, 0.0, 0.0), dt, e1, e2, sig, inv, cvf, np.zeros_like(T2),
+                             geometry=geo)
+        out[f"imc2d_{geo}"]["info_keys"] = key_tree(info)
+        seed(3)
+        out[f"imc2d_cf_{geo}"] = hist(*CF2.run_simulation(N, N, 0, Nmax, T2, T2, (1.0, 0.0, 0.0, 0.0), dt, e1, e2, sig,
+                                                          eos, inv, cvf, np.zeros_like(T2), tf, output_freq=of,
+                                                          geometry=geo))
+        st = CF2.init_simulation(N, T2, T2, e1, e2, eos, inv, geometry=geo)
+        _, info = CF2.step(st, N, N, 0, Nmax, (1.0, 0.0, 0.0, 0.0), dt, e1, e2, sig, inv, cvf, np.zeros_like(T2),
+                           geometry=geo)
+        out[f"imc2d_cf_{geo}"]["info_keys"] = key_tree(info)
+    seed(4)
+    out["imc1d_cf"] = hist(*CF1.run_simulation(N, N, 0, Nmax, T1, T1, (1.0, 0.0), dt, mesh, sig, eos, inv, cvf,
+                                               np.zeros(I), tf, output_freq=of))
+    st = CF1.init_simulation(N, T1, T1, mesh, eos, inv)
+    _, info = CF1.step(st, N, N, 0, Nmax, (1.0, 0.0), dt, mesh, sig, inv, cvf, np.zeros(I))
+    out["imc1d_cf"]["info_keys"] = key_tree(info)
+    # multigroup 2-D (xy strip, reflecting in y): (history, state)
+    Tm = np.full((len(m_e) - 1, 1), L["T0"])
+    seed(5)
+    history, _ = MG2.run_simulation(N, N, 0, Nmax, Tm, Tm, (1.0, 0.0, 0.0, 0.0), dt, m_e, m_y, gedges, gsig, eos, inv,
+                                    cvf, np.zeros_like(Tm), tf, reflect=(False, False, True, True), output_freq=of)
+    out["mg_imc2d"] = {"history_times": [float(h["time"]) for h in history],
+                       "history_keys": key_tree(history[-1]), "info_keys": None}
+    st = MG2.init_simulation(N, Tm, Tm, m_e, m_y, gedges, eos, inv)
+    _, info = MG2.step(st, N, N, 0, Nmax, (1.0, 0.0, 0.0, 0.0), dt, m_e, m_y, gedges, gsig, inv, cvf,
+                       np.zeros_like(Tm), reflect=(False, False, True, True))
+    out["mg_imc2d"]["info_keys"] = key_tree(info)
+    # multigroup sphere: (times, Tr_hist, T_hist, state, history)
+    Ts = np.full(6, L["T0"])
+    smesh = np.array([[i * 0.01, (i + 1) * 0.01] for i in range(6)])
+    seed(6)
+    times, Tr, T, _, history = MG1.run_simulation(N, N, 0, Nmax, Ts, Ts, (0.0, 1.0), dt, smesh, gedges, gsig, eos,
+                                                  inv, cvf, np.zeros(6), tf, output_freq=of)
+    out["mg_imc1d"] = hist(times, Tr, T)
+    out["mg_imc1d"]["history_times"] = [float(h["time"]) for h in history]
+    st = MG1.init_simulation(N, Ts, Ts, smesh, gedges, eos, inv)
+    _, info = MG1.step(st, N, N, 0, Nmax, (0.0, 1.0), dt, smesh, gedges, gsig, inv, cvf, np.zeros(6))
+    out["mg_imc1d"]["info_keys"] = key_tree(info)
+    return out
+
+
+def main_stats():
+    """Only the multi-seed statistics of the gray slab, RZ crooked pipe and multigroup steps."""
+    import contextlib
+    import io
+
+    t0 = time.time()
+    IMC1D, IMC2D = load_reference()
+    for name, fn in (("stats_slab.npz", lambda: run_stats_slab(IMC1D)), ("stats_rz.npz", lambda: run_stats_rz(IMC2D)),
+                     ("stats_mg.npz", lambda: run_stats_mg(load_reference_mg()))):
+        with contextlib.redirect_stdout(io.StringIO()):
+            s = fn()
+        np.savez_compressed(os.path.join(HERE, name), **s)
+        print(f"{name} written ({time.time() - t0:.1f} s)", flush=True)
+
+
+def main_loops():
+    import contextlib
+    import io
+    import json
+
+    t0 = time.time()
+    with contextlib.redirect_stdout(io.StringIO()):
+        loops = gen_loops()
+    with open(os.path.join(HERE, "loops.json"), "w") as f:
+        json.dump(loops, f, indent=1, sort_keys=True)
+    print(f"time-loop fixtures written ({time.time() - t0:.1f} s)")
+
+
 def main():
+    if not REF or not os.path.isdir(REF):
+        raise SystemExit("set RADTRANBOOK_REF to the reference checkout")
     if "--mg1d-only" in sys.argv:
         return main_mg1d()
     if "--cf-only" in sys.argv:
         return main_cf()
+    if "--loops-only" in sys.argv:
+        return main_loops()
+    if "--stats-only" in sys.argv:
+        return main_stats()
     t0 = time.time()
     IMC1D, IMC2D = load_reference()
     import contextlib

@@ -3,8 +3,9 @@ generator ran through the reference (tests/golden/make_golden.py: run_stats_slab
 run_stats_rz), expressed for the oracle and for the GPU drop-in API."""
 import numpy as np
 
-SLAB = dict(I=100, dx=0.002, cv=0.3, Ntarget=2000, Nboundary=2000, NMax=8000, dt=0.01, steps=5, T0=0.001)
-RZ = dict(nr=30, nz=105, Ntarget=6000, Nboundary=3000, Nmax=30000, dt=0.01, steps=3, T0=0.05)
+# the number of steps of each run is read from its fixture ("steps")
+SLAB = dict(I=100, dx=0.002, cv=0.3, Ntarget=2000, Nboundary=2000, NMax=8000, dt=0.01, T0=0.001)
+RZ = dict(nr=30, nz=105, Ntarget=6000, Nboundary=3000, Nmax=30000, dt=0.01, T0=0.05)
 
 
 def slab_mesh():

@@ -77,6 +77,7 @@ def test_multigroup_matches_reference_statistically():
         pytest.skip("stats_mg.npz not generated")
     ref = np.load(path)
     d, edges, nu = _mg_problem()
+    d["steps"] = int(ref["steps"])
     seeds = int(ref["seeds"])
     Ts = np.array([_run_oracle_mg(3000 + s, d, edges, nu)[0] for s in range(seeds)])
     m, se = Ts.mean(0), Ts.std(0, ddof=1) / np.sqrt(seeds)

@@ -26,7 +26,7 @@ def test_slab_marshak_matches_reference_statistically():
     for s in range(seeds):
         run = O.OracleGray("slab", e, [0.0, 1.0], np.diff(e), 1000 + s, S["Ntarget"], np.full(S["I"], S["T0"]),
                            np.full(S["I"], S["T0"]), lambda T: cv * T, lambda u: u / cv, nthreads=2)
-        for _ in range(S["steps"]):
+        for _ in range(int(ref["steps"])):
             run.step(S["Ntarget"], S["Nboundary"], 0, S["NMax"], [np.array([1.0]), None], S["dt"],
                      lambda T: 300.0 * T ** -3, lambda u: u / cv, lambda T: np.full_like(T, cv))
         Ts.append(run.T.copy())
@@ -46,7 +46,7 @@ def test_rz_crooked_pipe_matches_reference_statistically():
     for s in range(seeds):
         run = O.OracleGray("rz", r_e, z_e, vol, 2000 + s, R["Ntarget"], np.full(sig.shape, R["T0"]),
                            np.full(sig.shape, R["T0"]), lambda T: cvg * T, lambda u: u / cvg, nthreads=4)
-        for _ in range(R["steps"]):
+        for _ in range(int(ref["steps"])):
             run.step(R["Ntarget"], R["Nboundary"], 0, R["Nmax"], [None, None, face, None], R["dt"],
                      lambda T: sig.copy(), lambda u: u / cvg, lambda T: cvg.copy(),
                      reflect=(True, False, False, False), max_events=1_000_000)
