@@ -124,13 +124,21 @@ typedef struct imc_step_params {
   int64_t n_boundary_side[4];   /* > 0: boundary particles on that side instead of n_boundary
                                    (per-side budgets, MG_IMC/MG_IMC1D.py:1000-1040) */
   int32_t method;               /* IMC_METHOD_FLECK_CUMMINGS or IMC_METHOD_CARTER_FOREST (gray) */
-  int32_t pad_method;
+  uint32_t id_base;             /* Philox particle-id offset: the k-th source particle of each kind
+                                   and the k-th bank entry draw with particle id id_base + k.  0 for
+                                   a single process; the ranks of a partitioned step (each tracks
+                                   its share of the particles, IMC/IMC2DMPI.py:172-175) take
+                                   disjoint id ranges so their histories are independent */
   double cf_fastpath;           /* Carter-Forest stiff fast path: when rate * t_left exceeds it,
                                    capture with probability exp(-rate t_left) (0 = off) */
   const uint32_t* step_dev;     /* DEVICE pointer or NULL: when set, every kernel of the step reads
                                    the Philox step counter from it at run time instead of `step` */
   const double* dt_dev;         /* DEVICE pointer or NULL: likewise for dt.  With both set, a
                                    captured step is replayed (CUDA graph) for any step and dt. */
+  double energy_share;          /* fraction of the step's source energy (emission, fixed source,
+                                   boundary faces) this call issues; 0 or 1 = all of it.  A rank of a
+                                   partitioned step issues 1/ranks of it with its share of the
+                                   particles, so the ranks' sources together carry the energy once */
 } imc_step_params;
 
 /* Carter-Forest (IMC/IMC1D_CarterForest.py, IMC/IMC2D_CarterForest.py): no Fleck factor;

@@ -135,36 +135,15 @@ def _host_copy(t: torch.Tensor) -> np.ndarray:
     return a
 
 
-def allreduce_mean(dist, tensors: list) -> None:
-    """Replace every tensor by its mean over the ranks, with one all-reduce of their
-    concatenation (the replicas' only data exchange)."""
-    world = dist.get_world_size()
-    if world == 1:
-        return
-    sizes = [t.numel() for t in tensors]
-    buf = torch.cat([t.reshape(-1) for t in tensors])
-    dist.all_reduce(buf)
-    buf /= world
-    o = 0
-    for t, n in zip(tensors, sizes):
-        t.copy_(buf[o:o + n].view_as(t))
-        o += n
+def check_partition(eng: Engine, dist) -> tuple[int, int]:
+    """(rank, world) of a partitioned step; the state must have been initialised for it."""
+    from .partition import world_of
 
-
-def replica_mean(dist, values: list, device) -> list:
-    """Mean over the ranks of a few FP64 scalars (one all-reduce)."""
-    world = dist.get_world_size()
-    if world == 1:
-        return [float(v) for v in values]
-    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
-    dist.all_reduce(t)
-    return [float(x) / world for x in t.cpu()]
-
-
-def average_tallies(dist, eng: Engine) -> None:
-    """Mean over ranks of the deposition and intensity tallies, before the material update,
-    so every replica applies the same material state."""
-    allreduce_mean(dist, [eng.dep, eng.si])
+    rank, world = world_of(dist)
+    if (eng.rank, eng.world) != (rank, world):
+        raise ValueError("the state was initialised for rank %d of %d, the step runs as rank %d of %d "
+                         "(pass the same _allreduce to init_simulation)" % (eng.rank, eng.world, rank, world))
+    return rank, world
 
 
 def face_temperatures(dim: int, geometry: str, T_boundary, time_now: float, e1: np.ndarray, e2: np.ndarray,
@@ -214,12 +193,22 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
     callables the host synchronises once, at the end (sizes, energies and statistics come
     back in one device summary).
 
-    allreduce: a torch.distributed module when each rank runs an independent replica of the
-    problem (its own Philox key and full particle counts); the per-cell tallies and escaped
-    energy are averaged over ranks with one all-reduce before the material update, so every
-    rank holds the same material state (a replica-averaged estimate, N x the histories)."""
+    allreduce: a torch.distributed module for a particle-partitioned step (the process
+    parallelism of IMC/IMC1DMPI.py and IMC/IMC2DMPI.py, radtranbook_b200.partition): Ntarget,
+    Nboundary, Nsource and Nmax are totals, each rank tracks its share with its own Philox id
+    range and 1/world of the source energy, the per-cell deposition, intensity and emission
+    are summed over the ranks before the material update (so every rank holds the same
+    material state), each rank combs its census to its share of Nmax, and the ledger terms
+    are summed.  The state must come from init_simulation with the same allreduce."""
+    from .partition import local_count, sum_tensors, summary_totals
+
     t_step_start = _time.perf_counter()
     eng: Engine = state._engine
+    rank, world = check_partition(eng, allreduce)
+    dist = allreduce if world > 1 else None
+    if world > 1:
+        Ntarget, Nboundary, Nsource = (local_count(n, rank, world) for n in (Ntarget, Nboundary, Nsource))
+        Nmax = local_count(Nmax, rank, world) if Nmax > 0 else Nmax
     dim = state._dim
     like = state.grid(state._T)
     host_T = lambda: state.temperature  # noqa: E731
@@ -244,10 +233,8 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
                         refl, max_events=max_events, rz_linear_source=rz_linear_source, t_emit_floor=T_emit_floor,
                         method=_lib.METHOD_CARTER_FOREST if method == "cf" else _lib.METHOD_FLECK_CUMMINGS,
                         cf_fastpath=cf_fastpath)
-    world = 1
-    if allreduce is not None:
-        world = allreduce.get_world_size()
-        average_tallies(allreduce, eng)
+    # partition: the per-cell tallies of all ranks (the step's only data exchange)
+    sum_tensors(dist, [eng.dep, eng.si, eng.emitted])
 
     # material update: e += dep - emitted/V ; Tr from the path-length intensity.  The comb
     # does not need T: with a host inv_eos (and the comb discrepancy not booked into e), e is
@@ -261,6 +248,7 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
         e_ready.record()
     eng.comb_async(Nmax, state.count, state._e)
     if conserve_comb_energy:
+        sum_tensors(dist, [eng.disc])
         state._e.add_(eng.disc[: eng.nc] / eng.vol)
     if e_ready is not None:
         def e_host():
@@ -283,23 +271,24 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
         live = pre_comb.view("weight") > 0
         rad_c = torch.zeros(eng.nc, dtype=torch.float64, device=eng.device)
         rad_c.index_add_(0, pre_comb.view("cell")[live].long(), pre_comb.view("weight")[live].double())
+        sum_tensors(dist, [rad_c])
         state._Tr.copy_(torch.pow(rad_c / eng.vol / A_RAD, 0.25))
-    internal = float(sm.internal_energy)
-    rad = float(sm.comb_after)
-    comb_disc = float(sm.comb_before) - rad
-    boundary_emission = float(sum(sm.e_side))
-    boundary_loss = float(sum(sm.escaped))
-    stats = np.array(sm.stats[:], dtype=np.int64)
+    internal = float(sm.internal_energy)  # the same material state on every rank
+    # ledger terms and counts (summed over the ranks of a partition)
+    tot = summary_totals(dist, sm, eng.bank.size, eng.device)
+    rad, stats = tot["rad"], tot["stats"]
+    comb_disc = tot["comb_before"] - rad
+    boundary_emission, boundary_loss = float(tot["e_side"].sum()), float(tot["escaped"].sum())
+    source_emission, emission_total, weight_sum = tot["source_emission"], tot["emission_total"], tot["weight_sum"]
+    n_particles, n_tr = tot["n_particles"], tot["n_bank"]
     if conserve_comb_energy:
         internal += comb_disc
-    if allreduce is not None and world > 1:
-        rad, comb_disc, boundary_loss = replica_mean(allreduce, [rad, comb_disc, boundary_loss], eng.device)
     if not use_scalar_intensity_Tr:
         state.refresh_host()
     else:
         state.take_host_copies()
     total = internal + rad
-    energy_loss = total - state.previous_total_energy - boundary_emission + boundary_loss - float(sm.source_emission)
+    energy_loss = total - state.previous_total_energy - boundary_emission + boundary_loss - source_emission
     closure = energy_loss + (0.0 if conserve_comb_energy else comb_disc)
     state.time = state.time + dt
     state.previous_total_energy = total
@@ -307,26 +296,26 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
     t_end = _time.perf_counter()
     ms_src, ms_tr = eng.phase_times()
 
-    n_tr = int(sm.n_bank)
+    n_tr = int(n_tr)
     ev = int(stats[_lib.STAT_EVENTS])
     info = {
         "time": state.time,
         "radiation_temperature": state.radiation_temperature,
         "temperature": state.temperature,
-        "N_particles": int(eng.bank.size),
+        "N_particles": int(n_particles),
         "total_energy": total,
         "total_internal_energy": internal,
         "total_radiation_energy": rad,
         "boundary_emission": boundary_emission,
         "boundary_loss": boundary_loss,
-        "source_emission": float(sm.source_emission),
+        "source_emission": source_emission,
         "energy_loss": energy_loss,
         "ledger": {
             "comb_discrepancy": comb_disc,
             "closure": closure,
             "relative_closure": closure / max(abs(total), 1e-300),
-            "emission": float(sm.emission_total),
-            "weight_floor": 1e-10 * float(sm.weight_sum) / max(n_tr, 1),
+            "emission": emission_total,
+            "weight_floor": 1e-10 * weight_sum / max(n_tr, 1),
         },
         "profiling": {
             "phase_times_s": {
@@ -375,7 +364,16 @@ def tune(state: GrayState, grid: dict | None = None, repeats: int = 2) -> dict:
 
 
 def init_state(engine: Engine, dim: int, shape: tuple, Ntarget, Tinit, Tr_init, eos, inv_eos, Ntarget_ic,
-               T_emit_floor=0.0) -> GrayState:
+               T_emit_floor=0.0, dist=None) -> GrayState:
+    """State at t = 0 with the equilibrium initial census.  dist: a torch.distributed module
+    for a particle-partitioned run (each rank holds its share of the initial census, with
+    1/world of its energy; radiation temperature and energy from the summed census)."""
+    from .partition import local_count, sum_scalars, sum_tensors, world_of
+
+    rank, world = world_of(dist)
+    if world > 1:
+        engine.partition(rank, world)
+    dist = dist if world > 1 else None
     dev = engine.device
     Tg = torch.as_tensor(np.asarray(Tinit, dtype=np.float64), device=dev)
     Trg = torch.as_tensor(np.asarray(Tr_init, dtype=np.float64), device=dev)
@@ -388,12 +386,14 @@ def init_state(engine: Engine, dim: int, shape: tuple, Ntarget, Tinit, Tr_init, 
     back = evaluate(inv_eos, state.grid(state._e), lambda: state.grid(state._e).cpu().numpy(), Tg)
     assert torch.allclose(back, Tg), "Inverse EOS failed"
     N_ic = Ntarget if Ntarget_ic is None else Ntarget_ic
-    engine.init_census(state.flat(Trg), int(N_ic), T_emit_floor)
+    engine.init_census(state.flat(Trg), local_count(N_ic, rank, world), T_emit_floor)
     rad_cell = torch.zeros(engine.nc, dtype=torch.float64, device=dev)
     if engine.bank.size:
         rad_cell.index_add_(0, engine.bank.view("cell").long(), engine.bank.view("weight").double())
+    sum_tensors(dist, [rad_cell])
     state._Tr.copy_(torch.pow(rad_cell / engine.vol / A_RAD, 0.25))
     rad, internal = engine.energy_totals(state._e)
+    rad = sum_scalars(dist, [rad], dev)[0]
     state.previous_total_energy = internal + rad
     state.refresh_host()
     return state

@@ -68,8 +68,8 @@ class ImcStepParams(ctypes.Structure):
         ("block_size", c_int32), ("blocks_per_sm", c_int32), ("chunk", c_int32), ("reserved", c_int32),
         ("emission_fractions", c_void_p),
         ("n_boundary_side", c_int64 * 4),
-        ("method", c_int32), ("pad_method", c_int32), ("cf_fastpath", c_double),
-        ("step_dev", c_void_p), ("dt_dev", c_void_p),
+        ("method", c_int32), ("id_base", c_uint32), ("cf_fastpath", c_double),
+        ("step_dev", c_void_p), ("dt_dev", c_void_p), ("energy_share", c_double),
     ]
 
 

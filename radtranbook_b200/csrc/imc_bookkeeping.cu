@@ -70,7 +70,7 @@ __global__ void k_plan_cells(PlanArgs a) {
       E = decays ? A_RAD * T4 * -expm1(-rate * dt) / beta * a.vol[c] : A_RAD * T4 * C_LIGHT * sig * dt * a.vol[c];
     }
     if (a.t_emit_floor > 0.0 && T < a.t_emit_floor) E = 0.0;
-    a.emit_E[c] = E;
+    a.emit_E[c] = E * a.share;  // a rank of a partitioned step issues its share
   }
   // ---- tilt constants (emission; fixed-source RZ tilt uses the same T) ----
   {
@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(NT) k_plan(PlanArgs a) {
     double smax = 0.0;
     for (int c = t; c < nc; c += NT) {
       smax = fmax(smax, a.source[c]);
-      a.src_QV[c] = a.source[c] * dt * a.vol[c];
+      a.src_QV[c] = a.source[c] * dt * a.vol[c] * a.share;
     }
     red[t] = smax;
     __syncthreads();
@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(NT) k_plan(PlanArgs a) {
           else area = PI * (a.e1[q + 1] * a.e1[q + 1] - a.e1[q] * a.e1[q]);
         }
         const double T = Tf[q];
-        Ef[q] = (T > 0.0) ? A_RAD * C_LIGHT * T * T * T * T / 4.0 * area * dt : 0.0;
+        Ef[q] = (T > 0.0) ? A_RAD * C_LIGHT * T * T * T * T / 4.0 * area * dt * a.share : 0.0;
         Et += Ef[q];
         cdf[q] = Et;
       }
@@ -433,7 +433,7 @@ __global__ void k_plan_mg_cells(PlanMgArgs a) {
     double f = 1.0 / (1.0 + a.theta * beta * sp * C_LIGHT * dt);
     f = fmin(1.0, fmax(0.0, f));
     const double aT4 = (a.t_emit_floor > 0.0 && T < a.t_emit_floor) ? 0.0
-                                                                      : A_RAD * C_LIGHT * pow4(T) * dt * a.vol[c];
+                                                                      : A_RAD * C_LIGHT * pow4(T) * dt * a.vol[c] * a.share;
     double run = 0.0;
     for (int g = 0; g < G; ++g) {
       const size_t q = (size_t)g * nc + c;
@@ -453,7 +453,7 @@ __global__ void k_plan_mg_cells(PlanMgArgs a) {
     for (int c = t0; c < nc; c += stride) {
       double run = 0.0;
       for (int g = 0; g < G; ++g) {
-        run += a.source[(size_t)g * nc + c] * a.vol[c] * dt;
+        run += a.source[(size_t)g * nc + c] * a.vol[c] * dt * a.share;
         a.Sgc[(size_t)c * G + g] = run;
       }
       a.Sc[c] = run;
@@ -510,7 +510,7 @@ __global__ void __launch_bounds__(NT) k_plan_mg(PlanMgArgs a) {
         else if (along2) { const double R = side == 0 ? a.e1[0] : a.e1[a.nx]; area = 2.0 * PI * R * (a.e2[q + 1] - a.e2[q]); }
         else area = PI * (a.e1[q + 1] * a.e1[q + 1] - a.e1[q] * a.e1[q]);
         const double T = Tf[q];
-        Ef[q] = (T > 0.0) ? A_RAD * C_LIGHT * T * T * T * T / 4.0 * area * dt : 0.0;
+        Ef[q] = (T > 0.0) ? A_RAD * C_LIGHT * T * T * T * T / 4.0 * area * dt * a.share : 0.0;
         Et += Ef[q];
         cdf[q] = Et;
       }
@@ -580,7 +580,7 @@ __global__ void k_plan_mg1d_cells(PlanMgArgs a) {
       a.sass[q] = make_float2((float)sa, (float)ss);
       // MG_IMC/MG_IMC1D.py:346-350: path-length estimator below sigma_a = 1e-10
       a.cellf[q] = make_double2(1.0 / a.vol[c], sa > 1e-10 ? 1.0 / (sa * a.vol[c] * dt) : -1.0 / (a.vol[c] * dt));
-      a.emit_E[q] = cold ? 0.0 : A_RAD * C_LIGHT * pow4(T) * sa * b[g] * dt * a.vol[c];
+      a.emit_E[q] = cold ? 0.0 : A_RAD * C_LIGHT * pow4(T) * sa * b[g] * dt * a.vol[c] * a.share;
     }
   }
 }
@@ -617,7 +617,7 @@ __global__ void __launch_bounds__(NT) k_plan_mg1d(PlanMgArgs a) {
     double smax = 0.0;
     for (int q = t; q < ncg; q += NT) {
       smax = fmax(smax, a.source[q]);
-      a.src_QV[q] = a.source[q] * a.vol[q % nc] * dt;
+      a.src_QV[q] = a.source[q] * a.vol[q % nc] * dt * a.share;
     }
     red[t] = smax;
     __syncthreads();
@@ -650,7 +650,7 @@ __global__ void __launch_bounds__(NT) k_plan_mg1d(PlanMgArgs a) {
       double* cdf = a.face + (size_t)(side * 2 + 1) * a.nf;
       const double R = side == 0 ? a.e1[0] : a.e1[a.nx];
       const double T = Tf[0];
-      const double E = (T > 0.0) ? A_RAD * C_LIGHT * T * T * T * T / 4.0 * (4.0 * PI * R * R) * dt : 0.0;
+      const double E = (T > 0.0) ? A_RAD * C_LIGHT * T * T * T * T / 4.0 * (4.0 * PI * R * R) * dt * a.share : 0.0;
       Ef[0] = E;
       cdf[0] = E;
       if (E > 0.0) {

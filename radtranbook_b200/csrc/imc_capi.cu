@@ -113,6 +113,8 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   if (mg && (!tal->escaped_group || !tal->boundary_group)) return IMC_ERR_INVALID_ARG;
   if (!bank_ok(bank, two_d, mg) || !workspace) return IMC_ERR_INVALID_ARG;
   if (!(par->dt > 0.0) || par->n_target < 0 || par->n_boundary < 0 || par->n_source < 0) return IMC_ERR_INVALID_ARG;
+  if (!(par->energy_share >= 0.0 && par->energy_share <= 1.0)) return IMC_ERR_INVALID_ARG;
+  const double share = par->energy_share > 0.0 ? par->energy_share : 1.0;
   for (int q = 0; q < 4; ++q) if (par->n_boundary_side[q] < 0) return IMC_ERR_INVALID_ARG;
   const bool cf = par->method == IMC_METHOD_CARTER_FOREST;
   if (par->method != IMC_METHOD_FLECK_CUMMINGS && !cf) return IMC_ERR_INVALID_ARG;
@@ -140,6 +142,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   pa.rz_linear = par->rz_linear_source; pa.t_emit_floor = par->t_emit_floor;
   pa.method = par->method; pa.cf_rate = ws_ptr<float>(workspace, L.cf_rate);
   pa.dt_dev = par->dt_dev;
+  pa.share = share;
   pa.sa = tal->sigma_a; pa.ss = tal->sigma_s;
   pa.sass = ws_ptr<float2>(workspace, L.sass); pa.cellf = ws_ptr<double2>(workspace, L.cellf);
   pa.e1f = ws_ptr<float>(workspace, L.e1f); pa.e2f = ws_ptr<float>(workspace, L.e2f);
@@ -178,6 +181,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     pm.src_issued = pa.src_issued;
     pm.sum = sum;
     pm.dt_dev = par->dt_dev;
+    pm.share = share;
     IMC_CUDA(imc_launch_plan_mg1d(pm, s));
   } else {
     IMC_CUDA(cudaMemsetAsync(tal->boundary_group, 0, sizeof(double) * ng, s));
@@ -201,6 +205,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     pm.mixcdf = ws_ptr<double>(workspace, L.mixcdf);
     pm.sum = sum;
     pm.dt_dev = par->dt_dev;
+    pm.share = share;
     IMC_CUDA(imc_launch_plan_mg(pm, s));
   }
 
@@ -228,6 +233,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     ba.mixcdf = ws_ptr<double>(workspace, L.mixcdf); ba.boundary_group = tal->boundary_group;
     ba.below_last = mg1 ? 1 : 0;
     ba.dt_dev = par->dt_dev; ba.step_dev = par->step_dev;
+    ba.id_base = par->id_base;
     IMC_CUDA(imc_launch_fill_boundary(ba, s));
   }
   const int nbins = mg1 ? nc * ng : nc;  // source order positions (MG 1-D: (group, cell) bins)
@@ -238,6 +244,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     fa.geom = mesh->geometry; fa.nx = mesh->nx; fa.ny = mesh->ny; fa.nc = nc;
     fa.nbins = nbins; fa.bins_by_group = mg1 ? 1 : 0;
     fa.time_scale_dev = par->dt_dev; fa.step_dev = par->step_dev;
+    fa.id_base = par->id_base;
     fa.e1 = mesh->edges1; fa.e2 = mesh->edges2; fa.T = mat->temperature;
     fa.d_n = d_n; fa.d_base = d_base; fa.n_bound = n_bound;
     fa.off = off; fa.w = w; fa.tilt = tilt; fa.tilt_kind = kind;
@@ -261,6 +268,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     fm.p1 = bank->pos1; fm.p2 = p2; fm.d1 = bank->dir1; fm.d2 = d2; fm.wb = bank->weight;
     fm.t = bank->time; fm.cell = bank->cell; fm.group = bank->group;
     fm.time_scale_dev = par->dt_dev; fm.step_dev = par->step_dev;
+    fm.id_base = par->id_base;
     return imc_launch_fill_mg(fm, s);
   };
   const bool rzlin = mesh->geometry == IMC_GEOM_RZ && par->rz_linear_source;
@@ -314,6 +322,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   ta.cf_rate = cf ? pa.cf_rate : nullptr;
   ta.cf_fastpath = (float)par->cf_fastpath;
   ta.dt_dev = par->dt_dev; ta.step_dev = par->step_dev;
+  ta.id_base = par->id_base;
   int rm = 0;
   for (int q = 0; q < 4; ++q) if (par->reflect[q]) rm |= 1 << q;
   ta.reflect_mask = rm;

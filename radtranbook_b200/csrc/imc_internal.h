@@ -46,6 +46,7 @@ struct TrackArgs {
   float cf_fastpath;         // Carter-Forest stiff fast-path threshold (0 = off)
   const double* dt_dev;      // non-NULL: the step length is read from device memory (graph replay)
   const uint32_t* step_dev;  // non-NULL: the Philox step counter is read from device memory
+  uint32_t id_base;          // Philox particle id of bank entry k is id_base + k
 };
 
 cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool smem_cells, cudaStream_t s);
@@ -114,6 +115,7 @@ struct PlanArgs {
   int method;                      // IMC_METHOD_*
   float* cf_rate;                  // Carter-Forest: [c] re-emission rate (tilt[4c+3]: emission rate)
   const double* dt_dev;            // non-NULL: dt read from device memory (graph replay)
+  double share;                    // fraction of the source energy issued (1: all of it)
   // outputs
   double* sa; double* ss;          // FP64 [ncg]
   float2* sass;                    // FP32 [ncg]
@@ -189,6 +191,7 @@ struct FillArgs {
   // when k > cf_thr (else uniform); NULL otherwise
   const double* cf_rate4; double cf_thr;
   const double* time_scale_dev; const uint32_t* step_dev;  // non-NULL: read from device memory
+  uint32_t id_base;            // Philox particle id of source particle k is id_base + k
 };
 cudaError_t imc_launch_fill_volume(const FillArgs& a, cudaStream_t s);
 
@@ -206,6 +209,7 @@ struct BndArgs {
   int ng; const double* faceT; const double* gedges; const double* mixcdf; double* boundary_group;
   int below_last;              // MG 1-D: an energy below the lowest edge goes to the last group
   const double* dt_dev; const uint32_t* step_dev;  // non-NULL: read from device memory
+  uint32_t id_base;            // Philox particle id of face particle k is id_base + k
 };
 cudaError_t imc_launch_fill_boundary(const BndArgs& a, cudaStream_t s);
 
@@ -264,6 +268,7 @@ struct PlanMgArgs {
   double* emit_E; long long* emit_n; long long* emit_off; float* emit_w; double* emit_issued;
   double* src_QV; long long* src_n; long long* src_off; float* src_w; double* src_issued;
   const double* dt_dev;            // non-NULL: dt read from device memory (graph replay)
+  double share;                    // fraction of the source energy issued (1: all of it)
 };
 cudaError_t imc_launch_plan_mg(const PlanMgArgs& a, cudaStream_t s);
 cudaError_t imc_launch_plan_mg1d(const PlanMgArgs& a, cudaStream_t s);
@@ -291,5 +296,6 @@ struct FillMgArgs {
   uint64_t seed; uint32_t step; uint32_t tag;
   float* p1; float* p2; float* d1; float* d2; float* wb; float* t; int* cell; int* group;
   const double* time_scale_dev; const uint32_t* step_dev;  // non-NULL: read from device memory
+  uint32_t id_base;            // Philox particle id of source particle k is id_base + k
 };
 cudaError_t imc_launch_fill_mg(const FillMgArgs& a, cudaStream_t s);

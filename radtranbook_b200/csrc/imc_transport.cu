@@ -15,7 +15,7 @@
 // FP32; energy removed from a history is accounted as the exact FP64 difference of its
 // FP32 weights, accumulated in registers while the history stays in one cell and flushed
 // through warp-aggregated FP64 reductions when it leaves.  Random numbers: Philox keyed by
-// the run seed, counter (bank index, event number, step, TAG_TRANSPORT).
+// the run seed, counter (id_base + bank index, event number, step, TAG_TRANSPORT).
 #include "imc_device.cuh"
 #include "imc_internal.h"
 
@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
         if (!a.cap_is_reference) atomicOr(a.flags, (int)IMC_FLAG_EVENT_CAP);
         finished = true;
       } else {
-        const U4 r = draw(a.seed, pid, ev, stepk, TAG_TRANSPORT);
+        const U4 r = draw(a.seed, a.id_base + pid, ev, stepk, TAG_TRANSPORT);
         ++ev;
         float d, sb, L, xn = x, yn = y, un = u, vn = v;
         int evt, cross = X_NONE;

@@ -108,7 +108,8 @@ class Engine:
         self.nx, self.ny = len(e1) - 1, len(e2) - 1
         self.nc = self.nx * self.ny
         self.ng = n_groups
-        self.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+        self.rank, self.world = 0, 1
+        self.seed = seed
         dev = self.device
         f64 = dict(dtype=torch.float64, device=dev)
         self.e1 = torch.as_tensor(e1, **f64)
@@ -157,6 +158,40 @@ class Engine:
         self.ws = torch.empty(0, dtype=torch.uint8, device=dev)
         self.launch = dict(block_size=256, blocks_per_sm=4, chunk=512, smem_cells=0)
         self._last_transport = None
+        # particle partition over ranks (radtranbook_b200.partition): this rank's Philox id
+        # offset and share of the source energy; its comb and initial census use comb_seed
+        self.id_base = 0
+        self.energy_share = 1.0
+
+    @property
+    def seed(self) -> int:
+        return self._seed
+
+    @seed.setter
+    def seed(self, value: int) -> None:
+        self._seed = int(value) & 0xFFFFFFFFFFFFFFFF
+
+    @property
+    def comb_seed(self) -> int:
+        """Philox key of the comb and the initial census: the seed, or on rank r > 0 of a
+        partition a per-rank key derived from it."""
+        from .partition import rank_key
+
+        return rank_key(self._seed, getattr(self, "rank", 0))
+
+    ic_seed = comb_seed
+
+    def partition(self, rank: int, world: int) -> None:
+        """Make this engine rank `rank` of a `world`-rank particle partition: its sources and
+        tracking draw Philox ids from rank * (2^32 // world), it issues 1/world of every source
+        energy, and its comb and initial census use a per-rank key."""
+        from .partition import id_base
+
+        if not (0 <= rank < world):
+            raise ValueError("rank must be in [0, world)")
+        self.rank, self.world = int(rank), int(world)
+        self.id_base = id_base(rank, world)
+        self.energy_share = 1.0 / world
 
     # ------------------------------------------------------------------ helpers
     def _stream(self) -> int:
@@ -190,9 +225,11 @@ class Engine:
         n_out = ctypes.c_int64(0)
         cb = self.bank.c()
         st = self.lib.imc_init_census(ctypes.byref(self.cmesh), _ptr(tr_flat), int(n_target), float(t_emit_floor),
-                                      self.seed, ctypes.byref(cb), wsp, wsn, ctypes.byref(n_out), self._stream())
+                                      self.ic_seed, ctypes.byref(cb), wsp, wsn, ctypes.byref(n_out), self._stream())
         _lib.check("imc_init_census", st)
         self.bank.size = int(cb.size)
+        if self.energy_share != 1.0 and self.bank.size:
+            self.bank.weight[: self.bank.size].mul_(self.energy_share)  # this rank's share of the energy
         self._census_dev_valid = False
         return self.bank.size
 
@@ -238,7 +275,7 @@ class Engine:
         def run(cb):
             wsp, wsn = self._ws(max(src.size, 1))
             return self.lib.imc_comb(ctypes.byref(self.cmesh), ctypes.byref(cin), ctypes.byref(cb), int(n_max),
-                                     self.seed, int(step) & 0xFFFFFFFF, flags, _ptr(self.disc), wsp, wsn,
+                                     self.comb_seed, int(step) & 0xFFFFFFFF, flags, _ptr(self.disc), wsp, wsn,
                                      ctypes.byref(rep), self._stream())
 
         cb = self._call_bank("imc_comb", run, dst, lambda: rep.required_capacity)
@@ -288,6 +325,8 @@ class Engine:
         par.cf_fastpath = float(cf_fastpath)
         par.step_dev = _ptr(step_dev)
         par.dt_dev = _ptr(dt_dev)
+        par.id_base = int(self.id_base)
+        par.energy_share = float(self.energy_share)
         return par
 
     def _set_census_count(self, n: int) -> None:
@@ -350,13 +389,13 @@ class Engine:
         wsp, wsn = self._ws(max(self._upper, self.bank.capacity))
         if step_dev is not None:
             st = self.lib.imc_comb_async_dev(ctypes.byref(self.cmesh), ctypes.byref(cin), ctypes.byref(cout), n_max,
-                                             None if n_max_dev is None else n_max_dev.data_ptr(), self.seed,
+                                             None if n_max_dev is None else n_max_dev.data_ptr(), self.comb_seed,
                                              step_dev.data_ptr(), flags, _ptr(self.disc), _ptr(e),
                                              wsp, wsn, self.summary_dev.data_ptr(), self._stream())
             _lib.check("imc_comb_async_dev", st)
             return
         st = self.lib.imc_comb_async(ctypes.byref(self.cmesh), ctypes.byref(cin), ctypes.byref(cout), n_max,
-                                     self.seed, step & 0xFFFFFFFF, flags, _ptr(self.disc), _ptr(e),
+                                     self.comb_seed, step & 0xFFFFFFFF, flags, _ptr(self.disc), _ptr(e),
                                      wsp, wsn, self.summary_dev.data_ptr(), self._stream())
         _lib.check("imc_comb_async", st)
 

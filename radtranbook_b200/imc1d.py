@@ -38,20 +38,25 @@ def _edges(mesh):
 
 
 def init_simulation(Ntarget, Tinit, Tr_init, mesh, eos, inv_eos, Ntarget_ic=None, geometry="slab",
-                    T_emit_floor=0.0, seed=0x5EED0001):
+                    T_emit_floor=0.0, seed=0x5EED0001, _allreduce=None):
+    """_allreduce: a torch.distributed module for a particle-partitioned run (the process
+    parallelism of IMC/IMC1DMPI.py, radtranbook_b200.partition); every step then takes the
+    same one."""
     mesh = np.asarray(mesh, dtype=np.float64)
     eng = Engine(geometry, _edges(mesh), np.array([0.0, 1.0]), _cell_volumes(mesh, geometry), seed=seed,
                  capacity=4 * int(Ntarget) + 1024)
-    return init_state(eng, 1, (mesh.shape[0],), Ntarget, Tinit, Tr_init, eos, inv_eos, Ntarget_ic, T_emit_floor)
+    return init_state(eng, 1, (mesh.shape[0],), Ntarget, Tinit, Tr_init, eos, inv_eos, Ntarget_ic, T_emit_floor,
+                      dist=_allreduce)
 
 
 def step(state, Ntarget, Nboundary, Nsource, NMax, T_boundary, dt, mesh, sigma_a_func, inv_eos, cv, source,
          reflect=(False, False), theta=1.0, use_scalar_intensity_Tr=True, conserve_comb_energy=False,
-         T_emit_floor=0.0, geometry="slab"):
+         T_emit_floor=0.0, geometry="slab", _allreduce=None):
     return gray_step(state, Ntarget=Ntarget, Nboundary=Nboundary, Nsource=Nsource, Nmax=NMax,
                      T_boundary=T_boundary, dt=dt, sigma_a_func=sigma_a_func, inv_eos=inv_eos, cv=cv, source=source,
                      reflect=reflect, theta=theta, use_scalar_intensity_Tr=use_scalar_intensity_Tr,
-                     conserve_comb_energy=conserve_comb_energy, T_emit_floor=T_emit_floor, geometry=geometry)
+                     conserve_comb_energy=conserve_comb_energy, T_emit_floor=T_emit_floor, geometry=geometry,
+                     allreduce=_allreduce)
 
 
 def run_simulation(Ntarget, Nboundary, Nsource, NMax, Tinit, Tr_init, T_boundary, dt, mesh, sigma_a_func, eos,

@@ -30,10 +30,11 @@ __a = 0.01372
 SimulationState = GrayState
 
 
-def init_simulation(Ntarget, Tinit, Tr_init, mesh, eos, inv_eos, Ntarget_ic=None, geometry="slab", seed=0x5EED0001):
+def init_simulation(Ntarget, Tinit, Tr_init, mesh, eos, inv_eos, Ntarget_ic=None, geometry="slab", seed=0x5EED0001,
+                    _allreduce=None):
     # the Carter-Forest initial census is the Fleck-Cummings module's (ceil counts per cell)
     return _imc1d.init_simulation(Ntarget, Tinit, Tr_init, mesh, eos, inv_eos, Ntarget_ic=Ntarget_ic,
-                                  geometry=geometry, seed=seed)
+                                  geometry=geometry, seed=seed, _allreduce=_allreduce)
 
 
 def step(state, Ntarget, Nboundary, Nsource, NMax, T_boundary, dt, mesh, sigma_a_func, inv_eos, cv, source,

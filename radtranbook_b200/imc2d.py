@@ -38,11 +38,15 @@ def _flat_volumes(edges1, edges2, geometry):
 
 
 def init_simulation(Ntarget, Tinit, Tr_init, edges1, edges2, eos, inv_eos, Ntarget_ic=None, geometry="xy",
-                    seed=0x5EED0001):
+                    seed=0x5EED0001, _allreduce=None):
+    """_allreduce: a torch.distributed module for a particle-partitioned run (the process
+    parallelism of IMC/IMC2DMPI.py, radtranbook_b200.partition); every step then takes the
+    same one."""
     e1 = np.asarray(edges1, dtype=np.float64)
     e2 = np.asarray(edges2, dtype=np.float64)
     eng = Engine(geometry, e1, e2, _flat_volumes(e1, e2, geometry), seed=seed, capacity=4 * int(Ntarget) + 1024)
-    return init_state(eng, 2, (len(e1) - 1, len(e2) - 1), Ntarget, Tinit, Tr_init, eos, inv_eos, Ntarget_ic)
+    return init_state(eng, 2, (len(e1) - 1, len(e2) - 1), Ntarget, Tinit, Tr_init, eos, inv_eos, Ntarget_ic,
+                      dist=_allreduce)
 
 
 def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges2, sigma_a_func, inv_eos, cv,

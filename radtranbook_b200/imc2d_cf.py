@@ -33,9 +33,9 @@ _NO_PROGRESS_MAX_STREAK = 8
 
 
 def init_simulation(Ntarget, Tinit, Tr_init, edges1, edges2, eos, inv_eos, Ntarget_ic=None, geometry="xy",
-                    seed=0x5EED0001):
+                    seed=0x5EED0001, _allreduce=None):
     return _imc2d.init_simulation(Ntarget, Tinit, Tr_init, edges1, edges2, eos, inv_eos, Ntarget_ic=Ntarget_ic,
-                                  geometry=geometry, seed=seed)
+                                  geometry=geometry, seed=seed, _allreduce=_allreduce)
 
 
 def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges2, sigma_a_func, inv_eos, cv,

@@ -26,10 +26,11 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._gray import GrayState, _host_copy, _staged, average_tallies, face_temperatures, replica_mean
+from ._gray import GrayState, _host_copy, _staged, check_partition, face_temperatures
 from .engine import A_RAD, C_LIGHT, Engine
 from .materials import evaluate, evaluate_groups
 from .mg_imc2d import planck_fractions
+from .partition import local_count, sum_scalars, sum_tensors, summary_totals, world_of
 
 __c = 29.98
 __a = 0.01372
@@ -75,13 +76,19 @@ def _comb_mode(conserve_comb_energy) -> str:
 
 
 def init_simulation(Ntarget, Tinit, Tr_init, mesh, energy_edges, eos, inv_eos, Ntarget_ic=None, T_emit_floor=0.0,
-                    seed=0x5EED0001):
+                    seed=0x5EED0001, _allreduce=None):
+    """_allreduce: a torch.distributed module for a particle-partitioned run
+    (radtranbook_b200.partition); every step of the state then takes the same one."""
+    rank, world = world_of(_allreduce)
+    dist = _allreduce if world > 1 else None
     mesh = np.asarray(mesh, dtype=np.float64)
     I = mesh.shape[0]
     G = len(energy_edges) - 1
     edges = np.concatenate([mesh[:, 0], mesh[-1:, 1]])
     eng = Engine("spherical", edges, np.array([0.0, 1.0]), _volumes(mesh), seed=seed, n_groups=G,
                  group_edges=energy_edges, capacity=4 * int(Ntarget) + 1024)
+    if world > 1:
+        eng.partition(rank, world)
     dev = eng.device
     z = lambda: torch.zeros(I, dtype=torch.float64, device=dev)  # noqa: E731
     state = SimulationState1DMG(eng, 1, (I,), z(), z(), z(), 0.0, 0.0, 0)
@@ -93,13 +100,15 @@ def init_simulation(Ntarget, Tinit, Tr_init, mesh, energy_edges, eos, inv_eos, N
     assert torch.allclose(back, Tg), "Inverse EOS failed"
     N_ic = Ntarget if Ntarget_ic is None else Ntarget_ic
     tr = torch.as_tensor(np.asarray(Tr_init, dtype=np.float64), device=dev).reshape(-1)
-    eng.init_census(tr, int(N_ic), T_emit_floor)
+    eng.init_census(tr, local_count(N_ic, rank, world), T_emit_floor)
     rad, _ = _census_moments(eng)
+    sum_tensors(dist, [rad])
     state.__dict__["radiation_energy_by_group"] = rad.cpu().numpy().copy()
     state.__dict__["radiation_flux_by_group"] = np.zeros((G, I))
     state.__dict__["radiation_energy_by_group_postcomb"] = None
     state._Tr.copy_(torch.pow(rad.sum(0) / eng.vol / A_RAD, 0.25))
     radiation, internal = eng.energy_totals(state._e)
+    radiation = sum_scalars(dist, [radiation], dev)[0]
     state.previous_total_energy = internal + radiation
     state.refresh_host()
     return state
@@ -138,6 +147,9 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, mesh, energy_
          Nmax_final=None, _allreduce=None):
     t0 = _time.perf_counter()
     eng: Engine = state._engine
+    # particle partition (radtranbook_b200.partition): counts are totals, each rank takes its share
+    rank, world = check_partition(eng, _allreduce)
+    dist = _allreduce if world > 1 else None
     G, I = eng.ng, eng.nc
     mode = _comb_mode(conserve_comb_energy)
     like = state._T
@@ -170,16 +182,16 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, mesh, energy_
                               cache)
     refl = tuple(reflect) + (False,) * (4 - len(reflect))
     t_eval = _time.perf_counter()
-    eng.transport_async(state._T, sig.reshape(-1).contiguous(), cvv, src, state.count, dt, theta, Ntarget, Nboundary,
-                        Nsource, faces, refl, max_events=0, rz_linear_source=False, t_emit_floor=T_emit_floor,
-                        n_boundary_side=n_side)
-    world = 1
-    if _allreduce is not None:
-        world = _allreduce.get_world_size()
-        average_tallies(_allreduce, eng)
+    lc = lambda n: local_count(n, rank, world)  # noqa: E731
+    eng.transport_async(state._T, sig.reshape(-1).contiguous(), cvv, src, state.count, dt, theta, lc(Ntarget),
+                        lc(Nboundary), lc(Nsource), faces, refl, max_events=0, rz_linear_source=False,
+                        t_emit_floor=T_emit_floor, n_boundary_side=None if n_side is None else [lc(n) for n in n_side])
+    sum_tensors(dist, [eng.dep, eng.si, eng.emitted, eng.boundary_group, eng.escaped_group])
     eng.material_update(state._e, state._Tr)
-    eng.comb_async(Nmax, state.count, state._e, per_group=True, conserve_radiation=(mode == "radiation"))
+    nmax_l = lc(Nmax) if Nmax > 0 else (-lc(-Nmax) if Nmax < 0 else 0)
+    eng.comb_async(nmax_l, state.count, state._e, per_group=True, conserve_radiation=(mode == "radiation"))
     if mode == "material":
+        sum_tensors(dist, [eng.disc])
         state._e.add_(eng.disc.view(G, I).sum(0) / eng.vol)
     Tn = evaluate(inv_eos, state._e, lambda: _host_copy(state._e), like, **_staged(state, "T_new", I))
     state._T.copy_(Tn.reshape(-1))
@@ -195,32 +207,37 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, mesh, energy_
         live = w > 0
         rad_c = torch.zeros(I, dtype=torch.float64, device=eng.device)
         rad_c.index_add_(0, pre.view("cell").long()[live], w[live])
+        sum_tensors(dist, [rad_c])
         state._Tr.copy_(torch.pow(rad_c / eng.vol / A_RAD, 0.25))
         state.refresh_host()
     else:
         state.take_host_copies()
     rad_g, flux_g = _census_moments(eng)
-    internal = float(sm.internal_energy)
-    rad = float(sm.comb_after)
-    comb_disc = float(sm.comb_before) - rad
+    sum_tensors(dist, [rad_g, flux_g])
+    internal = float(sm.internal_energy)  # the same material state on every rank
+    tot = summary_totals(dist, sm, eng.bank.size, eng.device)  # summed over the ranks of a partition
+    rad = tot["rad"]
+    comb_disc = tot["comb_before"] - rad
     if mode == "material":
         internal += comb_disc
-    boundary_emission = float(sum(sm.e_side))
-    boundary_loss = float(sum(sm.escaped))
-    if _allreduce is not None and world > 1:
-        rad, comb_disc, boundary_loss = replica_mean(_allreduce, [rad, comb_disc, boundary_loss], eng.device)
+    boundary_emission = float(tot["e_side"].sum())
+    boundary_loss = float(tot["escaped"].sum())
+    source_emission = tot["source_emission"]
+    n_boundary = int(sum(sm.n_side))
+    if dist is not None:
+        n_boundary = int(sum_scalars(dist, [float(n_boundary)], eng.device)[0])
     total = internal + rad
     dE = total - state.previous_total_energy
-    residual = dE - boundary_emission + boundary_loss - float(sm.source_emission)
+    residual = dE - boundary_emission + boundary_loss - source_emission
     closure = residual + (0.0 if mode == "material" else comb_disc)
     state.__dict__["radiation_energy_by_group"] = rad_g.cpu().numpy().copy()
     state.__dict__["radiation_flux_by_group"] = flux_g.cpu().numpy().copy()
     state.time = state.time + dt
     state.previous_total_energy = total
     state.count += 1
-    stats = np.array(sm.stats[:], dtype=np.int64)
+    stats = tot["stats"]
     ms_src, ms_tr = eng.phase_times()
-    n_tr = int(sm.n_bank)
+    n_tr = tot["n_bank"]
     ev = int(stats[_lib.STAT_EVENTS])
     t_end = _time.perf_counter()
     info = {
@@ -229,22 +246,22 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, mesh, energy_
         "radiation_temperature": state.radiation_temperature.copy(),
         "radiation_energy_by_group": state.radiation_energy_by_group.copy(),
         "radiation_flux_by_group": state.radiation_flux_by_group.copy(),
-        "N_particles": int(eng.bank.size),
+        "N_particles": tot["n_particles"],
         "total_energy": total,
         "total_internal_energy": internal,
         "total_radiation_energy": rad,
         "boundary_emission": boundary_emission,
-        "N_boundary": int(sum(sm.n_side)),
+        "N_boundary": n_boundary,
         "boundary_loss": boundary_loss,
         "boundary_loss_by_group": eng.escaped_group.cpu().numpy().copy(),
-        "source_emission": float(sm.source_emission),
+        "source_emission": source_emission,
         "energy_residual": residual,
         "Nmax_next": (min(Nmax + Nmax_growth, Nmax_final) if Nmax_final is not None else Nmax + Nmax_growth)
         if Nmax_growth > 0 else Nmax,
         "ledger": {"comb_discrepancy": comb_disc, "closure": closure,
                    "relative_closure": closure / max(abs(total), 1e-300),
-                   "emission": float(sm.emission_total),
-                   "weight_floor": 1e-14 * float(sm.weight_sum) / max(n_tr, 1)},
+                   "emission": tot["emission_total"],
+                   "weight_floor": 1e-14 * tot["weight_sum"] / max(n_tr, 1)},
         "profiling": {
             "phase_times_s": {
                 "sampling": (t_eval - t0) + ms_src * 1e-3,

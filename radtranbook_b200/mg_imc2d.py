@@ -24,7 +24,8 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._gray import GrayState, _host_copy, _staged, average_tallies, face_temperatures, replica_mean
+from ._gray import GrayState, _host_copy, _staged, check_partition, face_temperatures
+from .partition import local_count, sum_scalars, sum_tensors, summary_totals, world_of
 from .engine import A_RAD, C_LIGHT, Engine
 from .materials import evaluate, evaluate_groups
 
@@ -101,13 +102,19 @@ class SimulationState2DMG(GrayState):
 
 
 def init_simulation(Ntarget, Tinit, Tr_init, edges1, edges2, energy_edges, eos, inv_eos, Ntarget_ic=None,
-                    T_emit_floor=0.0, geometry="xy", seed=0x5EED0001):
+                    T_emit_floor=0.0, geometry="xy", seed=0x5EED0001, _allreduce=None):
+    """_allreduce: a torch.distributed module for a particle-partitioned run
+    (radtranbook_b200.partition); every step of the state then takes the same one."""
+    rank, world = world_of(_allreduce)
+    dist = _allreduce if world > 1 else None
     e1 = np.asarray(edges1, dtype=np.float64)
     e2 = np.asarray(edges2, dtype=np.float64)
     G = len(energy_edges) - 1
     vol = _cell_volumes(e1, e2, geometry)
     eng = Engine(geometry, e1, e2, np.ascontiguousarray(vol.T).reshape(-1), seed=seed, n_groups=G,
                  group_edges=energy_edges, capacity=4 * int(Ntarget) + 1024)
+    if world > 1:
+        eng.partition(rank, world)
     dev = eng.device
     nx, ny = len(e1) - 1, len(e2) - 1
     state = SimulationState2DMG(eng, 2, (nx, ny), torch.zeros(eng.nc, dtype=torch.float64, device=dev),
@@ -121,13 +128,15 @@ def init_simulation(Ntarget, Tinit, Tr_init, edges1, edges2, energy_edges, eos, 
     assert torch.allclose(back, Tg), "Inverse EOS failed"
     N_ic = Ntarget if Ntarget_ic is None else Ntarget_ic
     tr = state.flat(torch.as_tensor(np.asarray(Tr_init, dtype=np.float64), device=dev))
-    eng.init_census(tr, int(N_ic), T_emit_floor)
+    eng.init_census(tr, local_count(N_ic, rank, world), T_emit_floor)
     rad = _rad_by_group(eng)
+    sum_tensors(dist, [rad])
     object.__setattr__(state, "_rad_group", rad)
     state.__dict__["radiation_energy_by_group"] = rad.view(G, ny, nx).transpose(1, 2).cpu().numpy().copy()
     state.__dict__["radiation_energy_by_group_postcomb"] = None
     state._Tr.copy_(torch.pow(rad.sum(0) / A_RAD, 0.25))
     radiation, internal = eng.energy_totals(state._e)
+    radiation = sum_scalars(dist, [radiation], dev)[0]
     state.previous_total_energy = internal + radiation
     state.refresh_host()
     return state
@@ -187,6 +196,9 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
         raise ValueError(f"Unknown geometry: {geometry}")
     t_step_start = _time.perf_counter()
     eng: Engine = state._engine
+    # particle partition (radtranbook_b200.partition): counts are totals, each rank takes its share
+    rank, world = check_partition(eng, _allreduce)
+    dist = _allreduce if world > 1 else None
     G, nc = eng.ng, eng.nc
     like = state.grid(state._T)
     host_T = lambda: state.temperature  # noqa: E731
@@ -236,20 +248,21 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
     faces = face_temperatures(2, geometry, T_boundary, state.time, e1, e2, boundary_source_func, eng.device, cache)
     refl = tuple(reflect) + (False,) * (4 - len(reflect))
     t_eval = _time.perf_counter()
-    eng.transport_async(state._T, sig.reshape(-1).contiguous(), cvv, src, state.count, dt, theta, Ntarget, Nboundary,
-                        Nsource, faces, refl, max_events=max_events_per_particle, rz_linear_source=False,
+    nt_l, nb_l, ns_l = (local_count(n, rank, world) for n in (Ntarget, Nboundary, Nsource))
+    nmax_l = local_count(Nmax, rank, world) if Nmax > 0 else Nmax
+    eng.transport_async(state._T, sig.reshape(-1).contiguous(), cvv, src, state.count, dt, theta, nt_l, nb_l, ns_l,
+                        faces, refl, max_events=max_events_per_particle, rz_linear_source=False,
                         t_emit_floor=T_emit_floor)
-    world = 1
-    if _allreduce is not None:
-        world = _allreduce.get_world_size()
-        average_tallies(_allreduce, eng)
+    sum_tensors(dist, [eng.dep, eng.si, eng.emitted, eng.boundary_group, eng.escaped_group])
     eng.material_update(state._e, state._Tr)
     rad_pre = eng.si.view(G, nc) / C_LIGHT  # radiation energy density by group (path length)
-    eng.comb_async(Nmax, state.count, state._e, per_group=True)
+    eng.comb_async(nmax_l, state.count, state._e, per_group=True)
     hb = _group_buffers(state, eng)
     eng.census_energy_async(hb["post_dev"], per_group=True)  # post-comb energy by (group, cell)
+    sum_tensors(dist, [hb["post_dev"]])
     hb["post_dev"].view(G, nc).div_(eng.vol.view(1, nc))
     if conserve_comb_energy:
+        sum_tensors(dist, [eng.disc])
         state._e.add_(eng.disc.view(G, nc).sum(0) / eng.vol)
     Tn = evaluate(inv_eos, state.grid(state._e), lambda: _host_copy(state.grid(state._e)), like,
                   **_staged(state, "T_new", nc))
@@ -274,25 +287,29 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
         w = pre.view("weight").double()
         live = w > 0
         acc.index_add_(0, (pre.view("cell").long() + nc * pre.view("group").long())[live], w[live])
+        sum_tensors(dist, [acc])
         rad_pre = acc.view(G, nc) / eng.vol.view(1, nc)
         state._Tr.copy_(torch.pow(rad_pre.sum(0) / A_RAD, 0.25))
         state.refresh_host()
     else:
         state.take_host_copies()
-    if eng.comb_repeated:  # the comb ran again after an overflow: rebuild from the new census
-        hb["post"].copy_(to_grid3(_rad_by_group(eng)))
-    internal = float(sm.internal_energy)
-    rad = float(sm.comb_after)
-    comb_disc = float(sm.comb_before) - rad
+    # the comb ran again after an overflow (on any rank): rebuild from the new census
+    if sum_scalars(dist, [float(eng.comb_repeated)], eng.device)[0] > 0:
+        post = _rad_by_group(eng)
+        sum_tensors(dist, [post])
+        hb["post"].copy_(to_grid3(post))
+    internal = float(sm.internal_energy)  # the same material state on every rank
+    tot = summary_totals(dist, sm, eng.bank.size, eng.device)  # summed over the ranks of a partition
+    rad = tot["rad"]
+    comb_disc = tot["comb_before"] - rad
     if conserve_comb_energy:
         internal += comb_disc
-    boundary_emission = float(sum(sm.e_side))
-    boundary_loss = float(sum(sm.escaped))
-    if _allreduce is not None and world > 1:
-        rad, comb_disc, boundary_loss = replica_mean(_allreduce, [rad, comb_disc, boundary_loss], eng.device)
+    boundary_emission = float(tot["e_side"].sum())
+    boundary_loss = float(tot["escaped"].sum())
+    source_emission = tot["source_emission"]
     total = internal + rad
     dE = total - state.previous_total_energy
-    residual = dE - boundary_emission + boundary_loss - float(sm.source_emission)
+    residual = dE - boundary_emission + boundary_loss - source_emission
     closure = residual + (0.0 if conserve_comb_energy else comb_disc)
     state.time = state.time + dt
     state.previous_total_energy = total
@@ -309,12 +326,12 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
     object.__setattr__(state, "_rad_group", rad_pre)
     state.__dict__["radiation_energy_by_group"] = rad_group_pre
     state.__dict__["radiation_energy_by_group_postcomb"] = rad_group_post
-    stats = np.array(sm.stats[:], dtype=np.int64)
+    stats = tot["stats"]
     bnd_group = hb["bnd"].numpy().copy()
     esc_group = hb["esc"].numpy().copy()
     ms_src, ms_tr = eng.phase_times()
     t_end = _time.perf_counter()
-    n_tr = int(sm.n_bank)
+    n_tr = tot["n_bank"]
     ev = int(stats[_lib.STAT_EVENTS])
     info = {
         "time": state.time,
@@ -322,7 +339,7 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
         "radiation_temperature": state.radiation_temperature,
         "radiation_energy_by_group": rad_group_pre,
         "radiation_energy_by_group_postcomb": rad_group_post,
-        "N_particles": int(eng.bank.size),
+        "N_particles": tot["n_particles"],
         "N_boundary": Nboundary,
         "N_target": Ntarget,
         "particle_budget_fmin": float(np.clip(particle_budget_fmin, 0.0, 0.5)),
@@ -333,24 +350,24 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
         "total_radiation_energy": rad,
         "boundary_emission": boundary_emission,
         "boundary_emission_by_group": bnd_group,
-        "boundary_emission_by_side": np.array(sm.e_side[:]),
+        "boundary_emission_by_side": tot["e_side"],
         "boundary_loss": boundary_loss,
         "boundary_outgoing": boundary_loss,
         "boundary_outgoing_by_group": esc_group,
-        "boundary_outgoing_by_side": np.array(sm.escaped[:]),
-        "source_emission": float(sm.source_emission),
-        "incoming_energy_total": boundary_emission + float(sm.source_emission),
+        "boundary_outgoing_by_side": tot["escaped"],
+        "source_emission": source_emission,
+        "incoming_energy_total": boundary_emission + source_emission,
         "outgoing_energy_total": boundary_loss,
         "dE_system": dE,
-        "energy_expected_dE": boundary_emission + float(sm.source_emission) - boundary_loss,
+        "energy_expected_dE": boundary_emission + source_emission - boundary_loss,
         "energy_residual": residual,
         "energy_loss": residual,
         "Nmax_next": (min(Nmax + Nmax_growth, Nmax_final) if Nmax_final is not None else Nmax + Nmax_growth)
         if Nmax_growth > 0 else Nmax,
         "ledger": {"comb_discrepancy": comb_disc, "closure": closure,
                    "relative_closure": closure / max(abs(total), 1e-300),
-                   "emission": float(sm.emission_total),
-                   "weight_floor": 1e-10 * float(sm.weight_sum) / max(n_tr, 1)},
+                   "emission": tot["emission_total"],
+                   "weight_floor": 1e-10 * tot["weight_sum"] / max(n_tr, 1)},
         "profiling": {
             "phase_times_s": {
                 "sampling": (t_eval - t_step_start) + ms_src * 1e-3,
