@@ -119,7 +119,9 @@ typedef struct imc_step_params {
   int32_t block_size;           /* tracking launch shape; 0 = tuned default */
   int32_t blocks_per_sm;
   int32_t chunk;                /* histories claimed per warp ticket (guided: at most this) */
-  int32_t reserved;             /* bit 0: shared-memory cell table (other bits ignored) */
+  int32_t reserved;             /* bit 0: shared-memory cell table (default: up to 4096 (group, cell)
+                                   entries); bit 1: per-block tallies in shared memory with that
+                                   table, bit 2: never (default: up to 2048 entries); others ignored */
   const double* emission_fractions; /* MG: [g] fixed emission spectrum, or NULL = Planck */
   int64_t n_boundary_side[4];   /* > 0: boundary particles on that side instead of n_boundary
                                    (per-side budgets, MG_IMC/MG_IMC1D.py:1000-1040) */

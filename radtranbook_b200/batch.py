@@ -309,11 +309,12 @@ def tune(engine: BatchEngine, grid: dict | None = None, repeats: int = 1) -> dic
 def run_plain(spec: BatchSpec, steps: int, instances=None, launch: dict | None = None) -> dict:
     """The same batch through the single-problem drop-in (radtranbook_b200.imc1d), one
     instance after the other; device material callables, so each step synchronises the
-    host once.  Returns per-instance final T, ledger closures and total events."""
+    host once.  Returns per-instance final T, ledger closures, total events and each step's
+    wall time (step_s[k][s], seconds; the step ends with its synchronisation)."""
     from . import imc1d
     from .materials import Constant, PowerLawOpacity, device_callable
 
-    out = {"T": [], "Tr": [], "max_rel_closure": [], "events": 0}
+    out = {"T": [], "Tr": [], "max_rel_closure": [], "events": 0, "step_s": []}
     ks = range(spec.K) if instances is None else instances
     for k in ks:
         nc = int(spec.n_cells[k])
@@ -330,12 +331,16 @@ def run_plain(spec: BatchSpec, steps: int, instances=None, launch: dict | None =
             st._engine.launch.update(launch)
         worst = 0.0
         refl = (bool(spec.reflect[k] & 1), bool(spec.reflect[k] & 2))
+        times = []
         for _ in range(steps):
+            t0 = time.perf_counter()
             st, info = imc1d.step(st, int(spec.n_target[k]), int(spec.n_boundary[k]), 0, int(spec.n_max[k]),
                                   (float(spec.face_T[k][0]), float(spec.face_T[k][1])), spec.dt, mesh, sigma,
                                   inv_eos, cv, np.zeros(nc), reflect=refl, theta=spec.theta)
+            times.append(time.perf_counter() - t0)
             worst = max(worst, abs(info["ledger"]["relative_closure"]))
             out["events"] += info["profiling"]["transport_events"]["total"]
+        out["step_s"].append(times)
         out["T"].append(st.temperature.copy())
         out["Tr"].append(st.radiation_temperature.copy())
         out["max_rel_closure"].append(worst)

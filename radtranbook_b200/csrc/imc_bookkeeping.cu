@@ -48,7 +48,10 @@ __global__ void k_plan_cells(PlanArgs a) {
     const double ss = a.sigma[c] * (1.0 - f);
     const double sa = a.sigma[c] * f;
     a.sa[c] = sa; a.ss[c] = ss;
-    a.sass[c] = make_float2((float)sa, (float)ss);
+    // tracking table: sigma_a below the estimator's threshold is entered as 0 (no capture; in
+    // FP32 exp(-sigma_a s) is 1 there anyway), which also marks the cell's intensity as the
+    // path-length sum w*s; elsewhere the intensity follows from the deposition
+    a.sass[c] = make_float2(sa > sa_thr ? (float)sa : 0.f, (float)ss);
     const double iv = 1.0 / a.vol[c];
     a.cellf[c] = make_double2(iv, sa > sa_thr ? 1.0 / (sa * a.vol[c] * dt) : -1.0 / (a.vol[c] * dt));
     double E = A_RAD * C_LIGHT * pow4(fmax(T, 0.0)) * sa * dt * a.vol[c];
@@ -440,7 +443,7 @@ __global__ void k_plan_mg_cells(PlanMgArgs a) {
       const double ss = a.sigma[q] * (1.0 - f);
       const double sa = a.sigma[q] * f;
       a.sa[q] = sa; a.ss[q] = ss;
-      a.sass[q] = make_float2((float)sa, (float)ss);
+      a.sass[q] = make_float2(sa > 1e-12 ? (float)sa : 0.f, (float)ss);  // 0: no capture, w*s intensity
       a.cellf[q] = make_double2(1.0 / a.vol[c], sa > 1e-12 ? 1.0 / (sa * a.vol[c] * dt) : -1.0 / (a.vol[c] * dt));
       const double bg = a.emission_fractions ? a.emission_fractions[g] : gc[g];
       run += sa * bg * aT4;
@@ -577,7 +580,7 @@ __global__ void k_plan_mg1d_cells(PlanMgArgs a) {
       const double sa = a.sigma[q] * f;
       const double ss = a.sigma[q] * (1.0 - f);
       a.sa[q] = sa; a.ss[q] = ss;
-      a.sass[q] = make_float2((float)sa, (float)ss);
+      a.sass[q] = make_float2(sa > 1e-10 ? (float)sa : 0.f, (float)ss);  // 0: no capture, w*s intensity
       // MG_IMC/MG_IMC1D.py:346-350: path-length estimator below sigma_a = 1e-10
       a.cellf[q] = make_double2(1.0 / a.vol[c], sa > 1e-10 ? 1.0 / (sa * a.vol[c] * dt) : -1.0 / (a.vol[c] * dt));
       a.emit_E[q] = cold ? 0.0 : A_RAD * C_LIGHT * pow4(T) * sa * b[g] * dt * a.vol[c] * a.share;

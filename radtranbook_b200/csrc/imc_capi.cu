@@ -335,8 +335,10 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   ta.dep_fx = dep_fx; ta.esc_fx = esc_fx;
   const int block = par->block_size > 0 ? par->block_size : 256;
   const int bps = par->blocks_per_sm > 0 ? par->blocks_per_sm : 3;
-  // reserved: bit 0 = stage the cell table in shared memory
+  // reserved: bit 0 = stage the cell table in shared memory; bit 1 = block tallies in shared
+  // memory, bit 2 = never (default: with the staged table up to 2048 (group, cell) entries)
   const bool smem_cells = (par->reserved & 1) ? true : ((long long)nc * ng <= 4096);
+  const bool smem_tally = smem_cells && !(par->reserved & 4) && ((par->reserved & 2) || (long long)nc * ng <= 2048);
   if (adj) {
     AdjointArgs A = *adj;
     A.t = ta; A.sa64 = tal->sigma_a; A.ss64 = tal->sigma_s; A.sig64 = mat->sigma;
@@ -344,7 +346,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     if (pe.ok) { IMC_CUDA(cudaEventRecord(pe.e[2], s)); pe.recorded = true; }
     return IMC_OK;
   }
-  IMC_CUDA(imc_launch_track(ta, mesh->geometry, block, sm_count() * bps, smem_cells, s));
+  IMC_CUDA(imc_launch_track(ta, mesh->geometry, block, sm_count() * bps, smem_cells, smem_tally, s));
   if (pe.ok) { IMC_CUDA(cudaEventRecord(pe.e[2], s)); pe.recorded = true; }
   IMC_CUDA(imc_launch_tally_finalize(ta, s));
   return IMC_OK;

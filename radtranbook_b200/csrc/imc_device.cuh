@@ -220,7 +220,7 @@ __device__ __forceinline__ double fx_inv_quantum(double wsum) { return wsum > 0.
 __device__ __forceinline__ unsigned long long fx_units(double e, double inv_q) { return __double2ull_rn(e * inv_q); }
 __device__ __forceinline__ double fx_energy(unsigned long long u, double wsum) { return (double)u * (wsum / FX_ONE); }
 
-// warp_tally2 with the first tally in fixed point
+// warp_tally2 with the first tally in fixed point (a zero value issues no reduction)
 __device__ __forceinline__ void warp_tally_fx(bool flush, int key, unsigned long long ua, double vb,
                                               unsigned long long* __restrict__ ta, double* __restrict__ tb,
                                               WarpStage* st) {
@@ -229,7 +229,7 @@ __device__ __forceinline__ void warp_tally_fx(bool flush, int key, unsigned long
   const int lane = threadIdx.x & 31;
   const unsigned peers = __match_any_sync(FULL, flush ? key : -1 - lane);
   if (__all_sync(FULL, !flush || __popc(peers) == 1)) {
-    if (flush) { if (ua) atomicAdd(ta + key, ua); atomicAdd(tb + key, vb); }
+    if (flush) { if (ua) atomicAdd(ta + key, ua); if (vb != 0.0) atomicAdd(tb + key, vb); }
     return;
   }
   unsigned long long* sa_u = reinterpret_cast<unsigned long long*>(st->a);
@@ -245,7 +245,7 @@ __device__ __forceinline__ void warp_tally_fx(bool flush, int key, unsigned long
       su += sa_u[l]; sb += st->b[l];
     }
     if (su) atomicAdd(ta + key, su);
-    atomicAdd(tb + key, sb);
+    if (sb != 0.0) atomicAdd(tb + key, sb);
   }
   __syncwarp();
 }

@@ -49,7 +49,9 @@ struct TrackArgs {
   uint32_t id_base;          // Philox particle id of bank entry k is id_base + k
 };
 
-cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool smem_cells, cudaStream_t s);
+// smem_tally: per-block deposition / intensity tallies in shared memory (with smem_cells only)
+cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool smem_cells, bool smem_tally,
+                             cudaStream_t s);
 // dep = fixed-point deposition / V, escaped (and escaped_group) from their fixed-point sums
 cudaError_t imc_launch_tally_finalize(const TrackArgs& a, cudaStream_t s);
 

@@ -37,7 +37,11 @@ enum : int { B_CENSUS = 0, B_FLOOR, B_REFLECT, B_CAP, B_ESCAPE, B_CAPTURE, B_N }
 // photon is re-emitted in the new direction the event drew after a delay ~ Exp(cf_rate) if that
 // falls inside the step, else captured (its weight deposited).  Histories at or below the
 // weight floor are not moved (they stay in census).
-template <int GEOM, bool SMEM_CELLS, bool MG, bool CF>
+// SMEM_TALLY (small meshes): the block sums its deposition (fixed point) and intensity per
+// (group, cell) in shared memory and adds them to the global tallies once, at its end.  On a
+// mesh of a few hundred cells every crossing would otherwise send its reductions to the few
+// dozen cells the wave occupies, which serialise in the L2.
+template <int GEOM, bool SMEM_CELLS, bool MG, bool CF, bool SMEM_TALLY>
 __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   const float dtk = a.dt_dev ? (float)*a.dt_dev : a.dt;  // graph replay: step length and Philox
   const uint32_t stepk = a.step_dev ? *a.step_dev : a.step;  // step counter from device memory
@@ -51,10 +55,18 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   float* E1 = reinterpret_cast<float*>(stages + nwarps);
   float* E2 = E1 + (a.nx + 1);
   float2* CS = reinterpret_cast<float2*>(E2 + (a.ny + 1) + ((a.nx + a.ny) & 1));
+  const int ncg = a.nc * a.ng;
+  // block tallies after the table (8-byte aligned: CS is), deposition then intensity
+  unsigned long long* TD = reinterpret_cast<unsigned long long*>(CS + (SMEM_CELLS ? ncg : 0));
+  double* TS = reinterpret_cast<double*>(TD + ncg);
+  unsigned long long* const dep_t = SMEM_TALLY ? TD : a.dep_fx;
+  double* const si_t = SMEM_TALLY ? TS : a.si;
   for (int q = threadIdx.x; q <= a.nx; q += blockDim.x) E1[q] = a.e1[q];
   for (int q = threadIdx.x; q <= a.ny; q += blockDim.x) E2[q] = a.e2[q];
   if (SMEM_CELLS)
-    for (int q = threadIdx.x; q < a.nc * a.ng; q += blockDim.x) CS[q] = a.sass[q];
+    for (int q = threadIdx.x; q < ncg; q += blockDim.x) CS[q] = a.sass[q];
+  if (SMEM_TALLY)
+    for (int q = threadIdx.x; q < ncg; q += blockDim.x) { TD[q] = 0ull; TS[q] = 0.0; }
   if (threadIdx.x < B_N) blk_cnt[threadIdx.x] = 0u;
   if (threadIdx.x < 4) blk_esc[threadIdx.x] = 0ull;
   __syncthreads();
@@ -77,7 +89,10 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   // refill, after a crossing) so the load overlaps the tally flush and refill of the loop end
   float2 tab = make_float2(0.f, 0.f);
   auto table = [&](int cq) { return SMEM_CELLS ? CS[cq] : __ldg(a.sass + cq); };
-  double acc_lost = 0.0, acc_wd = 0.0;  // energy removed / w*s in the current cell
+  // energy removed in the current cell visit: the per-flight differences telescope, so it is
+  // the weight at the visit's start minus the weight now (one FP64 difference at the flush)
+  float w_in = 0.f;
+  double acc_wd = 0.0;  // w*s in the current cell (cells without absorption only)
   unsigned s_bd = 0, s_sc = 0;          // per-event counters (census/cap counted at finish)
 
   const float c_light = (float)C_LIGHT;
@@ -134,6 +149,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
             if (ci < 0) { --cj; ci += a.nx; } else if (ci >= a.nx) { ++cj; ci -= a.nx; }
             tab = table(MG ? c + a.nc * grp : c);
             ev = 0;
+            w_in = w;
             has = true;
           }
         }
@@ -145,7 +161,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
 #ifdef IMC_CHECKED
     if (has && (ci < 0 || ci >= a.nx || cj < 0 || cj >= a.ny || !isfinite(w) || !isfinite(x) || !isfinite(dcen))) {
       atomicOr(a.flags, (int)IMC_FLAG_BOUNDS);
-      acc_lost = 0.0; acc_wd = 0.0;  // nothing is tallied at an invalid index
+      w_in = w; acc_wd = 0.0;  // nothing is tallied at an invalid index
       has = false;
     }
 #endif
@@ -282,10 +298,12 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
           if (cross != X_JM && cross != X_JP) yn = fminf(fmaxf(yn, zlo), zhi);
           xn = rn;
         }
-        // implicit capture; the energy removed is the exact difference of the FP32 weights
+        // implicit capture (the energy removed is counted at the flush, w_in - w)
         const float wn = (MG2 && !(sa > 1e-12f)) ? w : w * __expf(-sa * d);
-        acc_lost += (double)w - (double)wn;
-        acc_wd += (double)(w * d);
+        // path-length intensity: w*s is needed only in cells without absorption (table
+        // entry 0: below the estimator's threshold, or Carter-Forest); elsewhere it is
+        // lost / (sigma_a V dt), formed from the deposition tally when the step ends
+        if (!(sa > 0.f)) acc_wd += (double)(w * d);
         dcen -= d;
         bool captured = false;
         if (CF && evt == EV_SCATTER) {
@@ -302,7 +320,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
             if (ONED ? (tr > 1e-14f && delay < tr) : (delay < tr - 1e-15f)) dcen = fmaxf(0.f, (tr - delay) * c_light);
             else captured = true;
           }
-          if (captured) acc_lost += (double)w;
+          // a capture deposits the whole weight: w becomes 0 below, so w_in - w includes it
         }
         if (evt == EV_BOUNDARY) ++s_bd;
         else if (captured) atomicAdd(&blk_cnt[B_CAPTURE], 1u);
@@ -322,9 +340,9 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
           w = captured ? 0.f : wn; x = xn; y = yn; u = un; v = vn;
           if (CF && captured) finished = true;
           if (cross != X_NONE) {
-            // leaving the cell: flush the accumulators for the old cell
-            flush = true; flush_cell = cq; f_lost = acc_lost; f_wd = acc_wd;
-            acc_lost = 0.0; acc_wd = 0.0;
+            // leaving the cell: flush the visit (before an escape zeroes w) and start the next
+            flush = true; flush_cell = cq; f_lost = (double)w_in - (double)w; f_wd = acc_wd;
+            w_in = w; acc_wd = 0.0;
             int ni = ci, nj = cj;
             if (cross == X_IP) ++ni; else if (cross == X_IM) --ni; else if (cross == X_JP) ++nj; else --nj;
             int side = -1;
@@ -350,13 +368,16 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
           if (GEOM == G_SLAB || GEOM == G_SPHERE) {
             if (!CF && !finished && w < weight_floor) {
               // IMC/IMC1D.py:188-195: kill and deposit the remainder in the current cell
-              // (every cell, including the two edge cells the reference skips)
+              // (every cell, including the two edge cells the reference skips).  Without a
+              // crossing in this event the visit's flush at the history end (w_in - 0) carries
+              // it; after one, the old cell holds the flush slot and the remainder is added to
+              // the new cell here.  Its intensity share, lost / (sigma_a V dt), follows from the
+              // deposition tally.
               atomicAdd(&blk_cnt[B_FLOOR], 1u);
-              const int c2 = ci + a.nx * cj + (MG ? a.nc * grp : 0);
-              const double2 cf = __ldg(a.cellf + c2);
-              const double rem = (double)w;
-              atomicAdd(a.dep_fx + c2, fx_units(rem, inv_q));
-              if (cf.y > 0.0) atomicAdd(a.si + c2, rem * cf.y);
+              if (flush) {
+                const int c2 = ci + a.nx * cj + (MG ? a.nc * grp : 0);
+                atomicAdd(dep_t + c2, fx_units((double)w, inv_q));
+              }
               w = 0.f;
               finished = true;
             }
@@ -373,13 +394,14 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
         }
       }
       if (finished) {
-        // A history that ends without leaving its cell flushes that cell now.  (One that
-        // ended by crossing has already queued the old cell and holds nothing new: a 1-D
-        // weight-floor kill after a crossing deposits directly.)
-        if (!flush && (acc_lost != 0.0 || acc_wd != 0.0)) {
-          flush = true; flush_cell = cq; f_lost = acc_lost; f_wd = acc_wd;
+        // A history that ends without leaving its cell flushes that cell's visit now.  (One
+        // that ended by crossing has already queued the old cell and holds nothing new: a
+        // 1-D weight-floor kill after a crossing deposits directly.)
+        if (!flush) {
+          const double lost = (double)w_in - (double)w;
+          if (lost != 0.0 || acc_wd != 0.0) { flush = true; flush_cell = cq; f_lost = lost; f_wd = acc_wd; }
         }
-        acc_lost = 0.0; acc_wd = 0.0;
+        acc_wd = 0.0;
         a.w[pid] = w;
         // census, cap and frozen histories keep their (pre-event, when frozen) state
         if (w > 0.f) {
@@ -391,16 +413,14 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
       }
     }
     // ---------------- converged tally flush ----------------
-    // cellf[c] = (1/V, si factor): si factor > 0 is 1/(sigma_a V dt); < 0 is -1/(V dt),
-    // meaning the cell's sigma_a is below the threshold and w*s is the estimator.
+    // deposited energy in fixed point; w*s (raw, only from cells without absorption) in FP64
     unsigned long long ud = 0ull;
     double vs = 0.0;
     if (flush) {
-      const double2 cf = __ldg(a.cellf + flush_cell);
       ud = fx_units(f_lost, inv_q);
-      vs = cf.y > 0.0 ? f_lost * cf.y : -f_wd * cf.y;
+      vs = f_wd;
     }
-    warp_tally_fx(flush, flush_cell, ud, vs, a.dep_fx, a.si, st);
+    warp_tally_fx(flush, flush_cell, ud, vs, dep_t, si_t, st);
   }
 
   // ---------------- statistics ----------------
@@ -422,33 +442,53 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
     if (blk_cnt[B_ESCAPE]) atomicAdd(a.stats + S_ESCAPE, (unsigned long long)blk_cnt[B_ESCAPE]);
   }
   if (threadIdx.x < 4 && blk_esc[threadIdx.x] != 0ull) atomicAdd(a.esc_fx + threadIdx.x, blk_esc[threadIdx.x]);
+  if (SMEM_TALLY) {
+    // the block's tallies (every warp's last flush is behind the __syncthreads above)
+    for (int q = threadIdx.x; q < ncg; q += blockDim.x) {
+      if (TD[q]) atomicAdd(a.dep_fx + q, TD[q]);
+      if (TS[q] != 0.0) atomicAdd(a.si + q, TS[q]);
+    }
+  }
 }
 
-template <int GEOM, bool SM, bool MG, bool CF>
+template <int GEOM, bool SM, bool MG, bool CF, bool ST>
 cudaError_t launch_one(const TrackArgs& a, int block, int grid, cudaStream_t s) {
   const int nwarps = block / 32;
   size_t sh = nwarps * sizeof(WarpStage) + sizeof(float) * (a.nx + a.ny + 4);
   if (SM) sh += sizeof(float2) * a.nc * a.ng;
+  if (ST) sh += (sizeof(unsigned long long) + sizeof(double)) * a.nc * a.ng;
   if (sh > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_track<GEOM, SM, MG, CF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+    cudaError_t e = cudaFuncSetAttribute(k_track<GEOM, SM, MG, CF, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sh);
     if (e != cudaSuccess) return e;
   }
-  k_track<GEOM, SM, MG, CF><<<grid, block, sh, s>>>(a);
+  k_track<GEOM, SM, MG, CF, ST><<<grid, block, sh, s>>>(a);
   return cudaGetLastError();
 }
 
+// the block tallies are built only with the shared-memory cell table (small meshes)
 template <int GEOM, bool MG, bool CF = false>
-cudaError_t launch_geom(const TrackArgs& a, int block, int grid, bool sm, cudaStream_t s) {
-  return sm ? launch_one<GEOM, true, MG, CF>(a, block, grid, s) : launch_one<GEOM, false, MG, CF>(a, block, grid, s);
+cudaError_t launch_geom(const TrackArgs& a, int block, int grid, bool sm, bool st, cudaStream_t s) {
+  if (sm && st) return launch_one<GEOM, true, MG, CF, true>(a, block, grid, s);
+  return sm ? launch_one<GEOM, true, MG, CF, false>(a, block, grid, s)
+            : launch_one<GEOM, false, MG, CF, false>(a, block, grid, s);
 }
 
 // Fixed-point tallies to the FP64 outputs: deposition per unit volume per (group, cell),
-// escaped energy per side and (MG) per group.
+// escaped energy per side and (MG) per group, and the path-length intensity.
+// cellf[q] = (1/V, si factor): a factor > 0 is 1/(sigma_a V dt) and the cell's intensity is
+// its deposited energy times it (the sum over the cell's flights of (w - w') / (sigma_a V dt));
+// < 0 is -1/(V dt), the cell has no absorption and si holds the raw sum of w*s.
 __global__ void k_tally_finalize(TrackArgs a) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   const double W = *a.wsum;
   const int ncg = a.nc * a.ng;
-  if (q < ncg) a.dep[q] = fx_energy(a.dep_fx[q], W) * a.cellf[q].x;
+  if (q < ncg) {
+    const double2 cf = a.cellf[q];
+    const double E = fx_energy(a.dep_fx[q], W);
+    a.dep[q] = E * cf.x;
+    a.si[q] = cf.y > 0.0 ? E * cf.y : a.si[q] * -cf.y;
+  }
   else if (q < ncg + 4) a.escaped[q - ncg] = fx_energy(a.esc_fx[q - ncg], W);
   else if (q < ncg + 4 + a.ng && a.ng > 1) a.escaped_group[q - ncg - 4] = fx_energy(a.esc_fx[q - ncg], W);
 }
@@ -462,30 +502,30 @@ cudaError_t imc_launch_tally_finalize(const TrackArgs& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool sm, cudaStream_t s) {
+cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool sm, bool st, cudaStream_t s) {
   ++g_imc_launches;
   if (a.ng > 1) {  // multigroup: 2-D (MG_IMC/MG_IMC2D.py) and the 1-D sphere (MG_IMC/MG_IMC1D.py)
     switch (geom) {
-      case G_SPHERE: return launch_geom<G_SPHERE, true>(a, block, grid, sm, s);
-      case G_XY: return launch_geom<G_XY, true>(a, block, grid, sm, s);
-      case G_RZ: return launch_geom<G_RZ, true>(a, block, grid, sm, s);
+      case G_SPHERE: return launch_geom<G_SPHERE, true>(a, block, grid, sm, st, s);
+      case G_XY: return launch_geom<G_XY, true>(a, block, grid, sm, st, s);
+      case G_RZ: return launch_geom<G_RZ, true>(a, block, grid, sm, st, s);
       default: return cudaErrorInvalidValue;
     }
   }
   if (a.cf_rate) {  // Carter-Forest, gray
     switch (geom) {
-      case G_SLAB: return launch_geom<G_SLAB, false, true>(a, block, grid, sm, s);
-      case G_SPHERE: return launch_geom<G_SPHERE, false, true>(a, block, grid, sm, s);
-      case G_XY: return launch_geom<G_XY, false, true>(a, block, grid, sm, s);
-      case G_RZ: return launch_geom<G_RZ, false, true>(a, block, grid, sm, s);
+      case G_SLAB: return launch_geom<G_SLAB, false, true>(a, block, grid, sm, st, s);
+      case G_SPHERE: return launch_geom<G_SPHERE, false, true>(a, block, grid, sm, st, s);
+      case G_XY: return launch_geom<G_XY, false, true>(a, block, grid, sm, st, s);
+      case G_RZ: return launch_geom<G_RZ, false, true>(a, block, grid, sm, st, s);
       default: return cudaErrorInvalidValue;
     }
   }
   switch (geom) {
-    case G_SLAB: return launch_geom<G_SLAB, false>(a, block, grid, sm, s);
-    case G_SPHERE: return launch_geom<G_SPHERE, false>(a, block, grid, sm, s);
-    case G_XY: return launch_geom<G_XY, false>(a, block, grid, sm, s);
-    case G_RZ: return launch_geom<G_RZ, false>(a, block, grid, sm, s);
+    case G_SLAB: return launch_geom<G_SLAB, false>(a, block, grid, sm, st, s);
+    case G_SPHERE: return launch_geom<G_SPHERE, false>(a, block, grid, sm, st, s);
+    case G_XY: return launch_geom<G_XY, false>(a, block, grid, sm, st, s);
+    case G_RZ: return launch_geom<G_RZ, false>(a, block, grid, sm, st, s);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -317,7 +317,10 @@ class Engine:
         par.block_size = int(self.launch["block_size"])
         par.blocks_per_sm = int(self.launch["blocks_per_sm"])
         par.chunk = int(self.launch["chunk"])
-        par.reserved = int(bool(self.launch.get("smem_cells", 0)))
+        # bit 0: shared-memory cell table; block tallies in shared memory: bit 1 on, bit 2 off
+        # (launch["smem_tally"] 1 / 0; absent or None: the library's default)
+        st = self.launch.get("smem_tally")
+        par.reserved = int(bool(self.launch.get("smem_cells", 0))) | (2 if st == 1 else 4 if st == 0 else 0)
         par.emission_fractions = _ptr(self.emission_fractions)
         for q, n in enumerate(n_boundary_side or ()):
             par.n_boundary_side[q] = int(n)
