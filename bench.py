@@ -40,6 +40,7 @@ METRIC = "IMC track-segments/s and FOM=1/(rel.var*time) on 1 B200: plain vs batc
 UNIT = "track-segments/s"
 B_SEG_2D = 72  # bytes per 2-D gray segment: 36-byte record loaded + stored
 B_SEG_2D_MG = 80  # 2-D multigroup: the 36-byte record plus the group index, loaded + stored
+B_SEG_1D = 56  # 1-D gray: a 28-byte record loaded + stored
 # DRAM bytes the tracking kernel actually moves per segment on this workload: ncu
 # dram__bytes_read.sum + dram__bytes_write.sum of one full-size launch (401.4 MB for
 # 66.79 M segments); the histories stay in registers across their events.
@@ -540,12 +541,15 @@ def form_other_configs(steps: int = 20, warmup: int = 5) -> dict:
     st = imc1d.init_simulation(p["Ntarget"], p["Tinit"], p["Tr_init"], p["mesh"], p["eos_dev"], p["inv_eos_dev"],
                                seed=0xC0F1)
 
+    track = []  # tracking kernel time per step (ms, CUDA events in the library)
+
     def slab(st, n):
         seg = 0
         for _ in range(n):
             st, info = imc1d.step(st, p["Ntarget"], p["Nboundary"], 0, p["Nmax"], p["T_boundary"], p["dt"],
                                   p["mesh"], p["sigma_dev"], p["inv_eos_dev"], p["cv_dev"], p["source"])
             seg += info["profiling"]["transport_events"]["total"]
+            track.append(info["profiling"]["phase_times_s"]["transport"] * 1e3)
         return st, seg
 
     q = problems.marshak_mg()
@@ -559,19 +563,29 @@ def form_other_configs(steps: int = 20, warmup: int = 5) -> dict:
                                      q["edges1"], q["edges2"], q["energy_edges"], q["sigma_dev"], q["inv_eos_dev"],
                                      q["cv_dev"], q["source"], reflect=q["reflect"], geometry="xy")
             seg += info["profiling"]["transport_events"]["total"]
+            track.append(info["profiling"]["phase_times_s"]["transport"] * 1e3)
         return sm, seg
 
-    for tag, fn, s0 in (("slab_marshak_100_cells", slab, st), ("mg_marshak_200x10", mg, sm)):
+    peak, peak_kind = measured_peaks()
+    for tag, fn, s0, bseg, kern in (("slab_marshak_100_cells", slab, st, B_SEG_1D, "k_track<slab>"),
+                                    ("mg_marshak_200x10", mg, sm, B_SEG_2D_MG, "k_track<XY, multigroup>")):
         s0, _ = fn(s0, warmup)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
+        track.clear()
         e0.record()
         s0, seg = fn(s0, steps)
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
+        t_launch = float(np.mean(track)) * 1e-3
+        achieved = bseg * (seg / steps) / t_launch / 1e9
         out[tag] = {"steps": steps, "after_warmup_steps": warmup, "ms_per_step": ms / steps,
-                    "segments_per_step": seg / steps, "segments_per_s": seg / (ms * 1e-3)}
+                    "segments_per_step": seg / steps, "segments_per_s": seg / (ms * 1e-3),
+                    "track_ms_per_launch": t_launch * 1e3,
+                    "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                                 "frac": achieved / peak, "kernel": kern, "peak_source": peak_kind,
+                                 "bytes_per_segment_algorithmic": bseg}}
     return out
 
 

@@ -113,8 +113,13 @@ typedef struct imc_step_params {
                                    (sides 0/1: ny entries, 2/3: nx entries; 1-D: 1) */
   int64_t max_events;           /* events per history cap (2-D reference); <= 0: none */
   int32_t rz_linear_source;     /* RZ emission with the linear r/z tilt */
-  int32_t mg_reference_rules;   /* unused, must be 0: the multigroup event rules follow the
-                                   geometry (MG_IMC2D in xy / rz, MG_IMC1D on the sphere) */
+  int32_t census_bins;          /* 0, or IMC_CENSUS_BY_CELL / IMC_CENSUS_BY_GROUP_CELL: the tracking
+                                   kernel also sums the energy of the entries alive at the end of
+                                   the step per comb bin (cell, or (group, cell)) and counts them,
+                                   into the workspace, as each history ends; an imc_comb_async /
+                                   imc_comb_async_dev that follows on the same workspace and bank
+                                   with the flag IMC_COMB_CENSUS_READY (and the matching
+                                   IMC_COMB_PER_GROUP) uses them instead of a pass of its own */
   double t_emit_floor;
   int32_t block_size;           /* tracking launch shape; 0 = tuned default */
   int32_t blocks_per_sm;
@@ -237,7 +242,9 @@ IMC_API imc_status imc_material_update(const imc_mesh* mesh, const imc_tallies* 
  * once with its weight); n_max < 0 combs to |n_max| when at least |n_max| entries are
  * alive, else only drops dead entries (MG_IMC/MG_IMC1D.py:1194-1200).
  * disc[bin] = energy before - after. */
-enum { IMC_COMB_PER_GROUP = 1, IMC_COMB_CONSERVE_RADIATION = 2 };
+enum { IMC_COMB_PER_GROUP = 1, IMC_COMB_CONSERVE_RADIATION = 2,
+       IMC_COMB_CENSUS_READY = 4 /* async forms: the census sums come from the tracking call */ };
+enum { IMC_CENSUS_BY_CELL = 1, IMC_CENSUS_BY_GROUP_CELL = 2 };
 IMC_API imc_status imc_comb(const imc_mesh* mesh, const imc_bank* in, imc_bank* out, int64_t n_max,
                     uint64_t seed, uint32_t step, int32_t per_group, double* disc,
                     void* workspace, size_t workspace_bytes, imc_comb_report* report,

@@ -31,7 +31,8 @@ STATUS = {
 }
 OK, BANK_OVERFLOW = 0, 1
 
-COMB_PER_GROUP, COMB_CONSERVE_RADIATION = 1, 2  # imc_comb flags
+COMB_PER_GROUP, COMB_CONSERVE_RADIATION, COMB_CENSUS_READY = 1, 2, 4  # imc_comb flags
+CENSUS_BY_CELL, CENSUS_BY_GROUP_CELL = 1, 2  # imc_step_params.census_bins
 METHOD_FLECK_CUMMINGS, METHOD_CARTER_FOREST = 0, 1  # imc_step_params.method
 
 STAT_EVENTS, STAT_BOUNDARY, STAT_SCATTER, STAT_CENSUS, STAT_CAPTURE, STAT_FLOOR, STAT_REFLECT, STAT_CAP, STAT_ESCAPE, STAT_N = range(10)
@@ -63,7 +64,7 @@ class ImcStepParams(ctypes.Structure):
         ("n_target", c_int64), ("n_boundary", c_int64), ("n_source", c_int64),
         ("face_T", c_void_p * 4),
         ("max_events", c_int64),
-        ("rz_linear_source", c_int32), ("mg_reference_rules", c_int32),
+        ("rz_linear_source", c_int32), ("census_bins", c_int32),
         ("t_emit_floor", c_double),
         ("block_size", c_int32), ("blocks_per_sm", c_int32), ("chunk", c_int32), ("reserved", c_int32),
         ("emission_fractions", c_void_p),

@@ -114,6 +114,9 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   if (!bank_ok(bank, two_d, mg) || !workspace) return IMC_ERR_INVALID_ARG;
   if (!(par->dt > 0.0) || par->n_target < 0 || par->n_boundary < 0 || par->n_source < 0) return IMC_ERR_INVALID_ARG;
   if (!(par->energy_share >= 0.0 && par->energy_share <= 1.0)) return IMC_ERR_INVALID_ARG;
+  if (par->census_bins < 0 || par->census_bins > IMC_CENSUS_BY_GROUP_CELL ||
+      (par->census_bins == IMC_CENSUS_BY_GROUP_CELL && mesh->n_groups < 2))
+    return IMC_ERR_INVALID_ARG;
   const double share = par->energy_share > 0.0 ? par->energy_share : 1.0;
   for (int q = 0; q < 4; ++q) if (par->n_boundary_side[q] < 0) return IMC_ERR_INVALID_ARG;
   const bool cf = par->method == IMC_METHOD_CARTER_FOREST;
@@ -323,6 +326,15 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   ta.cf_fastpath = (float)par->cf_fastpath;
   ta.dt_dev = par->dt_dev; ta.step_dev = par->step_dev;
   ta.id_base = par->id_base;
+  if (par->census_bins && !adj) {
+    // census sums for the comb that follows on this workspace (IMC_COMB_CENSUS_READY)
+    const int nb = par->census_bins == IMC_CENSUS_BY_GROUP_CELL ? nc * ng : nc;
+    ta.ecen = ws_ptr<double>(workspace, L.ecen);
+    ta.n_live = ws_ptr<unsigned long long>(workspace, L.comb_mode + 8);
+    ta.ecen_by_group = par->census_bins == IMC_CENSUS_BY_GROUP_CELL ? 1 : 0;
+    IMC_CUDA(cudaMemsetAsync(ta.ecen, 0, sizeof(double) * nb, s));
+    IMC_CUDA(cudaMemsetAsync(ta.n_live, 0, sizeof(unsigned long long), s));
+  }
   int rm = 0;
   for (int q = 0; q < 4; ++q) if (par->reflect[q]) rm |= 1 << q;
   ta.reflect_mask = rm;
@@ -362,6 +374,7 @@ imc_status comb_async(const imc_mesh* mesh, const imc_bank* in, imc_bank* out, i
   if (!bank_ok(in, two_d) || !bank_ok(out, two_d) || !disc || !workspace || !sum) return IMC_ERR_INVALID_ARG;
   if (in->pos1 == out->pos1 || in->weight == out->weight) return IMC_ERR_INVALID_ARG;
   const bool by_group = (per_group & IMC_COMB_PER_GROUP) != 0;
+  const bool census_ready = (per_group & IMC_COMB_CENSUS_READY) != 0;  // sums made by the tracking
   if (by_group && (!in->group || !out->group)) return IMC_ERR_INVALID_ARG;
   const WsLayout L = imc_ws_layout(mesh, in->size);
   if (workspace_bytes < L.total) return IMC_ERR_WORKSPACE;
@@ -377,7 +390,7 @@ imc_status comb_async(const imc_mesh* mesh, const imc_bank* in, imc_bank* out, i
   ca.w = in->weight; ca.cell = in->cell; ca.group = in->group;
   ca.p1 = in->pos1; ca.p2 = two_d ? in->pos2 : nullptr; ca.d1 = in->dir1; ca.d2 = two_d ? in->dir2 : nullptr;
   ca.ecen = ws_ptr<double>(workspace, L.ecen); ca.ew = ws_ptr<double>(workspace, L.ew);
-  ca.ncopy = ws_ptr<double>(workspace, L.ncopy); ca.cnt = ws_ptr<int>(workspace, L.cnt);
+  ca.ncopy = ws_ptr<unsigned long long>(workspace, L.ncopy); ca.cnt = ws_ptr<int>(workspace, L.cnt);
   ca.blk = ws_ptr<long long>(workspace, L.blk);
   ca.seed = seed; ca.step = step; ca.step_dev = step_dev;
   ca.op1 = out->pos1; ca.op2 = two_d ? out->pos2 : nullptr; ca.od1 = out->dir1; ca.od2 = two_d ? out->dir2 : nullptr;
@@ -385,11 +398,15 @@ imc_status comb_async(const imc_mesh* mesh, const imc_bank* in, imc_bank* out, i
   ca.disc = disc;
   ca.sum = sum;
 
-  IMC_CUDA(cudaMemsetAsync(ca.ecen, 0, sizeof(double) * nb, s));
-  IMC_CUDA(cudaMemsetAsync(ca.ncopy, 0, sizeof(double) * nb, s));
+  IMC_CUDA(cudaMemsetAsync(ca.ncopy, 0, sizeof(unsigned long long) * nb, s));
   IMC_CUDA(cudaMemsetAsync(&sum->comb_after, 0, sizeof(double), s));
-  IMC_CUDA(cudaMemsetAsync(ca.mode, 0, 16, s));
-  IMC_CUDA(imc_launch_comb_ecen(ca, s));
+  if (census_ready) {
+    IMC_CUDA(cudaMemsetAsync(ca.mode, 0, 8, s));  // the live count (next 8 bytes) is the tracking's
+  } else {
+    IMC_CUDA(cudaMemsetAsync(ca.ecen, 0, sizeof(double) * nb, s));
+    IMC_CUDA(cudaMemsetAsync(ca.mode, 0, 16, s));
+    IMC_CUDA(imc_launch_comb_ecen(ca, s));
+  }
   CombPlanArgs cp{};
   cp.nb = nb; cp.ecen = ca.ecen; cp.ew = ca.ew; cp.sum = sum;
   // n_max > 0: comb to n_max; 0: keep every live entry; < 0: comb to |n_max| once at least

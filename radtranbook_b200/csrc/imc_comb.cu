@@ -41,7 +41,7 @@ __device__ __forceinline__ bool bin_ok(const CombArgs& a, int b) {
 // weight of every copy in bin b: the comb weight, or the bin's energy shared equally
 __device__ __forceinline__ float copy_weight(const CombArgs& a, int b) {
   if (!a.conserve_rad) return (float)a.ew[b];
-  const double n = a.ncopy[b];
+  const double n = (double)a.ncopy[b];
   return n > 0.0 ? (float)(a.ecen[b] / n) : 0.f;
 }
 
@@ -81,9 +81,8 @@ __global__ void __launch_bounds__(256) k_comb_ecen(CombArgs a) {
 __global__ void __launch_bounds__(CB) k_comb_count(CombArgs a) {
   const uint32_t step = a.step_dev ? *a.step_dev : a.step;  // graph replay
   __shared__ long long sh[CB / 32];
-  __shared__ WarpStage stages[CB / 32];
-  __shared__ BlockBins<CB> t;
-  bins_init(t);
+  __shared__ BlockCounts<CB> t;
+  counts_init(t);
   __syncthreads();
   const long long k = (long long)blockIdx.x * CB + threadIdx.x;
   const long long n_in = min((long long)*a.d_n_in, (long long)a.n_bound);  // the grid covers n_bound entries
@@ -105,11 +104,11 @@ __global__ void __launch_bounds__(CB) k_comb_count(CombArgs a) {
     a.cnt[k] = n;
   }
   // copies per bin: aggregated per warp, then per block (the bank is largely grouped by cell)
-  warp_bins_add(n > 0, b, (double)n, t, a.ncopy, stages + (threadIdx.x >> 5));
+  warp_counts_add(n > 0, b, (unsigned)n, t, a.ncopy);
   const unsigned ws = __reduce_add_sync(FULL, (unsigned)n);
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = ws;
   __syncthreads();
-  bins_flush(t, a.ncopy);
+  counts_flush(t, a.ncopy);
   if (threadIdx.x < 32) {
     unsigned long long v = sh[threadIdx.x];
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
@@ -195,7 +194,7 @@ __global__ void k_comb_disc(CombArgs a) {
   double after = 0.0;
   if (b < a.nb) {
     // compact only: every live entry kept with its weight, nothing is lost
-    after = *a.mode != 0 ? a.ecen[b] : a.ncopy[b] * (double)copy_weight(a, b);
+    after = *a.mode != 0 ? a.ecen[b] : (double)a.ncopy[b] * (double)copy_weight(a, b);
     a.disc[b] = a.ecen[b] - after;
   }
   after = warp_sum_d(after);

@@ -208,6 +208,50 @@ __device__ __forceinline__ void bins_flush(BlockBins<S>& t, double* __restrict__
     if (t.key[i] >= 0) atomicAdd(global + t.key[i], t.val[i]);
 }
 
+// The same per-block aggregation for integer counts (32-bit shared-memory adds, exact).
+template <int S>
+struct BlockCounts {
+  int key[S];
+  unsigned val[S];
+};
+
+template <int S>
+__device__ __forceinline__ void counts_init(BlockCounts<S>& t) {
+  for (int i = threadIdx.x; i < S; i += blockDim.x) { t.key[i] = -1; t.val[i] = 0u; }
+}
+
+template <int S>
+__device__ __forceinline__ void counts_add(BlockCounts<S>& t, int bin, unsigned v,
+                                           unsigned long long* __restrict__ global) {
+  const unsigned h = ((unsigned)bin * 2654435761u) >> 8;
+#pragma unroll 1
+  for (int p = 0; p < BINS_PROBES; ++p) {
+    const int s = (int)((h + (unsigned)p) & (unsigned)(S - 1));
+    const int old = atomicCAS(&t.key[s], -1, bin);
+    if (old == -1 || old == bin) { atomicAdd(&t.val[s], v); return; }
+  }
+  atomicAdd(global + bin, (unsigned long long)v);
+}
+
+// every lane calls it (converged): per-warp groups by bin (lanes' counts summed with the
+// group's leader), then one shared-memory add per group
+template <int S>
+__device__ __forceinline__ void warp_counts_add(bool add, int key, unsigned v, BlockCounts<S>& t,
+                                                unsigned long long* __restrict__ global) {
+  const unsigned fm = __ballot_sync(FULL, add);
+  if (fm == 0u) return;
+  const int lane = threadIdx.x & 31;
+  const unsigned peers = __match_any_sync(FULL, add ? key : -1 - lane);
+  const unsigned s = __reduce_add_sync(peers, add ? v : 0u);  // the group's sum, on every member
+  if (add && (__ffs(peers) - 1) == lane) counts_add(t, key, s, global);
+}
+
+template <int S>
+__device__ __forceinline__ void counts_flush(BlockCounts<S>& t, unsigned long long* __restrict__ global) {
+  for (int i = threadIdx.x; i < S; i += blockDim.x)
+    if (t.key[i] >= 0) atomicAdd(global + t.key[i], (unsigned long long)t.val[i]);
+}
+
 // ---- energy tallies in 64-bit fixed point ----
 // Deposited and escaped energy are summed as integers in units of q = W * 2^-60, W the
 // total weight tracked in the step (an upper bound of every such sum, so no total exceeds

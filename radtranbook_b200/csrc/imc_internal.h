@@ -47,6 +47,11 @@ struct TrackArgs {
   const double* dt_dev;      // non-NULL: the step length is read from device memory (graph replay)
   const uint32_t* step_dev;  // non-NULL: the Philox step counter is read from device memory
   uint32_t id_base;          // Philox particle id of bank entry k is id_base + k
+  // census sums for the comb (NULL: none): energy of the entries alive at the end of the
+  // step per bin (cell, + nc * group when ecen_by_group) and their count
+  double* ecen;
+  unsigned long long* n_live;
+  int ecen_by_group;
 };
 
 // smem_tally: per-block deposition / intensity tallies in shared memory (with smem_cells only)
@@ -86,7 +91,7 @@ struct WsLayout {
   size_t mg_gcdf, mg_ec, mg_cdf, mg_sgcdf, mg_sc, mg_scdf, mixcdf;  // multigroup tables
   size_t summary;             // imc_step_summary used by the synchronous wrappers
   size_t queue;               // uint64 ticket counter
-  size_t ecen, ew, ncopy;     // comb: double [nb], double [nb], long long [nb]
+  size_t ecen, ew, ncopy;     // comb: double [nb], double [nb], uint64 [nb]
   size_t cnt;                 // int32 [cap]    comb copies per entry
   size_t blk;                 // int64 [nblk+1] comb block totals / offsets
   size_t comb_mode;           // int32 mode + uint64 live-entry count (comb)
@@ -231,7 +236,7 @@ struct CombArgs {
   long long out_capacity;
   const float* w; const int* cell; const int* group;
   const float* p1; const float* p2; const float* d1; const float* d2;
-  double* ecen; double* ew; double* ncopy; int* cnt; long long* blk;  // ncopy: copies per bin (exact in FP64)
+  double* ecen; double* ew; unsigned long long* ncopy; int* cnt; long long* blk;  // ncopy: copies per bin
   uint64_t seed; uint32_t step;
   float* op1; float* op2; float* od1; float* od2; float* ow; float* ot; int* ocell; int* ogroup;
   double* disc;

@@ -94,6 +94,7 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   float w_in = 0.f;
   double acc_wd = 0.0;  // w*s in the current cell (cells without absorption only)
   unsigned s_bd = 0, s_sc = 0;          // per-event counters (census/cap counted at finish)
+  unsigned n_alive = 0;                 // entries alive at the end (census sums for the comb)
 
   const float c_light = (float)C_LIGHT;
   // weight floor, IMC/IMC1D.py:1007 / IMC/IMC2D.py:1771 (1e-10); MG_IMC/MG_IMC1D.py:1127 (1e-14)
@@ -129,7 +130,16 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
         pid = chunk_next + rank;
         w = a.w[pid];
         dcen = (dtk - a.t[pid]) * c_light;
-        if ((MG2 || CF ? w > weight_floor : w > 0.f) && dcen > 0.f) {
+        const bool moves = (MG2 || CF ? w > weight_floor : w > 0.f) && dcen > 0.f;
+        if (!moves && w > 0.f && a.ecen) {
+          // not tracked but alive: part of the census the comb sees
+          const int b = a.cell[pid] + (a.ecen_by_group ? a.nc * a.group[pid] : 0);
+#ifdef IMC_CHECKED
+          if (b >= 0 && b < a.nc * (a.ecen_by_group ? a.ng : 1))
+#endif
+          { atomicAdd(a.ecen + b, (double)w); ++n_alive; }
+        }
+        if (moves) {
           x = a.p1[pid]; u = a.d1[pid];
           if (MG) grp = a.group[pid];
           if (GEOM == G_XY || GEOM == G_RZ) { y = a.p2[pid]; v = a.d2[pid]; }
@@ -169,6 +179,8 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
     bool flush = false;
     int flush_cell = 0;
     double f_lost = 0.0, f_wd = 0.0;
+    bool cen = false;  // this history ended alive: its weight goes to the comb's census sums
+    int cen_bin = 0;
     if (has) {
       const int c = ci + a.nx * cj;
       const int cq = MG ? c + a.nc * grp : c;  // (group, cell) table / tally index
@@ -408,6 +420,8 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
           a.p1[pid] = x; a.d1[pid] = u;
           if (GEOM == G_XY || GEOM == G_RZ) { a.p2[pid] = y; a.d2[pid] = v; }
           a.cell[pid] = ci + a.nx * cj;
+          cen = true;
+          cen_bin = ci + a.nx * cj + (a.ecen_by_group ? a.nc * grp : 0);
         }
         has = false;
       }
@@ -421,10 +435,18 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
       vs = f_wd;
     }
     warp_tally_fx(flush, flush_cell, ud, vs, dep_t, si_t, st);
+    if (a.ecen) {
+      warp_tally1(cen, cen_bin, (double)w, a.ecen, st);
+      n_alive += cen ? 1u : 0u;
+    }
   }
 
   // ---------------- statistics ----------------
   const unsigned long long t_bd = warp_sum_u(s_bd), t_sc = warp_sum_u(s_sc);
+  if (a.ecen) {
+    const unsigned long long t_alive = warp_sum_u(n_alive);
+    if (lane == 0 && t_alive) atomicAdd(a.n_live, t_alive);
+  }
   if (lane == 0) {
     if (t_bd) atomicAdd(a.stats + S_BOUNDARY, t_bd);
     if (t_sc) atomicAdd(a.stats + S_SCATTER, t_sc);

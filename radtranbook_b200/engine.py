@@ -162,6 +162,10 @@ class Engine:
         # offset and share of the source energy; its comb and initial census use comb_seed
         self.id_base = 0
         self.energy_share = 1.0
+        # the asynchronous step's tracking sums the census per comb bin (cells, or (group, cell)
+        # on a multigroup mesh) and the comb that follows uses those sums
+        self.fuse_census = True
+        self._census_bins = 0
 
     @property
     def seed(self) -> int:
@@ -353,6 +357,10 @@ class Engine:
         self._par = self._params(step, dt, theta, n_target, n_boundary, n_source, face_T, reflect, max_events,
                                  rz_linear_source, t_emit_floor, n_boundary_side, method, cf_fastpath,
                                  step_dev, dt_dev)
+        self._census_bins = 0
+        if self.fuse_census:
+            self._census_bins = _lib.CENSUS_BY_GROUP_CELL if self.ng > 1 else _lib.CENSUS_BY_CELL
+        self._par.census_bins = self._census_bins
         bound = int(self.lib.imc_source_bound(ctypes.byref(self.cmesh), ctypes.byref(self._par)))
         self.bank.ensure(self.bank.size + bound)
         wsp, wsn = self._ws(self.bank.capacity)
@@ -378,8 +386,12 @@ class Engine:
         self.spare.ensure(want + 2 * self.nc * self.ng + 4096)
         if n_max_dev is not None and (step_dev is None or n_max <= 0):
             raise ValueError("n_max_dev needs step_dev and n_max > 0")
-        self._comb_args = (int(n_max), int(step), e, _comb_flags(per_group, conserve_radiation), step_dev,
-                           out_capacity, n_max_dev)
+        flags = _comb_flags(per_group, conserve_radiation)
+        want_bins = _lib.CENSUS_BY_GROUP_CELL if per_group else _lib.CENSUS_BY_CELL
+        if self._census_bins and self._census_bins == want_bins:
+            flags |= _lib.COMB_CENSUS_READY  # the tracking of this bank summed its census
+        self._census_bins = 0
+        self._comb_args = (int(n_max), int(step), e, flags, step_dev, out_capacity, n_max_dev)
         self._launch_comb()
 
     def _launch_comb(self) -> None:
