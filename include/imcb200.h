@@ -234,6 +234,27 @@ IMC_API imc_status imc_step_transport(const imc_mesh* mesh, const imc_material* 
 IMC_API imc_status imc_material_update(const imc_mesh* mesh, const imc_tallies* tal, double* e,
                                double* tr, void* stream);
 
+/* A gray material whose laws the device evaluates itself: linear EOS e = cv_eos * T, heat
+ * capacity cv, and opacity sigma(T) = sigma_A * T^-sigma_n clamped to [sigma_lo, sigma_hi]
+ * (a bound <= 0 is no bound; sigma_n = 0 is a constant).  Each *_array, when set, is a
+ * DEVICE array [c] that replaces its scalar (per-cell, temperature-independent values). */
+typedef struct imc_material_law {
+  double cv_eos;          const double* cv_eos_array;
+  double cv;              const double* cv_array;
+  double sigma_A, sigma_n, sigma_lo, sigma_hi;
+  const double* sigma_array;
+} imc_material_law;
+
+/* imc_material_update and the material temperature of the next step in one kernel (gray
+ * meshes): e and tr as imc_material_update, then T = e / cv_eos (the inverse EOS,
+ * IMC/IMC1D.py:1024 inv_eos), and the next step's sigma(T) and cv(T) of the law into
+ * sigma_next / cv_next (IMC/IMC1D.py:932-935 sigma_a_func(T), cv(T)), which a step's
+ * imc_material then takes as they are. */
+IMC_API imc_status imc_material_update_law(const imc_mesh* mesh, const imc_tallies* tal,
+                                           const imc_material_law* law, double* e, double* tr,
+                                           double* T, double* sigma_next, double* cv_next,
+                                           void* stream);
+
 /* Stochastic comb of bank `in` into bank `out` (census times reset to 0).
  * per_group is a set of flags: IMC_COMB_PER_GROUP combs per (cell, group) bin (MG);
  * IMC_COMB_CONSERVE_RADIATION gives every copy in a bin the bin's pre-comb energy divided

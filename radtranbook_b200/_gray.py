@@ -101,6 +101,7 @@ class GrayState:
             t = torch.as_tensor(np.asarray(value, dtype=np.float64), device=self._engine.device)
             (self._e if name == "internal_energy" else self._T).copy_(self.flat(t))
             self._host.pop(name, None)
+            self.__dict__.pop("_law_next", None)  # the next step's opacity follows a new T
             return
         object.__setattr__(self, name, value)
 
@@ -212,10 +213,17 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
     dim = state._dim
     like = state.grid(state._T)
     host_T = lambda: state.temperature  # noqa: E731
-    # host callables' results go up by asynchronous copies from pinned buffers of the state
-    # (refilled only next step, after this step's end-of-step synchronisation)
-    sigma = state.flat(evaluate(sigma_a_func, like, host_T, like, **_staged(state, "sigma", eng.nc)))
-    cvv = state.flat(evaluate(cv, like, host_T, like, **_staged(state, "cv", eng.nc)))
+    # a material the device evaluates itself (LinearEOS, Constant, PowerLawOpacity): the
+    # material update, inverse EOS and next step's opacity are one kernel at the step's end
+    law = _law(state, sigma_a_func, cv, inv_eos) if not conserve_comb_energy else None
+    nxt = state.__dict__.get("_law_next")
+    if law is not None and nxt is not None and nxt[0] == (id(sigma_a_func), id(cv)):
+        sigma, cvv = nxt[1], nxt[2]  # evaluated on the device at the end of the last step
+    else:
+        # host callables' results go up by asynchronous copies from pinned buffers of the state
+        # (refilled only next step, after this step's end-of-step synchronisation)
+        sigma = state.flat(evaluate(sigma_a_func, like, host_T, like, **_staged(state, "sigma", eng.nc)))
+        cvv = state.flat(evaluate(cv, like, host_T, like, **_staged(state, "cv", eng.nc)))
     src = None
     if Nsource > 0 and source is not None:
         src_t = source.double() if isinstance(source, torch.Tensor) else torch.as_tensor(
@@ -239,9 +247,20 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
     # material update: e += dep - emitted/V ; Tr from the path-length intensity.  The comb
     # does not need T: with a host inv_eos (and the comb discrepancy not booked into e), e is
     # copied out before the comb is queued, so the host evaluation overlaps the comb.
-    eng.material_update(state._e, state._Tr)
+    if law is not None:
+        nb = state.__dict__.get("_law_buf")
+        if nb is None or nb[0].numel() != eng.nc:
+            nb = tuple(torch.empty(eng.nc, dtype=torch.float64, device=eng.device) for _ in range(4))
+            object.__setattr__(state, "_law_buf", nb)
+        # two buffer pairs: the step reads one pair (its sigma, cv) while it writes the other
+        pair = nb[:2] if sigma.data_ptr() != nb[0].data_ptr() else nb[2:]
+        eng.material_update_law(state._e, state._Tr, state._T, law[0], pair[0], pair[1])
+        state.__dict__["_law_next"] = ((id(sigma_a_func), id(cv)), pair[0], pair[1])
+    else:
+        state.__dict__.pop("_law_next", None)
+        eng.material_update(state._e, state._Tr)
     e_ready = None
-    if not conserve_comb_energy and not is_device(inv_eos):
+    if law is None and not conserve_comb_energy and not is_device(inv_eos):
         e_pin = _pinned(state, "e_mid", eng.nc)
         e_pin.copy_(state._e, non_blocking=True)
         e_ready = torch.cuda.Event()
@@ -250,15 +269,18 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
     if conserve_comb_energy:
         sum_tensors(dist, [eng.disc])
         state._e.add_(eng.disc[: eng.nc] / eng.vol)
-    if e_ready is not None:
+    if law is not None:
+        pass  # T = e / cv came with the material update
+    elif e_ready is not None:
         def e_host():
             e_ready.synchronize()
             _lib.TRANSFER["d2h"] += e_pin.numel() * 8
             return e_pin.numpy().copy() if state._dim == 1 else e_pin.numpy().reshape(state._shape[1], state._shape[0]).T
         Tn = evaluate(inv_eos, state.grid(state._e), e_host, like, **_staged(state, "T_new", eng.nc))
+        state._T.copy_(state.flat(Tn))
     else:
         Tn = evaluate(inv_eos, state.grid(state._e), lambda: _host_copy(state.grid(state._e)), like)
-    state._T.copy_(state.flat(Tn))
+        state._T.copy_(state.flat(Tn))
     try:
         sm = eng.fetch(state.host_copies())
     except _lib.ImcError as ex:
@@ -349,6 +371,18 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
         te["absorption_capture_events"] = int(stats[_lib.STAT_CAPTURE])
         te["event_cap_hits"] = int(stats[_lib.STAT_CAP])
     return state, info
+
+
+def _law(state, sigma_a_func, cv, inv_eos):
+    """The device material law of these callables (cached on the state), or None."""
+    key = (id(sigma_a_func), id(cv), id(inv_eos))
+    cache = state.__dict__.get("_law_cache")
+    if cache is None or cache[0] != key:
+        from .materials import material_law
+
+        cache = (key, material_law(sigma_a_func, cv, inv_eos, state.flat, state._engine.device))
+        object.__setattr__(state, "_law_cache", cache)
+    return cache[1]
 
 
 def tune(state: GrayState, grid: dict | None = None, repeats: int = 2) -> dict:

@@ -74,6 +74,12 @@ class ImcStepParams(ctypes.Structure):
     ]
 
 
+class ImcMaterialLaw(ctypes.Structure):
+    _fields_ = [("cv_eos", c_double), ("cv_eos_array", c_void_p), ("cv", c_double), ("cv_array", c_void_p),
+                ("sigma_A", c_double), ("sigma_n", c_double), ("sigma_lo", c_double), ("sigma_hi", c_double),
+                ("sigma_array", c_void_p)]
+
+
 class ImcTallies(ctypes.Structure):
     _fields_ = [
         ("dep", c_void_p), ("si", c_void_p), ("emitted", c_void_p), ("sigma_a", c_void_p),
@@ -145,6 +151,8 @@ SIGNATURES = {
                                    POINTER(ImcBank), POINTER(ImcTallies), c_void_p, c_size_t,
                                    POINTER(ImcStepReport), c_void_p]),
     "imc_material_update": (c_int, [POINTER(ImcMesh), POINTER(ImcTallies), c_void_p, c_void_p, c_void_p]),
+    "imc_material_update_law": (c_int, [POINTER(ImcMesh), POINTER(ImcTallies), POINTER(ImcMaterialLaw), c_void_p,
+                                        c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "imc_comb": (c_int, [POINTER(ImcMesh), POINTER(ImcBank), POINTER(ImcBank), c_int64, c_uint64, c_uint32,
                          c_int32, c_void_p, c_void_p, c_size_t, POINTER(ImcCombReport), c_void_p]),
     "imc_comb_noalloc": (c_int, [POINTER(ImcMesh), POINTER(ImcBank), POINTER(ImcBank), c_int64, c_uint64,

@@ -261,6 +261,28 @@ __global__ void k_material(MatArgs a) {
   a.tr[c] = x > 0.0 ? sqrt(sqrt(x)) : 0.0;
 }
 
+// k_material, then T = e / cv_eos and the law's sigma(T), cv for the next step (gray)
+__global__ void k_material_law(MatArgs a, imc_material_law law, double* T, double* sigma_next, double* cv_next) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.nc) return;
+  const double e = a.e[c] + a.dep[c] - a.emitted[c] / a.vol[c];
+  a.e[c] = e;
+  const double x = a.si[c] / A_RAD / C_LIGHT;
+  a.tr[c] = x > 0.0 ? sqrt(sqrt(x)) : 0.0;
+  const double t = e / (law.cv_eos_array ? law.cv_eos_array[c] : law.cv_eos);
+  T[c] = t;
+  double sg;
+  if (law.sigma_array) {
+    sg = law.sigma_array[c];
+  } else {
+    sg = law.sigma_n == 0.0 ? law.sigma_A : law.sigma_A * pow(t, -law.sigma_n);
+    if (law.sigma_lo > 0.0) sg = fmax(sg, law.sigma_lo);
+    if (law.sigma_hi > 0.0) sg = fmin(sg, law.sigma_hi);
+  }
+  sigma_next[c] = sg;
+  cv_next[c] = law.cv_array ? law.cv_array[c] : law.cv;
+}
+
 // Single block: the canonical total of the census energy and the comb mode.
 __global__ void __launch_bounds__(NT) k_comb_plan(CombPlanArgs a) {
   __shared__ double red[NT];
@@ -309,6 +331,12 @@ cudaError_t imc_launch_ic_plan(const IcArgs& a, cudaStream_t s) {
 cudaError_t imc_launch_material(const MatArgs& a, cudaStream_t s) {
   ++g_imc_launches;
   k_material<<<(a.nc + 255) / 256, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+cudaError_t imc_launch_material_law(const MatArgs& a, const imc_material_law& law, double* T, double* sigma_next,
+                                    double* cv_next, cudaStream_t s) {
+  ++g_imc_launches;
+  k_material_law<<<(a.nc + 255) / 256, 256, 0, s>>>(a, law, T, sigma_next, cv_next);
   return cudaGetLastError();
 }
 cudaError_t imc_launch_comb_plan(const CombPlanArgs& a, cudaStream_t s) {

@@ -689,6 +689,22 @@ imc_status imc_material_update(const imc_mesh* mesh, const imc_tallies* tal, dou
   return IMC_OK;
 }
 
+imc_status imc_material_update_law(const imc_mesh* mesh, const imc_tallies* tal, const imc_material_law* law,
+                                   double* e, double* tr, double* T, double* sigma_next, double* cv_next,
+                                   void* stream) {
+  imc_status st = check_mesh(mesh);
+  if (st != IMC_OK) return st;
+  if (mesh->n_groups != 1) return IMC_ERR_INVALID_ARG;  // gray meshes
+  if (!tal || !tal->dep || !tal->si || !tal->emitted || !law || !e || !tr || !T || !sigma_next || !cv_next)
+    return IMC_ERR_INVALID_ARG;
+  if ((!law->cv_eos_array && !(law->cv_eos > 0.0)) || (!law->cv_array && !(law->cv > 0.0))) return IMC_ERR_INVALID_ARG;
+  MatArgs ma{};
+  ma.nc = mesh->nx * mesh->ny; ma.ng = 1; ma.vol = mesh->volume;
+  ma.dep = tal->dep; ma.si = tal->si; ma.emitted = tal->emitted; ma.e = e; ma.tr = tr;
+  IMC_CUDA(imc_launch_material_law(ma, *law, T, sigma_next, cv_next, (cudaStream_t)stream));
+  return IMC_OK;
+}
+
 imc_status imc_comb_async(const imc_mesh* mesh, const imc_bank* in, imc_bank* out, int64_t n_max, uint64_t seed,
                           uint32_t step, int32_t per_group, double* disc, const double* e, void* workspace,
                           size_t workspace_bytes, imc_step_summary* summary, void* stream) {

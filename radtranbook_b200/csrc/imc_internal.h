@@ -156,6 +156,9 @@ struct MatArgs {
   double* e; double* tr;
 };
 cudaError_t imc_launch_material(const MatArgs& a, cudaStream_t s);
+// the material update with the law's inverse EOS and next-step opacity / heat capacity
+cudaError_t imc_launch_material_law(const MatArgs& a, const imc_material_law& law, double* T, double* sigma_next,
+                                    double* cv_next, cudaStream_t s);
 
 struct CombPlanArgs {
   int nb;

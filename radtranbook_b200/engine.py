@@ -264,6 +264,13 @@ class Engine:
         _lib.check("imc_material_update", self.lib.imc_material_update(
             ctypes.byref(self.cmesh), ctypes.byref(self.ctal), _ptr(e), _ptr(tr), self._stream()))
 
+    def material_update_law(self, e, tr, T, law, sigma_next, cv_next) -> None:
+        """material_update, then T = e / cv and the next step's opacity and heat capacity of a
+        device-evaluated material law (imc_material_update_law), in one kernel."""
+        _lib.check("imc_material_update_law", self.lib.imc_material_update_law(
+            ctypes.byref(self.cmesh), ctypes.byref(self.ctal), ctypes.byref(law), _ptr(e), _ptr(tr), _ptr(T),
+            _ptr(sigma_next), _ptr(cv_next), self._stream()))
+
     def comb(self, n_max: int, step: int, per_group: bool = False, conserve_radiation: bool = False) -> ImcCombReport:
         """Comb the bank (n_max > 0: to n_max; 0: drop dead entries only; < 0: to |n_max| once
         at least |n_max| entries are alive)."""

@@ -98,14 +98,60 @@ class Constant:
         return np.broadcast_to(np.asarray(self.value, dtype=np.float64), np.shape(T))
 
 
+class _LinearEOSFunction:
+    """e = cv T (inverse=False) or T = e / cv (inverse=True), a device callable that carries
+    its heat capacity so the step can evaluate it on the device."""
+
+    _imc_device = True
+
+    def __init__(self, cv: Constant, inverse: bool):
+        self.cv, self.inverse = cv, inverse
+
+    def __call__(self, x):
+        return x / self.cv(x) if self.inverse else self.cv(x) * x
+
+
 class LinearEOS:
     """e = cv * T and its inverse, for a constant or per-cell cv (device callables)."""
 
     def __init__(self, cv):
         self.cv = Constant(cv)
-        self.eos = device_callable(lambda T: self.cv(T) * T)
-        self.inv_eos = device_callable(lambda e: e / self.cv(e))
+        self.eos = _LinearEOSFunction(self.cv, False)
+        self.inv_eos = _LinearEOSFunction(self.cv, True)
         self.cv_func = self.cv
+
+
+def material_law(sigma_a_func, cv, inv_eos, flat, device):
+    """The law of a gray material the device evaluates itself (imc_material_law), when the
+    callables are a LinearEOS inverse, a Constant heat capacity and a PowerLawOpacity or
+    Constant opacity; else None.  flat(tensor) puts a per-cell array in the engine's cell
+    order.  Returns (law, tensors the law points to)."""
+    from ._lib import ImcMaterialLaw
+
+    if not (isinstance(inv_eos, _LinearEOSFunction) and inv_eos.inverse and isinstance(cv, Constant)
+            and isinstance(sigma_a_func, (PowerLawOpacity, Constant))):
+        return None
+    keep = []
+
+    def scalar_or_array(const):
+        v = np.asarray(const.value, dtype=np.float64)
+        if v.ndim == 0:
+            return float(v), None
+        t = flat(torch.as_tensor(v, device=device)).contiguous()
+        keep.append(t)
+        return 0.0, t.data_ptr()
+
+    law = ImcMaterialLaw()
+    law.cv_eos, law.cv_eos_array = scalar_or_array(inv_eos.cv)
+    law.cv, law.cv_array = scalar_or_array(cv)
+    if isinstance(sigma_a_func, Constant):
+        law.sigma_A, law.sigma_array = scalar_or_array(sigma_a_func)
+        law.sigma_n = 0.0
+    else:
+        law.sigma_A, law.sigma_n = sigma_a_func.A, sigma_a_func.n
+        law.sigma_lo = float(sigma_a_func.lo) if sigma_a_func.lo is not None else 0.0
+        law.sigma_hi = float(sigma_a_func.hi) if sigma_a_func.hi is not None else 0.0
+    return law, keep
 
 
 class GroupedOpacity(list):

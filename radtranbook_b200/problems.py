@@ -22,7 +22,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from .materials import GroupedOpacity, device_callable
+from .materials import Constant, GroupedOpacity, LinearEOS, PowerLawOpacity, device_callable
 
 
 def marshak_slab(scale: float = 1.0) -> dict:
@@ -34,18 +34,16 @@ def marshak_slab(scale: float = 1.0) -> dict:
     def sigma_host(T):
         return 300.0 * np.power(T, -3.0)
 
-    @device_callable
-    def sigma_dev(T):
-        return 300.0 * torch.pow(T, -3.0)
-
+    # device versions: parametric materials the step evaluates on the device itself
+    eos = LinearEOS(cv_val)
     return dict(
         name="1-D gray slab Marshak wave (100 cells, sigma=300 T^-3)",
         geometry="slab", mesh=mesh, dim=1,
         Tinit=np.full(I, 0.001), Tr_init=np.full(I, 0.001),
-        sigma_host=sigma_host, sigma_dev=sigma_dev,
-        cv_host=lambda T: np.full_like(T, cv_val), cv_dev=device_callable(lambda T: torch.full_like(T, cv_val)),
+        sigma_host=sigma_host, sigma_dev=PowerLawOpacity(300.0, 3.0),
+        cv_host=lambda T: np.full_like(T, cv_val), cv_dev=eos.cv,
         eos_host=lambda T: cv_val * T, inv_eos_host=lambda e: e / cv_val,
-        eos_dev=device_callable(lambda T: cv_val * T), inv_eos_dev=device_callable(lambda e: e / cv_val),
+        eos_dev=eos.eos, inv_eos_dev=eos.inv_eos,
         Ntarget=int(20000 * scale), Nboundary=int(20000 * scale), Nsource=0, Nmax=int(80000 * scale),
         T_boundary=(1.0, 0.0), reflect=(False, False), dt=0.01, n_steps=100, source=np.zeros(I),
     )
@@ -69,29 +67,10 @@ def crooked_pipe(scale: float = 1.0, nr: int = 60, nz: int = 210) -> dict:
     thin = crooked_pipe_thin(R, Z)
     sig = np.where(thin, 0.2, 2000.0)
     cvg = np.where(thin, 0.001, 0.5)
-    cache = {}
-
-    def dev(a, T):
-        key = (id(a), T.device)
-        if key not in cache:
-            cache[key] = torch.as_tensor(a, dtype=torch.float64, device=T.device)
-        return cache[key]
-
-    @device_callable
-    def sigma_dev(T):
-        return dev(sig, T)
-
-    @device_callable
-    def cv_dev(T):
-        return dev(cvg, T)
-
-    @device_callable
-    def eos_dev(T):
-        return dev(cvg, T) * T
-
-    @device_callable
-    def inv_eos_dev(e):
-        return e / dev(cvg, e)
+    # device versions: parametric materials (per-cell constants, linear EOS) the step
+    # evaluates on the device itself
+    eos = LinearEOS(cvg)
+    sigma_dev, cv_dev, eos_dev, inv_eos_dev = Constant(sig), eos.cv, eos.eos, eos.inv_eos
 
     def bsf(r, z, side):
         return 0.5 if (side == "zmin" and r < 0.5) else 0.0

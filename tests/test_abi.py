@@ -51,7 +51,8 @@ def test_struct_layout_matches_header(tmp_path):
                "imc_step_params": _lib.ImcStepParams, "imc_tallies": _lib.ImcTallies,
                "imc_step_report": _lib.ImcStepReport, "imc_comb_report": _lib.ImcCombReport,
                "imc_step_summary": _lib.ImcStepSummary, "imc_batch": _lib.ImcBatch,
-               "imc_batch_state": _lib.ImcBatchState, "imc_batch_launch": _lib.ImcBatchLaunch}
+               "imc_batch_state": _lib.ImcBatchState, "imc_batch_launch": _lib.ImcBatchLaunch,
+               "imc_material_law": _lib.ImcMaterialLaw}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{ROOT}/include/imcb200.h"', "int main(){"]
     for cname, cls in structs.items():
         lines.append(f'printf("{cname} __sizeof__ %zu\\n", sizeof({cname}));')
