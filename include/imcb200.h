@@ -126,7 +126,9 @@ typedef struct imc_step_params {
   int32_t chunk;                /* histories claimed per warp ticket (guided: at most this) */
   int32_t reserved;             /* bit 0: shared-memory cell table (default: up to 4096 (group, cell)
                                    entries); bit 1: per-block tallies in shared memory with that
-                                   table, bit 2: never (default: up to 2048 entries); others ignored */
+                                   table, bit 2: never (default: up to 2048 entries); bit 3:
+                                   event-by-event tracking (workspace of imc_workspace_bytes_event);
+                                   others ignored */
   const double* emission_fractions; /* MG: [g] fixed emission spectrum, or NULL = Planck */
   int64_t n_boundary_side[4];   /* > 0: boundary particles on that side instead of n_boundary
                                    (per-side budgets, MG_IMC/MG_IMC1D.py:1000-1040) */
@@ -213,6 +215,14 @@ typedef struct imc_step_summary {
 
 /* Workspace bytes for a mesh and a bank capacity. */
 IMC_API size_t imc_workspace_bytes(const imc_mesh* mesh, int64_t bank_capacity);
+
+/* Workspace for a step with event-by-event tracking (imc_step_params.reserved bit 3): the
+ * history-based tracking kernel is replaced by the textbook event-based loop, one launch per
+ * event over the live histories with the survivors compacted between launches (the same
+ * physics and Philox draws per history; it synchronises the stream every few launches to read
+ * the live count, and does not take census_bins).  No reference counterpart: a second form of
+ * the tracking of IMC/IMC2D.py:938-1107, kept to compare the two on the hardware. */
+IMC_API size_t imc_workspace_bytes_event(const imc_mesh* mesh, int64_t bank_capacity);
 
 /* Equilibrium initial census at radiation temperature tr[c] into an empty bank.
  * (IMC/IMC1D.py:220-248, IMC/IMC2D.py:1110-1188, MG_IMC/MG_IMC2D.py:992-1235,

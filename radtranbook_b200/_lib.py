@@ -145,6 +145,7 @@ class ImcBatchLaunch(ctypes.Structure):
 
 SIGNATURES = {
     "imc_workspace_bytes": (c_size_t, [POINTER(ImcMesh), c_int64]),
+    "imc_workspace_bytes_event": (c_size_t, [POINTER(ImcMesh), c_int64]),
     "imc_init_census": (c_int, [POINTER(ImcMesh), c_void_p, c_int64, c_double, c_uint64, POINTER(ImcBank),
                                 c_void_p, c_size_t, POINTER(c_int64), c_void_p]),
     "imc_step_transport": (c_int, [POINTER(ImcMesh), POINTER(ImcMaterial), POINTER(ImcStepParams),

@@ -128,6 +128,12 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   const WsLayout L = imc_ws_layout(mesh, bank->capacity);
   if (workspace_bytes < L.total) return IMC_ERR_WORKSPACE;
   const int nc = mesh->nx * mesh->ny;
+  // reserved bit 3: event-by-event tracking, its scratch after the workspace layout
+  const bool event_mode = (par->reserved & 8) != 0;
+  if (event_mode) {
+    if (par->census_bins || adj) return IMC_ERR_INVALID_ARG;
+    if (workspace_bytes < L.total + imc_event_scratch_bytes(bank->capacity)) return IMC_ERR_WORKSPACE;
+  }
 
   // per-step fields of the summary (everything after n_census) start at zero
   IMC_CUDA(cudaMemsetAsync(reinterpret_cast<char*>(sum) + sizeof(int64_t), 0,
@@ -358,7 +364,14 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     if (pe.ok) { IMC_CUDA(cudaEventRecord(pe.e[2], s)); pe.recorded = true; }
     return IMC_OK;
   }
-  IMC_CUDA(imc_launch_track(ta, mesh->geometry, block, sm_count() * bps, smem_cells, smem_tally, s));
+  if (event_mode) {
+    bool cap_hit = false;
+    IMC_CUDA(imc_run_event_tracking(ta, mesh->geometry, static_cast<char*>(workspace) + L.total, bank->capacity,
+                                    n_upper, block, sm_count(), ta.max_events + 2, &cap_hit, s));
+    if (cap_hit) return IMC_ERR_EVENT_CAP;
+  } else {
+    IMC_CUDA(imc_launch_track(ta, mesh->geometry, block, sm_count() * bps, smem_cells, smem_tally, s));
+  }
   if (pe.ok) { IMC_CUDA(cudaEventRecord(pe.e[2], s)); pe.recorded = true; }
   IMC_CUDA(imc_launch_tally_finalize(ta, s));
   return IMC_OK;
@@ -498,6 +511,11 @@ extern "C" {
 size_t imc_workspace_bytes(const imc_mesh* mesh, int64_t bank_capacity) {
   if (!mesh) return 0;
   return imc_ws_layout(mesh, bank_capacity).total;
+}
+
+size_t imc_workspace_bytes_event(const imc_mesh* mesh, int64_t bank_capacity) {
+  if (!mesh) return 0;
+  return imc_ws_layout(mesh, bank_capacity).total + imc_event_scratch_bytes(bank_capacity);
 }
 
 int64_t imc_source_bound(const imc_mesh* mesh, const imc_step_params* par) {

@@ -57,6 +57,13 @@ struct TrackArgs {
 // smem_tally: per-block deposition / intensity tallies in shared memory (with smem_cells only)
 cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool smem_cells, bool smem_tally,
                              cudaStream_t s);
+// Event-by-event tracking (reserved bit 3 of imc_step_params): scratch bytes for a bank of
+// `capacity` entries, and the launch loop (synchronises the stream every 8 launches to read the
+// live count; *cap_hit when more than max_launches launches would be needed)
+size_t imc_event_scratch_bytes(long long capacity);
+cudaError_t imc_run_event_tracking(const TrackArgs& a, int geom, void* scratch, long long capacity,
+                                   long long n_upper, int block, int sms, long long max_launches, bool* cap_hit,
+                                   cudaStream_t s);
 // dep = fixed-point deposition / V, escaped (and escaped_group) from their fixed-point sums
 cudaError_t imc_launch_tally_finalize(const TrackArgs& a, cudaStream_t s);
 

@@ -202,7 +202,8 @@ class Engine:
         return torch.cuda.current_stream(self.device).cuda_stream
 
     def _ws(self, capacity: int) -> tuple[int, int]:
-        need = int(self.lib.imc_workspace_bytes(ctypes.byref(self.cmesh), int(capacity)))
+        size = self.lib.imc_workspace_bytes_event if self.launch.get("event_based") else self.lib.imc_workspace_bytes
+        need = int(size(ctypes.byref(self.cmesh), int(capacity)))
         if self.ws.numel() < need:
             self.ws = torch.empty(int(need * 1.25) + 4096, dtype=torch.uint8, device=self.device)
         return self.ws.data_ptr(), self.ws.numel()
@@ -332,6 +333,9 @@ class Engine:
         # (launch["smem_tally"] 1 / 0; absent or None: the library's default)
         st = self.launch.get("smem_tally")
         par.reserved = int(bool(self.launch.get("smem_cells", 0))) | (2 if st == 1 else 4 if st == 0 else 0)
+        # bit 3: the event-by-event form of the tracking (launch["event_based"] = 1)
+        if self.launch.get("event_based"):
+            par.reserved |= 8
         par.emission_fractions = _ptr(self.emission_fractions)
         for q, n in enumerate(n_boundary_side or ()):
             par.n_boundary_side[q] = int(n)
@@ -365,7 +369,7 @@ class Engine:
                                  rz_linear_source, t_emit_floor, n_boundary_side, method, cf_fastpath,
                                  step_dev, dt_dev)
         self._census_bins = 0
-        if self.fuse_census:
+        if self.fuse_census and not self.launch.get("event_based"):
             self._census_bins = _lib.CENSUS_BY_GROUP_CELL if self.ng > 1 else _lib.CENSUS_BY_CELL
         self._par.census_bins = self._census_bins
         bound = int(self.lib.imc_source_bound(ctypes.byref(self.cmesh), ctypes.byref(self._par)))
