@@ -361,6 +361,46 @@ def form_adjoint(repeats: int = 3, fd_cells: int = 64) -> dict:
             "fd_cells_within_2pct": int((rel <= 0.02).sum())}
 
 
+def form_event_based(steps: int = 10, warmup: int = 5, launch: dict | None = None) -> dict:
+    """The crooked-pipe step with the two forms of the tracking from the same state: the
+    persistent history-based kernel (each warp keeps 32 histories in registers and refills
+    idle lanes) and the event-by-event loop (one launch per event over the live histories,
+    survivors compacted between launches).  Both follow identical histories; CUDA events
+    around the tracking phase of each step."""
+    import torch
+
+    from radtranbook_b200 import imc2d, problems
+
+    p = problems.crooked_pipe()
+    out = {}
+    for name, ev in (("history_based", False), ("event_based", True)):
+        st = imc2d.init_simulation(p["Ntarget"], p["Tinit"], p["Tr_init"], p["edges1"], p["edges2"], p["eos_dev"],
+                                   p["inv_eos_dev"], geometry="rz", seed=0xE7E7)
+        if launch:
+            st._engine.launch.update(launch)
+        st._engine.launch["event_based"] = 1 if ev else 0
+        st, _, _, _ = _gpu_steps(p, st, warmup, True)
+        seg = 0
+        track = []
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(steps):
+            st, sg, _, info = _gpu_steps(p, st, 1, True)
+            seg += sg
+            track.append(info["profiling"]["phase_times_s"]["transport"] * 1e3)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out[name] = {"ms_per_step": ms / steps, "track_ms_per_step": float(np.mean(track)),
+                     "segments_per_step": seg / steps, "segments_per_s": seg / (ms * 1e-3),
+                     "tracking_segments_per_s": seg / (float(np.sum(track)) * 1e-3)}
+    out["event_over_history_tracking"] = (out["event_based"]["tracking_segments_per_s"]
+                                          / out["history_based"]["tracking_segments_per_s"])
+    out["workload"] = "crooked_pipe_rz_60x210"
+    return out
+
+
 def form_carter_forest(steps: int = 10, warmup: int = 2) -> dict:
     """The headline crooked-pipe step with Carter-Forest transport (IMC/IMC2D_CarterForest.py
     semantics): true absorption with delayed re-emission instead of the Fleck factor, same
@@ -737,7 +777,8 @@ def run_ours(args, rank: int, world: int):
     if world == 1 and not args.no_forms:
         forms = {"batched": form_batched(args.batch_steps, not args.no_tune), "adjoint": form_adjoint(),
                  "carter_forest": form_carter_forest(), "device_loop": form_device_loop(launch=dict(eng.launch)),
-                 "mg_crooked_pipe": form_mg_crooked_pipe(), "other_configs": form_other_configs()}
+                 "mg_crooked_pipe": form_mg_crooked_pipe(), "other_configs": form_other_configs(),
+                 "event_based": form_event_based(launch=dict(eng.launch))}
         forms["carter_forest"]["over_fleck_cummings"] = forms["carter_forest"]["segments_per_s"] / value
     if world == 1 and not args.no_fom:
         fom = {"gpu": fom_gpu(p, args.fom_steps, args.fom_seeds, dict(eng.launch))}
@@ -789,7 +830,7 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="skip the batched and adjoint forms")
     ap.add_argument("--only-form", default=None,
                     choices=["batched", "adjoint", "carter_forest", "device_loop", "mg_crooked_pipe",
-                             "mg_crooked_pipe_run", "other_configs"],
+                             "mg_crooked_pipe_run", "other_configs", "event_based"],
                     help="run one further form alone on GPU 0 and print its JSON (no headline line)")
     ap.add_argument("--batch-steps", type=int, default=50, help="steps of the batched form (the workload's 50)")
     ap.add_argument("--no-fom", action="store_true")
@@ -810,7 +851,7 @@ def main():
         fn = {"batched": lambda: form_batched(args.batch_steps, not args.no_tune), "adjoint": form_adjoint,
               "carter_forest": form_carter_forest, "device_loop": form_device_loop,
               "mg_crooked_pipe": form_mg_crooked_pipe, "mg_crooked_pipe_run": form_mg_crooked_pipe_run,
-              "other_configs": form_other_configs}[args.only_form]
+              "other_configs": form_other_configs, "event_based": form_event_based}[args.only_form]
         print(json.dumps({"form": args.only_form, **fn()}), flush=True)
         return
     if world > 1:
