@@ -567,7 +567,7 @@ def form_mg_crooked_pipe(steps: int = 12, warmup: int = 3) -> dict:
                             "max_relative_closure": res["max_relative_closure"]}}
 
 
-def form_other_configs(steps: int = 20, warmup: int = 5) -> dict:
+def form_other_configs(steps: int = 20, warmup: int = 5, tune: bool = True) -> dict:
     """The other two single-problem workloads at full size through the drop-in steps with device
     callables (CUDA-event timing of whole steps): the slab Marshak wave (20k + 20k particles
     per step, 100 cells) and the multigroup Marshak wave (1e6 particles per step, 200 cells x
@@ -607,9 +607,11 @@ def form_other_configs(steps: int = 20, warmup: int = 5) -> dict:
         return sm, seg
 
     peak, peak_kind = measured_peaks()
-    for tag, fn, s0, bseg, kern in (("slab_marshak_100_cells", slab, st, B_SEG_1D, "k_track<slab>"),
-                                    ("mg_marshak_200x10", mg, sm, B_SEG_2D_MG, "k_track<XY, multigroup>")):
+    for tag, fn, s0, bseg, kern, mod in (("slab_marshak_100_cells", slab, st, B_SEG_1D, "k_track<slab>", imc1d),
+                                         ("mg_marshak_200x10", mg, sm, B_SEG_2D_MG, "k_track<XY, multigroup>",
+                                          mg_imc2d)):
         s0, _ = fn(s0, warmup)
+        tuned = mod.tune(s0) if tune else None  # the launch shape for this problem (autotuner)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         track.clear()
@@ -623,6 +625,9 @@ def form_other_configs(steps: int = 20, warmup: int = 5) -> dict:
         out[tag] = {"steps": steps, "after_warmup_steps": warmup, "ms_per_step": ms / steps,
                     "segments_per_step": seg / steps, "segments_per_s": seg / (ms * 1e-3),
                     "track_ms_per_launch": t_launch * 1e3,
+                    "launch": dict(s0._engine.launch),
+                    "autotune": None if tuned is None else {"best_ms": tuned["best_ms"], "worst_ms": tuned["worst_ms"],
+                                                            "candidates": len(tuned["trials"])},
                     "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                                  "frac": achieved / peak, "kernel": kern, "peak_source": peak_kind,
                                  "bytes_per_segment_algorithmic": bseg}}
@@ -851,7 +856,8 @@ def main():
         fn = {"batched": lambda: form_batched(args.batch_steps, not args.no_tune), "adjoint": form_adjoint,
               "carter_forest": form_carter_forest, "device_loop": form_device_loop,
               "mg_crooked_pipe": form_mg_crooked_pipe, "mg_crooked_pipe_run": form_mg_crooked_pipe_run,
-              "other_configs": form_other_configs, "event_based": form_event_based}[args.only_form]
+              "other_configs": lambda: form_other_configs(tune=not args.no_tune),
+              "event_based": form_event_based}[args.only_form]
         print(json.dumps({"form": args.only_form, **fn()}), flush=True)
         return
     if world > 1:

@@ -20,7 +20,7 @@ from .engine import Bank, Engine
 
 DEFAULT_GRID = {
     "block_size": (128, 256),
-    "blocks_per_sm": (4, 8),
+    "blocks_per_sm": (2, 4, 8),  # 2: small banks, where fewer resident lanes keep warps fuller
     "chunk": (512, 1024, 2048, 4096, 8192),
     "smem_cells": (0, 1),
 }

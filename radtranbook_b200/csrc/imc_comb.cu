@@ -20,7 +20,9 @@ using namespace imcdev;
 
 namespace {
 
-constexpr int CB = 1024;  // comb block
+constexpr int TILE = 4096;      // entries per count / scatter block (one block total each for the scan)
+constexpr int CNT_T = 256;      // count threads per block (TILE / CNT_T entries each)
+constexpr int CNT_SLOTS = 512;  // count: shared-memory bins per block
 
 __device__ __forceinline__ int bin_of(const CombArgs& a, long long k) {
   return a.per_group ? a.cell[k] + a.nc * a.group[k] : a.cell[k];
@@ -78,41 +80,49 @@ __global__ void __launch_bounds__(256) k_comb_ecen(CombArgs a) {
   bins_flush(t, a.ecen);
 }
 
-__global__ void __launch_bounds__(CB) k_comb_count(CombArgs a) {
+// Each block combs a tile of TILE consecutive entries, CNT_T threads with TILE / CNT_T entries
+// each (coalesced across the block): copies per entry, copies per bin (per warp, then in the
+// block's table, flushed once) and the tile's total for the scan.
+__global__ void __launch_bounds__(CNT_T) k_comb_count(CombArgs a) {
   const uint32_t step = a.step_dev ? *a.step_dev : a.step;  // graph replay
-  __shared__ long long sh[CB / 32];
-  __shared__ BlockCounts<CB> t;
+  __shared__ unsigned sh[CNT_T / 32];
+  __shared__ BlockCounts<CNT_SLOTS> t;
   counts_init(t);
   __syncthreads();
-  const long long k = (long long)blockIdx.x * CB + threadIdx.x;
+  const long long tile0 = (long long)blockIdx.x * TILE;
   const long long n_in = min((long long)*a.d_n_in, (long long)a.n_bound);  // the grid covers n_bound entries
   const bool compact = *a.mode != 0;
-  int n = 0, b = 0;
-  if (k < n_in) {
-    const float wf = a.w[k];
-    const int bk = bin_of(a, k);  // loaded with the weight (k < n_in: in bounds)
-    if (wf > 0.f && bin_ok(a, bk)) {
-      b = bk;
-      const double ew = a.ew[b];
-      if (compact) {
-        n = 1;
-      } else if (ew > 0.0) {
-        const U4 r = draw(a.seed, (uint32_t)k, 0, step, TAG_COMB);
-        n = (int)floor((double)wf / ew + u01d(r.x));
+  unsigned tsum = 0;
+  for (int i = 0; i < TILE / CNT_T; ++i) {  // uniform trip count: warps stay converged
+    const long long k = tile0 + (long long)i * CNT_T + threadIdx.x;
+    int n = 0, b = 0;
+    if (k < n_in) {
+      const float wf = a.w[k];
+      const int bk = bin_of(a, k);  // loaded with the weight (k < n_in: in bounds)
+      if (wf > 0.f && bin_ok(a, bk)) {
+        b = bk;
+        const double ew = a.ew[b];
+        if (compact) {
+          n = 1;
+        } else if (ew > 0.0) {
+          const U4 r = draw(a.seed, (uint32_t)k, 0, step, TAG_COMB);
+          n = (int)floor((double)wf / ew + u01d(r.x));
+        }
       }
+      a.cnt[k] = n;
     }
-    a.cnt[k] = n;
+    // copies per bin: aggregated per warp, then per block (the bank is largely grouped by cell)
+    warp_counts_add(n > 0, b, (unsigned)n, t, a.ncopy);
+    tsum += (unsigned)n;
   }
-  // copies per bin: aggregated per warp, then per block (the bank is largely grouped by cell)
-  warp_counts_add(n > 0, b, (unsigned)n, t, a.ncopy);
-  const unsigned ws = __reduce_add_sync(FULL, (unsigned)n);
+  const unsigned ws = __reduce_add_sync(FULL, tsum);
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = ws;
   __syncthreads();
   counts_flush(t, a.ncopy);
-  if (threadIdx.x < 32) {
-    unsigned long long v = sh[threadIdx.x];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
-    if (threadIdx.x == 0) a.blk[blockIdx.x] = (long long)v;
+  if (threadIdx.x == 0) {
+    unsigned long long v = 0;
+    for (int q = 0; q < CNT_T / 32; ++q) v += sh[q];
+    a.blk[blockIdx.x] = (long long)v;
   }
 }
 
@@ -144,19 +154,27 @@ __global__ void __launch_bounds__(1024) k_comb_scan(long long* blk, long long nb
   }
 }
 
-// One thread per output copy: the tile's copy counts are scanned in shared memory, each
-// thread finds the entry of its copy by a binary search there and gathers the entry's fields
-// (cached: a tile's entries are few), so the output stores are contiguous across the warp.
-__global__ void __launch_bounds__(CB) k_comb_scatter(CombArgs a) {
-  __shared__ int incl[CB];
-  __shared__ int sh[CB / 32];
-  const long long tile0 = (long long)blockIdx.x * CB;
-  const long long k = tile0 + threadIdx.x;
+// One thread per output copy: the tile's copy counts are scanned in shared memory (each
+// thread owns 4 consecutive entries), each thread finds the entry of its copy by a binary
+// search there and gathers the entry's fields (cached: a tile's entries are few), so the
+// output stores are contiguous across the warp.
+__global__ void __launch_bounds__(1024) k_comb_scatter(CombArgs a) {
+  __shared__ int incl[TILE];
+  __shared__ int sh[32];
+  const long long tile0 = (long long)blockIdx.x * TILE;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const long long n_in = min((long long)*a.d_n_in, (long long)a.n_bound);
-  const int n = (k < n_in) ? a.cnt[k] : 0;
-  // block-inclusive scan of the copy counts
-  int x = n;
+  const long long k0 = tile0 + 4 * threadIdx.x;
+  int c[4] = {0, 0, 0, 0};
+  if (k0 + 3 < n_in) {
+    const int4 v = *reinterpret_cast<const int4*>(a.cnt + k0);  // 16-byte aligned: k0 % 4 == 0
+    c[0] = v.x; c[1] = v.y; c[2] = v.z; c[3] = v.w;
+  } else {
+    for (int j = 0; j < 4; ++j) if (k0 + j < n_in) c[j] = a.cnt[k0 + j];
+  }
+  const int s4 = c[0] + c[1] + c[2] + c[3];
+  // block-exclusive scan of the threads' sums, then the entries' inclusive sums
+  int x = s4;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) { const int y = __shfl_up_sync(FULL, x, o); if (lane >= o) x += y; }
   if (lane == 31) sh[wid] = x;
@@ -168,15 +186,17 @@ __global__ void __launch_bounds__(CB) k_comb_scatter(CombArgs a) {
     sh[lane] = v;
   }
   __syncthreads();
-  incl[threadIdx.x] = x + (wid ? sh[wid - 1] : 0);
+  int run = x - s4 + (wid ? sh[wid - 1] : 0);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) { run += c[j]; incl[4 * threadIdx.x + j] = run; }
   __syncthreads();
-  const int total = incl[CB - 1];
+  const int total = incl[TILE - 1];
   const long long out0 = a.blk[blockIdx.x];
   const bool compact = *a.mode != 0;
-  for (int o = threadIdx.x; o < total; o += CB) {
+  for (int o = threadIdx.x; o < total; o += blockDim.x) {
     const long long dst = out0 + o;
     if (dst >= a.out_capacity) break;  // overflow: flagged by the scan, caller regrows
-    int lo = 0, hi = CB - 1;  // the entry j with incl[j-1] <= o < incl[j]
+    int lo = 0, hi = TILE - 1;  // the entry j with incl[j-1] <= o < incl[j]
     while (lo < hi) { const int mid = (lo + hi) >> 1; if (incl[mid] > o) hi = mid; else lo = mid + 1; }
     const long long src = tile0 + lo;
     const int b = bin_of(a, src);
@@ -211,10 +231,10 @@ cudaError_t imc_launch_comb_ecen(const CombArgs& a, cudaStream_t s) {
 }
 
 cudaError_t imc_launch_comb_count(const CombArgs& a, cudaStream_t s) {
-  const long long nblk = (a.n_bound + CB - 1) / CB;
+  const long long nblk = (a.n_bound + TILE - 1) / TILE;
   if (nblk > 0) {
     ++g_imc_launches;
-    k_comb_count<<<(unsigned)nblk, CB, 0, s>>>(a);
+    k_comb_count<<<(unsigned)nblk, CNT_T, 0, s>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
@@ -224,10 +244,10 @@ cudaError_t imc_launch_comb_count(const CombArgs& a, cudaStream_t s) {
 }
 
 cudaError_t imc_launch_comb_scatter(const CombArgs& a, cudaStream_t s) {
-  const long long nblk = (a.n_bound + CB - 1) / CB;
+  const long long nblk = (a.n_bound + TILE - 1) / TILE;
   if (nblk > 0) {
     ++g_imc_launches;
-    k_comb_scatter<<<(unsigned)nblk, CB, 0, s>>>(a);
+    k_comb_scatter<<<(unsigned)nblk, 1024, 0, s>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
