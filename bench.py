@@ -517,7 +517,8 @@ def form_mg_crooked_pipe(steps: int = 12, warmup: int = 3) -> dict:
             st, info = mg_imc2d.step(st, p["Ntarget"], p["Nboundary"], 0, Nmax, p["T_boundary"], state["dt"], e1,
                                      e2, ge, p["sigma_dev"], p["inv_eos_dev"], p["cv_dev"], p["source"],
                                      reflect=p["reflect"], geometry="rz",
-                                     boundary_source_func=p["boundary_source_func"], T_emit_floor=p["T_emit_floor"])
+                                     boundary_source_func=p["boundary_source_func"], T_emit_floor=p["T_emit_floor"],
+                                     Nmax_growth=p["Nmax_growth"], Nmax_final=p["Nmax_final"])
             te = info["profiling"]["transport_events"]
             seg += te["total"]
             hist += te["n_particles_transported"]

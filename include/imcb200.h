@@ -58,7 +58,7 @@ typedef enum imc_status {
   IMC_ERR_TIMEOUT = 5,         /* a bounded device wait gave up */
   IMC_ERR_CUDA = 6,            /* CUDA runtime error (see imc_last_cuda_error) */
   IMC_ERR_INVALID_ARG = 7,
-  IMC_ERR_WORKSPACE = 8,       /* workspace too small */
+  IMC_ERR_WORKSPACE = 8,       /* workspace too small, or not 256-byte aligned */
   IMC_ERR_BOUNDS = 9           /* bounds-checked build only: an index or weight out of range */
 } imc_status;
 
@@ -244,21 +244,30 @@ IMC_API imc_status imc_step_transport(const imc_mesh* mesh, const imc_material* 
 IMC_API imc_status imc_material_update(const imc_mesh* mesh, const imc_tallies* tal, double* e,
                                double* tr, void* stream);
 
-/* A gray material whose laws the device evaluates itself: linear EOS e = cv_eos * T, heat
- * capacity cv, and opacity sigma(T) = sigma_A * T^-sigma_n clamped to [sigma_lo, sigma_hi]
- * (a bound <= 0 is no bound; sigma_n = 0 is a constant).  Each *_array, when set, is a
- * DEVICE array [c] that replaces its scalar (per-cell, temperature-independent values). */
+/* A material whose laws the device evaluates itself: linear EOS e = cv_eos * T, heat
+ * capacity cv, and opacity
+ *   sigma_g(T)[c] = sigma_A * max(T, sigma_T_floor)^-sigma_n * sigma_scale[c] * sigma_group[g]
+ * clamped to [sigma_lo, sigma_hi] (multiplied in that order; a bound <= 0 is no bound,
+ * sigma_T_floor <= 0 no floor, sigma_n = 0 a constant, a null sigma_scale / sigma_group a
+ * factor of 1).  cv_eos_array, cv_array and sigma_scale, when set, are DEVICE arrays [c];
+ * sigma_group is a DEVICE array [g] (multigroup meshes need it, or sigma_array).
+ * sigma_array, when set, replaces the whole opacity law by temperature-independent values,
+ * a DEVICE array [g][c]. */
 typedef struct imc_material_law {
   double cv_eos;          const double* cv_eos_array;
   double cv;              const double* cv_array;
   double sigma_A, sigma_n, sigma_lo, sigma_hi;
   const double* sigma_array;
+  const double* sigma_scale;
+  double sigma_T_floor;
+  const double* sigma_group;
 } imc_material_law;
 
-/* imc_material_update and the material temperature of the next step in one kernel (gray
- * meshes): e and tr as imc_material_update, then T = e / cv_eos (the inverse EOS,
- * IMC/IMC1D.py:1024 inv_eos), and the next step's sigma(T) and cv(T) of the law into
- * sigma_next / cv_next (IMC/IMC1D.py:932-935 sigma_a_func(T), cv(T)), which a step's
+/* imc_material_update and the material temperature of the next step in one kernel: e and
+ * tr as imc_material_update, then T = e / cv_eos (the inverse EOS, IMC/IMC1D.py:1024
+ * inv_eos; MG_IMC/MG_IMC2D.py:2037), and the next step's opacity and cv(T) of the law into
+ * sigma_next ([g][c]) and cv_next ([c]) (IMC/IMC1D.py:932-935 sigma_a_func(T), cv(T);
+ * MG_IMC/MG_IMC2D.py:1703-1710 one sigma_a_funcs[g](T) per group), which a step's
  * imc_material then takes as they are. */
 IMC_API imc_status imc_material_update_law(const imc_mesh* mesh, const imc_tallies* tal,
                                            const imc_material_law* law, double* e, double* tr,
@@ -274,7 +283,10 @@ IMC_API imc_status imc_material_update_law(const imc_mesh* mesh, const imc_talli
  * alive, else only drops dead entries (MG_IMC/MG_IMC1D.py:1194-1200).
  * disc[bin] = energy before - after. */
 enum { IMC_COMB_PER_GROUP = 1, IMC_COMB_CONSERVE_RADIATION = 2,
-       IMC_COMB_CENSUS_READY = 4 /* async forms: the census sums come from the tracking call */ };
+       IMC_COMB_CENSUS_READY = 4, /* async forms: the census sums come from the tracking call */
+       IMC_COMB_WRITE_AFTER = 8   /* disc holds 2 x bins: [bins, 2 bins) the energy after the
+                                     comb per bin (sum of its copies' FP32 weights in FP64;
+                                     divided by V: MG_IMC/MG_IMC2D.py:2017-2025) */ };
 enum { IMC_CENSUS_BY_CELL = 1, IMC_CENSUS_BY_GROUP_CELL = 2 };
 IMC_API imc_status imc_comb(const imc_mesh* mesh, const imc_bank* in, imc_bank* out, int64_t n_max,
                     uint64_t seed, uint32_t step, int32_t per_group, double* disc,

@@ -54,22 +54,25 @@ class GrayState:
         return grid.t().contiguous().view(-1)
 
     def host_copies(self):
-        """(device, pinned host) pairs for the end-of-step copy of e, T and Tr."""
-        hb = self.__dict__.get("_hbuf")
-        if hb is None:
-            hb = {k: torch.empty(self._engine.nc, dtype=torch.float64, pin_memory=True) for k in ("e", "T", "Tr")}
-            object.__setattr__(self, "_hbuf", hb)
-        return [(self._e, hb["e"]), (self._T, hb["T"]), (self._Tr, hb["Tr"])]
+        """(device, pinned host) pair for the end-of-step copy of e, T and Tr: the three fields
+        stacked on the device in the reference's layout ((nx, ny) in 2-D), one copy into a
+        fresh buffer of torch's caching pinned allocator, which the host arrays then view
+        (no host-side copy; a buffer returns to the cache once no array views it)."""
+        src = torch.stack([self.grid(self._e), self.grid(self._T), self.grid(self._Tr)]).reshape(-1)
+        pin = torch.empty(src.numel(), dtype=torch.float64, pin_memory=True)
+        object.__setattr__(self, "_hpin", pin)
+        return [(src, pin)]
 
     def take_host_copies(self) -> None:
-        """Host mirrors from the pinned buffers filled by the last fetch (no device access)."""
-        hb = self._hbuf
+        """Host mirrors from the pinned buffer filled by the last fetch (no device access)."""
+        nc = self._engine.nc
+        a = self._hpin.numpy()
+        shape = (nc,) if self._dim == 1 else tuple(self._shape)
         h = self._host
-        g = (lambda a: a) if self._dim == 1 else (lambda a: a.reshape(self._shape[1], self._shape[0]).T)
-        h["internal_energy"] = np.array(g(hb["e"].numpy()))
-        h["temperature"] = np.array(g(hb["T"].numpy()))
-        h["radiation_temperature"] = np.array(g(hb["Tr"].numpy()))
-        _lib.TRANSFER["d2h"] += 3 * 8 * self._engine.nc
+        h["internal_energy"] = a[:nc].reshape(shape)
+        h["temperature"] = a[nc:2 * nc].reshape(shape)
+        h["radiation_temperature"] = a[2 * nc:].reshape(shape)
+        _lib.TRANSFER["d2h"] += 3 * 8 * nc
 
     def refresh_host(self) -> None:
         h = self._host
@@ -386,14 +389,23 @@ def _law(state, sigma_a_func, cv, inv_eos):
 
 
 def tune(state: GrayState, grid: dict | None = None, repeats: int = 2) -> dict:
-    """Autotune the tracking launch shape on the state's census, replaying its last step's
-    transport (call after at least one step).  Installs the best shape on the engine."""
+    """Autotune the tracking launch shape on the state's census: the last step's transport
+    (sources, counts, step index) at the state's current temperature.  With a device-evaluated
+    material law the opacity and heat capacity are the law's at that temperature, i.e. the
+    next step's own inputs.  With other callables they are the last step's, evaluated at its
+    start temperature, which the material update has since replaced: where the opacity
+    depends on T, the replay's Fleck factor then differs from any real step's (a cell that
+    heated keeps its cold opacity next to its new T^3), and so does its number of events.
+    Call after at least one step.  Installs the best shape on the engine."""
     from .autotune import tune_tracking
 
     eng = state._engine
     if eng._last_transport is None:
         raise RuntimeError("tune() needs one completed step to replay")
     args, kwargs = eng._last_transport
+    nxt = state.__dict__.get("_law_next")
+    if nxt is not None:  # (T, sigma, cv) consistent: the next step's material inputs
+        args = (state._T, nxt[1].reshape(-1), nxt[2]) + tuple(args[3:])
     return tune_tracking(eng, args, kwargs, grid=grid, repeats=repeats)
 
 

@@ -31,7 +31,7 @@ STATUS = {
 }
 OK, BANK_OVERFLOW = 0, 1
 
-COMB_PER_GROUP, COMB_CONSERVE_RADIATION, COMB_CENSUS_READY = 1, 2, 4  # imc_comb flags
+COMB_PER_GROUP, COMB_CONSERVE_RADIATION, COMB_CENSUS_READY, COMB_WRITE_AFTER = 1, 2, 4, 8  # imc_comb flags
 CENSUS_BY_CELL, CENSUS_BY_GROUP_CELL = 1, 2  # imc_step_params.census_bins
 METHOD_FLECK_CUMMINGS, METHOD_CARTER_FOREST = 0, 1  # imc_step_params.method
 
@@ -77,7 +77,8 @@ class ImcStepParams(ctypes.Structure):
 class ImcMaterialLaw(ctypes.Structure):
     _fields_ = [("cv_eos", c_double), ("cv_eos_array", c_void_p), ("cv", c_double), ("cv_array", c_void_p),
                 ("sigma_A", c_double), ("sigma_n", c_double), ("sigma_lo", c_double), ("sigma_hi", c_double),
-                ("sigma_array", c_void_p)]
+                ("sigma_array", c_void_p), ("sigma_scale", c_void_p), ("sigma_T_floor", c_double),
+                ("sigma_group", c_void_p)]
 
 
 class ImcTallies(ctypes.Structure):

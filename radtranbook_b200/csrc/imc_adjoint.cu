@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(256) k_adjoint(AdjointArgs A) {
       if (ev >= (uint32_t)a.max_events) {
         finished = true;  // cap: the history stops where it is, in both passes
       } else {
-        const U4 r = draw(a.seed, a.id_base + pid, ev, a.step, TAG_TRANSPORT);
+        const U4 r = draw_rk(a.rk, a.id_base + pid, ev, a.step, TAG_TRANSPORT);
         ++ev;
         float d, sb, Lc, xn = x, yn = y, un = u, vn = v;
         int evt, cross = X_NONE;

@@ -261,26 +261,33 @@ __global__ void k_material(MatArgs a) {
   a.tr[c] = x > 0.0 ? sqrt(sqrt(x)) : 0.0;
 }
 
-// k_material, then T = e / cv_eos and the law's sigma(T), cv for the next step (gray)
+// k_material, then T = e / cv_eos and the law's opacity of every group and cv at that T for
+// the next step.  e and tr are k_material's sums (same order, so the same bits).
 __global__ void k_material_law(MatArgs a, imc_material_law law, double* T, double* sigma_next, double* cv_next) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= a.nc) return;
-  const double e = a.e[c] + a.dep[c] - a.emitted[c] / a.vol[c];
+  double dep = 0.0, si = 0.0;
+  for (int g = 0; g < a.ng; ++g) { dep += a.dep[(size_t)g * a.nc + c]; si += a.si[(size_t)g * a.nc + c]; }
+  const double e = a.e[c] + dep - a.emitted[c] / a.vol[c];
   a.e[c] = e;
-  const double x = a.si[c] / A_RAD / C_LIGHT;
+  const double x = si / A_RAD / C_LIGHT;
   a.tr[c] = x > 0.0 ? sqrt(sqrt(x)) : 0.0;
   const double t = e / (law.cv_eos_array ? law.cv_eos_array[c] : law.cv_eos);
   T[c] = t;
-  double sg;
+  cv_next[c] = law.cv_array ? law.cv_array[c] : law.cv;
   if (law.sigma_array) {
-    sg = law.sigma_array[c];
-  } else {
-    sg = law.sigma_n == 0.0 ? law.sigma_A : law.sigma_A * pow(t, -law.sigma_n);
+    for (int g = 0; g < a.ng; ++g) sigma_next[(size_t)g * a.nc + c] = law.sigma_array[(size_t)g * a.nc + c];
+    return;
+  }
+  const double tp = law.sigma_T_floor > 0.0 ? fmax(t, law.sigma_T_floor) : t;
+  double base = law.sigma_n == 0.0 ? law.sigma_A : law.sigma_A * pow(tp, -law.sigma_n);
+  if (law.sigma_scale) base = base * law.sigma_scale[c];
+  for (int g = 0; g < a.ng; ++g) {
+    double sg = law.sigma_group ? base * law.sigma_group[g] : base;
     if (law.sigma_lo > 0.0) sg = fmax(sg, law.sigma_lo);
     if (law.sigma_hi > 0.0) sg = fmin(sg, law.sigma_hi);
+    sigma_next[(size_t)g * a.nc + c] = sg;
   }
-  sigma_next[c] = sg;
-  cv_next[c] = law.cv_array ? law.cv_array[c] : law.cv;
 }
 
 // Single block: the canonical total of the census energy and the comb mode.
@@ -289,7 +296,7 @@ __global__ void __launch_bounds__(NT) k_comb_plan(CombPlanArgs a) {
   const double E = block_canon_sum(a.ecen, a.nb, red);
   // MG_IMC/MG_IMC1D.py:1194-1200: Nmax = 0 never combs; Nmax < 0 combs once |Nmax| entries live
   const bool compact = a.force_compact || (a.threshold > 0 && (long long)*a.n_live < a.threshold);
-  if (threadIdx.x == 0) { *a.mode = compact ? 1 : 0; a.sum->comb_before = E; }
+  if (threadIdx.x == 0) { *a.mode = compact ? 1 : 0; a.sum->comb_before = E; a.sum->comb_after = 0.0; }
 }
 
 // Wide: the comb weight of every bin, ecen / max(1, rint(Nmax ecen / E)).
@@ -302,6 +309,17 @@ __global__ void k_comb_weights(CombPlanArgs a) {
   double ew = 0.0;
   if (E > 0.0 && ec > 0.0) ew = ec / fmax(1.0, rint((double)n_max * ec / E));
   a.ew[b] = ew;
+  a.ncopy[b] = 0ull;
+}
+
+// Zero the regions of a ZeroList (one launch for a step's accumulators).
+__global__ void k_zero(ZeroList z) {
+  const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x, stride = (size_t)gridDim.x * blockDim.x;
+  for (int r = 0; r < z.n; ++r) {
+    unsigned long long* q = static_cast<unsigned long long*>(z.p[r]);
+    const size_t n8 = z.bytes[r] / 8;
+    for (size_t i = t0; i < n8; i += stride) q[i] = 0ull;
+  }
 }
 
 __global__ void __launch_bounds__(NT) k_canon_eV(const double* e, const double* vol, int nc, double* out) {
@@ -337,6 +355,15 @@ cudaError_t imc_launch_material_law(const MatArgs& a, const imc_material_law& la
                                     double* cv_next, cudaStream_t s) {
   ++g_imc_launches;
   k_material_law<<<(a.nc + 255) / 256, 256, 0, s>>>(a, law, T, sigma_next, cv_next);
+  return cudaGetLastError();
+}
+cudaError_t imc_launch_zero(const ZeroList& z, cudaStream_t s) {
+  unsigned long long most = 0;
+  for (int r = 0; r < z.n; ++r) most = std::max(most, z.bytes[r] / 8);
+  if (most == 0) return cudaSuccess;
+  ++g_imc_launches;
+  const unsigned blocks = (unsigned)std::min<unsigned long long>(1184ull, (most + 255) / 256);
+  k_zero<<<blocks, 256, 0, s>>>(z);
   return cudaGetLastError();
 }
 cudaError_t imc_launch_comb_plan(const CombPlanArgs& a, cudaStream_t s) {
@@ -426,30 +453,64 @@ __device__ void block_canon_prefix(const double* x, int n, double* out, double* 
   __syncthreads();
 }
 
-// Per-cell part of the 2-D multigroup plan, one thread per cell over a wide grid (each cell's
-// numbers depend on that cell alone, so the result is the single-block loop's).
-__global__ void k_plan_mg_cells(PlanMgArgs a) {
+// Mixture-of-Gammas CDF of the Planck group sampler, weights 1/n^4 over n = 1..200
+// (MG_IMC/MG_IMC2D.py:105-107), summed in order n = 1..200.  A constant: the compiler
+// evaluates it once (IEEE double, the order of the loop), the plan kernels copy it into the
+// step's workspace.
+struct MixCdf { double v[200]; };
+constexpr MixCdf mix_cdf_table() {
+  MixCdf m{};
+  double tot = 0.0, run = 0.0;
+  for (int n = 1; n <= 200; ++n) { const double d = (double)n; tot += 1.0 / (d * d * d * d); }
+  for (int n = 1; n <= 200; ++n) { const double d = (double)n; run += 1.0 / (d * d * d * d); m.v[n - 1] = run / tot; }
+  return m;
+}
+__device__ const MixCdf g_mix_cdf = mix_cdf_table();
+
+// The Planck edge integrals of the block's cells [c0, c0 + ncb) at the G + 1 group edges,
+// one (cell, edge) pair per thread: x and its series or tail value at [(c - c0)(G + 1) + k].
+// The tail costs up to 2 + 40/x exponentials, so this is most of a plan's arithmetic; spread
+// over all the block's threads it is no longer one long chain per cell.
+__device__ void block_planck_edges(const double* T, const double* gedges, int G, int c0, int ncb, double* sx,
+                                   double* ss) {
+  const int E = G + 1;
+  for (int i = threadIdx.x; i < ncb * E; i += blockDim.x) {
+    const int cl = i / E, k = i - cl * E;
+    const double Tc = T[c0 + cl];
+    const PlanckEdge pe = planck_edge(Tc > 0.0 ? gedges[k] / Tc : 0.0);
+    sx[i] = pe.x;
+    ss[i] = pe.s;
+  }
+  __syncthreads();
+}
+
+// Per-cell part of the 2-D multigroup plan.  A block takes cb consecutive cells: its threads
+// evaluate the cells' Planck edges into shared memory, then one thread per cell forms the
+// fractions, Planck-mean opacity, Fleck factor and emission by group (each cell's numbers
+// depend on that cell alone, so the result is the single-block loop's).
+__global__ void __launch_bounds__(256) k_plan_mg_cells(PlanMgArgs a, int cb) {
+  extern __shared__ double plan_sh[];
   const double dt = a.dt_dev ? *a.dt_dev : a.dt;  // device-resident step length (graph replay)
   const int nc = a.nc, G = a.ng;
   const int t0 = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
   for (int q = t0; q <= a.nx; q += stride) a.e1f[q] = (float)a.e1[q];
   for (int q = t0; q <= a.ny; q += stride) a.e2f[q] = (float)a.e2[q];
-  if (t0 == 0) {
-    // mixture-of-Gammas CDF over n = 1..200 with weights 1/n^4 (MG_IMC/MG_IMC2D.py:105-107)
-    double tot = 0.0;
-    for (int n = 1; n <= 200; ++n) { const double d = (double)n; tot += 1.0 / (d * d * d * d); }
-    double run = 0.0;
-    for (int n = 1; n <= 200; ++n) { const double d = (double)n; run += 1.0 / (d * d * d * d); a.mixcdf[n - 1] = run / tot; }
-  }
+  for (int q = t0; q < 200; q += stride) a.mixcdf[q] = g_mix_cdf.v[q];
+  const int c0 = blockIdx.x * cb, ncb = min(cb, nc - c0);
+  double* sx = plan_sh;
+  double* sv = plan_sh + (size_t)cb * (G + 1);
+  block_planck_edges(a.T, a.gedges, G, c0, ncb, sx, sv);
   // ---- per cell: Planck fractions, Planck-mean opacity, Fleck, emission by group ----
-  for (int c = t0; c < nc; c += stride) {
+  if ((int)threadIdx.x < ncb) {
+    const int c = c0 + threadIdx.x;
+    const int eb = threadIdx.x * (G + 1);
     const double T = a.T[c];
     if (!isfinite(T) || !(a.cv[c] > 0.0)) atomicOr(&a.sum->flags, (int)IMC_FLAG_NONFINITE);
     double* gc = a.Egc + (size_t)c * G;  // scratch: fractions, then cumulative emission
     double tot = 0.0;
-    PlanckEdge lo = planck_edge(T > 0.0 ? a.gedges[0] / T : 0.0);
+    PlanckEdge lo{sx[eb], sv[eb]};
     for (int g = 0; g < G; ++g) {
-      const PlanckEdge hi = planck_edge(T > 0.0 ? a.gedges[g + 1] / T : 0.0);
+      const PlanckEdge hi{sx[eb + g + 1], sv[eb + g + 1]};
       const double f = (T > 0.0) ? planck_frac(lo, hi) : 0.0;
       lo = hi;
       gc[g] = f > 0.0 ? f : 0.0;
@@ -569,26 +630,28 @@ __global__ void __launch_bounds__(NT) k_plan_mg(PlanMgArgs a) {
 // source: round, no minimum), inner / outer sphere boundary faces.
 // Per-shell part of the sphere plan, one thread per shell over a wide grid (each shell's
 // numbers depend on that shell alone, so the result is the single-block loop's).
-__global__ void k_plan_mg1d_cells(PlanMgArgs a) {
+__global__ void __launch_bounds__(256) k_plan_mg1d_cells(PlanMgArgs a, int cb) {
+  extern __shared__ double plan_sh[];
   const double dt = a.dt_dev ? *a.dt_dev : a.dt;  // device-resident step length (graph replay)
   const int nc = a.nc, G = a.ng;
   const int t0 = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
   for (int q = t0; q <= a.nx; q += stride) a.e1f[q] = (float)a.e1[q];
   for (int q = t0; q <= a.ny; q += stride) a.e2f[q] = (float)a.e2[q];
-  if (t0 == 0) {
-    double tot = 0.0;
-    for (int n = 1; n <= 200; ++n) { const double d = (double)n; tot += 1.0 / (d * d * d * d); }
-    double run = 0.0;
-    for (int n = 1; n <= 200; ++n) { const double d = (double)n; run += 1.0 / (d * d * d * d); a.mixcdf[n - 1] = run / tot; }
-  }
-  for (int c = t0; c < nc; c += stride) {
+  for (int q = t0; q < 200; q += stride) a.mixcdf[q] = g_mix_cdf.v[q];
+  const int c0 = blockIdx.x * cb, ncb = min(cb, nc - c0);
+  double* sx = plan_sh;
+  double* sv = plan_sh + (size_t)cb * (G + 1);
+  block_planck_edges(a.T, a.gedges, G, c0, ncb, sx, sv);
+  if ((int)threadIdx.x < ncb) {
+    const int c = c0 + threadIdx.x;
+    const int eb = threadIdx.x * (G + 1);
     const double T = a.T[c];
     if (!isfinite(T) || !(a.cv[c] > 0.0)) atomicOr(&a.sum->flags, (int)IMC_FLAG_NONFINITE);
     double* b = a.Egc + (size_t)c * G;  // scratch: Planck fractions of this cell
     double tot = 0.0;
-    PlanckEdge lo = planck_edge(T > 0.0 ? a.gedges[0] / T : 0.0);
+    PlanckEdge lo{sx[eb], sv[eb]};
     for (int g = 0; g < G; ++g) {
-      const PlanckEdge hi = planck_edge(T > 0.0 ? a.gedges[g + 1] / T : 0.0);
+      const PlanckEdge hi{sx[eb + g + 1], sv[eb + g + 1]};
       const double f = (T > 0.0) ? planck_frac(lo, hi) : 0.0;
       lo = hi;
       b[g] = f > 0.0 ? f : 0.0;
@@ -706,12 +769,7 @@ __global__ void __launch_bounds__(NT) k_plan_mg1d(PlanMgArgs a) {
 __global__ void __launch_bounds__(NT) k_ic_plan_mg(IcMgArgs a) {
   __shared__ double sh[NT];
   const int t = threadIdx.x;
-  if (t == 0) {
-    double tot = 0.0;
-    for (int n = 1; n <= 200; ++n) { const double d = (double)n; tot += 1.0 / (d * d * d * d); }
-    double run = 0.0;
-    for (int n = 1; n <= 200; ++n) { const double d = (double)n; run += 1.0 / (d * d * d * d); a.mixcdf[n - 1] = run / tot; }
-  }
+  for (int q = t; q < 200; q += NT) a.mixcdf[q] = g_mix_cdf.v[q];
   for (int c = t; c < a.nc; c += NT) {
     double e = A_RAD * pow4(a.tr[c]) * a.vol[c];
     if (a.t_emit_floor > 0.0 && a.tr[c] < a.t_emit_floor) e = 0.0;
@@ -728,18 +786,34 @@ __global__ void __launch_bounds__(NT) k_ic_plan_mg(IcMgArgs a) {
 
 }  // namespace
 
+// Launch shape of the per-cell multigroup plan: up to 32 cells a block, two doubles per
+// (cell, group edge) of shared memory; above 48 KB the kernel is opted in to more.
+template <typename K>
+cudaError_t launch_plan_cells(K kernel, const PlanMgArgs& a, cudaStream_t s) {
+  const long long E = (long long)a.ng + 1;
+  const int cb = (int)std::max(1LL, std::min(32LL, 3072LL / E));
+  const size_t smem = (size_t)2 * cb * E * sizeof(double);
+  if (smem > 48 * 1024) {
+    const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  const int blocks = (a.nc + cb - 1) / cb;
+  kernel<<<blocks, 256, smem, s>>>(a, cb);
+  return cudaSuccess;
+}
+
 cudaError_t imc_launch_plan_mg(const PlanMgArgs& a, cudaStream_t s) {
   g_imc_launches += 2;
-  const int n = std::max(a.nc, std::max(a.nx, a.ny) + 1);
-  k_plan_mg_cells<<<(n + 255) / 256, 256, 0, s>>>(a);
+  const cudaError_t e = launch_plan_cells(k_plan_mg_cells, a, s);
+  if (e != cudaSuccess) return e;
   k_plan_mg<<<1, NT, 0, s>>>(a);
   return cudaGetLastError();
 }
 
 cudaError_t imc_launch_plan_mg1d(const PlanMgArgs& a, cudaStream_t s) {
   g_imc_launches += 2;
-  const int n = std::max(a.nc, std::max(a.nx, a.ny) + 1);
-  k_plan_mg1d_cells<<<(n + 255) / 256, 256, 0, s>>>(a);
+  const cudaError_t e = launch_plan_cells(k_plan_mg1d_cells, a, s);
+  if (e != cudaSuccess) return e;
   k_plan_mg1d<<<1, NT, 0, s>>>(a);
   return cudaGetLastError();
 }

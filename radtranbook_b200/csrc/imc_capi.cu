@@ -74,6 +74,8 @@ bool bank_ok(const imc_bank* b, bool two_d, bool mg = false) {
   return b->size >= 0 && b->capacity >= b->size && b->capacity < (1LL << 31);
 }
 
+// the workspace is 256-byte aligned by contract (its tables hold 8- and 16-byte vectors)
+inline bool ws_misaligned(const void* workspace) { return (reinterpret_cast<uintptr_t>(workspace) & 255u) != 0; }
 inline bool mg_sphere(const imc_mesh* m) { return m->n_groups > 1 && m->geometry == IMC_GEOM_SPHERE; }
 
 inline long long side_count(const imc_step_params* p, int q) {
@@ -126,7 +128,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   const long long n_upper = bank->size + bound;
   if (n_upper > bank->capacity) return IMC_ERR_BANK_OVERFLOW;
   const WsLayout L = imc_ws_layout(mesh, bank->capacity);
-  if (workspace_bytes < L.total) return IMC_ERR_WORKSPACE;
+  if (workspace_bytes < L.total || ws_misaligned(workspace)) return IMC_ERR_WORKSPACE;
   const int nc = mesh->nx * mesh->ny;
   // reserved bit 3: event-by-event tracking, its scratch after the workspace layout
   const bool event_mode = (par->reserved & 8) != 0;
@@ -135,9 +137,31 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     if (workspace_bytes < L.total + imc_event_scratch_bytes(bank->capacity)) return IMC_ERR_WORKSPACE;
   }
 
-  // per-step fields of the summary (everything after n_census) start at zero
-  IMC_CUDA(cudaMemsetAsync(reinterpret_cast<char*>(sum) + sizeof(int64_t), 0,
-                           sizeof(imc_step_summary) - sizeof(int64_t), s));
+  // every per-step accumulator starts at zero, in one launch: the summary's per-step fields
+  // (everything after n_census), the group energies, the fixed-point tallies, the intensity,
+  // the statistics, the tracking ticket and the census sums for the comb
+  unsigned long long* dep_fx = ws_ptr<unsigned long long>(workspace, L.dep_fx);
+  unsigned long long* esc_fx = ws_ptr<unsigned long long>(workspace, L.esc_fx);
+  unsigned long long* queue = ws_ptr<unsigned long long>(workspace, L.queue);
+  {
+    ZeroList zl{};
+    zl.add(reinterpret_cast<char*>(sum) + sizeof(int64_t), sizeof(imc_step_summary) - sizeof(int64_t));
+    if (mg) {
+      zl.add(tal->boundary_group, sizeof(double) * ng);
+      zl.add(tal->escaped_group, sizeof(double) * ng);
+    }
+    zl.add(dep_fx, sizeof(unsigned long long) * nc * ng);
+    zl.add(esc_fx, sizeof(unsigned long long) * (4 + ng));
+    zl.add(tal->si, sizeof(double) * nc * ng);
+    zl.add(tal->stats, sizeof(unsigned long long) * IMC_STAT_N);
+    zl.add(queue, 8);
+    if (par->census_bins && !adj) {
+      const int nb = par->census_bins == IMC_CENSUS_BY_GROUP_CELL ? nc * ng : nc;
+      zl.add(ws_ptr<double>(workspace, L.ecen), sizeof(double) * nb);
+      zl.add(ws_ptr<unsigned long long>(workspace, L.comb_mode + 8), sizeof(unsigned long long));
+    }
+    IMC_CUDA(imc_launch_zero(zl, s));
+  }
 
   // ---- plan: Fleck, per-cell source counts / weights / offsets, boundary faces ----
   PlanArgs pa{};
@@ -168,8 +192,6 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   if (!mg) {
     IMC_CUDA(imc_launch_plan(pa, s));
   } else if (mg1) {
-    IMC_CUDA(cudaMemsetAsync(tal->boundary_group, 0, sizeof(double) * ng, s));
-    IMC_CUDA(cudaMemsetAsync(tal->escaped_group, 0, sizeof(double) * ng, s));
     pm.geom = mesh->geometry; pm.nx = mesh->nx; pm.ny = mesh->ny; pm.nc = nc; pm.ng = ng;
     pm.e1 = mesh->edges1; pm.e2 = mesh->edges2; pm.vol = mesh->volume;
     pm.T = mat->temperature; pm.sigma = mat->sigma; pm.cv = mat->cv; pm.source = mat->source;
@@ -193,8 +215,6 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     pm.share = share;
     IMC_CUDA(imc_launch_plan_mg1d(pm, s));
   } else {
-    IMC_CUDA(cudaMemsetAsync(tal->boundary_group, 0, sizeof(double) * ng, s));
-    IMC_CUDA(cudaMemsetAsync(tal->escaped_group, 0, sizeof(double) * ng, s));
     pm.geom = mesh->geometry; pm.nx = mesh->nx; pm.ny = mesh->ny; pm.nc = nc; pm.ng = ng;
     pm.e1 = mesh->edges1; pm.e2 = mesh->edges2; pm.vol = mesh->volume;
     pm.T = mat->temperature; pm.sigma = mat->sigma; pm.cv = mat->cv; pm.source = mat->source;
@@ -309,14 +329,6 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
 
   // ---- tracking ----
   if (pe.ok) IMC_CUDA(cudaEventRecord(pe.e[1], s));
-  unsigned long long* dep_fx = ws_ptr<unsigned long long>(workspace, L.dep_fx);
-  unsigned long long* esc_fx = ws_ptr<unsigned long long>(workspace, L.esc_fx);
-  IMC_CUDA(cudaMemsetAsync(dep_fx, 0, sizeof(unsigned long long) * nc * ng, s));
-  IMC_CUDA(cudaMemsetAsync(esc_fx, 0, sizeof(unsigned long long) * (4 + ng), s));
-  IMC_CUDA(cudaMemsetAsync(tal->si, 0, sizeof(double) * nc * ng, s));
-  IMC_CUDA(cudaMemsetAsync(tal->stats, 0, sizeof(unsigned long long) * IMC_STAT_N, s));
-  unsigned long long* queue = ws_ptr<unsigned long long>(workspace, L.queue);
-  IMC_CUDA(cudaMemsetAsync(queue, 0, 8, s));
   IMC_CUDA(imc_launch_wsum(bank->weight, &sum->n_bank, n_upper, &sum->weight_sum, s));
 
   TrackArgs ta{};
@@ -333,13 +345,11 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   ta.dt_dev = par->dt_dev; ta.step_dev = par->step_dev;
   ta.id_base = par->id_base;
   if (par->census_bins && !adj) {
-    // census sums for the comb that follows on this workspace (IMC_COMB_CENSUS_READY)
-    const int nb = par->census_bins == IMC_CENSUS_BY_GROUP_CELL ? nc * ng : nc;
+    // census sums for the comb that follows on this workspace (IMC_COMB_CENSUS_READY),
+    // zeroed with the step's accumulators
     ta.ecen = ws_ptr<double>(workspace, L.ecen);
     ta.n_live = ws_ptr<unsigned long long>(workspace, L.comb_mode + 8);
     ta.ecen_by_group = par->census_bins == IMC_CENSUS_BY_GROUP_CELL ? 1 : 0;
-    IMC_CUDA(cudaMemsetAsync(ta.ecen, 0, sizeof(double) * nb, s));
-    IMC_CUDA(cudaMemsetAsync(ta.n_live, 0, sizeof(unsigned long long), s));
   }
   int rm = 0;
   for (int q = 0; q < 4; ++q) if (par->reflect[q]) rm |= 1 << q;
@@ -347,6 +357,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   ta.max_events = par->max_events > 0 ? par->max_events : (long long)1 << 30;
   ta.cap_is_reference = par->max_events > 0 ? 1 : 0;
   ta.seed = par->seed; ta.step = par->step;
+  imcdev::philox_round_keys(ta.seed, ta.rk);
   ta.chunk = par->chunk > 0 ? par->chunk : 64;
   ta.group_edges = mesh->group_edges;
   ta.escaped_group = tal->escaped_group;
@@ -390,7 +401,7 @@ imc_status comb_async(const imc_mesh* mesh, const imc_bank* in, imc_bank* out, i
   const bool census_ready = (per_group & IMC_COMB_CENSUS_READY) != 0;  // sums made by the tracking
   if (by_group && (!in->group || !out->group)) return IMC_ERR_INVALID_ARG;
   const WsLayout L = imc_ws_layout(mesh, in->size);
-  if (workspace_bytes < L.total) return IMC_ERR_WORKSPACE;
+  if (workspace_bytes < L.total || ws_misaligned(workspace)) return IMC_ERR_WORKSPACE;
   const int nc = mesh->nx * mesh->ny;
   const int nb = by_group ? nc * mesh->n_groups : nc;
 
@@ -406,22 +417,23 @@ imc_status comb_async(const imc_mesh* mesh, const imc_bank* in, imc_bank* out, i
   ca.ncopy = ws_ptr<unsigned long long>(workspace, L.ncopy); ca.cnt = ws_ptr<int>(workspace, L.cnt);
   ca.blk = ws_ptr<long long>(workspace, L.blk);
   ca.seed = seed; ca.step = step; ca.step_dev = step_dev;
+  imcdev::philox_round_keys(seed, ca.rk);
   ca.op1 = out->pos1; ca.op2 = two_d ? out->pos2 : nullptr; ca.od1 = out->dir1; ca.od2 = two_d ? out->dir2 : nullptr;
   ca.ow = out->weight; ca.ot = out->time; ca.ocell = out->cell; ca.ogroup = out->group;
+  ca.vec16 = ((reinterpret_cast<uintptr_t>(in->weight) | reinterpret_cast<uintptr_t>(in->cell) |
+               reinterpret_cast<uintptr_t>(by_group ? in->group : in->cell)) & 15u) == 0;
   ca.disc = disc;
+  ca.after = (per_group & IMC_COMB_WRITE_AFTER) ? disc + nb : nullptr;
   ca.sum = sum;
 
-  IMC_CUDA(cudaMemsetAsync(ca.ncopy, 0, sizeof(unsigned long long) * nb, s));
-  IMC_CUDA(cudaMemsetAsync(&sum->comb_after, 0, sizeof(double), s));
-  if (census_ready) {
-    IMC_CUDA(cudaMemsetAsync(ca.mode, 0, 8, s));  // the live count (next 8 bytes) is the tracking's
-  } else {
+  // ncopy is zeroed by the comb plan's weights kernel, comb_after and the mode by the plan
+  if (!census_ready) {  // else the census sums and the live count are the tracking's
     IMC_CUDA(cudaMemsetAsync(ca.ecen, 0, sizeof(double) * nb, s));
     IMC_CUDA(cudaMemsetAsync(ca.mode, 0, 16, s));
     IMC_CUDA(imc_launch_comb_ecen(ca, s));
   }
   CombPlanArgs cp{};
-  cp.nb = nb; cp.ecen = ca.ecen; cp.ew = ca.ew; cp.sum = sum;
+  cp.nb = nb; cp.ecen = ca.ecen; cp.ew = ca.ew; cp.ncopy = ca.ncopy; cp.sum = sum;
   // n_max > 0: comb to n_max; 0: keep every live entry; < 0: comb to |n_max| once at least
   // |n_max| entries are alive (MG_IMC/MG_IMC1D.py:1194-1200)
   cp.n_max = n_max < 0 ? -n_max : n_max;
@@ -467,10 +479,13 @@ WsLayout imc_ws_layout(const imc_mesh* m, int64_t capacity) {
   }
   L.mixcdf = take(8 * 200);
   L.ecen = take(8 * ncg); L.ew = take(8 * ncg); L.ncopy = take(8 * ncg);
-  L.cnt = take(4 * cap); L.blk = take(8 * ((cap + 1023) / 1024 + 2));
   L.comb_mode = take(16);
   L.dep_fx = take(8 * ncg); L.esc_fx = take(8 * (4 + ng));
   L.cf_rate = take(4 * nc);
+  // The regions sized by the capacity come last, so every other offset is the same for any
+  // capacity: a comb, laid out for its input's size, finds the census sums and the live count
+  // where the tracking, laid out for the bank's capacity, left them.
+  L.cnt = take(4 * cap); L.blk = take(8 * ((cap + 1023) / 1024 + 2));
   L.total = o;
   return L;
 }
@@ -558,7 +573,7 @@ imc_status imc_init_census(const imc_mesh* mesh, const double* tr, int64_t n_tar
   const bool two_d = mesh->geometry >= IMC_GEOM_XY;
   if (!tr || !bank_ok(bank, two_d) || !workspace) return IMC_ERR_INVALID_ARG;
   const WsLayout L = imc_ws_layout(mesh, bank->capacity);
-  if (workspace_bytes < L.total) return IMC_ERR_WORKSPACE;
+  if (workspace_bytes < L.total || ws_misaligned(workspace)) return IMC_ERR_WORKSPACE;
   cudaStream_t s = (cudaStream_t)stream;
   const int nc = mesh->nx * mesh->ny;
   const long long bound = n_target + (long long)nc * (two_d ? 2 : 1);  // ceil (+1) and 2-D min 1 per cell
@@ -645,7 +660,7 @@ imc_status imc_step_transport(const imc_mesh* mesh, const imc_material* mat, con
   imc_status st = check_mesh(mesh);
   if (st != IMC_OK) return st;
   const WsLayout L = imc_ws_layout(mesh, bank->capacity);
-  if (!workspace || workspace_bytes < L.total) return IMC_ERR_WORKSPACE;
+  if (!workspace || workspace_bytes < L.total || ws_misaligned(workspace)) return IMC_ERR_WORKSPACE;
   cudaStream_t s = (cudaStream_t)stream;
   report->required_capacity = bank->size + source_bound(mesh, par);
   imc_step_summary* sum = internal_summary(workspace, L);
@@ -679,7 +694,7 @@ imc_status imc_adjoint_vjp(const imc_mesh* mesh, const imc_material* mat, const 
   if ((mesh->geometry != IMC_GEOM_XY && mesh->geometry != IMC_GEOM_RZ) || mesh->n_groups != 1)
     return IMC_ERR_BAD_GEOMETRY;
   const WsLayout L = imc_ws_layout(mesh, bank->capacity);
-  if (!workspace || workspace_bytes < L.total) return IMC_ERR_WORKSPACE;
+  if (!workspace || workspace_bytes < L.total || ws_misaligned(workspace)) return IMC_ERR_WORKSPACE;
   cudaStream_t s = (cudaStream_t)stream;
   imc_step_summary* sum = internal_summary(workspace, L);
   long long n_census = bank->size;
@@ -712,12 +727,13 @@ imc_status imc_material_update_law(const imc_mesh* mesh, const imc_tallies* tal,
                                    void* stream) {
   imc_status st = check_mesh(mesh);
   if (st != IMC_OK) return st;
-  if (mesh->n_groups != 1) return IMC_ERR_INVALID_ARG;  // gray meshes
   if (!tal || !tal->dep || !tal->si || !tal->emitted || !law || !e || !tr || !T || !sigma_next || !cv_next)
     return IMC_ERR_INVALID_ARG;
   if ((!law->cv_eos_array && !(law->cv_eos > 0.0)) || (!law->cv_array && !(law->cv > 0.0))) return IMC_ERR_INVALID_ARG;
+  const int ng = std::max(1, mesh->n_groups);
+  if (ng > 1 && !law->sigma_group && !law->sigma_array) return IMC_ERR_INVALID_ARG;  // one factor per group
   MatArgs ma{};
-  ma.nc = mesh->nx * mesh->ny; ma.ng = 1; ma.vol = mesh->volume;
+  ma.nc = mesh->nx * mesh->ny; ma.ng = ng; ma.vol = mesh->volume;
   ma.dep = tal->dep; ma.si = tal->si; ma.emitted = tal->emitted; ma.e = e; ma.tr = tr;
   IMC_CUDA(imc_launch_material_law(ma, *law, T, sigma_next, cv_next, (cudaStream_t)stream));
   return IMC_OK;
@@ -766,7 +782,7 @@ imc_status imc_comb(const imc_mesh* mesh, const imc_bank* in, imc_bank* out, int
   imc_status st = check_mesh(mesh);
   if (st != IMC_OK) return st;
   const WsLayout L = imc_ws_layout(mesh, in->size);
-  if (!workspace || workspace_bytes < L.total) return IMC_ERR_WORKSPACE;
+  if (!workspace || workspace_bytes < L.total || ws_misaligned(workspace)) return IMC_ERR_WORKSPACE;
   cudaStream_t s = (cudaStream_t)stream;
   report->n_in = in->size;
   imc_step_summary* sum = internal_summary(workspace, L);
@@ -831,7 +847,7 @@ imc_status imc_energy_totals(const imc_mesh* mesh, const imc_bank* bank, const d
   if (st != IMC_OK) return st;
   if (!bank || !bank->weight || !e || !radiation || !internal || !workspace) return IMC_ERR_INVALID_ARG;
   const WsLayout L = imc_ws_layout(mesh, 1);
-  if (workspace_bytes < L.total) return IMC_ERR_WORKSPACE;
+  if (workspace_bytes < L.total || ws_misaligned(workspace)) return IMC_ERR_WORKSPACE;
   cudaStream_t s = (cudaStream_t)stream;
   imc_step_summary* sum = internal_summary(workspace, L);
   long long n = bank->size;

@@ -8,7 +8,8 @@
 //   4. exclusive scan of block totals                                         k_comb_scan
 //   5. copies written in bank order (block-local scan + block offset; one
 //      thread per copy)                                                       k_comb_scatter
-//   6. disc[b] = ecen - (copies in b) * FP32(ew)                              k_comb_disc
+//   6. disc[b] = ecen - (copies in b) * FP32(ew), and optionally that energy
+//      after the comb per bin (exact: equal FP32 weights summed in FP64)         k_comb_disc
 // Order of the output bank = order of the input bank, so the result is deterministic.
 // Modes (MG_IMC/MG_IMC1D.py:1187-1200, 808-820): when the comb plan decides not to comb
 // (Nmax = 0, or fewer live entries than a threshold) every live entry is copied once with its
@@ -80,41 +81,77 @@ __global__ void __launch_bounds__(256) k_comb_ecen(CombArgs a) {
   bins_flush(t, a.ecen);
 }
 
-// Each block combs a tile of TILE consecutive entries, CNT_T threads with TILE / CNT_T entries
-// each (coalesced across the block): copies per entry, copies per bin (per warp, then in the
-// block's table, flushed once) and the tile's total for the scan.
+// Each block combs a tile of TILE consecutive entries; each of its CNT_T threads takes CNT_PER
+// consecutive entries (16-byte vector loads and stores when the bank arrays allow them):
+// copies per entry, the tile's total for the scan, and copies per bin, summed in registers
+// over runs of equal bins (the bank is largely grouped by cell) and added to the block's
+// table when the bin changes, so the loop has no warp-wide step.
+constexpr int CNT_PER = TILE / CNT_T;
+
+__device__ __forceinline__ int comb_copies(const CombArgs& a, long long k, float wf, int bk, bool compact,
+                                           uint32_t step, int& b) {
+  b = 0;
+  if (!(wf > 0.f) || !bin_ok(a, bk)) return 0;
+  b = bk;
+  if (compact) return 1;
+  const double ew = a.ew[b];
+  if (!(ew > 0.0)) return 0;
+  const U4 r = draw_rk(a.rk, (uint32_t)k, 0, step, TAG_COMB);
+  return (int)floor((double)wf / ew + u01d(r.x));
+}
+
 __global__ void __launch_bounds__(CNT_T) k_comb_count(CombArgs a) {
   const uint32_t step = a.step_dev ? *a.step_dev : a.step;  // graph replay
   __shared__ unsigned sh[CNT_T / 32];
   __shared__ BlockCounts<CNT_SLOTS> t;
   counts_init(t);
   __syncthreads();
-  const long long tile0 = (long long)blockIdx.x * TILE;
   const long long n_in = min((long long)*a.d_n_in, (long long)a.n_bound);  // the grid covers n_bound entries
   const bool compact = *a.mode != 0;
-  unsigned tsum = 0;
-  for (int i = 0; i < TILE / CNT_T; ++i) {  // uniform trip count: warps stay converged
-    const long long k = tile0 + (long long)i * CNT_T + threadIdx.x;
-    int n = 0, b = 0;
-    if (k < n_in) {
-      const float wf = a.w[k];
-      const int bk = bin_of(a, k);  // loaded with the weight (k < n_in: in bounds)
-      if (wf > 0.f && bin_ok(a, bk)) {
-        b = bk;
-        const double ew = a.ew[b];
-        if (compact) {
-          n = 1;
-        } else if (ew > 0.0) {
-          const U4 r = draw(a.seed, (uint32_t)k, 0, step, TAG_COMB);
-          n = (int)floor((double)wf / ew + u01d(r.x));
-        }
+  const long long k0 = (long long)blockIdx.x * TILE + (long long)threadIdx.x * CNT_PER;
+  unsigned tsum = 0, run_n = 0;
+  int run_b = -1;
+#pragma unroll 1
+  for (int j = 0; j < CNT_PER; j += 4) {
+    const long long kj = k0 + j;
+    float wv[4] = {0.f, 0.f, 0.f, 0.f};
+    int bv[4] = {0, 0, 0, 0};
+    if (a.vec16 && kj + 3 < n_in) {  // kj % 4 == 0: the 16-byte loads are aligned
+      const float4 W = *reinterpret_cast<const float4*>(a.w + kj);
+      const int4 C = *reinterpret_cast<const int4*>(a.cell + kj);
+      wv[0] = W.x; wv[1] = W.y; wv[2] = W.z; wv[3] = W.w;
+      bv[0] = C.x; bv[1] = C.y; bv[2] = C.z; bv[3] = C.w;
+      if (a.per_group) {
+        const int4 g = *reinterpret_cast<const int4*>(a.group + kj);
+        bv[0] += a.nc * g.x; bv[1] += a.nc * g.y; bv[2] += a.nc * g.z; bv[3] += a.nc * g.w;
       }
-      a.cnt[k] = n;
+    } else {
+      for (int q = 0; q < 4; ++q)
+        if (kj + q < n_in) { wv[q] = a.w[kj + q]; bv[q] = bin_of(a, kj + q); }
     }
-    // copies per bin: aggregated per warp, then per block (the bank is largely grouped by cell)
-    warp_counts_add(n > 0, b, (unsigned)n, t, a.ncopy);
-    tsum += (unsigned)n;
+    int nv[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      int b;
+      const int n = kj + q < n_in ? comb_copies(a, kj + q, wv[q], bv[q], compact, step, b) : 0;
+      nv[q] = n;
+      tsum += (unsigned)n;
+      if (n > 0) {
+        if (b != run_b) {
+          if (run_n) counts_add(t, run_b, run_n, a.ncopy);
+          run_b = b;
+          run_n = 0;
+        }
+        run_n += (unsigned)n;
+      }
+    }
+    if (kj + 3 < n_in) {
+      *reinterpret_cast<int4*>(a.cnt + kj) = make_int4(nv[0], nv[1], nv[2], nv[3]);  // workspace: aligned
+    } else {
+      for (int q = 0; q < 4; ++q) if (kj + q < n_in) a.cnt[kj + q] = nv[q];
+    }
   }
+  if (run_n) counts_add(t, run_b, run_n, a.ncopy);
   const unsigned ws = __reduce_add_sync(FULL, tsum);
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = ws;
   __syncthreads();
@@ -216,6 +253,7 @@ __global__ void k_comb_disc(CombArgs a) {
     // compact only: every live entry kept with its weight, nothing is lost
     after = *a.mode != 0 ? a.ecen[b] : (double)a.ncopy[b] * (double)copy_weight(a, b);
     a.disc[b] = a.ecen[b] - after;
+    if (a.after) a.after[b] = after;
   }
   after = warp_sum_d(after);
   if ((threadIdx.x & 31) == 0 && after != 0.0) atomicAdd(&a.sum->comb_after, after);

@@ -54,6 +54,29 @@ __device__ __forceinline__ U4 draw(uint64_t seed, uint32_t idx, uint32_t block, 
   return philox4x32_10(U4{idx, block, step, tag}, (uint32_t)seed, (uint32_t)(seed >> 32));
 }
 
+// The 20 round keys of a seed (k0 + r*0x9E3779B9, k1 + r*0xBB67AE85, r = 0..9), for kernels
+// that carry them in their parameter block: the rounds then read them as constant operands
+// instead of stepping the key in registers.  Same outputs as draw().
+__host__ __device__ inline void philox_round_keys(uint64_t seed, uint32_t* rk) {
+  uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  for (int r = 0; r < 10; ++r) {
+    rk[2 * r] = k0; rk[2 * r + 1] = k1;
+    k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+  }
+}
+
+__device__ __forceinline__ U4 draw_rk(const uint32_t* rk, uint32_t idx, uint32_t block, uint32_t step,
+                                      uint32_t tag) {
+  U4 c{idx, block, step, tag};
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+    const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+    c = U4{hi1 ^ c.y ^ rk[2 * r], lo1, hi0 ^ c.w ^ rk[2 * r + 1], lo0};
+  }
+  return c;
+}
+
 // -log(u) for u = u01: distance in mean free paths.
 __device__ __forceinline__ float neglog_u(uint32_t x) { return -logf(u01f(x)); }
 

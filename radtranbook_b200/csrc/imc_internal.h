@@ -14,6 +14,7 @@
 // Tracking
 // ---------------------------------------------------------------------------------
 struct TrackArgs {
+  uint32_t rk[20];           // Philox round keys of seed (philox_round_keys)
   int nx, ny, nc, ng;
   const float* e1;           // nx+1 edges (FP32 copy)
   const float* e2;           // ny+1
@@ -177,9 +178,20 @@ struct CombPlanArgs {
   int* mode;                       // out: 0 comb, 1 compact only
   const double* ecen;
   double* ew;
+  unsigned long long* ncopy;       // zeroed with the weights (the count accumulates into it)
   imc_step_summary* sum;
 };
 cudaError_t imc_launch_comb_plan(const CombPlanArgs& a, cudaStream_t s);
+
+// Up to 12 device regions zeroed by one launch (8-byte aligned, sizes multiples of 8): the
+// per-step tallies, counters and summary fields that a step's kernels accumulate into.
+struct ZeroList {
+  int n;
+  void* p[12];
+  unsigned long long bytes[12];
+  void add(void* ptr, size_t b) { if (ptr && b) { p[n] = ptr; bytes[n] = b; ++n; } }
+};
+cudaError_t imc_launch_zero(const ZeroList& z, cudaStream_t s);
 
 cudaError_t imc_launch_canon_sum_eV(const double* e, const double* vol, int nc, double* out, cudaStream_t s);
 
@@ -236,7 +248,9 @@ cudaError_t imc_launch_wsum(const float* w, const int64_t* d_n, long long n_boun
 // Comb kernels
 // ---------------------------------------------------------------------------------
 struct CombArgs {
+  uint32_t rk[20];             // Philox round keys of seed (philox_round_keys)
   int nc, nb, per_group;
+  int vec16;                   // w, cell (and group) 16-byte aligned: vector loads in the count
   int conserve_rad;            // copies in bin b weigh ecen[b] / ncopy[b] (bin energy kept)
   int* mode;                   // set by the comb plan: 0 comb, 1 compact only (copy live entries)
   const uint32_t* step_dev;    // non-NULL: the Philox step counter is read from device memory
@@ -250,6 +264,7 @@ struct CombArgs {
   uint64_t seed; uint32_t step;
   float* op1; float* op2; float* od1; float* od2; float* ow; float* ot; int* ocell; int* ogroup;
   double* disc;
+  double* after;               // nullable: energy after the comb per bin [nb]
   imc_step_summary* sum;
 };
 cudaError_t imc_launch_comb_ecen(const CombArgs& a, cudaStream_t s);

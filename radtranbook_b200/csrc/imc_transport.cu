@@ -93,7 +93,7 @@ __device__ __forceinline__ void history_event(const TrackArgs& a, Hist& h, EvOut
     if (!a.cap_is_reference) atomicOr(a.flags, (int)IMC_FLAG_EVENT_CAP);
     finished = true;
   } else {
-    const U4 r = draw(a.seed, a.id_base + pid, ev, stepk, TAG_TRANSPORT);
+    const U4 r = draw_rk(a.rk, a.id_base + pid, ev, stepk, TAG_TRANSPORT);
     ++ev;
     float d, sb, L, xn = x, yn = y, un = u, vn = v;
     int evt, cross = X_NONE;
@@ -486,7 +486,13 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
       ud = fx_units(f_lost, inv_q);
       vs = f_wd;
     }
-    warp_tally_fx(flush, flush_cell, ud, vs, dep_t, si_t, st);
+    if (SMEM_TALLY) {
+      // block tallies in shared memory: one shared atomic per flushing lane costs less than
+      // grouping the warp's lanes by cell first (the grouping pays off for global tallies)
+      if (flush) { if (ud) atomicAdd(dep_t + flush_cell, ud); if (vs != 0.0) atomicAdd(si_t + flush_cell, vs); }
+    } else {
+      warp_tally_fx(flush, flush_cell, ud, vs, dep_t, si_t, st);
+    }
     if (a.ecen) {
       warp_tally1(cen, cen_bin, (double)w, a.ecen, st);
       n_alive += cen ? 1u : 0u;

@@ -36,7 +36,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._gray import face_temperatures
+from ._gray import _law, face_temperatures
 from .engine import C_LIGHT
 from .materials import GroupedOpacity, evaluate, evaluate_groups, is_device
 
@@ -114,6 +114,15 @@ class DeviceLoop:
                        cf_fastpath=float(cf_fastpath), T_emit_floor=float(T_emit_floor))
         self.sigma_a_func, self.inv_eos, self.cv = sigma_a_func, inv_eos, cv
         self.conserve = bool(conserve_comb_energy)
+        # a device-evaluated material law (LinearEOS, Constant cv, PowerLawOpacity / Constant /
+        # GroupPowerLawOpacity): the material update kernel writes T and the next step's opacity
+        # and cv into one buffer pair, which the next step's plan reads (nothing later in a step
+        # reads them, so one pair serves every step of the graph)
+        self.law = _law(state, sigma_a_func, cv, inv_eos) if not self.conserve else None
+        self.law_key = (id(sigma_a_func), id(cv))
+        if self.law is not None:
+            self.law_sigma = torch.empty(eng.ng * eng.nc, dtype=torch.float64, device=dev)
+            self.law_cv = torch.empty(eng.nc, dtype=torch.float64, device=dev)
         self.refl = tuple(reflect) + (False,) * (4 - len(reflect))
         self.src = None
         if Nsource > 0 and source is not None:
@@ -148,16 +157,20 @@ class DeviceLoop:
         torch.index_select(self.step_sched, 0, self.k_dev, out=self.step_dev)
         torch.index_select(self.nmax_sched, 0, self.k_dev, out=self.nmax_dev)
         like = st.grid(st._T)
-        sigma = evaluate_groups(self.sigma_funcs, like, _no_host, like).transpose(1, 2).reshape(-1) \
-            if self.mg else st.flat(evaluate(self.sigma_funcs[0], like, _no_host, like))
-        cvv = st.flat(evaluate(self.cv, like, _no_host, like))
+        if self.law is not None:
+            sigma, cvv = self.law_sigma, self.law_cv
+        else:
+            sigma, cvv = self._materials(like)
         # the host-side step and dt are placeholders: the kernels read step_dev / dt_dev
         eng.transport_async(st._T, sigma, cvv, self.src, 0, 1.0, kw["theta"], kw["Ntarget"], kw["Nboundary"],
                             kw["Nsource"], self.faces, self.refl, max_events=kw["max_events"],
                             rz_linear_source=kw["rz_linear_source"], t_emit_floor=kw["T_emit_floor"],
                             method=kw["method"], cf_fastpath=kw["cf_fastpath"], step_dev=self.step_dev,
                             dt_dev=self.dt_dev)
-        eng.material_update(st._e, st._Tr)
+        if self.law is not None:
+            eng.material_update_law(st._e, st._Tr, st._T, self.law[0], self.law_sigma, self.law_cv)
+        else:
+            eng.material_update(st._e, st._Tr)
         if self.mg:
             self.rad_last.copy_(eng.si)
             if self.fid.numel():
@@ -167,8 +180,9 @@ class DeviceLoop:
                        out_capacity=self.cap_census, n_max_dev=self.nmax_dev)
         if self.conserve:
             st._e.add_((eng.disc.view(eng.ng, eng.nc).sum(0) if self.mg else eng.disc[: eng.nc]) / eng.vol)
-        Tn = evaluate(self.inv_eos, st.grid(st._e), _no_host, like)
-        st._T.copy_(st.flat(Tn))
+        if self.law is None:
+            Tn = evaluate(self.inv_eos, st.grid(st._e), _no_host, like)
+            st._T.copy_(st.flat(Tn))
         # epilogue: summary, fiducial temperatures, output snapshots
         self.hist_sum.index_copy_(0, self.k_dev, eng.summary_dev.view(1, -1))
         if self.fid.numel():
@@ -184,6 +198,13 @@ class DeviceLoop:
         eng.spare.size = self.cap_census
         eng.bank, eng.spare = eng.spare, eng.bank
         eng._census_dev_valid = True
+
+    def _materials(self, like) -> tuple:
+        """Opacity ([g][c] flat) and heat capacity of the material callables at the state's T."""
+        st = self.state
+        sigma = evaluate_groups(self.sigma_funcs, like, _no_host, like).transpose(1, 2).reshape(-1) \
+            if self.mg else st.flat(evaluate(self.sigma_funcs[0], like, _no_host, like))
+        return sigma, st.flat(evaluate(self.cv, like, _no_host, like))
 
     def _graph(self, n: int) -> torch.cuda.CUDAGraph:
         """The n-step graph starting from the bank that holds the census now (captured once;
@@ -261,6 +282,15 @@ class DeviceLoop:
             evaluate(f, like, _no_host, like)
         evaluate(self.cv, like, _no_host, like)
         evaluate(self.inv_eos, st.grid(st._e), _no_host, like)
+        if self.law is not None:  # the first step's opacity: the eager step's law output, else the callables
+            nxt = st.__dict__.get("_law_next")
+            if nxt is not None and nxt[0] == self.law_key:
+                self.law_sigma.copy_(nxt[1].reshape(-1))
+                self.law_cv.copy_(nxt[2])
+            else:
+                sigma, cvv = self._materials(like)
+                self.law_sigma.copy_(sigma)
+                self.law_cv.copy_(cvv)
         eng._set_census_count(eng.bank.size)
         eng.bank.size = eng.spare.size = self.cap_census
         g2 = self._graph(2) if n >= 2 else None
@@ -275,6 +305,10 @@ class DeviceLoop:
             eng.bank, eng.spare = eng.spare, eng.bank
         e1.record()
         torch.cuda.current_stream().synchronize()
+        if self.law is not None:  # an eager step after the loop continues from the loop's law output
+            st.__dict__["_law_next"] = (self.law_key, self.law_sigma, self.law_cv)
+        else:
+            st.__dict__.pop("_law_next", None)
         out = self._finish(dts, outs, labels)
         out["device_ms"] = e0.elapsed_time(e1)
         return out

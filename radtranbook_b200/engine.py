@@ -135,7 +135,9 @@ class Engine:
         self.sigma_s = torch.zeros(ncg, **f64)
         self.escaped = torch.zeros(4 + n_groups, **f64)
         self.stats = torch.zeros(_lib.STAT_N, dtype=torch.int64, device=dev)
-        self.disc = torch.zeros(ncg, **f64)
+        # comb discrepancy per bin, then (IMC_COMB_WRITE_AFTER) the energy after the comb per bin
+        self._disc2 = torch.zeros(2 * ncg, **f64)
+        self.disc, self.comb_after = self._disc2[:ncg], self._disc2[ncg:]
         self.ctal = ImcTallies(_ptr(self.dep), _ptr(self.si), _ptr(self.emitted), _ptr(self.sigma_a),
                                _ptr(self.sigma_s), _ptr(self.escaped), _ptr(self.stats),
                                _ptr(self.escaped_group), _ptr(self.boundary_group))
@@ -207,6 +209,14 @@ class Engine:
         if self.ws.numel() < need:
             self.ws = torch.empty(int(need * 1.25) + 4096, dtype=torch.uint8, device=self.device)
         return self.ws.data_ptr(), self.ws.numel()
+
+    def reserve(self, census: int, sources: int = 0) -> None:
+        """Size the bank and the spare bank for a census of up to `census` entries (a comb
+        target) plus `sources` new entries a step, so that a growing comb target reallocates
+        nothing (each bank otherwise grows by 1.25x when it runs out)."""
+        cap = int(1.15 * census) + 2 * self.nc * self.ng + 4096 + int(sources)
+        self.bank.ensure(cap)
+        self.spare.ensure(cap)
 
     def _call_bank(self, name: str, fn, bank: Bank, grow_from, *args):
         """Call fn(cbank, ...); on bank overflow grow `bank` and retry once."""
@@ -386,18 +396,19 @@ class Engine:
 
     def comb_async(self, n_max: int, step: int, e: torch.Tensor | None, per_group: bool = False,
                    conserve_radiation: bool = False, step_dev: torch.Tensor | None = None,
-                   out_capacity: int | None = None, n_max_dev: torch.Tensor | None = None) -> None:
+                   out_capacity: int | None = None, n_max_dev: torch.Tensor | None = None,
+                   write_after: bool = False) -> None:
         """Queue the comb (n_max semantics as comb()); fetch() completes it.  step_dev: device
         step counter (graph replay); n_max_dev: device int64 comb target read when the comb runs
         (with step_dev; n_max > 0 then sizes the spare bank); out_capacity: cap the combed census
         below the spare bank's capacity (a larger one is flagged as an overflow and the census
-        is emptied)."""
+        is emptied); write_after: the energy after the comb per bin goes to comb_after."""
         self.spare.size = 0
         want = int(1.15 * n_max) if n_max > 0 else self._upper
         self.spare.ensure(want + 2 * self.nc * self.ng + 4096)
         if n_max_dev is not None and (step_dev is None or n_max <= 0):
             raise ValueError("n_max_dev needs step_dev and n_max > 0")
-        flags = _comb_flags(per_group, conserve_radiation)
+        flags = _comb_flags(per_group, conserve_radiation) | (_lib.COMB_WRITE_AFTER if write_after else 0)
         want_bins = _lib.CENSUS_BY_GROUP_CELL if per_group else _lib.CENSUS_BY_CELL
         if self._census_bins and self._census_bins == want_bins:
             flags |= _lib.COMB_CENSUS_READY  # the tracking of this bank summed its census

@@ -122,14 +122,15 @@ class LinearEOS:
 
 
 def material_law(sigma_a_func, cv, inv_eos, flat, device):
-    """The law of a gray material the device evaluates itself (imc_material_law), when the
+    """The law of a material the device evaluates itself (imc_material_law), when the
     callables are a LinearEOS inverse, a Constant heat capacity and a PowerLawOpacity or
-    Constant opacity; else None.  flat(tensor) puts a per-cell array in the engine's cell
-    order.  Returns (law, tensors the law points to)."""
+    Constant opacity (gray) or a GroupPowerLawOpacity (multigroup); else None.  flat(tensor)
+    puts a per-cell array in the engine's cell order.  Returns (law, tensors the law points
+    to)."""
     from ._lib import ImcMaterialLaw
 
     if not (isinstance(inv_eos, _LinearEOSFunction) and inv_eos.inverse and isinstance(cv, Constant)
-            and isinstance(sigma_a_func, (PowerLawOpacity, Constant))):
+            and isinstance(sigma_a_func, (PowerLawOpacity, Constant, GroupPowerLawOpacity))):
         return None
     keep = []
 
@@ -144,7 +145,22 @@ def material_law(sigma_a_func, cv, inv_eos, flat, device):
     law = ImcMaterialLaw()
     law.cv_eos, law.cv_eos_array = scalar_or_array(inv_eos.cv)
     law.cv, law.cv_array = scalar_or_array(cv)
-    if isinstance(sigma_a_func, Constant):
+    if isinstance(sigma_a_func, GroupPowerLawOpacity):
+        o = sigma_a_func
+        law.sigma_A, law.sigma_n = o.A, o.n
+        law.sigma_lo = float(o.lo) if o.lo is not None else 0.0
+        law.sigma_hi = float(o.hi) if o.hi is not None else 0.0
+        law.sigma_T_floor = float(o.T_floor) if o.T_floor is not None else 0.0
+        sc = np.asarray(o.scale, dtype=np.float64)
+        if sc.ndim or float(sc) != 1.0:  # a per-cell factor (a scalar one as a constant array)
+            t = flat(torch.as_tensor(np.broadcast_to(sc, o.field_shape) if sc.ndim == 0 else sc,
+                                     device=device)).contiguous()
+            keep.append(t)
+            law.sigma_scale = t.data_ptr()
+        f = torch.as_tensor(o.factors, device=device)
+        keep.append(f)
+        law.sigma_group = f.data_ptr()
+    elif isinstance(sigma_a_func, Constant):
         law.sigma_A, law.sigma_array = scalar_or_array(sigma_a_func)
         law.sigma_n = 0.0
     else:
@@ -164,6 +180,65 @@ class GroupedOpacity(list):
     def __init__(self, funcs, all_groups):
         super().__init__(funcs)
         self.all_groups = all_groups
+
+
+class GroupPowerLawOpacity(GroupedOpacity):
+    """Multigroup opacity sigma_g(T) = A * max(T, T_floor)**(-n) * scale * factors[g], clamped
+    to [lo, hi] (multiplied in that order; T_floor / lo / hi None for none; scale a scalar or
+    a per-cell array shaped like the temperature field).  A GroupedOpacity: its per-group
+    callables and all_groups work on host arrays and device tensors alike.  With a LinearEOS
+    and a Constant heat capacity the multigroup steps evaluate it on the device themselves,
+    in the material update kernel (imc_material_law)."""
+
+    def __init__(self, A: float, n: float, factors, scale=1.0, T_floor: float | None = None,
+                 lo: float | None = None, hi: float | None = None, field_shape: tuple | None = None):
+        self.A, self.n = float(A), float(n)
+        self.factors = np.ascontiguousarray(factors, dtype=np.float64)
+        self.scale = scale
+        self.T_floor, self.lo, self.hi = T_floor, lo, hi
+        sc = np.asarray(scale)
+        self.field_shape = tuple(field_shape) if field_shape is not None else sc.shape
+        self._dev = {}
+        super().__init__([self._one(g) for g in range(len(self.factors))], self._all)
+
+    def _const(self, key, value, like):
+        k = (key, like.device)
+        if k not in self._dev:
+            self._dev[k] = torch.as_tensor(np.asarray(value, dtype=np.float64), device=like.device)
+        return self._dev[k]
+
+    def _base(self, T):
+        if isinstance(T, torch.Tensor):
+            tp = torch.clamp(T, min=self.T_floor) if self.T_floor is not None else T
+            b = self.A * torch.pow(tp, -self.n) if self.n != 0.0 else torch.full_like(T, self.A)
+            return b * self._const("scale", self.scale, T) if np.ndim(self.scale) else b * float(self.scale)
+        T = np.asarray(T, dtype=np.float64)
+        tp = np.maximum(T, self.T_floor) if self.T_floor is not None else T
+        b = self.A * np.power(tp, -self.n) if self.n != 0.0 else np.full_like(T, self.A)
+        return b * np.asarray(self.scale, dtype=np.float64)
+
+    def _clamp(self, s):
+        if self.lo is None and self.hi is None:
+            return s
+        if isinstance(s, torch.Tensor):
+            return torch.clamp(s, min=self.lo, max=self.hi)
+        return np.clip(s, self.lo, self.hi)
+
+    def _one(self, g):
+        f = float(self.factors[g])
+
+        def sigma_g(T):
+            return self._clamp(self._base(T) * f)
+        sigma_g._imc_device = True
+        return sigma_g
+
+    def _all(self, T):
+        b = self._base(T)
+        if isinstance(b, torch.Tensor):
+            f = self._const("factors", self.factors, b).view((-1,) + (1,) * b.dim())
+        else:
+            f = self.factors.reshape((-1,) + (1,) * b.ndim)
+        return self._clamp(b.unsqueeze(0) * f if isinstance(b, torch.Tensor) else b[None] * f)
 
 
 def evaluate_groups(funcs, T_dev: torch.Tensor, T_host_fn, like: torch.Tensor,

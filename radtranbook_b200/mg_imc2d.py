@@ -24,7 +24,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._gray import GrayState, _host_copy, _staged, check_partition, face_temperatures
+from ._gray import GrayState, _host_copy, _law, _staged, check_partition, face_temperatures
 from .partition import local_count, sum_scalars, sum_tensors, summary_totals, world_of
 from .engine import A_RAD, C_LIGHT, Engine
 from .materials import evaluate, evaluate_groups
@@ -155,16 +155,31 @@ def _rad_by_group(eng: Engine) -> torch.Tensor:
 
 
 def _group_buffers(state, eng: Engine) -> dict:
-    """Device buffer for the post-comb energy by group and pinned host buffers for the
-    end-of-step copies of the by-group fields (allocated once per state)."""
+    """Pinned host buffers for the end-of-step copies of the by-group fields: the boundary and
+    escaped energy by group (allocated once per state), and for the (G, nx, ny) radiation
+    energies a fresh pair each step from torch's caching pinned allocator, which the step's
+    info arrays then view without a host copy (a buffer returns to the cache once nothing
+    views it)."""
     hb = state.__dict__.get("_mg_hbuf")
     if hb is None:
-        n = eng.ng * eng.nc
-        hb = {"post_dev": torch.zeros(n, dtype=torch.float64, device=eng.device)}
-        for k, m in (("pre", n), ("post", n), ("bnd", eng.ng), ("esc", eng.ng)):
-            hb[k] = torch.zeros(m, dtype=torch.float64, pin_memory=True)
+        hb = {k: torch.zeros(eng.ng, dtype=torch.float64, pin_memory=True) for k in ("bnd", "esc")}
         object.__setattr__(state, "_mg_hbuf", hb)
-    return hb
+    n = eng.ng * eng.nc
+    return dict(hb, pre=torch.empty(n, dtype=torch.float64, pin_memory=True),
+                post=torch.empty(n, dtype=torch.float64, pin_memory=True))
+
+
+def _law_buffers(state, eng: Engine, sigma: torch.Tensor) -> tuple:
+    """The (opacity [g][c], heat capacity [c]) pair the material law kernel writes this step:
+    of two pairs, the one the step is not reading."""
+    nb = state.__dict__.get("_law_buf")
+    if nb is None or nb[0].numel() != eng.ng * eng.nc:
+        nb = (torch.empty(eng.ng * eng.nc, dtype=torch.float64, device=eng.device),
+              torch.empty(eng.nc, dtype=torch.float64, device=eng.device),
+              torch.empty(eng.ng * eng.nc, dtype=torch.float64, device=eng.device),
+              torch.empty(eng.nc, dtype=torch.float64, device=eng.device))
+        object.__setattr__(state, "_law_buf", nb)
+    return nb[:2] if sigma.data_ptr() != nb[0].data_ptr() else nb[2:]
 
 
 def _boundary_energy_estimate(geometry, e1, e2, Tb, dt, bsf) -> float:
@@ -202,10 +217,19 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
     G, nc = eng.ng, eng.nc
     like = state.grid(state._T)
     host_T = lambda: state.temperature  # noqa: E731
-    # host callables' results go up by asynchronous copies from pinned buffers of the state
-    sig = evaluate_groups(sigma_a_funcs, like, host_T, like,
-                          **_staged(state, "sigma_g", G * nc)).transpose(1, 2).reshape(G, -1)  # (G, nc)
-    cvv = state.flat(evaluate(cv, like, host_T, like, **_staged(state, "cv", nc)))
+    # a material the device evaluates itself (LinearEOS, Constant cv, GroupPowerLawOpacity):
+    # the material update, inverse EOS and next step's opacities are one kernel at the step's end
+    law = _law(state, sigma_a_funcs, cv, inv_eos) if not conserve_comb_energy else None
+    if law is not None and len(sigma_a_funcs) != G:
+        raise ValueError(f"{len(sigma_a_funcs)} opacity groups for a {G}-group state")
+    nxt = state.__dict__.get("_law_next")
+    if law is not None and nxt is not None and nxt[0] == (id(sigma_a_funcs), id(cv)):
+        sig, cvv = nxt[1].view(G, nc), nxt[2]  # evaluated on the device at the end of the last step
+    else:
+        # host callables' results go up by asynchronous copies from pinned buffers of the state
+        sig = evaluate_groups(sigma_a_funcs, like, host_T, like,
+                              **_staged(state, "sigma_g", G * nc)).transpose(1, 2).reshape(G, -1)  # (G, nc)
+        cvv = state.flat(evaluate(cv, like, host_T, like, **_staged(state, "cv", nc)))
     if emission_fractions is not None:
         eng.emission_fractions = torch.as_tensor(np.asarray(emission_fractions, dtype=np.float64), device=eng.device)
     else:
@@ -250,30 +274,40 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
     t_eval = _time.perf_counter()
     nt_l, nb_l, ns_l = (local_count(n, rank, world) for n in (Ntarget, Nboundary, Nsource))
     nmax_l = local_count(Nmax, rank, world) if Nmax > 0 else Nmax
+    if Nmax_final is not None and Nmax_growth > 0:  # size the banks once for the whole schedule
+        eng.reserve(local_count(max(int(Nmax_final), Nmax), rank, world), nt_l + 4 * nb_l + ns_l)
     eng.transport_async(state._T, sig.reshape(-1).contiguous(), cvv, src, state.count, dt, theta, nt_l, nb_l, ns_l,
                         faces, refl, max_events=max_events_per_particle, rz_linear_source=False,
                         t_emit_floor=T_emit_floor)
     sum_tensors(dist, [eng.dep, eng.si, eng.emitted, eng.boundary_group, eng.escaped_group])
-    eng.material_update(state._e, state._Tr)
+    if law is not None:
+        sig_next, cv_next = _law_buffers(state, eng, sig)
+        eng.material_update_law(state._e, state._Tr, state._T, law[0], sig_next, cv_next)
+        state.__dict__["_law_next"] = ((id(sigma_a_funcs), id(cv)), sig_next, cv_next)
+    else:
+        state.__dict__.pop("_law_next", None)
+        eng.material_update(state._e, state._Tr)
     rad_pre = eng.si.view(G, nc) / C_LIGHT  # radiation energy density by group (path length)
-    eng.comb_async(nmax_l, state.count, state._e, per_group=True)
+    # the comb also writes the energy after it per (group, cell) bin: the post-comb radiation
+    # energy by group without a pass over the new census
+    eng.comb_async(nmax_l, state.count, state._e, per_group=True, write_after=True)
     hb = _group_buffers(state, eng)
-    eng.census_energy_async(hb["post_dev"], per_group=True)  # post-comb energy by (group, cell)
-    sum_tensors(dist, [hb["post_dev"]])
-    hb["post_dev"].view(G, nc).div_(eng.vol.view(1, nc))
+    sum_tensors(dist, [eng.comb_after])
+    post_dev = eng.comb_after.view(G, nc) / eng.vol.view(1, nc)
     if conserve_comb_energy:
         sum_tensors(dist, [eng.disc])
         state._e.add_(eng.disc.view(G, nc).sum(0) / eng.vol)
-    Tn = evaluate(inv_eos, state.grid(state._e), lambda: _host_copy(state.grid(state._e)), like,
-                  **_staged(state, "T_new", nc))
-    state._T.copy_(state.flat(Tn))
+    if law is None:
+        Tn = evaluate(inv_eos, state.grid(state._e), lambda: _host_copy(state.grid(state._e)), like,
+                      **_staged(state, "T_new", nc))
+        state._T.copy_(state.flat(Tn))
     nx, ny = state._shape
 
     def to_grid3(x):  # device (G, nc) in flat cell order -> (G, nx, ny) C order, flattened
         return x.reshape(G, ny, nx).transpose(1, 2).reshape(-1)
 
     # the (G, nx, ny) transposes run on the device, so the host only copies contiguous arrays
-    group_copies = [(to_grid3(rad_pre), hb["pre"]), (to_grid3(hb["post_dev"]), hb["post"]),
+    group_copies = [(to_grid3(rad_pre), hb["pre"]), (to_grid3(post_dev), hb["post"]),
                     (eng.boundary_group, hb["bnd"]), (eng.escaped_group, hb["esc"])]
     try:
         sm = eng.fetch(state.host_copies() + group_copies)
@@ -315,8 +349,8 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
     state.previous_total_energy = total
     state.count += 1
 
-    def grid3(h):  # pinned host buffer, already (G, nx, ny) -> an array of its own
-        return h.numpy().reshape(G, nx, ny).copy()
+    def grid3(h):  # this step's pinned host buffer, already (G, nx, ny): the array views it
+        return h.numpy().reshape(G, nx, ny)
 
     if not use_scalar_intensity_Tr:
         hb["pre"].copy_(to_grid3(rad_pre))
@@ -425,6 +459,9 @@ def run_simulation(Ntarget, Nboundary, Nsource, Nmax, Tinit, Tr_init, T_boundary
         if step_count % output_freq == 0 or (final_time - t) < time_tol:
             info["cumulative_energy_residual"] = cumulative_residual
             info["net_boundary_energy"] = info["boundary_emission"] - info["boundary_outgoing"]
+            for k in ("radiation_energy_by_group", "radiation_energy_by_group_postcomb", "temperature",
+                      "radiation_temperature"):
+                info[k] = np.array(info[k])  # a kept record holds ordinary memory, not a pinned step buffer
             history.append(info)
     return history, state
 

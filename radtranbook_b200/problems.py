@@ -22,7 +22,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from .materials import Constant, GroupedOpacity, LinearEOS, PowerLawOpacity, device_callable
+from .materials import Constant, GroupedOpacity, GroupPowerLawOpacity, LinearEOS, PowerLawOpacity, device_callable
 
 
 def marshak_slab(scale: float = 1.0) -> dict:
@@ -143,16 +143,12 @@ def mg_crooked_pipe(n_groups: int = 10, nr: int = 60, nz: int = 210, mode: str =
         return host, device
 
     ops = [opacity(g) for g in range(n_groups)]
-    inv3 = [(float(edges[g]) ** -3, float(edges[g + 1]) ** -3) for g in range(n_groups)]
-
-    def all_groups(T):  # every group in one expression, the same arithmetic as each callable
-        key = ("inv3", T.device)
-        if key not in cache:
-            t = torch.tensor(inv3, dtype=torch.float64, device=T.device)
-            cache[key] = (t[:, 0].view(-1, 1, 1).contiguous(), t[:, 1].view(-1, 1, 1).contiguous())
-        lo3, hi3 = cache[key]
-        s = 10.0 * dev(rho, T) * torch.pow(torch.clamp(T, min=1e-2), -0.5)
-        return torch.sqrt(torch.clamp(s * lo3, max=1e14) * torch.clamp(s * hi3, max=1e14))
+    # On the device: 10 rho max(T, 0.01)^-1/2 (E_g E_g+1)^-3/2, the same function as the
+    # geometric mean above wherever the 1e14 cap does not bind, which is everywhere on this
+    # problem (10 rho max(T, 0.01)^-1/2 E^-3 <= 10 * 2 * 10 * 0.01^-3 = 2e8); a material law
+    # the multigroup step evaluates in its material update kernel.
+    sigma_dev = GroupPowerLawOpacity(10.0, 0.5, (edges[:-1] * edges[1:]) ** -1.5, scale=rho, T_floor=1e-2)
+    eos = LinearEOS(cvg)
     presets = {"quick": (20_000, 20_000, 100_000, 10_000, 500_000),
                "standard": (200_000, 200_000, 1_000_000, 50_000, 5_000_000)}
     nt, nb, nmax, ngrow, nfin = presets[mode]
@@ -164,10 +160,10 @@ def mg_crooked_pipe(n_groups: int = 10, nr: int = 60, nz: int = 210, mode: str =
         name=f"2-D RZ multigroup crooked pipe ({nr}x{nz}, {n_groups} groups)",
         geometry="rz", dim=2, edges1=r_edges, edges2=z_edges, energy_edges=edges, rho=rho,
         Tinit=np.full((nr, nz), 0.05), Tr_init=np.full((nr, nz), 0.05),
-        sigma_host=[h for h, _ in ops], sigma_dev=GroupedOpacity([d for _, d in ops], all_groups),
-        cv_host=lambda T: cvg.copy(), cv_dev=device_callable(lambda T: dev(cvg, T)),
+        sigma_host=[h for h, _ in ops], sigma_dev=sigma_dev, sigma_dev_callables=[d for _, d in ops],
+        cv_host=lambda T: cvg.copy(), cv_dev=eos.cv,
         eos_host=lambda T: cvg * T, inv_eos_host=lambda e: e / cvg,
-        eos_dev=device_callable(lambda T: dev(cvg, T) * T), inv_eos_dev=device_callable(lambda e: e / dev(cvg, e)),
+        eos_dev=eos.eos, inv_eos_dev=eos.inv_eos,
         Ntarget=nt, Nboundary=nb, Nsource=0, Nmax=nmax, Nmax_growth=ngrow, Nmax_final=nfin,
         T_boundary=(0.0, 0.0, 0.0, 0.0), reflect=(True, False, False, False), boundary_source_func=bsf,
         T_emit_floor=0.075, dt_initial=1e-4, dt_max=0.01, dt_growth=1.1, source=np.zeros((nr, nz)),
@@ -201,21 +197,20 @@ def marshak_mg(scale: float = 1.0) -> dict:
         return host, dev
 
     ops = [one(g) for g in range(10)]
-    kt = {}
-
-    def all_groups(T):  # every group in one expression, the same arithmetic as each callable
-        if T.device not in kt:
-            kt[T.device] = torch.tensor(10.0 * nu ** -3, dtype=torch.float64, device=T.device).view(-1, 1, 1)
-        return torch.clamp(kt[T.device] * torch.pow(T, -0.5), min=1e-2, max=1e6)
+    # on the device as a material law the multigroup step evaluates in its material update
+    # kernel: clamp(10 T^-1/2 nu_g^-3, 1e-2, 1e6), the host callables' function (the products
+    # in another order, so equal to rounding)
+    sigma_dev = GroupPowerLawOpacity(10.0, 0.5, nu ** -3, lo=1e-2, hi=1e6)
+    eos = LinearEOS(cv_val)
 
     return dict(
         name="multigroup Marshak wave (200 cells, 10 groups) on the 2-D multigroup step",
         geometry="xy", dim=2, edges1=e1, edges2=e2, energy_edges=edges,
         Tinit=np.full((nx, 1), 0.001), Tr_init=np.full((nx, 1), 0.001),
-        sigma_host=[h for h, _ in ops], sigma_dev=GroupedOpacity([d for _, d in ops], all_groups),
-        cv_host=lambda T: np.full_like(T, cv_val), cv_dev=device_callable(lambda T: torch.full_like(T, cv_val)),
+        sigma_host=[h for h, _ in ops], sigma_dev=sigma_dev, sigma_dev_callables=[d for _, d in ops],
+        cv_host=lambda T: np.full_like(T, cv_val), cv_dev=eos.cv,
         eos_host=lambda T: cv_val * T, inv_eos_host=lambda e: e / cv_val,
-        eos_dev=device_callable(lambda T: cv_val * T), inv_eos_dev=device_callable(lambda e: e / cv_val),
+        eos_dev=eos.eos, inv_eos_dev=eos.inv_eos,
         Ntarget=int(666667 * scale), Nboundary=int(333333 * scale), Nsource=0, Nmax=int(1330000 * scale),
         T_boundary=(1.0, 0.0, 0.0, 0.0), reflect=(False, False, True, True), dt=0.005, n_steps=200,
         source=np.zeros((nx, 1)),

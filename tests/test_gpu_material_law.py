@@ -8,13 +8,19 @@ the radiation temperature, T = e / cv and the next step's opacity in one kernel.
     event counts (exactly) over four steps, and both ledgers close to 1e-12;
   - the power law: after a slab step the opacity the kernel evaluated for the next step
     equals the law evaluated by torch on the new temperature (relative 1e-14), and setting
-    the temperature by hand discards it.
+    the temperature by hand discards it;
+  - the multigroup law (GroupPowerLawOpacity, the multigroup crooked pipe): after three
+    mg_imc2d steps the kernel's opacity of every group equals the law evaluated by torch on
+    the new temperature (relative 1e-14; torch takes T^-1/2 as rsqrt, the kernel as pow), its
+    heat capacity is the problem's, and T = e / cv exactly;
+  - the post-comb radiation energy by group that the comb writes per bin (copies x FP32
+    weight) equals the energy of the new census summed entry by entry (relative 1e-12).
 """
 import numpy as np
 import pytest
 import torch
 
-from radtranbook_b200 import imc1d, imc2d, problems
+from radtranbook_b200 import imc1d, imc2d, mg_imc2d, problems
 from radtranbook_b200.materials import device_callable
 
 pytestmark = pytest.mark.gpu
@@ -65,3 +71,43 @@ def test_power_law_next_opacity_is_the_law(cuda):
     st, info = imc1d.step(st, q["Ntarget"], q["Nboundary"], 0, q["Nmax"], q["T_boundary"], q["dt"], q["mesh"],
                           q["sigma_dev"], q["inv_eos_dev"], q["cv_dev"], q["source"])
     assert info["profiling"]["transport_events"]["total"] > 0
+
+
+def _mg_pipe_steps(p, steps):
+    e1, e2, ge = p["edges1"], p["edges2"], p["energy_edges"]
+    st = mg_imc2d.init_simulation(p["Ntarget"], p["Tinit"], p["Tr_init"], e1, e2, ge, p["eos_dev"],
+                                  p["inv_eos_dev"], T_emit_floor=p["T_emit_floor"], geometry="rz", seed=0x6A7)
+    dt, infos = p["dt_initial"], []
+    for k in range(steps):
+        st, info = mg_imc2d.step(st, p["Ntarget"], p["Nboundary"], 0, p["Nmax"] + k * p["Nmax_growth"],
+                                 p["T_boundary"], dt, e1, e2, ge, p["sigma_dev"], p["inv_eos_dev"], p["cv_dev"],
+                                 p["source"], reflect=p["reflect"], geometry="rz",
+                                 boundary_source_func=p["boundary_source_func"], T_emit_floor=p["T_emit_floor"],
+                                 Nmax_growth=p["Nmax_growth"], Nmax_final=p["Nmax_final"])
+        assert abs(info["ledger"]["relative_closure"]) < 1e-12
+        infos.append(info)
+        dt = min(dt * p["dt_growth"], p["dt_max"])
+    return st, infos
+
+
+def test_group_power_law_next_opacity_is_the_law(cuda):
+    p = problems.mg_crooked_pipe(nr=30, nz=105, mode="quick")
+    st, _ = _mg_pipe_steps(p, 3)
+    key, sig_next, cv_next = st.__dict__["_law_next"]
+    like = st.grid(st._T)
+    want = p["sigma_dev"].all_groups(like).transpose(1, 2).reshape(-1)  # (G, nx, ny) -> [g][c] cell order
+    torch.testing.assert_close(sig_next, want, rtol=1e-14, atol=0)
+    cvg = st.flat(torch.as_tensor(p["cv_host"](p["Tinit"]), device=cuda))
+    torch.testing.assert_close(cv_next, cvg, rtol=0, atol=0)
+    torch.testing.assert_close(st._T, st._e / cvg, rtol=0, atol=0)
+    assert float(st._T.max()) > 0.05  # heated near the source: the opacities changed
+
+
+def test_comb_after_energy_is_the_new_census(cuda):
+    p = problems.mg_crooked_pipe(nr=30, nz=105, mode="quick")
+    st, infos = _mg_pipe_steps(p, 2)
+    G, nx, ny = 10, 30, 105
+    census = mg_imc2d._rad_by_group(st._engine).view(G, ny, nx).transpose(1, 2).cpu().numpy()
+    post = infos[-1]["radiation_energy_by_group_postcomb"]
+    assert post.shape == (G, nx, ny) and post.sum() > 0
+    np.testing.assert_allclose(post, census, rtol=1e-12, atol=1e-300)

@@ -210,6 +210,32 @@ def test_mg1d_dropin_budget_and_threshold(cuda):
     assert 0 < info["N_particles"] <= info["profiling"]["transport_events"]["n_particles_transported"]
 
 
+def test_threshold_comb_reads_the_tracking_live_count(cuda):
+    """A threshold comb (Nmax < 0) decides from the live count the tracking leaves in the
+    workspace; tracking and comb lay the workspace out for different bank sizes, so that count
+    (like the census sums) must sit at an offset independent of them.  With every workspace
+    byte set to 0xFF before each step, a threshold far above the census still only drops dead
+    entries, step after step."""
+    from radtranbook_b200 import mg_imc1d
+
+    e = np.linspace(0.2, 1.0, 21)
+    mesh = np.stack([e[:-1], e[1:]], axis=1)
+    edges = np.logspace(-2, np.log10(20.0), 4)
+    cv = 0.2
+    funcs = [lambda T: np.full_like(T, 3.0)] * 3
+    st = mg_imc1d.init_simulation(2000, np.full(20, 0.1), np.full(20, 0.1), mesh, edges, lambda T: cv * T,
+                                  lambda u: u / cv)
+    args = (6000, 0, 0, -10**8, (0.5, 1.0), 0.01, mesh, edges, funcs, lambda u: u / cv, lambda T: cv + 0 * T,
+            np.zeros(20))
+    st, info = mg_imc1d.step(st, *args)  # sizes the workspace
+    for _ in range(3):
+        st._engine.ws.fill_(0xFF)
+        st, info = mg_imc1d.step(st, *args)
+        assert info["ledger"]["comb_discrepancy"] == 0.0
+        assert 0 < info["N_particles"] <= info["profiling"]["transport_events"]["n_particles_transported"]
+        assert abs(info["ledger"]["relative_closure"]) < 1e-12
+
+
 def test_mg1d_dropin_matches_reference_statistically(cuda):
     from radtranbook_b200 import mg_imc1d
     from tests.stat_problems import compare_means
