@@ -41,10 +41,13 @@ UNIT = "track-segments/s"
 B_SEG_2D = 72  # bytes per 2-D gray segment: 36-byte record loaded + stored
 B_SEG_2D_MG = 80  # 2-D multigroup: the 36-byte record plus the group index, loaded + stored
 B_SEG_1D = 56  # 1-D gray: a 28-byte record loaded + stored
-# DRAM bytes the tracking kernel actually moves per segment on this workload: ncu
-# dram__bytes_read.sum + dram__bytes_write.sum of one full-size launch (401.4 MB for
-# 66.79 M segments); the histories stay in registers across their events.
-DRAM_B_PER_SEG_MEASURED = 401.441024e6 / 66791775
+# DRAM bytes and warp instructions of the tracking kernel per segment on this workload, from
+# one full-size launch under ncu (dram__bytes_read.sum + dram__bytes_write.sum = 402.25 MB,
+# smsp__inst_executed.sum = 1.520 G, for 67.18 M segments); the histories stay in registers
+# across their events, and the kernel is bound by instruction issue.
+DRAM_B_PER_SEG_MEASURED = 402.252544e6 / 67176386
+WARP_INST_PER_SEG_MEASURED = 1520147524 / 67176386
+ISSUE_SLOTS_PER_CYCLE = 148 * 4  # SMs x warp schedulers, one warp instruction each per cycle
 
 
 def measured_peaks():
@@ -635,6 +638,48 @@ def form_other_configs(steps: int = 20, warmup: int = 5, tune: bool = True) -> d
     return out
 
 
+def form_slab_event_cap(steps: int = 15) -> dict:
+    """How the slab tracking kernel's time depends on its longest histories: after `steps`
+    drop-in steps of the slab Marshak wave, the transport of the next step (the state's census,
+    the law's opacity at the current temperature, the last step's sources) is replayed from the
+    same census with an events-per-history cap K (the reference's max_events_per_particle);
+    each replay reports the tracking time, the events and the histories the cap stopped (those
+    longer than K events)."""
+    import torch
+
+    from radtranbook_b200 import imc1d, problems
+    from radtranbook_b200._lib import STAT_CAP, STAT_EVENTS, ImcStepSummary
+    from radtranbook_b200.autotune import _restore, _snapshot
+
+    p = problems.marshak_slab()
+    st = imc1d.init_simulation(p["Ntarget"], p["Tinit"], p["Tr_init"], p["mesh"], p["eos_dev"], p["inv_eos_dev"],
+                               seed=0xC0F1)
+    for _ in range(steps):
+        st, _ = imc1d.step(st, p["Ntarget"], p["Nboundary"], 0, p["Nmax"], p["T_boundary"], p["dt"], p["mesh"],
+                           p["sigma_dev"], p["inv_eos_dev"], p["cv_dev"], p["source"])
+    eng = st._engine
+    args, kw = eng._last_transport
+    _, sig, cvv = st.__dict__["_law_next"]
+    args = (st._T, sig, cvv) + tuple(args[3:])
+    snap = _snapshot(eng.bank)
+    rows = []
+    for K in (0, 500, 400, 300, 200, 100):
+        best = float("inf")
+        for _ in range(3):
+            _restore(eng.bank, snap)
+            eng._census_dev_valid = False
+            eng.transport_async(*args, **dict(kw, max_events=K))
+            torch.cuda.synchronize()
+            best = min(best, eng.phase_times()[1])
+        sm = ImcStepSummary.from_buffer_copy(eng.summary_dev.cpu().numpy().tobytes())
+        rows.append({"cap": K, "track_ms": best, "events": int(sm.stats[STAT_EVENTS]),
+                     "histories_capped": int(sm.stats[STAT_CAP])})
+    _restore(eng.bank, snap)
+    eng._census_dev_valid = False
+    return {"workload": "slab_marshak_100_cells, transport of step %d replayed" % (steps + 1),
+            "census_entries": int(snap["_n"]), "launch": dict(eng.launch), "caps": rows}
+
+
 def form_mg_crooked_pipe_run(output_times=(1.0, 5.0, 10.0)) -> dict:
     """The multigroup crooked pipe driven by driver.mg_crooked_pipe_run to the last output time
     ('standard' preset, adaptive dt from 1e-4 ns by 1.1 to 0.01 ns, Nmax growing to 5e6):
@@ -769,10 +814,28 @@ def run_ours(args, rank: int, world: int):
     achieved = B_SEG_2D * seg_per_launch / t_launch / 1e9
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": DRAM_B_PER_SEG_MEASURED * seg_per_launch, "kernel": "k_track<RZ>", "peak_source": peak_kind,
-            "traffic_source": "ncu dram bytes of one full-size k_track launch (6.01 B/segment), scaled to the "
-                              "segments per launch of this run",
+            "traffic_source": "ncu dram bytes of one full-size k_track launch (%.2f B/segment), scaled to the "
+                              "segments per launch of this run" % DRAM_B_PER_SEG_MEASURED,
             "segments_per_launch": seg_per_launch, "bytes_per_segment_algorithmic": B_SEG_2D,
             "track_ms_per_launch": t_launch * 1e3}
+    # the bound the kernel actually meets: warp-instruction issue (4 schedulers per SM, one
+    # instruction per cycle each, at the SM clock sampled during the timed region)
+    csum = clocks.summary() or {}
+    mhz, clock_src = csum.get("sm_mhz"), "SM clock sampled in the timed region"
+    if not mhz:  # a timed region shorter than the sampling interval: the pool's maximum SM clock
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+                mhz, clock_src = float(json.load(f)["sm_max_mhz"]), "sm_max_mhz of MEASURED_PEAKS.json (no sample in the timed region)"
+        except (OSError, KeyError, ValueError):
+            mhz = None
+    if mhz:
+        ach = WARP_INST_PER_SEG_MEASURED * seg_per_launch / t_launch / 1e9
+        pk = ISSUE_SLOTS_PER_CYCLE * mhz * 1e6 / 1e9
+        roof["issue"] = {"bound": "issue", "achieved": ach, "peak": pk, "unit": "G warp-instructions/s", "frac": ach / pk,
+                         "warp_instructions_per_segment": WARP_INST_PER_SEG_MEASURED,
+                         "source": "ncu smsp__inst_executed.sum of one full-size k_track launch over its segments; "
+                                   "peak = 148 SMs x 4 schedulers x the SM clock", "clock_mhz": mhz,
+                         "clock_source": clock_src}
     cpu = None
     if not args.no_cpu_baseline:
         v, h, dtc, _ = cpu_oracle_run(args.cpu_scale, args.cpu_steps, 1, os.cpu_count() or 1)
@@ -836,7 +899,7 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="skip the batched and adjoint forms")
     ap.add_argument("--only-form", default=None,
                     choices=["batched", "adjoint", "carter_forest", "device_loop", "mg_crooked_pipe",
-                             "mg_crooked_pipe_run", "other_configs", "event_based"],
+                             "mg_crooked_pipe_run", "other_configs", "event_based", "slab_event_cap"],
                     help="run one further form alone on GPU 0 and print its JSON (no headline line)")
     ap.add_argument("--batch-steps", type=int, default=50, help="steps of the batched form (the workload's 50)")
     ap.add_argument("--no-fom", action="store_true")
@@ -858,7 +921,7 @@ def main():
               "carter_forest": form_carter_forest, "device_loop": form_device_loop,
               "mg_crooked_pipe": form_mg_crooked_pipe, "mg_crooked_pipe_run": form_mg_crooked_pipe_run,
               "other_configs": lambda: form_other_configs(tune=not args.no_tune),
-              "event_based": form_event_based}[args.only_form]
+              "event_based": form_event_based, "slab_event_cap": form_slab_event_cap}[args.only_form]
         print(json.dumps({"form": args.only_form, **fn()}), flush=True)
         return
     if world > 1:

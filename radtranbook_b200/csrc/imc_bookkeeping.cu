@@ -134,6 +134,41 @@ __global__ void k_plan_cells(PlanArgs a) {
   }
 }
 
+// Boundary-face source energies of one side, E_q = a c T_q^4 / 4 * area_q * dt * share, all
+// faces in parallel over the block; block_face_cdf then forms the side's cumulative sums.
+__device__ void block_face_energy(int geom, bool oned, int side, int nf, const double* Tf, const double* e1,
+                                  const double* e2, int nx, double dt, double share, double* Ef) {
+  const bool along2 = side < 2;
+  for (int q = threadIdx.x; q < nf; q += blockDim.x) {
+    double area;
+    if (oned) {
+      if (geom == G_SLAB) area = 1.0;
+      else { const double R = side == 0 ? e1[0] : e1[nx]; area = 4.0 * PI * R * R; }
+    } else if (geom == G_XY) {
+      area = along2 ? (e2[q + 1] - e2[q]) : (e1[q + 1] - e1[q]);
+    } else {
+      if (along2) { const double R = side == 0 ? e1[0] : e1[nx]; area = 2.0 * PI * R * (e2[q + 1] - e2[q]); }
+      else area = PI * (e1[q + 1] * e1[q + 1] - e1[q] * e1[q]);
+    }
+    const double T = Tf[q];
+    Ef[q] = (T > 0.0) ? A_RAD * C_LIGHT * T * T * T * T / 4.0 * area * dt * share : 0.0;
+  }
+}
+
+// one thread: cdf[q] = E_0 + ... + E_q in face order; returns the side's total
+__device__ double face_cdf_serial(const double* Ef, double* cdf, int nf) {
+  constexpr int B = 16;
+  double Et = 0.0;
+  for (int q0 = 0; q0 < nf; q0 += B) {
+    double v[B];
+#pragma unroll
+    for (int j = 0; j < B; ++j) v[j] = q0 + j < nf ? Ef[q0 + j] : 0.0;
+#pragma unroll
+    for (int j = 0; j < B; ++j) if (q0 + j < nf) { Et += v[j]; cdf[q0 + j] = Et; }
+  }
+  return Et;
+}
+
 __global__ void __launch_bounds__(NT) k_plan(PlanArgs a) {
   const double dt = a.dt_dev ? *a.dt_dev : a.dt;  // device-resident step length (graph replay)
   __shared__ double red[NT];
@@ -171,7 +206,14 @@ __global__ void __launch_bounds__(NT) k_plan(PlanArgs a) {
     }
   }
 
-  // ---- boundary faces (one thread per side, sequential cumulative sums) ----
+  // ---- boundary faces: energies in parallel, then one thread per side forms the side's
+  // cumulative sums in face order ----
+  for (int side = 0; side < 4; ++side) {
+    if (a.face_T[side] && a.n_side[side] > 0 && !(oned && side >= 2))
+      block_face_energy(a.geom, oned, side, oned ? 1 : (side < 2 ? a.ny : a.nx), a.face_T[side], a.e1, a.e2, a.nx,
+                        dt, a.share, a.face + (size_t)(side * 2 + 0) * a.nf);
+  }
+  __syncthreads();
   if (t < 4) {
     const int side = t;
     a.sum->n_side[side] = 0;
@@ -179,27 +221,9 @@ __global__ void __launch_bounds__(NT) k_plan(PlanArgs a) {
     const double* Tf = a.face_T[side];
     const long long nbs = a.n_side[side];
     if (Tf && nbs > 0 && !(oned && side >= 2)) {
-      const bool along2 = side < 2;
-      const int nf = oned ? 1 : (along2 ? a.ny : a.nx);
-      double* Ef = a.face + (size_t)(side * 2 + 0) * a.nf;
-      double* cdf = a.face + (size_t)(side * 2 + 1) * a.nf;
-      double Et = 0.0;
-      for (int q = 0; q < nf; ++q) {
-        double area;
-        if (oned) {
-          if (a.geom == G_SLAB) area = 1.0;
-          else { const double R = side == 0 ? a.e1[0] : a.e1[a.nx]; area = 4.0 * PI * R * R; }
-        } else if (a.geom == G_XY) {
-          area = along2 ? (a.e2[q + 1] - a.e2[q]) : (a.e1[q + 1] - a.e1[q]);
-        } else {
-          if (along2) { const double R = side == 0 ? a.e1[0] : a.e1[a.nx]; area = 2.0 * PI * R * (a.e2[q + 1] - a.e2[q]); }
-          else area = PI * (a.e1[q + 1] * a.e1[q + 1] - a.e1[q] * a.e1[q]);
-        }
-        const double T = Tf[q];
-        Ef[q] = (T > 0.0) ? A_RAD * C_LIGHT * T * T * T * T / 4.0 * area * dt * a.share : 0.0;
-        Et += Ef[q];
-        cdf[q] = Et;
-      }
+      const int nf = oned ? 1 : (side < 2 ? a.ny : a.nx);
+      const double Et = face_cdf_serial(a.face + (size_t)(side * 2 + 0) * a.nf,
+                                        a.face + (size_t)(side * 2 + 1) * a.nf, nf);
       if (Et > 0.0) {
         a.sum->n_side[side] = nbs;
         const float wq = (float)(Et / (double)nbs);
@@ -387,11 +411,21 @@ namespace {
 // Planck fraction F(x) = (15/pi^4) int_0^x t^3/(e^t-1) dt: Bernoulli series below x = 1,
 // exponential series above (Widger & Woodall 1976).  Same expansion as the oracle.
 // sum_k e^{-kx}(x^3/k + 3x^2/k^2 + 6x/k^3 + 6/k^4) = (pi^4/15)(1 - F(x)), for x >= 1
+// 1/k for the tail's terms, k < 64 (K = 2 + 40/x <= 42 for x >= 1): the correctly rounded
+// quotients, so each term is the one the division gives
+struct InvK { double v[64]; };
+constexpr InvK inv_k_table() {
+  InvK t{};
+  for (int k = 1; k < 64; ++k) t.v[k] = 1.0 / (double)k;
+  return t;
+}
+__device__ const InvK g_inv_k = inv_k_table();
+
 __device__ double planck_tail(double x) {
   double tail = 0.0;
   const int K = (int)(2.0 + 40.0 / x);
   for (int k = K; k >= 1; --k) {
-    const double kx = k * x, ik = 1.0 / k;
+    const double kx = k * x, ik = k < 64 ? g_inv_k.v[k] : 1.0 / k;
     tail += exp(-kx) * ik * (x * x * x + ik * (3.0 * x * x + ik * (6.0 * x + ik * 6.0)));
   }
   return tail;
@@ -435,7 +469,12 @@ __device__ double planck_frac(const PlanckEdge& e0, const PlanckEdge& e1) {
 }
 
 // canonical inclusive prefix sum of n values (the oracle's canon_prefix order)
+// The sequential parts load their operands a batch at a time into registers before the
+// dependent adds, so each add waits for the previous add only, not for a load issued after
+// the previous store (the compiler cannot reorder those: out may alias x); the adds and
+// their order are unchanged.
 __device__ void block_canon_prefix(const double* x, int n, double* out, double* sh) {
+  constexpr int B = 16;
   const int t = threadIdx.x;
   const int per = (n + NT - 1) / NT;
   const int lo = min(t * per, n), hi = min(lo + per, n);
@@ -445,11 +484,23 @@ __device__ void block_canon_prefix(const double* x, int n, double* out, double* 
   __syncthreads();
   if (t == 0) {
     double off = 0.0;
-    for (int q = 0; q < NT; ++q) { const double v = sh[q]; sh[q] = off; off += v; }
+    for (int q0 = 0; q0 < NT; q0 += 32) {
+      double v[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) v[j] = sh[q0 + j];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) { sh[q0 + j] = off; off += v[j]; }
+    }
   }
   __syncthreads();
   double run = sh[t];
-  for (int i = lo; i < hi; ++i) { run += x[i]; out[i] = run; }
+  for (int i0 = lo; i0 < hi; i0 += B) {
+    double v[B];
+#pragma unroll
+    for (int j = 0; j < B; ++j) v[j] = i0 + j < hi ? x[i0 + j] : 0.0;
+#pragma unroll
+    for (int j = 0; j < B; ++j) if (i0 + j < hi) { run += v[j]; out[i0 + j] = run; }
+  }
   __syncthreads();
 }
 
@@ -583,7 +634,13 @@ __global__ void __launch_bounds__(NT) k_plan_mg(PlanMgArgs a) {
     }
   }
 
-  // ---- boundary faces (as gray) ----
+  // ---- boundary faces (as gray: energies in parallel, cumulative sums per side) ----
+  for (int side = 0; side < 4; ++side) {
+    if (a.face_T[side] && a.n_side[side] > 0)
+      block_face_energy(a.geom, false, side, side < 2 ? a.ny : a.nx, a.face_T[side], a.e1, a.e2, a.nx, dt, a.share,
+                        a.face + (size_t)(side * 2 + 0) * a.nf);
+  }
+  __syncthreads();
   if (t < 4) {
     const int side = t;
     a.sum->n_side[side] = 0;
@@ -591,21 +648,9 @@ __global__ void __launch_bounds__(NT) k_plan_mg(PlanMgArgs a) {
     const double* Tf = a.face_T[side];
     const long long nbs = a.n_side[side];
     if (Tf && nbs > 0) {
-      const bool along2 = side < 2;
-      const int nf = along2 ? a.ny : a.nx;
-      double* Ef = a.face + (size_t)(side * 2 + 0) * a.nf;
-      double* cdf = a.face + (size_t)(side * 2 + 1) * a.nf;
-      double Et = 0.0;
-      for (int q = 0; q < nf; ++q) {
-        double area;
-        if (a.geom == G_XY) area = along2 ? (a.e2[q + 1] - a.e2[q]) : (a.e1[q + 1] - a.e1[q]);
-        else if (along2) { const double R = side == 0 ? a.e1[0] : a.e1[a.nx]; area = 2.0 * PI * R * (a.e2[q + 1] - a.e2[q]); }
-        else area = PI * (a.e1[q + 1] * a.e1[q + 1] - a.e1[q] * a.e1[q]);
-        const double T = Tf[q];
-        Ef[q] = (T > 0.0) ? A_RAD * C_LIGHT * T * T * T * T / 4.0 * area * dt * a.share : 0.0;
-        Et += Ef[q];
-        cdf[q] = Et;
-      }
+      const int nf = side < 2 ? a.ny : a.nx;
+      const double Et = face_cdf_serial(a.face + (size_t)(side * 2 + 0) * a.nf,
+                                        a.face + (size_t)(side * 2 + 1) * a.nf, nf);
       if (Et > 0.0) {
         a.sum->n_side[side] = nbs;
         a.sum->e_side[side] = (double)nbs * (double)(float)(Et / (double)nbs);
@@ -786,12 +831,13 @@ __global__ void __launch_bounds__(NT) k_ic_plan_mg(IcMgArgs a) {
 
 }  // namespace
 
-// Launch shape of the per-cell multigroup plan: up to 32 cells a block, two doubles per
-// (cell, group edge) of shared memory; above 48 KB the kernel is opted in to more.
+// Launch shape of the per-cell multigroup plan: as many cells a block as leave one
+// (cell, group edge) pair per thread (the edge integrals are the long part; at most 32 cells),
+// two doubles per pair of shared memory; above 48 KB the kernel is opted in to more.
 template <typename K>
 cudaError_t launch_plan_cells(K kernel, const PlanMgArgs& a, cudaStream_t s) {
   const long long E = (long long)a.ng + 1;
-  const int cb = (int)std::max(1LL, std::min(32LL, 3072LL / E));
+  const int cb = (int)std::max(1LL, std::min(32LL, 256LL / E));
   const size_t smem = (size_t)2 * cb * E * sizeof(double);
   if (smem > 48 * 1024) {
     const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -256,6 +256,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     ba.face = pa.face + (size_t)side * 2 * pa.nf;
     ba.d_n = &sum->n_side[side]; ba.d_base = &sum->base_side[side]; ba.n_bound = side_count(par, side);
     ba.dt = par->dt; ba.seed = par->seed; ba.step = par->step;
+    imcdev::philox_round_keys(ba.seed, ba.rk);
     ba.p1 = bank->pos1; ba.p2 = p2; ba.d1 = bank->dir1; ba.d2 = d2; ba.wb = bank->weight;
     ba.t = bank->time; ba.cell = bank->cell; ba.group = bank->group;
     ba.ng = ng; ba.faceT = par->face_T[side]; ba.gedges = mesh->group_edges;
@@ -278,6 +279,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     fa.d_n = d_n; fa.d_base = d_base; fa.n_bound = n_bound;
     fa.off = off; fa.w = w; fa.tilt = tilt; fa.tilt_kind = kind;
     fa.time_scale = par->dt; fa.seed = par->seed; fa.step = par->step; fa.tag = tag;
+    imcdev::philox_round_keys(fa.seed, fa.rk);
     fa.p1 = bank->pos1; fa.p2 = p2; fa.d1 = bank->dir1; fa.d2 = d2; fa.wb = bank->weight;
     fa.t = bank->time; fa.cell = bank->cell; fa.group = bank->group;
     if (cf_times) {
@@ -294,6 +296,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     fm.gedges = mesh->group_edges; fm.mixcdf = ws_ptr<double>(workspace, L.mixcdf);
     fm.d_n = d_n; fm.d_base = d_base; fm.n_bound = n_bound;
     fm.time_scale = par->dt; fm.seed = par->seed; fm.step = par->step; fm.tag = tag;
+    imcdev::philox_round_keys(fm.seed, fm.rk);
     fm.p1 = bank->pos1; fm.p2 = p2; fm.d1 = bank->dir1; fm.d2 = d2; fm.wb = bank->weight;
     fm.t = bank->time; fm.cell = bank->cell; fm.group = bank->group;
     fm.time_scale_dev = par->dt_dev; fm.step_dev = par->step_dev;
@@ -594,6 +597,7 @@ imc_status imc_init_census(const imc_mesh* mesh, const double* tr, int64_t n_tar
     fm.gedges = mesh->group_edges; fm.mixcdf = im.mixcdf;
     fm.d_n = &sum->n_emission; fm.d_base = &sum->base_emission; fm.n_bound = n_target;
     fm.time_scale = 0.0; fm.seed = seed; fm.step = 0; fm.tag = imcdev::TAG_IC;
+    imcdev::philox_round_keys(fm.seed, fm.rk);
     fm.p1 = bank->pos1; fm.p2 = bank->pos2; fm.d1 = bank->dir1; fm.d2 = bank->dir2; fm.wb = bank->weight;
     fm.t = bank->time; fm.cell = bank->cell; fm.group = bank->group;
     IMC_CUDA(imc_launch_fill_mg(fm, s));
@@ -629,6 +633,7 @@ imc_status imc_init_census(const imc_mesh* mesh, const double* tr, int64_t n_tar
   fa.d_n = &sum->n_emission; fa.d_base = &sum->base_emission; fa.n_bound = bound;
   fa.off = ia.off; fa.w = ia.w; fa.tilt = nullptr; fa.tilt_kind = 0;
   fa.time_scale = 0.0; fa.seed = seed; fa.step = 0; fa.tag = imcdev::TAG_IC;
+  imcdev::philox_round_keys(fa.seed, fa.rk);
   fa.nbins = nc; fa.bins_by_group = 0;
   if (mg1) {
     fa.tr = tr; fa.gedges = mesh->group_edges; fa.mixcdf = ws_ptr<double>(workspace, L.mixcdf);

@@ -199,6 +199,7 @@ cudaError_t imc_launch_canon_sum_eV(const double* e, const double* vol, int nc, 
 // Source fill kernels (element count and first bank index read from device memory)
 // ---------------------------------------------------------------------------------
 struct FillArgs {
+  uint32_t rk[20];             // Philox round keys of seed (philox_round_keys)
   int geom, nx, ny, nc;
   const double* e1; const double* e2;
   const double* T;
@@ -225,6 +226,7 @@ struct FillArgs {
 cudaError_t imc_launch_fill_volume(const FillArgs& a, cudaStream_t s);
 
 struct BndArgs {
+  uint32_t rk[20];             // Philox round keys of seed (philox_round_keys)
   int geom, nx, ny, side, nf;
   const double* e1; const double* e2;
   const double* face;          // [2][nf]: energies, cumulative (total = last)
@@ -317,6 +319,7 @@ cudaError_t imc_launch_ic_plan_mg(const IcMgArgs& a, cudaStream_t s);
 // categorical (cell ~ total, group ~ per-cell cumulative) multigroup source fill; the IC
 // variant samples the group from the Planck spectrum at tr[c] instead
 struct FillMgArgs {
+  uint32_t rk[20];             // Philox round keys of seed (philox_round_keys)
   int geom, nx, ny, nc, ng;
   const double* e1; const double* e2;
   const double* cdf;           // [c] canonical inclusive prefix of cell totals

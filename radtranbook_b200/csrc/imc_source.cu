@@ -50,8 +50,8 @@ __global__ void k_fill_volume(FillArgs a) {
     const int oc = o - g * a.nc;
     const int i = oc / a.ny, j = oc - i * a.ny;
     const int c = i + a.nx * j;
-    const U4 r = draw(a.seed, (uint32_t)k + a.id_base, 0, step, a.tag);
-    const U4 s = draw(a.seed, (uint32_t)k + a.id_base, 1, step, a.tag);
+    const U4 r = draw_rk(a.rk, (uint32_t)k + a.id_base, 0, step, a.tag);
+    const U4 s = draw_rk(a.rk, (uint32_t)k + a.id_base, 1, step, a.tag);
     const double u0 = u01d(r.x), u1 = u01d(r.y), u2 = u01d(r.z), u3 = u01d(r.w);
     const double s0 = u01d(s.x), s1 = u01d(s.y);
     const double ea = a.e1[i], eb = a.e1[i + 1];
@@ -106,7 +106,7 @@ __global__ void k_fill_volume(FillArgs a) {
     if (a.group) {
       int gb = g;
       if (a.tr) {  // MG 1-D initial census: Planck group at the cell's Tr (MG_IMC/MG_IMC1D.py:557-560)
-        const U4 d = draw(a.seed, (uint32_t)k + a.id_base, 2, step, a.tag);
+        const U4 d = draw_rk(a.rk, (uint32_t)k + a.id_base, 2, step, a.tag);
         gb = planck_group(a.tr[c], a.gedges, a.ng, a.mixcdf, s1, u01d(s.z), u01d(s.w), u01d(d.x), u01d(d.y), true);
       }
       a.group[b] = gb;
@@ -140,8 +140,8 @@ __global__ void k_fill_boundary(BndArgs a) {
   const double total = cdf[nf - 1];
   const float wq = (float)(total / (double)n);
   for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
-    const U4 ra = draw(a.seed, (uint32_t)k + a.id_base, 0, step, TAG_BOUNDARY | (uint32_t)a.side);
-    const U4 rb = draw(a.seed, (uint32_t)k + a.id_base, 1, step, TAG_BOUNDARY | (uint32_t)a.side);
+    const U4 ra = draw_rk(a.rk, (uint32_t)k + a.id_base, 0, step, TAG_BOUNDARY | (uint32_t)a.side);
+    const U4 rb = draw_rk(a.rk, (uint32_t)k + a.id_base, 1, step, TAG_BOUNDARY | (uint32_t)a.side);
     const double ua0 = u01d(ra.x), ua1 = u01d(ra.y), ua2 = u01d(ra.z), ua3 = u01d(ra.w);
     const double x = ua0 * total;
     int lo = 0, hi = nf;  // lower_bound(cdf, x)
@@ -197,7 +197,7 @@ __global__ void k_fill_boundary(BndArgs a) {
     if (a.group) {
       int g = 0;
       if (a.ng > 1) {
-        const U4 rd = draw(a.seed, (uint32_t)k + a.id_base, 2, step, TAG_BOUNDARY | (uint32_t)a.side);
+        const U4 rd = draw_rk(a.rk, (uint32_t)k + a.id_base, 2, step, TAG_BOUNDARY | (uint32_t)a.side);
         g = planck_group(a.faceT[q], a.gedges, a.ng, a.mixcdf, u01d(rb.y), u01d(rb.z), u01d(rb.w), u01d(rd.x),
                          u01d(rd.y), a.below_last != 0);
         if (g < kBndGroups) atomicAdd(&s_gcnt[g], 1u);
@@ -226,8 +226,8 @@ __global__ void k_fill_mg(FillMgArgs a) {
   const float wq = (float)(total / (double)n);
   const bool ic = a.gcdf == nullptr;
   for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
-    const U4 ra = draw(a.seed, (uint32_t)k + a.id_base, 0, step, a.tag);
-    const U4 rb = draw(a.seed, (uint32_t)k + a.id_base, 1, step, a.tag);
+    const U4 ra = draw_rk(a.rk, (uint32_t)k + a.id_base, 0, step, a.tag);
+    const U4 rb = draw_rk(a.rk, (uint32_t)k + a.id_base, 1, step, a.tag);
     const double x = u01d(ra.x) * total;
     int lo = 0, hi = a.nc;  // first c with cdf[c] > x
     while (lo < hi) { const int mid = (lo + hi) >> 1; if (a.cdf[mid] <= x) lo = mid + 1; else hi = mid; }
@@ -243,7 +243,7 @@ __global__ void k_fill_mg(FillMgArgs a) {
       for (int q = 0; q < a.ng; ++q) if (gc[q] >= y) { g = q; break; }
       up1 = u01d(ra.z); up2 = u01d(ra.w); ua = u01d(rb.x); ub = u01d(rb.y); ut = u01d(rb.z);
     } else {
-      const U4 rd = draw(a.seed, (uint32_t)k + a.id_base, 2, step, a.tag);
+      const U4 rd = draw_rk(a.rk, (uint32_t)k + a.id_base, 2, step, a.tag);
       up1 = u01d(ra.y); up2 = u01d(ra.z); ua = u01d(ra.w); ub = u01d(rb.x); ut = 0.0;
       g = planck_group(a.tr[c], a.gedges, a.ng, a.mixcdf, u01d(rb.y), u01d(rb.z), u01d(rb.w), u01d(rd.x), u01d(rd.y));
     }

@@ -287,11 +287,17 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
     else:
         state.__dict__.pop("_law_next", None)
         eng.material_update(state._e, state._Tr)
-    rad_pre = eng.si.view(G, nc) / C_LIGHT  # radiation energy density by group (path length)
-    # the comb also writes the energy after it per (group, cell) bin: the post-comb radiation
-    # energy by group without a pass over the new census
+    # the comb is queued first (the host prepares the by-group fields while it runs); it also
+    # writes the energy after it per (group, cell) bin: the post-comb radiation energy by
+    # group without a pass over the new census
     eng.comb_async(nmax_l, state.count, state._e, per_group=True, write_after=True)
+    rad_pre = eng.si.view(G, nc) / C_LIGHT  # radiation energy density by group (path length)
+    nx, ny = state._shape
     hb = _group_buffers(state, eng)
+
+    def to_grid3(x):  # device (G, nc) in flat cell order -> (G, nx, ny) C order, flattened
+        return x.reshape(G, ny, nx).transpose(1, 2).reshape(-1)
+
     sum_tensors(dist, [eng.comb_after])
     post_dev = eng.comb_after.view(G, nc) / eng.vol.view(1, nc)
     if conserve_comb_energy:
@@ -301,16 +307,11 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
         Tn = evaluate(inv_eos, state.grid(state._e), lambda: _host_copy(state.grid(state._e)), like,
                       **_staged(state, "T_new", nc))
         state._T.copy_(state.flat(Tn))
-    nx, ny = state._shape
-
-    def to_grid3(x):  # device (G, nc) in flat cell order -> (G, nx, ny) C order, flattened
-        return x.reshape(G, ny, nx).transpose(1, 2).reshape(-1)
-
     # the (G, nx, ny) transposes run on the device, so the host only copies contiguous arrays
-    group_copies = [(to_grid3(rad_pre), hb["pre"]), (to_grid3(post_dev), hb["post"]),
-                    (eng.boundary_group, hb["bnd"]), (eng.escaped_group, hb["esc"])]
+    group_copies = state.host_copies() + [(to_grid3(rad_pre), hb["pre"]), (to_grid3(post_dev), hb["post"]),
+                                          (eng.boundary_group, hb["bnd"]), (eng.escaped_group, hb["esc"])]
     try:
-        sm = eng.fetch(state.host_copies() + group_copies)
+        sm = eng.fetch(group_copies)
     except _lib.ImcError as ex:
         if ex.status == 3:
             raise AssertionError("non-finite or non-positive material state") from ex
