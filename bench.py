@@ -24,6 +24,7 @@ step), so the work per GPU is the one-GPU workload's ("scaling": "weak").
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -495,7 +496,10 @@ def form_mg_crooked_pipe(steps: int = 12, warmup: int = 3) -> dict:
     """The multigroup crooked pipe (MG_IMC/problems/crooked_pipe_multigroup_imc.py, 10 groups,
     60 x 210 RZ, 'standard' preset: 200k emission + 200k surface-source particles per step,
     Nmax 1e6 growing by 5e4 per step) through the mg_imc2d drop-in step with device
-    callables, dt from 1e-4 ns growing by 1.1; CUDA-event timing of whole steps.  The same
+    material laws, dt from 1e-4 ns growing by 1.1; CUDA-event timing of whole steps after
+    `warmup` untimed steps, with each step's host wall time (a step takes under 1 ms, so a
+    pause of the host, e.g. Python's cyclic garbage collector, shows as one long step; the
+    collector runs once before the timed steps).  The same
     steps (same dt and Nmax sequence, from the same state) are also run as the device-resident
     loop (one replayed graph, radtranbook_b200.driver.DeviceLoop)."""
     import torch
@@ -530,20 +534,26 @@ def form_mg_crooked_pipe(steps: int = 12, warmup: int = 3) -> dict:
             used.append(state["dt"])
             state["dt"] = min(state["dt"] * p["dt_growth"], p["dt_max"])
             state["k"] += 1
+            walls.append(time.perf_counter())
         return st, seg, hist, worst, info
 
-    track, used = [], []
+    track, used, walls = [], [], []
     st, _, _, _, _ = run(warmup, st)
     track.clear()
     del used[:]
+    del walls[:]
     e0 = torch.cuda.Event(enable_timing=True)
     e1_ = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
+    gc.collect()
     e0.record()
+    t_start = time.perf_counter()
     st, seg, hist, worst, info = run(steps, st)
     e1_.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1_)
+    step_wall_ms = list(np.diff([t_start] + walls) * 1e3)
+    track_ms = float(np.mean(track))  # before the device loop's warm-up steps append to it
     peak, _ = measured_peaks()
     dts = list(used)
     # the same steps as the device-resident loop
@@ -562,7 +572,9 @@ def form_mg_crooked_pipe(steps: int = 12, warmup: int = 3) -> dict:
     return {"workload": "mg_crooked_pipe_rz_60x210_10g_standard", "steps": steps, "warmup": warmup,
             "segments_per_s": seg / (ms * 1e-3), "histories_per_s": hist / (ms * 1e-3), "ms_per_step": ms / steps,
             "segments_per_step": seg / steps, "census_after": int(info["N_particles"]), "time_ns": float(st.time),
-            "transport_ms_per_step": float(np.mean(track)),
+            "transport_ms_per_step": track_ms, "step_wall_ms": [round(x, 4) for x in step_wall_ms],
+            "step_wall_ms_median": float(np.median(step_wall_ms)),
+            "step_transport_ms": [round(x, 4) for x in track[:steps]],
             "step_roofline_frac": B_SEG_2D_MG * seg / (ms * 1e-3) / 1e9 / peak,
             "bytes_per_segment_algorithmic": B_SEG_2D_MG, "energy_closure_max_rel": worst,
             "device_loop": {"ms_per_step": loop_ms, "speedup_over_eager": (ms / steps) / loop_ms,

@@ -369,6 +369,20 @@ IMC_API imc_status imc_comb_async_dev(const imc_mesh* mesh, const imc_bank* in, 
  * are clipped to it), so it can follow a queued comb without a host synchronisation.  Divided
  * by the cell volumes this is MG_IMC2D's post-comb radiation_energy_by_group
  * (MG_IMC/MG_IMC2D.py:2017-2025). */
+/* The fields a multigroup 2-D step reports, gathered in one device buffer in the reference's
+ * array order (cells as (nx, ny) C order, j fastest; groups outermost), so that one
+ * device-to-host copy of (2G + 3) nc + 2G doubles carries them all:
+ *   out[0, G nc)            si[g][c] / c, the radiation energy density by group before the comb
+ *                           (MG_IMC/MG_IMC2D.py:2017-2025 radiation_energy_by_group)
+ *   out[G nc, 2G nc)        after[g][c] / V[c], the same after the comb (after: the second half
+ *                           of an IMC_COMB_WRITE_AFTER disc)
+ *   out[2G nc, (2G+3) nc)   e, T, Tr (nc each)
+ *   then boundary_group and escaped_group (G each).
+ * No reference counterpart (the reference's arrays are host arrays already). */
+IMC_API imc_status imc_mg_report_fields(const imc_mesh* mesh, const double* si, const double* after,
+                                        const double* e, const double* T, const double* Tr,
+                                        const double* boundary_group, const double* escaped_group,
+                                        double* out, void* stream);
 IMC_API imc_status imc_bank_energy_by_bin(const imc_mesh* mesh, const imc_bank* bank, const int64_t* n_dev,
                                           int32_t per_group, double* out, void* stream);
 /* Device time (ms) of the source fill and of tracking in this host thread's last

@@ -174,6 +174,8 @@ SIGNATURES = {
                                c_int32, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p, c_void_p]),
     "imc_comb_async_dev": (c_int, [POINTER(ImcMesh), POINTER(ImcBank), POINTER(ImcBank), c_int64, c_void_p,
                                    c_uint64, c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p, c_void_p]),
+    "imc_mg_report_fields": (c_int, [POINTER(ImcMesh), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                     c_void_p, c_void_p, c_void_p]),
     "imc_bank_energy_by_bin": (c_int, [POINTER(ImcMesh), POINTER(ImcBank), c_void_p, c_int32, c_void_p,
                                        c_void_p]),
     "imc_phase_times": (c_int, [POINTER(ctypes.c_float), POINTER(ctypes.c_float)]),

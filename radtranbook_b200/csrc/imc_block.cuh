@@ -14,16 +14,18 @@ __device__ __forceinline__ double pow4(double T) { const double t2 = T * T; retu
 __device__ __forceinline__ double pow3(double T) { return T * T * T; }
 
 // 1024 strided partial sums, then a halving tree (the oracle's canon_sum).  Each partial
-// loads 8 of its terms at a time before adding them in order (same sum, fewer waits).
+// loads B of its terms at a time before adding them in order (same sum, fewer waits; B = 16
+// only where the kernel has registers to spare at 1024 threads).
+template <int B = 8>
 __device__ inline double block_canon_sum(const double* x, long long n, double* red) {
   const int t = threadIdx.x;
   double s = 0.0;
-  for (long long i0 = t; i0 < n; i0 += 8LL * NT) {
-    double v[8];
+  for (long long i0 = t; i0 < n; i0 += (long long)B * NT) {
+    double v[B];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) { const long long i = i0 + (long long)j * NT; v[j] = i < n ? x[i] : 0.0; }
+    for (int j = 0; j < B; ++j) { const long long i = i0 + (long long)j * NT; v[j] = i < n ? x[i] : 0.0; }
 #pragma unroll
-    for (int j = 0; j < 8; ++j) if (i0 + (long long)j * NT < n) s += v[j];
+    for (int j = 0; j < B; ++j) if (i0 + (long long)j * NT < n) s += v[j];
   }
   red[t] = s;
   __syncthreads();

@@ -317,7 +317,7 @@ __global__ void k_material_law(MatArgs a, imc_material_law law, double* T, doubl
 // Single block: the canonical total of the census energy and the comb mode.
 __global__ void __launch_bounds__(NT) k_comb_plan(CombPlanArgs a) {
   __shared__ double red[NT];
-  const double E = block_canon_sum(a.ecen, a.nb, red);
+  const double E = block_canon_sum<16>(a.ecen, a.nb, red);
   // MG_IMC/MG_IMC1D.py:1194-1200: Nmax = 0 never combs; Nmax < 0 combs once |Nmax| entries live
   const bool compact = a.force_compact || (a.threshold > 0 && (long long)*a.n_live < a.threshold);
   if (threadIdx.x == 0) { *a.mode = compact ? 1 : 0; a.sum->comb_before = E; a.sum->comb_after = 0.0; }
@@ -396,6 +396,38 @@ cudaError_t imc_launch_comb_plan(const CombPlanArgs& a, cudaStream_t s) {
   if (a.nb > 0) k_comb_weights<<<(a.nb + 255) / 256, 256, 0, s>>>(a);
   return cudaGetLastError();
 }
+// The multigroup step's reported fields in the reference's (nx, ny) order, one output each:
+// si / c and after / V by group, then e, T, Tr, then the two group sums (imc_mg_report_fields).
+__global__ void k_mg_report(ReportArgs a) {
+  const long long nc = (long long)a.nx * a.ny, gnc = nc * a.ng;
+  const long long n = 2 * gnc + 3 * nc + 2 * a.ng;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    double v;
+    if (q < 2 * gnc + 3 * nc) {
+      const long long part = q < 2 * gnc ? q / gnc : 2 + (q - 2 * gnc) / nc;  // 0 pre, 1 post, 2.. e T Tr
+      const long long r = q < 2 * gnc ? q % nc : (q - 2 * gnc) % nc;         // reference order i*ny + j
+      const long long g = q < 2 * gnc ? (q % gnc) / nc : 0;
+      const int i = (int)(r / a.ny), j = (int)(r - (long long)i * a.ny);
+      const long long c = i + (long long)a.nx * j;
+      if (part == 0) v = a.si[g * nc + c] / C_LIGHT;
+      else if (part == 1) v = a.after[g * nc + c] / a.vol[c];
+      else v = (part == 2 ? a.e : part == 3 ? a.T : a.Tr)[c];
+    } else {
+      const long long k = q - 2 * gnc - 3 * nc;
+      v = k < a.ng ? a.bnd[k] : a.esc[k - a.ng];
+    }
+    a.out[q] = v;
+  }
+}
+
+cudaError_t imc_launch_mg_report(const ReportArgs& a, cudaStream_t s) {
+  ++g_imc_launches;
+  const long long n = 2LL * a.nx * a.ny * a.ng + 3LL * a.nx * a.ny + 2LL * a.ng;
+  const unsigned blocks = (unsigned)std::min<long long>(4736LL, (n + 255) / 256);
+  k_mg_report<<<blocks, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
 cudaError_t imc_launch_canon_sum_eV(const double* e, const double* vol, int nc, double* out, cudaStream_t s) {
   ++g_imc_launches;
   k_canon_eV<<<1, NT, 0, s>>>(e, vol, nc, out);

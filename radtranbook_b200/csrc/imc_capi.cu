@@ -760,6 +760,21 @@ imc_status imc_comb_async_dev(const imc_mesh* mesh, const imc_bank* in, imc_bank
                     (cudaStream_t)stream, step_dev, n_max_dev);
 }
 
+imc_status imc_mg_report_fields(const imc_mesh* mesh, const double* si, const double* after, const double* e,
+                                const double* T, const double* Tr, const double* boundary_group,
+                                const double* escaped_group, double* out, void* stream) {
+  imc_status st = check_mesh(mesh);
+  if (st != IMC_OK) return st;
+  if (mesh->n_groups < 2 || mesh->geometry < IMC_GEOM_XY) return IMC_ERR_INVALID_ARG;  // 2-D multigroup
+  if (!si || !after || !e || !T || !Tr || !boundary_group || !escaped_group || !out) return IMC_ERR_INVALID_ARG;
+  ReportArgs ra{};
+  ra.nx = mesh->nx; ra.ny = mesh->ny; ra.ng = mesh->n_groups; ra.vol = mesh->volume;
+  ra.si = si; ra.after = after; ra.e = e; ra.T = T; ra.Tr = Tr; ra.bnd = boundary_group; ra.esc = escaped_group;
+  ra.out = out;
+  IMC_CUDA(imc_launch_mg_report(ra, (cudaStream_t)stream));
+  return IMC_OK;
+}
+
 imc_status imc_bank_energy_by_bin(const imc_mesh* mesh, const imc_bank* bank, const int64_t* n_dev,
                                   int32_t per_group, double* out, void* stream) {
   imc_status st = check_mesh(mesh);

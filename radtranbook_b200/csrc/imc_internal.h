@@ -194,6 +194,13 @@ struct ZeroList {
 cudaError_t imc_launch_zero(const ZeroList& z, cudaStream_t s);
 
 cudaError_t imc_launch_canon_sum_eV(const double* e, const double* vol, int nc, double* out, cudaStream_t s);
+struct ReportArgs {
+  int nx, ny, ng;
+  const double* vol; const double* si; const double* after;
+  const double* e; const double* T; const double* Tr; const double* bnd; const double* esc;
+  double* out;
+};
+cudaError_t imc_launch_mg_report(const ReportArgs& a, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------
 // Source fill kernels (element count and first bank index read from device memory)

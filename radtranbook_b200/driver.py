@@ -381,7 +381,6 @@ class DeviceLoop:
             out["fiducial_Erad_by_group"] = self.hist_Eg[:n].cpu().numpy().reshape(n, G, -1)[:, :, :nf] / C_LIGHT
             sE = self.snap_Eg
             out["snapshots_Erad_by_group"] = {label: grid3(sE[q]) for q, label in enumerate(labels)}
-            object.__setattr__(st, "_rad_group", (self.rad_last / C_LIGHT).view(G, -1).clone())
             st.__dict__["radiation_energy_by_group"] = grid3(self.rad_last)
             st.__dict__["radiation_energy_by_group_postcomb"] = None
             out["Nmax_next"] = self._nmax_schedule(1)[0]

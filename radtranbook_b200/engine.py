@@ -448,6 +448,19 @@ class Engine:
                                             self._stream())
         _lib.check("imc_bank_energy_by_bin", st)
 
+    def mg_report_fields(self, e: torch.Tensor, T: torch.Tensor, Tr: torch.Tensor) -> int:
+        """Queue imc_mg_report_fields into self.report_dev (2-D multigroup): the radiation
+        energy by group before (si / c) and after the comb (comb_after / V), e, T, Tr and the
+        boundary / escaped energy by group, in the reference's array order.  Returns its
+        length in doubles."""
+        n = (2 * self.ng + 3) * self.nc + 2 * self.ng
+        if getattr(self, "report_dev", None) is None or self.report_dev.numel() != n:
+            self.report_dev = torch.empty(n, dtype=torch.float64, device=self.device)
+        _lib.check("imc_mg_report_fields", self.lib.imc_mg_report_fields(
+            ctypes.byref(self.cmesh), _ptr(self.si), _ptr(self.comb_after), _ptr(e), _ptr(T), _ptr(Tr),
+            _ptr(self.boundary_group), _ptr(self.escaped_group), _ptr(self.report_dev), self._stream()))
+        return n
+
     def fetch(self, host_copies=()) -> ImcStepSummary:
         """Copy the summary (and any (device, pinned host) pairs) to the host and synchronise.
         A comb overflow is handled by growing the output bank and combing again (the input

@@ -131,7 +131,6 @@ def init_simulation(Ntarget, Tinit, Tr_init, edges1, edges2, energy_edges, eos, 
     eng.init_census(tr, local_count(N_ic, rank, world), T_emit_floor)
     rad = _rad_by_group(eng)
     sum_tensors(dist, [rad])
-    object.__setattr__(state, "_rad_group", rad)
     state.__dict__["radiation_energy_by_group"] = rad.view(G, ny, nx).transpose(1, 2).cpu().numpy().copy()
     state.__dict__["radiation_energy_by_group_postcomb"] = None
     state._Tr.copy_(torch.pow(rad.sum(0) / A_RAD, 0.25))
@@ -154,19 +153,18 @@ def _rad_by_group(eng: Engine) -> torch.Tensor:
     return acc.view(G, nc) / eng.vol.view(1, nc)
 
 
-def _group_buffers(state, eng: Engine) -> dict:
-    """Pinned host buffers for the end-of-step copies of the by-group fields: the boundary and
-    escaped energy by group (allocated once per state), and for the (G, nx, ny) radiation
-    energies a fresh pair each step from torch's caching pinned allocator, which the step's
-    info arrays then view without a host copy (a buffer returns to the cache once nothing
-    views it)."""
-    hb = state.__dict__.get("_mg_hbuf")
-    if hb is None:
-        hb = {k: torch.zeros(eng.ng, dtype=torch.float64, pin_memory=True) for k in ("bnd", "esc")}
-        object.__setattr__(state, "_mg_hbuf", hb)
-    n = eng.ng * eng.nc
-    return dict(hb, pre=torch.empty(n, dtype=torch.float64, pin_memory=True),
-                post=torch.empty(n, dtype=torch.float64, pin_memory=True))
+def _report_buffers(state, eng: Engine, n: int) -> dict:
+    """A fresh pinned host buffer of the step's n reported doubles (imc_mg_report_fields
+    layout) from torch's caching pinned allocator, and its parts: the radiation energy by
+    group before and after the comb, e / T / Tr (the state's host mirrors read them), the
+    boundary and escaped energy by group.  The step's arrays view it without a host copy; it
+    returns to the cache once nothing views it."""
+    G, nc = eng.ng, eng.nc
+    buf = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    o = 2 * G * nc + 3 * nc
+    object.__setattr__(state, "_hpin", buf[2 * G * nc:o])  # e, T, Tr for take_host_copies
+    return {"all": buf, "pre": buf[:G * nc], "post": buf[G * nc:2 * G * nc], "bnd": buf[o:o + G],
+            "esc": buf[o + G:o + 2 * G]}
 
 
 def _law_buffers(state, eng: Engine, sigma: torch.Tensor) -> tuple:
@@ -291,15 +289,12 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
     # writes the energy after it per (group, cell) bin: the post-comb radiation energy by
     # group without a pass over the new census
     eng.comb_async(nmax_l, state.count, state._e, per_group=True, write_after=True)
-    rad_pre = eng.si.view(G, nc) / C_LIGHT  # radiation energy density by group (path length)
     nx, ny = state._shape
-    hb = _group_buffers(state, eng)
 
     def to_grid3(x):  # device (G, nc) in flat cell order -> (G, nx, ny) C order, flattened
         return x.reshape(G, ny, nx).transpose(1, 2).reshape(-1)
 
     sum_tensors(dist, [eng.comb_after])
-    post_dev = eng.comb_after.view(G, nc) / eng.vol.view(1, nc)
     if conserve_comb_energy:
         sum_tensors(dist, [eng.disc])
         state._e.add_(eng.disc.view(G, nc).sum(0) / eng.vol)
@@ -307,11 +302,11 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
         Tn = evaluate(inv_eos, state.grid(state._e), lambda: _host_copy(state.grid(state._e)), like,
                       **_staged(state, "T_new", nc))
         state._T.copy_(state.flat(Tn))
-    # the (G, nx, ny) transposes run on the device, so the host only copies contiguous arrays
-    group_copies = state.host_copies() + [(to_grid3(rad_pre), hb["pre"]), (to_grid3(post_dev), hb["post"]),
-                                          (eng.boundary_group, hb["bnd"]), (eng.escaped_group, hb["esc"])]
+    # every reported field in the reference's layout in one device buffer (one kernel), then
+    # one copy into a fresh pinned buffer that the host arrays view
+    hb = _report_buffers(state, eng, eng.mg_report_fields(state._e, state._T, state._Tr))
     try:
-        sm = eng.fetch(group_copies)
+        sm = eng.fetch([(eng.report_dev, hb["all"])])
     except _lib.ImcError as ex:
         if ex.status == 3:
             raise AssertionError("non-finite or non-positive material state") from ex
@@ -326,6 +321,7 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
         rad_pre = acc.view(G, nc) / eng.vol.view(1, nc)
         state._Tr.copy_(torch.pow(rad_pre.sum(0) / A_RAD, 0.25))
         state.refresh_host()
+        hb["pre"].copy_(to_grid3(rad_pre))
     else:
         state.take_host_copies()
     # the comb ran again after an overflow (on any rank): rebuild from the new census
@@ -353,17 +349,14 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
     def grid3(h):  # this step's pinned host buffer, already (G, nx, ny): the array views it
         return h.numpy().reshape(G, nx, ny)
 
-    if not use_scalar_intensity_Tr:
-        hb["pre"].copy_(to_grid3(rad_pre))
     rad_group_pre = grid3(hb["pre"])
     rad_group_post = grid3(hb["post"])
     _lib.TRANSFER["d2h"] += 8 * (2 * G * nc + 2 * G)
-    object.__setattr__(state, "_rad_group", rad_pre)
     state.__dict__["radiation_energy_by_group"] = rad_group_pre
     state.__dict__["radiation_energy_by_group_postcomb"] = rad_group_post
     stats = tot["stats"]
-    bnd_group = hb["bnd"].numpy().copy()
-    esc_group = hb["esc"].numpy().copy()
+    bnd_group = hb["bnd"].numpy()
+    esc_group = hb["esc"].numpy()
     ms_src, ms_tr = eng.phase_times()
     t_end = _time.perf_counter()
     n_tr = tot["n_bank"]

@@ -111,3 +111,29 @@ def test_comb_after_energy_is_the_new_census(cuda):
     post = infos[-1]["radiation_energy_by_group_postcomb"]
     assert post.shape == (G, nx, ny) and post.sum() > 0
     np.testing.assert_allclose(post, census, rtol=1e-12, atol=1e-300)
+
+
+def test_mg_report_fields_are_the_engine_fields(cuda):
+    """The step's reported arrays come from one gather kernel (imc_mg_report_fields) and one
+    copy: they equal, bit for bit, the fields computed from the engine's tensors on the host
+    (si / c and comb_after / V by group, NumPy's correctly rounded divisions, transposed to
+    (G, nx, ny); T, Tr, e in (nx, ny); the boundary and escaped energy by group)."""
+    from radtranbook_b200.engine import C_LIGHT
+
+    p = problems.mg_crooked_pipe(nr=30, nz=105, mode="quick")
+    st, infos = _mg_pipe_steps(p, 2)
+    eng, info = st._engine, infos[-1]
+    G, nx, ny, nc = 10, 30, 105, 30 * 105
+
+    def grid3(x):
+        return x.reshape(G, ny, nx).transpose(0, 2, 1)
+
+    si, after, vol = (t.cpu().numpy() for t in (eng.si, eng.comb_after, eng.vol))
+    np.testing.assert_array_equal(info["radiation_energy_by_group"], grid3(si.reshape(G, nc) / C_LIGHT))
+    np.testing.assert_array_equal(info["radiation_energy_by_group_postcomb"],
+                                  grid3(after.reshape(G, nc) / vol.reshape(1, nc)))
+    np.testing.assert_array_equal(info["temperature"], st.grid(st._T).cpu().numpy())
+    np.testing.assert_array_equal(info["radiation_temperature"], st.grid(st._Tr).cpu().numpy())
+    np.testing.assert_array_equal(st.internal_energy, st.grid(st._e).cpu().numpy())
+    np.testing.assert_array_equal(info["boundary_emission_by_group"], eng.boundary_group.cpu().numpy())
+    np.testing.assert_array_equal(info["boundary_outgoing_by_group"], eng.escaped_group.cpu().numpy())
