@@ -432,7 +432,7 @@ def form_carter_forest(steps: int = 10, warmup: int = 2) -> dict:
             worst = max(worst, abs(info["ledger"]["relative_closure"]))
         return st, seg, capt, reem, worst
 
-    st, _, _, _, _ = run(warmup, st)
+    st = run(warmup, st)[0]  # no info of the warm-up kept (its arrays view the step's buffer)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
@@ -538,7 +538,7 @@ def form_mg_crooked_pipe(steps: int = 12, warmup: int = 3) -> dict:
         return st, seg, hist, worst, info
 
     track, used, walls = [], [], []
-    st, _, _, _, _ = run(warmup, st)
+    st = run(warmup, st)[0]  # no info of the warm-up kept (its arrays view the step's buffer)
     track.clear()
     del used[:]
     del walls[:]
@@ -559,7 +559,7 @@ def form_mg_crooked_pipe(steps: int = 12, warmup: int = 3) -> dict:
     # the same steps as the device-resident loop
     st2 = init()
     state.update(dt=p["dt_initial"], k=0)
-    st2, _, _, _, _ = run(warmup, st2)
+    st2 = run(warmup, st2)[0]
     loop = driver.DeviceLoop(st2, Ntarget=p["Ntarget"], Nboundary=p["Nboundary"], Nsource=0,
                              Nmax=p["Nmax"] + warmup * p["Nmax_growth"], T_boundary=p["T_boundary"],
                              sigma_a_func=p["sigma_dev"], inv_eos=p["inv_eos_dev"], cv=p["cv_dev"],

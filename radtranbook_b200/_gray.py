@@ -8,6 +8,7 @@ material energy, combs the census, and the energy ledger is closed in FP64.
 from __future__ import annotations
 
 import time as _time
+import weakref
 
 import numpy as np
 import torch
@@ -53,26 +54,61 @@ class GrayState:
             return grid.reshape(-1).contiguous()
         return grid.t().contiguous().view(-1)
 
+    # ---- the step's host arrays ----
+    # A step's reported arrays view a pinned buffer that the step's one device-to-host copy
+    # filled: a fresh buffer from torch's caching pinned allocator each step, so no host copy
+    # is made, and a buffer returns to the cache once nothing views it.  A caller that keeps
+    # the arrays of every step (a list of info dicts) would make the allocator pin new memory
+    # each step; once the arrays of a step are still alive two steps later (the caller's
+    # current info holds the previous step's), the state switches to one buffer of its own,
+    # overwritten each step, and returns copies.
+    def host_buffer(self, n: int) -> torch.Tensor:
+        """Pinned buffer of n doubles for this step's reported arrays."""
+        if not self.__dict__.get("_host_copy_mode"):
+            return torch.empty(n, dtype=torch.float64, pin_memory=True)
+        own = self.__dict__.get("_host_own")
+        if own is None or own.numel() < n:
+            own = torch.empty(n, dtype=torch.float64, pin_memory=True)
+            object.__setattr__(self, "_host_own", own)
+        return own[:n]
+
+    def publish(self, arrays: list) -> list:
+        """The arrays this step returns (views of host_buffer): copies in copy mode; else the
+        views, with weak references kept to see whether the caller keeps them."""
+        if self.__dict__.get("_host_copy_mode"):
+            return [np.array(a) for a in arrays]
+        refs = self.__dict__.setdefault("_host_refs", [])
+        refs.append([weakref.ref(a) for a in arrays])
+        if len(refs) > 2 and any(r() is not None for r in refs.pop(0)):
+            object.__setattr__(self, "_host_copy_mode", True)
+        return arrays
+
     def host_copies(self):
         """(device, pinned host) pair for the end-of-step copy of e, T and Tr: the three fields
-        stacked on the device in the reference's layout ((nx, ny) in 2-D), one copy into a
-        fresh buffer of torch's caching pinned allocator, which the host arrays then view
-        (no host-side copy; a buffer returns to the cache once no array views it)."""
+        stacked on the device in the reference's layout ((nx, ny) in 2-D), one copy into the
+        step's host buffer."""
         src = torch.stack([self.grid(self._e), self.grid(self._T), self.grid(self._Tr)]).reshape(-1)
-        pin = torch.empty(src.numel(), dtype=torch.float64, pin_memory=True)
+        pin = self.host_buffer(src.numel())
         object.__setattr__(self, "_hpin", pin)
         return [(src, pin)]
 
-    def take_host_copies(self) -> None:
-        """Host mirrors from the pinned buffer filled by the last fetch (no device access)."""
+    def take_host_copies(self, publish: bool = True) -> list:
+        """Host mirrors of e, T and Tr from the buffer filled by the last fetch (no device
+        access); publish=False leaves publishing them (with other arrays) to the caller, which
+        then sets the mirrors.  Returns the three arrays."""
         nc = self._engine.nc
         a = self._hpin.numpy()
         shape = (nc,) if self._dim == 1 else tuple(self._shape)
-        h = self._host
-        h["internal_energy"] = a[:nc].reshape(shape)
-        h["temperature"] = a[nc:2 * nc].reshape(shape)
-        h["radiation_temperature"] = a[2 * nc:].reshape(shape)
+        arrs = [a[:nc].reshape(shape), a[nc:2 * nc].reshape(shape), a[2 * nc:].reshape(shape)]
         _lib.TRANSFER["d2h"] += 3 * 8 * nc
+        if publish:
+            arrs = self.publish(arrs)
+            self.set_host_mirrors(arrs)
+        return arrs
+
+    def set_host_mirrors(self, arrs: list) -> None:
+        h = self._host
+        h["internal_energy"], h["temperature"], h["radiation_temperature"] = arrs
 
     def refresh_host(self) -> None:
         h = self._host

@@ -154,13 +154,12 @@ def _rad_by_group(eng: Engine) -> torch.Tensor:
 
 
 def _report_buffers(state, eng: Engine, n: int) -> dict:
-    """A fresh pinned host buffer of the step's n reported doubles (imc_mg_report_fields
-    layout) from torch's caching pinned allocator, and its parts: the radiation energy by
-    group before and after the comb, e / T / Tr (the state's host mirrors read them), the
-    boundary and escaped energy by group.  The step's arrays view it without a host copy; it
-    returns to the cache once nothing views it."""
+    """The step's pinned host buffer of n reported doubles (imc_mg_report_fields layout,
+    GrayState.host_buffer) and its parts: the radiation energy by group before and after the
+    comb, e / T / Tr (the state's host mirrors read them), the boundary and escaped energy by
+    group."""
     G, nc = eng.ng, eng.nc
-    buf = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    buf = state.host_buffer(n)
     o = 2 * G * nc + 3 * nc
     object.__setattr__(state, "_hpin", buf[2 * G * nc:o])  # e, T, Tr for take_host_copies
     return {"all": buf, "pre": buf[:G * nc], "post": buf[G * nc:2 * G * nc], "bnd": buf[o:o + G],
@@ -322,8 +321,9 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
         state._Tr.copy_(torch.pow(rad_pre.sum(0) / A_RAD, 0.25))
         state.refresh_host()
         hb["pre"].copy_(to_grid3(rad_pre))
+        eTT = []
     else:
-        state.take_host_copies()
+        eTT = state.take_host_copies(publish=False)
     # the comb ran again after an overflow (on any rank): rebuild from the new census
     if sum_scalars(dist, [float(eng.comb_repeated)], eng.device)[0] > 0:
         post = _rad_by_group(eng)
@@ -349,14 +349,14 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
     def grid3(h):  # this step's pinned host buffer, already (G, nx, ny): the array views it
         return h.numpy().reshape(G, nx, ny)
 
-    rad_group_pre = grid3(hb["pre"])
-    rad_group_post = grid3(hb["post"])
+    rad_group_pre, rad_group_post, bnd_group, esc_group, *eTT = state.publish(
+        [grid3(hb["pre"]), grid3(hb["post"]), hb["bnd"].numpy(), hb["esc"].numpy()] + eTT)
+    if eTT:
+        state.set_host_mirrors(eTT)
     _lib.TRANSFER["d2h"] += 8 * (2 * G * nc + 2 * G)
     state.__dict__["radiation_energy_by_group"] = rad_group_pre
     state.__dict__["radiation_energy_by_group_postcomb"] = rad_group_post
     stats = tot["stats"]
-    bnd_group = hb["bnd"].numpy()
-    esc_group = hb["esc"].numpy()
     ms_src, ms_tr = eng.phase_times()
     t_end = _time.perf_counter()
     n_tr = tot["n_bank"]
