@@ -272,15 +272,16 @@ def fom_cpu(scale: float, steps: int, seeds: int, nthreads: int) -> dict:
     return out
 
 
-def form_batched(steps: int, tune: bool) -> dict:
-    """Uneven 256-instance slab batch: the batched engine (one CUDA graph per step) and the
-    plain form (the single-problem drop-in, one instance after the other) on the same
-    histories (each instance draws identical Philox streams in both forms)."""
+def form_batched(steps: int, tune: bool, n_inst: int = 256, particle_scale: float = 1.0) -> dict:
+    """Uneven slab batch (n_inst instances, per-instance particles 10^U[4,6] x particle_scale):
+    the batched engine (one CUDA graph per step) and the plain form (the single-problem
+    drop-in, one instance after the other) on the same histories (each instance draws
+    identical Philox streams in both forms)."""
     import torch
 
     from radtranbook_b200 import _lib, batch
 
-    spec = batch.uneven_slab_batch()
+    spec = batch.uneven_slab_batch(n_inst=n_inst, particle_scale=particle_scale)
     eng = batch.BatchEngine(spec)
     eng.init()
     tuned = None
@@ -315,7 +316,8 @@ def form_batched(steps: int, tune: bool) -> dict:
     # the plain loop's time in the same windows: every instance's steps of that window
     st_s = np.array(pl["step_s"])  # [instance, step]
     win_p = [float(st_s[:, w * window:(w + 1) * window].sum()) for w in range(len(win_b))]
-    return {"workload": "uneven_slab_batch_256", "steps": steps, "instances": spec.K,
+    return {"workload": "uneven_slab_batch_%d%s" % (spec.K, "" if particle_scale == 1.0 else "_x%g" % particle_scale),
+            "steps": steps, "instances": spec.K,
             "particles_per_step": int((spec.n_target + spec.n_boundary).sum()),
             "batched_segments_per_s": ev_b / tb, "plain_segments_per_s": pl["events"] / tp,
             "speedup": (ev_b / tb) / (pl["events"] / tp), "same_histories": bool(ev_b == pl["events"]),
@@ -856,7 +858,9 @@ def run_ours(args, rank: int, world: int):
                          f"FP64 C++ oracle, OpenMP ({dtc:.1f} s)", "histories_per_s": h}
     forms = fom = None
     if world == 1 and not args.no_forms:
-        forms = {"batched": form_batched(args.batch_steps, not args.no_tune), "adjoint": form_adjoint(),
+        forms = {"batched": form_batched(args.batch_steps, not args.no_tune),
+                 "batched_small": form_batched(10, not args.no_tune, n_inst=512, particle_scale=0.01),
+                 "adjoint": form_adjoint(),
                  "carter_forest": form_carter_forest(), "device_loop": form_device_loop(launch=dict(eng.launch)),
                  "mg_crooked_pipe": form_mg_crooked_pipe(), "other_configs": form_other_configs(),
                  "event_based": form_event_based(launch=dict(eng.launch))}
@@ -911,7 +915,8 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="skip the batched and adjoint forms")
     ap.add_argument("--only-form", default=None,
                     choices=["batched", "adjoint", "carter_forest", "device_loop", "mg_crooked_pipe",
-                             "mg_crooked_pipe_run", "other_configs", "event_based", "slab_event_cap"],
+                             "mg_crooked_pipe_run", "other_configs", "event_based", "slab_event_cap",
+                             "batched_small"],
                     help="run one further form alone on GPU 0 and print its JSON (no headline line)")
     ap.add_argument("--batch-steps", type=int, default=50, help="steps of the batched form (the workload's 50)")
     ap.add_argument("--no-fom", action="store_true")
@@ -930,6 +935,7 @@ def main():
 
         torch.cuda.set_device(0)
         fn = {"batched": lambda: form_batched(args.batch_steps, not args.no_tune), "adjoint": form_adjoint,
+              "batched_small": lambda: form_batched(10, not args.no_tune, n_inst=512, particle_scale=0.01),
               "carter_forest": form_carter_forest, "device_loop": form_device_loop,
               "mg_crooked_pipe": form_mg_crooked_pipe, "mg_crooked_pipe_run": form_mg_crooked_pipe_run,
               "other_configs": lambda: form_other_configs(tune=not args.no_tune),
