@@ -1121,7 +1121,8 @@ int orc_adjoint_vjp(void* h, const orc_step_in* in, const double* cot, double* g
  * MG_IMC/MG_IMC2D.py:1314-1378 (per cell and group, bin = cell + ncell*group).
  *   ecen[b] = sum of live weights; desired = max(1, round_half_even(Nmax ecen/E));
  *   ew = ecen/desired; copies = floor(w/ew + xi), each of weight ew, in bank order.
- * xi: Philox (pre-comb index k, block 0, step, TAG_COMB).  Sets census times to 0.
+ * xi: word k % 4 of Philox block (k / 4, 1, step, TAG_COMB), k the pre-comb index.
+ * Sets census times to 0.
  * disc (per bin) = ecen - ecen_after.  Returns the new bank size. */
 /* Stochastic comb.  flags: bit 0 = bins per (cell, group), bit 1 = each bin's copies share
  * the bin's pre-comb energy equally (MG_IMC/MG_IMC1D.py:808-820, conserve_comb_energy =
@@ -1169,8 +1170,9 @@ long long orc_comb(void* h, long long Nmax, uint32_t step, int flags, double* di
     if (!(B.w[k] > 0)) continue;
     const int b = bin(k);
     if (!(ew[b] > 0)) continue;
-    Draw4 r = draw(P.seed, (uint32_t)k, 0, step, oracle::TAG_COMB);
-    nk[k] = (long long)std::floor(B.w[k] / ew[b] + r.u[0]);
+    // four consecutive entries share one Philox block: entry k takes word k % 4 of block k / 4
+    Draw4 r = draw(P.seed, (uint32_t)(k >> 2), 1, step, oracle::TAG_COMB);
+    nk[k] = (long long)std::floor(B.w[k] / ew[b] + r.u[k & 3]);
     if (nk[k] > 0) ncopy[b] += nk[k];
   }
   std::vector<double> wout(ew);

@@ -388,8 +388,8 @@ __global__ void __launch_bounds__(BATCH_TILE) k_bcomb_count(BatchArgs a) {
         bin = a.cell_off[k] + B.cell[pid];
         const double ew = a.ew[bin];
         if (ew > 0.0) {
-          const U4 r = draw(a.seed[k], (uint32_t)lid, 0, step, TAG_COMB);
-          n = (int)floor((double)wf / ew + u01d(r.x));
+          const U4 r = draw(a.seed[k], (uint32_t)(lid >> 2), 1, step, TAG_COMB);  // word lid % 4
+          n = (int)floor((double)wf / ew + u01d(u4_word(r, (int)(lid & 3))));
         }
       }
       a.cnt[q] = n;

@@ -88,16 +88,16 @@ __global__ void __launch_bounds__(256) k_comb_ecen(CombArgs a) {
 // table when the bin changes, so the loop has no warp-wide step.
 constexpr int CNT_PER = TILE / CNT_T;
 
-__device__ __forceinline__ int comb_copies(const CombArgs& a, long long k, float wf, int bk, bool compact,
-                                           uint32_t step, int& b) {
+// copies of one entry: floor(w / ew + xi), xi its comb uniform (word k % 4 of Philox block
+// (k / 4, 1, step, TAG_COMB), k the pre-comb index)
+__device__ __forceinline__ int comb_copies(const CombArgs& a, float wf, int bk, bool compact, uint32_t xw, int& b) {
   b = 0;
   if (!(wf > 0.f) || !bin_ok(a, bk)) return 0;
   b = bk;
   if (compact) return 1;
   const double ew = a.ew[b];
   if (!(ew > 0.0)) return 0;
-  const U4 r = draw_rk(a.rk, (uint32_t)k, 0, step, TAG_COMB);
-  return (int)floor((double)wf / ew + u01d(r.x));
+  return (int)floor((double)wf / ew + u01d(xw));
 }
 
 __global__ void __launch_bounds__(CNT_T) k_comb_count(CombArgs a) {
@@ -129,11 +129,15 @@ __global__ void __launch_bounds__(CNT_T) k_comb_count(CombArgs a) {
       for (int q = 0; q < 4; ++q)
         if (kj + q < n_in) { wv[q] = a.w[kj + q]; bv[q] = bin_of(a, kj + q); }
     }
+    // one Philox block for the four entries kj..kj+3 (kj % 4 == 0), drawn when one of them is alive
+    U4 r{0u, 0u, 0u, 0u};
+    if (!compact && (wv[0] > 0.f || wv[1] > 0.f || wv[2] > 0.f || wv[3] > 0.f))
+      r = draw_rk(a.rk, (uint32_t)(kj >> 2), 1, step, TAG_COMB);
     int nv[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       int b;
-      const int n = kj + q < n_in ? comb_copies(a, kj + q, wv[q], bv[q], compact, step, b) : 0;
+      const int n = kj + q < n_in ? comb_copies(a, wv[q], bv[q], compact, u4_word(r, q), b) : 0;
       nv[q] = n;
       tsum += (unsigned)n;
       if (n > 0) {

@@ -77,6 +77,12 @@ __device__ __forceinline__ U4 draw_rk(const uint32_t* rk, uint32_t idx, uint32_t
   return c;
 }
 
+// Word q (0..3) of a Philox block: the comb's uniform of pre-comb entry k is word k % 4 of
+// block (k / 4, 1), so four consecutive entries share one block.
+__device__ __forceinline__ uint32_t u4_word(const U4& r, int q) {
+  return q == 0 ? r.x : q == 1 ? r.y : q == 2 ? r.z : r.w;
+}
+
 // -log(u) for u = u01: distance in mean free paths.
 __device__ __forceinline__ float neglog_u(uint32_t x) { return -logf(u01f(x)); }
 
