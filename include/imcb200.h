@@ -386,7 +386,8 @@ IMC_API imc_status imc_mg_report_fields(const imc_mesh* mesh, const double* si, 
 IMC_API imc_status imc_bank_energy_by_bin(const imc_mesh* mesh, const imc_bank* bank, const int64_t* n_dev,
                                           int32_t per_group, double* out, void* stream);
 /* Device time (ms) of the source fill and of tracking in this host thread's last
- * imc_step_transport[_async]; valid once that work has completed. */
+ * imc_step_transport[_async].  Waits for that step's tracking to end (not for work queued
+ * after it, such as the comb), so a host can read the times while the comb runs. */
 IMC_API imc_status imc_phase_times(float* ms_sources, float* ms_transport);
 
 /* Sum of live weights (FP64) and of e[c]*V[c]; host results. */

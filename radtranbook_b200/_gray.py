@@ -16,6 +16,7 @@ import torch
 from . import _lib
 from .engine import A_RAD, C_LIGHT, Engine
 from .materials import evaluate, is_device
+from .partition import local_count, sum_tensors, summary_totals, world_of
 
 
 class GrayState:
@@ -177,8 +178,8 @@ def _host_copy(t: torch.Tensor) -> np.ndarray:
 
 def check_partition(eng: Engine, dist) -> tuple[int, int]:
     """(rank, world) of a partitioned step; the state must have been initialised for it."""
-    from .partition import world_of
-
+    if dist is None and eng.world == 1:
+        return 0, 1
     rank, world = world_of(dist)
     if (eng.rank, eng.world) != (rank, world):
         raise ValueError("the state was initialised for rank %d of %d, the step runs as rank %d of %d "
@@ -240,8 +241,6 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
     are summed over the ranks before the material update (so every rank holds the same
     material state), each rank combs its census to its share of Nmax, and the ledger terms
     are summed.  The state must come from init_simulation with the same allreduce."""
-    from .partition import local_count, sum_tensors, summary_totals
-
     t_step_start = _time.perf_counter()
     eng: Engine = state._engine
     rank, world = check_partition(eng, allreduce)
@@ -250,7 +249,7 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
         Ntarget, Nboundary, Nsource = (local_count(n, rank, world) for n in (Ntarget, Nboundary, Nsource))
         Nmax = local_count(Nmax, rank, world) if Nmax > 0 else Nmax
     dim = state._dim
-    like = state.grid(state._T)
+    like = None  # the reference-layout view of T, for host callables only
     host_T = lambda: state.temperature  # noqa: E731
     # a material the device evaluates itself (LinearEOS, Constant, PowerLawOpacity): the
     # material update, inverse EOS and next step's opacity are one kernel at the step's end
@@ -261,6 +260,7 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
     else:
         # host callables' results go up by asynchronous copies from pinned buffers of the state
         # (refilled only next step, after this step's end-of-step synchronisation)
+        like = state.grid(state._T)
         sigma = state.flat(evaluate(sigma_a_func, like, host_T, like, **_staged(state, "sigma", eng.nc)))
         cvv = state.flat(evaluate(cv, like, host_T, like, **_staged(state, "cv", eng.nc)))
     src = None
@@ -308,6 +308,8 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
     if conserve_comb_energy:
         sum_tensors(dist, [eng.disc])
         state._e.add_(eng.disc[: eng.nc] / eng.vol)
+    if law is None and like is None:
+        like = state.grid(state._T)
     if law is not None:
         pass  # T = e / cv came with the material update
     elif e_ready is not None:
@@ -320,8 +322,11 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
     else:
         Tn = evaluate(inv_eos, state.grid(state._e), lambda: _host_copy(state.grid(state._e)), like)
         state._T.copy_(state.flat(Tn))
+    copies = state.host_copies()
+    # the phase times wait for the tracking only: read while the comb still runs on the device
+    ms_src, ms_tr = eng.phase_times()
     try:
-        sm = eng.fetch(state.host_copies())
+        sm = eng.fetch(copies)
     except _lib.ImcError as ex:
         if ex.status == 3:
             raise AssertionError("Fleck factor out of bounds / non-positive temperature in material state") from ex
@@ -339,7 +344,7 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
     tot = summary_totals(dist, sm, eng.bank.size, eng.device)
     rad, stats = tot["rad"], tot["stats"]
     comb_disc = tot["comb_before"] - rad
-    boundary_emission, boundary_loss = float(tot["e_side"].sum()), float(tot["escaped"].sum())
+    boundary_emission, boundary_loss = tot["e_side_total"], tot["escaped_total"]
     source_emission, emission_total, weight_sum = tot["source_emission"], tot["emission_total"], tot["weight_sum"]
     n_particles, n_tr = tot["n_particles"], tot["n_bank"]
     if conserve_comb_energy:
@@ -355,7 +360,6 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
     state.previous_total_energy = total
     state.count += 1
     t_end = _time.perf_counter()
-    ms_src, ms_tr = eng.phase_times()
 
     n_tr = int(n_tr)
     ev = int(stats[_lib.STAT_EVENTS])

@@ -248,9 +248,15 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   if (pe.ok) IMC_CUDA(cudaEventRecord(pe.e[0], s));
   float *p2, *d2;
   set_bank(p2, d2, bank, two_d);
+  // every source of the step (and the sum of the tracked weights) in one launch
+  SourceJobs sj{};
+  imcdev::philox_round_keys(par->seed, sj.rk);
+  sj.wsum = &sum->weight_sum;
+  sj.census_w = bank->weight;
+  sj.n_census = &sum->n_census;
   for (int side = 0; side < 4; ++side) {
     if (!par->face_T[side] || side_count(par, side) <= 0) continue;
-    BndArgs ba{};
+    BndArgs& ba = sj.bnd[sj.n_bnd++];
     ba.geom = mesh->geometry; ba.nx = mesh->nx; ba.ny = mesh->ny; ba.side = side; ba.nf = pa.nf;
     ba.e1 = mesh->edges1; ba.e2 = mesh->edges2;
     ba.face = pa.face + (size_t)side * 2 * pa.nf;
@@ -264,13 +270,13 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     ba.below_last = mg1 ? 1 : 0;
     ba.dt_dev = par->dt_dev; ba.step_dev = par->step_dev;
     ba.id_base = par->id_base;
-    IMC_CUDA(imc_launch_fill_boundary(ba, s));
   }
   const int nbins = mg1 ? nc * ng : nc;  // source order positions (MG 1-D: (group, cell) bins)
   bool cf_times = false;
   auto fill = [&](const int64_t* d_n, const int64_t* d_base, long long n_bound, const long long* off,
                   const float* w, const double* tilt, int kind, uint32_t tag) -> cudaError_t {
-    FillArgs fa{};
+    if (sj.n_vol >= 2) return cudaErrorInvalidValue;
+    FillArgs& fa = sj.vol[sj.n_vol++];
     fa.geom = mesh->geometry; fa.nx = mesh->nx; fa.ny = mesh->ny; fa.nc = nc;
     fa.nbins = nbins; fa.bins_by_group = mg1 ? 1 : 0;
     fa.time_scale_dev = par->dt_dev; fa.step_dev = par->step_dev;
@@ -286,11 +292,12 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
       fa.cf_rate4 = pa.tilt + 3;
       fa.cf_thr = (mesh->geometry == IMC_GEOM_SLAB || mesh->geometry == IMC_GEOM_SPHERE) ? 1e-10 : 1e-12;
     }
-    return imc_launch_fill_volume(fa, s);
+    return cudaSuccess;
   };
   auto fill_mg = [&](const int64_t* d_n, const int64_t* d_base, long long n_bound, const double* cdf,
                      const double* gcdf, uint32_t tag) -> cudaError_t {
-    FillMgArgs fm{};
+    if (sj.n_vmg >= 2) return cudaErrorInvalidValue;
+    FillMgArgs& fm = sj.vmg[sj.n_vmg++];
     fm.geom = mesh->geometry; fm.nx = mesh->nx; fm.ny = mesh->ny; fm.nc = nc; fm.ng = ng;
     fm.e1 = mesh->edges1; fm.e2 = mesh->edges2; fm.cdf = cdf; fm.gcdf = gcdf; fm.tr = nullptr;
     fm.gedges = mesh->group_edges; fm.mixcdf = ws_ptr<double>(workspace, L.mixcdf);
@@ -301,7 +308,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     fm.t = bank->time; fm.cell = bank->cell; fm.group = bank->group;
     fm.time_scale_dev = par->dt_dev; fm.step_dev = par->step_dev;
     fm.id_base = par->id_base;
-    return imc_launch_fill_mg(fm, s);
+    return cudaSuccess;
   };
   const bool rzlin = mesh->geometry == IMC_GEOM_RZ && par->rz_linear_source;
   if (mg1) {
@@ -330,9 +337,23 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     cf_times = false;
   }
 
+  // two launches of the job table: the faces with the census weights, then the volume fills
+  // (one kernel holding every body would run the volume fill with fewer resident blocks)
+  {
+    const int nb = sj.n_jobs;
+    for (int q = 0; q < sj.n_bnd; ++q) sj.add(JOB_BOUNDARY, q, imc_source_blocks(sj.bnd[q].n_bound));
+    sj.add(JOB_CENSUS_WSUM, 0, std::min(imc_source_blocks(std::max<long long>(bank->size, 1)), 4 * sm_count()));
+    IMC_CUDA(imc_launch_sources(sj, s));
+    sj.n_jobs = nb;
+    for (int q = 0; q < sj.n_vol; ++q) sj.add(JOB_VOLUME, q, imc_source_blocks(sj.vol[q].n_bound));
+    IMC_CUDA(imc_launch_sources(sj, s));
+    sj.n_jobs = nb;
+    for (int q = 0; q < sj.n_vmg; ++q) sj.add(JOB_VOLUME_MG, q, imc_source_blocks(sj.vmg[q].n_bound));
+    IMC_CUDA(imc_launch_sources(sj, s));
+  }
+
   // ---- tracking ----
   if (pe.ok) IMC_CUDA(cudaEventRecord(pe.e[1], s));
-  IMC_CUDA(imc_launch_wsum(bank->weight, &sum->n_bank, n_upper, &sum->weight_sum, s));
 
   TrackArgs ta{};
   ta.nx = mesh->nx; ta.ny = mesh->ny; ta.nc = nc; ta.ng = ng;
@@ -563,6 +584,8 @@ unsigned long long imc_kernel_launches(void) { return g_imc_launches; }
 imc_status imc_phase_times(float* ms_sources, float* ms_transport) {
   PhaseEvents& pe = phase_events();
   if (!pe.ok || !pe.recorded || !ms_sources || !ms_transport) return IMC_ERR_INVALID_ARG;
+  // waits for the tracking to end, not for the rest of the stream (the comb may still run)
+  IMC_CUDA(cudaEventSynchronize(pe.e[2]));
   IMC_CUDA(cudaEventElapsedTime(ms_sources, pe.e[0], pe.e[1]));
   IMC_CUDA(cudaEventElapsedTime(ms_transport, pe.e[1], pe.e[2]));
   return IMC_OK;

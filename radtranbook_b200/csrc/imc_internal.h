@@ -253,6 +253,7 @@ cudaError_t imc_launch_fill_boundary(const BndArgs& a, cudaStream_t s);
 
 cudaError_t imc_launch_wsum(const float* w, const int64_t* d_n, long long n_bound, double* out, cudaStream_t s);
 
+
 // ---------------------------------------------------------------------------------
 // Comb kernels
 // ---------------------------------------------------------------------------------
@@ -341,3 +342,36 @@ struct FillMgArgs {
   uint32_t id_base;            // Philox particle id of source particle k is id_base + k
 };
 cudaError_t imc_launch_fill_mg(const FillMgArgs& a, cudaStream_t s);
+
+// All of a step's sources in one launch: each job (a boundary side, a volume source or its
+// multigroup form, the census weights) owns a contiguous range of blocks and runs the
+// body of its own kernel there, so the short jobs fill the SMs beside the long one instead
+// of waiting behind it.  With wsum set, every fill adds the weights it writes and the
+// census job adds the weights of entries [0, *n_census): wsum ends as the sum of all the
+// tracked weights (what imc_launch_wsum computes after separate fills).
+constexpr int kSourceJobsMax = 8;
+enum SourceJobKind { JOB_BOUNDARY = 0, JOB_VOLUME = 1, JOB_VOLUME_MG = 2, JOB_CENSUS_WSUM = 3 };
+struct SourceJobs {
+  uint32_t rk[20];             // Philox round keys of the run seed (every job's)
+  int n_jobs;
+  int kind[kSourceJobsMax];
+  int slot[kSourceJobsMax];    // index into bnd / vol / vmg
+  int first_block[kSourceJobsMax + 1];
+  BndArgs bnd[4];
+  FillArgs vol[2];
+  FillMgArgs vmg[2];
+  const float* census_w; const int64_t* n_census;
+  double* wsum;                // NULL: the weights are not summed
+  int n_bnd, n_vol, n_vmg;
+  // appends a job of kind k (its args already in bnd / vol / vmg at slot) with `blocks` blocks
+  bool add(int k, int sl, int blocks) {
+    if (n_jobs >= kSourceJobsMax || blocks < 1) return false;
+    if (n_jobs == 0) first_block[0] = 0;
+    kind[n_jobs] = k; slot[n_jobs] = sl;
+    first_block[n_jobs + 1] = first_block[n_jobs] + blocks;
+    ++n_jobs;
+    return true;
+  }
+};
+int imc_source_blocks(long long n_bound);
+cudaError_t imc_launch_sources(const SourceJobs& j, cudaStream_t s);

@@ -24,10 +24,28 @@ namespace {
 // Offsets sampled into shared memory for the first levels of the particle -> bin search.
 constexpr int kOffSamples = 1024;
 
-__global__ void k_fill_volume(FillArgs a) {
+// Adds the block's sum of v to *out (one FP64 atomic per block).  Every thread of the block
+// calls it.
+__device__ __forceinline__ void block_add_d(double v, double* out) {
+  __shared__ double sh[32];
+  v = warp_sum_d(v);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();  // the body's own shared-memory use is over
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    double t = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+    t = warp_sum_d(t);
+    if (lane == 0 && t != 0.0) atomicAdd(out, t);
+  }
+}
+
+// The bodies below run on blocks blk of nblk (a kernel of their own, or a job of
+// k_fill_sources); the boundary body with wsum adds the weights it writes to *wsum.
+__device__ __forceinline__ void fill_volume(const uint32_t* __restrict__ rk, const FillArgs& a, int blk, int nblk) {
   const double time_scale = a.time_scale_dev ? *a.time_scale_dev : a.time_scale;  // graph replay
   const uint32_t step = a.step_dev ? *a.step_dev : a.step;
-  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long stride = (long long)nblk * blockDim.x;
   const long long n = *a.d_n, base = *a.d_base;
   // s_off[q] = off[min((q + 1) * span, nbins)]: the search for the bin of particle k (the
   // smallest o with off[o + 1] > k) first finds its span of `span` bins in shared memory,
@@ -39,7 +57,7 @@ __global__ void k_fill_volume(FillArgs a) {
   const int m = (nbins + span - 1) / span;
   for (int q = threadIdx.x; q < m; q += blockDim.x) s_off[q] = a.off[min((q + 1) * span, nbins)];
   __syncthreads();
-  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+  for (long long k = (long long)blk * blockDim.x + threadIdx.x; k < n; k += stride) {
     // order position o with off[o] <= k < off[o+1] (k < n = off[nbins], so o < nbins)
     int qlo = 0, qhi = m - 1;
     while (qlo < qhi) { const int mid = (qlo + qhi) >> 1; if (s_off[mid] > k) qhi = mid; else qlo = mid + 1; }
@@ -50,8 +68,8 @@ __global__ void k_fill_volume(FillArgs a) {
     const int oc = o - g * a.nc;
     const int i = oc / a.ny, j = oc - i * a.ny;
     const int c = i + a.nx * j;
-    const U4 r = draw_rk(a.rk, (uint32_t)k + a.id_base, 0, step, a.tag);
-    const U4 s = draw_rk(a.rk, (uint32_t)k + a.id_base, 1, step, a.tag);
+    const U4 r = draw_rk(rk, (uint32_t)k + a.id_base, 0, step, a.tag);
+    const U4 s = draw_rk(rk, (uint32_t)k + a.id_base, 1, step, a.tag);
     const double u0 = u01d(r.x), u1 = u01d(r.y), u2 = u01d(r.z), u3 = u01d(r.w);
     const double s0 = u01d(s.x), s1 = u01d(s.y);
     const double ea = a.e1[i], eb = a.e1[i + 1];
@@ -106,13 +124,15 @@ __global__ void k_fill_volume(FillArgs a) {
     if (a.group) {
       int gb = g;
       if (a.tr) {  // MG 1-D initial census: Planck group at the cell's Tr (MG_IMC/MG_IMC1D.py:557-560)
-        const U4 d = draw_rk(a.rk, (uint32_t)k + a.id_base, 2, step, a.tag);
+        const U4 d = draw_rk(rk, (uint32_t)k + a.id_base, 2, step, a.tag);
         gb = planck_group(a.tr[c], a.gedges, a.ng, a.mixcdf, s1, u01d(s.z), u01d(s.w), u01d(d.x), u01d(d.y), true);
       }
       a.group[b] = gb;
     }
   }
 }
+
+__global__ void k_fill_volume(FillArgs a) { fill_volume(a.rk, a, blockIdx.x, gridDim.x); }
 
 // Boundary energy by group: every particle of a face has the same FP32 weight wq, so the
 // tally is (count of the group) x wq.  Counts go to shared memory per block (groups below
@@ -121,7 +141,8 @@ __global__ void k_fill_volume(FillArgs a) {
 // of one FP64 atomic per particle on a handful of addresses.
 constexpr int kBndGroups = 256;
 
-__global__ void k_fill_boundary(BndArgs a) {
+__device__ __forceinline__ void fill_boundary(const uint32_t* __restrict__ rk, const BndArgs& a, int blk, int nblk,
+                                              double* wsum) {
   __shared__ unsigned s_gcnt[kBndGroups];
   const bool tally_groups = a.group && a.ng > 1;
   if (tally_groups)
@@ -129,7 +150,7 @@ __global__ void k_fill_boundary(BndArgs a) {
   __syncthreads();
   const double dt = a.dt_dev ? *a.dt_dev : a.dt;  // graph replay
   const uint32_t step = a.step_dev ? *a.step_dev : a.step;
-  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long stride = (long long)nblk * blockDim.x;
   const bool oned = (a.geom == G_SLAB || a.geom == G_SPHERE);
   const bool along2 = a.side < 2;
   const int nf = oned ? 1 : (along2 ? a.ny : a.nx);
@@ -139,9 +160,11 @@ __global__ void k_fill_boundary(BndArgs a) {
   if (n <= 0) return;  // uniform across the grid: no block passes the barrier below alone
   const double total = cdf[nf - 1];
   const float wq = (float)(total / (double)n);
-  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
-    const U4 ra = draw_rk(a.rk, (uint32_t)k + a.id_base, 0, step, TAG_BOUNDARY | (uint32_t)a.side);
-    const U4 rb = draw_rk(a.rk, (uint32_t)k + a.id_base, 1, step, TAG_BOUNDARY | (uint32_t)a.side);
+  unsigned n_mine = 0;  // particles this thread writes, each of weight wq
+  for (long long k = (long long)blk * blockDim.x + threadIdx.x; k < n; k += stride) {
+    ++n_mine;
+    const U4 ra = draw_rk(rk, (uint32_t)k + a.id_base, 0, step, TAG_BOUNDARY | (uint32_t)a.side);
+    const U4 rb = draw_rk(rk, (uint32_t)k + a.id_base, 1, step, TAG_BOUNDARY | (uint32_t)a.side);
     const double ua0 = u01d(ra.x), ua1 = u01d(ra.y), ua2 = u01d(ra.z), ua3 = u01d(ra.w);
     const double x = ua0 * total;
     int lo = 0, hi = nf;  // lower_bound(cdf, x)
@@ -197,7 +220,7 @@ __global__ void k_fill_boundary(BndArgs a) {
     if (a.group) {
       int g = 0;
       if (a.ng > 1) {
-        const U4 rd = draw_rk(a.rk, (uint32_t)k + a.id_base, 2, step, TAG_BOUNDARY | (uint32_t)a.side);
+        const U4 rd = draw_rk(rk, (uint32_t)k + a.id_base, 2, step, TAG_BOUNDARY | (uint32_t)a.side);
         g = planck_group(a.faceT[q], a.gedges, a.ng, a.mixcdf, u01d(rb.y), u01d(rb.z), u01d(rb.w), u01d(rd.x),
                          u01d(rd.y), a.below_last != 0);
         if (g < kBndGroups) atomicAdd(&s_gcnt[g], 1u);
@@ -211,23 +234,26 @@ __global__ void k_fill_boundary(BndArgs a) {
     for (int g = threadIdx.x; g < min(a.ng, kBndGroups); g += blockDim.x)
       if (s_gcnt[g]) atomicAdd(a.boundary_group + g, (double)s_gcnt[g] * (double)wq);
   }
+  if (wsum) block_add_d((double)n_mine * (double)wq, wsum);
 }
+
+__global__ void k_fill_boundary(BndArgs a) { fill_boundary(a.rk, a, blockIdx.x, gridDim.x, nullptr); }
 
 // multigroup categorical sources (MG_IMC/MG_IMC2D.py:1098-1170, 1866-1943) and the MG
 // initial census (:992-1097): cell ~ canonical CDF over cells, group ~ the cell's cumulative
 // group emission (or the Planck spectrum at tr for the IC), equal weights, uniform position.
-__global__ void k_fill_mg(FillMgArgs a) {
+__device__ __forceinline__ void fill_mg(const uint32_t* __restrict__ rk, const FillMgArgs& a, int blk, int nblk) {
   const double time_scale = a.time_scale_dev ? *a.time_scale_dev : a.time_scale;  // graph replay
   const uint32_t step = a.step_dev ? *a.step_dev : a.step;
-  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long stride = (long long)nblk * blockDim.x;
   const long long n = *a.d_n, base = *a.d_base;
   if (n <= 0) return;
   const double total = a.cdf[a.nc - 1];
   const float wq = (float)(total / (double)n);
   const bool ic = a.gcdf == nullptr;
-  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
-    const U4 ra = draw_rk(a.rk, (uint32_t)k + a.id_base, 0, step, a.tag);
-    const U4 rb = draw_rk(a.rk, (uint32_t)k + a.id_base, 1, step, a.tag);
+  for (long long k = (long long)blk * blockDim.x + threadIdx.x; k < n; k += stride) {
+    const U4 ra = draw_rk(rk, (uint32_t)k + a.id_base, 0, step, a.tag);
+    const U4 rb = draw_rk(rk, (uint32_t)k + a.id_base, 1, step, a.tag);
     const double x = u01d(ra.x) * total;
     int lo = 0, hi = a.nc;  // first c with cdf[c] > x
     while (lo < hi) { const int mid = (lo + hi) >> 1; if (a.cdf[mid] <= x) lo = mid + 1; else hi = mid; }
@@ -243,7 +269,7 @@ __global__ void k_fill_mg(FillMgArgs a) {
       for (int q = 0; q < a.ng; ++q) if (gc[q] >= y) { g = q; break; }
       up1 = u01d(ra.z); up2 = u01d(ra.w); ua = u01d(rb.x); ub = u01d(rb.y); ut = u01d(rb.z);
     } else {
-      const U4 rd = draw_rk(a.rk, (uint32_t)k + a.id_base, 2, step, a.tag);
+      const U4 rd = draw_rk(rk, (uint32_t)k + a.id_base, 2, step, a.tag);
       up1 = u01d(ra.y); up2 = u01d(ra.z); ua = u01d(ra.w); ub = u01d(rb.x); ut = 0.0;
       g = planck_group(a.tr[c], a.gedges, a.ng, a.mixcdf, u01d(rb.y), u01d(rb.z), u01d(rb.w), u01d(rd.x), u01d(rd.y));
     }
@@ -258,6 +284,63 @@ __global__ void k_fill_mg(FillMgArgs a) {
     a.t[b] = (float)(ut * time_scale);
     a.cell[b] = c;
     a.group[b] = g;
+  }
+}
+
+__global__ void k_fill_mg(FillMgArgs a) { fill_mg(a.rk, a, blockIdx.x, gridDim.x); }
+
+// The weights of the census entries [0, *n_census) and of every volume source of the job
+// table, from its plan: order position o issues off[o+1] - off[o] particles of weight
+// w[c(o)] (w[o] with bins by group); a multigroup fill issues n particles of weight
+// (float)(total / n).  With the boundary jobs' own sums, *wsum ends as the sum of the
+// weights of every tracked entry.
+__device__ __forceinline__ void census_wsum(const SourceJobs& j, int blk, int nblk) {
+  const long long stride = (long long)nblk * blockDim.x;
+  const long long t0 = (long long)blk * blockDim.x + threadIdx.x;
+  const long long n = *j.n_census;
+  double s = 0.0;
+  for (long long k = t0; k < n; k += stride) s += (double)j.census_w[k];
+  for (int v = 0; v < j.n_vol; ++v) {
+    const FillArgs& a = j.vol[v];
+    for (long long o = t0; o < a.nbins; o += stride) {
+      const long long cnt = a.off[o + 1] - a.off[o];
+      if (cnt <= 0) continue;
+      int wi = (int)o;
+      if (!a.bins_by_group) { const int i = (int)o / a.ny, jj = (int)o - i * a.ny; wi = i + a.nx * jj; }
+      s += (double)cnt * (double)a.w[wi];
+    }
+  }
+  if (t0 == 0)
+    for (int v = 0; v < j.n_vmg; ++v) {
+      const long long nm = *j.vmg[v].d_n;
+      if (nm > 0) s += (double)nm * (double)(float)(j.vmg[v].cdf[j.vmg[v].nc - 1] / (double)nm);
+    }
+  block_add_d(s, j.wsum);
+}
+
+// Source jobs in one launch: block b runs the job whose range holds b.  KINDS (bits
+// 1 << JOB_*) selects the bodies compiled into an instance, so the volume fills keep the
+// registers of their own kernel instead of the largest of all the bodies.
+template <int KINDS>
+__global__ void __launch_bounds__(256) k_fill_sources(const __grid_constant__ SourceJobs j) {
+  int q = 0;
+  while (q + 1 < j.n_jobs && (int)blockIdx.x >= j.first_block[q + 1]) ++q;
+  const int blk = (int)blockIdx.x - j.first_block[q];
+  const int nblk = j.first_block[q + 1] - j.first_block[q];
+  constexpr bool VOL = KINDS & (1 << JOB_VOLUME), VMG = KINDS & (1 << JOB_VOLUME_MG);
+  constexpr bool BND = KINDS & (1 << JOB_BOUNDARY), CEN = KINDS & (1 << JOB_CENSUS_WSUM);
+  // one case per (kind, slot): constant indices keep every argument a direct operand of
+  // the parameter block (a run-time index would load them into registers)
+  switch (j.kind[q] * 4 + j.slot[q]) {
+    case JOB_VOLUME * 4 + 0: if (VOL) fill_volume(j.rk, j.vol[0], blk, nblk); break;
+    case JOB_VOLUME * 4 + 1: if (VOL) fill_volume(j.rk, j.vol[1], blk, nblk); break;
+    case JOB_VOLUME_MG * 4 + 0: if (VMG) fill_mg(j.rk, j.vmg[0], blk, nblk); break;
+    case JOB_VOLUME_MG * 4 + 1: if (VMG) fill_mg(j.rk, j.vmg[1], blk, nblk); break;
+    case JOB_BOUNDARY * 4 + 0: if (BND) fill_boundary(j.rk, j.bnd[0], blk, nblk, j.wsum); break;
+    case JOB_BOUNDARY * 4 + 1: if (BND) fill_boundary(j.rk, j.bnd[1], blk, nblk, j.wsum); break;
+    case JOB_BOUNDARY * 4 + 2: if (BND) fill_boundary(j.rk, j.bnd[2], blk, nblk, j.wsum); break;
+    case JOB_BOUNDARY * 4 + 3: if (BND) fill_boundary(j.rk, j.bnd[3], blk, nblk, j.wsum); break;
+    default: if (CEN) census_wsum(j, blk, nblk); break;
   }
 }
 
@@ -296,6 +379,25 @@ cudaError_t imc_launch_fill_boundary(const BndArgs& a, cudaStream_t s) {
   if (a.n_bound <= 0) return cudaSuccess;
   ++g_imc_launches;
   k_fill_boundary<<<grid_for(a.n_bound, 256), 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+int imc_source_blocks(long long n_bound) { return grid_for(n_bound, 256); }
+
+cudaError_t imc_launch_sources(const SourceJobs& j, cudaStream_t s) {
+  if (j.n_jobs <= 0) return cudaSuccess;
+  if (j.n_jobs > kSourceJobsMax) return cudaErrorInvalidValue;
+  int kinds = 0;
+  for (int q = 0; q < j.n_jobs; ++q) kinds |= 1 << j.kind[q];
+  const int grid = j.first_block[j.n_jobs];
+  constexpr int kVol = 1 << JOB_VOLUME, kVmg = 1 << JOB_VOLUME_MG;
+  constexpr int kAux = (1 << JOB_BOUNDARY) | (1 << JOB_CENSUS_WSUM);
+  ++g_imc_launches;
+  // an instance per kind of fill: the gray and the multigroup volume fills never share a step
+  if (kinds == kVol) k_fill_sources<kVol><<<grid, 256, 0, s>>>(j);
+  else if (kinds == kVmg) k_fill_sources<kVmg><<<grid, 256, 0, s>>>(j);
+  else if ((kinds & ~kAux) == 0) k_fill_sources<kAux><<<grid, 256, 0, s>>>(j);
+  else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
 

@@ -22,6 +22,11 @@ A_RAD = 0.01372
 C_LIGHT = 29.98
 
 
+# the current stream's raw handle without building a torch Stream object (which costs a few
+# microseconds of the host time a step leaves the device idle); the public call otherwise
+_RAW_STREAM = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+
+
 def _ptr(t: torch.Tensor | None) -> int | None:
     return None if t is None else t.data_ptr()
 
@@ -158,6 +163,7 @@ class Engine:
         self.bank = Bank(capacity, dev, mg)
         self.spare = Bank(capacity, dev, mg)
         self.ws = torch.empty(0, dtype=torch.uint8, device=dev)
+        self._ws_need = (None, 0)  # (capacity, event form) -> workspace bytes, of the last query
         self.launch = dict(block_size=256, blocks_per_sm=4, chunk=512, smem_cells=0)
         self._last_transport = None
         # particle partition over ranks (radtranbook_b200.partition): this rank's Philox id
@@ -201,11 +207,19 @@ class Engine:
 
     # ------------------------------------------------------------------ helpers
     def _stream(self) -> int:
+        if _RAW_STREAM is not None:
+            idx = self.device.index
+            return _RAW_STREAM(torch.cuda.current_device() if idx is None else idx)
         return torch.cuda.current_stream(self.device).cuda_stream
 
     def _ws(self, capacity: int) -> tuple[int, int]:
-        size = self.lib.imc_workspace_bytes_event if self.launch.get("event_based") else self.lib.imc_workspace_bytes
-        need = int(size(ctypes.byref(self.cmesh), int(capacity)))
+        key = (int(capacity), bool(self.launch.get("event_based")))
+        if self._ws_need[0] == key:
+            need = self._ws_need[1]
+        else:
+            size = self.lib.imc_workspace_bytes_event if key[1] else self.lib.imc_workspace_bytes
+            need = int(size(ctypes.byref(self.cmesh), key[0]))
+            self._ws_need = (key, need)
         if self.ws.numel() < need:
             self.ws = torch.empty(int(need * 1.25) + 4096, dtype=torch.uint8, device=self.device)
         return self.ws.data_ptr(), self.ws.numel()

@@ -195,8 +195,10 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, mesh, energy_
         state._e.add_(eng.disc.view(G, I).sum(0) / eng.vol)
     Tn = evaluate(inv_eos, state._e, lambda: _host_copy(state._e), like, **_staged(state, "T_new", I))
     state._T.copy_(Tn.reshape(-1))
+    copies = state.host_copies()
+    ms_src, ms_tr = eng.phase_times()  # waits for the tracking only (the comb still runs)
     try:
-        sm = eng.fetch(state.host_copies())
+        sm = eng.fetch(copies)
     except _lib.ImcError as ex:
         if ex.status == 3:
             raise AssertionError("non-finite or non-positive material state") from ex
@@ -220,8 +222,8 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, mesh, energy_
     comb_disc = tot["comb_before"] - rad
     if mode == "material":
         internal += comb_disc
-    boundary_emission = float(tot["e_side"].sum())
-    boundary_loss = float(tot["escaped"].sum())
+    boundary_emission = tot["e_side_total"]
+    boundary_loss = tot["escaped_total"]
     source_emission = tot["source_emission"]
     n_boundary = int(sum(sm.n_side))
     if dist is not None:
@@ -236,7 +238,6 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, mesh, energy_
     state.previous_total_energy = total
     state.count += 1
     stats = tot["stats"]
-    ms_src, ms_tr = eng.phase_times()
     n_tr = tot["n_bank"]
     ev = int(stats[_lib.STAT_EVENTS])
     t_end = _time.perf_counter()

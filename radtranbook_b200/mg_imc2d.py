@@ -304,6 +304,7 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
     # every reported field in the reference's layout in one device buffer (one kernel), then
     # one copy into a fresh pinned buffer that the host arrays view
     hb = _report_buffers(state, eng, eng.mg_report_fields(state._e, state._T, state._Tr))
+    ms_src, ms_tr = eng.phase_times()  # waits for the tracking only (the comb still runs)
     try:
         sm = eng.fetch([(eng.report_dev, hb["all"])])
     except _lib.ImcError as ex:
@@ -335,8 +336,8 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
     comb_disc = tot["comb_before"] - rad
     if conserve_comb_energy:
         internal += comb_disc
-    boundary_emission = float(tot["e_side"].sum())
-    boundary_loss = float(tot["escaped"].sum())
+    boundary_emission = tot["e_side_total"]
+    boundary_loss = tot["escaped_total"]
     source_emission = tot["source_emission"]
     total = internal + rad
     dE = total - state.previous_total_energy
@@ -357,7 +358,6 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
     state.__dict__["radiation_energy_by_group"] = rad_group_pre
     state.__dict__["radiation_energy_by_group_postcomb"] = rad_group_post
     stats = tot["stats"]
-    ms_src, ms_tr = eng.phase_times()
     t_end = _time.perf_counter()
     n_tr = tot["n_bank"]
     ev = int(stats[_lib.STAT_EVENTS])

@@ -82,12 +82,20 @@ def summary_totals(dist, sm, n_particles: int, device) -> dict:
     with one all-reduce: radiation energy after the comb ('rad') and before ('comb_before'),
     boundary emission and escape by side, fixed-source and emission energy, tracked weight,
     census entries after the comb ('n_particles'), tracked entries ('n_bank') and the event
-    statistics."""
+    statistics.  e_side_total / escaped_total: the sums over the sides."""
+    if dist is None or dist.get_world_size() == 1:
+        # one rank: the summary's own fields (this runs in the host time between two steps)
+        return {"rad": sm.comb_after, "comb_before": sm.comb_before, "e_side": np.array(sm.e_side),
+                "escaped": np.array(sm.escaped), "e_side_total": sum(sm.e_side), "escaped_total": sum(sm.escaped),
+                "source_emission": sm.source_emission, "emission_total": sm.emission_total,
+                "weight_sum": sm.weight_sum, "n_particles": int(n_particles), "n_bank": int(sm.n_bank),
+                "stats": np.array(sm.stats, dtype=np.int64)}
     vals = ([float(sm.comb_after), float(sm.comb_before)] + [float(x) for x in sm.e_side]
             + [float(x) for x in sm.escaped]
             + [float(sm.source_emission), float(sm.emission_total), float(sm.weight_sum), float(n_particles),
                float(sm.n_bank)] + [float(x) for x in sm.stats])
     v = sum_scalars(dist, vals, device)
     return {"rad": v[0], "comb_before": v[1], "e_side": np.array(v[2:6]), "escaped": np.array(v[6:10]),
+            "e_side_total": sum(v[2:6]), "escaped_total": sum(v[6:10]),
             "source_emission": v[10], "emission_total": v[11], "weight_sum": v[12], "n_particles": int(v[13]),
             "n_bank": int(v[14]), "stats": np.array(v[15:], dtype=np.int64)}
