@@ -30,6 +30,8 @@ using namespace imcblk;
 // Per-cell part of the plan, one thread per cell: Fleck factor, absorption / effective
 // scatter tables, emission energy, linear tilt constants, FP32 edges.
 __global__ void k_plan_cells(PlanArgs a) {
+  pdl_wait();     // the previous kernel of the stream has completed
+  pdl_trigger();  // the next one may be scheduled
   const double dt = a.dt_dev ? *a.dt_dev : a.dt;  // device-resident step length (graph replay)
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c <= a.nx) a.e1f[c] = (float)a.e1[c];
@@ -170,6 +172,8 @@ __device__ double face_cdf_serial(const double* Ef, double* cdf, int nf) {
 }
 
 __global__ void __launch_bounds__(NT) k_plan(PlanArgs a) {
+  pdl_wait();     // the previous kernel of the stream has completed
+  pdl_trigger();  // the next one may be scheduled
   const double dt = a.dt_dev ? *a.dt_dev : a.dt;  // device-resident step length (graph replay)
   __shared__ double red[NT];
   __shared__ long long sh[NT];
@@ -276,6 +280,8 @@ __global__ void __launch_bounds__(NT) k_ic_plan(IcArgs a) {
 }
 
 __global__ void k_material(MatArgs a) {
+  pdl_wait();     // the previous kernel of the stream has completed
+  pdl_trigger();  // the next one may be scheduled
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= a.nc) return;
   double dep = 0.0, si = 0.0;
@@ -288,6 +294,8 @@ __global__ void k_material(MatArgs a) {
 // k_material, then T = e / cv_eos and the law's opacity of every group and cv at that T for
 // the next step.  e and tr are k_material's sums (same order, so the same bits).
 __global__ void k_material_law(MatArgs a, imc_material_law law, double* T, double* sigma_next, double* cv_next) {
+  pdl_wait();     // the previous kernel of the stream has completed
+  pdl_trigger();  // the next one may be scheduled
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= a.nc) return;
   double dep = 0.0, si = 0.0;
@@ -316,6 +324,8 @@ __global__ void k_material_law(MatArgs a, imc_material_law law, double* T, doubl
 
 // Single block: the canonical total of the census energy and the comb mode.
 __global__ void __launch_bounds__(NT) k_comb_plan(CombPlanArgs a) {
+  pdl_wait();     // the previous kernel of the stream has completed
+  pdl_trigger();  // the next one may be scheduled
   __shared__ double red[NT];
   const double E = block_canon_sum<16>(a.ecen, a.nb, red);
   // MG_IMC/MG_IMC1D.py:1194-1200: Nmax = 0 never combs; Nmax < 0 combs once |Nmax| entries live
@@ -325,6 +335,8 @@ __global__ void __launch_bounds__(NT) k_comb_plan(CombPlanArgs a) {
 
 // Wide: the comb weight of every bin, ecen / max(1, rint(Nmax ecen / E)).
 __global__ void k_comb_weights(CombPlanArgs a) {
+  pdl_wait();     // the previous kernel of the stream has completed
+  pdl_trigger();  // the next one may be scheduled
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= a.nb) return;
   const double E = a.sum->comb_before;
@@ -338,6 +350,8 @@ __global__ void k_comb_weights(CombPlanArgs a) {
 
 // Zero the regions of a ZeroList (one launch for a step's accumulators).
 __global__ void k_zero(ZeroList z) {
+  pdl_wait();     // the previous kernel of the stream has completed
+  pdl_trigger();  // the next one may be scheduled
   const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x, stride = (size_t)gridDim.x * blockDim.x;
   for (int r = 0; r < z.n; ++r) {
     unsigned long long* q = static_cast<unsigned long long*>(z.p[r]);
@@ -347,6 +361,8 @@ __global__ void k_zero(ZeroList z) {
 }
 
 __global__ void __launch_bounds__(NT) k_canon_eV(const double* e, const double* vol, int nc, double* out) {
+  pdl_wait();     // the previous kernel of the stream has completed
+  pdl_trigger();  // the next one may be scheduled
   __shared__ double red[NT];
   const int t = threadIdx.x;
   double s = 0.0;
@@ -361,8 +377,8 @@ __global__ void __launch_bounds__(NT) k_canon_eV(const double* e, const double* 
 
 cudaError_t imc_launch_plan(const PlanArgs& a, cudaStream_t s) {
   g_imc_launches += 2;
-  k_plan_cells<<<(std::max(a.nc, std::max(a.nx, a.ny) + 1) + 255) / 256, 256, 0, s>>>(a);
-  k_plan<<<1, NT, 0, s>>>(a);
+  IMC_LAUNCH_PDL(k_plan_cells, (std::max(a.nc, std::max(a.nx, a.ny) + 1) + 255) / 256, 256, 0, s, a);
+  IMC_LAUNCH_PDL(k_plan, 1, NT, 0, s, a);
   return cudaGetLastError();
 }
 cudaError_t imc_launch_ic_plan(const IcArgs& a, cudaStream_t s) {
@@ -372,13 +388,13 @@ cudaError_t imc_launch_ic_plan(const IcArgs& a, cudaStream_t s) {
 }
 cudaError_t imc_launch_material(const MatArgs& a, cudaStream_t s) {
   ++g_imc_launches;
-  k_material<<<(a.nc + 255) / 256, 256, 0, s>>>(a);
+  IMC_LAUNCH_PDL(k_material, (a.nc + 255) / 256, 256, 0, s, a);
   return cudaGetLastError();
 }
 cudaError_t imc_launch_material_law(const MatArgs& a, const imc_material_law& law, double* T, double* sigma_next,
                                     double* cv_next, cudaStream_t s) {
   ++g_imc_launches;
-  k_material_law<<<(a.nc + 255) / 256, 256, 0, s>>>(a, law, T, sigma_next, cv_next);
+  IMC_LAUNCH_PDL(k_material_law, (a.nc + 255) / 256, 256, 0, s, a, law, T, sigma_next, cv_next);
   return cudaGetLastError();
 }
 cudaError_t imc_launch_zero(const ZeroList& z, cudaStream_t s) {
@@ -387,18 +403,20 @@ cudaError_t imc_launch_zero(const ZeroList& z, cudaStream_t s) {
   if (most == 0) return cudaSuccess;
   ++g_imc_launches;
   const unsigned blocks = (unsigned)std::min<unsigned long long>(1184ull, (most + 255) / 256);
-  k_zero<<<blocks, 256, 0, s>>>(z);
+  IMC_LAUNCH_PDL(k_zero, blocks, 256, 0, s, z);
   return cudaGetLastError();
 }
 cudaError_t imc_launch_comb_plan(const CombPlanArgs& a, cudaStream_t s) {
   g_imc_launches += 2;
-  k_comb_plan<<<1, NT, 0, s>>>(a);
-  if (a.nb > 0) k_comb_weights<<<(a.nb + 255) / 256, 256, 0, s>>>(a);
+  IMC_LAUNCH_PDL(k_comb_plan, 1, NT, 0, s, a);
+  if (a.nb > 0) IMC_LAUNCH_PDL(k_comb_weights, (a.nb + 255) / 256, 256, 0, s, a);
   return cudaGetLastError();
 }
 // The multigroup step's reported fields in the reference's (nx, ny) order, one output each:
 // si / c and after / V by group, then e, T, Tr, then the two group sums (imc_mg_report_fields).
 __global__ void k_mg_report(ReportArgs a) {
+  pdl_wait();     // the previous kernel of the stream has completed
+  pdl_trigger();  // the next one may be scheduled
   const long long nc = (long long)a.nx * a.ny, gnc = nc * a.ng;
   const long long n = 2 * gnc + 3 * nc + 2 * a.ng;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
@@ -424,13 +442,13 @@ cudaError_t imc_launch_mg_report(const ReportArgs& a, cudaStream_t s) {
   ++g_imc_launches;
   const long long n = 2LL * a.nx * a.ny * a.ng + 3LL * a.nx * a.ny + 2LL * a.ng;
   const unsigned blocks = (unsigned)std::min<long long>(4736LL, (n + 255) / 256);
-  k_mg_report<<<blocks, 256, 0, s>>>(a);
+  IMC_LAUNCH_PDL(k_mg_report, blocks, 256, 0, s, a);
   return cudaGetLastError();
 }
 
 cudaError_t imc_launch_canon_sum_eV(const double* e, const double* vol, int nc, double* out, cudaStream_t s) {
   ++g_imc_launches;
-  k_canon_eV<<<1, NT, 0, s>>>(e, vol, nc, out);
+  IMC_LAUNCH_PDL(k_canon_eV, 1, NT, 0, s, e, vol, nc, out);
   return cudaGetLastError();
 }
 
@@ -572,6 +590,8 @@ __device__ void block_planck_edges(const double* T, const double* gedges, int G,
 // fractions, Planck-mean opacity, Fleck factor and emission by group (each cell's numbers
 // depend on that cell alone, so the result is the single-block loop's).
 __global__ void __launch_bounds__(256) k_plan_mg_cells(PlanMgArgs a, int cb) {
+  pdl_wait();     // the previous kernel of the stream has completed
+  pdl_trigger();  // the next one may be scheduled
   extern __shared__ double plan_sh[];
   const double dt = a.dt_dev ? *a.dt_dev : a.dt;  // device-resident step length (graph replay)
   const int nc = a.nc, G = a.ng;
@@ -638,6 +658,8 @@ __global__ void __launch_bounds__(256) k_plan_mg_cells(PlanMgArgs a, int cb) {
 
 // Single-block part: canonical prefix sums and totals, counts, boundary faces, bank layout.
 __global__ void __launch_bounds__(NT) k_plan_mg(PlanMgArgs a) {
+  pdl_wait();     // the previous kernel of the stream has completed
+  pdl_trigger();  // the next one may be scheduled
   const double dt = a.dt_dev ? *a.dt_dev : a.dt;  // device-resident step length (graph replay)
   __shared__ double sh[NT];
   const int t = threadIdx.x;
@@ -708,6 +730,8 @@ __global__ void __launch_bounds__(NT) k_plan_mg(PlanMgArgs a) {
 // Per-shell part of the sphere plan, one thread per shell over a wide grid (each shell's
 // numbers depend on that shell alone, so the result is the single-block loop's).
 __global__ void __launch_bounds__(256) k_plan_mg1d_cells(PlanMgArgs a, int cb) {
+  pdl_wait();     // the previous kernel of the stream has completed
+  pdl_trigger();  // the next one may be scheduled
   extern __shared__ double plan_sh[];
   const double dt = a.dt_dev ? *a.dt_dev : a.dt;  // device-resident step length (graph replay)
   const int nc = a.nc, G = a.ng;
@@ -759,6 +783,8 @@ __global__ void __launch_bounds__(256) k_plan_mg1d_cells(PlanMgArgs a, int cb) {
 // Single-block part of the sphere plan: canonical totals, stratified counts and scans,
 // fixed source, boundary faces, bank layout.
 __global__ void __launch_bounds__(NT) k_plan_mg1d(PlanMgArgs a) {
+  pdl_wait();     // the previous kernel of the stream has completed
+  pdl_trigger();  // the next one may be scheduled
   const double dt = a.dt_dev ? *a.dt_dev : a.dt;  // device-resident step length (graph replay)
   __shared__ double red[NT];
   __shared__ long long sh[NT];
@@ -876,7 +902,7 @@ cudaError_t launch_plan_cells(K kernel, const PlanMgArgs& a, cudaStream_t s) {
     if (e != cudaSuccess) return e;
   }
   const int blocks = (a.nc + cb - 1) / cb;
-  kernel<<<blocks, 256, smem, s>>>(a, cb);
+  IMC_LAUNCH_PDL(kernel, blocks, 256, smem, s, a, cb);
   return cudaSuccess;
 }
 
@@ -884,7 +910,7 @@ cudaError_t imc_launch_plan_mg(const PlanMgArgs& a, cudaStream_t s) {
   g_imc_launches += 2;
   const cudaError_t e = launch_plan_cells(k_plan_mg_cells, a, s);
   if (e != cudaSuccess) return e;
-  k_plan_mg<<<1, NT, 0, s>>>(a);
+  IMC_LAUNCH_PDL(k_plan_mg, 1, NT, 0, s, a);
   return cudaGetLastError();
 }
 
@@ -892,7 +918,7 @@ cudaError_t imc_launch_plan_mg1d(const PlanMgArgs& a, cudaStream_t s) {
   g_imc_launches += 2;
   const cudaError_t e = launch_plan_cells(k_plan_mg1d_cells, a, s);
   if (e != cudaSuccess) return e;
-  k_plan_mg1d<<<1, NT, 0, s>>>(a);
+  IMC_LAUNCH_PDL(k_plan_mg1d, 1, NT, 0, s, a);
   return cudaGetLastError();
 }
 

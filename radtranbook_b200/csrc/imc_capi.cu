@@ -6,6 +6,7 @@
 // step summary, and the host supplies only upper bounds for grid sizes.  The synchronous
 // entry points wrap the asynchronous ones with one host<->device round trip each.
 #include <algorithm>
+#include <cstdlib>
 #include <cstddef>
 #include <cstring>
 #include <mutex>
@@ -13,6 +14,10 @@
 #include "imc_internal.h"
 
 unsigned long long g_imc_launches = 0;
+bool g_imc_pdl = [] {
+  const char* e = std::getenv("IMCB200_PDL");
+  return !(e && e[0] == '0');
+}();
 
 namespace {
 

@@ -54,6 +54,8 @@ constexpr int EBINS = 1024;     // shared-memory bins per block
 // Each block sums a contiguous run of ECH entries into its shared bins (warp groups first),
 // then adds one value per distinct bin to ecen.
 __global__ void __launch_bounds__(256) k_comb_ecen(CombArgs a) {
+  pdl_wait();     // the previous kernel of the stream has completed
+  pdl_trigger();  // the next one may be scheduled
   __shared__ BlockBins<EBINS> t;
   __shared__ WarpStage stages[8];
   WarpStage* st = stages + (threadIdx.x >> 5);
@@ -101,6 +103,8 @@ __device__ __forceinline__ int comb_copies(const CombArgs& a, float wf, int bk, 
 }
 
 __global__ void __launch_bounds__(CNT_T) k_comb_count(CombArgs a) {
+  pdl_wait();     // the previous kernel of the stream has completed
+  pdl_trigger();  // the next one may be scheduled
   const uint32_t step = a.step_dev ? *a.step_dev : a.step;  // graph replay
   __shared__ unsigned sh[CNT_T / 32];
   __shared__ BlockCounts<CNT_SLOTS> t;
@@ -170,6 +174,8 @@ __global__ void __launch_bounds__(CNT_T) k_comb_count(CombArgs a) {
 // exclusive scan of nblk block totals in place (blk[nblk] = total), single block
 __global__ void __launch_bounds__(1024) k_comb_scan(long long* blk, long long nblk, long long out_capacity,
                                                     imc_step_summary* sum) {
+  pdl_wait();     // the previous kernel of the stream has completed
+  pdl_trigger();  // the next one may be scheduled
   __shared__ long long sh[1024];
   const int t = threadIdx.x;
   const long long per = (nblk + 1023) / 1024;
@@ -200,6 +206,8 @@ __global__ void __launch_bounds__(1024) k_comb_scan(long long* blk, long long nb
 // search there and gathers the entry's fields (cached: a tile's entries are few), so the
 // output stores are contiguous across the warp.
 __global__ void __launch_bounds__(1024) k_comb_scatter(CombArgs a) {
+  pdl_wait();     // the previous kernel of the stream has completed
+  pdl_trigger();  // the next one may be scheduled
   __shared__ int incl[TILE];
   __shared__ int sh[32];
   const long long tile0 = (long long)blockIdx.x * TILE;
@@ -251,6 +259,8 @@ __global__ void __launch_bounds__(1024) k_comb_scatter(CombArgs a) {
 }
 
 __global__ void k_comb_disc(CombArgs a) {
+  pdl_wait();     // the previous kernel of the stream has completed
+  pdl_trigger();  // the next one may be scheduled
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   double after = 0.0;
   if (b < a.nb) {
@@ -268,7 +278,7 @@ __global__ void k_comb_disc(CombArgs a) {
 cudaError_t imc_launch_comb_ecen(const CombArgs& a, cudaStream_t s) {
   if (a.n_bound <= 0) return cudaSuccess;
   ++g_imc_launches;
-  k_comb_ecen<<<(unsigned)((a.n_bound + ECH - 1) / ECH), 256, 0, s>>>(a);
+  IMC_LAUNCH_PDL(k_comb_ecen, (unsigned)((a.n_bound + ECH - 1) / ECH), 256, 0, s, a);
   return cudaGetLastError();
 }
 
@@ -276,12 +286,12 @@ cudaError_t imc_launch_comb_count(const CombArgs& a, cudaStream_t s) {
   const long long nblk = (a.n_bound + TILE - 1) / TILE;
   if (nblk > 0) {
     ++g_imc_launches;
-    k_comb_count<<<(unsigned)nblk, CNT_T, 0, s>>>(a);
+    IMC_LAUNCH_PDL(k_comb_count, (unsigned)nblk, CNT_T, 0, s, a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
   ++g_imc_launches;
-  k_comb_scan<<<1, 1024, 0, s>>>(a.blk, nblk, a.out_capacity, a.sum);
+  IMC_LAUNCH_PDL(k_comb_scan, 1, 1024, 0, s, a.blk, nblk, a.out_capacity, a.sum);
   return cudaGetLastError();
 }
 
@@ -289,11 +299,11 @@ cudaError_t imc_launch_comb_scatter(const CombArgs& a, cudaStream_t s) {
   const long long nblk = (a.n_bound + TILE - 1) / TILE;
   if (nblk > 0) {
     ++g_imc_launches;
-    k_comb_scatter<<<(unsigned)nblk, 1024, 0, s>>>(a);
+    IMC_LAUNCH_PDL(k_comb_scatter, (unsigned)nblk, 1024, 0, s, a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
   ++g_imc_launches;
-  k_comb_disc<<<(a.nb + 255) / 256, 256, 0, s>>>(a);
+  IMC_LAUNCH_PDL(k_comb_disc, (a.nb + 255) / 256, 256, 0, s, a);
   return cudaGetLastError();
 }

@@ -285,6 +285,40 @@ cudaError_t imc_launch_philox(const uint32_t* ctr, uint32_t k0, uint32_t k1, uin
 
 extern unsigned long long g_imc_launches;
 
+// Programmatic dependent launch for the kernels of a step's chain: a kernel launched with
+// launch_pdl may be scheduled while the previous kernel of its stream drains, so its launch
+// latency hides behind that kernel's tail.  Such a kernel calls pdl_wait() before it touches
+// global memory (griddepcontrol.wait returns once the previous kernel has completed and its
+// writes are visible: a hardware dependency, no spin) and pdl_trigger() to let its own
+// successor be scheduled.  Without the attribute both are no-ops.  IMCB200_PDL=0 in the
+// environment launches without it.
+extern bool g_imc_pdl;
+
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t s,
+                       Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = g_imc_pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<Args&&>(args)...);
+}
+// launch_pdl(...) in a function returning cudaError_t: returns its error
+#define IMC_LAUNCH_PDL(...)                                     \
+  do {                                                          \
+    const cudaError_t e_pdl_ = launch_pdl(__VA_ARGS__);         \
+    if (e_pdl_ != cudaSuccess) return e_pdl_;                   \
+  } while (0)
+
 // ---------------------------------------------------------------------------------
 // Multigroup planning and sources
 // ---------------------------------------------------------------------------------

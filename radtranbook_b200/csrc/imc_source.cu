@@ -323,6 +323,8 @@ __device__ __forceinline__ void census_wsum(const SourceJobs& j, int blk, int nb
 // registers of their own kernel instead of the largest of all the bodies.
 template <int KINDS>
 __global__ void __launch_bounds__(256) k_fill_sources(const __grid_constant__ SourceJobs j) {
+  pdl_wait();     // the previous kernel of the stream has completed
+  pdl_trigger();  // the next one may be scheduled
   int q = 0;
   while (q + 1 < j.n_jobs && (int)blockIdx.x >= j.first_block[q + 1]) ++q;
   const int blk = (int)blockIdx.x - j.first_block[q];
@@ -394,9 +396,9 @@ cudaError_t imc_launch_sources(const SourceJobs& j, cudaStream_t s) {
   constexpr int kAux = (1 << JOB_BOUNDARY) | (1 << JOB_CENSUS_WSUM);
   ++g_imc_launches;
   // an instance per kind of fill: the gray and the multigroup volume fills never share a step
-  if (kinds == kVol) k_fill_sources<kVol><<<grid, 256, 0, s>>>(j);
-  else if (kinds == kVmg) k_fill_sources<kVmg><<<grid, 256, 0, s>>>(j);
-  else if ((kinds & ~kAux) == 0) k_fill_sources<kAux><<<grid, 256, 0, s>>>(j);
+  if (kinds == kVol) IMC_LAUNCH_PDL(k_fill_sources<kVol>, grid, 256, 0, s, j);
+  else if (kinds == kVmg) IMC_LAUNCH_PDL(k_fill_sources<kVmg>, grid, 256, 0, s, j);
+  else if ((kinds & ~kAux) == 0) IMC_LAUNCH_PDL(k_fill_sources<kAux>, grid, 256, 0, s, j);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }

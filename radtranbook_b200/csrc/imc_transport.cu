@@ -334,6 +334,8 @@ __device__ __forceinline__ void history_event(const TrackArgs& a, Hist& h, EvOut
 // dozen cells the wave occupies, which serialise in the L2.
 template <int GEOM, bool SMEM_CELLS, bool MG, bool CF, bool SMEM_TALLY>
 __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
+  pdl_wait();     // the previous kernel of the stream has completed
+  pdl_trigger();  // the next one may be scheduled
   const float dtk = a.dt_dev ? (float)*a.dt_dev : a.dt;  // graph replay: step length and Philox
   const uint32_t stepk = a.step_dev ? *a.step_dev : a.step;  // step counter from device memory
   extern __shared__ __align__(16) unsigned char smem[];
@@ -542,7 +544,7 @@ cudaError_t launch_one(const TrackArgs& a, int block, int grid, cudaStream_t s) 
                                          (int)sh);
     if (e != cudaSuccess) return e;
   }
-  k_track<GEOM, SM, MG, CF, ST><<<grid, block, sh, s>>>(a);
+  IMC_LAUNCH_PDL(k_track<GEOM, SM, MG, CF, ST>, grid, block, sh, s, a);
   return cudaGetLastError();
 }
 
@@ -733,6 +735,8 @@ cudaError_t launch_event_geom(const TrackArgs& a, int geom, const EventScratch& 
 // its deposited energy times it (the sum over the cell's flights of (w - w') / (sigma_a V dt));
 // < 0 is -1/(V dt), the cell has no absorption and si holds the raw sum of w*s.
 __global__ void k_tally_finalize(TrackArgs a) {
+  pdl_wait();     // the previous kernel of the stream has completed
+  pdl_trigger();  // the next one may be scheduled
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   const double W = *a.wsum;
   const int ncg = a.nc * a.ng;
@@ -751,7 +755,7 @@ __global__ void k_tally_finalize(TrackArgs a) {
 cudaError_t imc_launch_tally_finalize(const TrackArgs& a, cudaStream_t s) {
   ++g_imc_launches;
   const int n = a.nc * a.ng + 4 + a.ng;
-  k_tally_finalize<<<(n + 255) / 256, 256, 0, s>>>(a);
+  IMC_LAUNCH_PDL(k_tally_finalize, (n + 255) / 256, 256, 0, s, a);
   return cudaGetLastError();
 }
 
