@@ -93,6 +93,26 @@ class GrayState:
         object.__setattr__(self, "_hpin", pin)
         return [(src, pin)]
 
+    def host_copies_early(self) -> "torch.cuda.Event":
+        """Queue the copy of host_copies() on a side stream of the engine, after the work the
+        current stream holds so far (the material update), so that it runs beside the work
+        queued next (the comb).  Returns the side stream's event after the copy: the caller
+        synchronises the host on it before reading the buffer and before the step returns
+        (nothing that changes e, T or Tr is queued before then)."""
+        eng = self._engine
+        side = eng.__dict__.get("_side_stream")
+        if side is None:
+            side = torch.cuda.Stream(device=eng.device)
+            eng.__dict__["_side_stream"] = side
+        main = torch.cuda.current_stream(eng.device)
+        side.wait_stream(main)
+        with torch.cuda.stream(side):
+            for d, h in self.host_copies():
+                h.copy_(d, non_blocking=True)
+        done = torch.cuda.Event()
+        done.record(side)
+        return done
+
     def take_host_copies(self, publish: bool = True) -> list:
         """Host mirrors of e, T and Tr from the buffer filled by the last fetch (no device
         access); publish=False leaves publishing them (with other arrays) to the caller, which
@@ -298,6 +318,9 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
     else:
         state.__dict__.pop("_law_next", None)
         eng.material_update(state._e, state._Tr)
+    # with the device law (and no comb discrepancy booked into e), e, T and Tr are final now:
+    # their copy to the host runs on a side stream beside the comb
+    early = state.host_copies_early() if law is not None and not conserve_comb_energy else None
     e_ready = None
     if law is None and not conserve_comb_energy and not is_device(inv_eos):
         e_pin = _pinned(state, "e_mid", eng.nc)
@@ -322,7 +345,7 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
     else:
         Tn = evaluate(inv_eos, state.grid(state._e), lambda: _host_copy(state.grid(state._e)), like)
         state._T.copy_(state.flat(Tn))
-    copies = state.host_copies()
+    copies = state.host_copies() if early is None else ()
     # the phase times wait for the tracking only: read while the comb still runs on the device
     ms_src, ms_tr = eng.phase_times()
     try:
@@ -331,6 +354,8 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
         if ex.status == 3:
             raise AssertionError("Fleck factor out of bounds / non-positive temperature in material state") from ex
         raise
+    if early is not None:
+        early.synchronize()  # done long before the comb
     t_post = _time.perf_counter()
     pre_comb = eng.spare  # the tracked (pre-comb) bank after the swap
     if not use_scalar_intensity_Tr:
