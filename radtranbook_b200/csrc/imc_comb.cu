@@ -3,11 +3,11 @@
 //
 //   1. ecen[b]  = sum of live weights per bin (cell, or cell + nc*group)      k_comb_ecen
 //   2. ew[b]    = ecen / max(1, rint(Nmax ecen / E))                          k_comb_plan
-//   3. n_k      = floor(w_k / ew[b] + xi_k), xi from Philox (k, 0, step, TAG_COMB);
-//      per-block totals                                                       k_comb_count
+//   3. n_k      = floor(w_k / ew[b] + xi_k), xi word k % 4 of Philox block
+//      (k / 4, 1, step, TAG_COMB); per-block totals                          k_comb_count
 //   4. exclusive scan of block totals                                         k_comb_scan
-//   5. copies written in bank order (block-local scan + block offset; one
-//      thread per copy)                                                       k_comb_scatter
+//   5. copies written in bank order (block-local scan + block offset; entries
+//      staged in shared memory, one thread per output copy)                  k_comb_scatter
 //   6. disc[b] = ecen - (copies in b) * FP32(ew), and optionally that energy
 //      after the comb per bin (exact: equal FP32 weights summed in FP64)         k_comb_disc
 // Order of the output bank = order of the input bank, so the result is deterministic.
@@ -205,23 +205,67 @@ __global__ void __launch_bounds__(1024) k_comb_scan(long long* blk, long long nb
 // thread owns 4 consecutive entries), each thread finds the entry of its copy by a binary
 // search there and gathers the entry's fields (cached: a tile's entries are few), so the
 // output stores are contiguous across the warp.
+// Shared memory of k_comb_scatter: the tile's inclusive copy counts, then its entries'
+// fields (pos1, dir1, cell; pos2, dir2 in 2-D; group when the bank has one), TILE each.
+__host__ __device__ inline int scatter_fields(bool two_d, bool grp) { return 3 + (two_d ? 2 : 0) + (grp ? 1 : 0); }
+__host__ __device__ inline size_t scatter_smem(bool two_d, bool grp) {
+  return sizeof(int) * (size_t)TILE * (1 + scatter_fields(two_d, grp));
+}
+
+// The tile's entries are staged in shared memory with 16-byte loads (one thread per four
+// entries, as the count kernel tiled them), then one thread per output copy finds its entry
+// by a binary search of the scanned counts and copies its fields from shared memory, so the
+// global loads and the stores of a warp are both contiguous.
 __global__ void __launch_bounds__(1024) k_comb_scatter(CombArgs a) {
   pdl_wait();     // the previous kernel of the stream has completed
   pdl_trigger();  // the next one may be scheduled
-  __shared__ int incl[TILE];
+  extern __shared__ __align__(16) int sm_tile[];
   __shared__ int sh[32];
+  const bool two_d = a.p2 != nullptr, grp = a.group != nullptr;
+  int* incl = sm_tile;
+  float* sP1 = reinterpret_cast<float*>(incl + TILE);
+  float* sD1 = sP1 + TILE;
+  int* sC = reinterpret_cast<int*>(sD1 + TILE);
+  float* sP2 = reinterpret_cast<float*>(sC + TILE);   // 2-D only
+  float* sD2 = sP2 + TILE;                            // 2-D only
+  int* sG = reinterpret_cast<int*>(two_d ? sD2 + TILE : sP2);  // with a group array only
   const long long tile0 = (long long)blockIdx.x * TILE;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const long long n_in = min((long long)*a.d_n_in, (long long)a.n_bound);
-  const long long k0 = tile0 + 4 * threadIdx.x;
+  const int q0 = 4 * threadIdx.x;
+  const long long k0 = tile0 + q0;
+  const bool full = k0 + 3 < n_in;
   int c[4] = {0, 0, 0, 0};
-  if (k0 + 3 < n_in) {
+  if (full) {
     const int4 v = *reinterpret_cast<const int4*>(a.cnt + k0);  // 16-byte aligned: k0 % 4 == 0
     c[0] = v.x; c[1] = v.y; c[2] = v.z; c[3] = v.w;
   } else {
     for (int j = 0; j < 4; ++j) if (k0 + j < n_in) c[j] = a.cnt[k0 + j];
   }
   const int s4 = c[0] + c[1] + c[2] + c[3];
+  // stage the fields of the four entries (only where they have copies)
+  const uintptr_t al = reinterpret_cast<uintptr_t>(a.p1) | reinterpret_cast<uintptr_t>(a.d1) |
+                       reinterpret_cast<uintptr_t>(a.p2) | reinterpret_cast<uintptr_t>(a.d2);
+  if (s4 > 0) {
+    if (full && a.vec16 && (al & 15u) == 0) {
+      *reinterpret_cast<float4*>(sP1 + q0) = *reinterpret_cast<const float4*>(a.p1 + k0);
+      *reinterpret_cast<float4*>(sD1 + q0) = *reinterpret_cast<const float4*>(a.d1 + k0);
+      *reinterpret_cast<int4*>(sC + q0) = *reinterpret_cast<const int4*>(a.cell + k0);
+      if (two_d) {
+        *reinterpret_cast<float4*>(sP2 + q0) = *reinterpret_cast<const float4*>(a.p2 + k0);
+        *reinterpret_cast<float4*>(sD2 + q0) = *reinterpret_cast<const float4*>(a.d2 + k0);
+      }
+      if (grp) *reinterpret_cast<int4*>(sG + q0) = *reinterpret_cast<const int4*>(a.group + k0);
+    } else {
+      for (int j = 0; j < 4; ++j) {
+        if (c[j] == 0) continue;
+        const long long k = k0 + j;
+        sP1[q0 + j] = a.p1[k]; sD1[q0 + j] = a.d1[k]; sC[q0 + j] = a.cell[k];
+        if (two_d) { sP2[q0 + j] = a.p2[k]; sD2[q0 + j] = a.d2[k]; }
+        if (grp) sG[q0 + j] = a.group[k];
+      }
+    }
+  }
   // block-exclusive scan of the threads' sums, then the entries' inclusive sums
   int x = s4;
 #pragma unroll
@@ -237,7 +281,7 @@ __global__ void __launch_bounds__(1024) k_comb_scatter(CombArgs a) {
   __syncthreads();
   int run = x - s4 + (wid ? sh[wid - 1] : 0);
 #pragma unroll
-  for (int j = 0; j < 4; ++j) { run += c[j]; incl[4 * threadIdx.x + j] = run; }
+  for (int j = 0; j < 4; ++j) { run += c[j]; incl[q0 + j] = run; }
   __syncthreads();
   const int total = incl[TILE - 1];
   const long long out0 = a.blk[blockIdx.x];
@@ -247,14 +291,13 @@ __global__ void __launch_bounds__(1024) k_comb_scatter(CombArgs a) {
     if (dst >= a.out_capacity) break;  // overflow: flagged by the scan, caller regrows
     int lo = 0, hi = TILE - 1;  // the entry j with incl[j-1] <= o < incl[j]
     while (lo < hi) { const int mid = (lo + hi) >> 1; if (incl[mid] > o) hi = mid; else lo = mid + 1; }
-    const long long src = tile0 + lo;
-    const int b = bin_of(a, src);
-    a.op1[dst] = a.p1[src]; a.od1[dst] = a.d1[src];
-    if (a.op2) a.op2[dst] = a.p2[src];
-    if (a.od2) a.od2[dst] = a.d2[src];
-    a.ow[dst] = compact ? a.w[src] : copy_weight(a, b);
-    a.ot[dst] = 0.f; a.ocell[dst] = a.cell[src];
-    if (a.ogroup) a.ogroup[dst] = a.group[src];
+    const int cl = sC[lo];
+    const int gr = grp ? sG[lo] : 0;
+    a.op1[dst] = sP1[lo]; a.od1[dst] = sD1[lo];
+    if (two_d) { a.op2[dst] = sP2[lo]; a.od2[dst] = sD2[lo]; }
+    a.ow[dst] = compact ? a.w[tile0 + lo] : copy_weight(a, a.per_group ? cl + a.nc * gr : cl);
+    a.ot[dst] = 0.f; a.ocell[dst] = cl;
+    if (a.ogroup) a.ogroup[dst] = gr;
   }
 }
 
@@ -299,9 +342,18 @@ cudaError_t imc_launch_comb_scatter(const CombArgs& a, cudaStream_t s) {
   const long long nblk = (a.n_bound + TILE - 1) / TILE;
   if (nblk > 0) {
     ++g_imc_launches;
-    IMC_LAUNCH_PDL(k_comb_scatter, (unsigned)nblk, 1024, 0, s, a);
-    cudaError_t e = cudaGetLastError();
+    // the attribute allows the largest layout (2-D with groups), set once per device
+    static bool attr_set[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+      e = cudaFuncSetAttribute(k_comb_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)scatter_smem(true, true));
+      if (e != cudaSuccess) return e;
+      if (dev >= 0 && dev < 64) attr_set[dev] = true;
+    }
+    IMC_LAUNCH_PDL(k_comb_scatter, (unsigned)nblk, 1024, scatter_smem(a.p2 != nullptr, a.group != nullptr), s, a);
   }
   ++g_imc_launches;
   IMC_LAUNCH_PDL(k_comb_disc, (a.nb + 255) / 256, 256, 0, s, a);
