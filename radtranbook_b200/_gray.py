@@ -190,6 +190,35 @@ def _staged(state, key: str, n: int) -> dict:
     return {"stage": _pinned(state, key, n), "stage_dev": devs[key]}
 
 
+def _upload_flat(state, values, stage: torch.Tensor, dev: torch.Tensor) -> torch.Tensor:
+    """Copy a field given in the reference's layout ((nx, ny) in 2-D, or a scalar) to `dev`
+    in the engine's flat cell order c = i + nx*j: the reordering is done on the host, into
+    the pinned `stage`, so the asynchronous upload lands in place (no device transpose and
+    no device allocation).  Returns the first nc entries of dev."""
+    n = state._engine.nc
+    host = stage[:n].numpy()
+    v = np.asarray(values, dtype=np.float64)
+    if state._dim == 1:
+        np.copyto(host, np.broadcast_to(v, (n,)))
+    else:
+        nx, ny = state._shape
+        np.copyto(host.reshape(ny, nx), np.broadcast_to(v, (nx, ny)).T)
+    _lib.TRANSFER["h2d"] += n * 8
+    out = dev[:n]
+    out.copy_(stage[:n], non_blocking=True)
+    return out
+
+
+def _field_flat(state, fn, like: torch.Tensor, host_fn, key: str) -> torch.Tensor:
+    """A material callable on the temperature field, as a flat device field.  A device
+    callable runs on `like`; a host callable on host_fn()'s array, its result uploaded from
+    the state's pinned stage (refilled only next step, after this step's synchronisation)."""
+    if is_device(fn):
+        return state.flat(evaluate(fn, like, host_fn, like))
+    st = _staged(state, key, state._engine.nc)
+    return _upload_flat(state, fn(host_fn()), st["stage"], st["stage_dev"])
+
+
 def _host_copy(t: torch.Tensor) -> np.ndarray:
     a = t.cpu().numpy()
     _lib.TRANSFER["d2h"] += a.nbytes
@@ -281,8 +310,8 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
         # host callables' results go up by asynchronous copies from pinned buffers of the state
         # (refilled only next step, after this step's end-of-step synchronisation)
         like = state.grid(state._T)
-        sigma = state.flat(evaluate(sigma_a_func, like, host_T, like, **_staged(state, "sigma", eng.nc)))
-        cvv = state.flat(evaluate(cv, like, host_T, like, **_staged(state, "cv", eng.nc)))
+        sigma = _field_flat(state, sigma_a_func, like, host_T, "sigma")
+        cvv = _field_flat(state, cv, like, host_T, "cv")
     src = None
     if Nsource > 0 and source is not None:
         src_t = source.double() if isinstance(source, torch.Tensor) else torch.as_tensor(
@@ -318,15 +347,12 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
     else:
         state.__dict__.pop("_law_next", None)
         eng.material_update(state._e, state._Tr)
-    # with the device law (and no comb discrepancy booked into e), e, T and Tr are final now:
-    # their copy to the host runs on a side stream beside the comb
-    early = state.host_copies_early() if law is not None and not conserve_comb_energy else None
-    e_ready = None
-    if law is None and not conserve_comb_energy and not is_device(inv_eos):
-        e_pin = _pinned(state, "e_mid", eng.nc)
-        e_pin.copy_(state._e, non_blocking=True)
-        e_ready = torch.cuda.Event()
-        e_ready.record()
+    # e and Tr are final now (no comb discrepancy booked into e), and so is T with the device
+    # law: their copy to the host runs on a side stream beside the comb.  A host inv_eos then
+    # evaluates T from that copy of e while the comb runs.
+    host_inv = law is None and not conserve_comb_energy and not is_device(inv_eos)
+    early = state.host_copies_early() if (law is not None and not conserve_comb_energy) or host_inv else None
+    t_up = None
     eng.comb_async(Nmax, state.count, state._e)
     if conserve_comb_energy:
         sum_tensors(dist, [eng.disc])
@@ -335,13 +361,21 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
         like = state.grid(state._T)
     if law is not None:
         pass  # T = e / cv came with the material update
-    elif e_ready is not None:
-        def e_host():
-            e_ready.synchronize()
-            _lib.TRANSFER["d2h"] += e_pin.numel() * 8
-            return e_pin.numpy().copy() if state._dim == 1 else e_pin.numpy().reshape(state._shape[1], state._shape[0]).T
-        Tn = evaluate(inv_eos, state.grid(state._e), e_host, like, **_staged(state, "T_new", eng.nc))
-        state._T.copy_(state.flat(Tn))
+    elif host_inv:
+        # the early copy holds e, (the old) T and Tr in the reference's layout: T = inv_eos(e)
+        # replaces the T slot (the host mirror this step returns) and goes up to the device on
+        # the side stream (nothing queued on the current stream reads T before the step ends)
+        early.synchronize()
+        n = eng.nc
+        shape = (n,) if state._dim == 1 else tuple(state._shape)
+        hp = state._hpin.numpy()
+        Tn = np.asarray(inv_eos(hp[:n].reshape(shape)), dtype=np.float64)
+        np.copyto(hp[n:2 * n].reshape(shape), np.broadcast_to(Tn, shape))
+        side = eng.__dict__["_side_stream"]
+        with torch.cuda.stream(side):
+            _upload_flat(state, Tn, _pinned(state, "T_new", n), state._T)
+        t_up = torch.cuda.Event()
+        t_up.record(side)
     else:
         Tn = evaluate(inv_eos, state.grid(state._e), lambda: _host_copy(state.grid(state._e)), like)
         state._T.copy_(state.flat(Tn))
@@ -356,6 +390,8 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
         raise
     if early is not None:
         early.synchronize()  # done long before the comb
+    if t_up is not None:
+        t_up.synchronize()
     t_post = _time.perf_counter()
     pre_comb = eng.spare  # the tracked (pre-comb) bank after the swap
     if not use_scalar_intensity_Tr:
