@@ -162,6 +162,7 @@ class GrayState:
             (self._e if name == "internal_energy" else self._T).copy_(self.flat(t))
             self._host.pop(name, None)
             self.__dict__.pop("_law_next", None)  # the next step's opacity follows a new T
+            self.__dict__.pop("_host_next", None)
             return
         object.__setattr__(self, name, value)
 
@@ -188,6 +189,12 @@ def _staged(state, key: str, n: int) -> dict:
     if key not in devs or devs[key].numel() != n:
         devs[key] = torch.empty(n, dtype=torch.float64, device=state._engine.device)
     return {"stage": _pinned(state, key, n), "stage_dev": devs[key]}
+
+
+def _same(key, objs: tuple) -> bool:
+    """Whether a cached value was made for these objects: identity, not equality.  The cache
+    holds the objects themselves, so a freed callable's id cannot be reused while it lives."""
+    return key is not None and len(key) == len(objs) and all(a is b for a, b in zip(key, objs))
 
 
 def _upload_flat(state, values, stage: torch.Tensor, dev: torch.Tensor) -> torch.Tensor:
@@ -304,8 +311,11 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
     # material update, inverse EOS and next step's opacity are one kernel at the step's end
     law = _law(state, sigma_a_func, cv, inv_eos) if not conserve_comb_energy else None
     nxt = state.__dict__.get("_law_next")
-    if law is not None and nxt is not None and nxt[0] == (id(sigma_a_func), id(cv)):
+    hn = state.__dict__.pop("_host_next", None)
+    if law is not None and nxt is not None and _same(nxt[0], (sigma_a_func, cv)):
         sigma, cvv = nxt[1], nxt[2]  # evaluated on the device at the end of the last step
+    elif law is None and hn is not None and _same(hn[0], (sigma_a_func, cv)) and hn[1] == state.count:
+        sigma, cvv = hn[2], hn[3]  # host callables evaluated at this T while the last comb ran
     else:
         # host callables' results go up by asynchronous copies from pinned buffers of the state
         # (refilled only next step, after this step's end-of-step synchronisation)
@@ -343,7 +353,7 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
         # two buffer pairs: the step reads one pair (its sigma, cv) while it writes the other
         pair = nb[:2] if sigma.data_ptr() != nb[0].data_ptr() else nb[2:]
         eng.material_update_law(state._e, state._Tr, state._T, law[0], pair[0], pair[1])
-        state.__dict__["_law_next"] = ((id(sigma_a_func), id(cv)), pair[0], pair[1])
+        state.__dict__["_law_next"] = ((sigma_a_func, cv), pair[0], pair[1])
     else:
         state.__dict__.pop("_law_next", None)
         eng.material_update(state._e, state._Tr)
@@ -374,6 +384,15 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
         side = eng.__dict__["_side_stream"]
         with torch.cuda.stream(side):
             _upload_flat(state, Tn, _pinned(state, "T_new", n), state._T)
+            if not is_device(sigma_a_func) and not is_device(cv):
+                # the next step's opacity and heat capacity at this T (the host mirror it
+                # returns), while the comb runs; the next step takes them if it passes the same
+                # callables and nothing has set T since (this step's own inputs are read)
+                T_ref = hp[n:2 * n].reshape(shape)
+                st_s, st_c = _staged(state, "sigma", n), _staged(state, "cv", n)
+                sig_n = _upload_flat(state, sigma_a_func(T_ref), st_s["stage"], st_s["stage_dev"])
+                cv_n = _upload_flat(state, cv(T_ref), st_c["stage"], st_c["stage_dev"])
+                state.__dict__["_host_next"] = ((sigma_a_func, cv), state.count + 1, sig_n, cv_n)
         t_up = torch.cuda.Event()
         t_up.record(side)
     else:
@@ -479,9 +498,9 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
 
 def _law(state, sigma_a_func, cv, inv_eos):
     """The device material law of these callables (cached on the state), or None."""
-    key = (id(sigma_a_func), id(cv), id(inv_eos))
+    key = (sigma_a_func, cv, inv_eos)
     cache = state.__dict__.get("_law_cache")
-    if cache is None or cache[0] != key:
+    if cache is None or not _same(cache[0], key):
         from .materials import material_law
 
         cache = (key, material_law(sigma_a_func, cv, inv_eos, state.flat, state._engine.device))

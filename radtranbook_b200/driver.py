@@ -36,7 +36,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._gray import _law, face_temperatures
+from ._gray import _law, _same, face_temperatures
 from .engine import C_LIGHT
 from .materials import GroupedOpacity, evaluate, evaluate_groups, is_device
 
@@ -119,7 +119,7 @@ class DeviceLoop:
         # and cv into one buffer pair, which the next step's plan reads (nothing later in a step
         # reads them, so one pair serves every step of the graph)
         self.law = _law(state, sigma_a_func, cv, inv_eos) if not self.conserve else None
-        self.law_key = (id(sigma_a_func), id(cv))
+        self.law_key = (sigma_a_func, cv)
         if self.law is not None:
             self.law_sigma = torch.empty(eng.ng * eng.nc, dtype=torch.float64, device=dev)
             self.law_cv = torch.empty(eng.nc, dtype=torch.float64, device=dev)
@@ -284,7 +284,7 @@ class DeviceLoop:
         evaluate(self.inv_eos, st.grid(st._e), _no_host, like)
         if self.law is not None:  # the first step's opacity: the eager step's law output, else the callables
             nxt = st.__dict__.get("_law_next")
-            if nxt is not None and nxt[0] == self.law_key:
+            if nxt is not None and _same(nxt[0], self.law_key):
                 self.law_sigma.copy_(nxt[1].reshape(-1))
                 self.law_cv.copy_(nxt[2])
             else:
@@ -305,6 +305,7 @@ class DeviceLoop:
             eng.bank, eng.spare = eng.spare, eng.bank
         e1.record()
         torch.cuda.current_stream().synchronize()
+        st.__dict__.pop("_host_next", None)  # the loop's steps changed T
         if self.law is not None:  # an eager step after the loop continues from the loop's law output
             st.__dict__["_law_next"] = (self.law_key, self.law_sigma, self.law_cv)
         else:

@@ -24,7 +24,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._gray import GrayState, _host_copy, _law, _staged, check_partition, face_temperatures
+from ._gray import GrayState, _host_copy, _law, _same, _staged, check_partition, face_temperatures
 from .partition import local_count, sum_scalars, sum_tensors, summary_totals, world_of
 from .engine import A_RAD, C_LIGHT, Engine
 from .materials import evaluate, evaluate_groups
@@ -220,7 +220,7 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
     if law is not None and len(sigma_a_funcs) != G:
         raise ValueError(f"{len(sigma_a_funcs)} opacity groups for a {G}-group state")
     nxt = state.__dict__.get("_law_next")
-    if law is not None and nxt is not None and nxt[0] == (id(sigma_a_funcs), id(cv)):
+    if law is not None and nxt is not None and _same(nxt[0], (sigma_a_funcs, cv)):
         sig, cvv = nxt[1].view(G, nc), nxt[2]  # evaluated on the device at the end of the last step
     else:
         # host callables' results go up by asynchronous copies from pinned buffers of the state
@@ -280,7 +280,7 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
     if law is not None:
         sig_next, cv_next = _law_buffers(state, eng, sig)
         eng.material_update_law(state._e, state._Tr, state._T, law[0], sig_next, cv_next)
-        state.__dict__["_law_next"] = ((id(sigma_a_funcs), id(cv)), sig_next, cv_next)
+        state.__dict__["_law_next"] = ((sigma_a_funcs, cv), sig_next, cv_next)
     else:
         state.__dict__.pop("_law_next", None)
         eng.material_update(state._e, state._Tr)
