@@ -378,6 +378,9 @@ IMC_API imc_status imc_comb_async_dev(const imc_mesh* mesh, const imc_bank* in, 
  *                           of an IMC_COMB_WRITE_AFTER disc)
  *   out[2G nc, (2G+3) nc)   e, T, Tr (nc each)
  *   then boundary_group and escaped_group (G each).
+ * A NULL input skips its section (out keeps those entries), so the sections that are final
+ * before the comb (everything but `after`) can be gathered and copied while the comb runs and
+ * the post-comb section by a second call with only `after` set.  At least one input is set.
  * No reference counterpart (the reference's arrays are host arrays already). */
 IMC_API imc_status imc_mg_report_fields(const imc_mesh* mesh, const double* si, const double* after,
                                         const double* e, const double* T, const double* Tr,

@@ -100,10 +100,7 @@ class GrayState:
         synchronises the host on it before reading the buffer and before the step returns
         (nothing that changes e, T or Tr is queued before then)."""
         eng = self._engine
-        side = eng.__dict__.get("_side_stream")
-        if side is None:
-            side = torch.cuda.Stream(device=eng.device)
-            eng.__dict__["_side_stream"] = side
+        side = eng.side_stream()
         main = torch.cuda.current_stream(eng.device)
         side.wait_stream(main)
         with torch.cuda.stream(side):
@@ -381,7 +378,7 @@ def gray_step(state: GrayState, *, Ntarget, Nboundary, Nsource, Nmax, T_boundary
         hp = state._hpin.numpy()
         Tn = np.asarray(inv_eos(hp[:n].reshape(shape)), dtype=np.float64)
         np.copyto(hp[n:2 * n].reshape(shape), np.broadcast_to(Tn, shape))
-        side = eng.__dict__["_side_stream"]
+        side = eng.side_stream()
         with torch.cuda.stream(side):
             _upload_flat(state, Tn, _pinned(state, "T_new", n), state._T)
             if not is_device(sigma_a_func) and not is_device(cv):

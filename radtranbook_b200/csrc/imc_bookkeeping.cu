@@ -418,30 +418,34 @@ __global__ void k_mg_report(ReportArgs a) {
   pdl_wait();     // the previous kernel of the stream has completed
   pdl_trigger();  // the next one may be scheduled
   const long long nc = (long long)a.nx * a.ny, gnc = nc * a.ng;
-  const long long n = 2 * gnc + 3 * nc + 2 * a.ng;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+  for (long long q = a.q0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; q < a.q1;
+       q += (long long)gridDim.x * blockDim.x) {
     double v;
     if (q < 2 * gnc + 3 * nc) {
       const long long part = q < 2 * gnc ? q / gnc : 2 + (q - 2 * gnc) / nc;  // 0 pre, 1 post, 2.. e T Tr
+      const double* src = part == 0 ? a.si : part == 1 ? a.after : part == 2 ? a.e : part == 3 ? a.T : a.Tr;
+      if (!src) continue;  // a section left to another call
       const long long r = q < 2 * gnc ? q % nc : (q - 2 * gnc) % nc;         // reference order i*ny + j
       const long long g = q < 2 * gnc ? (q % gnc) / nc : 0;
       const int i = (int)(r / a.ny), j = (int)(r - (long long)i * a.ny);
       const long long c = i + (long long)a.nx * j;
-      if (part == 0) v = a.si[g * nc + c] / C_LIGHT;
-      else if (part == 1) v = a.after[g * nc + c] / a.vol[c];
-      else v = (part == 2 ? a.e : part == 3 ? a.T : a.Tr)[c];
+      if (part == 0) v = src[g * nc + c] / C_LIGHT;
+      else if (part == 1) v = src[g * nc + c] / a.vol[c];
+      else v = src[c];
     } else {
       const long long k = q - 2 * gnc - 3 * nc;
-      v = k < a.ng ? a.bnd[k] : a.esc[k - a.ng];
+      const double* src = k < a.ng ? a.bnd : a.esc;
+      if (!src) continue;
+      v = src[k < a.ng ? k : k - a.ng];
     }
     a.out[q] = v;
   }
 }
 
 cudaError_t imc_launch_mg_report(const ReportArgs& a, cudaStream_t s) {
+  if (a.q1 <= a.q0) return cudaSuccess;
   ++g_imc_launches;
-  const long long n = 2LL * a.nx * a.ny * a.ng + 3LL * a.nx * a.ny + 2LL * a.ng;
-  const unsigned blocks = (unsigned)std::min<long long>(4736LL, (n + 255) / 256);
+  const unsigned blocks = (unsigned)std::min<long long>(4736LL, (a.q1 - a.q0 + 255) / 256);
   IMC_LAUNCH_PDL(k_mg_report, blocks, 256, 0, s, a);
   return cudaGetLastError();
 }

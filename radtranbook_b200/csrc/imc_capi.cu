@@ -794,11 +794,16 @@ imc_status imc_mg_report_fields(const imc_mesh* mesh, const double* si, const do
   imc_status st = check_mesh(mesh);
   if (st != IMC_OK) return st;
   if (mesh->n_groups < 2 || mesh->geometry < IMC_GEOM_XY) return IMC_ERR_INVALID_ARG;  // 2-D multigroup
-  if (!si || !after || !e || !T || !Tr || !boundary_group || !escaped_group || !out) return IMC_ERR_INVALID_ARG;
+  if (!out || !(si || after || e || T || Tr || boundary_group || escaped_group)) return IMC_ERR_INVALID_ARG;
   ReportArgs ra{};
   ra.nx = mesh->nx; ra.ny = mesh->ny; ra.ng = mesh->n_groups; ra.vol = mesh->volume;
   ra.si = si; ra.after = after; ra.e = e; ra.T = T; ra.Tr = Tr; ra.bnd = boundary_group; ra.esc = escaped_group;
   ra.out = out;
+  // the post-comb section alone (the rest gathered by an earlier call) spans G nc entries
+  const long long gnc = (long long)mesh->nx * mesh->ny * mesh->n_groups;
+  const bool post_only = after && !si && !e && !T && !Tr && !boundary_group && !escaped_group;
+  ra.q0 = post_only ? gnc : 0;
+  ra.q1 = post_only ? 2 * gnc : 2 * gnc + 3LL * mesh->nx * mesh->ny + 2LL * mesh->n_groups;
   IMC_CUDA(imc_launch_mg_report(ra, (cudaStream_t)stream));
   return IMC_OK;
 }

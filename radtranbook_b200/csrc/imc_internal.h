@@ -199,6 +199,7 @@ struct ReportArgs {
   const double* vol; const double* si; const double* after;
   const double* e; const double* T; const double* Tr; const double* bnd; const double* esc;
   double* out;
+  long long q0, q1;  // the entries of out written: [q0, q1), sections whose input is NULL skipped
 };
 cudaError_t imc_launch_mg_report(const ReportArgs& a, cudaStream_t s);
 

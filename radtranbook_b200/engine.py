@@ -462,17 +462,35 @@ class Engine:
                                             self._stream())
         _lib.check("imc_bank_energy_by_bin", st)
 
-    def mg_report_fields(self, e: torch.Tensor, T: torch.Tensor, Tr: torch.Tensor) -> int:
-        """Queue imc_mg_report_fields into self.report_dev (2-D multigroup): the radiation
-        energy by group before (si / c) and after the comb (comb_after / V), e, T, Tr and the
-        boundary / escaped energy by group, in the reference's array order.  Returns its
-        length in doubles."""
+    def side_stream(self) -> torch.cuda.Stream:
+        """A second stream of the engine's device (created once): device-to-host copies of
+        fields that are final before the comb run on it beside the comb."""
+        side = self.__dict__.get("_side_stream")
+        if side is None:
+            side = torch.cuda.Stream(device=self.device)
+            self.__dict__["_side_stream"] = side
+        return side
+
+    def report_buffer(self) -> torch.Tensor:
+        """self.report_dev, (2G + 3) nc + 2G doubles (allocated once)."""
         n = (2 * self.ng + 3) * self.nc + 2 * self.ng
         if getattr(self, "report_dev", None) is None or self.report_dev.numel() != n:
             self.report_dev = torch.empty(n, dtype=torch.float64, device=self.device)
+        return self.report_dev
+
+    def mg_report_fields(self, e: torch.Tensor, T: torch.Tensor, Tr: torch.Tensor, sections: str = "all") -> int:
+        """Queue imc_mg_report_fields into self.report_dev (2-D multigroup): the radiation
+        energy by group before (si / c) and after the comb (comb_after / V), e, T, Tr and the
+        boundary / escaped energy by group, in the reference's array order.  sections: "all";
+        "early" (all but the post-comb energies, which are final only after the comb); "post"
+        (those alone).  Returns the buffer's length in doubles."""
+        n = self.report_buffer().numel()
+        early, post = sections in ("all", "early"), sections in ("all", "post")
         _lib.check("imc_mg_report_fields", self.lib.imc_mg_report_fields(
-            ctypes.byref(self.cmesh), _ptr(self.si), _ptr(self.comb_after), _ptr(e), _ptr(T), _ptr(Tr),
-            _ptr(self.boundary_group), _ptr(self.escaped_group), _ptr(self.report_dev), self._stream()))
+            ctypes.byref(self.cmesh), _ptr(self.si) if early else None, _ptr(self.comb_after) if post else None,
+            _ptr(e) if early else None, _ptr(T) if early else None, _ptr(Tr) if early else None,
+            _ptr(self.boundary_group) if early else None, _ptr(self.escaped_group) if early else None,
+            _ptr(self.report_dev), self._stream()))
         return n
 
     def fetch(self, host_copies=()) -> ImcStepSummary:

@@ -166,6 +166,24 @@ def _report_buffers(state, eng: Engine, n: int) -> dict:
             "esc": buf[o + G:o + 2 * G]}
 
 
+def _report_early(state, eng: Engine) -> tuple:
+    """Gather the report's sections that are final before the comb (all but the post-comb
+    energies) and copy them into this step's host buffer on the engine's side stream, after
+    the work the current stream holds (the material update), so both run beside the comb.
+    Returns (the side stream's event after the copies, the buffer's parts)."""
+    G, nc = eng.ng, eng.nc
+    hb = _report_buffers(state, eng, eng.report_buffer().numel())
+    side = eng.side_stream()
+    side.wait_stream(torch.cuda.current_stream(eng.device))
+    with torch.cuda.stream(side):
+        eng.mg_report_fields(state._e, state._T, state._Tr, sections="early")
+        hb["pre"].copy_(eng.report_dev[:G * nc], non_blocking=True)
+        hb["all"][2 * G * nc:].copy_(eng.report_dev[2 * G * nc:], non_blocking=True)
+    done = torch.cuda.Event()
+    done.record(side)
+    return done, hb
+
+
 def _law_buffers(state, eng: Engine, sigma: torch.Tensor) -> tuple:
     """The (opacity [g][c], heat capacity [c]) pair the material law kernel writes this step:
     of two pairs, the one the step is not reading."""
@@ -284,7 +302,10 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
     else:
         state.__dict__.pop("_law_next", None)
         eng.material_update(state._e, state._Tr)
-    # the comb is queued first (the host prepares the by-group fields while it runs); it also
+    # with the device law (and no comb discrepancy booked into e) every reported field but the
+    # post-comb energies is final now: gathered and copied to the host beside the comb
+    early = _report_early(state, eng) if law is not None and not conserve_comb_energy else None
+    # the comb is queued next (the host prepares the by-group fields while it runs); it also
     # writes the energy after it per (group, cell) bin: the post-comb radiation energy by
     # group without a pass over the new census
     eng.comb_async(nmax_l, state.count, state._e, per_group=True, write_after=True)
@@ -303,14 +324,22 @@ def step(state, Ntarget, Nboundary, Nsource, Nmax, T_boundary, dt, edges1, edges
         state._T.copy_(state.flat(Tn))
     # every reported field in the reference's layout in one device buffer (one kernel), then
     # one copy into a fresh pinned buffer that the host arrays view
-    hb = _report_buffers(state, eng, eng.mg_report_fields(state._e, state._T, state._Tr))
+    if early is None:
+        hb = _report_buffers(state, eng, eng.mg_report_fields(state._e, state._T, state._Tr))
+        copies = [(eng.report_dev, hb["all"])]
+    else:
+        hb = early[1]
+        eng.mg_report_fields(None, None, None, sections="post")
+        copies = [(eng.report_dev[G * nc:2 * G * nc], hb["post"])]
     ms_src, ms_tr = eng.phase_times()  # waits for the tracking only (the comb still runs)
     try:
-        sm = eng.fetch([(eng.report_dev, hb["all"])])
+        sm = eng.fetch(copies)
     except _lib.ImcError as ex:
         if ex.status == 3:
             raise AssertionError("non-finite or non-positive material state") from ex
         raise
+    if early is not None:
+        early[0].synchronize()  # done long before the comb
     if not use_scalar_intensity_Tr:
         pre = eng.spare
         acc = torch.zeros(G * nc, dtype=torch.float64, device=eng.device)
