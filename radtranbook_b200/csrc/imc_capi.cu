@@ -49,6 +49,28 @@ PhaseEvents& phase_events() {
   return pe;
 }
 
+// A second stream per device and host thread (non-blocking, created on first use) with a
+// fork and a join event: a step's boundary faces and tracked-weight sums are made on it beside
+// the volume fill.  NULL when it cannot be created (the step then runs both on its stream).
+struct SideStream {
+  cudaStream_t s = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  bool ok = false, tried = false;
+};
+SideStream* side_stream() {
+  static thread_local SideStream ss[16];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 16) return nullptr;
+  SideStream& x = ss[dev];
+  if (!x.tried) {
+    x.tried = true;
+    x.ok = cudaStreamCreateWithFlags(&x.s, cudaStreamNonBlocking) == cudaSuccess &&
+           cudaEventCreateWithFlags(&x.fork, cudaEventDisableTiming) == cudaSuccess &&
+           cudaEventCreateWithFlags(&x.join, cudaEventDisableTiming) == cudaSuccess;
+  }
+  return x.ok ? &x : nullptr;
+}
+
 int sm_count() {
   static int n = 0;
   if (!n) {
@@ -342,19 +364,31 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
     cf_times = false;
   }
 
-  // two launches of the job table: the faces with the census weights, then the volume fills
-  // (one kernel holding every body would run the volume fill with fewer resident blocks)
+  // two launches of the job table: the faces with the tracked-weight sums and the volume fills
+  // (one kernel holding every body would run the volume fill with fewer resident blocks).  With
+  // a large volume fill (crooked pipe RZ: 5 us less from plan to tracking) the first launch is
+  // forked onto the side stream and tracking waits for both; a small one (the multigroup
+  // crooked pipe's, where the fork's events cost 4 us more) runs after it on the step's stream.
+  long long vol_bound = 0;
+  for (int q = 0; q < sj.n_vol; ++q) vol_bound += sj.vol[q].n_bound;
+  SideStream* side = vol_bound >= (1LL << 19) ? side_stream() : nullptr;
   {
     const int nb = sj.n_jobs;
     for (int q = 0; q < sj.n_bnd; ++q) sj.add(JOB_BOUNDARY, q, imc_source_blocks(sj.bnd[q].n_bound));
     sj.add(JOB_CENSUS_WSUM, 0, std::min(imc_source_blocks(std::max<long long>(bank->size, 1)), 4 * sm_count()));
-    IMC_CUDA(imc_launch_sources(sj, s));
+    if (side) {
+      IMC_CUDA(cudaEventRecord(side->fork, s));
+      IMC_CUDA(cudaStreamWaitEvent(side->s, side->fork, 0));
+    }
+    IMC_CUDA(imc_launch_sources(sj, side ? side->s : s));
+    if (side) IMC_CUDA(cudaEventRecord(side->join, side->s));
     sj.n_jobs = nb;
     for (int q = 0; q < sj.n_vol; ++q) sj.add(JOB_VOLUME, q, imc_source_blocks(sj.vol[q].n_bound));
     IMC_CUDA(imc_launch_sources(sj, s));
     sj.n_jobs = nb;
     for (int q = 0; q < sj.n_vmg; ++q) sj.add(JOB_VOLUME_MG, q, imc_source_blocks(sj.vmg[q].n_bound));
     IMC_CUDA(imc_launch_sources(sj, s));
+    if (side) IMC_CUDA(cudaStreamWaitEvent(s, side->join, 0));
   }
 
   // ---- tracking ----

@@ -137,3 +137,21 @@ def test_mg_report_fields_are_the_engine_fields(cuda):
     np.testing.assert_array_equal(st.internal_energy, st.grid(st._e).cpu().numpy())
     np.testing.assert_array_equal(info["boundary_emission_by_group"], eng.boundary_group.cpu().numpy())
     np.testing.assert_array_equal(info["boundary_outgoing_by_group"], eng.escaped_group.cpu().numpy())
+
+
+def test_mg_report_sections_make_the_full_report(cuda):
+    """imc_mg_report_fields with NULL inputs skips their sections: the early call (all but the
+    post-comb energies) and the post-comb call fill, between them, the buffer one full call
+    fills, entry for entry."""
+    p = problems.mg_crooked_pipe(nr=30, nz=105, mode="quick")
+    st, _ = _mg_pipe_steps(p, 2)
+    eng = st._engine
+    eng.mg_report_fields(st._e, st._T, st._Tr)
+    full = eng.report_dev.clone()
+    eng.report_dev.fill_(float("nan"))
+    eng.mg_report_fields(st._e, st._T, st._Tr, sections="early")
+    G, nc = eng.ng, eng.nc
+    assert torch.isnan(eng.report_dev[G * nc:2 * G * nc]).all()  # the post-comb section is left alone
+    eng.mg_report_fields(None, None, None, sections="post")
+    torch.cuda.synchronize()
+    assert torch.equal(eng.report_dev, full)
