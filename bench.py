@@ -286,9 +286,12 @@ def form_batched(steps: int, tune: bool, n_inst: int = 256, particle_scale: floa
     eng.init()
     tuned = None
     if tune:
+        # tune on a developed state (the first step's histories, from the cold initial state,
+        # are far shorter than the run's): five eager steps, then the tuner replays the sixth
+        eng.step(5, graph=False)
         tuned = batch.tune(eng, grid={"block_size": (256,), "blocks_per_sm": (4, 8), "chunk": (1024, 4096),
-                                      "refill_min": (1, 8)})
-        eng.init()  # tuning replays the first step from the initial state; start over
+                                      "refill_min": (1, 8), "form": (1, 2)})
+        eng.init()  # start over from the initial state
     eng.capture()
     torch.cuda.synchronize()
     # the batched steps in windows of `window` steps (CUDA events around each window)

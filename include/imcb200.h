@@ -447,7 +447,13 @@ typedef struct imc_batch {
   const double* opacity_a;      /* [K] */
   const double* opacity_p;      /* [K] */
   const double* cv;             /* [K] */
+  int32_t max_cells;            /* the largest nc_k (host copy; 0: not given).  With 0 < max_cells <=
+                                   IMC_BATCH_SMEM_CELLS the tracking keeps the instance's cell
+                                   table and tallies of each work unit in shared memory */
 } imc_batch;
+
+/* largest instance whose cell table and tallies the batched tracking stages in shared memory */
+#define IMC_BATCH_SMEM_CELLS 2048
 
 /* per-instance energy ledger of the last step (FP64), ledger[k * IMC_BL_N + field] */
 enum {
@@ -486,6 +492,12 @@ typedef struct imc_batch_launch {  /* tracking kernel shape; 0 = default */
   int32_t blocks_per_sm;
   int32_t chunk;                /* histories per work-queue ticket (at most) */
   int32_t refill_min;           /* idle lanes a warp waits for before it refills (1..32) */
+  int32_t form;                 /* tracking form: 1 work units (a block takes chunk x warps entries
+                                   and stages each instance's tables and tallies in shared memory;
+                                   needs imc_batch.max_cells), 2 the entry queue (warps take entries
+                                   of any instance, tables and tallies in global memory; for many
+                                   small instances), 0 the library's choice (work units when
+                                   max_cells allows) */
 } imc_batch_launch;
 
 IMC_API size_t imc_batch_workspace_bytes(const imc_batch* b);

@@ -131,7 +131,8 @@ class ImcBatch(ctypes.Structure):
                 ("dt", c_double), ("theta", c_double),
                 ("cell_off", c_void_p), ("edges", c_void_p), ("slot_off", c_void_p), ("seed", c_void_p),
                 ("n_target", c_void_p), ("n_boundary", c_void_p), ("n_max", c_void_p), ("face_T", c_void_p),
-                ("reflect", c_void_p), ("opacity_a", c_void_p), ("opacity_p", c_void_p), ("cv", c_void_p)]
+                ("reflect", c_void_p), ("opacity_a", c_void_p), ("opacity_p", c_void_p), ("cv", c_void_p),
+                ("max_cells", c_int32)]
 
 
 class ImcBatchState(ctypes.Structure):
@@ -141,7 +142,8 @@ class ImcBatchState(ctypes.Structure):
 
 
 class ImcBatchLaunch(ctypes.Structure):
-    _fields_ = [("block_size", c_int32), ("blocks_per_sm", c_int32), ("chunk", c_int32), ("refill_min", c_int32)]
+    _fields_ = [("block_size", c_int32), ("blocks_per_sm", c_int32), ("chunk", c_int32), ("refill_min", c_int32),
+                ("form", c_int32)]
 
 
 SIGNATURES = {

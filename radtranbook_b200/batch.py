@@ -104,7 +104,11 @@ def slot_plan(spec: BatchSpec) -> tuple[np.ndarray, np.ndarray, int]:
 
 
 # --------------------------------------------------------------------------- engine
-DEFAULT_LAUNCH = {"block_size": 256, "blocks_per_sm": 4, "chunk": 1024, "refill_min": 1}
+# form: 1 work units (a block takes chunk x warps entries of one instance at a time and keeps
+# its cell table and tallies in shared memory), 2 the entry queue (warps take entries of any
+# instance; for many small instances); the engine's default follows the particles per instance
+DEFAULT_LAUNCH = {"block_size": 256, "blocks_per_sm": 4, "chunk": 1024, "refill_min": 1, "form": 0}
+UNITS_MIN_PARTICLES = 20_000  # mean particles per instance from which work units are the default
 
 
 class BatchEngine:
@@ -144,7 +148,8 @@ class BatchEngine:
         p = lambda name: self.d[name].data_ptr()  # noqa: E731
         self.cb = _lib.ImcBatch(K, self.n_cells, self.n_slots, max_new, float(spec.dt), float(spec.theta),
                                 p("cell_off"), p("edges"), p("slot_off"), p("seed"), p("n_target"), p("n_boundary"),
-                                p("n_max"), p("face_T"), p("reflect"), p("opacity_a"), p("opacity_p"), p("cv"))
+                                p("n_max"), p("face_T"), p("reflect"), p("opacity_a"), p("opacity_p"), p("cv"),
+                                int(np.max(spec.n_cells)))
         ns = self.n_slots
         self.banks = []
         for _ in range(2):
@@ -176,6 +181,8 @@ class BatchEngine:
         self.ws = torch.empty(int(self.lib.imc_batch_workspace_bytes(ctypes.byref(self.cb))), dtype=torch.uint8,
                               device=dev)
         self.launch = dict(DEFAULT_LAUNCH)
+        mean_particles = float(np.mean(spec.n_target + spec.n_boundary))
+        self.launch["form"] = 1 if mean_particles >= UNITS_MIN_PARTICLES else 2
         self.graph = None
         self._graph_launch = None
 
@@ -193,7 +200,7 @@ class BatchEngine:
     def _launch_c(self) -> _lib.ImcBatchLaunch:
         L = self.launch
         return _lib.ImcBatchLaunch(int(L["block_size"]), int(L["blocks_per_sm"]), int(L["chunk"]),
-                                   int(L["refill_min"]))
+                                   int(L["refill_min"]), int(L.get("form", 0)))
 
     def step_eager(self) -> None:
         """Enqueue one step of every instance (no synchronisation)."""
@@ -268,14 +275,16 @@ TUNE_GRID = {
     "blocks_per_sm": (4, 8),
     "chunk": (256, 1024, 4096),
     "refill_min": (1, 4, 16),
+    "form": (1, 2),
 }
 
 
 def tune(engine: BatchEngine, grid: dict | None = None, repeats: int = 1) -> dict:
     """Choose the tracking launch shape (block size, blocks per SM, work-queue ticket
-    size = the bank tile a warp takes, and refill cadence = how many idle lanes a warp
-    collects before it compacts them) by timing whole eager steps of the batch from its
-    current state (restored before every trial, so each trial is the same work)."""
+    size = the bank tile a warp takes, refill cadence = how many idle lanes a warp
+    collects before it compacts them, and the form: work units or the entry queue) by timing
+    whole eager steps of the batch from its current state (restored before every trial, so
+    each trial is the same work)."""
     import itertools
 
     g = dict(TUNE_GRID if grid is None else grid)

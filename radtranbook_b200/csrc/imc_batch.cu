@@ -339,6 +339,242 @@ __global__ void __launch_bounds__(256) k_btrack(BatchArgs a) {
   }
 }
 
+// Work-unit form of the tracking, for batches whose largest instance has at most
+// IMC_BATCH_SMEM_CELLS cells.  A block claims a unit of chunk x (warps per block) consecutive
+// entries of the batch (instance-major: one instance, or the end of one and the start of the
+// next) and tracks it instance by instance with all its warps, each warp refilling idle lanes
+// from a shared-memory cursor.  For the instance at hand the block keeps the cell table
+// (sigma_a, sigma_s), the edges and the intensity factor in shared memory and sums the
+// deposition (fixed point) and intensity tallies there, adding them to the instance's global
+// tallies when it moves to another instance: the single-problem kernel's on-chip tables, which
+// the entry-granular queue of k_btrack cannot keep because its warps draw entries of any
+// instance.  Per history the computation is k_btrack's (same Philox counters and arithmetic).
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) v += __shfl_down_sync(FULL, v, o);
+  return v;
+}
+
+__host__ __device__ inline size_t units_smem(int K, int M) {
+  return sizeof(long long) * (size_t)(K + 1) + (size_t)M * (8 + 8 + 8 + 8) + sizeof(float) * (size_t)(M + 1);
+}
+
+__global__ void __launch_bounds__(256) k_btrack_units(BatchArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ unsigned blk_cnt[B_N];
+  __shared__ unsigned long long s_base, s_cur;
+  const int M = a.max_cells;
+  long long* pref = reinterpret_cast<long long*>(smem);                                 // [K+1]
+  unsigned long long* TD = reinterpret_cast<unsigned long long*>(pref + (a.K + 1));    // [M] deposition
+  double* TS = reinterpret_cast<double*>(TD + M);                                       // [M] intensity
+  double* CF = TS + M;                                                                  // [M] cellf.y
+  float2* SS = reinterpret_cast<float2*>(CF + M);                                       // [M] (sa, ss)
+  float* EF = reinterpret_cast<float*>(SS + M);                                         // [M+1] edges
+  if (threadIdx.x < B_N) blk_cnt[threadIdx.x] = 0u;
+  load_pref(pref, a.live_pref, a.K);
+
+  const int lane = threadIdx.x & 31;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  const unsigned long long n = (unsigned long long)pref[a.K];
+  const BatchBank B = a.bank[*a.sel];
+  const uint32_t step = *a.step;
+  const float dt = (float)a.dt;
+  const float c_light = (float)C_LIGHT;
+  const unsigned long long unit = (unsigned long long)max(a.chunk, 32) * (blockDim.x >> 5);
+  unsigned s_bd = 0, s_sc = 0;
+  int cur_k = -1, cur_nc = 0, cur_cb = 0;  // block-uniform: the instance whose tallies are staged
+
+  for (;;) {
+    if (threadIdx.x == 0) s_base = atomicAdd(a.queue, unit);
+    __syncthreads();
+    const unsigned long long base = s_base;
+    if (base >= n) break;  // uniform: every thread read the same claim
+    const unsigned long long end = min(base + unit, n);
+    for (unsigned long long q0 = base; q0 < end;) {
+      const int k = find_inst(pref, a.K, (long long)q0);
+      const unsigned long long q1 = min(end, (unsigned long long)pref[k + 1]);
+      if (k != cur_k) {
+        // the staged tallies to the previous instance, then this instance's tables
+        for (int c = threadIdx.x; c < cur_nc; c += blockDim.x) {
+          if (TD[c]) atomicAdd(a.dep_fx + cur_cb + c, TD[c]);
+          if (TS[c] != 0.0) atomicAdd(a.si + cur_cb + c, TS[c]);
+        }
+        __syncthreads();
+        cur_k = k; cur_cb = a.cell_off[k]; cur_nc = a.cell_off[k + 1] - cur_cb;
+        for (int c = threadIdx.x; c < cur_nc; c += blockDim.x) {
+          TD[c] = 0ull; TS[c] = 0.0;
+          CF[c] = a.cellf[cur_cb + c].y;
+          SS[c] = a.sass[cur_cb + c];
+        }
+        for (int c = threadIdx.x; c <= cur_nc; c += blockDim.x) EF[c] = a.ef[cur_cb + k + c];
+      }
+      if (threadIdx.x == 0) s_cur = q0;
+      __syncthreads();
+      // the instance's constants (block-uniform)
+      const int nc = cur_nc;
+      const int rmask = a.reflect[k];
+      const uint64_t seed = a.seed[k];
+      const long long nbk = a.n_bank[k];
+      const double W = a.wsum[k];
+      const float wfloor = (float)(1e-10 * W / (double)(nbk > 0 ? nbk : 1));
+      const double inv_q = fx_inv_quantum(W);
+      const long long pk = pref[k], so = a.slot_off[k];
+      unsigned long long ev_acc = 0ull;
+      bool has = false, drained = false;
+      long long pid = 0;
+      uint32_t lid = 0, ev = 0;
+      int ci = 0;
+      float x = 0.f, u = 0.f, w = 0.f, dcen = 0.f;
+      double acc_lost = 0.0, acc_wd = 0.0;
+      for (;;) {
+        // ---- refill idle lanes from the block's cursor over [q0, q1) ----
+        unsigned need = __ballot_sync(FULL, !has);
+        while (need && !drained) {
+          unsigned long long b0 = 0;
+          if (lane == 0) b0 = atomicAdd(&s_cur, (unsigned long long)__popc(need));
+          b0 = __shfl_sync(FULL, b0, 0);
+          if (b0 >= q1) { drained = true; break; }
+          const unsigned rank = __popc(need & lt_mask);
+          if (!has && b0 + rank < q1) {
+            lid = (uint32_t)((long long)(b0 + rank) - pk);
+            pid = so + lid;
+            w = B.w[pid];
+            dcen = (dt - B.t[pid]) * c_light;
+            if (w > 0.f && dcen > 0.f) {
+              x = B.p1[pid]; u = B.d1[pid]; ci = B.cell[pid];
+              ev = 0;
+              has = true;
+            }
+          }
+          need = __ballot_sync(FULL, !has);
+        }
+        if (!__any_sync(FULL, has)) break;
+        bool flush = false;
+        int flush_cell = 0;
+        double f_lost = 0.0, f_wd = 0.0;
+        if (has) {
+          const float2 sq = SS[ci];
+          const float sa = sq.x, ss = sq.y;
+          bool finished = false;
+          if (ev >= (1u << 30)) {
+            atomicAdd(&blk_cnt[B_CAP], 1u);
+            atomicOr(a.flags, (int)IMC_FLAG_EVENT_CAP);
+            finished = true;
+          } else {
+            const U4 r = draw(seed, lid, ev, step, TAG_TRANSPORT);
+            ++ev;
+            const float xl = EF[ci], xr = EF[ci + 1];
+            const float L = xr - xl;
+            const float sb = slab_face(x, u, xl, xr);
+            float ds = BIGF;
+            {
+              const bool capped = ss * L > 10000.0f;
+              const float sig = capped ? 10000.0f / L : (ss > 1e-10f ? ss : 0.f);
+              if (sig > 0.f) {
+                const float s_other = fminf(sb, dcen);
+                const double t = (double)sig * (double)s_other;
+                bool may = true;
+                if (t < 0.01) {
+                  const double thr = 1.0 - t * (1.0 - t * (0.5 - t * (1.0 / 6.0)));
+                  may = u01d(r.x) > thr;
+                }
+                if (may) ds = capped ? neglog_u(r.x) * (L * 1e-4f) : __fdividef(neglog_u(r.x), ss);
+              }
+            }
+            float d = sb;
+            int evt = EV_BOUNDARY, cross = X_NONE;
+            if (ds < d) { d = ds; evt = EV_SCATTER; }
+            if (dcen < d) { d = dcen; evt = EV_CENSUS; }
+            float xn = fmaf(u, d, x), un = u;
+            if (evt == EV_BOUNDARY) { if (u > 0.f) { xn = xr; cross = X_IP; } else { xn = xl; cross = X_IM; } }
+            else { if (evt == EV_SCATTER) un = fmaf(2.f, u01f(r.y), -1.f); xn = fminf(fmaxf(xn, xl), xr); }
+            const float wn = w * __expf(-sa * d);
+            acc_lost += (double)w - (double)wn;
+            acc_wd += (double)(w * d);
+            dcen -= d;
+            if (evt == EV_BOUNDARY) ++s_bd; else if (evt == EV_SCATTER) ++s_sc;
+            else atomicAdd(&blk_cnt[B_CENSUS], 1u);
+            w = wn; x = xn; u = un;
+            if (cross != X_NONE) {
+              flush = true; flush_cell = ci; f_lost = acc_lost; f_wd = acc_wd;
+              acc_lost = 0.0; acc_wd = 0.0;
+              int ni = cross == X_IP ? ci + 1 : ci - 1;
+              const int side = ni < 0 ? 0 : (ni >= nc ? 1 : -1);
+              if (side >= 0) {
+                if ((rmask >> side) & 1) {
+                  u = -u;
+                  ni = side == 0 ? 0 : nc - 1;
+                  atomicAdd(&blk_cnt[B_REFLECT], 1u);
+                } else {
+                  atomicAdd(a.esc_fx + 2 * k + side, fx_units((double)w, inv_q));
+                  atomicAdd(&blk_cnt[B_ESCAPE], 1u);
+                  w = 0.f;
+                  finished = true;
+                  ni = ci;
+                }
+              }
+              ci = ni;
+            }
+            if (!finished && w < wfloor) {
+              // IMC/IMC1D.py:188-195: kill and deposit the remainder in the current cell
+              atomicAdd(&blk_cnt[B_FLOOR], 1u);
+              const double rem = (double)w;
+              atomicAdd(TD + ci, fx_units(rem, inv_q));
+              if (CF[ci] > 0.0) atomicAdd(TS + ci, rem * CF[ci]);
+              w = 0.f;
+              finished = true;
+            }
+            if (!finished && !(dcen > 0.f)) finished = true;
+          }
+          if (finished) {
+            if (!flush && (acc_lost != 0.0 || acc_wd != 0.0)) {
+              flush = true; flush_cell = ci; f_lost = acc_lost; f_wd = acc_wd;
+            }
+            acc_lost = 0.0; acc_wd = 0.0;
+            B.w[pid] = w;
+            if (w > 0.f) { B.p1[pid] = x; B.d1[pid] = u; B.cell[pid] = ci; }
+            ev_acc += ev;
+            has = false;
+          }
+        }
+        if (flush) {
+          // the cell visit's tallies into the block's staged ones (one shared atomic per lane)
+          const double cfy = CF[flush_cell];
+          const unsigned long long ud = fx_units(f_lost, inv_q);
+          const double vs = cfy > 0.0 ? f_lost * cfy : -f_wd * cfy;
+          if (ud) atomicAdd(TD + flush_cell, ud);
+          if (vs != 0.0) atomicAdd(TS + flush_cell, vs);
+        }
+      }
+      // the unit's events of this instance to its ledger, one atomic per warp
+      const unsigned long long t_ev = warp_sum_u64(ev_acc);
+      if (lane == 0 && t_ev) atomicAdd(a.ledger + (size_t)k * IMC_BL_N + IMC_BL_EVENTS, (double)t_ev);
+      __syncthreads();  // every warp is done with s_cur and the tables of this range
+      q0 = q1;
+    }
+  }
+  for (int c = threadIdx.x; c < cur_nc; c += blockDim.x) {
+    if (TD[c]) atomicAdd(a.dep_fx + cur_cb + c, TD[c]);
+    if (TS[c] != 0.0) atomicAdd(a.si + cur_cb + c, TS[c]);
+  }
+  const unsigned long long t_bd = warp_sum_u(s_bd), t_sc = warp_sum_u(s_sc);
+  if (lane == 0) {
+    if (t_bd) atomicAdd(a.stats + S_BOUNDARY, t_bd);
+    if (t_sc) atomicAdd(a.stats + S_SCATTER, t_sc);
+    if (t_bd + t_sc) atomicAdd(a.stats + S_EVENTS, t_bd + t_sc);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned long long cen = blk_cnt[B_CENSUS], cap = blk_cnt[B_CAP];
+    if (cen) atomicAdd(a.stats + S_CENSUS, cen);
+    if (cen + cap) atomicAdd(a.stats + S_EVENTS, cen + cap);
+    if (blk_cnt[B_FLOOR]) atomicAdd(a.stats + S_FLOOR, (unsigned long long)blk_cnt[B_FLOOR]);
+    if (blk_cnt[B_REFLECT]) atomicAdd(a.stats + S_REFLECT, (unsigned long long)blk_cnt[B_REFLECT]);
+    if (cap) atomicAdd(a.stats + S_CAP, cap);
+    if (blk_cnt[B_ESCAPE]) atomicAdd(a.stats + S_ESCAPE, (unsigned long long)blk_cnt[B_ESCAPE]);
+  }
+}
+
 // ---------------------------------------------------------------- comb
 // ecen[c] = sum of live weights per cell (all instances)
 __global__ void __launch_bounds__(256) k_bcomb_ecen(BatchArgs a) {
@@ -546,6 +782,15 @@ cudaError_t imc_batch_launch_wsum(const BatchArgs& a, cudaStream_t s) {
 
 cudaError_t imc_batch_launch_track(const BatchArgs& a, int block, int grid, cudaStream_t s) {
   ++g_imc_launches;
+  if (a.form != 2 && a.max_cells > 0 && a.max_cells <= IMC_BATCH_SMEM_CELLS) {
+    const size_t sh = units_smem(a.K, a.max_cells);
+    if (sh > 48 * 1024) {
+      const cudaError_t e = cudaFuncSetAttribute(k_btrack_units, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+      if (e != cudaSuccess) return e;
+    }
+    k_btrack_units<<<grid, block, sh, s>>>(a);
+    return cudaGetLastError();
+  }
   const size_t sh = (size_t)(block / 32) * sizeof(WarpStage) + pref_bytes(a);
   if (sh > 48 * 1024) {
     const cudaError_t e = cudaFuncSetAttribute(k_btrack, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
@@ -649,6 +894,7 @@ BatchArgs make_args(const imc_batch* b, const imc_batch_state* s, void* ws, cons
   a.e_emit = wp<double>(ws, L.e_emit); a.comb_before = wp<double>(ws, L.comb_before);
   a.cnt = wp<int>(ws, L.cnt); a.blk = wp<long long>(ws, L.blk); a.queue = wp<unsigned long long>(ws, L.queue);
   a.chunk = 1024; a.refill_min = 1;
+  a.max_cells = b->max_cells;
   return a;
 }
 
@@ -734,6 +980,7 @@ imc_status imc_batch_step(const imc_batch* b, imc_batch_state* s, const imc_batc
   BatchArgs a = make_args(b, s, workspace, L);
   if (launch && launch->chunk > 0) a.chunk = launch->chunk;
   if (launch && launch->refill_min > 0) a.refill_min = std::min(32, launch->refill_min);
+  if (launch) a.form = launch->form;
   int block = 256;
   const int grid = track_grid(launch, &block);
   BCUDA(imc_batch_launch_plan(a, cs));

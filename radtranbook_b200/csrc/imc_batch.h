@@ -57,6 +57,8 @@ struct BatchArgs {
   unsigned long long* queue;
   // tracking launch
   int chunk, refill_min;
+  int max_cells;         // largest nc_k (0: not given): the work-unit tracking stages tables in shared memory
+  int form;              // imc_batch_launch.form
 };
 
 constexpr int BATCH_TILE = 1024;   // comb tile (entries per block pass)

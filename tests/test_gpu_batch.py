@@ -24,9 +24,11 @@ def _rel_l1(a, b):
     return np.abs(a - b).sum() / max(np.abs(b).sum(), 1e-300)
 
 
-def test_batch_instances_reproduce_single_problem_runs(cuda):
+@pytest.mark.parametrize("form", [1, 2])  # work units (tables staged per instance), the entry queue
+def test_batch_instances_reproduce_single_problem_runs(cuda, form):
     spec = _small()
     eng = batch.BatchEngine(spec)
+    eng.launch["form"] = form
     eng.init()
     eng.step(3, graph=False)
     eng.check()
