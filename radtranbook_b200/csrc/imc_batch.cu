@@ -102,6 +102,11 @@ __global__ void k_bfill(BatchArgs a, int ic) {
 }
 
 // per-instance sum of the tracked entries' weights (the weight floor is 1e-10 * sum / n)
+// wsum[k] = sum of instance k's live weights.  Block b sums the contiguous entries
+// [b*per, (b+1)*per) (coalesced, block-strided by blockDim); each thread finds its entry's
+// instance once and advances it as its index passes instance boundaries (the entry space is
+// instance-major), adding its partial sum to wsum when it leaves an instance and, at the end,
+// through one warp-aggregated add per instance.
 __global__ void __launch_bounds__(256) k_bwsum(BatchArgs a) {
   extern __shared__ long long pref[];
   __shared__ WarpStage stages[8];
@@ -109,19 +114,22 @@ __global__ void __launch_bounds__(256) k_bwsum(BatchArgs a) {
   WarpStage* st = stages + (threadIdx.x >> 5);
   const BatchBank B = a.bank[*a.sel];
   const long long total = pref[a.K];
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long base = (long long)blockIdx.x * blockDim.x; base < total; base += stride) {
-    const long long q = base + threadIdx.x;
-    bool live = false;
-    int k = 0;
-    double w = 0.0;
-    if (q < total) {
-      k = find_inst(pref, a.K, q);
-      const float wf = B.w[a.slot_off[k] + (q - pref[k])];
-      if (wf > 0.f) { live = true; w = (double)wf; }
+  const long long per = (total + gridDim.x - 1) / gridDim.x;
+  const long long lo = min(total, per * (long long)blockIdx.x), hi = min(total, lo + per);
+  int k = lo + threadIdx.x < hi ? find_inst(pref, a.K, lo + threadIdx.x) : 0;
+  long long slot0 = a.slot_off[k] - pref[k];  // bank slot of entry q is slot0 + q within instance k
+  double s = 0.0;
+  for (long long q = lo + threadIdx.x; q < hi; q += blockDim.x) {
+    if (q >= pref[k + 1]) {  // left instance k (k < K - 1 here: q < total = pref[K])
+      if (s != 0.0) atomicAdd(a.wsum + k, s);
+      s = 0.0;
+      do { ++k; } while (q >= pref[k + 1]);
+      slot0 = a.slot_off[k] - pref[k];
     }
-    warp_tally1(live, k, w, a.wsum, st);
+    const float wf = B.w[slot0 + q];
+    if (wf > 0.f) s += (double)wf;
   }
+  warp_tally1(s != 0.0, k, s, a.wsum, st);
 }
 
 // ---------------------------------------------------------------- tracking
