@@ -373,6 +373,7 @@ __global__ void __launch_bounds__(256, 5) k_btrack_units(BatchArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ unsigned blk_cnt[B_N];
   __shared__ unsigned long long s_base, s_cur;
+  __shared__ uint32_t s_rk[20];  // Philox round keys of the staged instance's seed
   const int M = a.max_cells;
   long long* pref = reinterpret_cast<long long*>(smem);                                 // [K+1]
   unsigned long long* TD = reinterpret_cast<unsigned long long*>(pref + (a.K + 1));    // [M] deposition
@@ -417,13 +418,13 @@ __global__ void __launch_bounds__(256, 5) k_btrack_units(BatchArgs a) {
           SS[c] = a.sass[cur_cb + c];
         }
         for (int c = threadIdx.x; c <= cur_nc; c += blockDim.x) EF[c] = a.ef[cur_cb + k + c];
+        if (threadIdx.x == 0) philox_round_keys(a.seed[k], s_rk);
       }
       if (threadIdx.x == 0) s_cur = q0;
       __syncthreads();
       // the instance's constants (block-uniform)
       const int nc = cur_nc;
       const int rmask = a.reflect[k];
-      const uint64_t seed = a.seed[k];
       const long long nbk = a.n_bank[k];
       const double W = a.wsum[k];
       const float wfloor = (float)(1e-10 * W / (double)(nbk > 0 ? nbk : 1));
@@ -471,7 +472,7 @@ __global__ void __launch_bounds__(256, 5) k_btrack_units(BatchArgs a) {
             atomicOr(a.flags, (int)IMC_FLAG_EVENT_CAP);
             finished = true;
           } else {
-            const U4 r = draw(seed, lid, ev, step, TAG_TRANSPORT);
+            const U4 r = draw_rk(s_rk, lid, ev, step, TAG_TRANSPORT);
             ++ev;
             const float xl = EF[ci], xr = EF[ci + 1];
             const float L = xr - xl;
