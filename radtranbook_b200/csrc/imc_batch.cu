@@ -292,11 +292,7 @@ __global__ void __launch_bounds__(256) k_btrack(BatchArgs a) {
         if (!finished && w < wfloor) {
           // IMC/IMC1D.py:188-195: kill and deposit the remainder in the current cell
           atomicAdd(&blk_cnt[B_FLOOR], 1u);
-          const int c2 = cb + ci;
-          const double2 cf = __ldg(a.cellf + c2);
-          const double rem = (double)w;
-          atomicAdd(a.dep_fx + c2, fx_units(rem, inv_q));
-          if (cf.y > 0.0) atomicAdd(a.si + c2, rem * cf.y);
+          atomicAdd(a.dep_fx + cb + ci, fx_units((double)w, inv_q));  // its intensity follows from it
           w = 0.f;
           finished = true;
         }
@@ -323,7 +319,7 @@ __global__ void __launch_bounds__(256) k_btrack(BatchArgs a) {
     if (flush) {
       const double2 cf = __ldg(a.cellf + flush_cell);
       ud = fx_units(f_lost, inv_q);  // lanes of one cell share its instance's quantum
-      vs = cf.y > 0.0 ? f_lost * cf.y : -f_wd * cf.y;
+      vs = cf.y > 0.0 ? 0.0 : f_wd;  // raw w*s of a cell without absorption (the rest follows from ud)
     }
     warp_tally_fx(flush, flush_cell, ud, vs, a.dep_fx, a.si, st);
   }
@@ -436,7 +432,8 @@ __global__ void __launch_bounds__(256, 5) k_btrack_units(BatchArgs a) {
       uint32_t lid = 0, ev = 0;
       int ci = 0;
       float x = 0.f, u = 0.f, w = 0.f, dcen = 0.f;
-      double acc_lost = 0.0, acc_wd = 0.0;
+      float w_in = 0.f;     // weight at the start of the current cell visit
+      double acc_wd = 0.0;  // w*s in the current cell (cells without absorption only)
       for (;;) {
         // ---- refill idle lanes from the block's cursor over [q0, q1) ----
         unsigned need = __ballot_sync(FULL, !has);
@@ -454,6 +451,7 @@ __global__ void __launch_bounds__(256, 5) k_btrack_units(BatchArgs a) {
             if (w > 0.f && dcen > 0.f) {
               x = B.p1[pid]; u = B.d1[pid]; ci = B.cell[pid];
               ev = 0;
+              w_in = w;
               has = true;
             }
           }
@@ -499,16 +497,16 @@ __global__ void __launch_bounds__(256, 5) k_btrack_units(BatchArgs a) {
             float xn = fmaf(u, d, x), un = u;
             if (evt == EV_BOUNDARY) { if (u > 0.f) { xn = xr; cross = X_IP; } else { xn = xl; cross = X_IM; } }
             else { if (evt == EV_SCATTER) un = fmaf(2.f, u01f(r.y), -1.f); xn = fminf(fmaxf(xn, xl), xr); }
+            // implicit capture: the energy removed in a visit is counted at its flush, w_in - w
             const float wn = w * __expf(-sa * d);
-            acc_lost += (double)w - (double)wn;
-            acc_wd += (double)(w * d);
+            if (CF[ci] <= 0.0) acc_wd += (double)(w * d);
             dcen -= d;
             if (evt == EV_BOUNDARY) ++s_bd; else if (evt == EV_SCATTER) ++s_sc;
             else atomicAdd(&blk_cnt[B_CENSUS], 1u);
             w = wn; x = xn; u = un;
             if (cross != X_NONE) {
-              flush = true; flush_cell = ci; f_lost = acc_lost; f_wd = acc_wd;
-              acc_lost = 0.0; acc_wd = 0.0;
+              flush = true; flush_cell = ci; f_lost = (double)w_in - (double)w; f_wd = acc_wd;
+              w_in = w; acc_wd = 0.0;
               int ni = cross == X_IP ? ci + 1 : ci - 1;
               const int side = ni < 0 ? 0 : (ni >= nc ? 1 : -1);
               if (side >= 0) {
@@ -527,21 +525,23 @@ __global__ void __launch_bounds__(256, 5) k_btrack_units(BatchArgs a) {
               ci = ni;
             }
             if (!finished && w < wfloor) {
-              // IMC/IMC1D.py:188-195: kill and deposit the remainder in the current cell
+              // IMC/IMC1D.py:188-195: kill and deposit the remainder in the current cell.
+              // Without a crossing in this event the visit's flush at the history end (w_in - 0)
+              // carries it; after one, the old cell holds the flush slot and the remainder goes
+              // to the new cell here (its intensity follows from the deposition)
               atomicAdd(&blk_cnt[B_FLOOR], 1u);
-              const double rem = (double)w;
-              atomicAdd(TD + ci, fx_units(rem, inv_q));
-              if (CF[ci] > 0.0) atomicAdd(TS + ci, rem * CF[ci]);
+              if (flush) atomicAdd(TD + ci, fx_units((double)w, inv_q));
               w = 0.f;
               finished = true;
             }
             if (!finished && !(dcen > 0.f)) finished = true;
           }
           if (finished) {
-            if (!flush && (acc_lost != 0.0 || acc_wd != 0.0)) {
-              flush = true; flush_cell = ci; f_lost = acc_lost; f_wd = acc_wd;
+            if (!flush) {  // the visit the history ends in
+              const double lost = (double)w_in - (double)w;
+              if (lost != 0.0 || acc_wd != 0.0) { flush = true; flush_cell = ci; f_lost = lost; f_wd = acc_wd; }
             }
-            acc_lost = 0.0; acc_wd = 0.0;
+            acc_wd = 0.0;
             B.w[pid] = w;
             if (w > 0.f) { B.p1[pid] = x; B.d1[pid] = u; B.cell[pid] = ci; }
             ev_acc += ev;
@@ -549,12 +549,12 @@ __global__ void __launch_bounds__(256, 5) k_btrack_units(BatchArgs a) {
           }
         }
         if (flush) {
-          // the cell visit's tallies into the block's staged ones (one shared atomic per lane)
-          const double cfy = CF[flush_cell];
+          // the cell visit's tallies into the block's staged ones (one shared atomic per lane):
+          // deposition in fixed point, raw w*s only from a cell without absorption (an
+          // absorbing cell's intensity follows from its deposition in the material update)
           const unsigned long long ud = fx_units(f_lost, inv_q);
-          const double vs = cfy > 0.0 ? f_lost * cfy : -f_wd * cfy;
           if (ud) atomicAdd(TD + flush_cell, ud);
-          if (vs != 0.0) atomicAdd(TS + flush_cell, vs);
+          if (f_wd != 0.0) atomicAdd(TS + flush_cell, f_wd);
         }
       }
       // the unit's events of this instance to its ledger, one atomic per warp

@@ -61,11 +61,17 @@ __global__ void k_bmaterial_fleck(BatchArgs a, int update) {
   double T;
   if (update) {
     // deposition of the step from its fixed-point sum (units of wsum * 2^-60)
-    const double dep = fx_energy(a.dep_fx[c], a.wsum[k]) * (1.0 / V);  // as the single-problem finalize
+    const double E = fx_energy(a.dep_fx[c], a.wsum[k]);
+    const double dep = E * (1.0 / V);  // as the single-problem finalize
     a.dep[c] = dep;
     const double e = a.e[c] + dep - a.emitted[c] / V;
     a.e[c] = e;
-    const double x = a.si[c] / A_RAD / C_LIGHT;
+    // path-length intensity: an absorbing cell's from its deposition, E / (sigma_a V dt); the
+    // others' from their w*s tally, times 1 / (V dt) (the single-problem finalize)
+    const double cfy = a.cellf[c].y;
+    const double si = cfy > 0.0 ? E * cfy : a.si[c] * -cfy;
+    a.si[c] = si;
+    const double x = si / A_RAD / C_LIGHT;
     a.tr[c] = x > 0.0 ? sqrt(sqrt(x)) : 0.0;
     T = e / cv;  // e = cv T
     a.T[c] = T;
