@@ -272,7 +272,7 @@ def fom_cpu(scale: float, steps: int, seeds: int, nthreads: int) -> dict:
     return out
 
 
-def form_batched(steps: int, tune: bool, n_inst: int = 256, particle_scale: float = 1.0) -> dict:
+def form_batched(steps: int, tune: bool, n_inst: int = 256, particle_scale: float = 1.0, form: int = 0) -> dict:
     """Uneven slab batch (n_inst instances, per-instance particles 10^U[4,6] x particle_scale):
     the batched engine (one CUDA graph per step) and the plain form (the single-problem
     drop-in, one instance after the other) on the same histories (each instance draws
@@ -283,6 +283,8 @@ def form_batched(steps: int, tune: bool, n_inst: int = 256, particle_scale: floa
 
     spec = batch.uneven_slab_batch(n_inst=n_inst, particle_scale=particle_scale)
     eng = batch.BatchEngine(spec)
+    if form:
+        eng.launch["form"] = form  # fixed tracking form (1 work units, 2 entry queue)
     eng.init()
     tuned = None
     if tune:
@@ -290,7 +292,7 @@ def form_batched(steps: int, tune: bool, n_inst: int = 256, particle_scale: floa
         # are far shorter than the run's): five eager steps, then the tuner replays the sixth
         eng.step(5, graph=False)
         tuned = batch.tune(eng, grid={"block_size": (256,), "blocks_per_sm": (4, 8), "chunk": (1024, 4096),
-                                      "refill_min": (1, 8), "form": (1, 2)})
+                                      "refill_min": (1, 8), "form": (form,) if form else (1, 2)})
         eng.init()  # start over from the initial state
     eng.capture()
     torch.cuda.synchronize()
@@ -861,8 +863,9 @@ def run_ours(args, rank: int, world: int):
                          f"FP64 C++ oracle, OpenMP ({dtc:.1f} s)", "histories_per_s": h}
     forms = fom = None
     if world == 1 and not args.no_forms:
-        forms = {"batched": form_batched(args.batch_steps, not args.no_tune),
-                 "batched_small": form_batched(10, not args.no_tune, n_inst=512, particle_scale=0.01),
+        forms = {"batched": form_batched(args.batch_steps, not args.no_tune, form=args.batch_form),
+                 "batched_small": form_batched(10, not args.no_tune, n_inst=512, particle_scale=0.01,
+                                               form=args.batch_form),
                  "adjoint": form_adjoint(),
                  "carter_forest": form_carter_forest(), "device_loop": form_device_loop(launch=dict(eng.launch)),
                  "mg_crooked_pipe": form_mg_crooked_pipe(), "other_configs": form_other_configs(),
@@ -922,6 +925,8 @@ def main():
                              "batched_small"],
                     help="run one further form alone on GPU 0 and print its JSON (no headline line)")
     ap.add_argument("--batch-steps", type=int, default=50, help="steps of the batched form (the workload's 50)")
+    ap.add_argument("--batch-form", type=int, default=0, choices=(0, 1, 2),
+                    help="batched tracking form: 0 the tuner's choice, 1 work units, 2 the entry queue")
     ap.add_argument("--no-fom", action="store_true")
     ap.add_argument("--fom-seeds", type=int, default=32)
     ap.add_argument("--fom-steps", type=int, default=100)
@@ -937,8 +942,10 @@ def main():
         import torch
 
         torch.cuda.set_device(0)
-        fn = {"batched": lambda: form_batched(args.batch_steps, not args.no_tune), "adjoint": form_adjoint,
-              "batched_small": lambda: form_batched(10, not args.no_tune, n_inst=512, particle_scale=0.01),
+        fn = {"batched": lambda: form_batched(args.batch_steps, not args.no_tune, form=args.batch_form),
+              "adjoint": form_adjoint,
+              "batched_small": lambda: form_batched(10, not args.no_tune, n_inst=512, particle_scale=0.01,
+                                                    form=args.batch_form),
               "carter_forest": form_carter_forest, "device_loop": form_device_loop,
               "mg_crooked_pipe": form_mg_crooked_pipe, "mg_crooked_pipe_run": form_mg_crooked_pipe_run,
               "other_configs": lambda: form_other_configs(tune=not args.no_tune),
