@@ -768,9 +768,12 @@ def run_ours(args, rank: int, world: int):
     eng = state._engine
     tuned = None
     if args.launch:
-        # a fixed launch shape (block, blocks per SM, chunk, smem cells), e.g. the tuner's choice
-        b, bps, ch, sm = (int(x) for x in args.launch.split(","))
-        eng.launch.update(block_size=b, blocks_per_sm=bps, chunk=ch, smem_cells=sm)
+        # a fixed launch shape (block, blocks per SM, chunk, smem cells[, prefetched refills]),
+        # e.g. the tuner's choice
+        vals = [int(x) for x in args.launch.split(",")]
+        b, bps, ch, sm = vals[:4]
+        eng.launch.update(block_size=b, blocks_per_sm=bps, chunk=ch, smem_cells=sm,
+                          prefetch=vals[4] if len(vals) > 4 else 0)
         launch_shape = dict(eng.launch)
         tuned = {"best_ms": None, "worst_ms": None, "trials": [], "fixed": args.launch}
     elif not args.no_tune:
@@ -916,7 +919,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--launch", default=None,
-                    help="fixed tracking launch shape 'block,blocks_per_sm,chunk,smem_cells' instead of tuning")
+                    help="fixed tracking launch shape 'block,blocks_per_sm,chunk,smem_cells[,prefetch]' instead of tuning")
     ap.add_argument("--tune-log", default=None, help="write the autotuner's trials to this JSON file")
     ap.add_argument("--no-forms", action="store_true", help="skip the batched and adjoint forms")
     ap.add_argument("--only-form", default=None,
@@ -925,8 +928,8 @@ def main():
                              "batched_small"],
                     help="run one further form alone on GPU 0 and print its JSON (no headline line)")
     ap.add_argument("--batch-steps", type=int, default=50, help="steps of the batched form (the workload's 50)")
-    ap.add_argument("--batch-form", type=int, default=0, choices=(0, 1, 2),
-                    help="batched tracking form: 0 the tuner's choice, 1 work units, 2 the entry queue")
+    ap.add_argument("--batch-form", type=int, default=0, choices=(0, 1, 2, 3),
+                    help="batched tracking form: 0 the tuner's choice, 1 work units, 2 the entry queue, 3 work units with prefetched refills")
     ap.add_argument("--no-fom", action="store_true")
     ap.add_argument("--fom-seeds", type=int, default=32)
     ap.add_argument("--fom-steps", type=int, default=100)

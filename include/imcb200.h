@@ -128,7 +128,9 @@ typedef struct imc_step_params {
                                    entries); bit 1: per-block tallies in shared memory with that
                                    table, bit 2: never (default: up to 2048 entries); bit 3:
                                    event-by-event tracking (workspace of imc_workspace_bytes_event);
-                                   others ignored */
+                                   bit 4: prefetched refills (each lane copies its next history's
+                                   bank record into shared memory while it tracks the current one;
+                                   the same histories and tallies); others ignored */
   const double* emission_fractions; /* MG: [g] fixed emission spectrum, or NULL = Planck */
   int64_t n_boundary_side[4];   /* > 0: boundary particles on that side instead of n_boundary
                                    (per-side budgets, MG_IMC/MG_IMC1D.py:1000-1040) */
@@ -496,8 +498,10 @@ typedef struct imc_batch_launch {  /* tracking kernel shape; 0 = default */
                                    and stages each instance's tables and tallies in shared memory;
                                    needs imc_batch.max_cells), 2 the entry queue (warps take entries
                                    of any instance, tables and tallies in global memory; for many
-                                   small instances), 0 the library's choice (work units when
-                                   max_cells allows) */
+                                   small instances), 3 work units with prefetched refills (each
+                                   lane copies its next history's bank record into shared memory
+                                   while it tracks the current one), 0 the library's choice (work
+                                   units when max_cells allows) */
 } imc_batch_launch;
 
 IMC_API size_t imc_batch_workspace_bytes(const imc_batch* b);

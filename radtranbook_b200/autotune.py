@@ -6,6 +6,8 @@ ticket and refill finished lanes at every event boundary.  Its speed depends on:
   blocks_per_sm  resident blocks requested per SM (grid = blocks_per_sm x SMs)
   chunk          histories claimed per warp ticket (refill cadence / bank tile)
   smem_cells     stage the per-cell (sigma_a, sigma_s) table in shared memory
+  prefetch       lanes copy their next history's bank record to shared memory ahead of need
+                 (not in the default grid: slower on every workload measured)
 The tuner replays the engine's last transport on a snapshot of the census bank for every
 candidate (the Philox streams make each trial the identical work), times the tracking
 phase with CUDA events, restores the census and installs the fastest shape.

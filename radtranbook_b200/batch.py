@@ -106,7 +106,8 @@ def slot_plan(spec: BatchSpec) -> tuple[np.ndarray, np.ndarray, int]:
 # --------------------------------------------------------------------------- engine
 # form: 1 work units (a block takes chunk x warps entries of one instance at a time and keeps
 # its cell table and tallies in shared memory), 2 the entry queue (warps take entries of any
-# instance; for many small instances); the engine's default follows the particles per instance
+# instance; for many small instances), 3 work units whose lanes prefetch their next history's
+# bank record into shared memory; the engine's default follows the particles per instance
 DEFAULT_LAUNCH = {"block_size": 256, "blocks_per_sm": 4, "chunk": 1024, "refill_min": 1, "form": 0}
 UNITS_MIN_PARTICLES = 20_000  # mean particles per instance from which work units are the default
 
@@ -275,7 +276,7 @@ TUNE_GRID = {
     "blocks_per_sm": (4, 8),
     "chunk": (256, 1024, 4096),
     "refill_min": (1, 4, 16),
-    "form": (1, 2),
+    "form": (1, 2),  # form 3 (prefetched refills) measured slower; selectable, not tuned
 }
 
 

@@ -365,6 +365,14 @@ __host__ __device__ inline size_t units_smem(int K, int M) {
   return sizeof(long long) * (size_t)(K + 1) + (size_t)M * (8 + 8 + 8 + 8) + sizeof(float) * (size_t)(M + 1);
 }
 
+// Prefetched refills (form 3): every lane holds the bank record of its next history in a
+// shared-memory slot, copied there by cp.async while it tracks the current one, so a lane whose
+// history ends takes its next one from shared memory instead of stalling the warp on two
+// dependent HBM reads (weight and birth time, then position, direction and cell).
+constexpr int PF_FIELDS = 6;  // w, t, x, u, cell, entry index inside the instance
+__host__ __device__ inline size_t units_pf_smem(int block) { return sizeof(float) * PF_FIELDS * (size_t)block; }
+
+template <bool PF>
 __global__ void __launch_bounds__(256, 5) k_btrack_units(BatchArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ unsigned blk_cnt[B_N];
@@ -377,6 +385,10 @@ __global__ void __launch_bounds__(256, 5) k_btrack_units(BatchArgs a) {
   double* CF = TS + M;                                                                  // [M] cellf.y
   float2* SS = reinterpret_cast<float2*>(CF + M);                                       // [M] (sa, ss)
   float* EF = reinterpret_cast<float*>(SS + M);                                         // [M+1] edges
+  // PF: the lane's next bank record, field f of thread i at PQ[f * blockDim.x + i]
+  float* PQ = reinterpret_cast<float*>(smem + units_smem(a.K, M));
+  float* const my_pf = PQ + threadIdx.x;
+  const int pf_stride = blockDim.x;
   if (threadIdx.x < B_N) blk_cnt[threadIdx.x] = 0u;
   load_pref(pref, a.live_pref, a.K);
 
@@ -428,6 +440,7 @@ __global__ void __launch_bounds__(256, 5) k_btrack_units(BatchArgs a) {
       const long long pk = pref[k], so = a.slot_off[k];
       unsigned long long ev_acc = 0ull;
       bool has = false, drained = false;
+      bool pv = false;  // PF: the lane's slot holds a claimed record (copy issued)
       long long pid = 0;
       uint32_t lid = 0, ev = 0;
       int ci = 0;
@@ -436,7 +449,56 @@ __global__ void __launch_bounds__(256, 5) k_btrack_units(BatchArgs a) {
       double acc_wd = 0.0;  // w*s in the current cell (cells without absorption only)
       for (;;) {
         // ---- refill idle lanes from the block's cursor over [q0, q1) ----
-        unsigned need = __ballot_sync(FULL, !has);
+        if (PF) {
+          // An idle lane takes the record in its slot; every lane without a claimed record
+          // claims the next entry of the unit (one shared atomic per warp) and starts its copy.
+          // Leaves with every lane either tracking or holding no claim; at the unit's end the
+          // cursor is past q1 and no claim is left untaken.
+          for (;;) {
+            if (!has && pv) {
+              cp_async_wait_all();
+              pv = false;
+              lid = __float_as_uint(my_pf[5 * pf_stride]);
+              pid = so + lid;
+              w = my_pf[0];
+              dcen = (dt - my_pf[pf_stride]) * c_light;
+              if (w > 0.f && dcen > 0.f) {
+                x = my_pf[2 * pf_stride]; u = my_pf[3 * pf_stride]; ci = __float_as_int(my_pf[4 * pf_stride]);
+                ev = 0;
+                w_in = w;
+                has = true;
+              }
+            }
+            if (!drained) {
+              const unsigned pneed = __ballot_sync(FULL, !pv);
+              if (pneed) {
+                unsigned long long b0 = 0;
+                if (lane == 0) b0 = atomicAdd(&s_cur, (unsigned long long)__popc(pneed));
+                b0 = __shfl_sync(FULL, b0, 0);
+                if (b0 >= q1) {
+                  drained = true;
+                } else {
+                  const unsigned rank = __popc(pneed & lt_mask);
+                  if (!pv && b0 + rank < q1) {
+                    const uint32_t nl = (uint32_t)((long long)(b0 + rank) - pk);
+                    const long long np = so + nl;
+                    my_pf[5 * pf_stride] = __uint_as_float(nl);
+                    cp_async4(my_pf, B.w + np);
+                    cp_async4(my_pf + pf_stride, B.t + np);
+                    cp_async4(my_pf + 2 * pf_stride, B.p1 + np);
+                    cp_async4(my_pf + 3 * pf_stride, B.d1 + np);
+                    cp_async4(my_pf + 4 * pf_stride, B.cell + np);
+                    cp_async_commit();
+                    pv = true;
+                  }
+                }
+              }
+            }
+            if (!__any_sync(FULL, !has && pv)) break;
+          }
+          if (!__any_sync(FULL, has)) break;
+        }
+        unsigned need = PF ? 0u : __ballot_sync(FULL, !has);
         while (need && !drained) {
           unsigned long long b0 = 0;
           if (lane == 0) b0 = atomicAdd(&s_cur, (unsigned long long)__popc(need));
@@ -794,12 +856,14 @@ cudaError_t imc_batch_launch_wsum(const BatchArgs& a, cudaStream_t s) {
 cudaError_t imc_batch_launch_track(const BatchArgs& a, int block, int grid, cudaStream_t s) {
   ++g_imc_launches;
   if (a.form != 2 && a.max_cells > 0 && a.max_cells <= IMC_BATCH_SMEM_CELLS) {
-    const size_t sh = units_smem(a.K, a.max_cells);
+    const bool pf = a.form == 3;
+    const size_t sh = units_smem(a.K, a.max_cells) + (pf ? units_pf_smem(block) : 0);
+    auto kern = pf ? k_btrack_units<true> : k_btrack_units<false>;
     if (sh > 48 * 1024) {
-      const cudaError_t e = cudaFuncSetAttribute(k_btrack_units, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+      const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
       if (e != cudaSuccess) return e;
     }
-    k_btrack_units<<<grid, block, sh, s>>>(a);
+    kern<<<grid, block, sh, s>>>(a);
     return cudaGetLastError();
   }
   const size_t sh = (size_t)(block / 32) * sizeof(WarpStage) + pref_bytes(a);

@@ -431,6 +431,8 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
   // memory, bit 2 = never (default: with the staged table up to 2048 (group, cell) entries)
   const bool smem_cells = (par->reserved & 1) ? true : ((long long)nc * ng <= 4096);
   const bool smem_tally = smem_cells && !(par->reserved & 4) && ((par->reserved & 2) || (long long)nc * ng <= 2048);
+  // bit 4: prefetched refills (each lane's next bank record copied to shared memory ahead)
+  const bool prefetch = (par->reserved & 16) != 0;
   if (adj) {
     AdjointArgs A = *adj;
     A.t = ta; A.sa64 = tal->sigma_a; A.ss64 = tal->sigma_s; A.sig64 = mat->sigma;
@@ -444,7 +446,7 @@ imc_status transport_async(const imc_mesh* mesh, const imc_material* mat, const 
                                     n_upper, block, sm_count(), ta.max_events + 2, &cap_hit, s));
     if (cap_hit) return IMC_ERR_EVENT_CAP;
   } else {
-    IMC_CUDA(imc_launch_track(ta, mesh->geometry, block, sm_count() * bps, smem_cells, smem_tally, s));
+    IMC_CUDA(imc_launch_track(ta, mesh->geometry, block, sm_count() * bps, smem_cells, smem_tally, prefetch, s));
   }
   if (pe.ok) { IMC_CUDA(cudaEventRecord(pe.e[2], s)); pe.recorded = true; }
   IMC_CUDA(imc_launch_tally_finalize(ta, s));

@@ -132,6 +132,15 @@ __device__ __forceinline__ float inner_root(float r, float mu, float R, float b2
 // one FP64 red per tally.
 struct WarpStage { double a[32]; double b[32]; };
 
+// Asynchronous 4-byte global -> shared copies (cp.async): a thread starts the copies of a bank
+// record it will need later and waits for its own copies only when it reads them.
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 __device__ __forceinline__ void warp_tally2(bool flush, int key, double va, double vb,
                                             double* __restrict__ ta, double* __restrict__ tb,
                                             WarpStage* st) {

@@ -55,9 +55,10 @@ struct TrackArgs {
   int ecen_by_group;
 };
 
-// smem_tally: per-block deposition / intensity tallies in shared memory (with smem_cells only)
+// smem_tally: per-block deposition / intensity tallies in shared memory (with smem_cells only);
+// prefetch: lanes copy their next history's bank record into shared memory while they track
 cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool smem_cells, bool smem_tally,
-                             cudaStream_t s);
+                             bool prefetch, cudaStream_t s);
 // Event-by-event tracking (reserved bit 3 of imc_step_params): scratch bytes for a bank of
 // `capacity` entries, and the launch loop (synchronises the stream every 8 launches to read the
 // live count; *cap_hit when more than max_launches launches would be needed)

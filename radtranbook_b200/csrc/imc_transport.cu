@@ -332,8 +332,17 @@ __device__ __forceinline__ void history_event(const TrackArgs& a, Hist& h, EvOut
 // (group, cell) in shared memory and adds them to the global tallies once, at its end.  On a
 // mesh of a few hundred cells every crossing would otherwise send its reductions to the few
 // dozen cells the wave occupies, which serialise in the L2.
-template <int GEOM, bool SMEM_CELLS, bool MG, bool CF, bool SMEM_TALLY>
-__global__ void __launch_bounds__(256) k_track(TrackArgs a) {
+//
+// PF (prefetched refills): every lane keeps the bank record of its next history in a
+// shared-memory slot, copied there by cp.async while it tracks the current one, so a lane
+// whose history ends starts the next one from shared memory instead of holding its warp on two
+// dependent HBM reads (weight and birth time, then the rest of the record).  The histories,
+// their Philox counters and the tallies are the same; only which lane tracks which differs.
+enum : int { PF_W = 0, PF_T, PF_P1, PF_D1, PF_CELL, PF_P2, PF_D2, PF_GROUP, PF_PID, PF_NF };
+inline size_t pf_smem(int block) { return sizeof(float) * PF_NF * (size_t)block; }
+
+template <int GEOM, bool SMEM_CELLS, bool MG, bool CF, bool SMEM_TALLY, bool PF>
+__global__ void __launch_bounds__(256, PF ? 4 : 1) k_track(TrackArgs a) {  // PF: at most 64 registers
   pdl_wait();     // the previous kernel of the stream has completed
   pdl_trigger();  // the next one may be scheduled
   const float dtk = a.dt_dev ? (float)*a.dt_dev : a.dt;  // graph replay: step length and Philox
@@ -395,9 +404,104 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   const double inv_q = fx_inv_quantum(*a.wsum);  // fixed-point energy tallies
   const float inv_nx = 1.0f / (float)a.nx;  // cell -> (i, j) at refill without an integer divide
 
+  // PF: the lane's next bank record, field f of thread i at PQ[f * blockDim.x + i] (after the
+  // block tallies, or after the cell table without them)
+  float* const my_pf = (SMEM_TALLY ? reinterpret_cast<float*>(TS + ncg) : reinterpret_cast<float*>(TD)) + threadIdx.x;
+  const int pfs = blockDim.x;
+  bool pv = false;  // PF: the slot holds a claimed record (copies issued)
+
   for (;;) {
     // ---------------- refill idle lanes from the warp's chunk ----------------
-    unsigned need = __ballot_sync(FULL, !has);
+    if (PF) {
+      // An idle lane takes the record in its slot; every lane without a claim takes the next
+      // entry of the warp's chunk (a new guided ticket when it runs out) and starts its copies,
+      // which land while the lane tracks.  Leaves with every lane tracking or holding no claim;
+      // when the warp stops, the queue is past n and no claim is left untaken.
+      for (;;) {
+        if (!has && pv) {
+          cp_async_wait_all();
+          pv = false;
+          pid = __float_as_uint(my_pf[PF_PID * pfs]);
+          w = my_pf[0];
+          dcen = (dtk - my_pf[pfs]) * c_light;
+          const int c = __float_as_int(my_pf[PF_CELL * pfs]);
+          const int g = MG ? __float_as_int(my_pf[PF_GROUP * pfs]) : 0;
+          const bool moves = (MG2 || CF ? w > weight_floor : w > 0.f) && dcen > 0.f;
+          if (!moves && w > 0.f && a.ecen) {
+            const int b = c + (a.ecen_by_group ? a.nc * g : 0);
+#ifdef IMC_CHECKED
+            if (b >= 0 && b < a.nc * (a.ecen_by_group ? a.ng : 1))
+#endif
+            { atomicAdd(a.ecen + b, (double)w); ++n_alive; }
+          }
+          if (moves) {
+            x = my_pf[2 * pfs]; u = my_pf[3 * pfs];
+            if (MG) grp = g;
+            if (GEOM == G_XY || GEOM == G_RZ) { y = my_pf[PF_P2 * pfs]; v = my_pf[PF_D2 * pfs]; }
+#ifdef IMC_CHECKED
+            if (c < 0 || c >= a.nc || (MG && (grp < 0 || grp >= a.ng)) || !isfinite(w)) {
+              atomicOr(a.flags, (int)IMC_FLAG_BOUNDS);
+            } else
+#endif
+            {
+              cj = __float2int_rd(((float)c + 0.5f) * inv_nx);
+              ci = c - cj * a.nx;
+              if (ci < 0) { --cj; ci += a.nx; } else if (ci >= a.nx) { ++cj; ci -= a.nx; }
+              tab = table(MG ? c + a.nc * grp : c);
+              ev = 0;
+              w_in = w;
+              has = true;
+            }
+          }
+        }
+        if (!drained) {
+          const unsigned pneed = __ballot_sync(FULL, !pv);
+          if (pneed) {
+            if (chunk_next >= chunk_end) {
+              unsigned long long base = 0, claim = 0;
+              if (lane == 0) {
+                const unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(a.queue);
+                const unsigned long long left = cur < (unsigned long long)n ? (unsigned long long)n - cur : 0ull;
+                const unsigned long long nw = (unsigned long long)gridDim.x * (blockDim.x >> 5);
+                claim = min((unsigned long long)a.chunk, max(32ull, left / (2ull * nw)));
+                base = atomicAdd(a.queue, claim);
+              }
+              base = __shfl_sync(FULL, base, 0);
+              claim = __shfl_sync(FULL, claim, 0);
+              if (base >= (unsigned long long)n) {
+                drained = true;
+              } else {
+                chunk_next = (uint32_t)base;
+                chunk_end = (uint32_t)min(base + claim, (unsigned long long)n);
+              }
+            }
+            if (!drained) {
+              const uint32_t avail = chunk_end - chunk_next;
+              const uint32_t rank = __popc(pneed & lt_mask);
+              if (!pv && rank < avail) {
+                const uint32_t np = chunk_next + rank;
+                my_pf[PF_PID * pfs] = __uint_as_float(np);
+                cp_async4(my_pf, a.w + np);
+                cp_async4(my_pf + pfs, a.t + np);
+                cp_async4(my_pf + 2 * pfs, a.p1 + np);
+                cp_async4(my_pf + 3 * pfs, a.d1 + np);
+                cp_async4(my_pf + PF_CELL * pfs, a.cell + np);
+                if (GEOM == G_XY || GEOM == G_RZ) {
+                  cp_async4(my_pf + PF_P2 * pfs, a.p2 + np);
+                  cp_async4(my_pf + PF_D2 * pfs, a.d2 + np);
+                }
+                if (MG) cp_async4(my_pf + PF_GROUP * pfs, a.group + np);
+                cp_async_commit();
+                pv = true;
+              }
+              chunk_next += min((uint32_t)__popc(pneed), avail);
+            }
+          }
+        }
+        if (!__any_sync(FULL, !has && pv)) break;
+      }
+    }
+    unsigned need = PF ? 0u : __ballot_sync(FULL, !has);
     while (need && !drained) {
       if (chunk_next >= chunk_end) {
         // guided claim: a share of what is left, at most `chunk`, at least 32, so early
@@ -533,27 +637,34 @@ __global__ void __launch_bounds__(256) k_track(TrackArgs a) {
   }
 }
 
-template <int GEOM, bool SM, bool MG, bool CF, bool ST>
+template <int GEOM, bool SM, bool MG, bool CF, bool ST, bool PF>
 cudaError_t launch_one(const TrackArgs& a, int block, int grid, cudaStream_t s) {
   const int nwarps = block / 32;
   size_t sh = nwarps * sizeof(WarpStage) + sizeof(float) * (a.nx + a.ny + 4);
   if (SM) sh += sizeof(float2) * a.nc * a.ng;
   if (ST) sh += (sizeof(unsigned long long) + sizeof(double)) * a.nc * a.ng;
+  if (PF) sh += pf_smem(block);
   if (sh > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_track<GEOM, SM, MG, CF, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sh);
+    cudaError_t e = cudaFuncSetAttribute(k_track<GEOM, SM, MG, CF, ST, PF>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
     if (e != cudaSuccess) return e;
   }
-  IMC_LAUNCH_PDL(k_track<GEOM, SM, MG, CF, ST>, grid, block, sh, s, a);
+  IMC_LAUNCH_PDL((k_track<GEOM, SM, MG, CF, ST, PF>), grid, block, sh, s, a);
   return cudaGetLastError();
 }
 
 // the block tallies are built only with the shared-memory cell table (small meshes)
+template <int GEOM, bool MG, bool CF, bool PF>
+cudaError_t launch_pf(const TrackArgs& a, int block, int grid, bool sm, bool st, cudaStream_t s) {
+  if (sm && st) return launch_one<GEOM, true, MG, CF, true, PF>(a, block, grid, s);
+  return sm ? launch_one<GEOM, true, MG, CF, false, PF>(a, block, grid, s)
+            : launch_one<GEOM, false, MG, CF, false, PF>(a, block, grid, s);
+}
+
 template <int GEOM, bool MG, bool CF = false>
-cudaError_t launch_geom(const TrackArgs& a, int block, int grid, bool sm, bool st, cudaStream_t s) {
-  if (sm && st) return launch_one<GEOM, true, MG, CF, true>(a, block, grid, s);
-  return sm ? launch_one<GEOM, true, MG, CF, false>(a, block, grid, s)
-            : launch_one<GEOM, false, MG, CF, false>(a, block, grid, s);
+cudaError_t launch_geom(const TrackArgs& a, int block, int grid, bool sm, bool st, bool pf, cudaStream_t s) {
+  return pf ? launch_pf<GEOM, MG, CF, true>(a, block, grid, sm, st, s)
+            : launch_pf<GEOM, MG, CF, false>(a, block, grid, sm, st, s);
 }
 
 // ---------------------------------------------------------------------------------
@@ -810,30 +921,31 @@ cudaError_t imc_run_event_tracking(const TrackArgs& a, int geom, void* scratch, 
   return cudaSuccess;
 }
 
-cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool sm, bool st, cudaStream_t s) {
+cudaError_t imc_launch_track(const TrackArgs& a, int geom, int block, int grid, bool sm, bool st, bool pf,
+                             cudaStream_t s) {
   ++g_imc_launches;
   if (a.ng > 1) {  // multigroup: 2-D (MG_IMC/MG_IMC2D.py) and the 1-D sphere (MG_IMC/MG_IMC1D.py)
     switch (geom) {
-      case G_SPHERE: return launch_geom<G_SPHERE, true>(a, block, grid, sm, st, s);
-      case G_XY: return launch_geom<G_XY, true>(a, block, grid, sm, st, s);
-      case G_RZ: return launch_geom<G_RZ, true>(a, block, grid, sm, st, s);
+      case G_SPHERE: return launch_geom<G_SPHERE, true>(a, block, grid, sm, st, pf, s);
+      case G_XY: return launch_geom<G_XY, true>(a, block, grid, sm, st, pf, s);
+      case G_RZ: return launch_geom<G_RZ, true>(a, block, grid, sm, st, pf, s);
       default: return cudaErrorInvalidValue;
     }
   }
   if (a.cf_rate) {  // Carter-Forest, gray
     switch (geom) {
-      case G_SLAB: return launch_geom<G_SLAB, false, true>(a, block, grid, sm, st, s);
-      case G_SPHERE: return launch_geom<G_SPHERE, false, true>(a, block, grid, sm, st, s);
-      case G_XY: return launch_geom<G_XY, false, true>(a, block, grid, sm, st, s);
-      case G_RZ: return launch_geom<G_RZ, false, true>(a, block, grid, sm, st, s);
+      case G_SLAB: return launch_geom<G_SLAB, false, true>(a, block, grid, sm, st, pf, s);
+      case G_SPHERE: return launch_geom<G_SPHERE, false, true>(a, block, grid, sm, st, pf, s);
+      case G_XY: return launch_geom<G_XY, false, true>(a, block, grid, sm, st, pf, s);
+      case G_RZ: return launch_geom<G_RZ, false, true>(a, block, grid, sm, st, pf, s);
       default: return cudaErrorInvalidValue;
     }
   }
   switch (geom) {
-    case G_SLAB: return launch_geom<G_SLAB, false>(a, block, grid, sm, st, s);
-    case G_SPHERE: return launch_geom<G_SPHERE, false>(a, block, grid, sm, st, s);
-    case G_XY: return launch_geom<G_XY, false>(a, block, grid, sm, st, s);
-    case G_RZ: return launch_geom<G_RZ, false>(a, block, grid, sm, st, s);
+    case G_SLAB: return launch_geom<G_SLAB, false>(a, block, grid, sm, st, pf, s);
+    case G_SPHERE: return launch_geom<G_SPHERE, false>(a, block, grid, sm, st, pf, s);
+    case G_XY: return launch_geom<G_XY, false>(a, block, grid, sm, st, pf, s);
+    case G_RZ: return launch_geom<G_RZ, false>(a, block, grid, sm, st, pf, s);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -360,6 +360,9 @@ class Engine:
         # bit 3: the event-by-event form of the tracking (launch["event_based"] = 1)
         if self.launch.get("event_based"):
             par.reserved |= 8
+        # bit 4: prefetched refills (launch["prefetch"] = 1)
+        if self.launch.get("prefetch"):
+            par.reserved |= 16
         par.emission_fractions = _ptr(self.emission_fractions)
         for q, n in enumerate(n_boundary_side or ()):
             par.n_boundary_side[q] = int(n)

@@ -24,7 +24,7 @@ def _rel_l1(a, b):
     return np.abs(a - b).sum() / max(np.abs(b).sum(), 1e-300)
 
 
-@pytest.mark.parametrize("form", [1, 2])  # work units (tables staged per instance), the entry queue
+@pytest.mark.parametrize("form", [1, 2, 3])  # work units (tables staged per instance), the entry queue, prefetched work units
 def test_batch_instances_reproduce_single_problem_runs(cuda, form):
     spec = _small()
     eng = batch.BatchEngine(spec)
