@@ -928,6 +928,8 @@ def main():
                              "batched_small"],
                     help="run one further form alone on GPU 0 and print its JSON (no headline line)")
     ap.add_argument("--batch-steps", type=int, default=50, help="steps of the batched form (the workload's 50)")
+    ap.add_argument("--batch-instances", type=int, default=256,
+                    help="instances of the batched form (the workload's 256; fewer for a small profiling case)")
     ap.add_argument("--batch-form", type=int, default=0, choices=(0, 1, 2, 3),
                     help="batched tracking form: 0 the tuner's choice, 1 work units, 2 the entry queue, 3 work units with prefetched refills")
     ap.add_argument("--no-fom", action="store_true")
@@ -945,7 +947,8 @@ def main():
         import torch
 
         torch.cuda.set_device(0)
-        fn = {"batched": lambda: form_batched(args.batch_steps, not args.no_tune, form=args.batch_form),
+        fn = {"batched": lambda: form_batched(args.batch_steps, not args.no_tune, n_inst=args.batch_instances,
+                                             form=args.batch_form),
               "adjoint": form_adjoint,
               "batched_small": lambda: form_batched(10, not args.no_tune, n_inst=512, particle_scale=0.01,
                                                     form=args.batch_form),
