@@ -376,8 +376,8 @@ template <bool PF>
 __global__ void __launch_bounds__(256, 5) k_btrack_units(BatchArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ unsigned blk_cnt[B_N];
-  __shared__ unsigned long long s_base, s_cur;
-  __shared__ uint32_t s_rk[20];  // Philox round keys of the staged instance's seed
+  __shared__ unsigned long long s_base, s_cur, s_unit;
+  __shared__ __align__(16) uint32_t s_rk[20];  // Philox round keys of the staged instance's seed
   const int M = a.max_cells;
   long long* pref = reinterpret_cast<long long*>(smem);                                 // [K+1]
   unsigned long long* TD = reinterpret_cast<unsigned long long*>(pref + (a.K + 1));    // [M] deposition
@@ -404,11 +404,25 @@ __global__ void __launch_bounds__(256, 5) k_btrack_units(BatchArgs a) {
   int cur_k = -1, cur_nc = 0, cur_cb = 0;  // block-uniform: the instance whose tallies are staged
 
   for (;;) {
-    if (threadIdx.x == 0) s_base = atomicAdd(a.queue, unit);
+    if (threadIdx.x == 0) {
+      // full units while at least one per block is left; after that the rest shared over the
+      // blocks (a multiple of 32, at least one row per warp), so the blocks finish together
+      // instead of the last full units running on a few SMs
+      unsigned long long u = unit;
+      const unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(a.queue);
+      const unsigned long long left = cur < n ? n - cur : 0ull;
+      const unsigned long long nb = gridDim.x;
+      if (left < nb * unit) {
+        const unsigned long long floor_u = 32ull * (blockDim.x >> 5);
+        u = min(unit, max(floor_u, (left / nb + 31ull) & ~31ull));
+      }
+      s_unit = u;
+      s_base = atomicAdd(a.queue, u);
+    }
     __syncthreads();
     const unsigned long long base = s_base;
     if (base >= n) break;  // uniform: every thread read the same claim
-    const unsigned long long end = min(base + unit, n);
+    const unsigned long long end = min(base + s_unit, n);
     for (unsigned long long q0 = base; q0 < end;) {
       const int k = find_inst(pref, a.K, (long long)q0);
       const unsigned long long q1 = min(end, (unsigned long long)pref[k + 1]);
@@ -532,7 +546,7 @@ __global__ void __launch_bounds__(256, 5) k_btrack_units(BatchArgs a) {
             atomicOr(a.flags, (int)IMC_FLAG_EVENT_CAP);
             finished = true;
           } else {
-            const U4 r = draw_rk(s_rk, lid, ev, step, TAG_TRANSPORT);
+            const U4 r = draw_rk4(reinterpret_cast<const uint4*>(s_rk), lid, ev, step, TAG_TRANSPORT);
             ++ev;
             const float xl = EF[ci], xr = EF[ci + 1];
             const float L = xr - xl;

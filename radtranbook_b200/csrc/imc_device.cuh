@@ -77,6 +77,25 @@ __device__ __forceinline__ U4 draw_rk(const uint32_t* rk, uint32_t idx, uint32_t
   return c;
 }
 
+// draw_rk with the round keys read as five 16-byte words (rk4: the 20 keys of
+// philox_round_keys, 16-byte aligned, e.g. staged in shared memory): the same numbers, five
+// vector loads where draw_rk makes twenty scalar ones.
+__device__ __forceinline__ U4 draw_rk4(const uint4* rk4, uint32_t idx, uint32_t block, uint32_t step,
+                                       uint32_t tag) {
+  U4 c{idx, block, step, tag};
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    const uint4 k = rk4[q];
+    const uint32_t a0 = 0xD2511F53u * c.x, b0 = __umulhi(0xD2511F53u, c.x);
+    const uint32_t a1 = 0xCD9E8D57u * c.z, b1 = __umulhi(0xCD9E8D57u, c.z);
+    c = U4{b1 ^ c.y ^ k.x, a1, b0 ^ c.w ^ k.y, a0};
+    const uint32_t e0 = 0xD2511F53u * c.x, f0 = __umulhi(0xD2511F53u, c.x);
+    const uint32_t e1 = 0xCD9E8D57u * c.z, f1 = __umulhi(0xCD9E8D57u, c.z);
+    c = U4{f1 ^ c.y ^ k.z, e1, f0 ^ c.w ^ k.w, e0};
+  }
+  return c;
+}
+
 // Word q (0..3) of a Philox block: the comb's uniform of pre-comb entry k is word k % 4 of
 // block (k / 4, 1), so four consecutive entries share one block.
 __device__ __forceinline__ uint32_t u4_word(const U4& r, int q) {
